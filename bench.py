@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the plain per-frame GI path (trace + temporal + 3x a-trous +
+present) on the full-size workload: 256^3 world (seed 2), 1920x1080, 1 spp,
+2 indirect bounces, firefly clamp 10, along the 120-frame camera spline.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one frame.  Device time per frame comes from CUDA events the
+library records on its own stream around its kernels; the L2 is flushed (a
+256 MB write) before every timed frame, outside the events.  `value` is
+Mrays/s over all ranks (rays = trace invocations: primary + bounce + shadow).
+N > 1 runs independent replicas (one per GPU, no collective on the data
+path); the reported time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s & 1080p frame ms, plain vs batched+cache at equal MSE; p50/p99 latency"
+WORKLOAD = dict(kind=2, n=256, seed=2, W=1920, H=1080, bounces=2, fclamp=10.0, maxhist=64.0, flags=3, path_frames=120)
+WORKLOAD_NAME = ("plain GI frame (pathtrace+temporal+3x a-trous+present): 256^3 procedural world seed 2, "
+                 "1920x1080, 1 spp, 2 bounces, clamp 10, 120-frame camera spline")
+ALG_BYTES_PER_PX = 28          # pathtrace writes: radiance 8 + albedo 4 + G-buffer 16
+FRAME_BYTES_PER_PX = 196       # all passes, compulsory (pathtrace 28, temporal 56, a-trous 96, present 16)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per path-trace launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "pathtrace_1080p_256.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def frame_uniforms(vrt, spawn, f):
+    W, H = WORKLOAD["W"], WORKLOAD["H"]
+    k = f % WORKLOAD["path_frames"]
+    pose = vrt.camera_spline(spawn, k)
+    prev = vrt.camera_spline(spawn, k - 1) if k > 0 else None
+    return vrt.make_uniforms(pose, prev, vrt.Lighting(), f, WORKLOAD["bounces"], WORKLOAD["flags"], W, H, 1.0,
+                             WORKLOAD["maxhist"])
+
+
+def cpu_baseline_port(vox, spawn, vrt):
+    """The CPU oracle (scalar restatement of the same path, OpenMP over rows)
+    on one full frame of the workload: pathtrace + temporal + 3x a-trous + present."""
+    import numpy as np
+
+    import oracle
+    n, W, H = WORKLOAD["n"], WORKLOAD["W"], WORKLOAD["H"]
+    b, m = oracle.build_bricks(vox, n)
+    u = frame_uniforms(vrt, spawn, 0)
+    acc = np.zeros((H, W, 4), np.uint16)
+    g = np.zeros((H, W, 4), np.float32)
+    t0 = time.perf_counter()
+    r = oracle.frame(vox, b, m, n, vrt.uniforms_bytes(u), WORKLOAD["fclamp"], W, H, acc, g)
+    dt = time.perf_counter() - t0
+    rays = r["stats"]["rays"]
+    return {"value": round(rays / dt / 1e6, 3), "unit": "Mrays/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"1 full frame ({rays} rays) of the workload through the CPU oracle "
+                      f"(pathtrace+temporal+3x a-trous+present), {dt:.2f} s",
+            "frame_ms": round(dt * 1e3, 1)}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+    from voxelrt_b200._lib import lib as vlib
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    n, W, H = WORKLOAD["n"], WORKLOAD["W"], WORKLOAD["H"]
+    vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
+    ctx = vrt.Context(local)
+    scene = vrt.Scene(ctx, vox, n)
+    sess = vrt.Session(ctx, scene, W, H, firefly_clamp=WORKLOAD["fclamp"], accum_f32=False)
+    sess.set_timing(True)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+
+    for i in range(args.warmup):
+        sess.frame(frame_uniforms(vrt, spawn, i))
+        sess.stats()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    frame_ms, pt_ms, rays, dda_bytes, pixels, launches = [], [], 0, 0, 0, 0
+    for i in range(args.steps):
+        f = args.warmup + i
+        u = frame_uniforms(vrt, spawn, f)
+        flush.zero_()
+        torch.cuda.synchronize()
+        sess.frame(u)
+        st = sess.stats()
+        frame_ms.append(st.ms_total)
+        pt_ms.append(st.ms_pathtrace)
+        rays += st.rays
+        dda_bytes += 4 * (st.dda_outer + st.dda_inner + st.voxel_reads)
+        pixels += st.pixels
+        launches += st.launches
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = sum(frame_ms)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        r = torch.tensor([float(rays)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        total_ms_max, rays_all = float(t.item()), float(r.item())
+    else:
+        total_ms_max, rays_all = total_ms, float(rays)
+
+    # ---- end to end through the C ABI: host uniforms in, LDR frame out ----
+    ldr_host = torch.empty(W * H * 4, dtype=torch.uint8, pin_memory=True)
+    e2e_rays, e2e_s = 0, 0.0
+    for i in range(args.steps):
+        u = frame_uniforms(vrt, spawn, args.warmup + args.steps + i)
+        t0 = time.perf_counter()
+        sess.frame(u)
+        code = vlib.vrt_read_ldr(sess.h, ldr_host.data_ptr(), W * H * 4)
+        e2e_s += time.perf_counter() - t0
+        if code:
+            raise RuntimeError(vlib.vrt_last_error_string().decode())
+        e2e_rays += sess.stats().rays
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(r, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_rays = float(t.item()), float(r.item())
+
+    peak, peak_kind = measured_peaks()
+    alg_bytes = dda_bytes + ALG_BYTES_PER_PX * pixels
+    achieved = alg_bytes / (sum(pt_ms) / 1e3) / 1e9
+    traffic = profiled_traffic()
+    line = {
+        "metric": METRIC,
+        "value": round(rays_all / (total_ms_max / 1e3) / 1e6, 2),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms_max / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded procedural voxel world and camera path)",
+        "config": {"workload": WORKLOAD_NAME, "grid": n, "width": W, "height": H, "spp": 1,
+                   "bounces": WORKLOAD["bounces"], "history": "rgba16f, cap 64", "denoise": "a-trous 1/2/4",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
+        "frame_ms": {"mean": round(statistics.mean(frame_ms), 4),
+                     "p50": round(statistics.median(frame_ms), 4),
+                     "p99": round(float(np.percentile(frame_ms, 99)), 4)},
+        "pass_ms_mean": {"pathtrace": round(statistics.mean(pt_ms), 4)},
+        "rays_per_frame": round(rays / args.steps),
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_pathtrace", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": round(alg_bytes / args.steps),
+                     "note": "algorithmic bytes = 4*(brick words + mask words + voxel words read) over all rays "
+                             "+ 28 B/pixel written; the DDA working set is L2-resident"},
+        "e2e": {"value": round(e2e_rays / e2e_s / 1e6, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 304,
+                "d2h_bytes_per_step": W * H * 4,
+                "note": "vrt_frame (uniform block from the host) + vrt_read_ldr into pinned host memory, "
+                        "host wall clock per frame"},
+    }
+    if clk:
+        line["clocks"] = clk
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port(vox, spawn, vrt)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sess.close()
+    scene.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, world, rank):
+    """The reference's own CPU traversal (VoxelBench/pipeline/core.cpp:52-130
+    `trace`, compiled from the reference sources into oracle/_ref) replaying the
+    rays this workload traces (primary, bounce, sun shadow) on all host cores;
+    the CPU oracle's full path is used when that library is absent."""
+    if rank != 0:
+        return
+    import ctypes as C
+
+    import numpy as np
+
+    import oracle
+    import voxelrt_b200 as vrt
+    n, W, H = WORKLOAD["n"], WORKLOAD["W"], WORKLOAD["H"]
+    vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
+    threads = os.cpu_count() or 1
+    vb = oracle.ref_lib()
+    base = {"impl": "reference", "metric": METRIC, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural voxel world and camera path)",
+            "config": {"workload": WORKLOAD_NAME, "grid": n, "width": W, "height": H, "spp": 1,
+                       "bounces": WORKLOAD["bounces"], "history": "rgba16f, cap 64", "denoise": "a-trous 1/2/4",
+                       "parallelism": "host CPU"}}
+    b, m = oracle.build_bricks(vox, n)
+    if vb is not None:
+        occ = (vox != 0).astype(np.uint8)
+        assert vb.vb_set_grid(n, n, n, C.c_void_p(occ.ctypes.data)) == 0
+        row_step = 4
+        per_step = []
+        nrays = 0
+        for i in range(args.warmup + args.steps):
+            u = frame_uniforms(vrt, spawn, i)
+            rays = oracle.collect_rays(vox, b, m, n, vrt.uniforms_bytes(u), WORKLOAD["fclamp"], W, H,
+                                       i % row_step, H, row_step)
+            o = np.ascontiguousarray(rays[:, 0:3])
+            d = np.ascontiguousarray(rays[:, 3:6])
+            t = np.ascontiguousarray(rays[:, 6])
+            secs = vb.vb_time_trace(C.c_void_p(o.ctypes.data), C.c_void_p(d.ctypes.data), C.c_void_p(t.ctypes.data),
+                                    C.c_int(len(o)), C.c_int(threads))
+            if i >= args.warmup:
+                per_step.append(secs)
+                nrays += len(o)
+        secs = sum(per_step)
+        value = nrays / secs / 1e6
+        sample = (f"VoxelBench trace() (4^3 brickmap DDA, core.cpp:52-130) on the workload's occupancy grid, "
+                  f"replaying each frame's rays (every {row_step}th row: {nrays // args.steps} rays per step)")
+        kind = "reference"
+    else:
+        per_step = []
+        nrays = 0
+        for i in range(args.warmup + args.steps):
+            u = frame_uniforms(vrt, spawn, i)
+            t0 = time.perf_counter()
+            r = oracle.pathtrace(vox, b, m, n, vrt.uniforms_bytes(u), WORKLOAD["fclamp"], W, H, i % 8, H, 8)
+            if i >= args.warmup:
+                per_step.append(time.perf_counter() - t0)
+                nrays += r["stats"]["rays"]
+        secs = sum(per_step)
+        value = nrays / secs / 1e6
+        sample = "CPU oracle path trace of every 8th row per step (reference traversal library not built)"
+        kind = "port"
+    line = dict(base)
+    line.update({"value": round(value, 3), "ms_per_step": round(secs * 1e3 / args.steps, 3),
+                 "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": kind,
+                                  "sample": sample},
+                 "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * vrt.h -- C ABI of voxelrt_b200, a B200 (sm_100a) implementation of
+ * VoxelRT's plain per-frame global-illumination path:
+ *
+ *   pathtrace (two-level brick->voxel DDA, 1-spp path, sun-cone NEE,
+ *   emissive pickup, firefly clamp, albedo demodulation)
+ *   -> temporal reprojection -> 3x edge-aware a-trous -> present.
+ *
+ * Buffer formats follow the reference renderer (src/main.js:335-360,
+ * src/scene.js:411-433):
+ *   voxels     u32[N^3], index x + y*N + z*N*N, packed R | G<<8 | B<<16 | E<<24
+ *              (0 = air)                                   (voxel.wgsl:8-11)
+ *   bricks     u32[(N/8)^3], non-zero when any voxel of the 8^3 brick is solid
+ *   brickMasks u32[16*(N/8)^3], bit lx + 8*ly + 64*lz of brick bi in word
+ *              bi*16 + (bit>>5)
+ *   radiance   rgba16f (demodulated), albedo rgba8unorm (sqrt albedo),
+ *   gbuffer    rgba32f (normal, hit distance; sky = (-rd, -1)),
+ *   accum      rgba16f or rgba32f (history length in alpha), denoise rgba16f,
+ *   ldr        rgba8 (the headless stand-in for the canvas present pass).
+ *
+ * Conventions: every call returns VRT_OK (0) or a VRT_ERR_* code and never
+ * throws; vrt_last_error_string() describes the last failure on the calling
+ * thread.  Each context owns one CUDA stream; calls on one context are
+ * serialised by the caller (host-thread-safe per context).  Host pointers are
+ * plain host memory; "_device" entry points take device pointers.
+ */
+#ifndef VRT_H_
+#define VRT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VRT_ABI_VERSION 1
+
+enum {
+  VRT_OK = 0,
+  VRT_ERR_INVALID = 1,     /* bad argument or size                       */
+  VRT_ERR_CUDA = 2,        /* CUDA runtime error (message has details)   */
+  VRT_ERR_OOM = 3,         /* device allocation failed                   */
+  VRT_ERR_NO_DEVICE = 4,   /* no CUDA device / extension unusable        */
+  VRT_ERR_BUDGET = 5,      /* HBM admission budget exceeded              */
+  VRT_ERR_TIMEOUT = 6,     /* a bounded device wait gave up              */
+  VRT_ERR_STATE = 7        /* call not valid in the object's state       */
+};
+
+typedef struct VrtCtx VrtCtx;
+typedef struct VrtScene VrtScene;
+typedef struct VrtSession VrtSession;
+
+/* Uniform block, byte-identical to the reference's 304-byte UBO
+ * (common.wgsl:13-35, packed by main.js:399-426). */
+typedef struct VrtUniforms {
+  float invViewProj[16];   /* column-major, WebGPU clip z in [0,1]            */
+  float prevViewProj[16];
+  float camPos[4];         /* xyz metres, w = time                             */
+  float prevCamPos[4];
+  float sunDir[4];         /* xyz towards the sun, w = cos(angular radius)     */
+  float sunRadiance[4];    /* rgb irradiance, w = sky intensity                */
+  uint32_t params0[4];     /* x frame index (RNG stream), y bounces,
+                              z flags: bit0 temporal, bit1 denoise             */
+  float params1[4];        /* x width, y height, z exposure                    */
+  uint32_t params2[4];     /* x restir flags (must be 0 on this path)          */
+  float params3[4];
+  float params4[4];        /* y = max temporal history (default 64)            */
+  float params5[4];
+  float params6[4];
+} VrtUniforms;
+
+typedef struct VrtDeviceConfig {
+  int device;                 /* CUDA ordinal                                  */
+  uint64_t hbm_budget_bytes;  /* 0 = no admission limit                        */
+} VrtDeviceConfig;
+
+typedef struct VrtSessionConfig {
+  int width, height;          /* render size in pixels                         */
+  float firefly_clamp;        /* FCLAMP_VALUE (pathtrace.wgsl:35); <=0 = off   */
+  int accum_f32;              /* 1: rgba32f history, 0: rgba16f                */
+  int keep_radiance_f32;      /* 1: also store fp32 demodulated radiance       */
+} VrtSessionConfig;
+
+/* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,
+ * -1 on miss.  steps = brick iterations + voxel iterations entered;
+ * bytes = 4 * (brick words + mask words + voxel words read). */
+typedef struct VrtHit {
+  float t;                    /* metres, < 0 on miss                           */
+  float n[3];
+  uint32_t mat;
+  int32_t voxel[3];
+  int32_t face;
+  uint32_t steps;
+  uint32_t bytes;
+  uint32_t pad;
+} VrtHit;
+
+typedef struct VrtFrameStats {
+  uint64_t rays;              /* trace() invocations (primary+bounce+shadow)   */
+  uint64_t dda_outer;         /* brick iterations                              */
+  uint64_t dda_inner;         /* voxel iterations                              */
+  uint64_t voxel_reads;
+  uint64_t pixels;
+  float ms_pathtrace, ms_temporal, ms_atrous, ms_present, ms_total;
+  uint32_t launches;          /* kernels launched by the frame                 */
+  uint32_t pad;
+} VrtFrameStats;
+
+/* Camera pose of the reference's fly camera (camera.js:1-57). */
+typedef struct VrtCameraPose {
+  double pos[3];              /* metres                                        */
+  double yaw, pitch;          /* radians; yaw 0 faces +Z                       */
+  double fov_y;               /* radians (reference default 70 deg)            */
+  double near_z, far_z;       /* 0.05, 400 in the reference                    */
+} VrtCameraPose;
+
+typedef struct VrtLighting {
+  float sun_dir[3];           /* towards the sun, normalised by the callee     */
+  float sun_cos_radius;       /* cos(angular radius)                           */
+  float sun_irradiance[3];
+  float sky_intensity;
+} VrtLighting;
+
+/* Scene generators (host only; no GPU needed). */
+enum {
+  VRT_SCENE_VOXELRT = 0,      /* scene.js 'default' world (noise seed = seed)  */
+  VRT_SCENE_SMALL = 1,        /* 64^3 terrain + 24^3 Cornell box              */
+  VRT_SCENE_FULL = 2,         /* terrain, room, 40 trees, RGB lanterns        */
+  VRT_SCENE_RANDOM = 3        /* terrain + boxes, 0.1% emissive U(1,20)       */
+};
+
+/* ---- context ----------------------------------------------------------- */
+/* Replaces WebGPU requestAdapter/requestDevice (main.js:138-159). */
+int vrt_create(const VrtDeviceConfig* cfg, VrtCtx** out);
+int vrt_destroy(VrtCtx* ctx);
+int vrt_ctx_synchronize(VrtCtx* ctx);
+/* Bytes of device memory currently held by scenes and sessions of ctx. */
+uint64_t vrt_ctx_bytes_in_use(const VrtCtx* ctx);
+const char* vrt_last_error_string(void);
+int vrt_abi_version(void);
+
+/* ---- scene ------------------------------------------------------------- */
+/* Replaces generateScene() upload + brick build (main.js:188-203,
+ * scene.js:411-433): uploads voxels and builds bricks/masks on the device. */
+int vrt_scene_upload(VrtCtx* ctx, const uint32_t* voxels, int N, VrtScene** out);
+/* Same, with caller-built bricks and masks (reference writeBuffer path). */
+int vrt_scene_upload_prebuilt(VrtCtx* ctx, const uint32_t* voxels, const uint32_t* bricks,
+                              const uint32_t* brick_masks, int N, VrtScene** out);
+/* Sets every voxel of the inclusive box to value and updates the affected
+ * bricks and masks (VoxelBench scene events, scenes.h:8-12). */
+int vrt_scene_edit_box(VrtScene* scene, int x0, int y0, int z0, int x1, int y1, int z1,
+                       uint32_t value);
+int vrt_scene_read(VrtScene* scene, uint32_t* voxels, uint32_t* bricks, uint32_t* brick_masks);
+int vrt_scene_destroy(VrtScene* scene);
+
+/* ---- DDA parity entry (voxel.wgsl:73-157 trace/traceShadow) ------------ */
+int vrt_trace_rays(VrtScene* scene, const float* origins, const float* dirs, const float* tmax,
+                   int n, VrtHit* out);
+int vrt_trace_rays_device(VrtScene* scene, const float* d_origins, const float* d_dirs,
+                          const float* d_tmax, int n, VrtHit* d_out);
+
+/* ---- session (per-view render targets, main.js:335-360) ---------------- */
+int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg, VrtSession** out);
+int vrt_session_destroy(VrtSession* s);
+int vrt_session_set_scene(VrtSession* s, VrtScene* scene);
+/* Clears history (next frame starts with parity 0 and empty history). */
+int vrt_session_reset(VrtSession* s);
+/* One frame: pathtrace -> temporal -> (if params0.z bit1) a-trous x3 ->
+ * present, ping-ponging G-buffer/history by frame parity (main.js:680-772). */
+int vrt_frame(VrtSession* s, const VrtUniforms* u);
+/* Individual passes of the same frame (parity of the frame in flight). */
+int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u);
+int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u);
+int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int iteration /*0,1,2*/);
+int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
+/* Ends a frame driven pass by pass (advances parity). */
+int vrt_end_frame(VrtSession* s);
+/* Per-pass CUDA-event timings and in-kernel ray/step counters. */
+int vrt_session_set_timing(VrtSession* s, int enable);
+int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out);
+
+/* Readbacks of the last frame (HDR capture, main.js:571-661). bytes must be
+ * at least W*H*bpp; returns VRT_ERR_INVALID otherwise. */
+int vrt_read_radiance(VrtSession* s, void* host, size_t bytes);      /* rgba16f */
+int vrt_read_radiance_f32(VrtSession* s, void* host, size_t bytes);  /* rgba32f */
+int vrt_read_albedo(VrtSession* s, void* host, size_t bytes);        /* rgba8   */
+int vrt_read_gbuffer(VrtSession* s, void* host, size_t bytes);       /* rgba32f */
+int vrt_read_accum(VrtSession* s, void* host, size_t bytes);         /* f16/f32 */
+int vrt_read_denoise(VrtSession* s, int index, void* host, size_t bytes); /* rgba16f */
+int vrt_read_final(VrtSession* s, void* host, size_t bytes);         /* rgba16f/32f */
+int vrt_read_ldr(VrtSession* s, void* host, size_t bytes);           /* rgba8   */
+int vrt_read_hdr(VrtSession* s, float* host_rgb, size_t bytes);      /* f32 RGB */
+/* Writes history buffers (resume from a saved session state). */
+int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
+
+/* ---- host helpers (no GPU) --------------------------------------------- */
+/* Fills the uniform block like main.js writeUniforms (399-426). */
+int vrt_make_uniforms(const VrtCameraPose* cur, const VrtCameraPose* prev, const VrtLighting* light,
+                      uint32_t frame, uint32_t bounces, uint32_t flags, int width, int height,
+                      float exposure, float max_history, VrtUniforms* out);
+/* viewProj / invViewProj of camera.js:47-57 (column-major). */
+int vrt_camera_matrices(const VrtCameraPose* pose, double aspect, float* view_proj,
+                        float* inv_view_proj);
+/* Benchmark camera path from a spawn pose: per frame the yaw advances
+ * 0.5 degree and the position moves 0.05 m along the horizontal heading. */
+int vrt_camera_spline(const VrtCameraPose* spawn, int frame, VrtCameraPose* out);
+/* Procedural scenes; out_voxels holds N^3 words; spawn (may be NULL)
+ * receives the default camera pose for the scene. */
+int vrt_scene_generate(int kind, int N, uint32_t seed, uint32_t* out_voxels, VrtCameraPose* spawn);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VRT_H_ */

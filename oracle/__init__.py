@@ -1,0 +1,209 @@
+"""Test infrastructure: ctypes loader for the CPU oracle (liboracle.so) and the
+reference VoxelBench traversal (_ref/libvbref.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this package; the product (voxelrt_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libvbref.so"
+REF_SRC = Path("/root/reference/VoxelBench/pipeline")
+
+HIT_DTYPE = np.dtype([("t", "<f4"), ("n", "<f4", 3), ("mat", "<u4"), ("voxel", "<i4", 3), ("face", "<i4"),
+                      ("steps", "<u4"), ("bytes", "<u4"), ("pad", "<u4")])
+
+
+class OrcStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("outer", C.c_uint64), ("inner", C.c_uint64), ("vreads", C.c_uint64),
+                ("pixels", C.c_uint64)]
+
+
+def build(ref: bool | None = None) -> None:
+    """make -C oracle (and the reference traversal when its sources exist)."""
+    targets = ["all"]
+    if ref or (ref is None and REF_SRC.exists()):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build(ref=False)
+        _lib = C.CDLL(str(LIB))
+    return _lib
+
+
+def ref_lib() -> C.CDLL | None:
+    """The reference's VoxelBench traversal, or None when it was not built."""
+    global _ref
+    if _ref is None and REF_LIB.exists():
+        _ref = C.CDLL(str(REF_LIB))
+        _ref.vb_time_trace.restype = C.c_double
+        _ref.vb_copy_grid.restype = C.c_long
+    return _ref
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def build_bricks(vox: np.ndarray, n: int):
+    bg = n // 8
+    bricks = np.zeros(bg ** 3, np.uint32)
+    masks = np.zeros(16 * bg ** 3, np.uint32)
+    lib().orc_build_bricks(_p(np.ascontiguousarray(vox, np.uint32)), C.c_int(n), _p(bricks), _p(masks))
+    return bricks, masks
+
+
+def trace(vox, bricks, masks, n, o, d, tmax) -> np.ndarray:
+    o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+    d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tmax, np.float32).reshape(-1)
+    out = np.zeros(o.shape[0], HIT_DTYPE)
+    lib().orc_trace(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(o), _p(d), _p(t), C.c_int(o.shape[0]), _p(out))
+    return out
+
+
+def trace_naive(vox, n, o, d, tmax) -> np.ndarray:
+    o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+    d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tmax, np.float32).reshape(-1)
+    out = np.zeros(o.shape[0], HIT_DTYPE)
+    lib().orc_trace_naive(_p(vox), C.c_int(n), _p(o), _p(d), _p(t), C.c_int(o.shape[0]), _p(out))
+    return out
+
+
+def pathtrace(vox, bricks, masks, n, ubytes: bytes, fclamp: float, w: int, h: int, row0=0, row1=None, row_step=1):
+    """Returns dict rad16 (u16 HxWx4), rad32 (f32), alb8 (u8), gbuf (f32), stats."""
+    row1 = h if row1 is None else row1
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    rad16 = np.zeros((h, w, 4), np.uint16)
+    rad32 = np.zeros((h, w, 4), np.float32)
+    alb8 = np.zeros((h, w, 4), np.uint8)
+    gbuf = np.zeros((h, w, 4), np.float32)
+    st = OrcStats()
+    lib().orc_pathtrace(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_float(fclamp), C.c_int(w), C.c_int(h),
+                        C.c_int(row0), C.c_int(row1), C.c_int(row_step), _p(rad16), _p(rad32), _p(alb8), _p(gbuf),
+                        C.byref(st))
+    return {"rad16": rad16, "rad32": rad32, "alb8": alb8, "gbuf": gbuf,
+            "stats": {k: int(getattr(st, k)) for k, _ in OrcStats._fields_}}
+
+
+def temporal(ubytes, w, h, rad16, gcur, acc_prev, gprev, acc_f32: bool):
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    out = np.zeros((h, w, 4), np.float32 if acc_f32 else np.uint16)
+    lib().orc_temporal(_p(ub), C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(rad16)), _p(np.ascontiguousarray(gcur)),
+                       _p(np.ascontiguousarray(acc_prev)), _p(np.ascontiguousarray(gprev)), _p(out),
+                       C.c_int(int(acc_f32)))
+    return out
+
+
+def atrous(w, h, src, src_f32: bool, gbuf, step: int):
+    out = np.zeros((h, w, 4), np.uint16)
+    lib().orc_atrous(None, C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(src)), C.c_int(int(src_f32)),
+                     _p(np.ascontiguousarray(gbuf)), _p(out), C.c_int(step))
+    return out
+
+
+def present(ubytes, w, h, final, final_f32: bool, alb8):
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    out = np.zeros((h, w, 4), np.uint8)
+    lib().orc_present(_p(ub), C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(final)), C.c_int(int(final_f32)),
+                      _p(np.ascontiguousarray(alb8)), _p(out))
+    return out
+
+
+def hdr(w, h, final, final_f32: bool, alb8):
+    out = np.zeros((h, w, 3), np.float32)
+    lib().orc_hdr(C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(final)), C.c_int(int(final_f32)),
+                  _p(np.ascontiguousarray(alb8)), _p(out))
+    return out
+
+
+def accumulate_f64(vox, bricks, masks, n, ubytes, fclamp, w, h, frame0: int, spp: int, accum=None):
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    acc = np.zeros((h, w, 3), np.float64) if accum is None else accum
+    lib().orc_accumulate_f64(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_float(fclamp), C.c_int(w),
+                             C.c_int(h), C.c_uint32(frame0), C.c_int(spp), _p(acc))
+    return acc
+
+
+def collect_rays(vox, bricks, masks, n, ubytes, fclamp, w, h, row0=0, row1=None, row_step=1, cap=None):
+    """Rays (N x 7: origin xyz and maxT in voxel units, direction) traced by
+    the oracle path for the selected rows."""
+    row1 = h if row1 is None else row1
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    nrows = len(range(row0, min(row1, h), row_step))
+    cap = cap or nrows * w * 8
+    out = np.zeros((cap, 7), np.float32)
+    f = lib().orc_collect_rays
+    f.restype = C.c_long
+    total = f(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_float(fclamp), C.c_int(w), C.c_int(h),
+              C.c_int(row0), C.c_int(row1), C.c_int(row_step), _p(out), C.c_long(cap))
+    return out[:min(total, cap)]
+
+
+def camera_matrices(pos, yaw, pitch, fov_y, aspect, near_z=0.05, far_z=400.0):
+    p = (C.c_double * 3)(*pos)
+    vp = np.zeros(16, np.float32)
+    ivp = np.zeros(16, np.float32)
+    lib().orc_camera_matrices(p, C.c_double(yaw), C.c_double(pitch), C.c_double(fov_y), C.c_double(aspect),
+                              C.c_double(near_z), C.c_double(far_z), _p(vp), _p(ivp))
+    return vp, ivp
+
+
+def math_eval(fn: int, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros_like(x)
+    lib().orc_math_eval(C.c_int(fn), _p(x), _p(y), C.c_int(x.size))
+    return y
+
+
+def pcg_hash(v: int) -> int:
+    f = lib().orc_pcg_hash
+    f.restype = C.c_uint32
+    return int(f(C.c_uint32(v)))
+
+
+def frame(vox, bricks, masks, n, ubytes, fclamp, w, h, acc_prev, gprev, acc_f32=False):
+    """One full oracle frame: pathtrace -> temporal -> a-trous x3 (if the
+    denoise flag is set) -> present.  Returns every intermediate."""
+    pt = pathtrace(vox, bricks, masks, n, ubytes, fclamp, w, h)
+    flags = np.frombuffer(ubytes, np.uint32)[48 + 2]
+    acc = temporal(ubytes, w, h, pt["rad16"], pt["gbuf"], acc_prev, gprev, acc_f32)
+    res = dict(pt)
+    res["accum"] = acc
+    if flags & 2:
+        d_a = atrous(w, h, acc, acc_f32, pt["gbuf"], 1)
+        d_b = atrous(w, h, d_a, False, pt["gbuf"], 2)
+        d_a2 = atrous(w, h, d_b, False, pt["gbuf"], 4)
+        res["den"] = (d_a, d_b, d_a2)
+        fin, fin_f32 = d_a2, False
+    else:
+        fin, fin_f32 = acc, acc_f32
+    res["final"] = fin
+    res["ldr"] = present(ubytes, w, h, fin, fin_f32, pt["alb8"])
+    res["hdr"] = hdr(w, h, fin, fin_f32, pt["alb8"])
+    return res

@@ -1,0 +1,974 @@
+// ============================================================================
+// vrt_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+//
+// Scalar CPU restatement of VoxelRT's plain per-frame GI path, written from the
+// reference's WebGPU shaders and host code:
+//   src/shaders/voxel.wgsl:18-157     world access + two-level brick->voxel DDA
+//   src/shaders/common.wgsl:69-139    PCG RNG, camera ray, sky, sun cone, cosine lobe
+//   src/shaders/pathtrace.wgsl:248-330  plain (RF_RESTIR off) 1-spp path tracer
+//   src/shaders/temporal.wgsl:17-77   reprojection + history accumulation
+//   src/shaders/atrous.wgsl:26-83     edge-aware a-trous iteration
+//   src/shaders/present.wgsl:40-55    remodulate, exposure, ACES, gamma
+//   src/main.js:628-659               HDR capture = illum * (alb8/255)^2
+//   src/scene.js:411-433              brick occupancy words + 16-word masks
+//   src/math.js:3-74, src/camera.js:47-57   view/projection matrices
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs load
+// this library.  It is compiled with -ffp-contract=off so every + - * / is a
+// single IEEE-754 binary32 operation in source order, which is the contract
+// the CUDA kernels are held to bit-for-bit.
+//
+// Parity pin: the DDA is pinned to the reference's own CPU traversal
+// (VoxelBench/pipeline/core.cpp:23-50 traceNaive, double precision) through
+// golden ray fixtures generated from the reference sources (tests/golden).
+// The shading math (RNG, sampling, sky, temporal, a-trous, present) restates
+// WGSL that cannot execute here (no WebGPU implementation); that part is
+// "parity unpinned" against the reference and is checked statistically
+// (converged-image agreement with an FP64 accumulation).
+//
+// Transcendentals.  WGSL leaves sin/cos/exp/pow accuracy to the implementation
+// (absolute error up to 2^-11 for sin/cos).  The oracle and the kernels both
+// use the project's own definitions below (Cody-Waite reduction + Taylor
+// series), so both sides compute identical bits.
+// ============================================================================
+#include <cstdint>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// scalar helpers
+// ---------------------------------------------------------------------------
+inline uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float bitsf(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+struct f3 { float x, y, z; };
+inline f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+inline f3 add(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline f3 sub(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline f3 mul(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline f3 muls(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+inline f3 divv(f3 a, f3 b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline float dot3(f3 a, f3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline f3 cross3(f3 a, f3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline float length3(f3 a) { return std::sqrt(dot3(a, a)); }
+inline f3 normalize3(f3 a) { float l = length3(a); return mk(a.x / l, a.y / l, a.z / l); }
+inline float fminf_(float a, float b) { return b < a ? b : a; }   // WGSL min on non-NaN
+inline float fmaxf_(float a, float b) { return a < b ? b : a; }
+inline f3 min3(f3 a, f3 b) { return mk(fminf_(a.x, b.x), fminf_(a.y, b.y), fminf_(a.z, b.z)); }
+inline f3 max3(f3 a, f3 b) { return mk(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z)); }
+inline float clampf(float x, float lo, float hi) { return fminf_(fmaxf_(x, lo), hi); }
+inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }  // WGSL mix
+inline f3 mix3(f3 a, f3 b, float t) { return mk(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
+
+// ---------------------------------------------------------------------------
+// Project transcendentals (shared definition with the CUDA kernels).
+// ---------------------------------------------------------------------------
+// sin and cos of x, |x| <= 8.  Quadrant k = round(x / (pi/2)); the remainder is
+// formed Cody-Waite style with pi/2 = 201/128 + PIO2_LO, then evaluated by the
+// Taylor series of sin (to r^9) and cos (to r^10) about zero.
+inline void om_sincos(float x, float& s, float& c) {
+  const float TWO_OVER_PI = 0.636619747f;
+  const float PIO2_HI = 1.5703125f;
+  const float PIO2_LO = 0.000483826792f;
+  float kf = std::floor(x * TWO_OVER_PI + 0.5f);
+  int k = (int)kf;
+  float r = (x - kf * PIO2_HI) - kf * PIO2_LO;
+  float r2 = r * r;
+  float sp = r + (r * r2) * (-0.166666672f + r2 * (0.00833333377f +
+                 r2 * (-0.000198412701f + r2 * 2.75573188e-06f)));
+  float cp = 1.0f + r2 * (-0.5f + r2 * (0.0416666679f + r2 * (-0.00138888892f +
+                 r2 * (2.48015876e-05f + r2 * -2.755732e-07f))));
+  switch (k & 3) {
+    case 0: s = sp; c = cp; break;
+    case 1: s = cp; c = -sp; break;
+    case 2: s = -sp; c = -cp; break;
+    default: s = -cp; c = sp; break;
+  }
+}
+
+// 2^k for integer k in [-126, 127].
+inline float om_pow2i(int k) { return bitsf((uint32_t)(k + 127) << 23); }
+
+// e^r for |r| <= 0.35: Taylor series to r^7.
+inline float om_exp_poly(float r) {
+  return 1.0f + r * (1.0f + r * (0.5f + r * (0.166666672f + r * (0.0416666679f +
+         r * (0.00833333377f + r * (0.00138888892f + r * 0.000198412701f))))));
+}
+
+// e^x: k = round(x log2 e), r = x - k ln2 (ln2 split into 0x3f317200 + LN2_LO).
+inline float om_exp(float x) {
+  if (!(x > -87.0f)) return 0.0f;        // also maps NaN/-inf to 0
+  if (x > 88.0f) return INFINITY;
+  const float LOG2E = 1.44269502f;
+  const float LN2_HI = 0.693145751953125f;
+  const float LN2_LO = 1.42860677e-06f;
+  float kf = std::floor(x * LOG2E + 0.5f);
+  float r = (x - kf * LN2_HI) - kf * LN2_LO;
+  return om_exp_poly(r) * om_pow2i((int)kf);
+}
+
+// 2^z: k = round(z), f = z - k (exact), 2^f = e^(f ln2).
+inline float om_exp2(float z) {
+  if (!(z > -126.0f)) return 0.0f;
+  if (z > 127.0f) return INFINITY;
+  float kf = std::floor(z + 0.5f);
+  float f = z - kf;
+  return om_exp_poly(f * 0.693147182f) * om_pow2i((int)kf);
+}
+
+// log2(x) for finite x > 0: x = m 2^e with m in [sqrt(1/2), sqrt(2)],
+// log2(m) = (2/ln2) atanh(s), s = (m-1)/(m+1), atanh by its series to s^9.
+inline float om_log2(float x) {
+  uint32_t b = fbits(x);
+  int e = (int)(b >> 23) - 127;
+  if ((b >> 23) == 0) {                    // subnormal input
+    x = x * 8388608.0f; b = fbits(x); e = (int)(b >> 23) - 127 - 23;
+  }
+  float m = bitsf((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float s2 = s * s;
+  float at = s + (s * s2) * (0.333333343f + s2 * (0.200000003f + s2 * (0.142857149f + s2 * 0.111111112f)));
+  return (float)e + at * 2.88539004f;
+}
+
+// x^y for x >= 0, y > 0 (the only uses on this path); 0^y = 0.
+inline float om_pow(float x, float y) {
+  if (!(x > 0.0f)) return 0.0f;
+  return om_exp2(y * om_log2(x));
+}
+
+// ---------------------------------------------------------------------------
+// Storage formats
+// ---------------------------------------------------------------------------
+// binary32 -> binary16, round to nearest even (WebGPU rgba16float store).
+inline uint16_t f32_to_f16(float f) {
+  uint32_t x = fbits(f);
+  uint32_t sign = (x >> 16) & 0x8000u;
+  uint32_t ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return (uint16_t)(sign | (ax > 0x7f800000u ? 0x7e00u : 0x7c00u));
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);
+  if (ax < 0x38800000u) {
+    if (ax < 0x33000000u) return (uint16_t)sign;
+    uint32_t e = ax >> 23;
+    uint32_t m = (ax & 0x7fffffu) | 0x800000u;
+    uint32_t shift = 126u - e;
+    uint32_t q = m >> shift;
+    uint32_t rem = m & ((1u << shift) - 1u);
+    uint32_t half = 1u << (shift - 1u);
+    if (rem > half || (rem == half && (q & 1u))) q++;
+    return (uint16_t)(sign | q);
+  }
+  uint32_t r = ax - 0x38000000u;
+  uint32_t q = r >> 13;
+  uint32_t rem = r & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) q++;
+  return (uint16_t)(sign | q);
+}
+
+inline float f16_to_f32(uint16_t h) {
+  uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+  uint32_t e = (h >> 10) & 0x1fu;
+  uint32_t m = h & 0x3ffu;
+  if (e == 0) {
+    float v = (float)m * 5.96046448e-08f;       // m * 2^-24, exact
+    return sign ? -v : v;
+  }
+  if (e == 31) return bitsf(sign | 0x7f800000u | (m << 13));
+  return bitsf(sign | ((e + 112u) << 23) | (m << 13));
+}
+
+// rgba8unorm store: nearest of clamp(x,0,1)*255.
+inline uint8_t unorm8(float x) {
+  float c = clampf(x, 0.0f, 1.0f);
+  return (uint8_t)(int)std::floor(c * 255.0f + 0.5f);
+}
+
+// ---------------------------------------------------------------------------
+// Uniform block (common.wgsl:13-35), read by float offsets of the 304-B UBO.
+// ---------------------------------------------------------------------------
+struct Uni {
+  float invViewProj[16], prevViewProj[16];
+  float camPos[4], prevCamPos[4], sunDir[4], sunRadiance[4];
+  uint32_t params0[4];
+  float params1[4];
+  uint32_t params2[4];
+  float params3[4], params4[4], params5[4], params6[4];
+};
+static_assert(sizeof(Uni) == 304, "uniform block is 304 bytes");
+
+// WGSL mat4x4 * vec4 with column-major storage, summed column by column.
+inline void matvec4(const float* m, const float v[4], float out[4]) {
+  for (int r = 0; r < 4; r++) {
+    out[r] = ((m[0 + r] * v[0] + m[4 + r] * v[1]) + m[8 + r] * v[2]) + m[12 + r] * v[3];
+  }
+}
+
+const float PI = 3.14159274f;            // f32(3.14159265358979)
+const float TWO_PI = 6.28318548f;        // f32(2 * 3.14159265358979)
+const float INV_PI = 0.318309873f;       // f32(0.31830988618)
+const float VOXEL_SIZE = 0.0625f;        // scene.js:5
+const float INV_VOXEL = 16.0f;
+const int BRICK = 8;                     // scene.js:6
+const float EMISSIVE_SCALE = 24.0f;      // common.wgsl:11
+
+// ---------------------------------------------------------------------------
+// RNG: PCG hash (common.wgsl:69-84)
+// ---------------------------------------------------------------------------
+inline uint32_t pcg_hash(uint32_t v) {
+  v = v * 747796405u + 2891336453u;
+  uint32_t w = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+struct Rng {
+  uint32_t s;
+  float next() { s = pcg_hash(s); return (float)s * 2.3283064365386963e-10f; }  // f32(u32) * 2^-32
+};
+inline Rng init_rng(uint32_t px, uint32_t py, uint32_t frame) {
+  return Rng{pcg_hash(px + pcg_hash(py + pcg_hash(frame)))};
+}
+
+// ---------------------------------------------------------------------------
+// Voxel world + two-level DDA (voxel.wgsl:18-153)
+// ---------------------------------------------------------------------------
+struct World {
+  const uint32_t* vox;
+  const uint32_t* bricks;
+  const uint32_t* masks;
+  int N, BG;
+};
+
+struct Hit {
+  float t; f3 n; uint32_t mat;
+  int vx, vy, vz;
+  uint32_t outer, inner, vreads;   // iteration counters (the build's step count)
+};
+
+// floor to int with saturation, NaN -> 0 (the semantics of cvt.rmi.s32.f32;
+// WGSL's f32 -> i32 conversion also clamps to the i32 range).
+inline int ifloor(float x) {
+  float f = std::floor(x);
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return 2147483647;
+  if (f < -2147483648.0f) return (-2147483647 - 1);
+  return (int)f;
+}
+inline int iclamp(int x, int lo, int hi) { return std::min(std::max(x, lo), hi); }
+
+// safeInv (voxel.wgsl:65-71)
+inline f3 safe_inv(f3 v) {
+  f3 s = mk(v.x >= 0.0f ? 1.0f : -1.0f, v.y >= 0.0f ? 1.0f : -1.0f, v.z >= 0.0f ? 1.0f : -1.0f);
+  f3 a = mk(fmaxf_(std::fabs(v.x), 1e-8f), fmaxf_(std::fabs(v.y), 1e-8f), fmaxf_(std::fabs(v.z), 1e-8f));
+  return divv(s, a);
+}
+inline int sgn(float x) { return x > 0.0f ? 1 : (x < 0.0f ? -1 : 0); }
+
+// trace (voxel.wgsl:73-153)
+Hit trace(const World& W, f3 roWorld, f3 rd, float maxTWorld) {
+  Hit hit;
+  hit.t = -1.0f; hit.mat = 0u; hit.n = mk(-rd.x, -rd.y, -rd.z);
+  hit.vx = hit.vy = hit.vz = -1;
+  hit.outer = hit.inner = hit.vreads = 0;
+  const int N = W.N, BG = W.BG;
+
+  f3 ro = muls(roWorld, INV_VOXEL);
+  float maxT = maxTWorld * INV_VOXEL;
+  f3 invRd = safe_inv(rd);
+  int sx = sgn(rd.x), sy = sgn(rd.y), sz = sgn(rd.z);
+  f3 stepGE = mk(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
+
+  f3 t0 = mul(sub(mk(0, 0, 0), ro), invRd);
+  float G = (float)N;
+  f3 t1 = mul(sub(mk(G, G, G), ro), invRd);
+  f3 tmin3 = min3(t0, t1);
+  f3 tmax3 = max3(t0, t1);
+  float tEnter = fmaxf_(fmaxf_(tmin3.x, tmin3.y), fmaxf_(tmin3.z, 0.0f));
+  float tExit = fminf_(fminf_(tmax3.x, tmax3.y), fminf_(tmax3.z, maxT));
+  if (tEnter > tExit) return hit;
+
+  int ax;   // entry face axis (voxel.wgsl:95-98)
+  if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) ax = 0;
+  else if (tmin3.y >= tmin3.z) ax = 1;
+  else ax = 2;
+
+  float t = tEnter;
+  float tn = t + 1e-4f;
+  f3 startP = add(ro, muls(rd, tn));
+  int bx = iclamp(ifloor(startP.x / 8.0f), 0, BG - 1);
+  int by = iclamp(ifloor(startP.y / 8.0f), 0, BG - 1);
+  int bz = iclamp(ifloor(startP.z / 8.0f), 0, BG - 1);
+  f3 absInv = mk(std::fabs(invRd.x), std::fabs(invRd.y), std::fabs(invRd.z));
+  f3 tDeltaB = muls(absInv, 8.0f);
+  f3 tMaxB = mul(sub(muls(add(mk((float)bx, (float)by, (float)bz), stepGE), 8.0f), ro), invRd);
+
+  for (int iter = 0; iter < 3 * BG + 2; iter++) {
+    if (t > tExit) break;
+    hit.outer++;
+    uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)BG + (uint32_t)bz * (uint32_t)(BG * BG);
+    if (W.bricks[bi] != 0u) {
+      int mnx = bx * BRICK, mny = by * BRICK, mnz = bz * BRICK;
+      int mxx = mnx + BRICK - 1, mxy = mny + BRICK - 1, mxz = mnz + BRICK - 1;
+      float tp = t + 1e-4f;
+      f3 p = add(ro, muls(rd, tp));
+      int vx = iclamp(ifloor(p.x), mnx, mxx);
+      int vy = iclamp(ifloor(p.y), mny, mxy);
+      int vz = iclamp(ifloor(p.z), mnz, mxz);
+      f3 tMaxV = mul(sub(add(mk((float)vx, (float)vy, (float)vz), stepGE), ro), invRd);
+      float tCur = t;
+      int vax = ax;
+      for (int j = 0; j < 3 * BRICK; j++) {
+        hit.inner++;
+        uint32_t bit = (uint32_t)((vx - mnx) + (vy - mny) * BRICK + (vz - mnz) * BRICK * BRICK);
+        uint32_t word = W.masks[bi * 16u + (bit >> 5u)];
+        if ((word & (1u << (bit & 31u))) != 0u) {
+          uint32_t m = W.vox[(uint32_t)vx + (uint32_t)vy * (uint32_t)N + (uint32_t)vz * (uint32_t)(N * N)];
+          hit.vreads++;
+          if (tCur > maxT) return hit;
+          hit.t = tCur * VOXEL_SIZE;
+          // n = -vmask * stepDir with vmask one-hot on axis vax
+          float vm[3] = {0.0f, 0.0f, 0.0f};
+          vm[vax] = 1.0f;
+          hit.n = mk(-vm[0] * (float)sx, -vm[1] * (float)sy, -vm[2] * (float)sz);
+          hit.mat = m;
+          hit.vx = vx; hit.vy = vy; hit.vz = vz;
+          return hit;
+        }
+        if (tMaxV.x <= tMaxV.y && tMaxV.x <= tMaxV.z) {
+          tCur = tMaxV.x; tMaxV.x = tMaxV.x + absInv.x; vx += sx; vax = 0;
+        } else if (tMaxV.y <= tMaxV.z) {
+          tCur = tMaxV.y; tMaxV.y = tMaxV.y + absInv.y; vy += sy; vax = 1;
+        } else {
+          tCur = tMaxV.z; tMaxV.z = tMaxV.z + absInv.z; vz += sz; vax = 2;
+        }
+        if (vx < mnx || vy < mny || vz < mnz || vx > mxx || vy > mxy || vz > mxz) break;
+      }
+    }
+    if (tMaxB.x <= tMaxB.y && tMaxB.x <= tMaxB.z) {
+      t = tMaxB.x; tMaxB.x = tMaxB.x + tDeltaB.x; bx += sx; ax = 0;
+    } else if (tMaxB.y <= tMaxB.z) {
+      t = tMaxB.y; tMaxB.y = tMaxB.y + tDeltaB.y; by += sy; ax = 1;
+    } else {
+      t = tMaxB.z; tMaxB.z = tMaxB.z + tDeltaB.z; bz += sz; ax = 2;
+    }
+    if (bx < 0 || by < 0 || bz < 0 || bx >= BG || by >= BG || bz >= BG) break;
+  }
+  return hit;
+}
+
+// Face index of a hit normal: 0..5 = +x,-x,+y,-y,+z,-z (VoxelBench core.h:106).
+inline int face_of(f3 n) {
+  if (n.x > 0.5f) return 0;
+  if (n.x < -0.5f) return 1;
+  if (n.y > 0.5f) return 2;
+  if (n.y < -0.5f) return 3;
+  if (n.z > 0.5f) return 4;
+  if (n.z < -0.5f) return 5;
+  return -1;
+}
+
+// Material (voxel.wgsl:41-51)
+struct Mat { f3 albedo; float emissive; };
+inline Mat unpack_material(uint32_t m) {
+  Mat r;
+  const float s = 1.0f / 255.0f;
+  f3 a = muls(mk((float)(m & 0xffu), (float)((m >> 8) & 0xffu), (float)((m >> 16) & 0xffu)), s);
+  r.albedo = mul(a, a);
+  r.emissive = (float)((m >> 24) & 0xffu) * s;
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Camera, sky, sampling (common.wgsl:90-139)
+// ---------------------------------------------------------------------------
+inline f3 camera_ray(const Uni& u, float uvx, float uvy) {
+  float ndc[4] = {uvx * 2.0f - 1.0f, 1.0f - uvy * 2.0f, 1.0f, 1.0f};
+  float far[4];
+  matvec4(u.invViewProj, ndc, far);
+  f3 fp = mk(far[0] / far[3], far[1] / far[3], far[2] / far[3]);
+  return normalize3(sub(fp, mk(u.camPos[0], u.camPos[1], u.camPos[2])));
+}
+
+inline f3 sky_color(const Uni& u, f3 rd, bool withSunDisc) {
+  float up = clampf(rd.y, -1.0f, 1.0f);
+  f3 sky = mix3(mk(0.55f, 0.68f, 0.85f), mk(0.15f, 0.32f, 0.62f), om_pow(fmaxf_(up, 0.0f), 0.55f));
+  if (up < 0.0f) sky = mix3(sky, mk(0.28f, 0.26f, 0.24f), fminf_(1.0f, -up * 4.0f));
+  f3 sd = mk(u.sunDir[0], u.sunDir[1], u.sunDir[2]);
+  float sunAmt = fmaxf_(dot3(rd, sd), 0.0f);
+  float s2 = sunAmt * sunAmt, s4 = s2 * s2, s8 = s4 * s4;   // pow(sunAmt, 8)
+  sky = add(sky, muls(muls(mk(1.0f, 0.75f, 0.5f), s8), 0.2f));
+  if (withSunDisc && sunAmt > u.sunDir[3]) {
+    float solidAngle = TWO_PI * (1.0f - u.sunDir[3]);
+    float d = fmaxf_(solidAngle, 1e-4f);
+    sky = add(sky, mk(u.sunRadiance[0] / d, u.sunRadiance[1] / d, u.sunRadiance[2] / d));
+  }
+  return muls(sky, u.sunRadiance[3]);
+}
+
+inline f3 sample_sun_dir(const Uni& u, Rng& rng) {
+  float rx = rng.next();
+  float ry = rng.next();
+  float cosT = mixf(1.0f, u.sunDir[3], rx);
+  float sinT = std::sqrt(fmaxf_(0.0f, 1.0f - cosT * cosT));
+  float phi = TWO_PI * ry;
+  f3 w = mk(u.sunDir[0], u.sunDir[1], u.sunDir[2]);
+  f3 a = std::fabs(w.x) > 0.9f ? mk(0, 1, 0) : mk(1, 0, 0);
+  f3 tang = normalize3(cross3(a, w));
+  f3 bitan = cross3(w, tang);
+  float sp, cp; om_sincos(phi, sp, cp);
+  return normalize3(add(add(muls(tang, cp * sinT), muls(bitan, sp * sinT)), muls(w, cosT)));
+}
+
+inline f3 cosine_hemisphere(f3 n, Rng& rng) {
+  float rx = rng.next();
+  float ry = rng.next();
+  float phi = TWO_PI * rx;
+  float sr = std::sqrt(ry);
+  f3 a = std::fabs(n.x) > 0.9f ? mk(0, 1, 0) : mk(1, 0, 0);
+  f3 tang = normalize3(cross3(a, n));
+  f3 bitan = cross3(n, tang);
+  float sp, cp; om_sincos(phi, sp, cp);
+  f3 d = add(add(muls(tang, cp * sr), muls(bitan, sp * sr)), muls(n, std::sqrt(fmaxf_(0.0f, 1.0f - ry))));
+  return normalize3(d);
+}
+
+struct PixStats { uint64_t rays, outer, inner, vreads; };
+
+// When set, every trace() issued by path_pixel appends (origin, direction,
+// maxT) in voxel units -- the ray workload replayed by the reference
+// traversal timing (bench.py's reference arm).
+thread_local std::vector<float>* tl_ray_log = nullptr;
+
+inline Hit trace_logged(const World& W, f3 ro, f3 rd, float maxT) {
+  if (tl_ray_log) {
+    float r[7] = {ro.x * INV_VOXEL, ro.y * INV_VOXEL, ro.z * INV_VOXEL, rd.x, rd.y, rd.z, maxT * INV_VOXEL};
+    tl_ray_log->insert(tl_ray_log->end(), r, r + 7);
+  }
+  return trace(W, ro, rd, maxT);
+}
+
+// One pixel of the plain path (pathtrace.wgsl:248-330, baseline branch).
+// Writes radiance (rgba16f bits + optional fp32 copy), albedo (rgba8 sqrt),
+// G-buffer (rgba32f n,t).
+void path_pixel(const World& W, const Uni& u, float fclamp, uint32_t gx, uint32_t gy,
+                uint32_t dimx, uint32_t dimy, float rad_out[4], uint8_t alb_out[4], float gbuf_out[4],
+                PixStats& st) {
+  Rng rng = init_rng(gx, gy, u.params0[0]);
+  float jx = rng.next() - 0.5f;
+  float jy = rng.next() - 0.5f;
+  float uvx = (((float)gx + 0.5f) + jx) / (float)dimx;
+  float uvy = (((float)gy + 0.5f) + jy) / (float)dimy;
+  f3 ro = mk(u.camPos[0], u.camPos[1], u.camPos[2]);
+  f3 rd = camera_ray(u, uvx, uvy);
+
+  auto count = [&](const Hit& h) { st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads; };
+  Hit h0 = trace_logged(W, ro, rd, 1e4f);
+  count(h0);
+  if (h0.t < 0.0f) {
+    f3 sky = sky_color(u, rd, true);
+    rad_out[0] = sky.x; rad_out[1] = sky.y; rad_out[2] = sky.z; rad_out[3] = 1.0f;
+    alb_out[0] = alb_out[1] = alb_out[2] = alb_out[3] = 255;
+    gbuf_out[0] = -rd.x; gbuf_out[1] = -rd.y; gbuf_out[2] = -rd.z; gbuf_out[3] = -1.0f;
+    return;
+  }
+  Mat mat1 = unpack_material(h0.mat);
+  f3 x1 = add(ro, muls(rd, h0.t));
+  f3 n1 = h0.n;
+  alb_out[0] = unorm8(std::sqrt(mat1.albedo.x));
+  alb_out[1] = unorm8(std::sqrt(mat1.albedo.y));
+  alb_out[2] = unorm8(std::sqrt(mat1.albedo.z));
+  alb_out[3] = 255;
+  gbuf_out[0] = n1.x; gbuf_out[1] = n1.y; gbuf_out[2] = n1.z; gbuf_out[3] = h0.t;
+
+  f3 radiance = mk(0, 0, 0);
+  f3 tp = mk(1, 1, 1);
+  f3 pos = x1, n = n1;
+  Mat mat = mat1;
+  const uint32_t nB = u.params0[1];
+  f3 sunRad = mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
+  for (uint32_t bounce = 0; bounce <= nB; bounce++) {
+    if (mat.emissive > 0.0f) {
+      radiance = add(radiance, muls(mul(tp, mat.albedo), mat.emissive * EMISSIVE_SCALE));
+    }
+    f3 surf = add(pos, muls(n, 1e-3f));
+    f3 l = sample_sun_dir(u, rng);
+    float ndl = dot3(n, l);
+    if (ndl > 0.0f && l.y > 0.0f) {
+      Hit hs = trace_logged(W, surf, l, 1e4f);
+      count(hs);
+      if (!(hs.t >= 0.0f)) {
+        radiance = add(radiance, mul(muls(muls(mul(tp, mat.albedo), INV_PI), ndl), sunRad));
+      }
+    }
+    if (bounce == nB) break;
+    rd = cosine_hemisphere(n, rng);
+    tp = mul(tp, mat.albedo);
+    if (bounce >= 2u) {
+      float p = clampf(fmaxf_(tp.x, fmaxf_(tp.y, tp.z)), 0.05f, 0.95f);
+      if (rng.next() > p) break;
+      tp = mk(tp.x / p, tp.y / p, tp.z / p);
+    }
+    Hit h = trace_logged(W, surf, rd, 1e4f);
+    count(h);
+    if (h.t < 0.0f) {
+      radiance = add(radiance, mul(tp, sky_color(u, rd, false)));
+      break;
+    }
+    pos = add(surf, muls(rd, h.t));
+    n = h.n;
+    mat = unpack_material(h.mat);
+  }
+  if (!(fclamp <= 0.0f)) radiance = min3(radiance, mk(fclamp, fclamp, fclamp));
+  f3 den = max3(mat1.albedo, mk(1e-3f, 1e-3f, 1e-3f));
+  f3 demod = divv(radiance, den);
+  rad_out[0] = demod.x; rad_out[1] = demod.y; rad_out[2] = demod.z; rad_out[3] = 1.0f;
+}
+
+// Bilinear fetch with WebGPU's linear filter conventions: texel centres at
+// +0.5, clamp-to-edge addressing (default sampler, main.js:317).
+template <typename Fetch>
+void bilinear(Fetch fetch, int W, int H, float u, float v, float out[4]) {
+  float tx = u * (float)W - 0.5f;
+  float ty = v * (float)H - 0.5f;
+  float fx0 = std::floor(tx), fy0 = std::floor(ty);
+  float ax = tx - fx0, ay = ty - fy0;
+  int x0 = (int)fx0, y0 = (int)fy0;
+  int xa = iclamp(x0, 0, W - 1), xb = iclamp(x0 + 1, 0, W - 1);
+  int ya = iclamp(y0, 0, H - 1), yb = iclamp(y0 + 1, 0, H - 1);
+  float p00[4], p10[4], p01[4], p11[4];
+  fetch(xa, ya, p00); fetch(xb, ya, p10); fetch(xa, yb, p01); fetch(xb, yb, p11);
+  for (int c = 0; c < 4; c++) {
+    float top = p00[c] * (1.0f - ax) + p10[c] * ax;
+    float bot = p01[c] * (1.0f - ax) + p11[c] * ax;
+    out[c] = top * (1.0f - ay) + bot * ay;
+  }
+}
+
+inline float luminance(const float* c) { return (c[0] * 0.2126f + c[1] * 0.7152f) + c[2] * 0.0722f; }
+
+}  // namespace
+
+// ============================================================================
+// C ABI (ctypes) -- every function is test infrastructure.
+// ============================================================================
+extern "C" {
+
+struct OrcHit {           // 48 bytes, same field meaning as VrtHit in include/vrt.h
+  float t; float n[3]; uint32_t mat;
+  int32_t voxel[3]; int32_t face;
+  uint32_t steps;         // outer + inner iterations entered
+  uint32_t bytes;         // 4 * (brick words + mask words + voxel words read)
+  uint32_t pad;
+};
+
+struct OrcStats { uint64_t rays, outer, inner, vreads, pixels; };
+
+int orc_version(void) { return 1; }
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+// scene.js:411-433 -- brick occupancy word (1 if any voxel solid) and 16 mask
+// words per brick with bit = lx + 8 ly + 64 lz.
+void orc_build_bricks(const uint32_t* vox, int N, uint32_t* bricks, uint32_t* masks) {
+  const int BG = N / BRICK;
+  const size_t nb = (size_t)BG * BG * BG;
+  std::memset(masks, 0, nb * 16 * sizeof(uint32_t));
+  for (int bz = 0; bz < BG; bz++)
+    for (int by = 0; by < BG; by++)
+      for (int bx = 0; bx < BG; bx++) {
+        uint32_t occ = 0;
+        size_t bi = (size_t)bx + (size_t)by * BG + (size_t)bz * BG * BG;
+        for (int z = bz * BRICK; z < (bz + 1) * BRICK; z++)
+          for (int y = by * BRICK; y < (by + 1) * BRICK; y++)
+            for (int x = bx * BRICK; x < (bx + 1) * BRICK; x++)
+              if (vox[(size_t)x + (size_t)y * N + (size_t)z * N * N] != 0u) {
+                occ = 1;
+                int bit = (x - bx * BRICK) + (y - by * BRICK) * BRICK + (z - bz * BRICK) * BRICK * BRICK;
+                masks[bi * 16 + (bit >> 5)] |= 1u << (bit & 31);
+              }
+        bricks[bi] = occ;
+      }
+}
+
+static void fill_hit(const Hit& h, OrcHit& o) {
+  o.t = h.t; o.n[0] = h.n.x; o.n[1] = h.n.y; o.n[2] = h.n.z; o.mat = h.mat;
+  o.voxel[0] = h.vx; o.voxel[1] = h.vy; o.voxel[2] = h.vz;
+  o.face = h.t >= 0.0f ? face_of(h.n) : -1;
+  o.steps = h.outer + h.inner;
+  o.bytes = 4u * (h.outer + h.inner + h.vreads);
+  o.pad = 0;
+}
+
+// voxel.wgsl:73-153 over a batch of rays (origins in metres, unit dirs, maxT metres).
+void orc_trace(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+               const float* o, const float* d, const float* tmax, int n, OrcHit* out) {
+  World W{vox, bricks, masks, N, N / BRICK};
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    Hit h = trace(W, mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]), tmax[i]);
+    fill_hit(h, out[i]);
+  }
+}
+
+// Per-voxel DDA on the same packed-u32 layout (no brick level), in double
+// precision -- the equivalence check pattern of VoxelBench harness.cpp:205-239.
+// Returns the first solid voxel along the ray within tmax (metres) and its
+// entry face.  Origins inside the grid only; the origin voxel is tested too.
+void orc_trace_naive(const uint32_t* vox, int N, const float* o, const float* d, const float* tmax,
+                     int n, OrcHit* out) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    OrcHit& r = out[i];
+    std::memset(&r, 0, sizeof(r));
+    r.t = -1.0f; r.face = -1; r.voxel[0] = r.voxel[1] = r.voxel[2] = -1;
+    double ox = (double)o[3 * i] * 16.0, oy = (double)o[3 * i + 1] * 16.0, oz = (double)o[3 * i + 2] * 16.0;
+    double dx = d[3 * i], dy = d[3 * i + 1], dz = d[3 * i + 2];
+    double tm = (double)tmax[i] * 16.0;
+    int x = (int)std::floor(ox), y = (int)std::floor(oy), z = (int)std::floor(oz);
+    if (x < 0 || y < 0 || z < 0 || x >= N || y >= N || z >= N) continue;
+    int sx = dx > 0 ? 1 : -1, sy = dy > 0 ? 1 : -1, sz = dz > 0 ? 1 : -1;
+    double idx = 1.0 / (std::fabs(dx) + 1e-300), idy = 1.0 / (std::fabs(dy) + 1e-300), idz = 1.0 / (std::fabs(dz) + 1e-300);
+    double tx = (sx > 0 ? (x + 1 - ox) : (ox - x)) * idx;
+    double ty = (sy > 0 ? (y + 1 - oy) : (oy - y)) * idy;
+    double tz = (sz > 0 ? (z + 1 - oz) : (oz - z)) * idz;
+    double t = 0.0; int face = -1;
+    for (int it = 0; it < 4 * N + 8; it++) {
+      if (t > tm) break;
+      uint32_t m = vox[(size_t)x + (size_t)y * N + (size_t)z * N * N];
+      if (m != 0u) {
+        r.t = (float)(t / 16.0); r.mat = m; r.voxel[0] = x; r.voxel[1] = y; r.voxel[2] = z; r.face = face;
+        break;
+      }
+      if (tx <= ty && tx <= tz) { t = tx; tx += idx; x += sx; face = sx > 0 ? 1 : 0; }
+      else if (ty <= tz) { t = ty; ty += idy; y += sy; face = sy > 0 ? 3 : 2; }
+      else { t = tz; tz += idz; z += sz; face = sz > 0 ? 5 : 4; }
+      if (x < 0 || y < 0 || z < 0 || x >= N || y >= N || z >= N) break;
+    }
+  }
+}
+
+// pathtrace.wgsl:248-330 (plain branch) for rows [row0, row1) stepping row_step.
+// rad16: rgba16f bits W*H*4; rad32 (optional): fp32 radiance W*H*4;
+// alb8: rgba8 W*H*4; gbuf: rgba32f W*H*4.  Rows not visited are untouched.
+void orc_pathtrace(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                   const void* uniforms, float fclamp, int Wd, int Hd, int row0, int row1, int row_step,
+                   uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, OrcStats* stats) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  if (row_step < 1) row_step = 1;
+  std::vector<int> rows;
+  for (int y = row0; y < row1 && y < Hd; y += row_step) rows.push_back(y);
+  uint64_t rays = 0, outer = 0, inner = 0, vreads = 0, pix = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads, pix)
+  for (int ri = 0; ri < (int)rows.size(); ri++) {
+    int y = rows[ri];
+    PixStats st{0, 0, 0, 0};
+    for (int x = 0; x < Wd; x++) {
+      float rad[4], gb[4]; uint8_t al[4];
+      path_pixel(W, u, fclamp, (uint32_t)x, (uint32_t)y, (uint32_t)Wd, (uint32_t)Hd, rad, al, gb, st);
+      size_t p = (size_t)y * Wd + x;
+      for (int c = 0; c < 4; c++) {
+        if (rad16) rad16[4 * p + c] = f32_to_f16(rad[c]);
+        if (rad32) rad32[4 * p + c] = rad[c];
+        if (alb8) alb8[4 * p + c] = al[c];
+        if (gbuf) gbuf[4 * p + c] = gb[c];
+      }
+    }
+    rays += st.rays; outer += st.outer; inner += st.inner; vreads += st.vreads; pix += (uint64_t)Wd;
+  }
+  if (stats) { stats->rays = rays; stats->outer = outer; stats->inner = inner; stats->vreads = vreads; stats->pixels = pix; }
+}
+
+// temporal.wgsl:17-77.  accum_f32 selects rgba32f (1) or rgba16f (0) for the
+// history (accumPrev and accumOut), as main.js:148-149 chooses by adapter.
+void orc_temporal(const void* uniforms, int Wd, int Hd, const uint16_t* rad16, const float* gbufCur,
+                  const void* accumPrev, const float* gbufPrev, void* accumOut, int accum_f32) {
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  const bool temporalOn = (u.params0[2] & 1u) != 0u;
+  auto fetchPrev = [&](int x, int y, float out[4]) {
+    size_t p = (size_t)y * Wd + x;
+    for (int c = 0; c < 4; c++)
+      out[c] = accum_f32 ? ((const float*)accumPrev)[4 * p + c] : f16_to_f32(((const uint16_t*)accumPrev)[4 * p + c]);
+  };
+  auto store = [&](size_t p, const float v[4]) {
+    for (int c = 0; c < 4; c++) {
+      if (accum_f32) ((float*)accumOut)[4 * p + c] = v[c];
+      else ((uint16_t*)accumOut)[4 * p + c] = f32_to_f16(v[c]);
+    }
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int gy = 0; gy < Hd; gy++) {
+    for (int gx = 0; gx < Wd; gx++) {
+      size_t p = (size_t)gy * Wd + gx;
+      float cur[3] = {f16_to_f32(rad16[4 * p]), f16_to_f32(rad16[4 * p + 1]), f16_to_f32(rad16[4 * p + 2])};
+      const float* g = gbufCur + 4 * p;
+      if (g[3] < 0.0f || !temporalOn) {
+        float v[4] = {cur[0], cur[1], cur[2], 1.0f};
+        store(p, v);
+        continue;
+      }
+      float uvx = ((float)gx + 0.5f) / (float)Wd;
+      float uvy = ((float)gy + 0.5f) / (float)Hd;
+      f3 cr = camera_ray(u, uvx, uvy);
+      f3 worldPos = add(mk(u.camPos[0], u.camPos[1], u.camPos[2]), muls(cr, g[3]));
+      float wp[4] = {worldPos.x, worldPos.y, worldPos.z, 1.0f};
+      float pc[4];
+      matvec4(u.prevViewProj, wp, pc);
+      float color[3] = {cur[0], cur[1], cur[2]};
+      float history = 1.0f;
+      if (pc[3] > 0.0f) {
+        float ndx = pc[0] / pc[3], ndy = pc[1] / pc[3];
+        float pux = ndx * 0.5f + 0.5f;
+        float puy = (-ndy) * 0.5f + 0.5f;
+        if (pux > 0.0f && puy > 0.0f && pux < 1.0f && puy < 1.0f) {
+          int ppx = (int)(pux * (float)Wd), ppy = (int)(puy * (float)Hd);
+          const float* pg = gbufPrev + 4 * ((size_t)ppy * Wd + ppx);
+          f3 dv = sub(worldPos, mk(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]));
+          float expectedT = length3(dv);
+          bool depthOk = pg[3] > 0.0f && std::fabs(pg[3] - expectedT) < 0.08f * expectedT + 0.02f;
+          bool normalOk = ((pg[0] * g[0] + pg[1] * g[1]) + pg[2] * g[2]) > 0.85f;
+          if (depthOk && normalOk) {
+            float prev[4];
+            bilinear(fetchPrev, Wd, Hd, pux, puy, prev);
+            history = fminf_(prev[3], u.params4[1]) + 1.0f;
+            float alpha = 1.0f / history;
+            for (int c = 0; c < 3; c++) color[c] = mixf(prev[c], cur[c], alpha);
+          }
+        }
+      }
+      float v[4] = {color[0], color[1], color[2], history};
+      store(p, v);
+    }
+  }
+}
+
+// atrous.wgsl:26-83, one iteration at the given step (src/dst rgba16f).
+void orc_atrous(const void* uniforms, int Wd, int Hd, const void* src, int src_f32, const float* gbuf,
+                uint16_t* dst, int step) {
+  (void)uniforms;
+  const float K[3] = {0.375f, 0.25f, 0.0625f};
+  auto fetch = [&](size_t p, float out[4]) {
+    for (int c = 0; c < 4; c++)
+      out[c] = src_f32 ? ((const float*)src)[4 * p + c] : f16_to_f32(((const uint16_t*)src)[4 * p + c]);
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int py = 0; py < Hd; py++) {
+    for (int px = 0; px < Wd; px++) {
+      size_t p = (size_t)py * Wd + px;
+      float center[4]; fetch(p, center);
+      const float* g = gbuf + 4 * p;
+      if (g[3] < 0.0f) {
+        for (int c = 0; c < 4; c++) dst[4 * p + c] = f32_to_f16(center[c]);
+        continue;
+      }
+      float history = fmaxf_(center[3], 1.0f);
+      float lumC = luminance(center);
+      float relax = 2.0f / std::sqrt(history);
+      float sigmaL = fmaxf_(0.08f, relax);
+      float k00 = K[0] * K[0];
+      float sum[3] = {(center[0] * K[0]) * K[0], (center[1] * K[0]) * K[0], (center[2] * K[0]) * K[0]};
+      float wSum = k00;
+      for (int dy = -2; dy <= 2; dy++) {
+        for (int dx = -2; dx <= 2; dx++) {
+          if (dx == 0 && dy == 0) continue;
+          int qx = px + dx * step, qy = py + dy * step;
+          if (qx < 0 || qy < 0 || qx >= Wd || qy >= Hd) continue;
+          size_t q = (size_t)qy * Wd + qx;
+          float cq[4]; fetch(q, cq);
+          const float* gq = gbuf + 4 * q;
+          if (gq[3] < 0.0f) continue;
+          float wKernel = K[std::abs(dx)] * K[std::abs(dy)];
+          float nd = fmaxf_((g[0] * gq[0] + g[1] * gq[1]) + g[2] * gq[2], 0.0f);
+          float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;   // pow(., 32)
+          float wDepth = om_exp(-std::fabs(g[3] - gq[3]) / (0.05f * g[3] + 0.01f));
+          float wLum = om_exp(-std::fabs(lumC - luminance(cq)) / sigmaL);
+          float w = ((wKernel * n32) * wDepth) * wLum;
+          for (int c = 0; c < 3; c++) sum[c] = sum[c] + cq[c] * w;
+          wSum = wSum + w;
+        }
+      }
+      float den = fmaxf_(wSum, 1e-6f);
+      float v[4] = {sum[0] / den, sum[1] / den, sum[2] / den, center[3]};
+      for (int c = 0; c < 4; c++) dst[4 * p + c] = f32_to_f16(v[c]);
+    }
+  }
+}
+
+// present.wgsl:40-55 as a headless pass: texel-centre fetch of the final
+// illumination and the sqrt-albedo, remodulate, expose, ACES, gamma 1/2.2.
+void orc_present(const void* uniforms, int Wd, int Hd, const void* finalTex, int final_f32,
+                 const uint8_t* alb8, uint8_t* out_rgba8) {
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  const float exposure = u.params1[2];
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < Hd; y++) {
+    for (int x = 0; x < Wd; x++) {
+      size_t p = (size_t)y * Wd + x;
+      for (int c = 0; c < 3; c++) {
+        float il = final_f32 ? ((const float*)finalTex)[4 * p + c] : f16_to_f32(((const uint16_t*)finalTex)[4 * p + c]);
+        float as = (float)alb8[4 * p + c] / 255.0f;
+        float al = as * as;
+        float v = (il * al) * exposure;
+        float num = v * (2.51f * v + 0.03f);
+        float den = v * (2.43f * v + 0.59f) + 0.14f;
+        float t = clampf(num / den, 0.0f, 1.0f);
+        float g = om_pow(t, 0.454545468f);   // f32(1/2.2)
+        out_rgba8[4 * p + c] = unorm8(g);
+      }
+      out_rgba8[4 * p + 3] = 255;
+    }
+  }
+}
+
+// main.js:628-659: hdr = illum * (a/255) * (a/255), evaluated in double (JS
+// numbers) and stored as f32.
+void orc_hdr(int Wd, int Hd, const void* finalTex, int final_f32, const uint8_t* alb8, float* out_rgb) {
+  for (size_t p = 0; p < (size_t)Wd * Hd; p++) {
+    for (int c = 0; c < 3; c++) {
+      double il = final_f32 ? (double)((const float*)finalTex)[4 * p + c]
+                            : (double)f16_to_f32(((const uint16_t*)finalTex)[4 * p + c]);
+      double a = (double)alb8[4 * p + c] / 255.0;
+      out_rgb[3 * p + c] = (float)((il * a) * a);
+    }
+  }
+}
+
+// FP64 accumulation of the per-sample HDR radiance (radiance before
+// demodulation = demod * albedo is not recoverable bit-exactly, so the
+// accumulator sums the fp32 per-sample value rad*alb8^2/255^2 in double).
+// frames [frame0, frame0+spp) with the camera of `uniforms`.
+void orc_accumulate_f64(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                        const void* uniforms, float fclamp, int Wd, int Hd, uint32_t frame0, int spp,
+                        double* accum_rgb) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u0; std::memcpy(&u0, uniforms, sizeof(Uni));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int y = 0; y < Hd; y++) {
+    PixStats st{0, 0, 0, 0};
+    Uni u = u0;
+    for (int s = 0; s < spp; s++) {
+      u.params0[0] = frame0 + (uint32_t)s;
+      for (int x = 0; x < Wd; x++) {
+        float rad[4], gb[4]; uint8_t al[4];
+        path_pixel(W, u, fclamp, (uint32_t)x, (uint32_t)y, (uint32_t)Wd, (uint32_t)Hd, rad, al, gb, st);
+        size_t p = (size_t)y * Wd + x;
+        for (int c = 0; c < 3; c++) {
+          double a = (double)al[c] / 255.0;
+          accum_rgb[3 * p + c] += ((double)rad[c] * a) * a;
+        }
+      }
+    }
+  }
+}
+
+// Camera matrices (math.js:3-74, camera.js:47-57), evaluated in double like
+// JavaScript and stored as f32.  out: viewProj[16], invViewProj[16].
+static void js_mul(const float* a, const float* b, float* out) {
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++) {
+      double s = 0.0;
+      for (int k = 0; k < 4; k++) s += (double)a[k * 4 + r] * (double)b[c * 4 + k];
+      out[c * 4 + r] = (float)s;
+    }
+}
+
+void orc_camera_matrices(const double pos[3], double yaw, double pitch, double fovY, double aspect,
+                         double nearZ, double farZ, float* viewProj, float* invViewProj) {
+  double f = 1.0 / std::tan(fovY / 2.0);
+  float P[16] = {0}, IP[16] = {0};
+  P[0] = (float)(f / aspect); P[5] = (float)f; P[10] = (float)(farZ / (nearZ - farZ)); P[11] = -1.0f;
+  P[14] = (float)((nearZ * farZ) / (nearZ - farZ));
+  IP[0] = (float)(aspect / f); IP[5] = (float)(1.0 / f); IP[11] = (float)((nearZ - farZ) / (nearZ * farZ));
+  IP[14] = -1.0f; IP[15] = (float)(1.0 / nearZ);
+  double cp = std::cos(pitch), sp = std::sin(pitch), cy = std::cos(yaw), sy = std::sin(yaw);
+  double fw[3] = {sy * cp, sp, cy * cp};
+  double rt[3] = {-cy, 0.0, sy};
+  double up[3] = {rt[1] * fw[2] - rt[2] * fw[1], rt[2] * fw[0] - rt[0] * fw[2], rt[0] * fw[1] - rt[1] * fw[0]};
+  float C2W[16] = {(float)rt[0], (float)rt[1], (float)rt[2], 0.0f,
+                   (float)up[0], (float)up[1], (float)up[2], 0.0f,
+                   (float)-fw[0], (float)-fw[1], (float)-fw[2], 0.0f,
+                   (float)pos[0], (float)pos[1], (float)pos[2], 1.0f};
+  double z[3] = {-fw[0], -fw[1], -fw[2]};
+  auto dt = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  float W2C[16] = {(float)rt[0], (float)up[0], (float)z[0], 0.0f,
+                   (float)rt[1], (float)up[1], (float)z[1], 0.0f,
+                   (float)rt[2], (float)up[2], (float)z[2], 0.0f,
+                   (float)-dt(rt, pos), (float)-dt(up, pos), (float)-dt(z, pos), 1.0f};
+  js_mul(P, W2C, viewProj);
+  js_mul(C2W, IP, invViewProj);
+}
+
+// Scalar checks of the project transcendentals and storage conversions.
+void orc_math_eval(int fn, const float* x, float* y, int n) {
+  for (int i = 0; i < n; i++) {
+    float s, c;
+    switch (fn) {
+      case 0: om_sincos(x[i], s, c); y[i] = s; break;
+      case 1: om_sincos(x[i], s, c); y[i] = c; break;
+      case 2: y[i] = om_exp(x[i]); break;
+      case 3: y[i] = om_log2(x[i]); break;
+      case 4: y[i] = om_pow(x[i], 0.55f); break;
+      case 5: y[i] = om_pow(x[i], 0.454545468f); break;
+      case 6: y[i] = f16_to_f32(f32_to_f16(x[i])); break;
+      default: y[i] = NAN;
+    }
+  }
+}
+
+uint32_t orc_pcg_hash(uint32_t v) { return pcg_hash(v); }
+
+// Runs the path of rows [row0,row1) step row_step and returns every ray it
+// traced as 7 floats (origin xyz and maxT in voxel units, unit direction).
+// Writes at most `cap` rays to out7; returns the total number traced.
+long orc_collect_rays(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                      const void* uniforms, float fclamp, int Wd, int Hd, int row0, int row1, int row_step,
+                      float* out7, long cap) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  if (row_step < 1) row_step = 1;
+  std::vector<int> rows;
+  for (int y = row0; y < row1 && y < Hd; y += row_step) rows.push_back(y);
+  std::vector<std::vector<float>> logs(rows.size());
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ri = 0; ri < (int)rows.size(); ri++) {
+    tl_ray_log = &logs[ri];
+    PixStats st{0, 0, 0, 0};
+    for (int x = 0; x < Wd; x++) {
+      float rad[4], gb[4]; uint8_t al[4];
+      path_pixel(W, u, fclamp, (uint32_t)x, (uint32_t)rows[ri], (uint32_t)Wd, (uint32_t)Hd, rad, al, gb, st);
+    }
+    tl_ray_log = nullptr;
+  }
+  long total = 0;
+  for (auto& l : logs) {
+    long n = (long)(l.size() / 7);
+    long room = cap - total;
+    if (room > 0) std::memcpy(out7 + 7 * total, l.data(), sizeof(float) * 7 * (size_t)std::min(n, room));
+    total += n;
+  }
+  return total;
+}
+
+}  // extern "C"

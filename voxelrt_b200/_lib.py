@@ -1,0 +1,157 @@
+"""ctypes view of include/vrt.h (libvrt.so).
+
+The library is the product: this module only loads it and mirrors the C
+structs.  A missing library is an ImportError -- there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "libvrt.so"
+
+VRT_OK = 0
+ERR_NAMES = {1: "INVALID", 2: "CUDA", 3: "OOM", 4: "NO_DEVICE", 5: "BUDGET", 6: "TIMEOUT", 7: "STATE"}
+
+VRT_SCENE_VOXELRT = 0
+VRT_SCENE_SMALL = 1
+VRT_SCENE_FULL = 2
+VRT_SCENE_RANDOM = 3
+
+
+class VrtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"VRT_ERR_{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class VrtUniforms(C.Structure):
+    _fields_ = [
+        ("invViewProj", C.c_float * 16),
+        ("prevViewProj", C.c_float * 16),
+        ("camPos", C.c_float * 4),
+        ("prevCamPos", C.c_float * 4),
+        ("sunDir", C.c_float * 4),
+        ("sunRadiance", C.c_float * 4),
+        ("params0", C.c_uint32 * 4),
+        ("params1", C.c_float * 4),
+        ("params2", C.c_uint32 * 4),
+        ("params3", C.c_float * 4),
+        ("params4", C.c_float * 4),
+        ("params5", C.c_float * 4),
+        ("params6", C.c_float * 4),
+    ]
+
+
+class VrtDeviceConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class VrtSessionConfig(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("firefly_clamp", C.c_float),
+                ("accum_f32", C.c_int), ("keep_radiance_f32", C.c_int)]
+
+
+class VrtHit(C.Structure):
+    _fields_ = [("t", C.c_float), ("n", C.c_float * 3), ("mat", C.c_uint32), ("voxel", C.c_int32 * 3),
+                ("face", C.c_int32), ("steps", C.c_uint32), ("bytes", C.c_uint32), ("pad", C.c_uint32)]
+
+
+HIT_DTYPE = np.dtype([("t", "<f4"), ("n", "<f4", 3), ("mat", "<u4"), ("voxel", "<i4", 3), ("face", "<i4"),
+                      ("steps", "<u4"), ("bytes", "<u4"), ("pad", "<u4")])
+
+
+class VrtFrameStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("dda_outer", C.c_uint64), ("dda_inner", C.c_uint64),
+                ("voxel_reads", C.c_uint64), ("pixels", C.c_uint64), ("ms_pathtrace", C.c_float),
+                ("ms_temporal", C.c_float), ("ms_atrous", C.c_float), ("ms_present", C.c_float),
+                ("ms_total", C.c_float), ("launches", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class VrtCameraPose(C.Structure):
+    _fields_ = [("pos", C.c_double * 3), ("yaw", C.c_double), ("pitch", C.c_double), ("fov_y", C.c_double),
+                ("near_z", C.c_double), ("far_z", C.c_double)]
+
+
+class VrtLighting(C.Structure):
+    _fields_ = [("sun_dir", C.c_float * 3), ("sun_cos_radius", C.c_float), ("sun_irradiance", C.c_float * 3),
+                ("sky_intensity", C.c_float)]
+
+
+assert C.sizeof(VrtUniforms) == 304
+assert C.sizeof(VrtHit) == 48 == HIT_DTYPE.itemsize
+
+P = C.c_void_p
+I = C.c_int
+U32 = C.c_uint32
+SZ = C.c_size_t
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "vrt_abi_version": (I, []),
+    "vrt_last_error_string": (C.c_char_p, []),
+    "vrt_create": (I, [C.POINTER(VrtDeviceConfig), C.POINTER(P)]),
+    "vrt_destroy": (I, [P]),
+    "vrt_ctx_synchronize": (I, [P]),
+    "vrt_ctx_bytes_in_use": (C.c_uint64, [P]),
+    "vrt_scene_upload": (I, [P, P, I, C.POINTER(P)]),
+    "vrt_scene_upload_prebuilt": (I, [P, P, P, P, I, C.POINTER(P)]),
+    "vrt_scene_edit_box": (I, [P, I, I, I, I, I, I, U32]),
+    "vrt_scene_read": (I, [P, P, P, P]),
+    "vrt_scene_destroy": (I, [P]),
+    "vrt_trace_rays": (I, [P, P, P, P, I, P]),
+    "vrt_trace_rays_device": (I, [P, P, P, P, I, P]),
+    "vrt_session_create": (I, [P, P, C.POINTER(VrtSessionConfig), C.POINTER(P)]),
+    "vrt_session_destroy": (I, [P]),
+    "vrt_session_set_scene": (I, [P, P]),
+    "vrt_session_reset": (I, [P]),
+    "vrt_frame": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_pathtrace": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_temporal": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_atrous": (I, [P, C.POINTER(VrtUniforms), I]),
+    "vrt_pass_present": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_end_frame": (I, [P]),
+    "vrt_session_set_timing": (I, [P, I]),
+    "vrt_session_last_stats": (I, [P, C.POINTER(VrtFrameStats)]),
+    "vrt_read_radiance": (I, [P, P, SZ]),
+    "vrt_read_radiance_f32": (I, [P, P, SZ]),
+    "vrt_read_albedo": (I, [P, P, SZ]),
+    "vrt_read_gbuffer": (I, [P, P, SZ]),
+    "vrt_read_accum": (I, [P, P, SZ]),
+    "vrt_read_denoise": (I, [P, I, P, SZ]),
+    "vrt_read_final": (I, [P, P, SZ]),
+    "vrt_read_ldr": (I, [P, P, SZ]),
+    "vrt_read_hdr": (I, [P, P, SZ]),
+    "vrt_write_history": (I, [P, P, P]),
+    "vrt_make_uniforms": (I, [C.POINTER(VrtCameraPose), C.POINTER(VrtCameraPose), C.POINTER(VrtLighting), U32, U32,
+                              U32, I, I, C.c_float, C.c_float, C.POINTER(VrtUniforms)]),
+    "vrt_camera_matrices": (I, [C.POINTER(VrtCameraPose), C.c_double, P, P]),
+    "vrt_camera_spline": (I, [C.POINTER(VrtCameraPose), I, C.POINTER(VrtCameraPose)]),
+    "vrt_scene_generate": (I, [I, I, U32, P, C.POINTER(VrtCameraPose)]),
+}
+
+
+def _load() -> C.CDLL:
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python -m voxelrt_b200.build` (no CPU fallback exists)")
+    lib = C.CDLL(str(_LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(code: int) -> None:
+    if code != VRT_OK:
+        raise VrtError(code, lib.vrt_last_error_string().decode(errors="replace"))
+
+
+def ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)

@@ -1,0 +1,254 @@
+"""Pythonic host interface over the C ABI, mirroring the reference renderer's
+operator surface: a device context, a device-resident voxel scene
+(generateScene + brick build, scene.js), per-view sessions holding the render
+targets (main.js:335-360), and frame()/pass calls in the reference pass order
+(main.js:680-772).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import (HIT_DTYPE, VrtCameraPose, VrtDeviceConfig, VrtFrameStats, VrtLighting, VrtSessionConfig,
+                   VrtUniforms, check, lib, ptr)
+
+# Reference constants (scene.js:5-6, common.wgsl:11)
+VOXEL_SIZE = 1.0 / 16.0
+BRICK = 8
+FLAG_TEMPORAL = 1
+FLAG_DENOISE = 2
+
+
+@dataclass
+class Lighting:
+    """Sun and sky (uniform slots sunDir / sunRadiance)."""
+    sun_dir: tuple = (0.3, 0.8, 0.5)
+    sun_cos_radius: float = math.cos(math.radians(0.27))
+    sun_irradiance: tuple = (3.0, 3.0, 3.0)
+    sky_intensity: float = 1.0
+
+    def c(self) -> VrtLighting:
+        l = VrtLighting()
+        l.sun_dir[:] = [float(v) for v in self.sun_dir]
+        l.sun_cos_radius = float(self.sun_cos_radius)
+        l.sun_irradiance[:] = [float(v) for v in self.sun_irradiance]
+        l.sky_intensity = float(self.sky_intensity)
+        return l
+
+    @staticmethod
+    def reference_default() -> "Lighting":
+        """main.js:402-412: azimuth 0.9, elevation 0.85, radius 0.03 rad, E=(5,4.5,3.8)."""
+        el, az = 0.85, 0.9
+        return Lighting((math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az)),
+                        math.cos(0.03), (5.0, 4.5, 3.8), 1.0)
+
+
+@dataclass
+class CameraPose:
+    pos: tuple
+    yaw: float = 0.0
+    pitch: float = 0.0
+    fov_y: float = math.radians(70.0)
+    near_z: float = 0.05
+    far_z: float = 400.0
+
+    def c(self) -> VrtCameraPose:
+        p = VrtCameraPose()
+        p.pos[:] = [float(v) for v in self.pos]
+        p.yaw, p.pitch, p.fov_y, p.near_z, p.far_z = self.yaw, self.pitch, self.fov_y, self.near_z, self.far_z
+        return p
+
+    @staticmethod
+    def from_c(p: VrtCameraPose) -> "CameraPose":
+        return CameraPose(tuple(p.pos), p.yaw, p.pitch, p.fov_y, p.near_z, p.far_z)
+
+
+def generate_scene(kind: int, n: int, seed: int):
+    """Procedural voxel world (packed u32, N^3) and its default camera pose."""
+    vox = np.empty(n * n * n, np.uint32)
+    spawn = VrtCameraPose()
+    check(lib.vrt_scene_generate(int(kind), int(n), int(seed) & 0xFFFFFFFF, ptr(vox), C.byref(spawn)))
+    return vox, CameraPose.from_c(spawn)
+
+
+def camera_spline(spawn: CameraPose, frame: int) -> CameraPose:
+    out = VrtCameraPose()
+    check(lib.vrt_camera_spline(C.byref(spawn.c()), int(frame), C.byref(out)))
+    return CameraPose.from_c(out)
+
+
+def camera_matrices(pose: CameraPose, aspect: float):
+    vp = np.empty(16, np.float32)
+    ivp = np.empty(16, np.float32)
+    check(lib.vrt_camera_matrices(C.byref(pose.c()), float(aspect), ptr(vp), ptr(ivp)))
+    return vp, ivp
+
+
+def make_uniforms(cur: CameraPose, prev: CameraPose | None, light: Lighting, frame: int, bounces: int, flags: int,
+                  width: int, height: int, exposure: float = 1.0, max_history: float = 64.0) -> VrtUniforms:
+    u = VrtUniforms()
+    check(lib.vrt_make_uniforms(C.byref(cur.c()), C.byref(prev.c()) if prev is not None else None,
+                                C.byref(light.c()), int(frame) & 0xFFFFFFFF, int(bounces), int(flags), int(width),
+                                int(height), float(exposure), float(max_history), C.byref(u)))
+    return u
+
+
+def uniforms_bytes(u: VrtUniforms) -> bytes:
+    return C.string_at(C.addressof(u), C.sizeof(u))
+
+
+class Context:
+    """A CUDA device with its own stream and an HBM admission budget."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        cfg = VrtDeviceConfig(int(device), int(hbm_budget_bytes))
+        h = C.c_void_p()
+        check(lib.vrt_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def synchronize(self) -> None:
+        check(lib.vrt_ctx_synchronize(self.h))
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib.vrt_ctx_bytes_in_use(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            lib.vrt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """Device-resident voxel grid + bricks + masks (+ occupancy bitmap)."""
+
+    def __init__(self, ctx: Context, voxels: np.ndarray, n: int, bricks=None, masks=None):
+        voxels = np.ascontiguousarray(voxels, np.uint32)
+        assert voxels.size == n ** 3
+        h = C.c_void_p()
+        if bricks is None:
+            check(lib.vrt_scene_upload(ctx.h, ptr(voxels), int(n), C.byref(h)))
+        else:
+            b = np.ascontiguousarray(bricks, np.uint32)
+            m = np.ascontiguousarray(masks, np.uint32)
+            check(lib.vrt_scene_upload_prebuilt(ctx.h, ptr(voxels), ptr(b), ptr(m), int(n), C.byref(h)))
+        self.h, self.ctx, self.n = h, ctx, n
+
+    def edit_box(self, x0, y0, z0, x1, y1, z1, value: int) -> None:
+        check(lib.vrt_scene_edit_box(self.h, x0, y0, z0, x1, y1, z1, int(value) & 0xFFFFFFFF))
+
+    def read(self):
+        n, bg = self.n, self.n // BRICK
+        v = np.empty(n ** 3, np.uint32)
+        b = np.empty(bg ** 3, np.uint32)
+        m = np.empty(16 * bg ** 3, np.uint32)
+        check(lib.vrt_scene_read(self.h, ptr(v), ptr(b), ptr(m)))
+        return v, b, m
+
+    def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax: np.ndarray) -> np.ndarray:
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(tmax, np.float32).reshape(-1)
+        n = o.shape[0]
+        out = np.zeros(n, HIT_DTYPE)
+        check(lib.vrt_trace_rays(self.h, ptr(o), ptr(d), ptr(t), n, ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            lib.vrt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Session:
+    """Render targets of one view (radiance, albedo, G-buffer x2, history x2,
+    denoise x2, LDR) and the frame loop over them."""
+
+    def __init__(self, ctx: Context, scene: Scene, width: int, height: int, firefly_clamp: float = 48.0,
+                 accum_f32: bool = False, keep_radiance_f32: bool = False):
+        cfg = VrtSessionConfig(int(width), int(height), float(firefly_clamp), int(bool(accum_f32)),
+                               int(bool(keep_radiance_f32)))
+        h = C.c_void_p()
+        check(lib.vrt_session_create(ctx.h, scene.h, C.byref(cfg), C.byref(h)))
+        self.h, self.ctx, self.scene = h, ctx, scene
+        self.w, self.h_px = int(width), int(height)
+        self.accum_f32 = bool(accum_f32)
+
+    # frame + passes --------------------------------------------------------
+    def frame(self, u: VrtUniforms) -> None:
+        check(lib.vrt_frame(self.h, C.byref(u)))
+
+    def pathtrace(self, u): check(lib.vrt_pass_pathtrace(self.h, C.byref(u)))
+    def temporal(self, u): check(lib.vrt_pass_temporal(self.h, C.byref(u)))
+    def atrous(self, u, it): check(lib.vrt_pass_atrous(self.h, C.byref(u), int(it)))
+    def present(self, u): check(lib.vrt_pass_present(self.h, C.byref(u)))
+    def end_frame(self): check(lib.vrt_end_frame(self.h))
+    def reset(self): check(lib.vrt_session_reset(self.h))
+
+    def set_scene(self, scene: Scene) -> None:
+        check(lib.vrt_session_set_scene(self.h, scene.h))
+        self.scene = scene
+
+    def set_timing(self, on: bool) -> None:
+        check(lib.vrt_session_set_timing(self.h, int(bool(on))))
+
+    def stats(self) -> VrtFrameStats:
+        s = VrtFrameStats()
+        check(lib.vrt_session_last_stats(self.h, C.byref(s)))
+        return s
+
+    # readbacks -------------------------------------------------------------
+    def _read(self, fn, dtype, comps, *extra):
+        a = np.empty((self.h_px, self.w, comps), dtype)
+        check(fn(self.h, *extra, ptr(a), a.nbytes))
+        return a
+
+    def radiance(self): return self._read(lib.vrt_read_radiance, np.uint16, 4)
+    def radiance_f32(self): return self._read(lib.vrt_read_radiance_f32, np.float32, 4)
+    def albedo(self): return self._read(lib.vrt_read_albedo, np.uint8, 4)
+    def gbuffer(self): return self._read(lib.vrt_read_gbuffer, np.float32, 4)
+    def ldr(self): return self._read(lib.vrt_read_ldr, np.uint8, 4)
+    def denoise(self, i): return self._read(lib.vrt_read_denoise, np.uint16, 4, int(i))
+
+    def accum(self):
+        return self._read(lib.vrt_read_accum, np.float32 if self.accum_f32 else np.uint16, 4)
+
+    def final(self, denoised: bool):
+        f32 = self.accum_f32 and not denoised
+        return self._read(lib.vrt_read_final, np.float32 if f32 else np.uint16, 4)
+
+    def hdr(self):
+        a = np.empty((self.h_px, self.w, 3), np.float32)
+        check(lib.vrt_read_hdr(self.h, ptr(a), a.nbytes))
+        return a
+
+    def write_history(self, accum_prev: np.ndarray | None, gbuf_prev: np.ndarray | None) -> None:
+        a = None if accum_prev is None else np.ascontiguousarray(accum_prev)
+        g = None if gbuf_prev is None else np.ascontiguousarray(gbuf_prev, np.float32)
+        check(lib.vrt_write_history(self.h, ptr(a) if a is not None else None, ptr(g) if g is not None else None))
+
+    def close(self) -> None:
+        if self.h:
+            lib.vrt_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,624 @@
+// vrt_api.cpp -- host side of the C ABI (include/vrt.h).
+//
+// Owns contexts (device + stream + HBM admission budget), device-resident
+// scenes and per-view sessions, and drives the reference's pass order
+// (main.js:680-772): pathtrace -> temporal -> a-trous x3 -> present, with
+// G-buffer and history ping-ponged by frame parity (main.js:429-431) and the
+// a-trous chain accum -> dA -> dB -> dA (main.js:503-507).
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <mutex>
+#include "vrt_internal.h"
+
+using namespace vrt;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                           \
+  do {                                                                                           \
+    cudaError_t e_ = (expr);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      return fail(e_ == cudaErrorMemoryAllocation ? VRT_ERR_OOM : VRT_ERR_CUDA, "%s: %s (%s:%d)", \
+                  #expr, cudaGetErrorString(e_), __FILE__, __LINE__);                            \
+    }                                                                                            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// objects
+// ---------------------------------------------------------------------------
+struct VrtCtx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;   // 0 = unlimited
+  uint64_t used = 0;
+};
+
+struct VrtScene {
+  VrtCtx* ctx = nullptr;
+  SceneDev dev;
+  uint64_t bytes = 0;
+};
+
+struct VrtSession {
+  VrtCtx* ctx = nullptr;
+  VrtScene* scene = nullptr;
+  int W = 0, H = 0;
+  float fclamp = 48.0f;
+  bool acc_f32 = false;
+  bool keep_f32 = false;
+  uint64_t bytes = 0;
+  // render targets (main.js:82-90 equivalents)
+  void* rad16 = nullptr;
+  void* rad32 = nullptr;
+  uint32_t* alb8 = nullptr;
+  void* gbuf[2] = {nullptr, nullptr};
+  void* accum[2] = {nullptr, nullptr};
+  void* den[2] = {nullptr, nullptr};
+  uint32_t* ldr = nullptr;
+  unsigned long long* stats = nullptr;
+  // frame state
+  uint64_t frame_counter = 0;     // host frame index (parity source)
+  bool last_denoise = false;
+  bool have_frame = false;
+  int last_parity = 0;
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[6] = {};
+  uint32_t launches = 0;
+};
+
+static int set_dev(VrtCtx* ctx) {
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  return VRT_OK;
+}
+
+static int dev_alloc(VrtCtx* ctx, void** p, size_t bytes, uint64_t* acct) {
+  if (ctx->budget && ctx->used + bytes > ctx->budget)
+    return fail(VRT_ERR_BUDGET, "HBM budget exceeded: in use %llu + request %zu > budget %llu",
+                (unsigned long long)ctx->used, bytes, (unsigned long long)ctx->budget);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(VRT_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->used += bytes;
+  *acct += bytes;
+  return VRT_OK;
+}
+
+static void dev_free(VrtCtx* ctx, void* p, size_t bytes, uint64_t* acct) {
+  if (!p) return;
+  cudaFree(p);
+  ctx->used -= bytes;
+  *acct -= bytes;
+}
+
+extern "C" {
+
+int vrt_abi_version(void) { return VRT_ABI_VERSION; }
+const char* vrt_last_error_string(void) { return g_err.c_str(); }
+
+int vrt_create(const VrtDeviceConfig* cfg, VrtCtx** out) {
+  if (!out) return fail(VRT_ERR_INVALID, "vrt_create: out is NULL");
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(VRT_ERR_NO_DEVICE, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+  VrtCtx* c = new VrtCtx();
+  c->device = cfg ? cfg->device : 0;
+  c->budget = cfg ? cfg->hbm_budget_bytes : 0;
+  if (c->device < 0 || c->device >= n) {
+    delete c;
+    return fail(VRT_ERR_INVALID, "device %d out of range (%d devices)", cfg ? cfg->device : 0, n);
+  }
+  e = cudaSetDevice(c->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(VRT_ERR_CUDA, "context init: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return VRT_OK;
+}
+
+int vrt_destroy(VrtCtx* ctx) {
+  if (!ctx) return VRT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return VRT_OK;
+}
+
+int vrt_ctx_synchronize(VrtCtx* ctx) {
+  if (!ctx) return fail(VRT_ERR_INVALID, "ctx is NULL");
+  if (int r = set_dev(ctx)) return r;
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return VRT_OK;
+}
+
+uint64_t vrt_ctx_bytes_in_use(const VrtCtx* ctx) { return ctx ? ctx->used : 0; }
+
+// ---------------------------------------------------------------------------
+// scenes
+// ---------------------------------------------------------------------------
+static int scene_alloc(VrtCtx* ctx, int N, VrtScene** out) {
+  if (!ctx || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (N < 8 || N % 8 != 0 || N > 2048) return fail(VRT_ERR_INVALID, "grid size %d must be a multiple of 8 in [8, 2048]", N);
+  if (int r = set_dev(ctx)) return r;
+  VrtScene* s = new VrtScene();
+  s->ctx = ctx;
+  s->dev.N = N;
+  s->dev.BG = N / 8;
+  const size_t nv = (size_t)N * N * N, nb = (size_t)s->dev.BG * s->dev.BG * s->dev.BG;
+  int r = dev_alloc(ctx, (void**)&s->dev.vox, nv * 4, &s->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&s->dev.bricks, nb * 4, &s->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&s->dev.masks, nb * 64, &s->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&s->dev.bits, occ_words(s->dev.BG) * 4 + 128, &s->bytes);
+  if (r) {
+    std::string keep = g_err;
+    vrt_scene_destroy(s);
+    g_err = keep;
+    return r;
+  }
+  *out = s;
+  return VRT_OK;
+}
+
+int vrt_scene_upload(VrtCtx* ctx, const uint32_t* voxels, int N, VrtScene** out) {
+  if (!voxels) return fail(VRT_ERR_INVALID, "voxels is NULL");
+  VrtScene* s = nullptr;
+  if (int r = scene_alloc(ctx, N, &s)) return r;
+  const size_t nv = (size_t)N * N * N;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(s->dev.vox, voxels, nv * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_build_bricks(s->dev, 0, 0, 0, s->dev.BG - 1, s->dev.BG - 1, s->dev.BG - 1, st);
+  if (e == cudaSuccess) e = launch_build_bits(s->dev, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    vrt_scene_destroy(s);
+    return fail(VRT_ERR_CUDA, "scene upload: %s", cudaGetErrorString(e));
+  }
+  *out = s;
+  return VRT_OK;
+}
+
+int vrt_scene_upload_prebuilt(VrtCtx* ctx, const uint32_t* voxels, const uint32_t* bricks,
+                              const uint32_t* brick_masks, int N, VrtScene** out) {
+  if (!voxels || !bricks || !brick_masks) return fail(VRT_ERR_INVALID, "NULL buffer");
+  VrtScene* s = nullptr;
+  if (int r = scene_alloc(ctx, N, &s)) return r;
+  const size_t nv = (size_t)N * N * N, nb = (size_t)s->dev.BG * s->dev.BG * s->dev.BG;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(s->dev.vox, voxels, nv * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->dev.bricks, bricks, nb * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->dev.masks, brick_masks, nb * 64, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_build_bits(s->dev, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    vrt_scene_destroy(s);
+    return fail(VRT_ERR_CUDA, "scene upload: %s", cudaGetErrorString(e));
+  }
+  *out = s;
+  return VRT_OK;
+}
+
+int vrt_scene_edit_box(VrtScene* s, int x0, int y0, int z0, int x1, int y1, int z1, uint32_t value) {
+  if (!s) return fail(VRT_ERR_INVALID, "scene is NULL");
+  const int N = s->dev.N;
+  if (x0 > x1) std::swap(x0, x1);
+  if (y0 > y1) std::swap(y0, y1);
+  if (z0 > z1) std::swap(z0, z1);
+  x0 = std::max(x0, 0); y0 = std::max(y0, 0); z0 = std::max(z0, 0);
+  x1 = std::min(x1, N - 1); y1 = std::min(y1, N - 1); z1 = std::min(z1, N - 1);
+  if (x0 > x1 || y0 > y1 || z0 > z1) return VRT_OK;   // box fully outside: nothing to do
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  CUDA_TRY(launch_fill_box(s->dev, x0, y0, z0, x1, y1, z1, value, st));
+  CUDA_TRY(launch_build_bricks(s->dev, x0 / 8, y0 / 8, z0 / 8, x1 / 8, y1 / 8, z1 / 8, st));
+  CUDA_TRY(launch_build_bits(s->dev, st));
+  return VRT_OK;
+}
+
+int vrt_scene_read(VrtScene* s, uint32_t* voxels, uint32_t* bricks, uint32_t* masks) {
+  if (!s) return fail(VRT_ERR_INVALID, "scene is NULL");
+  if (int r = set_dev(s->ctx)) return r;
+  const size_t N = s->dev.N, nb = (size_t)s->dev.BG * s->dev.BG * s->dev.BG;
+  cudaStream_t st = s->ctx->stream;
+  if (voxels) CUDA_TRY(cudaMemcpyAsync(voxels, s->dev.vox, N * N * N * 4, cudaMemcpyDeviceToHost, st));
+  if (bricks) CUDA_TRY(cudaMemcpyAsync(bricks, s->dev.bricks, nb * 4, cudaMemcpyDeviceToHost, st));
+  if (masks) CUDA_TRY(cudaMemcpyAsync(masks, s->dev.masks, nb * 64, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return VRT_OK;
+}
+
+int vrt_scene_destroy(VrtScene* s) {
+  if (!s) return VRT_OK;
+  VrtCtx* c = s->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  const size_t N = s->dev.N, nb = (size_t)s->dev.BG * s->dev.BG * s->dev.BG;
+  dev_free(c, s->dev.vox, N * N * N * 4, &s->bytes);
+  dev_free(c, s->dev.bricks, nb * 4, &s->bytes);
+  dev_free(c, s->dev.masks, nb * 64, &s->bytes);
+  dev_free(c, s->dev.bits, occ_words(s->dev.BG) * 4 + 128, &s->bytes);
+  delete s;
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// DDA parity entry
+// ---------------------------------------------------------------------------
+int vrt_trace_rays_device(VrtScene* s, const float* o, const float* d, const float* tmax, int n, VrtHit* out) {
+  if (!s || n < 0) return fail(VRT_ERR_INVALID, "bad argument");
+  if (n == 0) return VRT_OK;
+  if (!o || !d || !tmax || !out) return fail(VRT_ERR_INVALID, "NULL buffer");
+  if (int r = set_dev(s->ctx)) return r;
+  CUDA_TRY(launch_trace_rays(s->dev, o, d, tmax, n, out, s->ctx->stream));
+  return VRT_OK;
+}
+
+int vrt_trace_rays(VrtScene* s, const float* o, const float* d, const float* tmax, int n, VrtHit* out) {
+  if (!s || n < 0) return fail(VRT_ERR_INVALID, "bad argument");
+  if (n == 0) return VRT_OK;
+  if (!o || !d || !tmax || !out) return fail(VRT_ERR_INVALID, "NULL buffer");
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  char* buf = nullptr;
+  const size_t bo = (size_t)n * 12, bt = (size_t)n * 4, bh = (size_t)n * sizeof(VrtHit);
+  CUDA_TRY(cudaMalloc(&buf, 2 * bo + bt + bh));
+  float* dO = (float*)buf;
+  float* dD = (float*)(buf + bo);
+  float* dT = (float*)(buf + 2 * bo);
+  VrtHit* dH = (VrtHit*)(buf + 2 * bo + bt);
+  cudaError_t e = cudaMemcpyAsync(dO, o, bo, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dD, d, bo, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dT, tmax, bt, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_trace_rays(s->dev, dO, dD, dT, n, dH, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dH, bh, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(VRT_ERR_CUDA, "trace_rays: %s", cudaGetErrorString(e));
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sessions
+// ---------------------------------------------------------------------------
+static size_t px(const VrtSession* s) { return (size_t)s->W * s->H; }
+static size_t acc_bpp(const VrtSession* s) { return s->acc_f32 ? 16 : 8; }
+
+int vrt_session_destroy(VrtSession* s) {
+  if (!s) return VRT_OK;
+  VrtCtx* c = s->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  const size_t P = px(s);
+  dev_free(c, s->rad16, P * 8, &s->bytes);
+  dev_free(c, s->rad32, P * 16, &s->bytes);
+  dev_free(c, s->alb8, P * 4, &s->bytes);
+  for (int i = 0; i < 2; i++) {
+    dev_free(c, s->gbuf[i], P * 16, &s->bytes);
+    dev_free(c, s->accum[i], P * acc_bpp(s), &s->bytes);
+    dev_free(c, s->den[i], P * 8, &s->bytes);
+  }
+  dev_free(c, s->ldr, P * 4, &s->bytes);
+  dev_free(c, s->stats, kStatCount * 8, &s->bytes);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  delete s;
+  return VRT_OK;
+}
+
+int vrt_session_reset(VrtSession* s) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = set_dev(s->ctx)) return r;
+  const size_t P = px(s);
+  cudaStream_t st = s->ctx->stream;
+  for (int i = 0; i < 2; i++) {
+    CUDA_TRY(cudaMemsetAsync(s->gbuf[i], 0, P * 16, st));
+    CUDA_TRY(cudaMemsetAsync(s->accum[i], 0, P * acc_bpp(s), st));
+    CUDA_TRY(cudaMemsetAsync(s->den[i], 0, P * 8, st));
+  }
+  CUDA_TRY(cudaMemsetAsync(s->rad16, 0, P * 8, st));
+  if (s->rad32) CUDA_TRY(cudaMemsetAsync(s->rad32, 0, P * 16, st));
+  CUDA_TRY(cudaMemsetAsync(s->alb8, 0, P * 4, st));
+  CUDA_TRY(cudaMemsetAsync(s->ldr, 0, P * 4, st));
+  CUDA_TRY(cudaMemsetAsync(s->stats, 0, kStatCount * 8, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  s->frame_counter = 0;
+  s->have_frame = false;
+  s->last_parity = 0;
+  return VRT_OK;
+}
+
+int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg, VrtSession** out) {
+  if (!ctx || !scene || !cfg || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (cfg->width < 1 || cfg->height < 1 || cfg->width > 16384 || cfg->height > 16384)
+    return fail(VRT_ERR_INVALID, "render size %dx%d out of range", cfg->width, cfg->height);
+  if (scene->ctx != ctx) return fail(VRT_ERR_INVALID, "scene belongs to another context");
+  if (int r = set_dev(ctx)) return r;
+  VrtSession* s = new VrtSession();
+  s->ctx = ctx;
+  s->scene = scene;
+  s->W = cfg->width;
+  s->H = cfg->height;
+  s->fclamp = cfg->firefly_clamp;
+  s->acc_f32 = cfg->accum_f32 != 0;
+  s->keep_f32 = cfg->keep_radiance_f32 != 0;
+  const size_t P = px(s);
+  int r = dev_alloc(ctx, &s->rad16, P * 8, &s->bytes);
+  if (!r && s->keep_f32) r = dev_alloc(ctx, &s->rad32, P * 16, &s->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&s->alb8, P * 4, &s->bytes);
+  for (int i = 0; i < 2 && !r; i++) {
+    r = dev_alloc(ctx, &s->gbuf[i], P * 16, &s->bytes);
+    if (!r) r = dev_alloc(ctx, &s->accum[i], P * acc_bpp(s), &s->bytes);
+    if (!r) r = dev_alloc(ctx, &s->den[i], P * 8, &s->bytes);
+  }
+  if (!r) r = dev_alloc(ctx, (void**)&s->ldr, P * 4, &s->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&s->stats, kStatCount * 8, &s->bytes);
+  if (!r) {
+    for (auto& e : s->ev) {
+      if (cudaEventCreate(&e) != cudaSuccess) { r = fail(VRT_ERR_CUDA, "cudaEventCreate failed"); break; }
+    }
+  }
+  if (!r) r = vrt_session_reset(s);
+  if (r) {
+    std::string keep = g_err;
+    vrt_session_destroy(s);
+    g_err = keep;
+    return r;
+  }
+  *out = s;
+  return VRT_OK;
+}
+
+int vrt_session_set_scene(VrtSession* s, VrtScene* scene) {
+  if (!s || !scene || scene->ctx != s->ctx) return fail(VRT_ERR_INVALID, "bad scene");
+  s->scene = scene;
+  return VRT_OK;
+}
+
+int vrt_session_set_timing(VrtSession* s, int enable) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  s->timing = enable != 0;
+  return VRT_OK;
+}
+
+static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
+  if (!u) return fail(VRT_ERR_INVALID, "uniforms is NULL");
+  if ((int)u->params1[0] != s->W || (int)u->params1[1] != s->H)
+    return fail(VRT_ERR_INVALID, "uniform render size %gx%g does not match session %dx%d", u->params1[0],
+                u->params1[1], s->W, s->H);
+  if (u->params2[0] != 0u)
+    return fail(VRT_ERR_INVALID, "restir flags 0x%x set: only the plain path (preset=base) is implemented",
+                u->params2[0]);
+  return VRT_OK;
+}
+
+static int parity_of(const VrtSession* s) { return (int)(s->frame_counter & 1u); }
+
+int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (int r = set_dev(s->ctx)) return r;
+  PathOut o;
+  o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
+  CUDA_TRY(launch_pathtrace(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->ctx->stream));
+  s->launches++;
+  return VRT_OK;
+}
+
+int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (int r = set_dev(s->ctx)) return r;
+  const int p = parity_of(s);
+  CUDA_TRY(launch_temporal(*u, s->W, s->H, s->rad16, s->gbuf[p], s->accum[1 - p], s->gbuf[1 - p], s->accum[p],
+                           s->acc_f32, s->ctx->stream));
+  s->launches++;
+  return VRT_OK;
+}
+
+int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int it) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (it < 0 || it > 2) return fail(VRT_ERR_INVALID, "a-trous iteration %d not in 0..2", it);
+  if (int r = set_dev(s->ctx)) return r;
+  const int p = parity_of(s);
+  // chain accum -> dA (1) -> dB (2) -> dA (4)   (main.js:503-507)
+  const void* src = it == 0 ? s->accum[p] : (it == 1 ? s->den[0] : s->den[1]);
+  const bool src_f32 = it == 0 && s->acc_f32;
+  void* dst = it == 1 ? s->den[1] : s->den[0];
+  CUDA_TRY(launch_atrous(s->W, s->H, src, src_f32, s->gbuf[p], dst, 1 << it, s->ctx->stream));
+  s->launches++;
+  return VRT_OK;
+}
+
+static const void* final_buf(const VrtSession* s, int parity, bool denoise, bool* f32) {
+  *f32 = !denoise && s->acc_f32;
+  return denoise ? s->den[0] : s->accum[parity];
+}
+
+int vrt_pass_present(VrtSession* s, const VrtUniforms* u) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (int r = set_dev(s->ctx)) return r;
+  const bool denoise = (u->params0[2] & 2u) != 0u;
+  bool f32;
+  const void* fin = final_buf(s, parity_of(s), denoise, &f32);
+  CUDA_TRY(launch_present(*u, s->W, s->H, fin, f32, s->alb8, s->ldr, s->ctx->stream));
+  s->launches++;
+  s->last_denoise = denoise;
+  return VRT_OK;
+}
+
+int vrt_end_frame(VrtSession* s) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  s->last_parity = parity_of(s);
+  s->have_frame = true;
+  s->frame_counter++;
+  return VRT_OK;
+}
+
+int vrt_frame(VrtSession* s, const VrtUniforms* u) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  s->launches = 0;
+  CUDA_TRY(cudaMemsetAsync(s->stats, 0, kStatCount * 8, st));
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[0], st));
+  if (int r = vrt_pass_pathtrace(s, u)) return r;
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[1], st));
+  if (int r = vrt_pass_temporal(s, u)) return r;
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[2], st));
+  const bool denoise = (u->params0[2] & 2u) != 0u;
+  if (denoise)
+    for (int it = 0; it < 3; it++)
+      if (int r = vrt_pass_atrous(s, u, it)) return r;
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[3], st));
+  if (int r = vrt_pass_present(s, u)) return r;
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[4], st));
+  return vrt_end_frame(s);
+}
+
+int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
+  if (!s || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(s->ctx)) return r;
+  std::memset(out, 0, sizeof(*out));
+  unsigned long long h[kStatCount];
+  CUDA_TRY(cudaMemcpyAsync(h, s->stats, sizeof h, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  out->rays = h[kStatRays];
+  out->dda_outer = h[kStatOuter];
+  out->dda_inner = h[kStatInner];
+  out->voxel_reads = h[kStatVReads];
+  out->pixels = h[kStatPixels];
+  out->launches = s->launches;
+  if (s->timing && s->have_frame) {
+    float a = 0, b = 0, c = 0, d = 0;
+    CUDA_TRY(cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
+    CUDA_TRY(cudaEventElapsedTime(&c, s->ev[2], s->ev[3]));
+    CUDA_TRY(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
+    out->ms_pathtrace = a; out->ms_temporal = b; out->ms_atrous = c; out->ms_present = d;
+    out->ms_total = a + b + c + d;
+  }
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// readbacks
+// ---------------------------------------------------------------------------
+static int read_buf(VrtSession* s, const void* dev, size_t need, void* host, size_t bytes) {
+  if (!s || !host) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (!dev) return fail(VRT_ERR_STATE, "buffer not allocated for this session");
+  if (bytes < need) return fail(VRT_ERR_INVALID, "host buffer %zu bytes < %zu needed", bytes, need);
+  if (int r = set_dev(s->ctx)) return r;
+  CUDA_TRY(cudaMemcpyAsync(host, dev, need, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  return VRT_OK;
+}
+
+static int done_parity(const VrtSession* s) { return s->have_frame ? s->last_parity : parity_of(s); }
+
+int vrt_read_radiance(VrtSession* s, void* h, size_t b) { return read_buf(s, s ? s->rad16 : nullptr, s ? px(s) * 8 : 0, h, b); }
+int vrt_read_radiance_f32(VrtSession* s, void* h, size_t b) { return read_buf(s, s ? s->rad32 : nullptr, s ? px(s) * 16 : 0, h, b); }
+int vrt_read_albedo(VrtSession* s, void* h, size_t b) { return read_buf(s, s ? s->alb8 : nullptr, s ? px(s) * 4 : 0, h, b); }
+int vrt_read_gbuffer(VrtSession* s, void* h, size_t b) {
+  return read_buf(s, s ? s->gbuf[done_parity(s)] : nullptr, s ? px(s) * 16 : 0, h, b);
+}
+int vrt_read_accum(VrtSession* s, void* h, size_t b) {
+  return read_buf(s, s ? s->accum[done_parity(s)] : nullptr, s ? px(s) * acc_bpp(s) : 0, h, b);
+}
+int vrt_read_denoise(VrtSession* s, int i, void* h, size_t b) {
+  if (i < 0 || i > 1) return fail(VRT_ERR_INVALID, "denoise index %d", i);
+  return read_buf(s, s ? s->den[i] : nullptr, s ? px(s) * 8 : 0, h, b);
+}
+int vrt_read_final(VrtSession* s, void* h, size_t b) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  bool f32;
+  const void* fin = final_buf(s, done_parity(s), s->last_denoise, &f32);
+  return read_buf(s, fin, px(s) * (f32 ? 16 : 8), h, b);
+}
+int vrt_read_ldr(VrtSession* s, void* h, size_t b) { return read_buf(s, s ? s->ldr : nullptr, s ? px(s) * 4 : 0, h, b); }
+
+static float half_to_float(uint16_t hbits) {
+  const uint32_t sign = (uint32_t)(hbits & 0x8000u) << 16;
+  const uint32_t e = (hbits >> 10) & 0x1fu, m = hbits & 0x3ffu;
+  uint32_t out;
+  if (e == 0) {
+    float v = (float)m * 5.96046448e-08f;
+    return sign ? -v : v;
+  }
+  if (e == 31) out = sign | 0x7f800000u | (m << 13);
+  else out = sign | ((e + 112u) << 23) | (m << 13);
+  float f;
+  std::memcpy(&f, &out, 4);
+  return f;
+}
+
+// HDR capture of main.js:628-659: illum * (a/255)^2 in double, stored f32.
+int vrt_read_hdr(VrtSession* s, float* rgb, size_t bytes) {
+  if (!s || !rgb) return fail(VRT_ERR_INVALID, "NULL argument");
+  const size_t P = px(s);
+  if (bytes < P * 12) return fail(VRT_ERR_INVALID, "host buffer %zu bytes < %zu needed", bytes, P * 12);
+  bool f32;
+  final_buf(s, done_parity(s), s->last_denoise, &f32);
+  std::vector<uint8_t> fin(P * (f32 ? 16 : 8));
+  std::vector<uint8_t> alb(P * 4);
+  if (int r = vrt_read_final(s, fin.data(), fin.size())) return r;
+  if (int r = vrt_read_albedo(s, alb.data(), alb.size())) return r;
+  for (size_t p = 0; p < P; p++) {
+    for (int c = 0; c < 3; c++) {
+      double il;
+      if (f32) {
+        float v;
+        std::memcpy(&v, fin.data() + p * 16 + c * 4, 4);
+        il = v;
+      } else {
+        uint16_t hb;
+        std::memcpy(&hb, fin.data() + p * 8 + c * 2, 2);
+        il = half_to_float(hb);
+      }
+      const double a = (double)alb[p * 4 + c] / 255.0;
+      rgb[p * 3 + c] = (float)((il * a) * a);
+    }
+  }
+  return VRT_OK;
+}
+
+int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = set_dev(s->ctx)) return r;
+  const int prev = 1 - parity_of(s);
+  cudaStream_t st = s->ctx->stream;
+  if (accum_prev) CUDA_TRY(cudaMemcpyAsync(s->accum[prev], accum_prev, px(s) * acc_bpp(s), cudaMemcpyHostToDevice, st));
+  if (gbuf_prev) CUDA_TRY(cudaMemcpyAsync(s->gbuf[prev], gbuf_prev, px(s) * 16, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return VRT_OK;
+}
+
+}  // extern "C"

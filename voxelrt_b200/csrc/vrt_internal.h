@@ -1,0 +1,50 @@
+// vrt_internal.h -- launch wrappers shared by the C-ABI layer and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/vrt.h"
+
+namespace vrt {
+
+// Device-resident scene: packed voxels, per-brick words and masks, plus the
+// 1-bit-per-brick occupancy bitmap the traversal stages in shared memory.
+struct SceneDev {
+  uint32_t* vox = nullptr;     // N^3
+  uint32_t* bricks = nullptr;  // BG^3
+  uint32_t* masks = nullptr;   // 16 * BG^3
+  uint32_t* bits = nullptr;    // ceil(BG^3 / 32)
+  int N = 0, BG = 0;
+};
+
+inline size_t occ_words(int BG) { return ((size_t)BG * BG * BG + 31) / 32; }
+
+// Per-frame counters written by the path kernel (u64 each).
+enum StatSlot { kStatRays = 0, kStatOuter, kStatInner, kStatVReads, kStatPixels, kStatCount = 8 };
+
+// Device pointers of one frame's path-trace outputs.
+struct PathOut {
+  void* rad16 = nullptr;       // rgba16f  (uint2 per pixel)
+  void* rad32 = nullptr;       // rgba32f  (optional)
+  uint32_t* alb8 = nullptr;    // rgba8
+  void* gbuf = nullptr;        // rgba32f  (float4 per pixel)
+  unsigned long long* stats = nullptr;
+};
+
+cudaError_t launch_build_bricks(const SceneDev& s, int bx0, int by0, int bz0, int bx1, int by1, int bz1,
+                                cudaStream_t st);
+cudaError_t launch_build_bits(const SceneDev& s, cudaStream_t st);
+cudaError_t launch_fill_box(const SceneDev& s, int x0, int y0, int z0, int x1, int y1, int z1, uint32_t value,
+                            cudaStream_t st);
+cudaError_t launch_pathtrace(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                             const PathOut& out, cudaStream_t st);
+cudaError_t launch_trace_rays(const SceneDev& s, const float* o, const float* d, const float* tmax, int n,
+                              VrtHit* out, cudaStream_t st);
+cudaError_t launch_temporal(const VrtUniforms& u, int W, int H, const void* rad16, const void* gcur,
+                            const void* acc_prev, const void* gprev, void* acc_out, bool acc_f32,
+                            cudaStream_t st);
+cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
+                          cudaStream_t st);
+cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
+                           const uint32_t* alb8, uint32_t* ldr, cudaStream_t st);
+
+}  // namespace vrt
