@@ -743,7 +743,7 @@ void orc_temporal(const void* uniforms, int Wd, int Hd, const uint16_t* rad16, c
         float pux = ndx * 0.5f + 0.5f;
         float puy = (-ndy) * 0.5f + 0.5f;
         if (pux > 0.0f && puy > 0.0f && pux < 1.0f && puy < 1.0f) {
-          int ppx = (int)(pux * (float)Wd), ppy = (int)(puy * (float)Hd);
+          int ppx = std::min((int)(pux * (float)Wd), Wd - 1), ppy = std::min((int)(puy * (float)Hd), Hd - 1);
           const float* pg = gbufPrev + 4 * ((size_t)ppy * Wd + ppx);
           f3 dv = sub(worldPos, mk(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]));
           float expectedT = length3(dv);

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(256) k_temporal(Uni u, int W, int H, const uin
       const float pux = ndx * 0.5f + 0.5f;
       const float puy = (-ndy) * 0.5f + 0.5f;
       if (pux > 0.0f && puy > 0.0f && pux < 1.0f && puy < 1.0f) {
-        const int ppx = (int)(pux * (float)W), ppy = (int)(puy * (float)H);
+        const int ppx = min((int)(pux * (float)W), W - 1), ppy = min((int)(puy * (float)H), H - 1);
         const float4 pg = __ldg(gprev + ((size_t)ppy * W + ppx));
         const F3 dv = wp - f3(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]);
         const float expectedT = __fsqrt_rn(dot3(dv, dv));
