@@ -268,6 +268,16 @@ VRT_DI bool brick_occupied(const uint32_t* occ, uint32_t bi) {
   return (occ[bi >> 5] >> (bi & 31u)) & 1u;
 }
 
+// One component of hit.n = -vmask * vec3<f32>(stepDir) (voxel.wgsl:126) with
+// IEEE signed zeros: -1*s on the stepped axis, -0*s elsewhere.  The sign bit
+// is set exactly when s >= 0; the magnitude is 1 only on the stepped axis with
+// s != 0.  Written on the bits so no compiler rewrite can drop a -0.
+VRT_DI float face_normal_component(bool on_axis, int s) {
+  const uint32_t sign = s >= 0 ? 0x80000000u : 0u;
+  const uint32_t mag = (on_axis && s != 0) ? 0x3f800000u : 0u;
+  return __uint_as_float(sign | mag);
+}
+
 // trace(): the reference's two-level Amanatides-Woo walk.  Outer loop over
 // 8^3 bricks (at most 3*BGRID+2 steps), inner per-voxel loop (at most 24
 // steps) inside occupied bricks; brick occupancy comes from a 1-bit-per-brick
@@ -294,7 +304,8 @@ VRT_DI DHit trace(const DScene& S, const uint32_t* occ, F3 roW, F3 rd, float max
   const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
 
   const float G = (float)S.N;
-  const F3 t0 = (f3(0.0f, 0.0f, 0.0f) - ro) * invRd;
+  // 0 - ro, not -ro: +0 stays +0 (voxel.wgsl:86).
+  const F3 t0 = f3(__fsub_rn(0.0f, ro.x), __fsub_rn(0.0f, ro.y), __fsub_rn(0.0f, ro.z)) * invRd;
   const F3 t1 = (f3(G, G, G) - ro) * invRd;
   const F3 tmin3 = min3(t0, t1);
   const F3 tmax3 = max3(t0, t1);
@@ -341,8 +352,8 @@ VRT_DI DHit trace(const DScene& S, const uint32_t* occ, F3 roW, F3 rd, float max
           if (kCount) cnt.vreads++;
           if (tCur > maxT) return hit;
           hit.t = tCur * kVoxelSize;
-          hit.n = f3(-(vax == 0 ? 1.0f : 0.0f) * (float)sx, -(vax == 1 ? 1.0f : 0.0f) * (float)sy,
-                     -(vax == 2 ? 1.0f : 0.0f) * (float)sz);
+          hit.n = f3(face_normal_component(vax == 0, sx), face_normal_component(vax == 1, sy),
+                     face_normal_component(vax == 2, sz));
           hit.mat = m;
           hit.vx = vx; hit.vy = vy; hit.vz = vz;
           return hit;
