@@ -44,6 +44,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
     return ap.parse_args()
 
 
@@ -165,7 +166,8 @@ def run_ours(args, world, rank, local):
     vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
     ctx = vrt.Context(local)
     scene = vrt.Scene(ctx, vox, n)
-    sess = vrt.Session(ctx, scene, W, H, firefly_clamp=WORKLOAD["fclamp"], accum_f32=False)
+    sess = vrt.Session(ctx, scene, W, H, firefly_clamp=WORKLOAD["fclamp"], accum_f32=False,
+                       path_kernel=args.path_kernel)
     sess.set_timing(True)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -245,6 +247,7 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD_NAME, "grid": n, "width": W, "height": H, "spp": 1,
                    "bounces": WORKLOAD["bounces"], "history": "rgba16f, cap 64", "denoise": "a-trous 1/2/4",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "path_kernel": args.path_kernel,
                    "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
         "frame_ms": {"mean": round(statistics.mean(frame_ms), 4),
                      "p50": round(statistics.median(frame_ms), 4),
@@ -252,7 +255,7 @@ def run_ours(args, world, rank, local):
         "pass_ms_mean": {"pathtrace": round(statistics.mean(pt_ms), 4)},
         "rays_per_frame": round(rays / args.steps),
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_pathtrace", "achieved": round(achieved, 1), "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "path trace pass (all its kernels)", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic,
                      "algorithmic_bytes_per_launch": round(alg_bytes / args.steps),

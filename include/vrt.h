@@ -80,7 +80,21 @@ typedef struct VrtSessionConfig {
   float firefly_clamp;        /* FCLAMP_VALUE (pathtrace.wgsl:35); <=0 = off   */
   int accum_f32;              /* 1: rgba32f history, 0: rgba16f                */
   int keep_radiance_f32;      /* 1: also store fp32 demodulated radiance       */
+  int path_kernel;            /* VRT_PATH_WAVEFRONT (default) or _MEGAKERNEL   */
 } VrtSessionConfig;
+
+enum {
+  VRT_PATH_WAVEFRONT = 0,     /* queued waves + persistent refilling DDA       */
+  VRT_PATH_MEGAKERNEL = 1     /* one thread walks a whole path                 */
+};
+
+/* Launch-shape knobs of the wavefront path tracer; 0 keeps the default. */
+typedef struct VrtTuning {
+  int refill_min;             /* idle lanes of a warp that trigger a refill    */
+  int trace_blocks_per_sm;    /* persistent DDA blocks per SM (0 = max)        */
+  int shade_blocks_per_sm;    /* shading kernel blocks per SM                  */
+  int reserved;
+} VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,
  * -1 on miss.  steps = brick iterations + voxel iterations entered;
@@ -176,6 +190,7 @@ int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int iteration /*0,1,2*/
 int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
 /* Ends a frame driven pass by pass (advances parity). */
 int vrt_end_frame(VrtSession* s);
+int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t);
 /* Per-pass CUDA-event timings and in-kernel ray/step counters. */
 int vrt_session_set_timing(VrtSession* s, int enable);
 int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out);

@@ -130,12 +130,13 @@ def test_edit_box_updates_bricks_and_traces(ctx, vrt, orc):
 # --------------------------------------------------------------------------
 # Path-trace pass (pathtrace.wgsl:248-330)
 # --------------------------------------------------------------------------
-def _pathtrace_pair(vrt, orc, ctx, kind, n, seed, W, H, bounces, fclamp, frame, pose=None, rows=None):
+def _pathtrace_pair(vrt, orc, ctx, kind, n, seed, W, H, bounces, fclamp, frame, pose=None, rows=None,
+                    kernel="wavefront"):
     vox, spawn = vrt.generate_scene(kind, n, seed)
     pose = pose or spawn
     b, m = orc.build_bricks(vox, n)
     sc = vrt.Scene(ctx, vox, n)
-    s = vrt.Session(ctx, sc, W, H, firefly_clamp=fclamp, keep_radiance_f32=True)
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=fclamp, keep_radiance_f32=True, path_kernel=kernel)
     u = vrt.make_uniforms(pose, None, vrt.Lighting(), frame, bounces, 3, W, H, 1.0, 64.0)
     s.set_timing(True)
     s.frame(u)
@@ -157,9 +158,10 @@ def _compare_pathtrace(got, ref, rows=slice(None)):
         assert np.array_equal(got[k][rows].view(np.uint32), ref[k][rows].view(np.uint32)), k
 
 
+@pytest.mark.parametrize("kernel", ["wavefront", "megakernel"])
 @pytest.mark.parametrize("bounces", [0, 1, 2, 4, 6])
-def test_pathtrace_small_config(ctx, vrt, orc, bounces):
-    got, ref, st = _pathtrace_pair(vrt, orc, ctx, 1, 64, 1, 256, 144, bounces, 10.0, 3)
+def test_pathtrace_small_config(ctx, vrt, orc, bounces, kernel):
+    got, ref, st = _pathtrace_pair(vrt, orc, ctx, 1, 64, 1, 256, 144, bounces, 10.0, 3, kernel=kernel)
     _compare_pathtrace(got, ref)
     assert st.rays == ref["stats"]["rays"]
     assert st.dda_outer == ref["stats"]["outer"] and st.dda_inner == ref["stats"]["inner"]
@@ -167,9 +169,11 @@ def test_pathtrace_small_config(ctx, vrt, orc, bounces):
     assert st.pixels == 256 * 144
 
 
-def test_pathtrace_full_config_rows(ctx, vrt, orc):
+@pytest.mark.parametrize("kernel", ["wavefront", "megakernel"])
+def test_pathtrace_full_config_rows(ctx, vrt, orc, kernel):
     """1920x1080 on the 256^3 world: every 27th row checked against the oracle."""
-    got, ref, st = _pathtrace_pair(vrt, orc, ctx, 2, 256, 2, 1920, 1080, 2, 10.0, 0, rows=(0, 1080, 27))
+    got, ref, st = _pathtrace_pair(vrt, orc, ctx, 2, 256, 2, 1920, 1080, 2, 10.0, 0, rows=(0, 1080, 27),
+                                   kernel=kernel)
     _compare_pathtrace(got, ref, rows=slice(0, 1080, 27))
     assert st.pixels == 1920 * 1080
 
@@ -184,6 +188,32 @@ def test_pathtrace_odd_sizes(ctx, vrt, orc, W, H):
 def test_pathtrace_firefly_clamp_off(ctx, vrt, orc):
     got, ref, _ = _pathtrace_pair(vrt, orc, ctx, 1, 64, 1, 128, 72, 3, 0.0, 5)
     _compare_pathtrace(got, ref)
+
+
+def test_wavefront_invariant_to_launch_shape(ctx, vrt):
+    """Queue order and refill policy must not change any bit of the image."""
+    W, H, n = 320, 180, 256
+    vox, spawn = vrt.generate_scene(2, n, 2)
+    sc = vrt.Scene(ctx, vox, n)
+    u = vrt.make_uniforms(vrt.camera_spline(spawn, 40), None, vrt.Lighting(), 9, 4, 3, W, H)
+    outs = []
+    for kernel, tune in [("megakernel", None), ("wavefront", (16, 0, 8)), ("wavefront", (1, 1, 1)),
+                         ("wavefront", (32, 2, 32)), ("wavefront", (8, 0, 4))]:
+        s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True, path_kernel=kernel)
+        if tune:
+            s.set_tuning(*tune)
+        s.set_timing(True)
+        s.frame(u)
+        st = s.stats()
+        outs.append((s.radiance_f32().copy(), s.gbuffer().copy(), s.albedo().copy(),
+                     (st.rays, st.dda_outer, st.dda_inner, st.voxel_reads, st.pixels)))
+        s.close()
+    for o in outs[1:]:
+        assert np.array_equal(o[0].view(np.uint32), outs[0][0].view(np.uint32))
+        assert np.array_equal(o[1].view(np.uint32), outs[0][1].view(np.uint32))
+        assert np.array_equal(o[2], outs[0][2])
+        assert o[3] == outs[0][3]
+    sc.close()
 
 
 # --------------------------------------------------------------------------

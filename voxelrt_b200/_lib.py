@@ -51,7 +51,16 @@ class VrtDeviceConfig(C.Structure):
 
 class VrtSessionConfig(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("firefly_clamp", C.c_float),
-                ("accum_f32", C.c_int), ("keep_radiance_f32", C.c_int)]
+                ("accum_f32", C.c_int), ("keep_radiance_f32", C.c_int), ("path_kernel", C.c_int)]
+
+
+class VrtTuning(C.Structure):
+    _fields_ = [("refill_min", C.c_int), ("trace_blocks_per_sm", C.c_int), ("shade_blocks_per_sm", C.c_int),
+                ("reserved", C.c_int)]
+
+
+PATH_WAVEFRONT = 0
+PATH_MEGAKERNEL = 1
 
 
 class VrtHit(C.Structure):
@@ -114,6 +123,7 @@ SIGNATURES = {
     "vrt_pass_present": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_end_frame": (I, [P]),
     "vrt_session_set_timing": (I, [P, I]),
+    "vrt_session_set_tuning": (I, [P, C.POINTER(VrtTuning)]),
     "vrt_session_last_stats": (I, [P, C.POINTER(VrtFrameStats)]),
     "vrt_read_radiance": (I, [P, P, SZ]),
     "vrt_read_radiance_f32": (I, [P, P, SZ]),
@@ -145,7 +155,19 @@ def _load() -> C.CDLL:
     return lib
 
 
-lib = _load()
+class _Lib:
+    """Loads libvrt.so on first use (so the build step can import this
+    package before the library exists); any use without the library raises."""
+
+    _cdll = None
+
+    def __getattr__(self, name):
+        if _Lib._cdll is None:
+            _Lib._cdll = _load()
+        return getattr(_Lib._cdll, name)
+
+
+lib = _Lib()
 
 
 def check(code: int) -> None:

@@ -12,8 +12,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import (HIT_DTYPE, VrtCameraPose, VrtDeviceConfig, VrtFrameStats, VrtLighting, VrtSessionConfig,
-                   VrtUniforms, check, lib, ptr)
+from ._lib import (HIT_DTYPE, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtDeviceConfig, VrtFrameStats,
+                   VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms, check, lib, ptr)
 
 # Reference constants (scene.js:5-6, common.wgsl:11)
 VOXEL_SIZE = 1.0 / 16.0
@@ -180,9 +180,10 @@ class Session:
     denoise x2, LDR) and the frame loop over them."""
 
     def __init__(self, ctx: Context, scene: Scene, width: int, height: int, firefly_clamp: float = 48.0,
-                 accum_f32: bool = False, keep_radiance_f32: bool = False):
+                 accum_f32: bool = False, keep_radiance_f32: bool = False, path_kernel: str = "wavefront"):
+        pk = {"wavefront": PATH_WAVEFRONT, "megakernel": PATH_MEGAKERNEL}[path_kernel]
         cfg = VrtSessionConfig(int(width), int(height), float(firefly_clamp), int(bool(accum_f32)),
-                               int(bool(keep_radiance_f32)))
+                               int(bool(keep_radiance_f32)), pk)
         h = C.c_void_p()
         check(lib.vrt_session_create(ctx.h, scene.h, C.byref(cfg), C.byref(h)))
         self.h, self.ctx, self.scene = h, ctx, scene
@@ -203,6 +204,10 @@ class Session:
     def set_scene(self, scene: Scene) -> None:
         check(lib.vrt_session_set_scene(self.h, scene.h))
         self.scene = scene
+
+    def set_tuning(self, refill_min: int = 0, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0) -> None:
+        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), 0)
+        check(lib.vrt_session_set_tuning(self.h, C.byref(t)))
 
     def set_timing(self, on: bool) -> None:
         check(lib.vrt_session_set_timing(self.h, int(bool(on))))

@@ -73,6 +73,12 @@ struct VrtSession {
   void* den[2] = {nullptr, nullptr};
   uint32_t* ldr = nullptr;
   unsigned long long* stats = nullptr;
+  // wavefront scratch
+  int path_kernel = VRT_PATH_WAVEFRONT;
+  void* wf_mem = nullptr;
+  size_t wf_bytes = 0;
+  WavefrontBufs wf;
+  WavefrontTuning tune;
   // frame state
   uint64_t frame_counter = 0;     // host frame index (parity source)
   bool last_denoise = false;
@@ -324,6 +330,7 @@ int vrt_session_destroy(VrtSession* s) {
   }
   dev_free(c, s->ldr, P * 4, &s->bytes);
   dev_free(c, s->stats, kStatCount * 8, &s->bytes);
+  dev_free(c, s->wf_mem, s->wf_bytes, &s->bytes);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
   delete s;
@@ -378,6 +385,21 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
   }
   if (!r) r = dev_alloc(ctx, (void**)&s->ldr, P * 4, &s->bytes);
   if (!r) r = dev_alloc(ctx, (void**)&s->stats, kStatCount * 8, &s->bytes);
+  s->path_kernel = cfg->path_kernel == VRT_PATH_MEGAKERNEL ? VRT_PATH_MEGAKERNEL : VRT_PATH_WAVEFRONT;
+  if (!r && s->path_kernel == VRT_PATH_WAVEFRONT) {
+    const int max_waves = 72;
+    s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves);
+    r = dev_alloc(ctx, &s->wf_mem, s->wf_bytes, &s->bytes);
+    if (!r) {
+      char* m = (char*)s->wf_mem;
+      void** f4[7] = {&s->wf.R0, &s->wf.R1, &s->wf.R2, &s->wf.S0, &s->wf.S1, &s->wf.S2, &s->wf.hit};
+      for (auto* f : f4) { *f = m; m += P * 16; }
+      for (int i = 0; i < 2; i++) { s->wf.q[i] = (uint32_t*)m; m += P * 8; }
+      for (int i = 0; i < 2; i++) { s->wf.act[i] = (uint32_t*)m; m += P * 4; }
+      s->wf.ctr = (int*)m;
+      s->wf.max_waves = max_waves;
+    }
+  }
   if (!r) {
     for (auto& e : s->ev) {
       if (cudaEventCreate(&e) != cudaSuccess) { r = fail(VRT_ERR_CUDA, "cudaEventCreate failed"); break; }
@@ -397,6 +419,17 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
 int vrt_session_set_scene(VrtSession* s, VrtScene* scene) {
   if (!s || !scene || scene->ctx != s->ctx) return fail(VRT_ERR_INVALID, "bad scene");
   s->scene = scene;
+  return VRT_OK;
+}
+
+int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
+  if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64)
+    return fail(VRT_ERR_INVALID, "tuning out of range");
+  s->tune.refill_min = t->refill_min ? t->refill_min : 16;
+  s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
+  s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 8;
   return VRT_OK;
 }
 
@@ -425,8 +458,13 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (int r = set_dev(s->ctx)) return r;
   PathOut o;
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
-  CUDA_TRY(launch_pathtrace(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->ctx->stream));
-  s->launches++;
+  if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
+    CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
+                              &s->launches));
+  } else {
+    CUDA_TRY(launch_pathtrace(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->ctx->stream));
+    s->launches++;
+  }
   return VRT_OK;
 }
 

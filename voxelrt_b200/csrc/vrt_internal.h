@@ -30,6 +30,30 @@ struct PathOut {
   unsigned long long* stats = nullptr;
 };
 
+// Scratch of the wavefront path tracer (per session, carved from one
+// allocation): per-pixel path state, ray queues, active lists, counters.
+struct WavefrontBufs {
+  void *R0 = nullptr, *R1 = nullptr, *R2 = nullptr;   // float4 per pixel
+  void *S0 = nullptr, *S1 = nullptr, *S2 = nullptr;   // float4 per pixel
+  void* hit = nullptr;                                // uint4 per pixel
+  uint32_t* q[2] = {nullptr, nullptr};                // 2P entries each
+  uint32_t* act[2] = {nullptr, nullptr};              // P entries each
+  int* ctr = nullptr;                                 // 4 ints per wave
+  int max_waves = 0;
+};
+
+// Launch-shape knobs of the wavefront tracer (chosen by the autotuner).
+struct WavefrontTuning {
+  int refill_min = 16;          // idle lanes that trigger a warp refill
+  int trace_blocks_per_sm = 0;  // 0 = occupancy maximum
+  int shade_blocks_per_sm = 8;
+};
+
+size_t wavefront_bytes(int W, int H, int max_waves);
+cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                             const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
+                             cudaStream_t st, uint32_t* launches);
+
 cudaError_t launch_build_bricks(const SceneDev& s, int bx0, int by0, int bz0, int bx1, int by1, int bz1,
                                 cudaStream_t st);
 cudaError_t launch_build_bits(const SceneDev& s, cudaStream_t st);
