@@ -209,6 +209,23 @@ int vrt_read_hdr(VrtSession* s, float* host_rgb, size_t bytes);      /* f32 RGB 
 /* Writes history buffers (resume from a saved session state). */
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
 
+/* ---- allocation-free denoise ------------------------------------------- */
+/* No counterpart in the reference.  The 3-iteration a-trous chain (steps
+ * 1, 2, 4) on caller-owned device buffers, for callers that cannot allocate
+ * device memory when they denoise (an engine whose device memory belongs to
+ * its own allocator/budget, or a frame loop that must not call cudaMalloc,
+ * which synchronizes the device).  d_accum: history, rgba16f (accum_f32 = 0)
+ * or rgba32f (1); d_gbuf: rgba32f normal + distance; d_out: rgba16f result.
+ * At most 1920x1080 pixels (VRT_ERR_INVALID above that).  The intermediate
+ * image lives in a fixed 16,588,800-byte device array of the library, held on
+ * every GPU that loads it; the first call on a device looks up that array's
+ * address (make the first call before any stream capture).  Calls share the
+ * array: calls that overlap on the GPU race and must be ordered by the
+ * caller.  Work is queued on `stream` (a cudaStream_t, NULL = legacy default);
+ * nothing is allocated or freed. */
+int vrt_denoise_atrous_noalloc(const void* d_accum, int accum_f32, const float* d_gbuf, void* d_out, int width,
+                               int height, void* stream);
+
 /* ---- host helpers (no GPU) --------------------------------------------- */
 /* Fills the uniform block like main.js writeUniforms (399-426). */
 int vrt_make_uniforms(const VrtCameraPose* cur, const VrtCameraPose* prev, const VrtLighting* light,

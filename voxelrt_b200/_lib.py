@@ -135,6 +135,7 @@ SIGNATURES = {
     "vrt_read_ldr": (I, [P, P, SZ]),
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
+    "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
     "vrt_make_uniforms": (I, [C.POINTER(VrtCameraPose), C.POINTER(VrtCameraPose), C.POINTER(VrtLighting), U32, U32,
                               U32, I, I, C.c_float, C.c_float, C.POINTER(VrtUniforms)]),
     "vrt_camera_matrices": (I, [C.POINTER(VrtCameraPose), C.c_double, P, P]),

@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libvrt.so"
 
-CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_wavefront.cu"]
+CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_wavefront.cu", "k_noalloc.cu"]
 CPP_SOURCES = ["vrt_api.cpp", "scene_gen.cpp"]
 HEADERS = ["vrt_device.cuh", "vrt_internal.h"]
 

@@ -31,6 +31,8 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+int vrt::set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 #define CUDA_TRY(expr)                                                                           \
   do {                                                                                           \
     cudaError_t e_ = (expr);                                                                     \

@@ -49,6 +49,9 @@ struct WavefrontTuning {
   int shade_blocks_per_sm = 8;
 };
 
+// Records `msg` as the calling thread's vrt_last_error_string(); returns code.
+int set_error(int code, const char* msg);
+
 size_t wavefront_bytes(int W, int H, int max_waves);
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
