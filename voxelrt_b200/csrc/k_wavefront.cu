@@ -75,27 +75,38 @@ VRT_DI F3 hit_normal(int vax, F3 rd) {
 }
 
 // ---------------------------------------------------------------------------
-// Flat two-level DDA (voxel.wgsl:73-153 as a resumable state machine).
-// Modes mirror the nested loops: CHECK = head of the brick loop, INNER = one
-// voxel iteration, BSTEP = the brick step after the voxel loop.
+// Two-level DDA as one resumable iteration shared by both levels
+// (voxel.wgsl:73-153).  Each call performs
+//   [pending step at the current level] + [test of the current cell],
+// so lanes walking bricks and lanes walking voxels execute the same code
+// with level-selected operands.  Transitions reproduce the nested loops:
+//   brick test occupied  -> descend (entry voxel from t + 1e-4, next call
+//                           tests it without stepping)
+//   voxel test occupied  -> hit (voxel read, maxT check)
+//   voxel step leaves the brick, or 24 voxel tests done -> brick step pending
+// Steps use fma(|invRd|, scale, tMax), which equals the reference's
+// tMax + |invRd|*8 (brick) and tMax + |invRd| (voxel) bit for bit because
+// |invRd|*8 and |invRd|*1 are exact.
+// Counters follow the oracle: outer = brick iterations entered, inner =
+// voxel iterations entered, vreads = voxel words read.
 // ---------------------------------------------------------------------------
-enum : int { kModeCheck = 0, kModeInner = 1, kModeBStep = 2, kModeDone = 3 };
+enum : int { kLevelVoxel = 1, kPending = 2, kDone = 4 };
 
 struct FlatDDA {
   F3 ro, invRd;
-  float maxT, tExit, t, tCur;
+  float maxT, tExit;
+  float t, tCur;                // brick-level t, voxel-level t
   F3 tMaxB, tMaxV;
-  int bx, by, bz, vx, vy, vz;
-  int ax, vax, iter, j, mode;
-  int sgn;          // packed signs: bits 0-1 sx+1, 2-3 sy+1, 4-5 sz+1
+  int bx, by, bz;               // brick cell
+  int lx, ly, lz;               // voxel cell, local to the brick (0..7)
+  int sx, sy, sz;
+  int ax, vax, iter, j;
+  int state;
   float tHit;
   uint32_t mat;
 
-  VRT_DI int sx() const { return (sgn & 3) - 1; }
-  VRT_DI int sy() const { return ((sgn >> 2) & 3) - 1; }
-  VRT_DI int sz() const { return ((sgn >> 4) & 3) - 1; }
+  VRT_DI bool done() const { return (state & kDone) != 0; }
 
-  // Grid clip, entry face and first brick (voxel.wgsl:79-104).
   VRT_DI void init(const DScene& S, F3 roW, F3 rd, float maxTW) {
     tHit = -1.0f;
     mat = 0u;
@@ -106,10 +117,9 @@ struct FlatDDA {
     const float sgy = rd.y >= 0.0f ? 1.0f : -1.0f;
     const float sgz = rd.z >= 0.0f ? 1.0f : -1.0f;
     invRd = f3(sgx / fmax_(fabsf(rd.x), 1e-8f), sgy / fmax_(fabsf(rd.y), 1e-8f), sgz / fmax_(fabsf(rd.z), 1e-8f));
-    const int isx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
-    const int isy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
-    const int isz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);
-    sgn = (isx + 1) | ((isy + 1) << 2) | ((isz + 1) << 4);
+    sx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
+    sy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
+    sz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);
     const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
     const float G = (float)S.N;
     const F3 t0 = f3(__fsub_rn(0.0f, ro.x), __fsub_rn(0.0f, ro.y), __fsub_rn(0.0f, ro.z)) * invRd;
@@ -119,7 +129,9 @@ struct FlatDDA {
     const float tEnter = fmax_(fmax_(tmin3.x, tmin3.y), fmax_(tmin3.z, 0.0f));
     tExit = fmin_(fmin_(tmax3.x, tmax3.y), fmin_(tmax3.z, maxT));
     iter = 0;
-    if (tEnter > tExit) { mode = kModeDone; return; }
+    j = 0;
+    lx = ly = lz = 0;
+    if (tEnter > tExit) { state = kDone; return; }
     if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) ax = 0;
     else if (tmin3.y >= tmin3.z) ax = 1;
     else ax = 2;
@@ -129,75 +141,84 @@ struct FlatDDA {
     by = iclamp_(ifloor_(sp.y / 8.0f), 0, S.BG - 1);
     bz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
     tMaxB = ((f3((float)bx, (float)by, (float)bz) + stepGE) * 8.0f - ro) * invRd;
-    mode = kModeCheck;
+    state = 0;   // brick level, test first
   }
 
-  // One iteration of the walk.  `rd` is the ray direction (world = voxel
-  // direction).  Counters follow the oracle: outer = brick iterations
-  // entered, inner = voxel iterations entered, vreads = voxel words read.
   VRT_DI void step(const DScene& S, const uint32_t* occ, F3 rd, DCount& c) {
-    const F3 absInv = f3(fabsf(invRd.x), fabsf(invRd.y), fabsf(invRd.z));
-    if (mode == kModeInner) {
-      if (j >= 3 * kBrick) {
-        mode = kModeBStep;
-      } else {
-        j++;
-        c.inner++;
-        const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
-        const uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)S.BG + (uint32_t)bz * (uint32_t)(S.BG * S.BG);
-        const uint32_t bit = (uint32_t)((vx - mnx) + (vy - mny) * 8 + (vz - mnz) * 64);
-        const uint32_t word = __ldg(S.masks + (size_t)bi * 16u + (bit >> 5));
-        if ((word >> (bit & 31u)) & 1u) {
-          mat = __ldg(S.vox + ((uint32_t)vx + (uint32_t)vy * (uint32_t)S.N + (uint32_t)vz * (uint32_t)(S.N * S.N)));
-          c.vreads++;
-          if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
-          else mat = 0u;
-          mode = kModeDone;
+    const bool lv = (state & kLevelVoxel) != 0;
+    if (state & kPending) {
+      // ---- one DDA step at the current level --------------------------
+      const float mx = lv ? tMaxV.x : tMaxB.x;
+      const float my = lv ? tMaxV.y : tMaxB.y;
+      const float mz = lv ? tMaxV.z : tMaxB.z;
+      const bool cx = mx <= my && mx <= mz;
+      const bool cy = !cx && my <= mz;
+      const bool cz = !cx && !cy;
+      const float tn = cx ? mx : (cy ? my : mz);
+      const float ia = fabsf(cx ? invRd.x : (cy ? invRd.y : invRd.z));
+      const float nv = __fmaf_rn(ia, lv ? 1.0f : 8.0f, tn);
+      const F3 m = f3(cx ? nv : mx, cy ? nv : my, cz ? nv : mz);
+      const int a = cx ? 0 : (cy ? 1 : 2);
+      const int dx = cx ? sx : 0, dy = cy ? sy : 0, dz = cz ? sz : 0;
+      if (lv) {
+        tMaxV = m; tCur = tn; vax = a;
+        lx += dx; ly += dy; lz += dz;
+        if ((unsigned)(lx | ly | lz) > 7u) {
+          state = kPending;                  // left the brick: brick step next
           return;
         }
-        if (tMaxV.x <= tMaxV.y && tMaxV.x <= tMaxV.z) {
-          tCur = tMaxV.x; tMaxV.x = tMaxV.x + absInv.x; vx += sx(); vax = 0;
-        } else if (tMaxV.y <= tMaxV.z) {
-          tCur = tMaxV.y; tMaxV.y = tMaxV.y + absInv.y; vy += sy(); vax = 1;
-        } else {
-          tCur = tMaxV.z; tMaxV.z = tMaxV.z + absInv.z; vz += sz(); vax = 2;
-        }
-        if (vx < mnx || vy < mny || vz < mnz || vx > mnx + 7 || vy > mny + 7 || vz > mnz + 7) mode = kModeBStep;
-      }
-    }
-    if (mode == kModeBStep) {
-      const F3 tDeltaB = absInv * 8.0f;
-      if (tMaxB.x <= tMaxB.y && tMaxB.x <= tMaxB.z) {
-        t = tMaxB.x; tMaxB.x = tMaxB.x + tDeltaB.x; bx += sx(); ax = 0;
-      } else if (tMaxB.y <= tMaxB.z) {
-        t = tMaxB.y; tMaxB.y = tMaxB.y + tDeltaB.y; by += sy(); ax = 1;
       } else {
-        t = tMaxB.z; tMaxB.z = tMaxB.z + tDeltaB.z; bz += sz(); ax = 2;
+        tMaxB = m; t = tn; ax = a;
+        bx += dx; by += dy; bz += dz;
+        if ((unsigned)bx >= (unsigned)S.BG || (unsigned)by >= (unsigned)S.BG || (unsigned)bz >= (unsigned)S.BG) {
+          state = kDone;
+          return;
+        }
       }
-      if (bx < 0 || by < 0 || bz < 0 || bx >= S.BG || by >= S.BG || bz >= S.BG) { mode = kModeDone; return; }
-      mode = kModeCheck;
+      state &= ~kPending;
     }
-    if (mode == kModeCheck) {
-      if (iter >= 3 * S.BG + 2 || t > tExit) { mode = kModeDone; return; }
+    // ---- test the current cell ------------------------------------------
+    const uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)S.BG + (uint32_t)bz * (uint32_t)(S.BG * S.BG);
+    const uint32_t lbit = (uint32_t)(lx + ly * 8 + lz * 64);
+    if (lv) {
+      if (j >= 3 * kBrick) { state = kPending; return; }   // voxel loop exhausted
+      j++;
+      c.inner++;
+    } else {
+      if (iter >= 3 * S.BG + 2 || t > tExit) { state = kDone; return; }
       iter++;
       c.outer++;
-      const uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)S.BG + (uint32_t)bz * (uint32_t)(S.BG * S.BG);
-      if (brick_occupied(occ, bi)) {
-        const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
-        const F3 p = ro + rd * (t + 1e-4f);
-        vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
-        vy = iclamp_(ifloor_(p.y), mny, mny + 7);
-        vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
-        const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
-        tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
-        tCur = t;
-        vax = ax;
-        j = 0;
-        mode = kModeInner;
-      } else {
-        mode = kModeBStep;
-      }
     }
+    const uint32_t* wp = lv ? (S.masks + (size_t)bi * 16u + (lbit >> 5)) : (occ + (bi >> 5));
+    const uint32_t sh = lv ? (lbit & 31u) : (bi & 31u);
+    const bool hitcell = ((*wp >> sh) & 1u) != 0u;
+    if (!hitcell) {
+      state |= kPending;
+      return;
+    }
+    if (lv) {
+      const uint32_t vx = (uint32_t)(bx * kBrick + lx), vy = (uint32_t)(by * kBrick + ly),
+                     vz = (uint32_t)(bz * kBrick + lz);
+      mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
+      c.vreads++;
+      if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
+      else mat = 0u;
+      state = kDone;
+      return;
+    }
+    // descend into the occupied brick
+    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
+    const F3 p = ro + rd * (t + 1e-4f);
+    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
+    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
+    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
+    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
+    tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
+    lx = vx - mnx; ly = vy - mny; lz = vz - mnz;
+    tCur = t;
+    vax = ax;
+    j = 0;
+    state = kLevelVoxel;
   }
 };
 
@@ -269,8 +290,8 @@ __global__ void __launch_bounds__(256) k_wf_trace(DScene S, WfDev b, int wave, i
       continue;
     }
     if (active) {
-      if (d.mode != kModeDone) d.step(S, occ, rd, c);
-      if (d.mode == kModeDone) {
+      if (!d.done()) d.step(S, occ, rd, c);
+      if (d.done()) {
         const uint32_t p = entry & ~kShadowBit;
         uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + p);
         if (entry & kShadowBit) {
