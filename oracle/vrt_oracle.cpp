@@ -787,6 +787,11 @@ void orc_atrous(const void* uniforms, int Wd, int Hd, const void* src, int src_f
       float lumC = luminance(center);
       float relax = 2.0f / std::sqrt(history);
       float sigmaL = fmaxf_(0.08f, relax);
+      // wDepth * wLum = exp(-|dt|/(0.05 t + 0.01)) * exp(-|dL|/sigmaL) evaluated
+      // as exp(-(|dt| * invD + |dL| * invS)) with the two reciprocals taken once
+      // per pixel: within WGSL's accuracy for '/' (2.5 ULP) and exp.
+      float invD = 1.0f / (0.05f * g[3] + 0.01f);
+      float invS = 1.0f / sigmaL;
       float k00 = K[0] * K[0];
       float sum[3] = {(center[0] * K[0]) * K[0], (center[1] * K[0]) * K[0], (center[2] * K[0]) * K[0]};
       float wSum = k00;
@@ -802,9 +807,9 @@ void orc_atrous(const void* uniforms, int Wd, int Hd, const void* src, int src_f
           float wKernel = K[std::abs(dx)] * K[std::abs(dy)];
           float nd = fmaxf_((g[0] * gq[0] + g[1] * gq[1]) + g[2] * gq[2], 0.0f);
           float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;   // pow(., 32)
-          float wDepth = om_exp(-std::fabs(g[3] - gq[3]) / (0.05f * g[3] + 0.01f));
-          float wLum = om_exp(-std::fabs(lumC - luminance(cq)) / sigmaL);
-          float w = ((wKernel * n32) * wDepth) * wLum;
+          if (n32 == 0.0f) continue;   // zero weight: the tap adds nothing
+          float e = om_exp(-(std::fabs(g[3] - gq[3]) * invD + std::fabs(lumC - luminance(cq)) * invS));
+          float w = (wKernel * n32) * e;
           for (int c = 0; c < 3; c++) sum[c] = sum[c] + cq[c] * w;
           wSum = wSum + w;
         }

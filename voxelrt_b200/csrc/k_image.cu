@@ -89,6 +89,9 @@ __global__ void __launch_bounds__(256) k_temporal(Uni u, int W, int H, const uin
 // normal^32 * exp(-|dt|/(0.05 t + 0.01)) * exp(-|dL|/sigmaL),
 // sigmaL = max(0.08, 2/sqrt(max(history,1))); sky and out-of-image taps skipped.
 // ---------------------------------------------------------------------------
+// B3-spline taps (atrous.wgsl:26): 3/8, 1/4, 1/16 for |d| = 0, 1, 2.
+VRT_DI float b3_weight(int d) { return d == 0 ? 0.375f : ((d == 1 || d == -1) ? 0.25f : 0.0625f); }
+
 template <bool kSrcF32>
 __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __restrict__ src,
                                                 const float4* __restrict__ gbuf, uint2* __restrict__ dst, int step) {
@@ -102,7 +105,6 @@ __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __rest
     dst[p] = pack_h4(center.x, center.y, center.z, center.w);
     return;
   }
-  const float K[3] = {0.375f, 0.25f, 0.0625f};
   const float history = fmax_(center.w, 1.0f);
   const float lumC = luminance(center.x, center.y, center.z);
   const float sigmaL = fmax_(0.08f, 2.0f / __fsqrt_rn(history));
@@ -110,7 +112,10 @@ __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __rest
   float sg = (center.y * 0.375f) * 0.375f;
   float sb = (center.z * 0.375f) * 0.375f;
   float wSum = 0.140625f;
-  const float depthScale = 0.05f * g.w + 0.01f;
+  // exp(-|dt|/(0.05 t + 0.01)) * exp(-|dL|/sigmaL) as one exp of the summed
+  // exponents with per-pixel reciprocals (within WGSL's '/' and exp accuracy).
+  const float invD = 1.0f / (0.05f * g.w + 0.01f);
+  const float invS = 1.0f / sigmaL;
 #pragma unroll
   for (int dy = -2; dy <= 2; dy++) {
 #pragma unroll
@@ -121,13 +126,13 @@ __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __rest
       const size_t q = (size_t)qy * W + qx;
       const float4 gq = __ldg(gbuf + q);
       if (gq.w < 0.0f) continue;
-      const float4 cq = load_px(src, kSrcF32, q);
-      const float wKernel = K[dx < 0 ? -dx : dx] * K[dy < 0 ? -dy : dy];
       const float nd = fmax_((g.x * gq.x + g.y * gq.y) + g.z * gq.z, 0.0f);
       const float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;
-      const float wDepth = exp_(-fabsf(g.w - gq.w) / depthScale);
-      const float wLum = exp_(-fabsf(lumC - luminance(cq.x, cq.y, cq.z)) / sigmaL);
-      const float w = ((wKernel * n32) * wDepth) * wLum;
+      if (n32 == 0.0f) continue;
+      const float4 cq = load_px(src, kSrcF32, q);
+      const float wKernel = b3_weight(dx) * b3_weight(dy);
+      const float e = exp_(-(fabsf(g.w - gq.w) * invD + fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
+      const float w = (wKernel * n32) * e;
       sr = sr + cq.x * w;
       sg = sg + cq.y * w;
       sb = sb + cq.z * w;
