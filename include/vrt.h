@@ -93,7 +93,7 @@ typedef struct VrtTuning {
   int refill_min;             /* idle lanes of a warp that trigger a refill    */
   int trace_blocks_per_sm;    /* persistent DDA blocks per SM (0 = max)        */
   int shade_blocks_per_sm;    /* shading kernel blocks per SM                  */
-  int reserved;
+  int trace_variant;          /* 0: free registers, 1/2: >= 5/6 blocks per SM   */
 } VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,
@@ -118,6 +118,8 @@ typedef struct VrtFrameStats {
   uint64_t pixels;
   float ms_pathtrace, ms_temporal, ms_atrous, ms_present, ms_total;
   uint32_t launches;          /* kernels launched by the frame                 */
+  uint32_t trace_launches;    /* wavefront trace launches timed in ms_trace    */
+  float ms_trace;             /* summed duration of those trace launches       */
   uint32_t pad;
 } VrtFrameStats;
 
@@ -191,6 +193,7 @@ int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
 /* Ends a frame driven pass by pass (advances parity). */
 int vrt_end_frame(VrtSession* s);
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t);
+int vrt_session_get_tuning(VrtSession* s, VrtTuning* t);
 /* Per-pass CUDA-event timings and in-kernel ray/step counters. */
 int vrt_session_set_timing(VrtSession* s, int enable);
 int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out);

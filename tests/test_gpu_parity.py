@@ -197,8 +197,8 @@ def test_wavefront_invariant_to_launch_shape(ctx, vrt):
     sc = vrt.Scene(ctx, vox, n)
     u = vrt.make_uniforms(vrt.camera_spline(spawn, 40), None, vrt.Lighting(), 9, 4, 3, W, H)
     outs = []
-    for kernel, tune in [("megakernel", None), ("wavefront", (16, 0, 8)), ("wavefront", (1, 1, 1)),
-                         ("wavefront", (32, 2, 32)), ("wavefront", (8, 0, 4))]:
+    for kernel, tune in [("megakernel", None), ("wavefront", (16, 0, 8, 0)), ("wavefront", (1, 1, 1, 0)),
+                         ("wavefront", (32, 2, 32, 1)), ("wavefront", (8, 0, 4, 2)), ("wavefront", (12, 0, 16, 1))]:
         s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True, path_kernel=kernel)
         if tune:
             s.set_tuning(*tune)

@@ -56,7 +56,7 @@ class VrtSessionConfig(C.Structure):
 
 class VrtTuning(C.Structure):
     _fields_ = [("refill_min", C.c_int), ("trace_blocks_per_sm", C.c_int), ("shade_blocks_per_sm", C.c_int),
-                ("reserved", C.c_int)]
+                ("trace_variant", C.c_int)]
 
 
 PATH_WAVEFRONT = 0
@@ -76,7 +76,8 @@ class VrtFrameStats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("dda_outer", C.c_uint64), ("dda_inner", C.c_uint64),
                 ("voxel_reads", C.c_uint64), ("pixels", C.c_uint64), ("ms_pathtrace", C.c_float),
                 ("ms_temporal", C.c_float), ("ms_atrous", C.c_float), ("ms_present", C.c_float),
-                ("ms_total", C.c_float), ("launches", C.c_uint32), ("pad", C.c_uint32)]
+                ("ms_total", C.c_float), ("launches", C.c_uint32), ("trace_launches", C.c_uint32),
+                ("ms_trace", C.c_float), ("pad", C.c_uint32)]
 
 
 class VrtCameraPose(C.Structure):
@@ -124,6 +125,7 @@ SIGNATURES = {
     "vrt_end_frame": (I, [P]),
     "vrt_session_set_timing": (I, [P, I]),
     "vrt_session_set_tuning": (I, [P, C.POINTER(VrtTuning)]),
+    "vrt_session_get_tuning": (I, [P, C.POINTER(VrtTuning)]),
     "vrt_session_last_stats": (I, [P, C.POINTER(VrtFrameStats)]),
     "vrt_read_radiance": (I, [P, P, SZ]),
     "vrt_read_radiance_f32": (I, [P, P, SZ]),

@@ -205,9 +205,15 @@ class Session:
         check(lib.vrt_session_set_scene(self.h, scene.h))
         self.scene = scene
 
-    def set_tuning(self, refill_min: int = 0, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0) -> None:
-        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), 0)
+    def set_tuning(self, refill_min: int = 0, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
+                   trace_variant: int = 0) -> None:
+        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant))
         check(lib.vrt_session_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self) -> tuple:
+        t = VrtTuning()
+        check(lib.vrt_session_get_tuning(self.h, C.byref(t)))
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant)
 
     def set_timing(self, on: bool) -> None:
         check(lib.vrt_session_set_timing(self.h, int(bool(on))))

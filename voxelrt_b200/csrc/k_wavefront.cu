@@ -243,9 +243,11 @@ __global__ void __launch_bounds__(256) k_wf_generate(Uni u, int W, int H, WfDev 
 // ---------------------------------------------------------------------------
 // persistent queue tracer
 // ---------------------------------------------------------------------------
-template <bool kSmem>
-__global__ void __launch_bounds__(256) k_wf_trace(DScene S, WfDev b, int wave, int implicit_n, int refill_min,
-                                                  unsigned long long* stats) {
+// kMinBlocks > 1 caps registers so that many 256-thread blocks stay
+// resident per SM (the tracer is latency-bound; see the tuning sweep).
+template <bool kSmem, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(DScene S, WfDev b, int wave, int implicit_n,
+                                                              int refill_min, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
   const uint32_t* occ = S.bits;
   if (kSmem) {
@@ -492,23 +494,34 @@ size_t wavefront_bytes(int W, int H, int max_waves) {
   return P * 16 * 7 + P * 4 * 2 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
 }
 
-static int trace_blocks(int smem, int* blocks_out) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+template <bool kSmem, int kMinBlocks>
+static cudaError_t launch_trace_variant(int smem, int blocks_per_sm, int sms, const DScene& d, const WfDev& b, int w,
+                                       int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
+  auto* fn = k_wf_trace<kSmem, kMinBlocks>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
   }
-  int per = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_wf_trace<true>, 256, smem);
-  if (e != cudaSuccess || per < 1) per = 1;
-  *blocks_out = sms * per;
-  return sms;
+  int per = blocks_per_sm;
+  if (per <= 0) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem);
+    if (e != cudaSuccess || per < 1) per = 1;
+  }
+  fn<<<sms * per, 256, smem, st>>>(d, b, w, implicit_n, refill, stats);
+  return cudaGetLastError();
+}
+
+static int sm_count() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 1;
 }
 
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
-                             cudaStream_t st, uint32_t* launches) {
+                             cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves,
+                             int* timed_waves) {
   Uni u;
   std::memcpy(&u, &uu, sizeof(Uni));
   const int P = W * H;
@@ -519,29 +532,40 @@ cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fcl
   DScene d = to_dscene(s);
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
   if (e != cudaSuccess) return e;
-  const int smem = (int)(occ_words(s.BG) * sizeof(uint32_t));
-  const bool use_smem = smem <= 64 * 1024;
-  if (use_smem && smem > 48 * 1024) {
-    e = cudaFuncSetAttribute(k_wf_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-  }
-  int tblocks = 0;
-  const int sms = trace_blocks(use_smem ? smem : 0, &tblocks);
-  if (tune.trace_blocks_per_sm > 0) tblocks = sms * tune.trace_blocks_per_sm;
-  const int refill = tune.refill_min > 0 ? tune.refill_min : 16;
+  const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
+  const bool use_smem = smem_occ <= 64 * 1024;
+  const int smem = use_smem ? smem_occ : 0;
+  const int sms = sm_count();
+  const int refill = tune.refill_min > 0 ? tune.refill_min : 12;
   const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 8);
   uint32_t nl = 0;
   k_wf_generate<<<(P + 255) / 256, 256, 0, st>>>(u, W, H, b);
   nl++;
+  int timed = 0;
   for (int w = 0; w < waves; w++) {
-    if (use_smem) k_wf_trace<true><<<tblocks, 256, smem, st>>>(d, b, w, w == 0 ? P : 0, refill, out.stats);
-    else k_wf_trace<false><<<tblocks, 256, 0, st>>>(d, b, w, w == 0 ? P : 0, refill, out.stats);
+    const bool tm = trace_ev && w < max_timed_waves;
+    if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
+    const int impl = w == 0 ? P : 0;
+    const int tb = tune.trace_blocks_per_sm;
+    if (use_smem) {
+      if (tune.trace_variant == 1) e = launch_trace_variant<true, 5>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
+      else if (tune.trace_variant == 2) e = launch_trace_variant<true, 6>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
+      else e = launch_trace_variant<true, 1>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
+    } else {
+      if (tune.trace_variant == 1) e = launch_trace_variant<false, 5>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
+      else if (tune.trace_variant == 2) e = launch_trace_variant<false, 6>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
+      else e = launch_trace_variant<false, 1>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
+    }
+    if (e != cudaSuccess) return e;
+    if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
+    if (tm) timed++;
     nl++;
     if (w == 0) k_wf_shade_primary<<<sblocks, 256, 0, st>>>(u, fclamp, W, H, b, out);
     else k_wf_shade<<<sblocks, 256, 0, st>>>(u, fclamp, b, out, w);
     nl++;
   }
   if (launches) *launches += nl;
+  if (timed_waves) *timed_waves = timed;
   return cudaGetLastError();
 }
 

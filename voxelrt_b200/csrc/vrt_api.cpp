@@ -89,6 +89,9 @@ struct VrtSession {
   // timing
   bool timing = false;
   cudaEvent_t ev[6] = {};
+  static constexpr int kTimedWaves = 16;
+  cudaEvent_t tev[2 * kTimedWaves] = {};   // brackets of each wave's trace kernel
+  int timed_waves = 0;
   uint32_t launches = 0;
 };
 
@@ -335,6 +338,8 @@ int vrt_session_destroy(VrtSession* s) {
   dev_free(c, s->wf_mem, s->wf_bytes, &s->bytes);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : s->tev)
+    if (e) cudaEventDestroy(e);
   delete s;
   return VRT_OK;
 }
@@ -406,6 +411,10 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
     for (auto& e : s->ev) {
       if (cudaEventCreate(&e) != cudaSuccess) { r = fail(VRT_ERR_CUDA, "cudaEventCreate failed"); break; }
     }
+    for (auto& e : s->tev) {
+      if (r) break;
+      if (cudaEventCreate(&e) != cudaSuccess) { r = fail(VRT_ERR_CUDA, "cudaEventCreate failed"); break; }
+    }
   }
   if (!r) r = vrt_session_reset(s);
   if (r) {
@@ -424,14 +433,24 @@ int vrt_session_set_scene(VrtSession* s, VrtScene* scene) {
   return VRT_OK;
 }
 
+int vrt_session_get_tuning(VrtSession* s, VrtTuning* t) {
+  if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
+  t->refill_min = s->tune.refill_min;
+  t->trace_blocks_per_sm = s->tune.trace_blocks_per_sm;
+  t->shade_blocks_per_sm = s->tune.shade_blocks_per_sm;
+  t->trace_variant = s->tune.trace_variant;
+  return VRT_OK;
+}
+
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64)
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 2)
     return fail(VRT_ERR_INVALID, "tuning out of range");
-  s->tune.refill_min = t->refill_min ? t->refill_min : 16;
+  s->tune.refill_min = t->refill_min ? t->refill_min : 12;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
-  s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 8;
+  s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
+  s->tune.trace_variant = t->trace_variant;
   return VRT_OK;
 }
 
@@ -462,7 +481,8 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
   if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
     CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
-                              &s->launches));
+                              &s->launches, s->timing ? s->tev : nullptr, VrtSession::kTimedWaves,
+                              &s->timed_waves));
   } else {
     CUDA_TRY(launch_pathtrace(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->ctx->stream));
     s->launches++;
@@ -528,6 +548,7 @@ int vrt_frame(VrtSession* s, const VrtUniforms* u) {
   if (int r = set_dev(s->ctx)) return r;
   cudaStream_t st = s->ctx->stream;
   s->launches = 0;
+  s->timed_waves = 0;
   CUDA_TRY(cudaMemsetAsync(s->stats, 0, kStatCount * 8, st));
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[0], st));
   if (int r = vrt_pass_pathtrace(s, u)) return r;
@@ -565,6 +586,14 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
     CUDA_TRY(cudaEventElapsedTime(&d, s->ev[3], s->ev[4]));
     out->ms_pathtrace = a; out->ms_temporal = b; out->ms_atrous = c; out->ms_present = d;
     out->ms_total = a + b + c + d;
+    float tr = 0.0f;
+    for (int w = 0; w < s->timed_waves; w++) {
+      float x = 0.0f;
+      CUDA_TRY(cudaEventElapsedTime(&x, s->tev[2 * w], s->tev[2 * w + 1]));
+      tr += x;
+    }
+    out->ms_trace = tr;
+    out->trace_launches = (uint32_t)s->timed_waves;
   }
   return VRT_OK;
 }

@@ -44,18 +44,22 @@ struct WavefrontBufs {
 
 // Launch-shape knobs of the wavefront tracer (chosen by the autotuner).
 struct WavefrontTuning {
-  int refill_min = 16;          // idle lanes that trigger a warp refill
+  int refill_min = 12;          // idle lanes that trigger a warp refill
   int trace_blocks_per_sm = 0;  // 0 = occupancy maximum
-  int shade_blocks_per_sm = 8;
+  int shade_blocks_per_sm = 16;
+  int trace_variant = 0;        // 0: registers unconstrained, 1: >= 5 blocks/SM, 2: >= 6 blocks/SM
 };
 
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
 size_t wavefront_bytes(int W, int H, int max_waves);
+// When trace_ev is non-null, events trace_ev[2w], trace_ev[2w+1] bracket the
+// trace kernel of wave w (w < max_timed_waves); *timed_waves receives the count.
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
-                             cudaStream_t st, uint32_t* launches);
+                             cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev = nullptr,
+                             int max_timed_waves = 0, int* timed_waves = nullptr);
 
 cudaError_t launch_build_bricks(const SceneDev& s, int bx0, int by0, int bz0, int bx1, int by1, int bz1,
                                 cudaStream_t st);
