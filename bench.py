@@ -119,6 +119,19 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_over_ranks(dist, device, seconds_or_ms: float, count: float):
+    """Replica aggregation: the job's time is the slowest rank's, the work is
+    the sum over ranks.  Returns (max time, summed count)."""
+    if dist is None:
+        return float(seconds_or_ms), float(count)
+    import torch
+    t = torch.tensor([float(seconds_or_ms)], dtype=torch.float64, device=device)
+    c = torch.tensor([float(count)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def frame_uniforms(vrt, spawn, f):
     W, H = WORKLOAD["W"], WORKLOAD["H"]
     k = f % WORKLOAD["path_frames"]
@@ -204,13 +217,7 @@ def run_ours(args, world, rank, local):
     total_ms = sum(frame_ms)
     if dist:
         dist.barrier()
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        r = torch.tensor([float(rays)], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        total_ms_max, rays_all = float(t.item()), float(r.item())
-    else:
-        total_ms_max, rays_all = total_ms, float(rays)
+    total_ms_max, rays_all = reduce_over_ranks(dist, f"cuda:{local}", total_ms, rays)
 
     # ---- end to end through the C ABI: host uniforms in, LDR frame out ----
     ldr_host = torch.empty(W * H * 4, dtype=torch.uint8, pin_memory=True)
@@ -224,12 +231,7 @@ def run_ours(args, world, rank, local):
         if code:
             raise RuntimeError(vlib.vrt_last_error_string().decode())
         e2e_rays += sess.stats().rays
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_rays = float(t.item()), float(r.item())
+    e2e_s, e2e_rays = reduce_over_ranks(dist, f"cuda:{local}", e2e_s, e2e_rays)
 
     peak, peak_kind = measured_peaks()
     if args.path_kernel == "wavefront" and trace_launches:
