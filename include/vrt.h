@@ -194,6 +194,11 @@ int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
 int vrt_end_frame(VrtSession* s);
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t);
 int vrt_session_get_tuning(VrtSession* s, VrtTuning* t);
+/* Autotuner (no counterpart in the reference): times `frames` path-trace
+ * passes of `u` for each candidate launch shape of the wavefront tracer and
+ * keeps the fastest (returned in *best, its median pass time in *best_ms).
+ * Resets the session's history. */
+int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms);
 /* Per-pass CUDA-event timings and in-kernel ray/step counters. */
 int vrt_session_set_timing(VrtSession* s, int enable);
 int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out);

@@ -342,3 +342,18 @@ def test_hbm_budget_admission(vrt):
     sc.close()
     assert c.bytes_in_use == 0
     c.close()
+
+
+def test_autotune_picks_a_candidate_and_keeps_results(ctx, vrt):
+    W, H, n = 320, 180, 128
+    vox, spawn = vrt.generate_scene(2, n, 3)
+    sc = vrt.Scene(ctx, vox, n)
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+    u = vrt.make_uniforms(spawn, None, vrt.Lighting(), 4, 2, 3, W, H)
+    s.frame(u)
+    before = s.radiance_f32().copy()
+    tune, ms = s.autotune(u, frames=2)
+    assert ms > 0 and tune[0] in (4, 8, 12, 16, 24) and tune[3] in (0, 1) and s.get_tuning() == tune
+    s.frame(u)                                  # history was reset: same first frame again
+    assert np.array_equal(s.radiance_f32().view(np.uint32), before.view(np.uint32))
+    s.close(); sc.close()

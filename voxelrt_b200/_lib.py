@@ -126,6 +126,7 @@ SIGNATURES = {
     "vrt_session_set_timing": (I, [P, I]),
     "vrt_session_set_tuning": (I, [P, C.POINTER(VrtTuning)]),
     "vrt_session_get_tuning": (I, [P, C.POINTER(VrtTuning)]),
+    "vrt_session_autotune": (I, [P, C.POINTER(VrtUniforms), I, C.POINTER(VrtTuning), C.POINTER(C.c_float)]),
     "vrt_session_last_stats": (I, [P, C.POINTER(VrtFrameStats)]),
     "vrt_read_radiance": (I, [P, P, SZ]),
     "vrt_read_radiance_f32": (I, [P, P, SZ]),

@@ -210,6 +210,13 @@ class Session:
         t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant))
         check(lib.vrt_session_set_tuning(self.h, C.byref(t)))
 
+    def autotune(self, u: VrtUniforms, frames: int = 3):
+        """Picks the fastest wavefront launch shape for frames like `u`; resets history."""
+        t = VrtTuning()
+        ms = C.c_float()
+        check(lib.vrt_session_autotune(self.h, C.byref(u), int(frames), C.byref(t), C.byref(ms)))
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant), float(ms.value)
+
     def get_tuning(self) -> tuple:
         t = VrtTuning()
         check(lib.vrt_session_get_tuning(self.h, C.byref(t)))

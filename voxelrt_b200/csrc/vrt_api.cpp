@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <mutex>
+#include <algorithm>
 #include "vrt_internal.h"
 
 using namespace vrt;
@@ -452,6 +453,55 @@ int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   s->tune.trace_variant = t->trace_variant;
   return VRT_OK;
+}
+
+static int check_uniforms(const VrtSession* s, const VrtUniforms* u);
+
+// Autotuner: renders `frames` path-trace passes of `u` per candidate launch
+// shape (refill threshold x occupancy variant x shading grid) and keeps the
+// candidate with the smallest median pass time.  The session's history is
+// reset afterwards (the candidate frames are not part of any sequence).
+int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms) {
+  if (!s || !u || frames < 1) return fail(VRT_ERR_INVALID, "bad argument");
+  if (s->path_kernel != VRT_PATH_WAVEFRONT) return fail(VRT_ERR_STATE, "autotune needs the wavefront path kernel");
+  if (int r = check_uniforms(s, u)) return r;
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  static const int refills[] = {4, 8, 12, 16, 24};
+  static const int variants[] = {0, 1};
+  static const int shades[] = {8, 16, 32};
+  const WavefrontTuning keep = s->tune;
+  WavefrontTuning win = keep;
+  float win_ms = 1e30f;
+  std::vector<float> ms((size_t)frames);
+  for (int rf : refills)
+    for (int va : variants)
+      for (int sh : shades) {
+        s->tune.refill_min = rf;
+        s->tune.trace_variant = va;
+        s->tune.shade_blocks_per_sm = sh;
+        s->tune.trace_blocks_per_sm = 0;
+        if (int r = vrt_pass_pathtrace(s, u)) { s->tune = keep; return r; }   // warm-up
+        for (int f = 0; f < frames; f++) {
+          CUDA_TRY(cudaEventRecord(s->ev[0], st));
+          if (int r = vrt_pass_pathtrace(s, u)) { s->tune = keep; return r; }
+          CUDA_TRY(cudaEventRecord(s->ev[1], st));
+          CUDA_TRY(cudaEventSynchronize(s->ev[1]));
+          CUDA_TRY(cudaEventElapsedTime(&ms[(size_t)f], s->ev[0], s->ev[1]));
+        }
+        std::sort(ms.begin(), ms.end());
+        const float med = ms[(size_t)frames / 2];
+        if (med < win_ms) { win_ms = med; win = s->tune; }
+      }
+  s->tune = win;
+  if (best) {
+    best->refill_min = win.refill_min;
+    best->trace_blocks_per_sm = win.trace_blocks_per_sm;
+    best->shade_blocks_per_sm = win.shade_blocks_per_sm;
+    best->trace_variant = win.trace_variant;
+  }
+  if (best_ms) *best_ms = win_ms;
+  return vrt_session_reset(s);
 }
 
 int vrt_session_set_timing(VrtSession* s, int enable) {
