@@ -50,6 +50,7 @@ enum {
 typedef struct VrtCtx VrtCtx;
 typedef struct VrtScene VrtScene;
 typedef struct VrtSession VrtSession;
+typedef struct VrtBatch VrtBatch;
 
 /* Uniform block, byte-identical to the reference's 304-byte UBO
  * (common.wgsl:13-35, packed by main.js:399-426). */
@@ -85,7 +86,9 @@ typedef struct VrtSessionConfig {
 
 enum {
   VRT_PATH_WAVEFRONT = 0,     /* queued waves + persistent refilling DDA       */
-  VRT_PATH_MEGAKERNEL = 1     /* one thread walks a whole path                 */
+  VRT_PATH_MEGAKERNEL = 1,    /* one thread walks a whole path                 */
+  VRT_PATH_BATCH_ONLY = 2     /* rendered only through a VrtBatch: the session
+                                 holds no path-tracing scratch of its own      */
 };
 
 /* Launch-shape knobs of the wavefront path tracer; 0 keeps the default. */
@@ -216,6 +219,26 @@ int vrt_read_ldr(VrtSession* s, void* host, size_t bytes);           /* rgba8   
 int vrt_read_hdr(VrtSession* s, float* host_rgb, size_t bytes);      /* f32 RGB */
 /* Writes history buffers (resume from a saved session state). */
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
+
+/* ---- batched frames (no counterpart in the reference) ------------------ */
+/* A batch renders one frame for each of n sessions of one context in a
+ * single launch sequence: one wavefront path trace over all sessions' pixels
+ * (one persistent trace launch per wave serving every scene), then one
+ * temporal, three a-trous and one present launch over all sessions.  Each
+ * session keeps its own buffers, history and frame parity; every image is
+ * bit-identical to rendering the session alone with vrt_frame.  The launch
+ * sequence is captured once as a CUDA graph and replayed (re-captured when
+ * the largest bounce count or the tuning changes). */
+int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch** out);
+int vrt_batch_destroy(VrtBatch* b);
+/* u: n uniform blocks, one per session, in creation order. */
+int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u);
+int vrt_batch_set_graph(VrtBatch* b, int enable);
+int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t);
+/* Autotuner over whole batch frames (resets every session's history). */
+int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms);
+/* Counters of the last batch frame; ms_total = device time of the frame. */
+int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out);
 
 /* ---- allocation-free denoise ------------------------------------------- */
 /* No counterpart in the reference.  The 3-iteration a-trous chain (steps

@@ -61,6 +61,7 @@ class VrtTuning(C.Structure):
 
 PATH_WAVEFRONT = 0
 PATH_MEGAKERNEL = 1
+PATH_BATCH_ONLY = 2
 
 
 class VrtHit(C.Structure):
@@ -139,6 +140,13 @@ SIGNATURES = {
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
+    "vrt_batch_create": (I, [P, C.POINTER(P), I, C.POINTER(P)]),
+    "vrt_batch_destroy": (I, [P]),
+    "vrt_batch_frame": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_batch_set_graph": (I, [P, I]),
+    "vrt_batch_set_tuning": (I, [P, C.POINTER(VrtTuning)]),
+    "vrt_batch_autotune": (I, [P, C.POINTER(VrtUniforms), I, C.POINTER(VrtTuning), C.POINTER(C.c_float)]),
+    "vrt_batch_last_stats": (I, [P, C.POINTER(VrtFrameStats)]),
     "vrt_make_uniforms": (I, [C.POINTER(VrtCameraPose), C.POINTER(VrtCameraPose), C.POINTER(VrtLighting), U32, U32,
                               U32, I, I, C.c_float, C.c_float, C.POINTER(VrtUniforms)]),
     "vrt_camera_matrices": (I, [C.POINTER(VrtCameraPose), C.c_double, P, P]),

@@ -12,7 +12,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import (HIT_DTYPE, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtDeviceConfig, VrtFrameStats,
+from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtDeviceConfig, VrtFrameStats,
                    VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms, check, lib, ptr)
 
 # Reference constants (scene.js:5-6, common.wgsl:11)
@@ -181,7 +181,7 @@ class Session:
 
     def __init__(self, ctx: Context, scene: Scene, width: int, height: int, firefly_clamp: float = 48.0,
                  accum_f32: bool = False, keep_radiance_f32: bool = False, path_kernel: str = "wavefront"):
-        pk = {"wavefront": PATH_WAVEFRONT, "megakernel": PATH_MEGAKERNEL}[path_kernel]
+        pk = {"wavefront": PATH_WAVEFRONT, "megakernel": PATH_MEGAKERNEL, "batch_only": PATH_BATCH_ONLY}[path_kernel]
         cfg = VrtSessionConfig(int(width), int(height), float(firefly_clamp), int(bool(accum_f32)),
                                int(bool(keep_radiance_f32)), pk)
         h = C.c_void_p()
@@ -263,6 +263,51 @@ class Session:
     def close(self) -> None:
         if self.h:
             lib.vrt_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """One frame for each of several sessions in a single launch sequence
+    (replayed as a CUDA graph); images equal each session rendered alone."""
+
+    def __init__(self, ctx: Context, sessions: list):
+        arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
+        h = C.c_void_p()
+        check(lib.vrt_batch_create(ctx.h, arr, len(sessions), C.byref(h)))
+        self.h, self.ctx, self.sessions = h, ctx, list(sessions)
+
+    def frame(self, uniforms: list) -> None:
+        arr = (VrtUniforms * len(uniforms))(*uniforms)
+        check(lib.vrt_batch_frame(self.h, arr))
+
+    def set_graph(self, on: bool) -> None:
+        check(lib.vrt_batch_set_graph(self.h, int(bool(on))))
+
+    def set_tuning(self, refill_min=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, trace_variant=0) -> None:
+        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant))
+        check(lib.vrt_batch_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, uniforms: list, frames: int = 2):
+        arr = (VrtUniforms * len(uniforms))(*uniforms)
+        t = VrtTuning()
+        ms = C.c_float()
+        check(lib.vrt_batch_autotune(self.h, arr, int(frames), C.byref(t), C.byref(ms)))
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant), float(ms.value)
+
+    def stats(self) -> VrtFrameStats:
+        s = VrtFrameStats()
+        check(lib.vrt_batch_last_stats(self.h, C.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self.h:
+            lib.vrt_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

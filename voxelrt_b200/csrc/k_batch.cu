@@ -1,0 +1,86 @@
+// k_batch.cu -- many independent views rendered in one launch sequence.
+//
+// A batch frame renders one frame for each of n sessions (different scenes,
+// sizes, bounce counts, cameras).  The sessions' pixels are laid out back to
+// back in one global index space; every kernel finds the job of a pixel by a
+// binary search over the jobs' first pixels.  The wavefront path tracer runs
+// over all jobs at once -- one persistent trace launch per wave serves rays
+// of every scene -- followed by one temporal, three a-trous and one present
+// launch over all jobs.  Per-pixel arithmetic is the single-session code
+// (wavefront_core.cuh, image_core.cuh), so each job's image is bit-identical
+// to rendering that session alone.
+#include <cstddef>
+#include "wavefront_core.cuh"
+#include "image_core.cuh"
+
+namespace vrt {
+
+static_assert(sizeof(JobDev) == sizeof(JobHost), "job table layouts differ");
+static_assert(offsetof(JobDev, S) == offsetof(JobHost, vox), "job table layouts differ");
+static_assert(offsetof(JobDev, out) == offsetof(JobHost, rad16), "job table layouts differ");
+static_assert(offsetof(JobDev, W) == offsetof(JobHost, W), "job table layouts differ");
+static_assert(offsetof(JobDev, acc_prev) == offsetof(JobHost, acc_prev), "job table layouts differ");
+static_assert(offsetof(JobDev, acc_f32) == offsetof(JobHost, acc_f32), "job table layouts differ");
+
+// temporal.wgsl:17-77 over all jobs.
+__global__ void __launch_bounds__(256) k_b_temporal(MultiJob J, uint32_t P) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P) return;
+  const int j = J.job_of(g);
+  const JobDev& jd = J.jobs[j];
+  const int W = jd.W, H = jd.H;
+  const uint32_t lp = g - jd.first;
+  const int x = (int)(lp % (uint32_t)W), y = (int)(lp / (uint32_t)W);
+  const float4 res = temporal_pixel(jd.u, W, H, x, y, jd.out.rad16, jd.out.gbuf, jd.acc_prev, jd.acc_f32 != 0,
+                                    jd.gbuf_prev);
+  store_px(jd.acc_cur, jd.acc_f32 != 0, lp, res);
+}
+
+// atrous.wgsl:26-83 iteration `it` (step 1 << it) of every job whose denoise
+// flag is set; chain accum -> dA -> dB -> dA (main.js:503-507).
+__global__ void __launch_bounds__(256) k_b_atrous(MultiJob J, uint32_t P, int it) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P) return;
+  const int j = J.job_of(g);
+  const JobDev& jd = J.jobs[j];
+  if ((jd.u.params0[2] & 2u) == 0u) return;
+  const int W = jd.W, H = jd.H;
+  const uint32_t lp = g - jd.first;
+  const int x = (int)(lp % (uint32_t)W), y = (int)(lp / (uint32_t)W);
+  const void* src = it == 0 ? jd.acc_cur : (it == 1 ? (const void*)jd.den0 : (const void*)jd.den1);
+  const bool srcF32 = it == 0 && jd.acc_f32 != 0;
+  uint2* dst = it == 1 ? jd.den1 : jd.den0;
+  const float4 v = atrous_pixel(W, H, x, y, src, srcF32, jd.out.gbuf, 1 << it);
+  dst[lp] = pack_h4(v.x, v.y, v.z, v.w);
+}
+
+// present.wgsl:40-55 over all jobs.
+__global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P) return;
+  const int j = J.job_of(g);
+  const JobDev& jd = J.jobs[j];
+  const uint32_t lp = g - jd.first;
+  const bool denoise = (jd.u.params0[2] & 2u) != 0u;
+  const float4 il = denoise ? load_px(jd.den0, false, lp) : load_px(jd.acc_cur, jd.acc_f32 != 0, lp);
+  jd.ldr[lp] = present_pixel(jd.u.params1[2], il, __ldg(jd.out.alb8 + lp));
+}
+
+cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
+                               const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
+                               cudaStream_t st, uint32_t* launches) {
+  MultiJob J;
+  J.jobs = (const JobDev*)d_jobs;
+  J.firsts = d_firsts;
+  J.n = n;
+  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr);
+  if (e != cudaSuccess) return e;
+  const unsigned blocks = (P + 255) / 256;
+  k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
+  for (int it = 0; it < 3; it++) k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);
+  k_b_present<<<blocks, 256, 0, st>>>(J, P);
+  if (launches) *launches += 5;
+  return cudaGetLastError();
+}
+
+}  // namespace vrt

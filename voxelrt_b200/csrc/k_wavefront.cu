@@ -1,4 +1,5 @@
-// k_wavefront.cu -- wavefront form of the plain path tracer (sm_100a).
+// k_wavefront.cu -- wavefront form of the plain path tracer (sm_100a), for
+// one session.
 //
 // The megakernel (k_trace.cu) runs one path per thread; its warps idle on
 // sky pixels, skipped shadow rays and on the longest DDA walk of each warp
@@ -14,559 +15,43 @@
 //
 // Queues and active-path lists are compacted with warp ballots (one atomic
 // per warp).  The trace kernel is persistent: each warp owns 32 lanes that
-// walk the DDA as a flat state machine (brick check / brick step / voxel
-// test+step); lanes whose ray ended are refilled from the queue once enough
-// of them are idle, so warps stay full until the queue drains.
+// walk the DDA as a flat state machine shared by brick-level and voxel-level
+// lanes; lanes whose ray ended are refilled from the queue once enough of
+// them are idle, so warps stay full until the queue drains.  The kernels are
+// defined in wavefront_core.cuh and shared with the batched form (k_batch.cu).
 //
 // The per-path arithmetic (RNG draws, shading, order of radiance sums) is
 // exactly the megakernel's, so results are bit-identical to it and to the
 // CPU oracle.
-#include "vrt_device.cuh"
-#include "vrt_internal.h"
+#include "wavefront_core.cuh"
 #include <cstring>
 
 namespace vrt {
-
-constexpr uint32_t kFlagShadow = 1u;     // a shadow ray of the previous vertex is pending
-constexpr uint32_t kFlagTerminal = 2u;   // no bounce ray: finalize after the shadow ray
-constexpr uint32_t kShadowBit = 0x80000000u;
-
-struct WfDev {
-  float4* R0;      // ray origin: camera position (primary) or surf = pos + n*1e-3
-  float4* R1;      // primary / bounce direction
-  float4* R2;      // sun direction of the pending shadow ray
-  float4* S0;      // radiance xyz, w = RNG state bits
-  float4* S1;      // throughput xyz, w = primary material bits
-  float4* S2;      // pending sun contribution xyz, w = flags
-  uint4* hit;      // x = t bits, y = material, z = entry axis, w = shadow occluded
-  uint32_t* q0;    // ray queues (entry = pixel | kShadowBit for shadow rays), capacity 2P
-  uint32_t* q1;
-  uint32_t* a0;    // active path lists, capacity P
-  uint32_t* a1;
-  int* ctr;        // per wave k: [4k] queue count, [4k+1] queue head, [4k+2] active count
-};
-
-VRT_DI uint32_t* queue_of(const WfDev& b, int wave) { return (wave & 1) ? b.q1 : b.q0; }
-VRT_DI uint32_t* active_of(const WfDev& b, int wave) { return (wave & 1) ? b.a1 : b.a0; }
-
-// Warp-aggregated append: one atomicAdd per warp, slots in lane order.  All
-// 32 lanes must call it (pred false for lanes with nothing to append).
-VRT_DI uint32_t warp_append(int* counter, bool pred) {
-  const unsigned mask = __ballot_sync(0xffffffffu, pred);
-  if (!mask) return 0u;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(counter, __popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return (uint32_t)base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-}
-
-VRT_DI F3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
-
-// Normal of a hit on entry axis `vax` for direction rd (same value the DDA
-// returns: -vmask * sign(rd)).
-VRT_DI F3 hit_normal(int vax, F3 rd) {
-  const int sx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
-  const int sy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
-  const int sz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);
-  return f3(face_normal_component(vax == 0, sx), face_normal_component(vax == 1, sy),
-            face_normal_component(vax == 2, sz));
-}
-
-// ---------------------------------------------------------------------------
-// Two-level DDA as one resumable iteration shared by both levels
-// (voxel.wgsl:73-153).  Each call performs
-//   [pending step at the current level] + [test of the current cell],
-// so lanes walking bricks and lanes walking voxels execute the same code
-// with level-selected operands.  Transitions reproduce the nested loops:
-//   brick test occupied  -> descend (entry voxel from t + 1e-4, next call
-//                           tests it without stepping)
-//   voxel test occupied  -> hit (voxel read, maxT check)
-//   voxel step leaves the brick, or 24 voxel tests done -> brick step pending
-// Steps use fma(|invRd|, scale, tMax), which equals the reference's
-// tMax + |invRd|*8 (brick) and tMax + |invRd| (voxel) bit for bit because
-// |invRd|*8 and |invRd|*1 are exact.
-// Counters follow the oracle: outer = brick iterations entered, inner =
-// voxel iterations entered, vreads = voxel words read.
-// ---------------------------------------------------------------------------
-enum : int { kLevelVoxel = 1, kPending = 2, kDone = 4 };
-
-struct FlatDDA {
-  F3 ro, invRd;
-  float maxT, tExit;
-  float t, tCur;                // brick-level t, voxel-level t
-  F3 tMaxB, tMaxV;
-  int bx, by, bz;               // brick cell
-  int lx, ly, lz;               // voxel cell, local to the brick (0..7)
-  int sx, sy, sz;
-  int ax, vax, iter, j;
-  int state;
-  float tHit;
-  uint32_t mat;
-
-  VRT_DI bool done() const { return (state & kDone) != 0; }
-
-  VRT_DI void init(const DScene& S, F3 roW, F3 rd, float maxTW) {
-    tHit = -1.0f;
-    mat = 0u;
-    vax = 0;
-    ro = roW * kInvVoxel;
-    maxT = maxTW * kInvVoxel;
-    const float sgx = rd.x >= 0.0f ? 1.0f : -1.0f;
-    const float sgy = rd.y >= 0.0f ? 1.0f : -1.0f;
-    const float sgz = rd.z >= 0.0f ? 1.0f : -1.0f;
-    invRd = f3(sgx / fmax_(fabsf(rd.x), 1e-8f), sgy / fmax_(fabsf(rd.y), 1e-8f), sgz / fmax_(fabsf(rd.z), 1e-8f));
-    sx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
-    sy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
-    sz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);
-    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
-    const float G = (float)S.N;
-    const F3 t0 = f3(__fsub_rn(0.0f, ro.x), __fsub_rn(0.0f, ro.y), __fsub_rn(0.0f, ro.z)) * invRd;
-    const F3 t1 = (f3(G, G, G) - ro) * invRd;
-    const F3 tmin3 = min3(t0, t1);
-    const F3 tmax3 = max3(t0, t1);
-    const float tEnter = fmax_(fmax_(tmin3.x, tmin3.y), fmax_(tmin3.z, 0.0f));
-    tExit = fmin_(fmin_(tmax3.x, tmax3.y), fmin_(tmax3.z, maxT));
-    iter = 0;
-    j = 0;
-    lx = ly = lz = 0;
-    if (tEnter > tExit) { state = kDone; return; }
-    if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) ax = 0;
-    else if (tmin3.y >= tmin3.z) ax = 1;
-    else ax = 2;
-    t = tEnter;
-    const F3 sp = ro + rd * (t + 1e-4f);
-    bx = iclamp_(ifloor_(sp.x / 8.0f), 0, S.BG - 1);
-    by = iclamp_(ifloor_(sp.y / 8.0f), 0, S.BG - 1);
-    bz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
-    tMaxB = ((f3((float)bx, (float)by, (float)bz) + stepGE) * 8.0f - ro) * invRd;
-    state = 0;   // brick level, test first
-  }
-
-  VRT_DI void step(const DScene& S, const uint32_t* occ, F3 rd, DCount& c) {
-    const bool lv = (state & kLevelVoxel) != 0;
-    if (state & kPending) {
-      // ---- one DDA step at the current level --------------------------
-      const float mx = lv ? tMaxV.x : tMaxB.x;
-      const float my = lv ? tMaxV.y : tMaxB.y;
-      const float mz = lv ? tMaxV.z : tMaxB.z;
-      const bool cx = mx <= my && mx <= mz;
-      const bool cy = !cx && my <= mz;
-      const bool cz = !cx && !cy;
-      const float tn = cx ? mx : (cy ? my : mz);
-      const float ia = fabsf(cx ? invRd.x : (cy ? invRd.y : invRd.z));
-      const float nv = __fmaf_rn(ia, lv ? 1.0f : 8.0f, tn);
-      const F3 m = f3(cx ? nv : mx, cy ? nv : my, cz ? nv : mz);
-      const int a = cx ? 0 : (cy ? 1 : 2);
-      const int dx = cx ? sx : 0, dy = cy ? sy : 0, dz = cz ? sz : 0;
-      if (lv) {
-        tMaxV = m; tCur = tn; vax = a;
-        lx += dx; ly += dy; lz += dz;
-        if ((unsigned)(lx | ly | lz) > 7u) {
-          state = kPending;                  // left the brick: brick step next
-          return;
-        }
-      } else {
-        tMaxB = m; t = tn; ax = a;
-        bx += dx; by += dy; bz += dz;
-        if ((unsigned)bx >= (unsigned)S.BG || (unsigned)by >= (unsigned)S.BG || (unsigned)bz >= (unsigned)S.BG) {
-          state = kDone;
-          return;
-        }
-      }
-      state &= ~kPending;
-    }
-    // ---- test the current cell ------------------------------------------
-    const uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)S.BG + (uint32_t)bz * (uint32_t)(S.BG * S.BG);
-    const uint32_t lbit = (uint32_t)(lx + ly * 8 + lz * 64);
-    if (lv) {
-      if (j >= 3 * kBrick) { state = kPending; return; }   // voxel loop exhausted
-      j++;
-      c.inner++;
-    } else {
-      if (iter >= 3 * S.BG + 2 || t > tExit) { state = kDone; return; }
-      iter++;
-      c.outer++;
-    }
-    const uint32_t* wp = lv ? (S.masks + (size_t)bi * 16u + (lbit >> 5)) : (occ + (bi >> 5));
-    const uint32_t sh = lv ? (lbit & 31u) : (bi & 31u);
-    const bool hitcell = ((*wp >> sh) & 1u) != 0u;
-    if (!hitcell) {
-      state |= kPending;
-      return;
-    }
-    if (lv) {
-      const uint32_t vx = (uint32_t)(bx * kBrick + lx), vy = (uint32_t)(by * kBrick + ly),
-                     vz = (uint32_t)(bz * kBrick + lz);
-      mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
-      c.vreads++;
-      if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
-      else mat = 0u;
-      state = kDone;
-      return;
-    }
-    // descend into the occupied brick
-    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
-    const F3 p = ro + rd * (t + 1e-4f);
-    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
-    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
-    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
-    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
-    tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
-    lx = vx - mnx; ly = vy - mny; lz = vz - mnz;
-    tCur = t;
-    vax = ax;
-    j = 0;
-    state = kLevelVoxel;
-  }
-};
-
-// ---------------------------------------------------------------------------
-// generate: RNG stream, jitter, camera ray (pathtrace.wgsl:249-263)
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_wf_generate(Uni u, int W, int H, WfDev b) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= W * H) return;
-  const uint32_t gx = (uint32_t)(i % W), gy = (uint32_t)(i / W);
-  uint32_t rng = init_rng(gx, gy, u.params0[0]);
-  const float jx = rand_(rng) - 0.5f;
-  const float jy = rand_(rng) - 0.5f;
-  const float uvx = (((float)gx + 0.5f) + jx) / (float)W;
-  const float uvy = (((float)gy + 0.5f) + jy) / (float)H;
-  const F3 rd = camera_ray(u, uvx, uvy);
-  b.R0[i] = make_float4(u.camPos[0], u.camPos[1], u.camPos[2], 0.0f);
-  b.R1[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-  b.S0[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
-}
-
-// ---------------------------------------------------------------------------
-// persistent queue tracer
-// ---------------------------------------------------------------------------
-// kMinBlocks > 1 caps registers so that many 256-thread blocks stay
-// resident per SM (the tracer is latency-bound; see the tuning sweep).
-template <bool kSmem, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(DScene S, WfDev b, int wave, int implicit_n,
-                                                              int refill_min, unsigned long long* stats) {
-  extern __shared__ uint32_t s_occ[];
-  const uint32_t* occ = S.bits;
-  if (kSmem) {
-    const int nwords = (S.BG * S.BG * S.BG + 31) >> 5;
-    for (int i = threadIdx.x; i < nwords; i += blockDim.x) s_occ[i] = __ldg(S.bits + i);
-    __syncthreads();
-    occ = s_occ;
-  }
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int n = implicit_n > 0 ? implicit_n : b.ctr[4 * wave];
-  int* head = b.ctr + 4 * wave + 1;
-  const uint32_t* queue = queue_of(b, wave);
-  DCount c{0u, 0u, 0u, 0u};
-  FlatDDA d;
-  F3 rd = f3(0.0f, 0.0f, 0.0f);
-  uint32_t entry = 0u;
-  bool active = false, drained = false;
-  while (true) {
-    const unsigned idle = __ballot_sync(full, !active);
-    const int nidle = __popc(idle);
-    if (!drained && (nidle >= refill_min || nidle == 32)) {
-      int base = 0;
-      if (lane == 0) base = atomicAdd(head, nidle);
-      base = __shfl_sync(full, base, 0);
-      if (base + nidle >= n) drained = true;
-      if (!active) {
-        const int slot = base + __popc(idle & ((1u << lane) - 1u));
-        if (slot < n) {
-          entry = implicit_n > 0 ? (uint32_t)slot : queue[slot];
-          const uint32_t p = entry & ~kShadowBit;
-          const F3 ro = xyz(b.R0[p]);
-          rd = (entry & kShadowBit) ? xyz(b.R2[p]) : xyz(b.R1[p]);
-          c.rays++;
-          d.init(S, ro, rd, 1e4f);
-          active = true;
-        }
-      }
-    }
-    if (!__any_sync(full, active)) {
-      if (drained) break;
-      continue;
-    }
-    if (active) {
-      if (!d.done()) d.step(S, occ, rd, c);
-      if (d.done()) {
-        const uint32_t p = entry & ~kShadowBit;
-        uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + p);
-        if (entry & kShadowBit) {
-          h[3] = d.tHit >= 0.0f ? 1u : 0u;
-        } else {
-          *reinterpret_cast<uint2*>(h) = make_uint2(__float_as_uint(d.tHit), d.mat);
-          h[2] = (uint32_t)d.vax;
-        }
-        active = false;
-      }
-    }
-  }
-  if (stats) {
-    const uint32_t r = __reduce_add_sync(full, c.rays);
-    const uint32_t o = __reduce_add_sync(full, c.outer);
-    const uint32_t in = __reduce_add_sync(full, c.inner);
-    const uint32_t v = __reduce_add_sync(full, c.vreads);
-    if (lane == 0) {
-      atomicAdd(stats + kStatRays, (unsigned long long)r);
-      atomicAdd(stats + kStatOuter, (unsigned long long)o);
-      atomicAdd(stats + kStatInner, (unsigned long long)in);
-      atomicAdd(stats + kStatVReads, (unsigned long long)v);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// shading
-// ---------------------------------------------------------------------------
-VRT_DI void finalize(const PathOut& out, size_t p, F3 radiance, uint32_t mat1bits, float fclamp) {
-  const Mat mat1 = unpack_material(mat1bits);
-  if (!(fclamp <= 0.0f)) radiance = min3(radiance, f3(fclamp, fclamp, fclamp));
-  const F3 den = max3(mat1.albedo, f3(1e-3f, 1e-3f, 1e-3f));
-  const float4 rad = make_float4(radiance.x / den.x, radiance.y / den.y, radiance.z / den.z, 1.0f);
-  reinterpret_cast<uint2*>(out.rad16)[p] = pack_h4(rad.x, rad.y, rad.z, rad.w);
-  if (out.rad32) reinterpret_cast<float4*>(out.rad32)[p] = rad;
-}
-
-// Vertex k of a path (pathtrace.wgsl:297-320 loop body up to the trace call).
-// Returns whether the path stays active (some ray was queued).
-VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, int wave, uint32_t p, uint32_t k, F3 pos, F3 n, Mat mat,
-                         F3& radiance, F3& tp, uint32_t& rng, uint32_t mat1bits, bool& want_shadow,
-                         bool& want_bounce) {
-  if (mat.emissive > 0.0f) radiance = radiance + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
-  const F3 surf = pos + n * 1e-3f;
-  const F3 l = sample_sun_dir(u, rng);
-  const float ndl = dot3(n, l);
-  uint32_t flags = 0u;
-  F3 sunc = f3(0.0f, 0.0f, 0.0f);
-  want_shadow = ndl > 0.0f && l.y > 0.0f;
-  if (want_shadow) {
-    const F3 sunRad = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
-    sunc = (((tp * mat.albedo) * kInvPi) * ndl) * sunRad;
-    flags |= kFlagShadow;
-    b.R2[p] = make_float4(l.x, l.y, l.z, 0.0f);
-  }
-  want_bounce = false;
-  if (k == u.params0[1]) {
-    flags |= kFlagTerminal;
-  } else {
-    const F3 rd = cosine_hemisphere(n, rng);
-    tp = tp * mat.albedo;
-    bool alive = true;
-    if (k >= 2u) {
-      const float pr = clamp_(fmax_(tp.x, fmax_(tp.y, tp.z)), 0.05f, 0.95f);
-      if (rand_(rng) > pr) alive = false;
-      else tp = f3(tp.x / pr, tp.y / pr, tp.z / pr);
-    }
-    if (alive) {
-      want_bounce = true;
-      b.R1[p] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-    } else {
-      flags |= kFlagTerminal;
-    }
-  }
-  b.R0[p] = make_float4(surf.x, surf.y, surf.z, 0.0f);
-  b.S0[p] = make_float4(radiance.x, radiance.y, radiance.z, __uint_as_float(rng));
-  b.S1[p] = make_float4(tp.x, tp.y, tp.z, __uint_as_float(mat1bits));
-  b.S2[p] = make_float4(sunc.x, sunc.y, sunc.z, __uint_as_float(flags));
-  return want_shadow || want_bounce;
-}
-
-// Appends this warp's new rays / active paths for the next wave.
-VRT_DI void emit(const WfDev& b, int next, uint32_t p, bool shadow, bool bounce, bool keep) {
-  uint32_t* q = queue_of(b, next);
-  uint32_t* a = active_of(b, next);
-  int* c = b.ctr + 4 * next;
-  const uint32_t s1 = warp_append(c, shadow);
-  if (shadow) q[s1] = p | kShadowBit;
-  const uint32_t s2 = warp_append(c, bounce);
-  if (bounce) q[s2] = p;
-  const uint32_t s3 = warp_append(c + 2, keep);
-  if (keep) a[s3] = p;
-}
-
-// shade(0): primary hits over all pixels.
-__global__ void __launch_bounds__(256) k_wf_shade_primary(Uni u, float fclamp, int W, int H, WfDev b, PathOut out) {
-  const int P = W * H;
-  const int stride = gridDim.x * blockDim.x;
-  if (out.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(out.stats + kStatPixels, (unsigned long long)P);
-  for (int base = blockIdx.x * blockDim.x; base < P; base += stride) {
-    const int i = base + threadIdx.x;
-    bool shadow = false, bounce = false, keep = false;
-    const uint32_t p = (uint32_t)i;
-    if (i < P) {
-      const uint4 h = b.hit[p];
-      const F3 rd = xyz(b.R1[p]);
-      const float t = __uint_as_float(h.x);
-      if (t < 0.0f) {
-        const F3 sky = sky_color(u, rd, true);
-        reinterpret_cast<uint2*>(out.rad16)[p] = pack_h4(sky.x, sky.y, sky.z, 1.0f);
-        if (out.rad32) reinterpret_cast<float4*>(out.rad32)[p] = make_float4(sky.x, sky.y, sky.z, 1.0f);
-        out.alb8[p] = 0xffffffffu;
-        reinterpret_cast<float4*>(out.gbuf)[p] = make_float4(-rd.x, -rd.y, -rd.z, -1.0f);
-      } else {
-        const Mat mat1 = unpack_material(h.y);
-        const F3 ro = f3(u.camPos[0], u.camPos[1], u.camPos[2]);
-        const F3 x1 = ro + rd * t;
-        const F3 n1 = hit_normal((int)h.z, rd);
-        out.alb8[p] = unorm8_(__fsqrt_rn(mat1.albedo.x)) | (unorm8_(__fsqrt_rn(mat1.albedo.y)) << 8) |
-                      (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
-        reinterpret_cast<float4*>(out.gbuf)[p] = make_float4(n1.x, n1.y, n1.z, t);
-        uint32_t rng = __float_as_uint(b.S0[p].w);
-        F3 radiance = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
-        keep = shade_vertex(u, b, 0, p, 0u, x1, n1, mat1, radiance, tp, rng, h.y, shadow, bounce);
-        if (!keep) finalize(out, p, radiance, h.y, fclamp);
-      }
-    }
-    emit(b, 1, p, shadow, bounce, keep);
-  }
-}
-
-// shade(k), k >= 1: resolve vertex k-1's shadow ray, then the bounce hit.
-__global__ void __launch_bounds__(256) k_wf_shade(Uni u, float fclamp, WfDev b, PathOut out, int wave) {
-  const int n = b.ctr[4 * wave + 2];
-  const uint32_t* list = active_of(b, wave);
-  const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    const int i = base + threadIdx.x;
-    bool shadow = false, bounce = false, keep = false;
-    uint32_t p = 0u;
-    if (i < n) {
-      p = list[i];
-      const float4 s0 = b.S0[p];
-      const float4 s1 = b.S1[p];
-      const float4 s2 = b.S2[p];
-      const uint4 h = b.hit[p];
-      F3 radiance = xyz(s0);
-      F3 tp = xyz(s1);
-      uint32_t rng = __float_as_uint(s0.w);
-      const uint32_t mat1bits = __float_as_uint(s1.w);
-      const uint32_t flags = __float_as_uint(s2.w);
-      if ((flags & kFlagShadow) && h.w == 0u) radiance = radiance + xyz(s2);
-      bool done = (flags & kFlagTerminal) != 0u;
-      if (!done) {
-        const F3 rd = xyz(b.R1[p]);
-        const F3 surf = xyz(b.R0[p]);
-        const float t = __uint_as_float(h.x);
-        if (t < 0.0f) {
-          radiance = radiance + tp * sky_color(u, rd, false);
-          done = true;
-        } else {
-          const F3 pos = surf + rd * t;
-          const F3 nrm = hit_normal((int)h.z, rd);
-          const Mat mat = unpack_material(h.y);
-          keep = shade_vertex(u, b, wave, p, (uint32_t)wave, pos, nrm, mat, radiance, tp, rng, mat1bits, shadow,
-                              bounce);
-          done = !keep;
-        }
-      }
-      if (done) finalize(out, p, radiance, mat1bits, fclamp);
-    }
-    emit(b, wave + 1, p, shadow, bounce, keep);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// host side
-// ---------------------------------------------------------------------------
-static WfDev to_wf(const WavefrontBufs& w) {
-  WfDev d;
-  d.R0 = (float4*)w.R0; d.R1 = (float4*)w.R1; d.R2 = (float4*)w.R2;
-  d.S0 = (float4*)w.S0; d.S1 = (float4*)w.S1; d.S2 = (float4*)w.S2;
-  d.hit = (uint4*)w.hit;
-  d.q0 = w.q[0]; d.q1 = w.q[1]; d.a0 = w.act[0]; d.a1 = w.act[1];
-  d.ctr = w.ctr;
-  return d;
-}
-
-static DScene to_dscene(const SceneDev& s) {
-  DScene d;
-  d.vox = s.vox; d.masks = s.masks; d.bits = s.bits; d.N = s.N; d.BG = s.BG;
-  return d;
-}
 
 size_t wavefront_bytes(int W, int H, int max_waves) {
   const size_t P = (size_t)W * H;
   return P * 16 * 7 + P * 4 * 2 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
 }
 
-template <bool kSmem, int kMinBlocks>
-static cudaError_t launch_trace_variant(int smem, int blocks_per_sm, int sms, const DScene& d, const WfDev& b, int w,
-                                       int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
-  auto* fn = k_wf_trace<kSmem, kMinBlocks>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-  }
-  int per = blocks_per_sm;
-  if (per <= 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, smem);
-    if (e != cudaSuccess || per < 1) per = 1;
-  }
-  fn<<<sms * per, 256, smem, st>>>(d, b, w, implicit_n, refill, stats);
-  return cudaGetLastError();
-}
-
-static int sm_count() {
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms > 0 ? sms : 1;
-}
-
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
                              cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves,
                              int* timed_waves) {
-  Uni u;
-  std::memcpy(&u, &uu, sizeof(Uni));
-  const int P = W * H;
-  const int nB = (int)u.params0[1];
-  const int waves = nB + 2;
-  if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
-  WfDev b = to_wf(wb);
-  DScene d = to_dscene(s);
-  cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
-  if (e != cudaSuccess) return e;
+  SingleJob job;
+  std::memcpy(&job.u, &uu, sizeof(Uni));
+  job.S.vox = s.vox; job.S.masks = s.masks; job.S.bits = s.bits; job.S.N = s.N; job.S.BG = s.BG;
+  job.out.rad16 = (uint2*)out.rad16;
+  job.out.rad32 = (float4*)out.rad32;
+  job.out.alb8 = out.alb8;
+  job.out.gbuf = (float4*)out.gbuf;
+  job.fclamp = fclamp;
+  job.W = W;
+  job.H = H;
+  const int waves = (int)job.u.params0[1] + 2;
   const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
-  const bool use_smem = smem_occ <= 64 * 1024;
-  const int smem = use_smem ? smem_occ : 0;
-  const int sms = sm_count();
-  const int refill = tune.refill_min > 0 ? tune.refill_min : 12;
-  const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 8);
-  uint32_t nl = 0;
-  k_wf_generate<<<(P + 255) / 256, 256, 0, st>>>(u, W, H, b);
-  nl++;
-  int timed = 0;
-  for (int w = 0; w < waves; w++) {
-    const bool tm = trace_ev && w < max_timed_waves;
-    if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
-    const int impl = w == 0 ? P : 0;
-    const int tb = tune.trace_blocks_per_sm;
-    if (use_smem) {
-      if (tune.trace_variant == 1) e = launch_trace_variant<true, 5>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
-      else if (tune.trace_variant == 2) e = launch_trace_variant<true, 6>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
-      else e = launch_trace_variant<true, 1>(smem, tb, sms, d, b, w, impl, refill, out.stats, st);
-    } else {
-      if (tune.trace_variant == 1) e = launch_trace_variant<false, 5>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
-      else if (tune.trace_variant == 2) e = launch_trace_variant<false, 6>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
-      else e = launch_trace_variant<false, 1>(0, tb, sms, d, b, w, impl, refill, out.stats, st);
-    }
-    if (e != cudaSuccess) return e;
-    if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
-    if (tm) timed++;
-    nl++;
-    if (w == 0) k_wf_shade_primary<<<sblocks, 256, 0, st>>>(u, fclamp, W, H, b, out);
-    else k_wf_shade<<<sblocks, 256, 0, st>>>(u, fclamp, b, out, w);
-    nl++;
-  }
-  if (launches) *launches += nl;
-  if (timed_waves) *timed_waves = timed;
-  return cudaGetLastError();
+  const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
+  return wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
+                         max_timed_waves, timed_waves);
 }
 
 }  // namespace vrt

@@ -393,7 +393,8 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
   }
   if (!r) r = dev_alloc(ctx, (void**)&s->ldr, P * 4, &s->bytes);
   if (!r) r = dev_alloc(ctx, (void**)&s->stats, kStatCount * 8, &s->bytes);
-  s->path_kernel = cfg->path_kernel == VRT_PATH_MEGAKERNEL ? VRT_PATH_MEGAKERNEL : VRT_PATH_WAVEFRONT;
+  s->path_kernel = (cfg->path_kernel == VRT_PATH_MEGAKERNEL || cfg->path_kernel == VRT_PATH_BATCH_ONLY)
+                       ? cfg->path_kernel : VRT_PATH_WAVEFRONT;
   if (!r && s->path_kernel == VRT_PATH_WAVEFRONT) {
     const int max_waves = 72;
     s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves);
@@ -529,6 +530,8 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (int r = set_dev(s->ctx)) return r;
   PathOut o;
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
+  if (s->path_kernel == VRT_PATH_BATCH_ONLY)
+    return fail(VRT_ERR_STATE, "session was created for batches only (VRT_PATH_BATCH_ONLY)");
   if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
     CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
                               &s->launches, s->timing ? s->tev : nullptr, VrtSession::kTimedWaves,
@@ -726,6 +729,276 @@ int vrt_read_hdr(VrtSession* s, float* rgb, size_t bytes) {
       rgb[p * 3 + c] = (float)((il * a) * a);
     }
   }
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct VrtBatch {
+  VrtCtx* ctx = nullptr;
+  std::vector<VrtSession*> sessions;
+  uint32_t P = 0;
+  uint64_t bytes = 0;
+  JobHost* h_jobs = nullptr;          // pinned staging of the job table
+  void* d_jobs = nullptr;
+  uint32_t* d_firsts = nullptr;
+  void* wf_mem = nullptr;
+  size_t wf_bytes = 0;
+  WavefrontBufs wf;
+  WavefrontTuning tune;
+  unsigned long long* stats = nullptr;
+  bool use_graph = true;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_waves = -1;
+  WavefrontTuning graph_tune;
+  cudaEvent_t ev_start = nullptr, ev_end = nullptr, ev_upload = nullptr;
+  bool uploaded = false;
+  uint32_t launches = 0;
+  bool have_frame = false;
+};
+
+static void batch_drop_graph(VrtBatch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  b->gexec = nullptr;
+  b->graph_waves = -1;
+}
+
+extern "C" {
+
+int vrt_batch_destroy(VrtBatch* b) {
+  if (!b) return VRT_OK;
+  VrtCtx* c = b->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  batch_drop_graph(b);
+  dev_free(c, b->d_jobs, b->sessions.size() * sizeof(JobHost), &b->bytes);
+  dev_free(c, b->d_firsts, b->sessions.size() * 4, &b->bytes);
+  dev_free(c, b->wf_mem, b->wf_bytes, &b->bytes);
+  dev_free(c, b->stats, kStatCount * 8, &b->bytes);
+  if (b->h_jobs) cudaFreeHost(b->h_jobs);
+  for (cudaEvent_t e : {b->ev_start, b->ev_end, b->ev_upload})
+    if (e) cudaEventDestroy(e);
+  delete b;
+  return VRT_OK;
+}
+
+int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch** out) {
+  if (!ctx || !sessions || n < 1 || !out) return fail(VRT_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  uint64_t P = 0;
+  for (int i = 0; i < n; i++) {
+    if (!sessions[i] || sessions[i]->ctx != ctx) return fail(VRT_ERR_INVALID, "session %d is NULL or of another context", i);
+    for (int k = 0; k < i; k++)
+      if (sessions[k] == sessions[i]) return fail(VRT_ERR_INVALID, "session %d appears twice", i);
+    P += (uint64_t)sessions[i]->W * sessions[i]->H;
+  }
+  if (P >= (1ull << 31)) return fail(VRT_ERR_INVALID, "batch of %llu pixels exceeds 2^31", (unsigned long long)P);
+  if (int r = set_dev(ctx)) return r;
+  VrtBatch* b = new VrtBatch();
+  b->ctx = ctx;
+  b->sessions.assign(sessions, sessions + n);
+  b->P = (uint32_t)P;
+  const int max_waves = 72;
+  b->wf_bytes = wavefront_bytes((int)b->P, 1, max_waves);
+  int r = dev_alloc(ctx, &b->wf_mem, b->wf_bytes, &b->bytes);
+  if (!r) r = dev_alloc(ctx, &b->d_jobs, (size_t)n * sizeof(JobHost), &b->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&b->d_firsts, (size_t)n * 4, &b->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&b->stats, kStatCount * 8, &b->bytes);
+  if (!r && cudaMallocHost((void**)&b->h_jobs, (size_t)n * sizeof(JobHost)) != cudaSuccess)
+    r = fail(VRT_ERR_OOM, "pinned job table");
+  if (!r && (cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_end) != cudaSuccess ||
+             cudaEventCreateWithFlags(&b->ev_upload, cudaEventDisableTiming) != cudaSuccess))
+    r = fail(VRT_ERR_CUDA, "cudaEventCreate failed");
+  if (r) {
+    std::string keep = g_err;
+    vrt_batch_destroy(b);
+    g_err = keep;
+    return r;
+  }
+  const size_t Pz = b->P;
+  char* m = (char*)b->wf_mem;
+  void** f4[7] = {&b->wf.R0, &b->wf.R1, &b->wf.R2, &b->wf.S0, &b->wf.S1, &b->wf.S2, &b->wf.hit};
+  for (auto* f : f4) { *f = m; m += Pz * 16; }
+  for (int i = 0; i < 2; i++) { b->wf.q[i] = (uint32_t*)m; m += Pz * 8; }
+  for (int i = 0; i < 2; i++) { b->wf.act[i] = (uint32_t*)m; m += Pz * 4; }
+  b->wf.ctr = (int*)m;
+  b->wf.max_waves = max_waves;
+  std::vector<uint32_t> firsts((size_t)n);
+  uint32_t acc = 0;
+  for (int i = 0; i < n; i++) { firsts[(size_t)i] = acc; acc += (uint32_t)(sessions[i]->W * sessions[i]->H); }
+  cudaError_t e = cudaMemcpyAsync(b->d_firsts, firsts.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    vrt_batch_destroy(b);
+    return fail(VRT_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));
+  }
+  *out = b;
+  return VRT_OK;
+}
+
+int vrt_batch_set_graph(VrtBatch* b, int enable) {
+  if (!b) return fail(VRT_ERR_INVALID, "batch is NULL");
+  b->use_graph = enable != 0;
+  if (!b->use_graph) batch_drop_graph(b);
+  return VRT_OK;
+}
+
+int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
+  if (!b || !t) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 2)
+    return fail(VRT_ERR_INVALID, "tuning out of range");
+  b->tune.refill_min = t->refill_min ? t->refill_min : 12;
+  b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
+  b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
+  b->tune.trace_variant = t->trace_variant;
+  return VRT_OK;
+}
+
+static bool same_tuning(const WavefrontTuning& a, const WavefrontTuning& c) {
+  return a.refill_min == c.refill_min && a.trace_blocks_per_sm == c.trace_blocks_per_sm &&
+         a.shade_blocks_per_sm == c.shade_blocks_per_sm && a.trace_variant == c.trace_variant;
+}
+
+int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u) {
+  if (!b || !u) return fail(VRT_ERR_INVALID, "NULL argument");
+  const int n = (int)b->sessions.size();
+  int maxB = 0;
+  for (int i = 0; i < n; i++) {
+    if (int r = check_uniforms(b->sessions[(size_t)i], &u[i])) return r;
+    maxB = std::max(maxB, (int)u[i].params0[1]);
+  }
+  const int waves = maxB + 2;
+  if (waves + 1 > b->wf.max_waves) return fail(VRT_ERR_INVALID, "bounce count %d too large for a batch", maxB);
+  if (int r = set_dev(b->ctx)) return r;
+  cudaStream_t st = b->ctx->stream;
+  // the staging table may still be read by the previous frame's upload
+  if (b->uploaded) CUDA_TRY(cudaEventSynchronize(b->ev_upload));
+  uint32_t first = 0;
+  for (int i = 0; i < n; i++) {
+    VrtSession* s = b->sessions[(size_t)i];
+    JobHost& j = b->h_jobs[i];
+    std::memset(&j, 0, sizeof j);
+    const int p = parity_of(s);
+    j.u = u[i];
+    j.vox = s->scene->dev.vox; j.masks = s->scene->dev.masks; j.bits = s->scene->dev.bits;
+    j.N = s->scene->dev.N; j.BG = s->scene->dev.BG;
+    j.rad16 = s->rad16; j.rad32 = s->rad32; j.alb8 = s->alb8; j.gbuf = s->gbuf[p];
+    j.W = s->W; j.H = s->H; j.first = first; j.fclamp = s->fclamp;
+    j.acc_prev = s->accum[1 - p]; j.acc_cur = s->accum[p]; j.gbuf_prev = s->gbuf[1 - p];
+    j.den0 = s->den[0]; j.den1 = s->den[1]; j.ldr = s->ldr; j.acc_f32 = s->acc_f32 ? 1 : 0;
+    first += (uint32_t)(s->W * s->H);
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, (size_t)n * sizeof(JobHost), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(b->ev_upload, st));
+  b->uploaded = true;
+  CUDA_TRY(cudaMemsetAsync(b->stats, 0, kStatCount * 8, st));
+  CUDA_TRY(cudaEventRecord(b->ev_start, st));
+  b->launches = 0;
+  if (b->use_graph) {
+    if (!b->gexec || b->graph_waves != waves || !same_tuning(b->graph_tune, b->tune)) {
+      batch_drop_graph(b);
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      uint32_t nl = 0;
+      cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, n, b->P, waves, b->wf, b->tune, b->stats, st, &nl);
+      cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+      if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(VRT_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+      }
+      e = cudaGraphInstantiate(&b->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        b->gexec = nullptr;
+        return fail(VRT_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+      }
+      b->graph_waves = waves;
+      b->graph_tune = b->tune;
+      b->launches = nl;
+    } else {
+      b->launches = (uint32_t)(1 + 2 * waves + 5);
+    }
+    CUDA_TRY(cudaGraphLaunch(b->gexec, st));
+  } else {
+    CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, n, b->P, waves, b->wf, b->tune, b->stats, st, &b->launches));
+  }
+  CUDA_TRY(cudaEventRecord(b->ev_end, st));
+  for (int i = 0; i < n; i++) {
+    VrtSession* s = b->sessions[(size_t)i];
+    s->last_denoise = (u[i].params0[2] & 2u) != 0u;
+    s->launches = 0;
+    vrt_end_frame(s);
+  }
+  b->have_frame = true;
+  return VRT_OK;
+}
+
+int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out) {
+  if (!b || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(b->ctx)) return r;
+  std::memset(out, 0, sizeof(*out));
+  unsigned long long h[kStatCount];
+  CUDA_TRY(cudaMemcpyAsync(h, b->stats, sizeof h, cudaMemcpyDeviceToHost, b->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  out->rays = h[kStatRays];
+  out->dda_outer = h[kStatOuter];
+  out->dda_inner = h[kStatInner];
+  out->voxel_reads = h[kStatVReads];
+  out->pixels = h[kStatPixels];
+  out->launches = b->launches;
+  if (b->have_frame) {
+    float ms = 0.0f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, b->ev_start, b->ev_end));
+    out->ms_total = ms;
+  }
+  return VRT_OK;
+}
+
+int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms) {
+  if (!b || !u || frames < 1) return fail(VRT_ERR_INVALID, "bad argument");
+  static const int refills[] = {4, 8, 12, 16, 24};
+  static const int variants[] = {0, 1};
+  static const int shades[] = {8, 16, 32};
+  const WavefrontTuning keep = b->tune;
+  const bool keep_graph = b->use_graph;
+  WavefrontTuning win = keep;
+  float win_ms = 1e30f;
+  std::vector<float> ms((size_t)frames);
+  b->use_graph = false;
+  for (int rf : refills)
+    for (int va : variants)
+      for (int sh : shades) {
+        b->tune.refill_min = rf;
+        b->tune.trace_variant = va;
+        b->tune.shade_blocks_per_sm = sh;
+        b->tune.trace_blocks_per_sm = 0;
+        int r = vrt_batch_frame(b, u);
+        for (int f = 0; f < frames && !r; f++) {
+          r = vrt_batch_frame(b, u);
+          VrtFrameStats st;
+          if (!r) r = vrt_batch_last_stats(b, &st);
+          ms[(size_t)f] = st.ms_total;
+        }
+        if (r) { b->tune = keep; b->use_graph = keep_graph; return r; }
+        std::sort(ms.begin(), ms.end());
+        if (ms[(size_t)frames / 2] < win_ms) { win_ms = ms[(size_t)frames / 2]; win = b->tune; }
+      }
+  b->tune = win;
+  b->use_graph = keep_graph;
+  batch_drop_graph(b);
+  if (best) {
+    best->refill_min = win.refill_min;
+    best->trace_blocks_per_sm = win.trace_blocks_per_sm;
+    best->shade_blocks_per_sm = win.shade_blocks_per_sm;
+    best->trace_variant = win.trace_variant;
+  }
+  if (best_ms) *best_ms = win_ms;
+  for (VrtSession* s : b->sessions)
+    if (int r = vrt_session_reset(s)) return r;
   return VRT_OK;
 }
 

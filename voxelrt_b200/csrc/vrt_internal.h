@@ -50,6 +50,37 @@ struct WavefrontTuning {
   int trace_variant = 0;        // 0: registers unconstrained, 1: >= 5 blocks/SM, 2: >= 6 blocks/SM
 };
 
+// Host mirror of the device job table entry (JobDev in wavefront_core.cuh):
+// one session rendered inside a batch frame.  Same field order and layout.
+struct JobHost {
+  VrtUniforms u;
+  const uint32_t* vox;
+  const uint32_t* masks;
+  const uint32_t* bits;
+  int N, BG;
+  void* rad16;
+  void* rad32;
+  uint32_t* alb8;
+  void* gbuf;
+  int W, H;
+  uint32_t first;
+  float fclamp;
+  const void* acc_prev;
+  void* acc_cur;
+  const void* gbuf_prev;
+  void* den0;
+  void* den1;
+  uint32_t* ldr;
+  int acc_f32;
+  int pad[3];
+};
+
+// One batch frame over n jobs of P pixels in total: wavefront path trace
+// (waves = max bounces + 2), temporal, 3x a-trous, present.
+cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
+                               const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
+                               cudaStream_t st, uint32_t* launches);
+
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
