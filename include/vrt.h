@@ -51,6 +51,7 @@ typedef struct VrtCtx VrtCtx;
 typedef struct VrtScene VrtScene;
 typedef struct VrtSession VrtSession;
 typedef struct VrtBatch VrtBatch;
+typedef struct VrtServer VrtServer;
 
 /* Uniform block, byte-identical to the reference's 304-byte UBO
  * (common.wgsl:13-35, packed by main.js:399-426). */
@@ -233,12 +234,55 @@ int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch**
 int vrt_batch_destroy(VrtBatch* b);
 /* u: n uniform blocks, one per session, in creation order. */
 int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u);
+/* One frame for the m sessions idx[0..m) of the batch (indices in creation
+ * order), uniforms u[0..m); launched directly, without the graph. */
+int vrt_batch_frame_subset(VrtBatch* b, const int* idx, int m, const VrtUniforms* u);
 int vrt_batch_set_graph(VrtBatch* b, int enable);
 int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t);
 /* Autotuner over whole batch frames (resets every session's history). */
 int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms);
 /* Counters of the last batch frame; ms_total = device time of the frame. */
 int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out);
+
+/* ---- serving (no counterpart in the reference) -------------------------- */
+/* A voxel edit applied to a session's scene before its frame renders. */
+typedef struct VrtEditBox {
+  int x0, y0, z0, x1, y1, z1;   /* inclusive voxel box (clipped to the grid)    */
+  uint32_t value;               /* packed voxel written (0 = carve to air)      */
+  int pad;
+} VrtEditBox;
+
+typedef struct VrtCompletion {
+  uint64_t ticket;
+  int session;
+  int pad;
+  double t_arrival;             /* seconds on the server clock                  */
+  double t_done;                /* device completion time on the same clock     */
+} VrtCompletion;
+
+/* Continuous batching over device-resident sessions (each should own its
+ * scene when requests carry edits).  A request renders the next frame of one
+ * session after applying its edits.  Requests queue in arrival order; every
+ * launch takes the oldest pending request of each idle session into one batch
+ * frame, so requests that arrive while others are on the GPU join the next
+ * launch; up to max_in_flight batch frames are queued on the device at once.
+ * Frames of one session are rendered in request order, so each result equals
+ * rendering the same request sequence alone. */
+int vrt_server_create(VrtCtx* ctx, VrtSession* const* sessions, int n, int max_in_flight, VrtServer** out);
+int vrt_server_destroy(VrtServer* sv);
+/* Seconds since the server was created (clock of t_arrival / t_done). */
+double vrt_server_now(VrtServer* sv);
+/* t_arrival < 0 means now.  ldr_out (may be NULL) receives the frame's rgba8
+ * image (W*H*4 bytes) when the request completes; pinned memory keeps the
+ * copy asynchronous. */
+int vrt_server_submit(VrtServer* sv, int session, const VrtUniforms* u, const VrtEditBox* edits, int n_edits,
+                      double t_arrival, void* ldr_out, uint64_t* ticket);
+/* Non-blocking: retires finished requests into out[0..max_out) and launches
+ * new batch frames while device slots are free. */
+int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
+/* Blocks until every submitted request completed (or out[] is full). */
+int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
+int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
 
 /* ---- allocation-free denoise ------------------------------------------- */
 /* No counterpart in the reference.  The 3-iteration a-trous chain (steps

@@ -1,0 +1,99 @@
+"""Serving (vrt_server_*): requests of several sessions, with voxel edits
+between frames, are batched continuously; each request's image must equal the
+image of the same request sequence rendered alone, session by session."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SESSIONS = [(2, 128, 11, 320, 180, 2), (1, 64, 1, 256, 144, 3), (3, 128, 4, 200, 112, 1), (2, 256, 2, 480, 270, 2)]
+
+
+@pytest.fixture(scope="module")
+def ctx(vrt):
+    c = vrt.Context(0)
+    yield c
+    c.close()
+
+
+def _requests(vrt, spawns, n_req, seed):
+    rng = np.random.default_rng(seed)
+    frames = [0] * len(SESSIONS)
+    reqs = []
+    for _ in range(n_req):
+        k = int(rng.integers(0, len(SESSIONS)))
+        kind, n, sd, W, H, nb = SESSIONS[k]
+        f = frames[k]
+        frames[k] += 1
+        pose = vrt.camera_spline(spawns[k], f)
+        prev = vrt.camera_spline(spawns[k], f - 1) if f else None
+        u = vrt.make_uniforms(pose, prev, vrt.Lighting(), 7 + f, nb, 3, W, H)
+        size = rng.integers(1, 17, 3)
+        lo = rng.integers(0, n - 16, 3)
+        val = 0 if rng.random() < 0.5 else int(rng.integers(1, 1 << 24))
+        edits = [(int(lo[0]), int(lo[1]), int(lo[2]), int(lo[0] + size[0] - 1), int(lo[1] + size[1] - 1),
+                  int(lo[2] + size[2] - 1), val)]
+        reqs.append((k, u, edits))
+    return reqs
+
+
+def test_server_results_equal_alone(ctx, vrt):
+    vox, spawns, served, ref_sc, ref_s, srv_sc = [], [], [], [], [], []
+    for kind, n, sd, W, H, nb in SESSIONS:
+        v, sp = vrt.generate_scene(kind, n, sd)
+        vox.append(v)
+        spawns.append(sp)
+        sc = vrt.Scene(ctx, v, n)
+        srv_sc.append(sc)
+        served.append(vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, path_kernel="batch_only"))
+        rsc = vrt.Scene(ctx, v, n)
+        ref_sc.append(rsc)
+        ref_s.append(vrt.Session(ctx, rsc, W, H, firefly_clamp=10.0))
+    reqs = _requests(vrt, spawns, 24, 3)
+    server = vrt.Server(ctx, served, max_in_flight=2)
+    outs = []
+    tickets = {}
+    done = []
+    for i, (k, u, edits) in enumerate(reqs):
+        W, H = SESSIONS[k][3], SESSIONS[k][4]
+        buf = np.zeros(W * H * 4, np.uint8)
+        outs.append(buf)
+        tickets[server.submit(k, u, edits, ldr_out=buf)] = i
+        if i % 5 == 4:
+            done += server.poll()             # requests keep arriving while batches run
+    done += server.drain()
+    assert sorted(tickets) == sorted(t for t, *_ in done)
+    for t, sess, t_arr, t_done in done:
+        assert t_done >= t_arr - 1e-3
+    # the same requests, session by session, through plain frames
+    for i, (k, u, edits) in enumerate(reqs):
+        for e in edits:
+            ref_sc[k].edit_box(*e)
+        ref_s[k].frame(u)
+        want = ref_s[k].ldr().ravel()
+        assert np.array_equal(outs[i], want), f"request {i} (session {k}) differs"
+    for k in range(len(SESSIONS)):
+        assert np.array_equal(served[k].accum(), ref_s[k].accum())
+        v1, b1, m1 = srv_sc[k].read()
+        v2, b2, m2 = ref_sc[k].read()
+        assert np.array_equal(v1, v2) and np.array_equal(b1, b2) and np.array_equal(m1, m2)
+    server.close()
+    for s in served + ref_s:
+        s.close()
+    for sc in srv_sc + ref_sc:
+        sc.close()
+
+
+def test_server_admission_budget(vrt):
+    c = vrt.Context(0, hbm_budget_bytes=64 << 20)
+    vox, _ = vrt.generate_scene(1, 64, 1)
+    sc = vrt.Scene(c, vox, 64)
+    ok = [vrt.Session(c, sc, 640, 360, path_kernel="batch_only")]
+    with pytest.raises(vrt.VrtError) as e:
+        for _ in range(8):
+            ok.append(vrt.Session(c, sc, 640, 360, path_kernel="batch_only"))
+    assert e.value.code == 5
+    for s in ok:
+        s.close()
+    sc.close()
+    c.close()

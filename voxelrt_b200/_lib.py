@@ -64,6 +64,16 @@ PATH_MEGAKERNEL = 1
 PATH_BATCH_ONLY = 2
 
 
+class VrtEditBox(C.Structure):
+    _fields_ = [("x0", C.c_int), ("y0", C.c_int), ("z0", C.c_int), ("x1", C.c_int), ("y1", C.c_int),
+                ("z1", C.c_int), ("value", C.c_uint32), ("pad", C.c_int)]
+
+
+class VrtCompletion(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("session", C.c_int), ("pad", C.c_int), ("t_arrival", C.c_double),
+                ("t_done", C.c_double)]
+
+
 class VrtHit(C.Structure):
     _fields_ = [("t", C.c_float), ("n", C.c_float * 3), ("mat", C.c_uint32), ("voxel", C.c_int32 * 3),
                 ("face", C.c_int32), ("steps", C.c_uint32), ("bytes", C.c_uint32), ("pad", C.c_uint32)]
@@ -140,9 +150,18 @@ SIGNATURES = {
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
+    "vrt_server_create": (I, [P, C.POINTER(P), I, I, C.POINTER(P)]),
+    "vrt_server_destroy": (I, [P]),
+    "vrt_server_now": (C.c_double, [P]),
+    "vrt_server_submit": (I, [P, I, C.POINTER(VrtUniforms), C.POINTER(VrtEditBox), I, C.c_double, P,
+                              C.POINTER(C.c_uint64)]),
+    "vrt_server_poll": (I, [P, C.POINTER(VrtCompletion), I, C.POINTER(I)]),
+    "vrt_server_drain": (I, [P, C.POINTER(VrtCompletion), I, C.POINTER(I)]),
+    "vrt_server_pending": (I, [P, C.POINTER(I), C.POINTER(I)]),
     "vrt_batch_create": (I, [P, C.POINTER(P), I, C.POINTER(P)]),
     "vrt_batch_destroy": (I, [P]),
     "vrt_batch_frame": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_batch_frame_subset": (I, [P, P, I, C.POINTER(VrtUniforms)]),
     "vrt_batch_set_graph": (I, [P, I]),
     "vrt_batch_set_tuning": (I, [P, C.POINTER(VrtTuning)]),
     "vrt_batch_autotune": (I, [P, C.POINTER(VrtUniforms), I, C.POINTER(VrtTuning), C.POINTER(C.c_float)]),

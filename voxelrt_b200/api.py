@@ -12,8 +12,9 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtDeviceConfig, VrtFrameStats,
-                   VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms, check, lib, ptr)
+from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtCompletion,
+                   VrtDeviceConfig, VrtEditBox, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
+                   check, lib, ptr)
 
 # Reference constants (scene.js:5-6, common.wgsl:11)
 VOXEL_SIZE = 1.0 / 16.0
@@ -308,6 +309,57 @@ class Batch:
     def close(self) -> None:
         if self.h:
             lib.vrt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous batching over device-resident sessions (vrt_server_*)."""
+
+    def __init__(self, ctx: Context, sessions: list, max_in_flight: int = 2):
+        arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
+        h = C.c_void_p()
+        check(lib.vrt_server_create(ctx.h, arr, len(sessions), int(max_in_flight), C.byref(h)))
+        self.h, self.ctx, self.sessions = h, ctx, list(sessions)
+        self._buf = (VrtCompletion * 4096)()
+
+    def now(self) -> float:
+        return float(lib.vrt_server_now(self.h))
+
+    def submit(self, session: int, u: VrtUniforms, edits=(), t_arrival: float = -1.0, ldr_out=None) -> int:
+        """edits: iterable of (x0, y0, z0, x1, y1, z1, value); ldr_out: uint8 array of W*H*4 or None."""
+        eds = (VrtEditBox * max(1, len(edits)))(*[VrtEditBox(*e, 0) for e in edits]) if edits else None
+        t = C.c_uint64()
+        check(lib.vrt_server_submit(self.h, int(session), C.byref(u), eds, len(edits), float(t_arrival),
+                                    ptr(ldr_out) if ldr_out is not None else None, C.byref(t)))
+        return int(t.value)
+
+    def _collect(self, fn):
+        n = C.c_int()
+        check(fn(self.h, self._buf, len(self._buf), C.byref(n)))
+        return [(c.ticket, c.session, c.t_arrival, c.t_done) for c in self._buf[:n.value]]
+
+    def poll(self):
+        return self._collect(lib.vrt_server_poll)
+
+    def drain(self):
+        out = []
+        while True:
+            got = self._collect(lib.vrt_server_drain)
+            out += got
+            q, f = C.c_int(), C.c_int()
+            check(lib.vrt_server_pending(self.h, C.byref(q), C.byref(f)))
+            if q.value == 0 and f.value == 0:
+                return out
+
+    def close(self) -> None:
+        if self.h:
+            lib.vrt_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

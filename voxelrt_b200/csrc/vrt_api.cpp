@@ -13,6 +13,8 @@
 #include <vector>
 #include <mutex>
 #include <algorithm>
+#include <chrono>
+#include <deque>
 #include "vrt_internal.h"
 
 using namespace vrt;
@@ -743,6 +745,7 @@ struct VrtBatch {
   uint32_t P = 0;
   uint64_t bytes = 0;
   JobHost* h_jobs = nullptr;          // pinned staging of the job table
+  uint32_t* h_firsts = nullptr;       // pinned staging of the jobs' first pixels
   void* d_jobs = nullptr;
   uint32_t* d_firsts = nullptr;
   void* wf_mem = nullptr;
@@ -779,6 +782,7 @@ int vrt_batch_destroy(VrtBatch* b) {
   dev_free(c, b->wf_mem, b->wf_bytes, &b->bytes);
   dev_free(c, b->stats, kStatCount * 8, &b->bytes);
   if (b->h_jobs) cudaFreeHost(b->h_jobs);
+  if (b->h_firsts) cudaFreeHost(b->h_firsts);
   for (cudaEvent_t e : {b->ev_start, b->ev_end, b->ev_upload})
     if (e) cudaEventDestroy(e);
   delete b;
@@ -807,7 +811,8 @@ int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch**
   if (!r) r = dev_alloc(ctx, &b->d_jobs, (size_t)n * sizeof(JobHost), &b->bytes);
   if (!r) r = dev_alloc(ctx, (void**)&b->d_firsts, (size_t)n * 4, &b->bytes);
   if (!r) r = dev_alloc(ctx, (void**)&b->stats, kStatCount * 8, &b->bytes);
-  if (!r && cudaMallocHost((void**)&b->h_jobs, (size_t)n * sizeof(JobHost)) != cudaSuccess)
+  if (!r && (cudaMallocHost((void**)&b->h_jobs, (size_t)n * sizeof(JobHost)) != cudaSuccess ||
+             cudaMallocHost((void**)&b->h_firsts, (size_t)n * 4) != cudaSuccess))
     r = fail(VRT_ERR_OOM, "pinned job table");
   if (!r && (cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_end) != cudaSuccess ||
              cudaEventCreateWithFlags(&b->ev_upload, cudaEventDisableTiming) != cudaSuccess))
@@ -863,23 +868,37 @@ static bool same_tuning(const WavefrontTuning& a, const WavefrontTuning& c) {
          a.shade_blocks_per_sm == c.shade_blocks_per_sm && a.trace_variant == c.trace_variant;
 }
 
-int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u) {
-  if (!b || !u) return fail(VRT_ERR_INVALID, "NULL argument");
+}  // extern "C"
+
+// One frame for sessions idx[0..m) of the batch (all of them when idx is
+// NULL), uniforms u[0..m).  The CUDA graph is used only for the full set in
+// creation order.
+static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniforms* u) {
   const int n = (int)b->sessions.size();
+  if (m < 1 || m > n) return fail(VRT_ERR_INVALID, "job count %d not in 1..%d", m, n);
+  bool full = idx == nullptr && m == n;
+  std::vector<VrtSession*> ss((size_t)m);
+  for (int i = 0; i < m; i++) {
+    const int k = idx ? idx[i] : i;
+    if (k < 0 || k >= n) return fail(VRT_ERR_INVALID, "job index %d out of range", k);
+    ss[(size_t)i] = b->sessions[(size_t)k];
+    for (int q = 0; q < i; q++)
+      if (ss[(size_t)q] == ss[(size_t)i]) return fail(VRT_ERR_INVALID, "session %d listed twice", k);
+  }
   int maxB = 0;
-  for (int i = 0; i < n; i++) {
-    if (int r = check_uniforms(b->sessions[(size_t)i], &u[i])) return r;
+  for (int i = 0; i < m; i++) {
+    if (int r = check_uniforms(ss[(size_t)i], &u[i])) return r;
     maxB = std::max(maxB, (int)u[i].params0[1]);
   }
   const int waves = maxB + 2;
   if (waves + 1 > b->wf.max_waves) return fail(VRT_ERR_INVALID, "bounce count %d too large for a batch", maxB);
   if (int r = set_dev(b->ctx)) return r;
   cudaStream_t st = b->ctx->stream;
-  // the staging table may still be read by the previous frame's upload
+  // the staging tables may still be read by the previous frame's upload
   if (b->uploaded) CUDA_TRY(cudaEventSynchronize(b->ev_upload));
   uint32_t first = 0;
-  for (int i = 0; i < n; i++) {
-    VrtSession* s = b->sessions[(size_t)i];
+  for (int i = 0; i < m; i++) {
+    VrtSession* s = ss[(size_t)i];
     JobHost& j = b->h_jobs[i];
     std::memset(&j, 0, sizeof j);
     const int p = parity_of(s);
@@ -890,21 +909,24 @@ int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u) {
     j.W = s->W; j.H = s->H; j.first = first; j.fclamp = s->fclamp;
     j.acc_prev = s->accum[1 - p]; j.acc_cur = s->accum[p]; j.gbuf_prev = s->gbuf[1 - p];
     j.den0 = s->den[0]; j.den1 = s->den[1]; j.ldr = s->ldr; j.acc_f32 = s->acc_f32 ? 1 : 0;
+    b->h_firsts[i] = first;
     first += (uint32_t)(s->W * s->H);
   }
-  CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, (size_t)n * sizeof(JobHost), cudaMemcpyHostToDevice, st));
+  const uint32_t P = first;
+  CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, (size_t)m * sizeof(JobHost), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(b->d_firsts, b->h_firsts, (size_t)m * 4, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(b->ev_upload, st));
   b->uploaded = true;
   CUDA_TRY(cudaMemsetAsync(b->stats, 0, kStatCount * 8, st));
   CUDA_TRY(cudaEventRecord(b->ev_start, st));
   b->launches = 0;
-  if (b->use_graph) {
+  if (b->use_graph && full) {
     if (!b->gexec || b->graph_waves != waves || !same_tuning(b->graph_tune, b->tune)) {
       batch_drop_graph(b);
       cudaGraph_t graph = nullptr;
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       uint32_t nl = 0;
-      cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, n, b->P, waves, b->wf, b->tune, b->stats, st, &nl);
+      cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl);
       cudaError_t e2 = cudaStreamEndCapture(st, &graph);
       if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -918,23 +940,33 @@ int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u) {
       }
       b->graph_waves = waves;
       b->graph_tune = b->tune;
-      b->launches = nl;
-    } else {
-      b->launches = (uint32_t)(1 + 2 * waves + 5);
     }
+    b->launches = (uint32_t)(1 + 2 * waves + 5);
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
-    CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, n, b->P, waves, b->wf, b->tune, b->stats, st, &b->launches));
+    CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
-  for (int i = 0; i < n; i++) {
-    VrtSession* s = b->sessions[(size_t)i];
+  for (int i = 0; i < m; i++) {
+    VrtSession* s = ss[(size_t)i];
     s->last_denoise = (u[i].params0[2] & 2u) != 0u;
     s->launches = 0;
     vrt_end_frame(s);
   }
   b->have_frame = true;
   return VRT_OK;
+}
+
+extern "C" {
+
+int vrt_batch_frame(VrtBatch* b, const VrtUniforms* u) {
+  if (!b || !u) return fail(VRT_ERR_INVALID, "NULL argument");
+  return batch_frame_impl(b, nullptr, (int)b->sessions.size(), u);
+}
+
+int vrt_batch_frame_subset(VrtBatch* b, const int* idx, int m, const VrtUniforms* u) {
+  if (!b || !idx || !u) return fail(VRT_ERR_INVALID, "NULL argument");
+  return batch_frame_impl(b, idx, m, u);
 }
 
 int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out) {
@@ -999,6 +1031,222 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
   if (best_ms) *best_ms = win_ms;
   for (VrtSession* s : b->sessions)
     if (int r = vrt_session_reset(s)) return r;
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// serving: continuous batching over device-resident sessions
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct VrtServer {
+  struct Req {
+    uint64_t ticket = 0;
+    int session = 0;
+    VrtUniforms u;
+    std::vector<VrtEditBox> edits;
+    double t_arrival = 0.0;
+    void* ldr_out = nullptr;
+  };
+  struct Flight {
+    cudaEvent_t done = nullptr;
+    std::vector<Req> reqs;
+  };
+  VrtCtx* ctx = nullptr;
+  VrtBatch* batch = nullptr;
+  int n = 0;
+  int max_in_flight = 2;
+  std::deque<Req> pending;
+  std::deque<Flight> flights;
+  std::vector<char> busy;
+  std::vector<cudaEvent_t> spare_events;
+  uint64_t next_ticket = 1;
+  std::chrono::steady_clock::time_point t0;
+  cudaEvent_t ref = nullptr;     // device time origin
+  double ref_host = 0.0;         // host time (s) at which `ref` had completed
+  uint64_t completed = 0;
+  uint64_t launched_frames = 0;
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+static int server_launch(VrtServer* sv) {
+  // oldest pending request of every idle session, in arrival order
+  std::vector<char> picked((size_t)sv->n, 0);
+  std::vector<VrtServer::Req> take;
+  for (auto it = sv->pending.begin(); it != sv->pending.end();) {
+    const int k = it->session;
+    if (!sv->busy[(size_t)k] && !picked[(size_t)k]) {
+      picked[(size_t)k] = 1;
+      take.push_back(std::move(*it));
+      it = sv->pending.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  if (take.empty()) return VRT_OK;
+  cudaStream_t st = sv->ctx->stream;
+  std::vector<int> idx;
+  std::vector<VrtUniforms> us;
+  for (auto& r : take) {
+    VrtSession* s = sv->batch->sessions[(size_t)r.session];
+    for (const VrtEditBox& e : r.edits)
+      if (int rc = vrt_scene_edit_box(s->scene, e.x0, e.y0, e.z0, e.x1, e.y1, e.z1, e.value)) return rc;
+    idx.push_back(r.session);
+    us.push_back(r.u);
+  }
+  if (int rc = batch_frame_impl(sv->batch, idx.data(), (int)idx.size(), us.data())) return rc;
+  for (auto& r : take) {
+    VrtSession* s = sv->batch->sessions[(size_t)r.session];
+    if (r.ldr_out)
+      CUDA_TRY(cudaMemcpyAsync(r.ldr_out, s->ldr, px(s) * 4, cudaMemcpyDeviceToHost, st));
+    sv->busy[(size_t)r.session] = 1;
+  }
+  VrtServer::Flight f;
+  if (!sv->spare_events.empty()) {
+    f.done = sv->spare_events.back();
+    sv->spare_events.pop_back();
+  } else {
+    CUDA_TRY(cudaEventCreate(&f.done));
+  }
+  CUDA_TRY(cudaEventRecord(f.done, st));
+  f.reqs = std::move(take);
+  sv->flights.push_back(std::move(f));
+  sv->launched_frames++;
+  return VRT_OK;
+}
+
+// Retires finished flights into out[]; returns the number written.
+static int server_retire(VrtServer* sv, VrtCompletion* out, int max_out, bool block, int* err) {
+  int k = 0;
+  *err = VRT_OK;
+  while (!sv->flights.empty()) {
+    VrtServer::Flight& f = sv->flights.front();
+    if ((int)f.reqs.size() > max_out - k) break;
+    cudaError_t q = block ? cudaEventSynchronize(f.done) : cudaEventQuery(f.done);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) { *err = fail(VRT_ERR_CUDA, "server: %s", cudaGetErrorString(q)); break; }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, sv->ref, f.done);
+    const double t_done = sv->ref_host + ms / 1e3;
+    for (auto& r : f.reqs) {
+      out[k].ticket = r.ticket;
+      out[k].session = r.session;
+      out[k].pad = 0;
+      out[k].t_arrival = r.t_arrival;
+      out[k].t_done = t_done;
+      k++;
+      sv->busy[(size_t)r.session] = 0;
+      sv->completed++;
+    }
+    sv->spare_events.push_back(f.done);
+    sv->flights.pop_front();
+  }
+  return k;
+}
+
+extern "C" {
+
+int vrt_server_create(VrtCtx* ctx, VrtSession* const* sessions, int n, int max_in_flight, VrtServer** out) {
+  if (!ctx || !sessions || n < 1 || !out || max_in_flight < 1 || max_in_flight > 8)
+    return fail(VRT_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  VrtServer* sv = new VrtServer();
+  sv->ctx = ctx;
+  sv->n = n;
+  sv->max_in_flight = max_in_flight;
+  sv->busy.assign((size_t)n, 0);
+  sv->t0 = std::chrono::steady_clock::now();
+  if (int r = vrt_batch_create(ctx, sessions, n, &sv->batch)) {
+    delete sv;
+    return r;
+  }
+  sv->batch->use_graph = false;
+  cudaError_t e = cudaEventCreate(&sv->ref);
+  if (e == cudaSuccess) e = cudaEventRecord(sv->ref, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(sv->ref);
+  if (e != cudaSuccess) {
+    vrt_batch_destroy(sv->batch);
+    delete sv;
+    return fail(VRT_ERR_CUDA, "server setup: %s", cudaGetErrorString(e));
+  }
+  sv->ref_host = sv->now();
+  *out = sv;
+  return VRT_OK;
+}
+
+int vrt_server_destroy(VrtServer* sv) {
+  if (!sv) return VRT_OK;
+  cudaSetDevice(sv->ctx->device);
+  cudaStreamSynchronize(sv->ctx->stream);
+  for (auto& f : sv->flights) cudaEventDestroy(f.done);
+  for (cudaEvent_t e : sv->spare_events) cudaEventDestroy(e);
+  if (sv->ref) cudaEventDestroy(sv->ref);
+  vrt_batch_destroy(sv->batch);
+  delete sv;
+  return VRT_OK;
+}
+
+double vrt_server_now(VrtServer* sv) { return sv ? sv->now() : 0.0; }
+
+int vrt_server_submit(VrtServer* sv, int session, const VrtUniforms* u, const VrtEditBox* edits, int n_edits,
+                      double t_arrival, void* ldr_out, uint64_t* ticket) {
+  if (!sv || !u || session < 0 || session >= sv->n || n_edits < 0 || (n_edits && !edits))
+    return fail(VRT_ERR_INVALID, "bad argument");
+  if (int r = check_uniforms(sv->batch->sessions[(size_t)session], u)) return r;
+  VrtServer::Req r;
+  r.ticket = sv->next_ticket++;
+  r.session = session;
+  r.u = *u;
+  r.edits.assign(edits, edits + n_edits);
+  r.t_arrival = t_arrival >= 0.0 ? t_arrival : sv->now();
+  r.ldr_out = ldr_out;
+  sv->pending.push_back(std::move(r));
+  if (ticket) *ticket = sv->pending.back().ticket;
+  return VRT_OK;
+}
+
+int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out) {
+  if (!sv || (max_out > 0 && !out) || !n_out) return fail(VRT_ERR_INVALID, "bad argument");
+  *n_out = 0;
+  if (int r = set_dev(sv->ctx)) return r;
+  int err = VRT_OK;
+  *n_out = server_retire(sv, out, max_out, false, &err);
+  if (err) return err;
+  while ((int)sv->flights.size() < sv->max_in_flight && !sv->pending.empty()) {
+    const size_t before = sv->flights.size();
+    if (int r = server_launch(sv)) return r;
+    if (sv->flights.size() == before) break;   // every pending request waits for a busy session
+  }
+  return VRT_OK;
+}
+
+int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out) {
+  if (!sv || (max_out > 0 && !out) || !n_out) return fail(VRT_ERR_INVALID, "bad argument");
+  *n_out = 0;
+  if (int r = set_dev(sv->ctx)) return r;
+  while (!sv->pending.empty() || !sv->flights.empty()) {
+    int k = 0;
+    if (int r = vrt_server_poll(sv, out + *n_out, max_out - *n_out, &k)) return r;
+    *n_out += k;
+    if (sv->flights.empty()) continue;
+    if ((int)sv->flights.front().reqs.size() > max_out - *n_out) break;   // caller's buffer is full
+    int err = VRT_OK;
+    VrtServer::Flight& f = sv->flights.front();
+    (void)f;
+    const int got = server_retire(sv, out + *n_out, max_out - *n_out, true, &err);
+    if (err) return err;
+    *n_out += got;
+  }
+  return VRT_OK;
+}
+
+int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight) {
+  if (!sv) return fail(VRT_ERR_INVALID, "server is NULL");
+  if (queued) *queued = (int)sv->pending.size();
+  if (in_flight) *in_flight = (int)sv->flights.size();
   return VRT_OK;
 }
 
