@@ -284,6 +284,12 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
 
+/* ---- radiance cache tensor-core diagnostics ----------------------------- */
+/* No counterpart in the reference.  Runs one tcgen05 GEMM on host data to check
+ * the shared-memory operand layouts: mode 0: D[128 x N] = A[128 x K] B[N x K]^T;
+ * mode 1: D[K x N] = A[128 x K]^T B[128 x N].  A, B are bf16 bit patterns. */
+int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint16_t* B, float* D);
+
 /* ---- allocation-free denoise ------------------------------------------- */
 /* No counterpart in the reference.  The 3-iteration a-trous chain (steps
  * 1, 2, 4) on caller-owned device buffers, for callers that cannot allocate

@@ -150,6 +150,7 @@ SIGNATURES = {
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
+    "vrt_mlp_selftest_gemm": (I, [I, I, I, P, P, P]),
     "vrt_server_create": (I, [P, C.POINTER(P), I, I, C.POINTER(P)]),
     "vrt_server_destroy": (I, [P]),
     "vrt_server_now": (C.c_double, [P]),

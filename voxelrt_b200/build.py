@@ -21,9 +21,9 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libvrt.so"
 
-CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_wavefront.cu", "k_noalloc.cu", "k_batch.cu"]
+CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_wavefront.cu", "k_noalloc.cu", "k_batch.cu", "k_mlp.cu"]
 CPP_SOURCES = ["vrt_api.cpp", "scene_gen.cpp"]
-HEADERS = ["vrt_device.cuh", "vrt_internal.h", "wavefront_core.cuh", "image_core.cuh"]
+HEADERS = ["vrt_device.cuh", "vrt_internal.h", "wavefront_core.cuh", "image_core.cuh", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP_CONTRACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
