@@ -52,6 +52,7 @@ typedef struct VrtScene VrtScene;
 typedef struct VrtSession VrtSession;
 typedef struct VrtBatch VrtBatch;
 typedef struct VrtServer VrtServer;
+typedef struct VrtMlp VrtMlp;
 
 /* Uniform block, byte-identical to the reference's 304-byte UBO
  * (common.wgsl:13-35, packed by main.js:399-426). */
@@ -283,6 +284,36 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 /* Blocks until every submitted request completed (or out[] is full). */
 int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
+
+/* ---- radiance cache MLP (no counterpart in the reference) --------------- */
+/* A 4-layer MLP (80 -> 64 -> 64 -> 64 -> 3, ReLU, no biases) mapping an
+ * encoded path vertex to outgoing radiance.  Input per query: 9 floats --
+ * position (metres), normal, albedo; the position is normalised by `extent`
+ * (the world size in metres) and encoded as sin/cos of 12 octaves per axis.
+ * BF16 weights and activations on the tensor cores (tcgen05, FP32
+ * accumulation in TMEM); FP32 master weights and Adam (b1 0.9, b2 0.99).
+ * Loss: relative L2, sum_c (o - y)^2 / (o^2 + 0.01), mean over samples.
+ * Parameters: row-major W_l [K_in x N_out] back to back, the output layer
+ * padded to 16 columns (columns 3..15 stay 0): vrt_mlp_num_params() floats. */
+int vrt_mlp_create(VrtCtx* ctx, uint32_t seed, VrtMlp** out);
+int vrt_mlp_destroy(VrtMlp* m);
+int vrt_mlp_num_params(void);
+int vrt_mlp_get_params(VrtMlp* m, float* host);
+/* Sets the FP32 master weights and resets the Adam state. */
+int vrt_mlp_set_params(VrtMlp* m, const float* host);
+/* Encoded inputs (n x 80 bf16 bit patterns). */
+int vrt_mlp_encode_device(VrtMlp* m, const float* d_q9, int n, float extent, uint16_t* d_feat);
+/* d_out3: n x 3 predicted radiance. */
+int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, float* d_out3);
+/* Gradient of the mean loss (d_grad: vrt_mlp_num_params() floats, may be NULL);
+ * *loss_out (may be NULL) receives the mean loss. */
+int vrt_mlp_gradient_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* d_grad,
+                            float* loss_out);
+/* `steps` Adam steps on the samples; *loss_out (may be NULL): loss before the first step. */
+int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float lr, int steps,
+                         float* loss_out);
+/* Reports a tensor-core wait that ran out in any earlier call (VRT_ERR_TIMEOUT). */
+int vrt_mlp_check(VrtMlp* m);
 
 /* ---- radiance cache tensor-core diagnostics ----------------------------- */
 /* No counterpart in the reference.  Runs one tcgen05 GEMM on host data to check

@@ -32,3 +32,140 @@ def test_umma_gemm_layouts(vrt, mode, K, N):
     rows = 128 if mode == 0 else K
     err = np.abs(D[:rows] - ref) / (np.abs(ref) + 1.0)
     assert err.max() < 1e-5, f"max err {err.max()}"
+
+
+EXTENT = 16.0
+
+
+def _queries(rng, n, extent=EXTENT):
+    q = np.zeros((n, 9), np.float32)
+    q[:, :3] = rng.uniform(-0.25 * extent, 1.25 * extent, size=(n, 3))   # outside the world too
+    nrm = rng.normal(size=(n, 3))
+    q[:, 3:6] = nrm / np.linalg.norm(nrm, axis=1, keepdims=True)
+    q[:, 6:9] = rng.uniform(0, 1, size=(n, 3))
+    y = (q[:, 6:9] * (0.6 + 0.4 * np.sin(q[:, :1] * 0.9) * np.cos(q[:, 2:3] * 0.5)) *
+         (1.0 + q[:, 4:5])).astype(np.float32)
+    return q, y
+
+
+def _cuda(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture
+def cache(vrt):
+    ctx = vrt.Context(0)
+    rc = vrt.RadianceCache(ctx, seed=7, extent=EXTENT)
+    yield rc
+    rc.close()
+    ctx.close()
+
+
+@pytest.mark.parametrize("n", [1, 127, 1000])
+def test_mlp_encode_bit_exact(vrt, orc, cache, n):
+    import torch
+    from oracle import mlp_ref as M
+    q, _ = _queries(np.random.default_rng(n), n)
+    feat = torch.zeros(n * 80, dtype=torch.int16, device="cuda")
+    cache.encode(_cuda(q), feat)
+    got = feat.cpu().numpy().view(np.uint16).reshape(n, 80)
+    want = M.bf16_bits(M.encode(q, EXTENT))
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("n", [1, 200, 5000])
+def test_mlp_infer_matches_oracle(vrt, orc, cache, n):
+    import torch
+    from oracle import mlp_ref as M
+    q, _ = _queries(np.random.default_rng(10 + n), n)
+    out = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    cache.infer(_cuda(q), out)
+    got = out.cpu().numpy().reshape(n, 3)
+    o, _, _ = M.forward(M.encode(q, EXTENT), cache.params())
+    ref = o[:, :3]
+    # fp32 tensor-core sums vs fp64 sums: outputs agree to 1e-5 of the output
+    # scale except where a hidden activation sits on a bf16 rounding boundary
+    # and rounds the other way (a relative step of 2^-8 in one activation):
+    # at most 1% of the outputs, each within 5e-3 of the scale
+    scale = max(np.abs(ref).max(), 1e-3)
+    err = np.abs(got - ref)
+    assert err.max() <= 5e-3 * scale, err.max()
+    assert np.mean(err > 1e-5 * scale) <= 0.01, np.mean(err > 1e-5 * scale)
+
+
+@pytest.mark.parametrize("n", [1, 3000, 148 * 128 * 2 + 77])
+def test_mlp_gradient_matches_oracle(vrt, orc, cache, n):
+    """Backward pass (dX by K-major MMAs, dW by MN-major MMAs accumulated in
+    TMEM over a CTA's tiles, fixed-order cross-CTA reduction) against the
+    restatement; the largest case gives every CTA two or three tiles."""
+    import torch
+    from oracle import mlp_ref as M
+    rng = np.random.default_rng(20 + n)
+    q, y = _queries(rng, n)
+    p = cache.params()
+    g = torch.zeros(M.N_PARAMS, dtype=torch.float32, device="cuda")
+    loss = cache.gradient(_cuda(q), _cuda(y), g)
+    got = g.cpu().numpy()
+    want_loss, want = M.gradient(M.encode(q, EXTENT), y, p)
+    assert abs(loss - want_loss) <= 1e-4 * abs(want_loss) + 1e-7, (loss, want_loss)
+    # per layer: |gpu - oracle| <= 2e-3 * max|oracle| + 1e-2 * |oracle|; the
+    # relative Frobenius error stays below 2e-3
+    off = 0
+    for k, m in M.SHAPES:
+        a, b = got[off:off + k * m], want[off:off + k * m]
+        scale = np.abs(b).max()
+        assert np.all(np.abs(a - b) <= 2e-3 * scale + 1e-2 * np.abs(b)), (k, m, np.abs(a - b).max(), scale)
+        off += k * m
+    assert np.linalg.norm(got - want) <= 2e-3 * np.linalg.norm(want)
+
+
+def test_mlp_gradient_deterministic(vrt, cache):
+    import torch
+    q, y = _queries(np.random.default_rng(5), 40000)
+    qd, yd = _cuda(q), _cuda(y)
+    g1 = torch.zeros(14336, dtype=torch.float32, device="cuda")
+    g2 = torch.zeros_like(g1)
+    l1 = cache.gradient(qd, yd, g1)
+    l2 = cache.gradient(qd, yd, g2)
+    assert l1 == l2
+    assert torch.equal(g1, g2)
+
+
+def test_mlp_adam_step_matches_oracle(vrt, orc, cache):
+    import torch
+    from oracle import mlp_ref as M
+    q, y = _queries(np.random.default_rng(6), 4096)
+    qd, yd = _cuda(q), _cuda(y)
+    w0 = cache.params()
+    cache.set_params(w0)                      # zero Adam state
+    m = np.zeros_like(w0)
+    v = np.zeros_like(w0)
+    w = w0
+    g = torch.zeros(M.N_PARAMS, dtype=torch.float32, device="cuda")
+    for step in (1, 2, 3):
+        cache.gradient(qd, yd, g)             # the gradient the next step uses
+        cache.train(qd, yd, lr=1e-3, steps=1)
+        w, m, v = M.adam(w, m, v, g.cpu().numpy(), step, 1e-3)
+        np.testing.assert_allclose(cache.params(), w, rtol=1e-5, atol=1e-7)
+
+
+def test_mlp_training_reduces_loss(vrt, cache):
+    q, y = _queries(np.random.default_rng(7), 16384)
+    qd, yd = _cuda(q), _cuda(y)
+    l0 = cache.train(qd, yd, lr=1e-2, steps=1)
+    for _ in range(6):
+        cache.train(qd, yd, lr=1e-2, steps=50)
+    l1 = cache.gradient(qd, yd)
+    assert np.isfinite(l1) and l1 < 0.2 * l0, (l0, l1)
+
+
+def test_mlp_rejects_bad_arguments(vrt, cache):
+    import torch
+    q = torch.zeros(9, dtype=torch.float32, device="cuda")
+    y = torch.zeros(3, dtype=torch.float32, device="cuda")
+    from voxelrt_b200._lib import lib
+    import ctypes as C
+    assert lib.vrt_mlp_train_device(cache.h, C.c_void_p(q.data_ptr()), C.c_void_p(y.data_ptr()), 0,
+                                    C.c_float(16.0), C.c_float(1e-3), 1, None) != 0
+    assert lib.vrt_mlp_infer_device(cache.h, C.c_void_p(q.data_ptr()), 1, C.c_float(0.0), C.c_void_p(y.data_ptr())) != 0

@@ -151,6 +151,16 @@ SIGNATURES = {
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
     "vrt_mlp_selftest_gemm": (I, [I, I, I, P, P, P]),
+    "vrt_mlp_create": (I, [P, U32, C.POINTER(P)]),
+    "vrt_mlp_destroy": (I, [P]),
+    "vrt_mlp_num_params": (I, []),
+    "vrt_mlp_get_params": (I, [P, P]),
+    "vrt_mlp_set_params": (I, [P, P]),
+    "vrt_mlp_encode_device": (I, [P, P, I, C.c_float, P]),
+    "vrt_mlp_infer_device": (I, [P, P, I, C.c_float, P]),
+    "vrt_mlp_gradient_device": (I, [P, P, P, I, C.c_float, P, C.POINTER(C.c_float)]),
+    "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
+    "vrt_mlp_check": (I, [P]),
     "vrt_server_create": (I, [P, C.POINTER(P), I, I, C.POINTER(P)]),
     "vrt_server_destroy": (I, [P]),
     "vrt_server_now": (C.c_double, [P]),

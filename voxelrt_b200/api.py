@@ -367,3 +367,81 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class RadianceCache:
+    """The radiance-cache MLP (vrt_mlp_*): BF16 tensor-core inference and
+    training on device buffers.  Device arrays are torch CUDA tensors
+    (contiguous float32; encoded features uint16/int16); each call orders
+    itself after the caller's CUDA work and finishes before it returns."""
+
+    N_PARAMS = 14336
+
+    def __init__(self, ctx: Context, seed: int = 1, extent: float = 16.0):
+        h = C.c_void_p()
+        check(lib.vrt_mlp_create(ctx.h, C.c_uint32(seed & 0xFFFFFFFF), C.byref(h)))
+        self.h, self.ctx, self.extent = h, ctx, float(extent)
+
+    @staticmethod
+    def _dp(t):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()):
+            raise ValueError("expected a contiguous CUDA tensor")
+        return C.c_void_p(t.data_ptr())
+
+    @staticmethod
+    def _sync():
+        import torch
+        torch.cuda.synchronize()
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.N_PARAMS, np.float32)
+        check(lib.vrt_mlp_get_params(self.h, ptr(out)))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        if p.size != self.N_PARAMS:
+            raise ValueError("wrong parameter count")
+        check(lib.vrt_mlp_set_params(self.h, ptr(p)))
+
+    def encode(self, q9, out) -> None:
+        self._sync()
+        check(lib.vrt_mlp_encode_device(self.h, self._dp(q9), q9.numel() // 9, C.c_float(self.extent), self._dp(out)))
+        self.ctx.synchronize()
+
+    def infer(self, q9, out3) -> None:
+        self._sync()
+        check(lib.vrt_mlp_infer_device(self.h, self._dp(q9), q9.numel() // 9, C.c_float(self.extent), self._dp(out3)))
+        self.ctx.synchronize()
+        check(lib.vrt_mlp_check(self.h))
+
+    def gradient(self, q9, y3, grad_out=None) -> float:
+        self._sync()
+        loss = C.c_float()
+        check(lib.vrt_mlp_gradient_device(self.h, self._dp(q9), self._dp(y3), q9.numel() // 9,
+                                          C.c_float(self.extent),
+                                          self._dp(grad_out) if grad_out is not None else None, C.byref(loss)))
+        self.ctx.synchronize()
+        return float(loss.value)
+
+    def train(self, q9, y3, lr: float = 1e-3, steps: int = 1) -> float:
+        """`steps` Adam steps; returns the loss before the first one."""
+        self._sync()
+        loss = C.c_float()
+        check(lib.vrt_mlp_train_device(self.h, self._dp(q9), self._dp(y3), q9.numel() // 9, C.c_float(self.extent),
+                                       C.c_float(lr), int(steps), C.byref(loss)))
+        self.ctx.synchronize()
+        check(lib.vrt_mlp_check(self.h))
+        return float(loss.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            check(lib.vrt_mlp_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

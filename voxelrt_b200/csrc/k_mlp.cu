@@ -7,7 +7,12 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "umma.cuh"
+#include "vrt_device.cuh"
 #include "vrt_internal.h"
+#include <cuda_bf16.h>
+#include <vector>
+#include <cmath>
+#include <algorithm>
 
 namespace vrt {
 
@@ -84,6 +89,422 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(int mode, int K, int N
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 64);
+}
+
+
+// ===========================================================================
+// The radiance-cache MLP: 80 -> 64 -> 64 -> 64 -> 3 (output padded to 16),
+// ReLU on the hidden layers, no biases (the encoding carries a constant 1).
+// Parameters: W_l row-major [K_in x N_out], fp32 masters + bf16 copy.
+// ===========================================================================
+namespace mlp {
+constexpr int kIn = 80, kHid = 64, kOutPad = 16, kOut = 3;
+constexpr int kL0 = kIn * kHid, kL1 = kHid * kHid, kL2 = kHid * kHid, kL3 = kHid * kOutPad;
+constexpr int kOff0 = 0, kOff1 = kL0, kOff2 = kL0 + kL1, kOff3 = kL0 + kL1 + kL2;
+constexpr int kParams = kL0 + kL1 + kL2 + kL3;   // 14336
+constexpr int kFreqs = 12;
+
+// shared-memory plan of the training kernel (bytes)
+constexpr int kWf0 = 0, kWf1 = kWf0 + kHid * kIn * 2, kWf2 = kWf1 + kHid * kHid * 2, kWf3 = kWf2 + kHid * kHid * 2;
+constexpr int kWb1 = kWf3 + kOutPad * kHid * 2, kWb2 = kWb1 + kHid * kHid * 2, kWb3 = kWb2 + kHid * kHid * 2;
+constexpr int kA0 = kWb3 + kHid * kOutPad * 2, kA1 = kA0 + 128 * kIn * 2, kA2 = kA1 + 128 * kHid * 2;
+constexpr int kA3 = kA2 + 128 * kHid * 2, kDY = kA3 + 128 * kHid * 2, kEnd = kDY + 128 * kHid * 2;
+constexpr int kTrainSmem = kEnd + 4096;   // slack: MN-major views read up to 1 KB past a buffer
+// inference kernel: forward weights + two activation buffers
+constexpr int kIA0 = kWb1, kIA1 = kIA0 + 128 * kIn * 2, kIEnd = kIA1 + 128 * kIn * 2;
+constexpr int kInferSmem = kIEnd + 4096;
+
+// TMEM columns (fp32) of the training kernel
+constexpr uint32_t kTFwd = 0, kTDx = 64, kTW0 = 128, kTW1 = 192, kTW2 = 256, kTW3 = 320;
+
+__device__ __forceinline__ uint16_t f2bf(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+
+// Input encoding of one query: position (metres) normalised by the world
+// extent, 12 octaves of sin/cos(2^f * pi * p) per axis, normal, albedo, 1, 0.
+__device__ __forceinline__ void encode(const float* q, float extent, float* f) {
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float p = q[a] / extent;
+    float scale = 0.5f;
+#pragma unroll
+    for (int k = 0; k < kFreqs; k++) {
+      const float x = p * scale;
+      const float t = x - floorf(x);
+      float sn, cs;
+      sincos_(kTwoPi * t, sn, cs);
+      f[6 * k + a] = sn;
+      f[6 * k + 3 + a] = cs;
+      scale = scale * 2.0f;
+    }
+  }
+  f[72] = q[3]; f[73] = q[4]; f[74] = q[5];
+  f[75] = q[6]; f[76] = q[7]; f[77] = q[8];
+  f[78] = 1.0f; f[79] = 0.0f;
+}
+
+// Loads bf16 weights (row-major [K_in x N_out]) into the canonical smem
+// layouts: forward B = W^T (rows N_out, K = K_in); backward B = W (rows K_in,
+// K = N_out).
+__device__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w, bool backward) {
+  for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
+    int l, kin, nout, off;
+    if (i < kOff1) { l = 0; kin = kIn; nout = kHid; off = kOff0; }
+    else if (i < kOff2) { l = 1; kin = kHid; nout = kHid; off = kOff1; }
+    else if (i < kOff3) { l = 2; kin = kHid; nout = kHid; off = kOff2; }
+    else { l = 3; kin = kHid; nout = kOutPad; off = kOff3; }
+    const int k = (i - off) / nout, n = (i - off) % nout;
+    const uint16_t v = w[i];
+    const int fbase = l == 0 ? kWf0 : (l == 1 ? kWf1 : (l == 2 ? kWf2 : kWf3));
+    *reinterpret_cast<uint16_t*>(smem + fbase + umma::canon_off(n, k, kin)) = v;
+    if (backward && l > 0) {
+      const int bbase = l == 1 ? kWb1 : (l == 2 ? kWb2 : kWb3);
+      *reinterpret_cast<uint16_t*>(smem + bbase + umma::canon_off(k, n, nout)) = v;
+    }
+  }
+}
+
+struct Ctl {
+  uint64_t* mbar;
+  uint32_t phase;
+  bool ok;
+};
+
+// One elected thread issues `nk` K-steps of D = A * B (both K-major).
+__device__ __forceinline__ void issue_fwd(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, bool acc0) {
+  const uint32_t id = umma::idesc_bf16(128, N, false, false);
+  for (int ks = 0; ks < K / 16; ks++)
+    umma::mma_bf16(tmem, umma::desc_kmajor(a + 256u * ks, K), umma::desc_kmajor(b + 256u * ks, K), id,
+                   (acc0 || ks > 0) ? 1u : 0u);
+}
+
+// dW[K_in x N] (+)= X^T Y over the 128 samples of the tile (MN-major views).
+__device__ __forceinline__ void issue_dw(uint32_t tmem, uint32_t x, int Cx, uint32_t y, int N, bool acc0) {
+  const uint32_t id = umma::idesc_bf16(128, N, true, true);
+  for (int ks = 0; ks < 128 / 16; ks++)
+    umma::mma_bf16(tmem, umma::desc_mnmajor(x + 32u * Cx * ks, Cx), umma::desc_mnmajor(y + 32u * N * ks, N), id,
+                   (acc0 || ks > 0) ? 1u : 0u);
+}
+
+// All threads: commit (thread 0) and wait for the MMAs, bounded.
+__device__ __forceinline__ void sync_mma(Ctl& c) {
+  if (threadIdx.x == 0) umma::commit(c.mbar);
+  const bool ok = umma::mbar_wait(c.mbar, c.phase, kMbarSpin);
+  c.phase ^= 1u;
+  c.ok = __syncthreads_and(ok ? 1 : 0) && c.ok;
+  umma::fence_after_sync();
+}
+
+// Thread-to-smem handoff before the tensor core reads what threads wrote.
+__device__ __forceinline__ void publish() {
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+}
+
+// Reads `n` fp32 columns [col, col+n) of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_row(uint32_t tbase, uint32_t col, int n, float* out) {
+  const uint32_t lane = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
+  for (int c0 = 0; c0 < n; c0 += 16) {
+    float v[16];
+    umma::tmem_ld16(tbase + lane + col + (uint32_t)c0, v);
+#pragma unroll
+    for (int j = 0; j < 16; j++) out[c0 + j] = v[j];
+  }
+}
+
+// Forward of the tile: activations written to A1..A3 (bf16), output o[16].
+// Returns ReLU masks of the three hidden layers.
+__device__ void forward_tile(uint8_t* smem, uint32_t tbase, Ctl& c, int a_in, int a1, int a2, int a3, float* o,
+                             uint64_t* mask) {
+  const uint32_t s0 = umma::smem_u32(smem);
+  const int ain[3] = {a_in, a1, a2};
+  const int aout[3] = {a1, a2, a3};
+  const int wf[3] = {kWf0, kWf1, kWf2};
+  const int t = threadIdx.x;
+  for (int l = 0; l < 3; l++) {
+    const int K = l == 0 ? kIn : kHid;
+    if (t == 0) issue_fwd(tbase + kTFwd, s0 + ain[l], s0 + wf[l], K, kHid, false);
+    sync_mma(c);
+    float h[kHid];
+    tmem_row(tbase, kTFwd, kHid, h);
+    uint64_t m = 0;
+#pragma unroll
+    for (int j = 0; j < kHid; j++) {
+      const float v = h[j] > 0.0f ? h[j] : 0.0f;
+      if (h[j] > 0.0f) m |= 1ull << j;
+      *reinterpret_cast<uint16_t*>(smem + aout[l] + umma::canon_off(t, j, kHid)) = f2bf(v);
+    }
+    mask[l] = m;
+    publish();
+  }
+  if (t == 0) issue_fwd(tbase + kTFwd, s0 + a3, s0 + kWf3, kHid, kOutPad, false);
+  sync_mma(c);
+  tmem_row(tbase, kTFwd, kOutPad, o);
+}
+
+// Writes the encoded input of sample `q` (or zeros) into row t of A0.
+__device__ __forceinline__ void stage_input(uint8_t* smem, int a0, const float* __restrict__ q9, int n, int idx,
+                                            float extent) {
+  float f[kIn];
+  if (idx < n) {
+    float q[9];
+#pragma unroll
+    for (int j = 0; j < 9; j++) q[j] = q9[(size_t)idx * 9 + j];
+    encode(q, extent, f);
+  } else {
+#pragma unroll
+    for (int j = 0; j < kIn; j++) f[j] = 0.0f;
+  }
+#pragma unroll
+  for (int j = 0; j < kIn; j++)
+    *reinterpret_cast<uint16_t*>(smem + a0 + umma::canon_off(threadIdx.x, j, kIn)) = f2bf(f[j]);
+}
+
+}  // namespace mlp
+
+// Encoded inputs as bf16 (for checking against the CPU restatement).
+__global__ void k_mlp_encode(const float* __restrict__ q9, int n, float extent, uint16_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float q[9], f[mlp::kIn];
+  for (int j = 0; j < 9; j++) q[j] = q9[(size_t)i * 9 + j];
+  mlp::encode(q, extent, f);
+  for (int j = 0; j < mlp::kIn; j++) out[(size_t)i * mlp::kIn + j] = mlp::f2bf(f[j]);
+}
+
+// Inference: out[i*3 + c] = MLP(encode(q_i)).
+__global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ w, const float* __restrict__ q9,
+                                                   int n, float extent, float* __restrict__ out,
+                                                   int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
+  if (t == 0) umma::mbar_init(&mbar, 1);
+  mlp::load_weights(smem, w, false);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = tmem_base;
+  mlp::Ctl c{&mbar, 0u, true};
+  const int tiles = (n + 127) / 128;
+  for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
+    const int idx = tile * 128 + t;
+    mlp::stage_input(smem, mlp::kIA0, q9, n, idx, extent);
+    mlp::publish();
+    float o[mlp::kOutPad];
+    uint64_t mask[3];
+    // activations ping-pong between the two buffers (A1 = IA1, A2 = IA0, A3 = IA1)
+    mlp::forward_tile(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, o, mask);
+    if (c.ok && idx < n)
+      for (int j = 0; j < mlp::kOut; j++) out[(size_t)idx * 3 + j] = o[j];
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
+  if (!c.ok && t == 0) atomicExch(err, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tbase, 64);
+}
+
+// One gradient pass over n samples: per-CTA partial dW (sum over the CTA's
+// tiles) of the relative L2 loss sum_c (o_c - y_c)^2 / (o_c^2 + 0.01), the
+// denominator held constant (not differentiated).
+__global__ void __launch_bounds__(128, 1) k_mlp_grad(const uint16_t* __restrict__ w, const float* __restrict__ q9,
+                                                     const float* __restrict__ y3, int n, float extent,
+                                                     float* __restrict__ partial, float* __restrict__ loss,
+                                                     int* __restrict__ err) {
+  using namespace mlp;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  __shared__ float s_loss[4];
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 512);
+  if (t == 0) umma::mbar_init(&mbar, 1);
+  load_weights(smem, w, true);
+  for (int i = t; i < (kTrainSmem - kEnd) / 4; i += 128) reinterpret_cast<uint32_t*>(smem + kEnd)[i] = 0u;
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = tmem_base;
+  const uint32_t s0 = umma::smem_u32(smem);
+  Ctl c{&mbar, 0u, true};
+  float lsum = 0.0f;
+  const int tiles = (n + 127) / 128;
+  bool first = true;
+  for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
+    const int idx = tile * 128 + t;
+    stage_input(smem, kA0, q9, n, idx, extent);
+    publish();
+    float o[kOutPad];
+    uint64_t mask[3];
+    forward_tile(smem, tbase, c, kA0, kA1, kA2, kA3, o, mask);
+    // loss gradient dL/do (rows of padding samples are zero)
+#pragma unroll
+    for (int j = 0; j < kOutPad; j++) {
+      float g = 0.0f;
+      if (idx < n && j < kOut) {
+        const float d = o[j] - y3[(size_t)idx * 3 + j];
+        const float den = o[j] * o[j] + 0.01f;
+        g = 2.0f * d / den;
+        lsum += d * d / den;
+      }
+      *reinterpret_cast<uint16_t*>(smem + kDY + umma::canon_off(t, j, kOutPad)) = f2bf(g);
+    }
+    publish();
+    // layer 3: dW3 += A3^T dO ; dX3 = dO W3^T
+    if (t == 0) {
+      issue_dw(tbase + kTW3, s0 + kA3, kHid, s0 + kDY, kOutPad, !first);
+      issue_fwd(tbase + kTDx, s0 + kDY, s0 + kWb3, kOutPad, kHid, false);
+    }
+    sync_mma(c);
+    const int abuf[3] = {kA1, kA2, kA3};
+    const int wb[3] = {kWb1, kWb2, kWb3};
+    const uint32_t tw[3] = {kTW0, kTW1, kTW2};
+    for (int l = 2; l >= 0; l--) {
+      // dH_{l+1} = dX_{l+1} * relu'(h_{l+1}) -> dY buffer (K-major rows = samples, C = 64)
+      float dx[kHid];
+      tmem_row(tbase, kTDx, kHid, dx);
+#pragma unroll
+      for (int j = 0; j < kHid; j++) {
+        const float g = ((mask[l] >> j) & 1ull) ? dx[j] : 0.0f;
+        *reinterpret_cast<uint16_t*>(smem + kDY + umma::canon_off(t, j, kHid)) = f2bf(g);
+      }
+      publish();
+      if (t == 0) {
+        // dW_l += A_l^T dH_{l+1}   (A_0 has 80 columns)
+        const int ain = l == 0 ? kA0 : abuf[l - 1];
+        issue_dw(tbase + tw[l], s0 + ain, l == 0 ? kIn : kHid, s0 + kDY, kHid, !first);
+        if (l > 0) issue_fwd(tbase + kTDx, s0 + kDY, s0 + wb[l - 1], kHid, kHid, false);
+      }
+      sync_mma(c);
+    }
+    first = false;
+  }
+  // partial gradients of this CTA: lane = input feature row, columns = outputs
+  float* pc = partial + (size_t)blockIdx.x * kParams;
+  if (c.ok) {
+    const int kin[4] = {kIn, kHid, kHid, kHid};
+    const int nout[4] = {kHid, kHid, kHid, kOutPad};
+    const int off[4] = {kOff0, kOff1, kOff2, kOff3};
+    const uint32_t tw[4] = {kTW0, kTW1, kTW2, kTW3};
+    for (int l = 0; l < 4; l++) {
+      float row[kHid];
+      tmem_row(tbase, tw[l], nout[l], row);
+      if (t < kin[l])
+        for (int j = 0; j < nout[l]; j++) pc[off[l] + t * nout[l] + j] = first ? 0.0f : row[j];
+    }
+  }
+  // loss of this CTA
+  for (int o2 = 16; o2 > 0; o2 >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o2);
+  if ((t & 31) == 0) s_loss[warp] = lsum;
+  __syncthreads();
+  if (t == 0) {
+    loss[blockIdx.x] = (s_loss[0] + s_loss[1]) + (s_loss[2] + s_loss[3]);
+    if (!c.ok) atomicExch(err, 1);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tbase, 512);
+}
+
+// grad[i] = sum over CTAs of partial[cta][i] / n  (fixed order: deterministic)
+__global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, float inv_n, float* __restrict__ grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= mlp::kParams) return;
+  float s = 0.0f;
+  for (int c = 0; c < ctas; c++) s += partial[(size_t)c * mlp::kParams + i];
+  grad[i] = s * inv_n;
+}
+
+// Adam on fp32 masters; writes the bf16 copy.  Output columns >= 3 stay 0.
+__global__ void k_mlp_adam(float* __restrict__ wm, float* __restrict__ m, float* __restrict__ v,
+                           const float* __restrict__ grad, uint16_t* __restrict__ wb, float lr, float b1, float b2,
+                           float eps, float bc1, float bc2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= mlp::kParams) return;
+  if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) { wm[i] = 0.0f; wb[i] = 0; return; }
+  const float g = grad[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * g;
+  const float vi = b2 * v[i] + (1.0f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / bc1, vh = vi / bc2;
+  const float w = wm[i] - lr * mh / (sqrtf(vh) + eps);
+  wm[i] = w;
+  wb[i] = mlp::f2bf(w);
+}
+
+__global__ void k_mlp_to_bf16(const float* __restrict__ wm, uint16_t* __restrict__ wb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < mlp::kParams) wb[i] = mlp::f2bf(wm[i]);
+}
+
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+// ---------------------------------------------------------------------------
+int mlp_num_params() { return mlp::kParams; }
+
+static int sm_count_mlp() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 1;
+}
+
+int mlp_max_ctas() { return sm_count_mlp(); }
+
+cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_mlp_encode<<<(n + 127) / 128, 128, 0, st>>>(q9, n, extent, out);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, float extent, float* out, int* err,
+                      cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kInferSmem);
+  if (e != cudaSuccess) return e;
+  const int tiles = (n + 127) / 128;
+  const int grid = std::min(tiles, sm_count_mlp() * 2);
+  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(wb, q9, n, extent, out, err);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, float extent, float* partial,
+                         float* loss_ctas, int* err, float* grad, int* ctas_used, cudaStream_t st) {
+  if (n <= 0) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
+  if (e != cudaSuccess) return e;
+  const int tiles = (n + 127) / 128;
+  const int grid = std::min(tiles, sm_count_mlp());
+  k_mlp_grad<<<grid, 128, mlp::kTrainSmem, st>>>(wb, q9, y3, n, extent, partial, loss_ctas, err);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, 1.0f / (float)n, grad);
+  if (ctas_used) *ctas_used = grid;
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
+                     cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
+  const float bc1 = 1.0f - std::pow(b1, (float)step), bc2 = 1.0f - std::pow(b2, (float)step);
+  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, bc1, bc2);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st) {
+  k_mlp_to_bf16<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, wb);
+  return cudaGetLastError();
 }
 
 }  // namespace vrt

@@ -14,6 +14,7 @@
 #include <mutex>
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <deque>
 #include "vrt_internal.h"
 
@@ -1248,6 +1249,200 @@ int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight) {
   if (queued) *queued = (int)sv->pending.size();
   if (in_flight) *in_flight = (int)sv->flights.size();
   return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// radiance-cache MLP
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct VrtMlp {
+  VrtCtx* ctx = nullptr;
+  uint64_t bytes = 0;
+  float* wm = nullptr;      // fp32 masters
+  float* m = nullptr;       // Adam first moment
+  float* v = nullptr;       // Adam second moment
+  float* grad = nullptr;
+  uint16_t* wb = nullptr;   // bf16 copy read by the kernels
+  float* partial = nullptr; // per-CTA gradient partials
+  float* loss = nullptr;    // per-CTA loss sums
+  int* err = nullptr;
+  int step = 0;
+  int P = 0, ctas = 0;
+};
+
+// He-normal initial weights from a PCG-hash stream (Box-Muller).
+static void mlp_init_host(std::vector<float>& w, uint32_t seed) {
+  const int P = mlp_num_params();
+  w.assign((size_t)P, 0.0f);
+  auto h = [](uint32_t v) {
+    v = v * 747796405u + 2891336453u;
+    uint32_t x = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+    return (x >> 22u) ^ x;
+  };
+  const int kin[4] = {80, 64, 64, 64}, nout[4] = {64, 64, 64, 16};
+  int off = 0;
+  uint32_t s = h(seed ^ 0x5eed1234u);
+  for (int l = 0; l < 4; l++) {
+    const double std_ = std::sqrt(2.0 / kin[l]);
+    for (int k = 0; k < kin[l]; k++)
+      for (int n = 0; n < nout[l]; n++) {
+        s = h(s);
+        const double u1 = ((double)s + 1.0) / 4294967297.0;
+        s = h(s);
+        const double u2 = (double)s / 4294967296.0;
+        double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2) * std_;
+        if (l == 3) z = n < 3 ? z * 0.1 : 0.0;
+        w[(size_t)off + (size_t)k * nout[l] + n] = (float)z;
+      }
+    off += kin[l] * nout[l];
+  }
+}
+
+extern "C" {
+
+int vrt_mlp_num_params(void) { return mlp_num_params(); }
+
+int vrt_mlp_destroy(VrtMlp* m) {
+  if (!m) return VRT_OK;
+  VrtCtx* c = m->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  const size_t P = (size_t)m->P;
+  dev_free(c, m->wm, P * 4, &m->bytes);
+  dev_free(c, m->m, P * 4, &m->bytes);
+  dev_free(c, m->v, P * 4, &m->bytes);
+  dev_free(c, m->grad, P * 4, &m->bytes);
+  dev_free(c, m->wb, P * 2, &m->bytes);
+  dev_free(c, m->partial, P * 4 * (size_t)m->ctas, &m->bytes);
+  dev_free(c, m->loss, (size_t)m->ctas * 4, &m->bytes);
+  dev_free(c, m->err, 16, &m->bytes);
+  delete m;
+  return VRT_OK;
+}
+
+int vrt_mlp_set_params(VrtMlp* m, const float* host) {
+  if (!m || !host) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(m->ctx)) return r;
+  cudaStream_t st = m->ctx->stream;
+  const size_t P = (size_t)m->P;
+  CUDA_TRY(cudaMemcpyAsync(m->wm, host, P * 4, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(m->m, 0, P * 4, st));
+  CUDA_TRY(cudaMemsetAsync(m->v, 0, P * 4, st));
+  CUDA_TRY(mlp_to_bf16(m->wm, m->wb, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  m->step = 0;
+  return VRT_OK;
+}
+
+int vrt_mlp_get_params(VrtMlp* m, float* host) {
+  if (!m || !host) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(m->ctx)) return r;
+  CUDA_TRY(cudaMemcpyAsync(host, m->wm, (size_t)m->P * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(m->ctx->stream));
+  return VRT_OK;
+}
+
+int vrt_mlp_create(VrtCtx* ctx, uint32_t seed, VrtMlp** out) {
+  if (!ctx || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (int r = set_dev(ctx)) return r;
+  VrtMlp* m = new VrtMlp();
+  m->ctx = ctx;
+  m->P = mlp_num_params();
+  m->ctas = mlp_max_ctas();
+  const size_t P = (size_t)m->P;
+  int r = dev_alloc(ctx, (void**)&m->wm, P * 4, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->m, P * 4, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->v, P * 4, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->grad, P * 4, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->wb, P * 2, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->partial, P * 4 * (size_t)m->ctas, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->loss, (size_t)m->ctas * 4, &m->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&m->err, 16, &m->bytes);
+  if (!r && cudaMemset(m->err, 0, 16) != cudaSuccess) r = fail(VRT_ERR_CUDA, "memset");
+  if (!r) {
+    std::vector<float> w;
+    mlp_init_host(w, seed);
+    r = vrt_mlp_set_params(m, w.data());
+  }
+  if (r) {
+    std::string keep = g_err;
+    vrt_mlp_destroy(m);
+    g_err = keep;
+    return r;
+  }
+  *out = m;
+  return VRT_OK;
+}
+
+static int mlp_check_err(VrtMlp* m) {
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, m->err, 4, cudaMemcpyDeviceToHost, m->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(m->ctx->stream));
+  if (h) {
+    cudaMemsetAsync(m->err, 0, 4, m->ctx->stream);
+    return fail(VRT_ERR_TIMEOUT, "radiance cache: a tensor-core completion wait ran out");
+  }
+  return VRT_OK;
+}
+
+int vrt_mlp_encode_device(VrtMlp* m, const float* d_q9, int n, float extent, uint16_t* d_feat) {
+  if (!m || n < 0 || (n && (!d_q9 || !d_feat)) || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
+  if (int r = set_dev(m->ctx)) return r;
+  CUDA_TRY(mlp_encode(d_q9, n, extent, d_feat, m->ctx->stream));
+  return VRT_OK;
+}
+
+int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, float* d_out3) {
+  if (!m || n < 0 || (n && (!d_q9 || !d_out3)) || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
+  if (int r = set_dev(m->ctx)) return r;
+  CUDA_TRY(mlp_infer(m->wb, d_q9, n, extent, d_out3, m->err, m->ctx->stream));
+  return VRT_OK;
+}
+
+static int mlp_grad_impl(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* loss_out) {
+  int ctas = 0;
+  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, extent, m->partial, m->loss, m->err, m->grad, &ctas,
+                        m->ctx->stream));
+  if (loss_out) {
+    std::vector<float> l((size_t)ctas);
+    CUDA_TRY(cudaMemcpyAsync(l.data(), m->loss, (size_t)ctas * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
+    if (int r = mlp_check_err(m)) return r;
+    double s = 0.0;
+    for (float x : l) s += x;
+    *loss_out = (float)(s / (double)n);
+  }
+  return VRT_OK;
+}
+
+int vrt_mlp_gradient_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* d_grad,
+                            float* loss_out) {
+  if (!m || n < 1 || !d_q9 || !d_y3 || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
+  if (int r = set_dev(m->ctx)) return r;
+  if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, loss_out)) return r;
+  if (d_grad)
+    CUDA_TRY(cudaMemcpyAsync(d_grad, m->grad, (size_t)m->P * 4, cudaMemcpyDeviceToDevice, m->ctx->stream));
+  return mlp_check_err(m);
+}
+
+int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float lr, int steps,
+                         float* loss_out) {
+  if (!m || n < 1 || !d_q9 || !d_y3 || !(extent > 0.0f) || steps < 1 || !(lr > 0.0f))
+    return fail(VRT_ERR_INVALID, "bad argument");
+  if (int r = set_dev(m->ctx)) return r;
+  for (int i = 0; i < steps; i++) {
+    if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, (loss_out && i == 0) ? loss_out : nullptr)) return r;
+    m->step++;
+    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step, m->ctx->stream));
+  }
+  return VRT_OK;
+}
+
+int vrt_mlp_check(VrtMlp* m) {
+  if (!m) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(m->ctx)) return r;
+  return mlp_check_err(m);
 }
 
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev) {

@@ -81,6 +81,19 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
                                cudaStream_t st, uint32_t* launches);
 
+// Radiance-cache MLP kernels (k_mlp.cu).  q9: n x 9 floats (position in
+// metres, normal, albedo); y3: n x 3 target radiance; weights bf16 row-major.
+int mlp_num_params();
+int mlp_max_ctas();
+cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cudaStream_t st);
+cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, float extent, float* out, int* err,
+                      cudaStream_t st);
+cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, float extent, float* partial,
+                         float* loss_ctas, int* err, float* grad, int* ctas_used, cudaStream_t st);
+cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
+                     cudaStream_t st);
+cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st);
+
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
