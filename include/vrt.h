@@ -125,6 +125,10 @@ typedef struct VrtFrameStats {
   uint32_t launches;          /* kernels launched by the frame                 */
   uint32_t trace_launches;    /* wavefront trace launches timed in ms_trace    */
   float ms_trace;             /* summed duration of those trace launches       */
+  uint32_t cache_on;          /* 1: the frame was cache-assisted               */
+  uint64_t cache_queries;     /* paths that ended in a cache query             */
+  uint64_t cache_samples;     /* training samples produced by training paths   */
+  float ms_cache;             /* cache inference + resolve + training steps    */
   uint32_t pad;
 } VrtFrameStats;
 
@@ -315,10 +319,41 @@ int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n,
 /* Reports a tensor-core wait that ran out in any earlier call (VRT_ERR_TIMEOUT). */
 int vrt_mlp_check(VrtMlp* m);
 
+/* ---- cache-assisted path tracing (no counterpart in the reference) ------- */
+/* With the cache enabled a session's path-trace pass works as follows:
+ *  - one pixel of every 4x4 block (rotating with the frame index) traces a
+ *    full training path of `train_bounces` bounces (the plain estimator);
+ *    its vertices 0..train_vertices-1 become training samples
+ *    (position, normal, albedo -> reflected radiance gathered after it);
+ *  - every other path ends at its first bounce hit: emission is picked up
+ *    there and the reflected radiance is the network's prediction;
+ *  - after the waves: one inference over the queries, then `train_steps`
+ *    Adam steps of `train_batch` samples drawn from this frame's samples.
+ * The uniforms' bounce count is ignored while the cache is on.  Wavefront
+ * sessions only. */
+typedef struct VrtCacheConfig {
+  int enabled;
+  int train_bounces;          /* default 6                                     */
+  int train_vertices;         /* 1..8, default 3                               */
+  int train_batch;            /* samples per Adam step, default 65536          */
+  int train_steps;            /* Adam steps per frame, default 1               */
+  float learning_rate;        /* default 1e-2                                  */
+  uint32_t seed;              /* initial weights                               */
+  int pad;
+} VrtCacheConfig;
+int vrt_session_set_cache(VrtSession* s, const VrtCacheConfig* cfg);
+/* The session's network (owned by the session; NULL before the cache was enabled). */
+int vrt_session_cache_mlp(VrtSession* s, VrtMlp** out);
+/* Training samples of the last cache-assisted frame (in production order):
+ * up to `cap` rows of q9 (position, normal, albedo) and y3 (target);
+ * *count receives the number produced. */
+int vrt_session_read_cache_samples(VrtSession* s, float* q9, float* y3, int cap, int* count);
+
 /* ---- radiance cache tensor-core diagnostics ----------------------------- */
 /* No counterpart in the reference.  Runs one tcgen05 GEMM on host data to check
  * the shared-memory operand layouts: mode 0: D[128 x N] = A[128 x K] B[N x K]^T;
- * mode 1: D[K x N] = A[128 x K]^T B[128 x N].  A, B are bf16 bit patterns. */
+ * mode 1: D[K x N] = A[128 x K]^T B[128 x N]; mode 2: D[128 x N] = A[128 x K] B[K x N]
+ * (B read MN-major).  A, B are bf16 bit patterns. */
 int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint16_t* B, float* D);
 
 /* ---- allocation-free denoise ------------------------------------------- */

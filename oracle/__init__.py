@@ -181,6 +181,21 @@ def math_eval(fn: int, x: np.ndarray) -> np.ndarray:
     return y
 
 
+CACHE_PIX_DTYPE = np.dtype([("role", "<i4"), ("has_query", "<i4"), ("nrec", "<i4"), ("pad", "<i4"),
+                            ("den", "<f4", 3), ("radiance", "<f4", 3), ("tp1", "<f4", 3), ("q9", "<f4", 9),
+                            ("rec", "<f4", (8, 15))])
+
+
+def cache_paths(vox, bricks, masks, n, ubytes, w, h, phase: int, train_bounces: int, rec_vertices: int):
+    """Per-pixel cache-assisted estimator parts (CACHE_PIX_DTYPE, h x w)."""
+    assert lib().orc_cache_pix_bytes() == CACHE_PIX_DTYPE.itemsize
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    out = np.zeros(h * w, CACHE_PIX_DTYPE)
+    lib().orc_cache_paths(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_int(w), C.c_int(h),
+                          C.c_uint32(phase), C.c_uint32(train_bounces), C.c_int(rec_vertices), _p(out))
+    return out.reshape(h, w)
+
+
 def pcg_hash(v: int) -> int:
     f = lib().orc_pcg_hash
     f.restype = C.c_uint32

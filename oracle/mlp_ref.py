@@ -7,10 +7,12 @@ kernels in voxelrt_b200/csrc/k_mlp.cu compute, so that tests can check them:
 
 * input encoding of a query (position in metres, normal, albedo): the
   position divided by the world extent, then for 12 octaves k and each axis
-  sin/cos(2*pi * frac(p * 0.5 * 2^k)), followed by normal, albedo, 1, 0
-  (80 features), rounded to bf16.  sin/cos are the project's own sincos
-  (om_sincos in vrt_oracle.cpp, the same code the kernels run), so the
-  features are bit-exact;
+  sin/cos(2*pi * 2^k * frac(p / 2)), followed by normal, albedo, 1, 0
+  (80 features), rounded to bf16.  Octave 0 uses the project's own sincos
+  (om_sincos in vrt_oracle.cpp, the same code the kernels run); octave k+1
+  follows from octave k by sin 2a = (sin a cos a) * 2 and
+  cos 2a = (cos a - sin a)(cos a + sin a) in fp32, as the kernels evaluate
+  them, so the features are bit-exact;
 * 80 -> 64 -> 64 -> 64 -> 3 ReLU network without biases; weights and hidden
   activations bf16, sums in fp32 (fp64 here);
 * loss: mean over samples of sum_c (o_c - y_c)^2 / (o_c^2 + 0.01), the
@@ -73,15 +75,16 @@ def encode(q9: np.ndarray, extent: float) -> np.ndarray:
     q = np.ascontiguousarray(q9, np.float32).reshape(-1, 9)
     n = q.shape[0]
     f = np.zeros((n, N_IN), np.float32)
-    p = q[:, :3] / np.float32(extent)
-    scale = np.float32(0.5)
+    x = (q[:, :3] / np.float32(extent)) * np.float32(0.5)
+    t = x - np.floor(x)
+    arg = (TWO_PI_F32 * t).astype(np.float32)
+    sn = math_eval(0, arg.ravel()).reshape(n, 3)
+    cs = math_eval(1, arg.ravel()).reshape(n, 3)
     for k in range(N_FREQS):
-        x = p * scale
-        t = x - np.floor(x)
-        arg = (TWO_PI_F32 * t).astype(np.float32)
-        f[:, 6 * k:6 * k + 3] = math_eval(0, arg.ravel()).reshape(n, 3)
-        f[:, 6 * k + 3:6 * k + 6] = math_eval(1, arg.ravel()).reshape(n, 3)
-        scale = np.float32(scale * 2)
+        f[:, 6 * k:6 * k + 3] = sn
+        f[:, 6 * k + 3:6 * k + 6] = cs
+        # octave k+1 by the double-angle identities, in the kernels' fp32 order
+        sn, cs = (sn * cs) * np.float32(2.0), (cs - sn) * (cs + sn)
     f[:, 72:78] = q[:, 3:9]
     f[:, 78] = 1.0
     return bf16_round(f)

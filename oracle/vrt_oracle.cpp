@@ -532,6 +532,91 @@ void path_pixel(const World& W, const Uni& u, float fclamp, uint32_t gx, uint32_
   rad_out[0] = demod.x; rad_out[1] = demod.y; rad_out[2] = demod.z; rad_out[3] = 1.0f;
 }
 
+// The cache-assisted estimator (voxelrt_b200/csrc/wavefront_core.cuh), per
+// pixel.  No counterpart in the reference: the path is the plain one above
+// with two roles.  Training pixels -- (x & 3, y & 3) == (phase & 3,
+// phase >> 2) -- trace `train_bounces` bounces and record their vertices
+// 0..rec_vertices-1 after the emission pickup (position, normal, albedo,
+// radiance so far, throughput); every other path stops at its first bounce
+// hit after the emission pickup there, leaving the reflected radiance to the
+// network (query = position, normal, albedo; throughput tp1).
+struct OrcCachePix {
+  int32_t role;        // 0: primary miss, 1: training path, 2: cache-terminated path
+  int32_t has_query;   // role 2: the bounce ray hit a surface
+  int32_t nrec;        // role 1: vertices recorded
+  int32_t pad;
+  float den[3];        // max(albedo of vertex 0, 1e-3)
+  float radiance[3];   // role 1: final radiance before the clamp; role 2: before the cache term
+  float tp1[3];        // role 2: throughput reaching vertex 1
+  float q9[9];         // role 2: the query
+  float rec[8][15];    // role 1: position, normal, albedo, radiance, throughput
+};
+
+void cache_pixel(const World& W, const Uni& u, uint32_t gx, uint32_t gy, uint32_t dimx, uint32_t dimy,
+                 uint32_t phase, uint32_t train_bounces, int rec_vertices, OrcCachePix& o) {
+  std::memset(&o, 0, sizeof o);
+  Rng rng = init_rng(gx, gy, u.params0[0]);
+  float jx = rng.next() - 0.5f;
+  float jy = rng.next() - 0.5f;
+  float uvx = (((float)gx + 0.5f) + jx) / (float)dimx;
+  float uvy = (((float)gy + 0.5f) + jy) / (float)dimy;
+  f3 ro = mk(u.camPos[0], u.camPos[1], u.camPos[2]);
+  f3 rd = camera_ray(u, uvx, uvy);
+  Hit h0 = trace(W, ro, rd, 1e4f);
+  if (h0.t < 0.0f) return;
+  const bool train = (gx & 3u) == (phase & 3u) && (gy & 3u) == (phase >> 2);
+  o.role = train ? 1 : 2;
+  Mat mat1 = unpack_material(h0.mat);
+  f3 den = max3(mat1.albedo, mk(1e-3f, 1e-3f, 1e-3f));
+  o.den[0] = den.x; o.den[1] = den.y; o.den[2] = den.z;
+  f3 radiance = mk(0, 0, 0);
+  f3 tp = mk(1, 1, 1);
+  f3 pos = add(ro, muls(rd, h0.t)), n = h0.n;
+  Mat mat = mat1;
+  const uint32_t nB = train ? train_bounces : 1u;
+  f3 sunRad = mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
+  for (uint32_t bounce = 0; bounce <= nB; bounce++) {
+    if (mat.emissive > 0.0f) radiance = add(radiance, muls(mul(tp, mat.albedo), mat.emissive * EMISSIVE_SCALE));
+    if (!train && bounce == 1u) {
+      o.has_query = 1;
+      const float q[9] = {pos.x, pos.y, pos.z, n.x, n.y, n.z, mat.albedo.x, mat.albedo.y, mat.albedo.z};
+      std::memcpy(o.q9, q, sizeof q);
+      o.tp1[0] = tp.x; o.tp1[1] = tp.y; o.tp1[2] = tp.z;
+      break;
+    }
+    if (train && (int)bounce < rec_vertices) {
+      const float r[15] = {pos.x, pos.y, pos.z, n.x, n.y, n.z, mat.albedo.x, mat.albedo.y, mat.albedo.z,
+                           radiance.x, radiance.y, radiance.z, tp.x, tp.y, tp.z};
+      std::memcpy(o.rec[bounce], r, sizeof r);
+      o.nrec = (int)bounce + 1;
+    }
+    f3 surf = add(pos, muls(n, 1e-3f));
+    f3 l = sample_sun_dir(u, rng);
+    float ndl = dot3(n, l);
+    if (ndl > 0.0f && l.y > 0.0f) {
+      Hit hs = trace(W, surf, l, 1e4f);
+      if (!(hs.t >= 0.0f)) radiance = add(radiance, mul(muls(muls(mul(tp, mat.albedo), INV_PI), ndl), sunRad));
+    }
+    if (bounce == nB) break;
+    rd = cosine_hemisphere(n, rng);
+    tp = mul(tp, mat.albedo);
+    if (bounce >= 2u) {
+      float p = clampf(fmaxf_(tp.x, fmaxf_(tp.y, tp.z)), 0.05f, 0.95f);
+      if (rng.next() > p) break;
+      tp = mk(tp.x / p, tp.y / p, tp.z / p);
+    }
+    Hit h = trace(W, surf, rd, 1e4f);
+    if (h.t < 0.0f) {
+      radiance = add(radiance, mul(tp, sky_color(u, rd, false)));
+      break;
+    }
+    pos = add(surf, muls(rd, h.t));
+    n = h.n;
+    mat = unpack_material(h.mat);
+  }
+  o.radiance[0] = radiance.x; o.radiance[1] = radiance.y; o.radiance[2] = radiance.z;
+}
+
 // Bilinear fetch with WebGPU's linear filter conventions: texel centres at
 // +0.5, clamp-to-edge addressing (default sampler, main.js:317).
 template <typename Fetch>
@@ -943,6 +1028,21 @@ void orc_math_eval(int fn, const float* x, float* y, int n) {
 }
 
 uint32_t orc_pcg_hash(uint32_t v) { return pcg_hash(v); }
+
+// Cache-assisted estimator of every pixel (OrcCachePix per pixel, row-major).
+int orc_cache_pix_bytes(void) { return (int)sizeof(OrcCachePix); }
+
+void orc_cache_paths(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                     const void* uniforms, int Wd, int Hd, uint32_t phase, uint32_t train_bounces,
+                     int rec_vertices, OrcCachePix* out) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int y = 0; y < Hd; y++)
+    for (int x = 0; x < Wd; x++)
+      cache_pixel(W, u, (uint32_t)x, (uint32_t)y, (uint32_t)Wd, (uint32_t)Hd, phase, train_bounces, rec_vertices,
+                  out[(size_t)y * Wd + x]);
+}
 
 // Runs the path of rows [row0,row1) step row_step and returns every ray it
 // traced as 7 floats (origin xyz and maxT in voxel units, unit direction).

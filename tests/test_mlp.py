@@ -17,19 +17,20 @@ def from_bf16(b):
 
 
 @pytest.mark.parametrize("mode,K,N", [(0, 16, 16), (0, 64, 64), (0, 80, 64), (0, 64, 16), (0, 128, 32),
-                                      (1, 64, 64), (1, 80, 64), (1, 64, 16), (1, 128, 16)])
+                                      (1, 64, 64), (1, 80, 64), (1, 64, 16), (1, 128, 16),
+                                      (2, 16, 64), (2, 64, 64), (2, 128, 32)])
 def test_umma_gemm_layouts(vrt, mode, K, N):
     import ctypes as C
     rng = np.random.default_rng(K * 7 + N + mode)
     A = to_bf16(rng.normal(size=(128, K)))
-    B = to_bf16(rng.normal(size=(N, K) if mode == 0 else (128, N)))
+    B = to_bf16(rng.normal(size={0: (N, K), 1: (128, N), 2: (K, N)}[mode]))
     D = np.zeros((128, N), np.float32)
     code = vrt.lib.vrt_mlp_selftest_gemm(mode, K, N, C.c_void_p(A.ctypes.data), C.c_void_p(B.ctypes.data),
                                          C.c_void_p(D.ctypes.data))
     assert code == 0, vrt.lib.vrt_last_error_string().decode()
     a, b = from_bf16(A).astype(np.float64), from_bf16(B).astype(np.float64)
-    ref = a @ b.T if mode == 0 else a.T @ b
-    rows = 128 if mode == 0 else K
+    ref = {0: lambda: a @ b.T, 1: lambda: a.T @ b, 2: lambda: a @ b}[mode]()
+    rows = K if mode == 1 else 128
     err = np.abs(D[:rows] - ref) / (np.abs(ref) + 1.0)
     assert err.max() < 1e-5, f"max err {err.max()}"
 

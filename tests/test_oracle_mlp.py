@@ -36,9 +36,13 @@ def test_encode_layout(orc):
     np.testing.assert_array_equal(f[:, 78], 1.0)
     np.testing.assert_array_equal(f[:, 79], 0.0)
     np.testing.assert_array_equal(f[:, 72:78], M.bf16_round(q[:, 3:9]))
-    # octave 0, axis 0: sin(2 pi frac(p / extent * 0.5))
-    ref = np.sin(2 * np.pi * ((q[:, 0] / 16.0 * 0.5) % 1.0))
-    assert np.max(np.abs(f[:, 0] - ref)) < 8e-3
+    # octave k, axis 0: sin(2 pi 2^k frac(p / extent * 0.5)); the double-angle
+    # recurrence stays within the bf16 step of the exact value
+    for k in range(12):
+        ref = np.sin(2 * np.pi * 2.0 ** k * ((q[:, 0] / 16.0 * 0.5) % 1.0))
+        assert np.max(np.abs(f[:, 6 * k] - ref)) < 8e-3, k
+        ref = np.cos(2 * np.pi * 2.0 ** k * ((q[:, 0] / 16.0 * 0.5) % 1.0))
+        assert np.max(np.abs(f[:, 6 * k + 3] - ref)) < 8e-3, k
 
 
 def test_bf16_round_ties_to_even():

@@ -88,7 +88,14 @@ class VrtFrameStats(C.Structure):
                 ("voxel_reads", C.c_uint64), ("pixels", C.c_uint64), ("ms_pathtrace", C.c_float),
                 ("ms_temporal", C.c_float), ("ms_atrous", C.c_float), ("ms_present", C.c_float),
                 ("ms_total", C.c_float), ("launches", C.c_uint32), ("trace_launches", C.c_uint32),
-                ("ms_trace", C.c_float), ("pad", C.c_uint32)]
+                ("ms_trace", C.c_float), ("cache_on", C.c_uint32), ("cache_queries", C.c_uint64),
+                ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("pad", C.c_uint32)]
+
+
+class VrtCacheConfig(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("train_bounces", C.c_int), ("train_vertices", C.c_int),
+                ("train_batch", C.c_int), ("train_steps", C.c_int), ("learning_rate", C.c_float),
+                ("seed", C.c_uint32), ("pad", C.c_int)]
 
 
 class VrtCameraPose(C.Structure):
@@ -161,6 +168,9 @@ SIGNATURES = {
     "vrt_mlp_gradient_device": (I, [P, P, P, I, C.c_float, P, C.POINTER(C.c_float)]),
     "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
     "vrt_mlp_check": (I, [P]),
+    "vrt_session_set_cache": (I, [P, P]),
+    "vrt_session_cache_mlp": (I, [P, C.POINTER(P)]),
+    "vrt_session_read_cache_samples": (I, [P, P, P, I, C.POINTER(I)]),
     "vrt_server_create": (I, [P, C.POINTER(P), I, I, C.POINTER(P)]),
     "vrt_server_destroy": (I, [P]),
     "vrt_server_now": (C.c_double, [P]),

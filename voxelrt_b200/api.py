@@ -13,7 +13,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtCompletion,
-                   VrtDeviceConfig, VrtEditBox, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
+                   VrtCacheConfig, VrtDeviceConfig, VrtEditBox, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
                    check, lib, ptr)
 
 # Reference constants (scene.js:5-6, common.wgsl:11)
@@ -222,6 +222,42 @@ class Session:
         t = VrtTuning()
         check(lib.vrt_session_get_tuning(self.h, C.byref(t)))
         return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant)
+
+    def set_cache(self, enabled: bool = True, train_bounces: int = 6, train_vertices: int = 3,
+                  train_batch: int = 65536, train_steps: int = 1, learning_rate: float = 1e-2, seed: int = 1) -> None:
+        """Cache-assisted path tracing (vrt_session_set_cache)."""
+        cfg = VrtCacheConfig(int(bool(enabled)), int(train_bounces), int(train_vertices), int(train_batch),
+                             int(train_steps), float(learning_rate), int(seed) & 0xFFFFFFFF, 0)
+        check(lib.vrt_session_set_cache(self.h, C.byref(cfg)))
+
+    def cache_params(self) -> np.ndarray:
+        """FP32 master weights of the session's cache network."""
+        m = C.c_void_p()
+        check(lib.vrt_session_cache_mlp(self.h, C.byref(m)))
+        if not m.value:
+            raise RuntimeError("the cache was never enabled on this session")
+        out = np.zeros(RadianceCache.N_PARAMS, np.float32)
+        check(lib.vrt_mlp_get_params(m, ptr(out)))
+        return out
+
+    def set_cache_params(self, p: np.ndarray) -> None:
+        m = C.c_void_p()
+        check(lib.vrt_session_cache_mlp(self.h, C.byref(m)))
+        if not m.value:
+            raise RuntimeError("the cache was never enabled on this session")
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib.vrt_mlp_set_params(m, ptr(p)))
+
+    def cache_samples(self, cap: int | None = None):
+        """(q9 [n x 9], y3 [n x 3], produced) of the last cache-assisted frame."""
+        if cap is None:
+            cap = ((self.w + 3) // 4) * ((self.h_px + 3) // 4) * 8
+        q = np.zeros((cap, 9), np.float32)
+        y = np.zeros((cap, 3), np.float32)
+        n = C.c_int()
+        check(lib.vrt_session_read_cache_samples(self.h, ptr(q), ptr(y), int(cap), C.byref(n)))
+        k = min(n.value, cap)
+        return q[:k], y[:k], n.value
 
     def set_timing(self, on: bool) -> None:
         check(lib.vrt_session_set_timing(self.h, int(bool(on))))

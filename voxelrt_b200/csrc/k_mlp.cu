@@ -32,14 +32,19 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(int mode, int K, int N
   uint8_t* sB = smem + 36 * 1024;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
   if (tid == 0) umma::mbar_init(&mbar, 1);
-  if (mode == 0) {
+  if (mode == 0 || mode == 2) {
     for (int i = tid; i < 128 * K; i += 128) {
       const int r = i / K, c = i % K;
       *reinterpret_cast<uint16_t*>(sA + umma::canon_off(r, c, K)) = A[i];
     }
     for (int i = tid; i < N * K; i += 128) {
-      const int r = i / K, c = i % K;
-      *reinterpret_cast<uint16_t*>(sB + umma::canon_off(r, c, K)) = B[i];
+      if (mode == 0) {
+        const int r = i / K, c = i % K;
+        *reinterpret_cast<uint16_t*>(sB + umma::canon_off(r, c, K)) = B[i];
+      } else {   // B given as [K x N], rows = K: read MN-major
+        const int r = i / N, c = i % N;
+        *reinterpret_cast<uint16_t*>(sB + umma::canon_off(r, c, N)) = B[i];
+      }
     }
   } else {
     const int C = K;   // X has C columns
@@ -64,6 +69,11 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(int mode, int K, int N
       for (int ks = 0; ks < K / 16; ks++)
         umma::mma_bf16(tbase, umma::desc_kmajor(a0 + 256u * ks, K), umma::desc_kmajor(b0 + 256u * ks, K), id,
                        ks > 0 ? 1u : 0u);
+    } else if (mode == 2) {
+      const uint32_t id = umma::idesc_bf16(128, N, false, true);
+      for (int ks = 0; ks < K / 16; ks++)
+        umma::mma_bf16(tbase, umma::desc_kmajor(a0 + 256u * ks, K), umma::desc_mnmajor(b0 + 32u * N * ks, N), id,
+                       ks > 0 ? 1u : 0u);
     } else {
       const int C = K;
       const uint32_t id = umma::idesc_bf16(128, N, true, true);
@@ -76,7 +86,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(int mode, int K, int N
   const bool ok = __syncthreads_and(umma::mbar_wait(&mbar, 0, kMbarSpin) ? 1 : 0);
   umma::fence_after_sync();
   if (ok) {
-    const int rows = mode == 0 ? 128 : K;
+    const int rows = mode == 1 ? K : 128;
     for (int c0 = 0; c0 < N; c0 += 16) {
       float v[16];
       umma::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
@@ -104,18 +114,22 @@ constexpr int kOff0 = 0, kOff1 = kL0, kOff2 = kL0 + kL1, kOff3 = kL0 + kL1 + kL2
 constexpr int kParams = kL0 + kL1 + kL2 + kL3;   // 14336
 constexpr int kFreqs = 12;
 
-// shared-memory plan of the training kernel (bytes)
+// forward weight copies (bytes): W_l^T as [N_out rows x K_in columns], K-major
 constexpr int kWf0 = 0, kWf1 = kWf0 + kHid * kIn * 2, kWf2 = kWf1 + kHid * kHid * 2, kWf3 = kWf2 + kHid * kHid * 2;
-constexpr int kWb1 = kWf3 + kOutPad * kHid * 2, kWb2 = kWb1 + kHid * kHid * 2, kWb3 = kWb2 + kHid * kHid * 2;
-constexpr int kA0 = kWb3 + kHid * kOutPad * 2, kA1 = kA0 + 128 * kIn * 2, kA2 = kA1 + 128 * kHid * 2;
-constexpr int kA3 = kA2 + 128 * kHid * 2, kDY = kA3 + 128 * kHid * 2, kEnd = kDY + 128 * kHid * 2;
-constexpr int kTrainSmem = kEnd + 4096;   // slack: MN-major views read up to 1 KB past a buffer
+constexpr int kWEnd = kWf3 + kOutPad * kHid * 2;   // 28 KB
+// training kernel: two groups of 128 samples (threads 0-127, 128-255), each
+// with its own input, activation and gradient tiles
+constexpr int kGA0 = 0, kGA1 = kGA0 + 128 * kIn * 2, kGA2 = kGA1 + 128 * kHid * 2, kGA3 = kGA2 + 128 * kHid * 2;
+constexpr int kGDY = kGA3 + 128 * kHid * 2, kGStride = kGDY + 128 * kHid * 2;   // 84 KB per group
+constexpr int kGBase = kWEnd, kGEnd = kGBase + 2 * kGStride;
+constexpr int kTrainSmem = kGEnd + 1024;   // slack: MN-major views read up to 1 KB past a tile
 // inference kernel: forward weights + two activation buffers
-constexpr int kIA0 = kWb1, kIA1 = kIA0 + 128 * kIn * 2, kIEnd = kIA1 + 128 * kIn * 2;
+constexpr int kIA0 = kWEnd, kIA1 = kIA0 + 128 * kIn * 2, kIEnd = kIA1 + 128 * kIn * 2;
 constexpr int kInferSmem = kIEnd + 4096;
 
-// TMEM columns (fp32) of the training kernel
-constexpr uint32_t kTFwd = 0, kTDx = 64, kTW0 = 128, kTW1 = 192, kTW2 = 256, kTW3 = 320;
+// TMEM columns (fp32): layer outputs / input gradients of group g at 64 g,
+// weight gradients accumulated over all of a CTA's samples at kTW*
+constexpr uint32_t kTFwd = 0, kTW0 = 128, kTW1 = 192, kTW2 = 256, kTW3 = 320;
 
 __device__ __forceinline__ uint16_t f2bf(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
@@ -123,21 +137,27 @@ __device__ __forceinline__ uint16_t f2bf(float x) {
 __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 
 // Input encoding of one query: position (metres) normalised by the world
-// extent, 12 octaves of sin/cos(2^f * pi * p) per axis, normal, albedo, 1, 0.
+// extent, then per axis sin/cos(2 pi 2^k frac(p / 2)) for octaves k = 0..11,
+// followed by normal, albedo, 1, 0.  Only octave 0 calls sincos_; each
+// higher octave follows by the double-angle identities
+//   sin 2a = 2 sin a cos a,  cos 2a = (cos a - sin a)(cos a + sin a),
+// which keeps the per-query cost at 3 sincos_ calls (the rounding error
+// doubles per octave: ~2e-4 at octave 11, far below the bf16 step).
 __device__ __forceinline__ void encode(const float* q, float extent, float* f) {
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    const float p = q[a] / extent;
-    float scale = 0.5f;
+    const float x = (q[a] / extent) * 0.5f;
+    const float t = x - floorf(x);
+    float sn, cs;
+    sincos_(kTwoPi * t, sn, cs);
 #pragma unroll
     for (int k = 0; k < kFreqs; k++) {
-      const float x = p * scale;
-      const float t = x - floorf(x);
-      float sn, cs;
-      sincos_(kTwoPi * t, sn, cs);
       f[6 * k + a] = sn;
       f[6 * k + 3 + a] = cs;
-      scale = scale * 2.0f;
+      const float s2 = (sn * cs) * 2.0f;
+      const float c2 = (cs - sn) * (cs + sn);
+      sn = s2;
+      cs = c2;
     }
   }
   f[72] = q[3]; f[73] = q[4]; f[74] = q[5];
@@ -145,10 +165,30 @@ __device__ __forceinline__ void encode(const float* q, float extent, float* f) {
   f[78] = 1.0f; f[79] = 0.0f;
 }
 
+// Packs 8 floats as bf16 (RNE) into one 16-byte chunk, element 0 lowest.
+__device__ __forceinline__ uint4 pack8(const float* v) {
+  uint4 r;
+  uint32_t* w = &r.x;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t*>(&h);
+  }
+  return r;
+}
+
+// Row `row` of a row-chunked tile with C columns from C floats (16-byte stores).
+__device__ __forceinline__ void store_row(uint8_t* tile, int row, int C, const float* v) {
+#pragma unroll
+  for (int cg = 0; cg < C / 8; cg++)
+    *reinterpret_cast<uint4*>(tile + umma::canon_off(row, 8 * cg, C)) = pack8(v + 8 * cg);
+}
+
 // Loads bf16 weights (row-major [K_in x N_out]) into the canonical smem
-// layouts: forward B = W^T (rows N_out, K = K_in); backward B = W (rows K_in,
-// K = N_out).
-__device__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w, bool backward) {
+// layout W^T: rows N_out, columns K_in.  Read K-major it is the B operand of
+// the forward GEMMs; read MN-major it is the B operand W of the input-gradient
+// GEMMs dX = dH W^T.
+__device__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w) {
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
     int l, kin, nout, off;
     if (i < kOff1) { l = 0; kin = kIn; nout = kHid; off = kOff0; }
@@ -156,13 +196,8 @@ __device__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w, bool
     else if (i < kOff3) { l = 2; kin = kHid; nout = kHid; off = kOff2; }
     else { l = 3; kin = kHid; nout = kOutPad; off = kOff3; }
     const int k = (i - off) / nout, n = (i - off) % nout;
-    const uint16_t v = w[i];
     const int fbase = l == 0 ? kWf0 : (l == 1 ? kWf1 : (l == 2 ? kWf2 : kWf3));
-    *reinterpret_cast<uint16_t*>(smem + fbase + umma::canon_off(n, k, kin)) = v;
-    if (backward && l > 0) {
-      const int bbase = l == 1 ? kWb1 : (l == 2 ? kWb2 : kWb3);
-      *reinterpret_cast<uint16_t*>(smem + bbase + umma::canon_off(k, n, nout)) = v;
-    }
+    *reinterpret_cast<uint16_t*>(smem + fbase + umma::canon_off(n, k, kin)) = w[i];
   }
 }
 
@@ -188,6 +223,15 @@ __device__ __forceinline__ void issue_dw(uint32_t tmem, uint32_t x, int Cx, uint
                    (acc0 || ks > 0) ? 1u : 0u);
 }
 
+// dX[128 x N] = dH[128 x K] * W^T from the forward weight copy read MN-major
+// (W^T stored with rows K = N_out and columns N = K_in).
+__device__ __forceinline__ void issue_dx(uint32_t tmem, uint32_t a, int K, uint32_t w, int N) {
+  const uint32_t id = umma::idesc_bf16(128, N, false, true);
+  for (int ks = 0; ks < K / 16; ks++)
+    umma::mma_bf16(tmem, umma::desc_kmajor(a + 256u * ks, K), umma::desc_mnmajor(w + 32u * N * ks, N), id,
+                   ks > 0 ? 1u : 0u);
+}
+
 // All threads: commit (thread 0) and wait for the MMAs, bounded.
 __device__ __forceinline__ void sync_mma(Ctl& c) {
   if (threadIdx.x == 0) umma::commit(c.mbar);
@@ -205,63 +249,89 @@ __device__ __forceinline__ void publish() {
   umma::fence_after_sync();
 }
 
-// Reads `n` fp32 columns [col, col+n) of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_row(uint32_t tbase, uint32_t col, int n, float* out) {
-  const uint32_t lane = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
-  for (int c0 = 0; c0 < n; c0 += 16) {
-    float v[16];
-    umma::tmem_ld16(tbase + lane + col + (uint32_t)c0, v);
+// Reads `n` (16 or 64) fp32 columns [col, col+n) of this thread's TMEM lane:
+// all loads issued, then one wait.
+template <int n>
+__device__ __forceinline__ void tmem_row(uint32_t tbase, uint32_t col, float* out) {
+  const uint32_t lane = (uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16;   // warp w: lanes 32 (w % 4) ..
+  uint32_t r[n];
 #pragma unroll
-    for (int j = 0; j < 16; j++) out[c0 + j] = v[j];
-  }
+  for (int c0 = 0; c0 < n; c0 += 16) umma::tmem_ld16_raw(tbase + lane + col + (uint32_t)c0, r + c0);
+#pragma unroll
+  for (int c0 = 0; c0 < n; c0 += 16) umma::tmem_wait_dep(r + c0);
+#pragma unroll
+  for (int i = 0; i < n; i++) out[i] = __uint_as_float(r[i]);
 }
 
-// Forward of the tile: activations written to A1..A3 (bf16), output o[16].
-// Returns ReLU masks of the three hidden layers.
-__device__ void forward_tile(uint8_t* smem, uint32_t tbase, Ctl& c, int a_in, int a1, int a2, int a3, float* o,
-                             uint64_t* mask) {
+// Forward of G tiles of 128 samples (thread t: group t / 128, row t % 128):
+// activations written to A1..A3 (bf16) of the thread's group (group g's
+// tiles at +g * gstride), output o[16].  Returns the three hidden layers'
+// ReLU masks.  Thread 0 issues every group's MMAs.
+template <int G>
+__device__ __forceinline__ void forward_tile(uint8_t* smem, uint32_t tbase, Ctl& c, int a_in, int a1, int a2, int a3,
+                                             int gstride, float* o, uint64_t* mask) {
   const uint32_t s0 = umma::smem_u32(smem);
   const int ain[3] = {a_in, a1, a2};
   const int aout[3] = {a1, a2, a3};
   const int wf[3] = {kWf0, kWf1, kWf2};
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, g = t >> 7, r = t & 127;
+  const uint32_t tcol = kTFwd + 64u * (uint32_t)g;
+#pragma unroll
   for (int l = 0; l < 3; l++) {
     const int K = l == 0 ? kIn : kHid;
-    if (t == 0) issue_fwd(tbase + kTFwd, s0 + ain[l], s0 + wf[l], K, kHid, false);
+    if (t == 0)
+      for (int q = 0; q < G; q++)
+        issue_fwd(tbase + kTFwd + 64u * q, s0 + ain[l] + q * gstride, s0 + wf[l], K, kHid, false);
     sync_mma(c);
     float h[kHid];
-    tmem_row(tbase, kTFwd, kHid, h);
+    tmem_row<kHid>(tbase, tcol, h);
     uint64_t m = 0;
 #pragma unroll
     for (int j = 0; j < kHid; j++) {
-      const float v = h[j] > 0.0f ? h[j] : 0.0f;
       if (h[j] > 0.0f) m |= 1ull << j;
-      *reinterpret_cast<uint16_t*>(smem + aout[l] + umma::canon_off(t, j, kHid)) = f2bf(v);
+      else h[j] = 0.0f;
     }
+    store_row(smem + aout[l] + g * gstride, r, kHid, h);
     mask[l] = m;
     publish();
   }
-  if (t == 0) issue_fwd(tbase + kTFwd, s0 + a3, s0 + kWf3, kHid, kOutPad, false);
+  if (t == 0)
+    for (int q = 0; q < G; q++) issue_fwd(tbase + kTFwd + 64u * q, s0 + a3 + q * gstride, s0 + kWf3, kHid, kOutPad, false);
   sync_mma(c);
-  tmem_row(tbase, kTFwd, kOutPad, o);
+  tmem_row<kOutPad>(tbase, tcol, o);
 }
 
-// Writes the encoded input of sample `q` (or zeros) into row t of A0.
-__device__ __forceinline__ void stage_input(uint8_t* smem, int a0, const float* __restrict__ q9, int n, int idx,
-                                            float extent) {
+// Writes the encoded input of sample `src` (zeros when idx >= n) into row
+// `row` of the input tile.
+__device__ __forceinline__ void stage_input(uint8_t* tile, int row, const float* __restrict__ q9, int n, int idx,
+                                            float extent, int src) {
   float f[kIn];
   if (idx < n) {
     float q[9];
 #pragma unroll
-    for (int j = 0; j < 9; j++) q[j] = q9[(size_t)idx * 9 + j];
+    for (int j = 0; j < 9; j++) q[j] = q9[(size_t)src * 9 + j];
     encode(q, extent, f);
   } else {
 #pragma unroll
     for (int j = 0; j < kIn; j++) f[j] = 0.0f;
   }
-#pragma unroll
-  for (int j = 0; j < kIn; j++)
-    *reinterpret_cast<uint16_t*>(smem + a0 + umma::canon_off(threadIdx.x, j, kIn)) = f2bf(f[j]);
+  store_row(tile, row, kIn, f);
+}
+
+// Source index of training sample idx: in order when the population fits the
+// step, else a uniform draw (with replacement) from the population.
+__device__ __forceinline__ int sample_source(int idx, int pop, bool draw, uint32_t seed) {
+  if (!draw) return idx;
+  const uint32_t h = pcg_hash(seed ^ pcg_hash((uint32_t)idx * 2654435761u + 0x9e3779b9u));
+  return (int)(((uint64_t)h * (uint64_t)(uint32_t)pop) >> 32);
+}
+
+// (samples used by a step, population, draw?) for the selection rule of mlp_gradient.
+__device__ __forceinline__ void sample_counts(int n, const int* n_dev, int pop_cap, int& nn, int& pop, bool& draw) {
+  if (!n_dev) { nn = n; pop = n; draw = false; return; }
+  pop = min(max(*n_dev, 0), pop_cap);
+  nn = min(pop, n);
+  draw = pop > n;
 }
 
 }  // namespace mlp
@@ -278,15 +348,16 @@ __global__ void k_mlp_encode(const float* __restrict__ q9, int n, float extent, 
 
 // Inference: out[i*3 + c] = MLP(encode(q_i)).
 __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ w, const float* __restrict__ q9,
-                                                   int n, float extent, float* __restrict__ out,
-                                                   int* __restrict__ err) {
+                                                   int n, const int* __restrict__ n_dev, float extent,
+                                                   float* __restrict__ out, int* __restrict__ err) {
+  if (n_dev) n = min(*n_dev, n);
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
   if (t == 0) umma::mbar_init(&mbar, 1);
-  mlp::load_weights(smem, w, false);
+  mlp::load_weights(smem, w);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
@@ -295,12 +366,12 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ 
   const int tiles = (n + 127) / 128;
   for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
     const int idx = tile * 128 + t;
-    mlp::stage_input(smem, mlp::kIA0, q9, n, idx, extent);
+    mlp::stage_input(smem + mlp::kIA0, t, q9, n, idx, extent, idx);
     mlp::publish();
     float o[mlp::kOutPad];
     uint64_t mask[3];
     // activations ping-pong between the two buffers (A1 = IA1, A2 = IA0, A3 = IA1)
-    mlp::forward_tile(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, o, mask);
+    mlp::forward_tile<1>(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, 0, o, mask);
     if (c.ok && idx < n)
       for (int j = 0; j < mlp::kOut; j++) out[(size_t)idx * 3 + j] = o[j];
     umma::fence_before_sync();
@@ -313,93 +384,114 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ 
   if (warp == 0) umma::tmem_free(tbase, 64);
 }
 
-// One gradient pass over n samples: per-CTA partial dW (sum over the CTA's
-// tiles) of the relative L2 loss sum_c (o_c - y_c)^2 / (o_c^2 + 0.01), the
-// denominator held constant (not differentiated).
-__global__ void __launch_bounds__(128, 1) k_mlp_grad(const uint16_t* __restrict__ w, const float* __restrict__ q9,
-                                                     const float* __restrict__ y3, int n, float extent,
-                                                     float* __restrict__ partial, float* __restrict__ loss,
-                                                     int* __restrict__ err) {
+// One gradient pass: per-CTA partial dW (sum over the CTA's samples) of the
+// relative L2 loss sum_c (o_c - y_c)^2 / (o_c^2 + 0.01), the denominator held
+// constant (not differentiated).  256 threads work on 256 samples per
+// iteration as two groups of 128; thread 0 issues all MMAs, so the weight
+// gradients of both groups accumulate in order into the same TMEM columns.
+// Input gradients dX = dH W^T read the forward weight copy MN-major; weight
+// gradients dW = X^T dH read the activation tiles MN-major (no transposes).
+__global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict__ w, const float* __restrict__ q9,
+                                                     const float* __restrict__ y3, int n_req,
+                                                     const int* __restrict__ n_dev, int pop_cap, uint32_t seed,
+                                                     float extent, float* __restrict__ partial,
+                                                     float* __restrict__ loss, int* __restrict__ err) {
   using namespace mlp;
+  int n, pop;
+  bool draw;
+  sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
-  __shared__ float s_loss[4];
-  const int t = threadIdx.x, warp = t >> 5;
+  __shared__ float s_loss[8];
+  const int t = threadIdx.x, warp = t >> 5, g = t >> 7, r = t & 127;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 512);
   if (t == 0) umma::mbar_init(&mbar, 1);
-  load_weights(smem, w, true);
-  for (int i = t; i < (kTrainSmem - kEnd) / 4; i += 128) reinterpret_cast<uint32_t*>(smem + kEnd)[i] = 0u;
+  load_weights(smem, w);
+  for (int i = t; i < (kTrainSmem - kGEnd) / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(smem + kGEnd)[i] = 0u;
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   const uint32_t s0 = umma::smem_u32(smem);
+  const uint32_t gs = (uint32_t)kGStride;
+  uint8_t* mine = smem + kGBase + g * kGStride;   // this thread's group tiles
   Ctl c{&mbar, 0u, true};
   float lsum = 0.0f;
-  const int tiles = (n + 127) / 128;
+  const int tiles = (n + 255) / 256;
   bool first = true;
   for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
-    const int idx = tile * 128 + t;
-    stage_input(smem, kA0, q9, n, idx, extent);
+    const int idx = tile * 256 + t;
+    const int src = idx < n ? sample_source(idx, pop, draw, seed) : 0;
+    stage_input(mine + kGA0, r, q9, n, idx, extent, src);
     publish();
     float o[kOutPad];
     uint64_t mask[3];
-    forward_tile(smem, tbase, c, kA0, kA1, kA2, kA3, o, mask);
+    forward_tile<2>(smem, tbase, c, kGBase + kGA0, kGBase + kGA1, kGBase + kGA2, kGBase + kGA3, kGStride, o, mask);
     // loss gradient dL/do (rows of padding samples are zero)
+    float gy[kOutPad];
 #pragma unroll
     for (int j = 0; j < kOutPad; j++) {
-      float g = 0.0f;
+      float gv = 0.0f;
       if (idx < n && j < kOut) {
-        const float d = o[j] - y3[(size_t)idx * 3 + j];
+        const float d = o[j] - y3[(size_t)src * 3 + j];
         const float den = o[j] * o[j] + 0.01f;
-        g = 2.0f * d / den;
+        gv = 2.0f * d / den;
         lsum += d * d / den;
       }
-      *reinterpret_cast<uint16_t*>(smem + kDY + umma::canon_off(t, j, kOutPad)) = f2bf(g);
+      gy[j] = gv;
     }
+    store_row(mine + kGDY, r, kOutPad, gy);
     publish();
+    const uint32_t A[4] = {s0 + kGBase + kGA0, s0 + kGBase + kGA1, s0 + kGBase + kGA2, s0 + kGBase + kGA3};
+    const uint32_t DY = s0 + kGBase + kGDY;
     // layer 3: dW3 += A3^T dO ; dX3 = dO W3^T
     if (t == 0) {
-      issue_dw(tbase + kTW3, s0 + kA3, kHid, s0 + kDY, kOutPad, !first);
-      issue_fwd(tbase + kTDx, s0 + kDY, s0 + kWb3, kOutPad, kHid, false);
+      issue_dw(tbase + kTW3, A[3], kHid, DY, kOutPad, !first);
+      issue_dw(tbase + kTW3, A[3] + gs, kHid, DY + gs, kOutPad, true);
+      for (int q = 0; q < 2; q++) issue_dx(tbase + kTFwd + 64u * q, DY + q * gs, kOutPad, s0 + kWf3, kHid);
     }
     sync_mma(c);
-    const int abuf[3] = {kA1, kA2, kA3};
-    const int wb[3] = {kWb1, kWb2, kWb3};
+    const uint32_t wf[3] = {kWf1, kWf2, kWf3};
     const uint32_t tw[3] = {kTW0, kTW1, kTW2};
-    for (int l = 2; l >= 0; l--) {
-      // dH_{l+1} = dX_{l+1} * relu'(h_{l+1}) -> dY buffer (K-major rows = samples, C = 64)
-      float dx[kHid];
-      tmem_row(tbase, kTDx, kHid, dx);
 #pragma unroll
-      for (int j = 0; j < kHid; j++) {
-        const float g = ((mask[l] >> j) & 1ull) ? dx[j] : 0.0f;
-        *reinterpret_cast<uint16_t*>(smem + kDY + umma::canon_off(t, j, kHid)) = f2bf(g);
-      }
+    for (int l = 2; l >= 0; l--) {
+      // dH_{l+1} = dX_{l+1} * relu'(h_{l+1}) -> the group's dY tile (C = 64)
+      float dx[kHid];
+      tmem_row<kHid>(tbase, kTFwd + 64u * (uint32_t)g, dx);
+#pragma unroll
+      for (int j = 0; j < kHid; j++)
+        if (!((mask[l] >> j) & 1ull)) dx[j] = 0.0f;
+      store_row(mine + kGDY, r, kHid, dx);
       publish();
       if (t == 0) {
-        // dW_l += A_l^T dH_{l+1}   (A_0 has 80 columns)
-        const int ain = l == 0 ? kA0 : abuf[l - 1];
-        issue_dw(tbase + tw[l], s0 + ain, l == 0 ? kIn : kHid, s0 + kDY, kHid, !first);
-        if (l > 0) issue_fwd(tbase + kTDx, s0 + kDY, s0 + wb[l - 1], kHid, kHid, false);
+        // dW_l += A_l^T dH_{l+1}   (A_0 has 80 columns);  dX_l = dH_{l+1} W_l^T
+        const int cx = l == 0 ? kIn : kHid;
+        issue_dw(tbase + tw[l], A[l], cx, DY, kHid, !first);
+        issue_dw(tbase + tw[l], A[l] + gs, cx, DY + gs, kHid, true);
+        if (l > 0)
+          for (int q = 0; q < 2; q++) issue_dx(tbase + kTFwd + 64u * q, DY + q * gs, kHid, s0 + wf[l - 1], kHid);
       }
       sync_mma(c);
     }
     first = false;
   }
-  // partial gradients of this CTA: lane = input feature row, columns = outputs
+  // partial gradients of this CTA: TMEM lane = input feature row, columns = outputs
   float* pc = partial + (size_t)blockIdx.x * kParams;
   if (c.ok) {
     const int kin[4] = {kIn, kHid, kHid, kHid};
     const int nout[4] = {kHid, kHid, kHid, kOutPad};
     const int off[4] = {kOff0, kOff1, kOff2, kOff3};
-    const uint32_t tw[4] = {kTW0, kTW1, kTW2, kTW3};
+    const uint32_t twa[4] = {kTW0, kTW1, kTW2, kTW3};
+#pragma unroll
     for (int l = 0; l < 4; l++) {
       float row[kHid];
-      tmem_row(tbase, tw[l], nout[l], row);
-      if (t < kin[l])
-        for (int j = 0; j < nout[l]; j++) pc[off[l] + t * nout[l] + j] = first ? 0.0f : row[j];
+      if (l < 3) tmem_row<kHid>(tbase, twa[l], row);
+      else tmem_row<kOutPad>(tbase, twa[l], row);
+      if (g == 0 && r < kin[l]) {
+#pragma unroll
+        for (int j = 0; j < (l < 3 ? kHid : kOutPad); j++) pc[off[l] + r * nout[l] + j] = first ? 0.0f : row[j];
+      }
     }
   }
   // loss of this CTA
@@ -407,7 +499,9 @@ __global__ void __launch_bounds__(128, 1) k_mlp_grad(const uint16_t* __restrict_
   if ((t & 31) == 0) s_loss[warp] = lsum;
   __syncthreads();
   if (t == 0) {
-    loss[blockIdx.x] = (s_loss[0] + s_loss[1]) + (s_loss[2] + s_loss[3]);
+    float a = 0.0f;
+    for (int i = 0; i < 8; i++) a += s_loss[i];
+    loss[blockIdx.x] = a;
     if (!c.ok) atomicExch(err, 1);
   }
   umma::fence_before_sync();
@@ -416,9 +510,14 @@ __global__ void __launch_bounds__(128, 1) k_mlp_grad(const uint16_t* __restrict_
 }
 
 // grad[i] = sum over CTAs of partial[cta][i] / n  (fixed order: deterministic)
-__global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, float inv_n, float* __restrict__ grad) {
+__global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, int n_req, const int* __restrict__ n_dev,
+                             int pop_cap, float* __restrict__ grad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
+  int n, pop;
+  bool draw;
+  mlp::sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
+  const float inv_n = n > 0 ? 1.0f / (float)n : 0.0f;
   float s = 0.0f;
   for (int c = 0; c < ctas; c++) s += partial[(size_t)c * mlp::kParams + i];
   grad[i] = s * inv_n;
@@ -427,9 +526,10 @@ __global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, float 
 // Adam on fp32 masters; writes the bf16 copy.  Output columns >= 3 stay 0.
 __global__ void k_mlp_adam(float* __restrict__ wm, float* __restrict__ m, float* __restrict__ v,
                            const float* __restrict__ grad, uint16_t* __restrict__ wb, float lr, float b1, float b2,
-                           float eps, float bc1, float bc2) {
+                           float eps, float bc1, float bc2, const int* __restrict__ n_dev) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
+  if (n_dev && *n_dev <= 0) return;
   if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) { wm[i] = 0.0f; wb[i] = 0; return; }
   const float g = grad[i];
   const float mi = b1 * m[i] + (1.0f - b1) * g;
@@ -468,37 +568,47 @@ cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cuda
   return cudaGetLastError();
 }
 
-cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, float extent, float* out, int* err,
-                      cudaStream_t st) {
+cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_dev, float extent, float* out,
+                      int* err, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kInferSmem);
-  if (e != cudaSuccess) return e;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kInferSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
   const int tiles = (n + 127) / 128;
-  const int grid = std::min(tiles, sm_count_mlp() * 2);
-  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(wb, q9, n, extent, out, err);
+  const int grid = std::min(tiles, sm_count_mlp() * 3);   // 3 x 72 KB of shared memory per SM
+  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(wb, q9, n, n_dev, extent, out, err);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, float extent, float* partial,
-                         float* loss_ctas, int* err, float* grad, int* ctas_used, cudaStream_t st) {
+cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
+                         int pop_cap, uint32_t draw_seed, float extent, float* partial, float* loss_ctas, int* err,
+                         float* grad, int* ctas_used, cudaStream_t st) {
   if (n <= 0) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
-  if (e != cudaSuccess) return e;
-  const int tiles = (n + 127) / 128;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int tiles = (n + 255) / 256;
   const int grid = std::min(tiles, sm_count_mlp());
-  k_mlp_grad<<<grid, 128, mlp::kTrainSmem, st>>>(wb, q9, y3, n, extent, partial, loss_ctas, err);
-  e = cudaGetLastError();
+  k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(wb, q9, y3, n, n_dev, pop_cap, draw_seed, extent, partial,
+                                                 loss_ctas, err);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, 1.0f / (float)n, grad);
+  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, n, n_dev, pop_cap, grad);
   if (ctas_used) *ctas_used = grid;
   return cudaGetLastError();
 }
 
 cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
-                     cudaStream_t st) {
+                     const int* n_dev, cudaStream_t st) {
   const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
   const float bc1 = 1.0f - std::pow(b1, (float)step), bc2 = 1.0f - std::pow(b2, (float)step);
-  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, bc1, bc2);
+  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, bc1, bc2, n_dev);
   return cudaGetLastError();
 }
 
@@ -513,9 +623,9 @@ using namespace vrt;
 
 // Diagnostic of the tensor-core operand layouts (see k_umma_selftest).
 extern "C" int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint16_t* B, float* D) {
-  if (!A || !B || !D || (mode != 0 && mode != 1) || N < 16 || N > 64 || N % 16 || K < 16 || K > 128 || K % 16)
+  if (!A || !B || !D || mode < 0 || mode > 2 || N < 16 || N > 64 || N % 16 || K < 16 || K > 128 || K % 16)
     return set_error(VRT_ERR_INVALID, "vrt_mlp_selftest_gemm: bad argument");
-  const size_t na = (size_t)128 * K, nb = mode == 0 ? (size_t)N * K : (size_t)128 * N;
+  const size_t na = (size_t)128 * K, nb = mode == 1 ? (size_t)128 * N : (size_t)N * K;
   const size_t nd = (size_t)128 * N;
   void* buf = nullptr;
   cudaError_t e = cudaMalloc(&buf, (na + nb) * 2 + nd * 4 + 16);

@@ -24,6 +24,7 @@
 // exactly the megakernel's, so results are bit-identical to it and to the
 // CPU oracle.
 #include "wavefront_core.cuh"
+#include <algorithm>
 #include <cstring>
 
 namespace vrt {
@@ -33,10 +34,7 @@ size_t wavefront_bytes(int W, int H, int max_waves) {
   return P * 16 * 7 + P * 4 * 2 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
 }
 
-cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
-                             const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
-                             cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves,
-                             int* timed_waves) {
+static SingleJob make_job(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H, const PathOut& out) {
   SingleJob job;
   std::memcpy(&job.u, &uu, sizeof(Uni));
   job.S.vox = s.vox; job.S.masks = s.masks; job.S.bits = s.bits; job.S.N = s.N; job.S.BG = s.BG;
@@ -47,11 +45,29 @@ cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fcl
   job.fclamp = fclamp;
   job.W = W;
   job.H = H;
-  const int waves = (int)job.u.params0[1] + 2;
+  return job;
+}
+
+cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
+                             const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
+                             cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves,
+                             int* timed_waves, const CacheDev* cache) {
+  const SingleJob job = make_job(s, uu, fclamp, W, H, out);
+  // cache-assisted frames run as many waves as their training paths need
+  const int waves = (cache && cache->on ? (int)cache->train_bounces : (int)job.u.params0[1]) + 2;
   const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
   const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
   return wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
-                         max_timed_waves, timed_waves);
+                         max_timed_waves, timed_waves, cache);
+}
+
+cudaError_t launch_cache_resolve(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
+                                 const PathOut& out, const WavefrontBufs& wb, const CacheDev& cc, const float* pred,
+                                 cudaStream_t st) {
+  const SingleJob job = make_job(s, uu, fclamp, W, H, out);
+  const int blocks = std::min((W * H + 255) / 256, wf_sm_count() * 8);
+  k_cache_resolve<SingleJob><<<blocks, 256, 0, st>>>(job, wf_view(wb), cc, pred, out.stats);
+  return cudaGetLastError();
 }
 
 }  // namespace vrt

@@ -97,6 +97,16 @@ struct VrtSession {
   cudaEvent_t tev[2 * kTimedWaves] = {};   // brackets of each wave's trace kernel
   int timed_waves = 0;
   uint32_t launches = 0;
+  // radiance cache
+  VrtCacheConfig cache_cfg{};
+  bool cache_on = false;
+  VrtMlp* mlp = nullptr;
+  void* cache_mem = nullptr;
+  size_t cache_bytes = 0;
+  CacheDev cache{};
+  float* pred = nullptr;
+  cudaEvent_t cev[2] = {};
+  bool cache_timed = false;
 };
 
 static int set_dev(VrtCtx* ctx) {
@@ -340,6 +350,10 @@ int vrt_session_destroy(VrtSession* s) {
   dev_free(c, s->ldr, P * 4, &s->bytes);
   dev_free(c, s->stats, kStatCount * 8, &s->bytes);
   dev_free(c, s->wf_mem, s->wf_bytes, &s->bytes);
+  dev_free(c, s->cache_mem, s->cache_bytes, &s->bytes);
+  if (s->mlp) vrt_mlp_destroy(s->mlp);
+  for (auto& e : s->cev)
+    if (e) cudaEventDestroy(e);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : s->tev)
@@ -526,6 +540,7 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
 }
 
 static int parity_of(const VrtSession* s) { return (int)(s->frame_counter & 1u); }
+static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o);
 
 int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
@@ -535,6 +550,7 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
   if (s->path_kernel == VRT_PATH_BATCH_ONLY)
     return fail(VRT_ERR_STATE, "session was created for batches only (VRT_PATH_BATCH_ONLY)");
+  if (s->cache_on) return cache_frame(s, u, o);
   if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
     CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
                               &s->launches, s->timing ? s->tev : nullptr, VrtSession::kTimedWaves,
@@ -634,6 +650,13 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
   out->voxel_reads = h[kStatVReads];
   out->pixels = h[kStatPixels];
   out->launches = s->launches;
+  out->cache_on = s->cache_on ? 1u : 0u;
+  out->cache_queries = h[kStatCacheQueries];
+  out->cache_samples = h[kStatCacheSamples];
+  if (s->cache_on && s->mlp) {
+    if (int r = vrt_mlp_check(s->mlp)) return r;
+  }
+  if (s->timing && s->have_frame && s->cache_timed) CUDA_TRY(cudaEventElapsedTime(&out->ms_cache, s->cev[0], s->cev[1]));
   if (s->timing && s->have_frame) {
     float a = 0, b = 0, c = 0, d = 0;
     CUDA_TRY(cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
@@ -1397,13 +1420,13 @@ int vrt_mlp_encode_device(VrtMlp* m, const float* d_q9, int n, float extent, uin
 int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, float* d_out3) {
   if (!m || n < 0 || (n && (!d_q9 || !d_out3)) || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
   if (int r = set_dev(m->ctx)) return r;
-  CUDA_TRY(mlp_infer(m->wb, d_q9, n, extent, d_out3, m->err, m->ctx->stream));
+  CUDA_TRY(mlp_infer(m->wb, d_q9, n, nullptr, extent, d_out3, m->err, m->ctx->stream));
   return VRT_OK;
 }
 
 static int mlp_grad_impl(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* loss_out) {
   int ctas = 0;
-  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, extent, m->partial, m->loss, m->err, m->grad, &ctas,
+  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, nullptr, n, 0u, extent, m->partial, m->loss, m->err, m->grad, &ctas,
                         m->ctx->stream));
   if (loss_out) {
     std::vector<float> l((size_t)ctas);
@@ -1434,7 +1457,7 @@ int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n,
   for (int i = 0; i < steps; i++) {
     if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, (loss_out && i == 0) ? loss_out : nullptr)) return r;
     m->step++;
-    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step, m->ctx->stream));
+    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step, nullptr, m->ctx->stream));
   }
   return VRT_OK;
 }
@@ -1443,6 +1466,128 @@ int vrt_mlp_check(VrtMlp* m) {
   if (!m) return fail(VRT_ERR_INVALID, "NULL argument");
   if (int r = set_dev(m->ctx)) return r;
   return mlp_check_err(m);
+}
+
+// ---------------------------------------------------------------------------
+// cache-assisted sessions
+// ---------------------------------------------------------------------------
+int vrt_session_cache_mlp(VrtSession* s, VrtMlp** out) {
+  if (!s || !out) return fail(VRT_ERR_INVALID, "NULL argument");
+  *out = s->mlp;
+  return VRT_OK;
+}
+
+int vrt_session_set_cache(VrtSession* s, const VrtCacheConfig* cfg_in) {
+  if (!s || !cfg_in) return fail(VRT_ERR_INVALID, "NULL argument");
+  VrtCacheConfig cfg = *cfg_in;
+  if (!cfg.enabled) {
+    s->cache_on = false;
+    return VRT_OK;
+  }
+  if (s->path_kernel != VRT_PATH_WAVEFRONT) return fail(VRT_ERR_STATE, "the cache needs the wavefront path kernel");
+  if (cfg.train_bounces == 0) cfg.train_bounces = 6;
+  if (cfg.train_vertices == 0) cfg.train_vertices = 3;
+  if (cfg.train_batch == 0) cfg.train_batch = 65536;
+  if (cfg.train_steps == 0) cfg.train_steps = 1;
+  if (cfg.learning_rate == 0.0f) cfg.learning_rate = 1e-2f;
+  if (cfg.train_bounces < 1 || cfg.train_bounces + 3 > s->wf.max_waves || cfg.train_vertices < 1 ||
+      cfg.train_vertices > kCacheMaxRec || cfg.train_batch < 1 || cfg.train_batch > (1 << 22) ||
+      cfg.train_steps < 0 || cfg.train_steps > 64 || !(cfg.learning_rate > 0.0f))
+    return fail(VRT_ERR_INVALID, "cache configuration out of range");
+  if (int r = set_dev(s->ctx)) return r;
+  VrtCtx* c = s->ctx;
+  const size_t P = px(s);
+  const int TW = (s->W + 3) / 4, TH = (s->H + 3) / 4;
+  const size_t T = (size_t)TW * TH;
+  const size_t cap = T * (size_t)cfg.train_vertices;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t b_rec = al(T * kCacheMaxRec * 64), b_recn = al(T * 4), b_q = al(P * 36), b_qpix = al(P * 4),
+               b_ctr = 256, b_cq = al(cap * 36), b_cy = al(cap * 12), b_pred = al(P * 12);
+  const size_t need = b_rec + b_recn + b_q + b_qpix + b_ctr + b_cq + b_cy + b_pred;
+  if (need != s->cache_bytes) {
+    cudaStreamSynchronize(c->stream);
+    dev_free(c, s->cache_mem, s->cache_bytes, &s->bytes);
+    s->cache_bytes = 0;
+    if (int r = dev_alloc(c, &s->cache_mem, need, &s->bytes)) return r;
+    s->cache_bytes = need;
+  }
+  char* m = (char*)s->cache_mem;
+  CacheDev& d = s->cache;
+  std::memset(&d, 0, sizeof d);
+  d.rec = (float4*)m; m += b_rec;
+  d.rec_n = (int*)m; m += b_recn;
+  d.qbuf = (float*)m; m += b_q;
+  d.qpix = (uint32_t*)m; m += b_qpix;
+  d.qcount = (int*)m;
+  d.cand_count = (int*)m + 1;
+  m += b_ctr;
+  d.cand_q9 = (float*)m; m += b_cq;
+  d.cand_y3 = (float*)m; m += b_cy;
+  s->pred = (float*)m;
+  d.cand_cap = (int)cap;
+  d.TW = TW;
+  d.train_bounces = (uint32_t)cfg.train_bounces;
+  d.rec_vertices = cfg.train_vertices;
+  d.tclamp = s->fclamp;
+  if (!s->mlp) {
+    if (int r = vrt_mlp_create(c, cfg.seed, &s->mlp)) return r;
+  }
+  if (!s->cev[0]) {
+    for (auto& e : s->cev)
+      if (cudaEventCreate(&e) != cudaSuccess) return fail(VRT_ERR_CUDA, "cudaEventCreate failed");
+  }
+  s->cache_cfg = cfg;
+  s->cache_on = true;
+  return VRT_OK;
+}
+
+int vrt_session_read_cache_samples(VrtSession* s, float* q9, float* y3, int cap, int* count) {
+  if (!s || !count || cap < 0 || (cap > 0 && (!q9 || !y3))) return fail(VRT_ERR_INVALID, "bad argument");
+  if (!s->cache_mem) return fail(VRT_ERR_STATE, "the cache was never enabled on this session");
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  int n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, s->cache.cand_count, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  *count = n;
+  const int k = std::min(std::min(n, s->cache.cand_cap), cap);
+  if (k > 0) {
+    CUDA_TRY(cudaMemcpyAsync(q9, s->cache.cand_q9, (size_t)k * 36, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(y3, s->cache.cand_y3, (size_t)k * 12, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  return VRT_OK;
+}
+
+// One cache-assisted path-trace pass: waves (training + query paths),
+// inference over the queries, resolve, then the frame's training steps.
+static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o) {
+  cudaStream_t st = s->ctx->stream;
+  VrtMlp* m = s->mlp;
+  CacheDev d = s->cache;
+  d.on = 1;
+  const uint32_t frame = u->params0[0];
+  d.phase = (frame * 7u) & 15u;   // 7 is odd: all 16 positions within 16 frames
+  const int P = s->W * s->H;
+  const float extent = (float)s->scene->dev.N * 0.0625f;
+  CUDA_TRY(cudaMemsetAsync(d.qcount, 0, 8, st));
+  CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, st, &s->launches,
+                            s->timing ? s->tev : nullptr, VrtSession::kTimedWaves, &s->timed_waves, &d));
+  s->cache_timed = s->timing;
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->cev[0], st));
+  CUDA_TRY(mlp_infer(m->wb, d.qbuf, P, d.qcount, extent, s->pred, m->err, st));
+  CUDA_TRY(launch_cache_resolve(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, d, s->pred, st));
+  s->launches += 2;
+  for (int k = 0; k < s->cache_cfg.train_steps; k++) {
+    const uint32_t seed = frame * 0x9e3779b9u + (uint32_t)k * 0x85ebca6bu + 0x1234567u;
+    CUDA_TRY(mlp_gradient(m->wb, d.cand_q9, d.cand_y3, s->cache_cfg.train_batch, d.cand_count, d.cand_cap, seed,
+                          extent, m->partial, m->loss, m->err, m->grad, nullptr, st));
+    m->step++;
+    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, s->cache_cfg.learning_rate, m->step, d.cand_count, st));
+    s->launches += 3;
+  }
+  if (s->timing) CUDA_TRY(cudaEventRecord(s->cev[1], st));
+  return VRT_OK;
 }
 
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev) {

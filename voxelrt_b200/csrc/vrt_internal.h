@@ -19,7 +19,10 @@ struct SceneDev {
 inline size_t occ_words(int BG) { return ((size_t)BG * BG * BG + 31) / 32; }
 
 // Per-frame counters written by the path kernel (u64 each).
-enum StatSlot { kStatRays = 0, kStatOuter, kStatInner, kStatVReads, kStatPixels, kStatCount = 8 };
+enum StatSlot {
+  kStatRays = 0, kStatOuter, kStatInner, kStatVReads, kStatPixels, kStatCacheQueries, kStatCacheSamples,
+  kStatCount = 8
+};
 
 // Device pointers of one frame's path-trace outputs.
 struct PathOut {
@@ -41,6 +44,29 @@ struct WavefrontBufs {
   int* ctr = nullptr;                                 // 4 ints per wave
   int max_waves = 0;
 };
+
+// Radiance-cache state of one cache-assisted wavefront frame (device
+// pointers; see wavefront_core.cuh for how the kernels use it).
+constexpr int kCacheMaxRec = 8;   // record slots per training path
+
+struct CacheDev {
+  int on;
+  uint32_t train_bounces;   // bounce count of training paths
+  int rec_vertices;         // vertices 0..rec_vertices-1 give training samples
+  uint32_t phase;           // training pixels: (x & 3, y & 3) == (phase & 3, phase >> 2)
+  int TW;                   // training paths per image row: ceil(W / 4)
+  float tclamp;             // per-channel clamp of training targets (<= 0: none)
+  float4* rec;              // [T][kCacheMaxRec][4]: (pos, R.x) (normal, R.y) (albedo, R.z) (tp, 0)
+  int* rec_n;               // [T] records written by the training path
+  float* qbuf;              // [P][9] cache queries: position, normal, albedo
+  uint32_t* qpix;           // [P] path id of each query
+  int* qcount;
+  float* cand_q9;           // [cap][9] training samples
+  float* cand_y3;           // [cap][3]
+  int* cand_count;          // samples produced this frame (may exceed cap)
+  int cand_cap;
+};
+
 
 // Launch-shape knobs of the wavefront tracer (chosen by the autotuner).
 struct WavefrontTuning {
@@ -86,12 +112,19 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
 int mlp_num_params();
 int mlp_max_ctas();
 cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cudaStream_t st);
-cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, float extent, float* out, int* err,
-                      cudaStream_t st);
-cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, float extent, float* partial,
-                         float* loss_ctas, int* err, float* grad, int* ctas_used, cudaStream_t st);
+// n_dev (may be null): the query count is read on the device, n is its upper bound.
+cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_dev, float extent, float* out,
+                      int* err, cudaStream_t st);
+// Sample selection: with n_dev null the n samples in order; otherwise the
+// population is min(*n_dev, pop_cap) samples and a step uses min(population,
+// n) of them -- all of them in order when they fit, else n uniform draws
+// (with replacement) keyed by draw_seed.
+cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
+                         int pop_cap, uint32_t draw_seed, float extent, float* partial, float* loss_ctas, int* err,
+                         float* grad, int* ctas_used, cudaStream_t st);
+// n_dev (may be null): the step is skipped when *n_dev == 0.
 cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
-                     cudaStream_t st);
+                     const int* n_dev, cudaStream_t st);
 cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st);
 
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
@@ -100,10 +133,16 @@ int set_error(int code, const char* msg);
 size_t wavefront_bytes(int W, int H, int max_waves);
 // When trace_ev is non-null, events trace_ev[2w], trace_ev[2w+1] bracket the
 // trace kernel of wave w (w < max_timed_waves); *timed_waves receives the count.
+// cache (may be null): cache-assisted frame (training + query paths).
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
                              cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev = nullptr,
-                             int max_timed_waves = 0, int* timed_waves = nullptr);
+                             int max_timed_waves = 0, int* timed_waves = nullptr, const CacheDev* cache = nullptr);
+// Finishes the cache-terminated paths of a cache-assisted frame with the
+// network's predictions pred[3 * query].
+cudaError_t launch_cache_resolve(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                                 const PathOut& out, const WavefrontBufs& wb, const CacheDev& cc, const float* pred,
+                                 cudaStream_t st);
 
 cudaError_t launch_build_bricks(const SceneDev& s, int bx0, int by0, int bz0, int bx1, int by1, int bz1,
                                 cudaStream_t st);

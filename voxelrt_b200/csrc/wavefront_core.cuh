@@ -5,6 +5,7 @@
 #pragma once
 #include "vrt_device.cuh"
 #include "vrt_internal.h"
+#include <cstring>
 
 namespace vrt {
 
@@ -278,6 +279,88 @@ struct MultiJob {
 };
 
 // ---------------------------------------------------------------------------
+// radiance cache hooks (single session).  With the cache on, 1/16 of the
+// pixels (one position of every 4x4 block, rotating per frame) trace full
+// training paths of `train_bounces` bounces and record their first
+// `rec_vertices` vertices; every other path ends at its first bounce hit
+// (vertex 1): its emission is picked up there and the reflected radiance at
+// that point is queried from the network after the waves.
+// ---------------------------------------------------------------------------
+enum : int { kRolePlain = 0, kRoleTrain = 1, kRoleQuery = 2 };
+
+VRT_DI int cache_role(const CacheDev& c, uint32_t lp, int W) {
+  if (!c.on) return kRolePlain;
+  const uint32_t x = lp % (uint32_t)W, y = lp / (uint32_t)W;
+  return ((x & 3u) == (c.phase & 3u) && (y & 3u) == (c.phase >> 2)) ? kRoleTrain : kRoleQuery;
+}
+
+VRT_DI uint32_t train_index(const CacheDev& c, uint32_t lp, int W) {
+  const uint32_t x = lp % (uint32_t)W, y = lp / (uint32_t)W;
+  return (y >> 2) * (uint32_t)c.TW + (x >> 2);
+}
+
+// Record slot of vertex k of a training path (nullptr: nothing to record).
+VRT_DI float4* rec_slot(const CacheDev& c, int role, uint32_t lp, int W, uint32_t k) {
+  if (role != kRoleTrain || (int)k >= c.rec_vertices) return nullptr;
+  const uint32_t ti = train_index(c, lp, W);
+  c.rec_n[ti] = (int)k + 1;
+  return c.rec + ((size_t)ti * kCacheMaxRec + k) * 4;
+}
+
+VRT_DI float cache_target(float rfin, float rk, float tpk, float clampv) {
+  float v = tpk > 1e-6f ? (rfin - rk) / tpk : 0.0f;
+  v = fmax_(v, 0.0f);
+  if (clampv > 0.0f) v = fmin_(v, clampv);
+  return v;
+}
+
+// Training samples of finished training paths: for each recorded vertex k,
+// the radiance the path gathered after vertex k's emission pickup per unit
+// of the throughput that reached it, (R_final - R_k) / tp_k -- the reflected
+// radiance estimate at x_k.  Warp-aggregated append; all 32 lanes call.
+VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nrec = fin ? c.rec_n[ti] : 0;
+  int incl = nrec;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(full, incl, 31);
+  if (total == 0) return;
+  int base = 0;
+  if (lane == 31) base = atomicAdd(c.cand_count, total);
+  base = __shfl_sync(full, base, 31);
+  int slot = base + incl - nrec;
+  for (int k = 0; k < nrec && slot < c.cand_cap; k++, slot++) {
+    const float4* r = c.rec + ((size_t)ti * kCacheMaxRec + k) * 4;
+    const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+    float* q = c.cand_q9 + (size_t)slot * 9;
+    q[0] = r0.x; q[1] = r0.y; q[2] = r0.z;
+    q[3] = r1.x; q[4] = r1.y; q[5] = r1.z;
+    q[6] = r2.x; q[7] = r2.y; q[8] = r2.z;
+    float* y = c.cand_y3 + (size_t)slot * 3;
+    y[0] = cache_target(rfin.x, r0.w, r3.x, c.tclamp);
+    y[1] = cache_target(rfin.y, r1.w, r3.y, c.tclamp);
+    y[2] = cache_target(rfin.z, r2.w, r3.z, c.tclamp);
+  }
+}
+
+// Appends a cache query of path g at its vertex 1.  All 32 lanes call.
+VRT_DI void cache_emit_query(const CacheDev& c, bool q, uint32_t g, F3 pos, F3 n, F3 alb) {
+  const uint32_t slot = warp_append(c.qcount, q);
+  if (q) {
+    float* d = c.qbuf + (size_t)slot * 9;
+    d[0] = pos.x; d[1] = pos.y; d[2] = pos.z;
+    d[3] = n.x; d[4] = n.y; d[5] = n.z;
+    d[6] = alb.x; d[7] = alb.y; d[8] = alb.z;
+    c.qpix[slot] = g;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // shading
 // ---------------------------------------------------------------------------
 VRT_DI void finalize(const JobOut& out, uint32_t lp, F3 radiance, uint32_t mat1bits, float fclamp) {
@@ -291,10 +374,19 @@ VRT_DI void finalize(const JobOut& out, uint32_t lp, F3 radiance, uint32_t mat1b
 
 // Vertex k of a path (pathtrace.wgsl:297-320 loop body up to the trace call),
 // path state at index g.  Returns whether the path stays active.
+// kmax: the path's last vertex (the uniforms' bounce count for plain paths).
+// rec (may be null): training record of this vertex, written after the
+// emission pickup.
 VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, uint32_t g, uint32_t k, F3 pos, F3 n, Mat mat,
                          F3& radiance, F3& tp, uint32_t& rng, uint32_t mat1bits, bool& want_shadow,
-                         bool& want_bounce) {
+                         bool& want_bounce, uint32_t kmax, float4* rec) {
   if (mat.emissive > 0.0f) radiance = radiance + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
+  if (rec) {
+    rec[0] = make_float4(pos.x, pos.y, pos.z, radiance.x);
+    rec[1] = make_float4(n.x, n.y, n.z, radiance.y);
+    rec[2] = make_float4(mat.albedo.x, mat.albedo.y, mat.albedo.z, radiance.z);
+    rec[3] = make_float4(tp.x, tp.y, tp.z, 0.0f);
+  }
   const F3 surf = pos + n * 1e-3f;
   const F3 l = sample_sun_dir(u, rng);
   const float ndl = dot3(n, l);
@@ -308,7 +400,7 @@ VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, uint32_t g, uint32_t k, F
     b.R2[g] = make_float4(l.x, l.y, l.z, 0.0f);
   }
   want_bounce = false;
-  if (k == u.params0[1]) {
+  if (k == kmax) {
     flags |= kFlagTerminal;
   } else {
     const F3 rd = cosine_hemisphere(n, rng);
@@ -450,12 +542,16 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(J jobs, WfDev b, i
 
 // shade(0): primary hits over all pixels.
 template <class J>
-__global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, WfDev b, unsigned long long* stats) {
+__global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, WfDev b, unsigned long long* stats,
+                                                          CacheDev cc) {
   const uint32_t stride = gridDim.x * blockDim.x;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + kStatPixels, (unsigned long long)P);
   for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += stride) {
     const uint32_t g = base + threadIdx.x;
     bool shadow = false, bounce = false, keep = false;
+    bool fin_train = false;
+    uint32_t ti = 0u;
+    F3 rfin = f3(0.0f, 0.0f, 0.0f);
     if (g < P) {
       const int j = jobs.job_of(g);
       const Uni& u = jobs.uni(j);
@@ -480,27 +576,41 @@ __global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, Wf
         out.gbuf[lp] = make_float4(n1.x, n1.y, n1.z, t);
         uint32_t rng = __float_as_uint(b.S0[g].w);
         F3 radiance = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
-        keep = shade_vertex(u, b, g, 0u, x1, n1, mat1, radiance, tp, rng, h.y, shadow, bounce);
-        if (!keep) finalize(out, lp, radiance, h.y, jobs.clamp(j));
+        const int W = jobs.width(j);
+        const int role = cache_role(cc, lp, W);
+        const uint32_t kmax = role == kRolePlain ? u.params0[1] : (role == kRoleTrain ? cc.train_bounces : 1u);
+        keep = shade_vertex(u, b, g, 0u, x1, n1, mat1, radiance, tp, rng, h.y, shadow, bounce, kmax,
+                            rec_slot(cc, role, lp, W, 0u));
+        if (!keep) {
+          finalize(out, lp, radiance, h.y, jobs.clamp(j));
+          if (role == kRoleTrain) { fin_train = true; ti = train_index(cc, lp, W); rfin = radiance; }
+        }
       }
     }
     emit(b, 1, g, shadow, bounce, keep);
+    if (cc.on) cache_emit_samples(cc, fin_train, ti, rfin);
   }
 }
 
 // shade(k), k >= 1: resolve vertex k-1's shadow ray, then the bounce hit.
 template <class J>
-__global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave) {
+__global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave, CacheDev cc) {
   const int n = b.ctr[4 * wave + 2];
   const uint32_t* list = active_of(b, wave);
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
     const int i = base + threadIdx.x;
     bool shadow = false, bounce = false, keep = false;
+    bool fin_train = false, query = false;
+    uint32_t ti = 0u;
+    F3 rfin = f3(0.0f, 0.0f, 0.0f), qpos = rfin, qn = rfin, qalb = rfin;
     uint32_t g = 0u;
     if (i < n) {
       g = list[i];
       const int j = jobs.job_of(g);
+      const uint32_t lp = g - jobs.first(j);
+      const int W = jobs.width(j);
+      const int role = cache_role(cc, lp, W);
       const float4 s0 = b.S0[g];
       const float4 s1 = b.S1[g];
       const float4 s2 = b.S2[g];
@@ -524,13 +634,52 @@ __global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave) {
           const F3 pos = surf + rd * t;
           const F3 nrm = hit_normal((int)h.z, rd);
           const Mat mat = unpack_material(h.y);
-          keep = shade_vertex(u, b, g, (uint32_t)wave, pos, nrm, mat, radiance, tp, rng, mat1bits, shadow, bounce);
-          done = !keep;
+          if (role == kRoleQuery) {
+            // path ends at vertex 1: emission here, reflected radiance from the cache
+            if (mat.emissive > 0.0f) radiance = radiance + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
+            b.S0[g] = make_float4(radiance.x, radiance.y, radiance.z, __uint_as_float(rng));
+            query = true;
+            qpos = pos; qn = nrm; qalb = mat.albedo;
+          } else {
+            const uint32_t kmax = role == kRolePlain ? u.params0[1] : cc.train_bounces;
+            keep = shade_vertex(u, b, g, (uint32_t)wave, pos, nrm, mat, radiance, tp, rng, mat1bits, shadow, bounce,
+                                kmax, rec_slot(cc, role, lp, W, (uint32_t)wave));
+            done = !keep;
+          }
         }
       }
-      if (done) finalize(jobs.outs(j), g - jobs.first(j), radiance, mat1bits, jobs.clamp(j));
+      if (done) {
+        finalize(jobs.outs(j), lp, radiance, mat1bits, jobs.clamp(j));
+        if (role == kRoleTrain) { fin_train = true; ti = train_index(cc, lp, W); rfin = radiance; }
+      }
     }
     emit(b, wave + 1, g, shadow, bounce, keep);
+    if (cc.on) {
+      cache_emit_query(cc, query, g, qpos, qn, qalb);
+      cache_emit_samples(cc, fin_train, ti, rfin);
+    }
+  }
+}
+
+// Cache-terminated paths: radiance += throughput at vertex 1 * predicted
+// reflected radiance there, then the usual clamp / demodulation / store.
+template <class J>
+__global__ void __launch_bounds__(256) k_cache_resolve(J jobs, WfDev b, CacheDev cc, const float* __restrict__ pred,
+                                                       unsigned long long* stats) {
+  const int n = *cc.qcount;
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(stats + kStatCacheQueries, (unsigned long long)n);
+    atomicAdd(stats + kStatCacheSamples, (unsigned long long)min(*cc.cand_count, cc.cand_cap));
+  }
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t g = cc.qpix[i];
+    const int j = jobs.job_of(g);
+    const float4 s0 = b.S0[g];
+    const float4 s1 = b.S1[g];
+    const F3 L = f3(fmax_(pred[3 * i], 0.0f), fmax_(pred[3 * i + 1], 0.0f), fmax_(pred[3 * i + 2], 0.0f));
+    const F3 radiance = xyz(s0) + xyz(s1) * L;
+    finalize(jobs.outs(j), g - jobs.first(j), radiance, __float_as_uint(s1.w), jobs.clamp(j));
   }
 }
 
@@ -576,9 +725,13 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 template <class J>
 cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                             const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
-                            uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
+                            uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
+                            const CacheDev* cache = nullptr) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   const WfDev b = wf_view(wb);
+  CacheDev cc;
+  std::memset(&cc, 0, sizeof cc);
+  if (cache) cc = *cache;
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
   if (e != cudaSuccess) return e;
   const int sms = wf_sm_count();
@@ -606,8 +759,8 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
     if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
     if (tm) timed++;
     nl++;
-    if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
-    else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
+    if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats, cc);
+    else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w, cc);
     nl++;
   }
   if (launches) *launches += nl;
