@@ -45,9 +45,10 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
-    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve"],
+    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
-                         "serve: Poisson request stream over 32 sessions")
+                         "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
+                         "path tracing at matched MSE")
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
@@ -484,6 +485,136 @@ def run_batched(args, local):
     ctx.close()
 
 
+CACHE_SCENES = [
+    # (label, scene kind, grid, seed, width, height, reference image)
+    ("64^3 test scene (Cornell room on terrain, seed 1)", 1, 64, 1, 256, 144, "cache_reference_64_256x144.npz"),
+    ("256^3 world (seed 2)", 2, 256, 2, 480, 270, "cache_reference_256_480x270.npz"),
+]
+CACHE_CFG = dict(train_bounces=6, train_vertices=3, train_batch=65536, train_steps=1, learning_rate=1e-2, seed=1)
+
+
+def cache_quality(vrt, ctx, scene, spawn, W, H, ref, bounces, cache, warm, K):
+    """MSE against the FP64 reference of K consecutive 1-spp frames (static
+    camera at the spawn pose) after `warm` frames: the mean per-frame MSE,
+    the MSE of the K-frame average, and the implied per-frame variance and
+    squared bias (MSE_K = bias^2 + var / K)."""
+    import numpy as np
+
+    from voxelrt_b200.quality import hdr_image, mse
+    s = vrt.Session(ctx, scene, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+    if cache:
+        s.set_cache(**cache)
+    light = vrt.Lighting()
+    for f in range(warm):
+        s.pathtrace(vrt.make_uniforms(spawn, None, light, f, bounces, 0, W, H))
+        s.end_frame()
+    per, acc = [], np.zeros_like(ref)
+    for f in range(warm, warm + K):
+        s.pathtrace(vrt.make_uniforms(spawn, None, light, f, bounces, 0, W, H))
+        s.end_frame()
+        img = hdr_image(s)
+        per.append(mse(img, ref))
+        acc += img
+    s.close()
+    m1, mk = float(np.mean(per)), mse(acc / K, ref)
+    var = max(m1 - mk, 0.0) * K / (K - 1)
+    return {"mse_1spp": round(m1, 6), f"mse_{K}frame_mean": round(mk, 6), "var": round(var, 6),
+            "bias2": round(mk - var / K, 7)}
+
+
+def run_cache(args, local):
+    """Cache-assisted path tracing against plain 2- and 6-bounce tracing.
+
+    Quality: MSE against a 4096-spp FP64 plain 6-bounce reference (committed
+    fixtures) on two scenes.  Speed: full frames (trace + temporal + 3x
+    a-trous + present) of the 256^3 world at 1920x1080 from its spawn pose,
+    after the cache trained on the preceding frames.  Matched MSE: the MSE of
+    a 64-frame accumulation (the temporal history cap) of the cache form; the
+    plain form needs s* = var / (64 (MSE_cache - bias^2)) samples per frame to
+    reach it, i.e. s* times its path-tracing pass per frame."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+    torch.cuda.set_device(local)
+    ctx = vrt.Context(local)
+    K, WARM_TRAIN = 64, 256
+    forms = [("plain_2bounce", 2, None), ("plain_6bounce", 6, None), ("cache", 2, CACHE_CFG)]
+    quality = {}
+    for label, kind, n, seed, W, H, refname in CACHE_SCENES:
+        ref = np.load(ROOT / "tests" / "golden" / refname)["ref"].astype(np.float64)
+        vox, spawn = vrt.generate_scene(kind, n, seed)
+        sc = vrt.Scene(ctx, vox, n)
+        quality[label] = {name: cache_quality(vrt, ctx, sc, spawn, W, H, ref, b, c, WARM_TRAIN if c else 0, K)
+                          for name, b, c in forms}
+        quality[label]["resolution"] = f"{W}x{H}"
+        sc.close()
+    # speed at 1080p on the 256^3 world
+    W, H = 1920, 1080
+    vox, spawn = vrt.generate_scene(2, 256, 2)
+    sc = vrt.Scene(ctx, vox, 256)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    light = vrt.Lighting()
+    speed = {}
+    for name, b, c in forms:
+        s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0)
+        if c:
+            s.set_cache(**c)
+        s.set_timing(True)
+        warm = max(args.warmup, 3) + (64 if c else 0)
+        for f in range(warm):
+            s.frame(vrt.make_uniforms(spawn, None, light, f, b, 3, W, H, 1.0, 64.0))
+        rows = []
+        for f in range(warm, warm + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s.frame(vrt.make_uniforms(spawn, None, light, f, b, 3, W, H, 1.0, 64.0))
+            st = s.stats()
+            rows.append((st.ms_total, st.ms_pathtrace, st.ms_cache, st.rays, st.launches, st.cache_queries,
+                         st.cache_samples))
+        a = np.array(rows, np.float64)
+        speed[name] = {"frame_ms": round(float(a[:, 0].mean()), 4), "frame_ms_p50": round(float(np.median(a[:, 0])), 4),
+                       "frame_ms_p99": round(float(np.percentile(a[:, 0], 99)), 4),
+                       "pathtrace_ms": round(float(a[:, 1].mean()), 4), "cache_ms": round(float(a[:, 2].mean()), 4),
+                       "fps": round(1e3 / float(a[:, 0].mean()), 1), "rays_per_frame": round(float(a[:, 3].mean())),
+                       "mrays_s": round(float(a[:, 3].sum()) / (float(a[:, 0].sum()) / 1e3) / 1e6, 1),
+                       "launches_per_frame": round(float(a[:, 4].mean()), 1)}
+        if c:
+            speed[name]["queries_per_frame"] = round(float(a[:, 5].mean()))
+            speed[name]["training_samples_per_frame"] = round(float(a[:, 6].mean()))
+        s.close()
+    sc.close()
+    ctx.close()
+    # matched MSE (256^3 world quality, 1080p speed of the same view)
+    q = quality[CACHE_SCENES[1][0]]
+    target = q["cache"][f"mse_{K}frame_mean"]
+    matched = {}
+    for name in ("plain_2bounce", "plain_6bounce"):
+        var, bias2 = q[name]["var"], q[name]["bias2"]
+        sp = speed[name]
+        if target <= bias2:
+            matched[name] = {"spp_needed": None, "note": "the plain form's bias alone exceeds the cache form's MSE"}
+            continue
+        s_star = max(1.0, var / (K * (target - bias2)))
+        ms = s_star * sp["pathtrace_ms"] + (sp["frame_ms"] - sp["pathtrace_ms"])
+        matched[name] = {"spp_needed": round(s_star, 3), "frame_ms_at_matched_mse": round(ms, 4),
+                         "cache_speedup": round(ms / speed["cache"]["frame_ms"], 3)}
+    line = {
+        "metric": "1080p frames/s of cache-assisted vs plain path tracing at matched MSE (FP64 4096-spp reference)",
+        "mode": "cache", "value": speed["cache"]["fps"], "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": speed["cache"]["frame_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 path tracing; bf16 MLP with f32 accumulation",
+        "data": "synthetic (seeded procedural voxel worlds, static spawn camera)",
+        "config": {"workload": "256^3 world seed 2, 1920x1080, 1 spp, full frame (trace + temporal + 3x a-trous "
+                               "+ present), static spawn camera; quality on two scenes at the stated resolutions",
+                   "cache": CACHE_CFG, "quality_frames": K, "cache_training_frames_before_quality": WARM_TRAIN,
+                   "reference": "plain 6-bounce path, 4096 spp, FP64 accumulation (tests/golden)",
+                   "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
+        "quality": quality, "speed_1080p": speed, "matched_mse_64frame": matched,
+    }
+    print(json.dumps(line), flush=True)
+
+
 SERVE_RES = [((640, 360), 0.40), ((1280, 720), 0.35), ((1920, 1080), 0.20), ((2560, 1440), 0.05)]
 
 
@@ -597,6 +728,9 @@ def main():
     elif args.mode == "serve":
         if rank == 0:
             run_serve(args, local)
+    elif args.mode == "cache":
+        if rank == 0:
+            run_cache(args, local)
     else:
         run_ours(args, world, rank, local)
 

@@ -6,8 +6,10 @@ targets (main.js:335-360), and frame()/pass calls in the reference pass order
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import math
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -15,6 +17,26 @@ import numpy as np
 from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtCompletion,
                    VrtCacheConfig, VrtDeviceConfig, VrtEditBox, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
                    check, lib, ptr)
+
+# Live handles, closed in dependency order when the interpreter exits (objects
+# still alive at exit would otherwise be finalized in arbitrary order, after
+# parts of the runtime they need are gone).
+_LIVE = {k: weakref.WeakSet() for k in ("server", "batch", "cache", "session", "scene", "context")}
+
+
+def _track(kind: str, obj) -> None:
+    _LIVE[kind].add(obj)
+
+
+@atexit.register
+def _close_all() -> None:
+    for kind in ("server", "batch", "cache", "session", "scene", "context"):
+        for obj in list(_LIVE[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
 
 # Reference constants (scene.js:5-6, common.wgsl:11)
 VOXEL_SIZE = 1.0 / 16.0
@@ -109,6 +131,7 @@ class Context:
         h = C.c_void_p()
         check(lib.vrt_create(C.byref(cfg), C.byref(h)))
         self.h = h
+        _track("context", self)
 
     def synchronize(self) -> None:
         check(lib.vrt_ctx_synchronize(self.h))
@@ -143,6 +166,7 @@ class Scene:
             m = np.ascontiguousarray(masks, np.uint32)
             check(lib.vrt_scene_upload_prebuilt(ctx.h, ptr(voxels), ptr(b), ptr(m), int(n), C.byref(h)))
         self.h, self.ctx, self.n = h, ctx, n
+        _track("scene", self)
 
     def edit_box(self, x0, y0, z0, x1, y1, z1, value: int) -> None:
         check(lib.vrt_scene_edit_box(self.h, x0, y0, z0, x1, y1, z1, int(value) & 0xFFFFFFFF))
@@ -190,6 +214,7 @@ class Session:
         self.h, self.ctx, self.scene = h, ctx, scene
         self.w, self.h_px = int(width), int(height)
         self.accum_f32 = bool(accum_f32)
+        _track("session", self)
 
     # frame + passes --------------------------------------------------------
     def frame(self, u: VrtUniforms) -> None:
@@ -318,6 +343,7 @@ class Batch:
         h = C.c_void_p()
         check(lib.vrt_batch_create(ctx.h, arr, len(sessions), C.byref(h)))
         self.h, self.ctx, self.sessions = h, ctx, list(sessions)
+        _track("batch", self)
 
     def frame(self, uniforms: list) -> None:
         arr = (VrtUniforms * len(uniforms))(*uniforms)
@@ -363,6 +389,7 @@ class Server:
         check(lib.vrt_server_create(ctx.h, arr, len(sessions), int(max_in_flight), C.byref(h)))
         self.h, self.ctx, self.sessions = h, ctx, list(sessions)
         self._buf = (VrtCompletion * 4096)()
+        _track("server", self)
 
     def now(self) -> float:
         return float(lib.vrt_server_now(self.h))
@@ -417,6 +444,7 @@ class RadianceCache:
         h = C.c_void_p()
         check(lib.vrt_mlp_create(ctx.h, C.c_uint32(seed & 0xFFFFFFFF), C.byref(h)))
         self.h, self.ctx, self.extent = h, ctx, float(extent)
+        _track("cache", self)
 
     @staticmethod
     def _dp(t):
