@@ -127,3 +127,41 @@ def test_trained_cache_gains_over_plain_and_untrained(vrt):
     assert trained < 0.85 * plain2
     assert trained < 0.85 * untrained
     assert rays_c < rays2
+
+
+def test_cache_jobs_in_a_batch_match_alone(vrt):
+    """Cache-assisted sessions inside a batch (with a plain session beside
+    them): the first frame is bit-identical to each session rendered alone
+    (queries and predictions do not depend on the order the batch appends
+    them in); later frames agree within the training's summation-order noise."""
+    ctx = vrt.Context(0)
+    specs = [(vrt.VRT_SCENE_SMALL, 64, 1, 160, 90, True), (vrt.VRT_SCENE_RANDOM, 128, 7, 96, 64, False),
+             (vrt.VRT_SCENE_SMALL, 64, 2, 200, 120, True)]
+    alone, inb, poses = [], [], []
+    for kind, n, seed, W, H, cache in specs:
+        vox, spawn = vrt.generate_scene(kind, n, seed)
+        sc = vrt.Scene(ctx, vox, n)
+        a = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+        b = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True, path_kernel="batch_only")
+        if cache:
+            a.set_cache(seed=seed + 10)
+            b.set_cache(seed=seed + 10)
+        alone.append(a)
+        inb.append(b)
+        poses.append(spawn)
+    batch = vrt.Batch(ctx, inb)
+    for f in range(3):
+        us = [vrt.make_uniforms(poses[i], None, vrt.Lighting(), f, 2, 3, specs[i][3], specs[i][4])
+              for i in range(len(specs))]
+        batch.frame(us)
+        for i, s in enumerate(alone):
+            s.frame(us[i])
+        for i in range(len(specs)):
+            x, y = inb[i].radiance_f32(), alone[i].radiance_f32()
+            if f == 0 or not specs[i][5]:
+                np.testing.assert_array_equal(x, y)
+            else:
+                np.testing.assert_allclose(x, y, rtol=2e-2, atol=2e-3)
+            np.testing.assert_array_equal(inb[i].albedo(), alone[i].albedo())
+    st = batch.stats()
+    assert st.cache_queries > 0 and st.cache_samples > 0

@@ -55,8 +55,13 @@ def _run(cmd: list[str], verbose: bool) -> None:
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ...")
-    if verbose and (r.stdout or r.stderr):
-        print(r.stdout + r.stderr, flush=True)
+    out = r.stdout + r.stderr
+    if verbose and out:
+        print(out, flush=True)
+    elif "warning" in out:
+        # warnings are never silent (a host call of a device-only function,
+        # for one, compiles to a stub that ends the process at run time)
+        sys.stderr.write(out)
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

@@ -21,6 +21,7 @@ static_assert(offsetof(JobDev, out) == offsetof(JobHost, rad16), "job table layo
 static_assert(offsetof(JobDev, W) == offsetof(JobHost, W), "job table layouts differ");
 static_assert(offsetof(JobDev, acc_prev) == offsetof(JobHost, acc_prev), "job table layouts differ");
 static_assert(offsetof(JobDev, acc_f32) == offsetof(JobHost, acc_f32), "job table layouts differ");
+static_assert(offsetof(JobDev, cache) == offsetof(JobHost, cache), "job table layouts differ");
 
 // temporal.wgsl:17-77 over all jobs.
 __global__ void __launch_bounds__(256) k_b_temporal(MultiJob J, uint32_t P) {
@@ -68,13 +69,18 @@ __global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P) {
 
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
-                               cudaStream_t st, uint32_t* launches) {
+                               cudaStream_t st, uint32_t* launches, const CacheLaunch* cls, int ncl) {
   MultiJob J;
   J.jobs = (const JobDev*)d_jobs;
   J.firsts = d_firsts;
   J.n = n;
-  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr);
+  J.cache_jobs = ncl;
+  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n);
   if (e != cudaSuccess) return e;
+  // each cache job's inference, resolve and training, in job order
+  const WfDev b = wf_view(wb);
+  for (int k = 0; k < ncl; k++)
+    if ((e = launch_cache_post(J, b, cls[k], stats, st, launches)) != cudaSuccess) return e;
   const unsigned blocks = (P + 255) / 256;
   k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
   for (int it = 0; it < 3; it++) k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);

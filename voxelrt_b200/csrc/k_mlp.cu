@@ -394,12 +394,14 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ 
 __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict__ w, const float* __restrict__ q9,
                                                      const float* __restrict__ y3, int n_req,
                                                      const int* __restrict__ n_dev, int pop_cap, uint32_t seed,
-                                                     float extent, float* __restrict__ partial,
-                                                     float* __restrict__ loss, int* __restrict__ err) {
+                                                     const int* __restrict__ step, float extent,
+                                                     float* __restrict__ partial, float* __restrict__ loss,
+                                                     int* __restrict__ err) {
   using namespace mlp;
   int n, pop;
   bool draw;
   sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
+  if (step) seed ^= pcg_hash((uint32_t)*step + 0x6a09e667u);
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -510,13 +512,15 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict_
 }
 
 // grad[i] = sum over CTAs of partial[cta][i] / n  (fixed order: deterministic)
+// Thread 0 advances the Adam step counter (when the step has samples).
 __global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, int n_req, const int* __restrict__ n_dev,
-                             int pop_cap, float* __restrict__ grad) {
+                             int pop_cap, float* __restrict__ grad, int* __restrict__ step) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
   int n, pop;
   bool draw;
   mlp::sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
+  if (i == 0 && step && n > 0) *step += 1;
   const float inv_n = n > 0 ? 1.0f / (float)n : 0.0f;
   float s = 0.0f;
   for (int c = 0; c < ctas; c++) s += partial[(size_t)c * mlp::kParams + i];
@@ -526,10 +530,12 @@ __global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, int n_
 // Adam on fp32 masters; writes the bf16 copy.  Output columns >= 3 stay 0.
 __global__ void k_mlp_adam(float* __restrict__ wm, float* __restrict__ m, float* __restrict__ v,
                            const float* __restrict__ grad, uint16_t* __restrict__ wb, float lr, float b1, float b2,
-                           float eps, float bc1, float bc2, const int* __restrict__ n_dev) {
+                           float eps, const int* __restrict__ step, const int* __restrict__ n_dev) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
   if (n_dev && *n_dev <= 0) return;
+  const float t = (float)*step;
+  const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
   if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) { wm[i] = 0.0f; wb[i] = 0; return; }
   const float g = grad[i];
   const float mi = b1 * m[i] + (1.0f - b1) * g;
@@ -584,8 +590,8 @@ cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_d
 }
 
 cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
-                         int pop_cap, uint32_t draw_seed, float extent, float* partial, float* loss_ctas, int* err,
-                         float* grad, int* ctas_used, cudaStream_t st) {
+                         int pop_cap, uint32_t draw_seed, int* step, float extent, float* partial, float* loss_ctas,
+                         int* err, float* grad, int* ctas_used, cudaStream_t st) {
   if (n <= 0) return cudaErrorInvalidValue;
   static bool attr = false;
   if (!attr) {
@@ -595,20 +601,19 @@ cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, i
   }
   const int tiles = (n + 255) / 256;
   const int grid = std::min(tiles, sm_count_mlp());
-  k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(wb, q9, y3, n, n_dev, pop_cap, draw_seed, extent, partial,
+  k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(wb, q9, y3, n, n_dev, pop_cap, draw_seed, step, extent, partial,
                                                  loss_ctas, err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, n, n_dev, pop_cap, grad);
+  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, n, n_dev, pop_cap, grad, step);
   if (ctas_used) *ctas_used = grid;
   return cudaGetLastError();
 }
 
-cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
+cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, const int* step,
                      const int* n_dev, cudaStream_t st) {
   const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
-  const float bc1 = 1.0f - std::pow(b1, (float)step), bc2 = 1.0f - std::pow(b2, (float)step);
-  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, bc1, bc2, n_dev);
+  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, step, n_dev);
   return cudaGetLastError();
 }
 

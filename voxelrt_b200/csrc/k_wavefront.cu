@@ -51,23 +51,22 @@ static SingleJob make_job(const SceneDev& s, const VrtUniforms& uu, float fclamp
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
                              cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves,
-                             int* timed_waves, const CacheDev* cache) {
-  const SingleJob job = make_job(s, uu, fclamp, W, H, out);
+                             int* timed_waves, const CacheLaunch* cache, cudaEvent_t* cache_ev) {
+  SingleJob job = make_job(s, uu, fclamp, W, H, out);
+  std::memset(&job.cc, 0, sizeof job.cc);
+  if (cache) job.cc = cache->cd;
   // cache-assisted frames run as many waves as their training paths need
-  const int waves = (cache && cache->on ? (int)cache->train_bounces : (int)job.u.params0[1]) + 2;
+  const int waves = (job.cc.on ? (int)job.cc.train_bounces : (int)job.u.params0[1]) + 2;
   const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
   const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
-  return wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
-                         max_timed_waves, timed_waves, cache);
-}
-
-cudaError_t launch_cache_resolve(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
-                                 const PathOut& out, const WavefrontBufs& wb, const CacheDev& cc, const float* pred,
-                                 cudaStream_t st) {
-  const SingleJob job = make_job(s, uu, fclamp, W, H, out);
-  const int blocks = std::min((W * H + 255) / 256, wf_sm_count() * 8);
-  k_cache_resolve<SingleJob><<<blocks, 256, 0, st>>>(job, wf_view(wb), cc, pred, out.stats);
-  return cudaGetLastError();
+  cudaError_t e = wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
+                                  max_timed_waves, timed_waves);
+  if (e != cudaSuccess || !job.cc.on) return e;
+  if (cache_ev && (e = cudaEventRecord(cache_ev[0], st)) != cudaSuccess) return e;
+  e = launch_cache_post(job, wf_view(wb), *cache, out.stats, st, launches);
+  if (e != cudaSuccess) return e;
+  if (cache_ev) e = cudaEventRecord(cache_ev[1], st);
+  return e;
 }
 
 }  // namespace vrt

@@ -107,7 +107,10 @@ struct VrtSession {
   float* pred = nullptr;
   cudaEvent_t cev[2] = {};
   bool cache_timed = false;
+  uint64_t cache_version = 0;     // changes with every vrt_session_set_cache
 };
+
+constexpr int kMaxWaves = 72;   // wave counters allocated per wavefront scratch
 
 static int set_dev(VrtCtx* ctx) {
   CUDA_TRY(cudaSetDevice(ctx->device));
@@ -413,7 +416,7 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
   s->path_kernel = (cfg->path_kernel == VRT_PATH_MEGAKERNEL || cfg->path_kernel == VRT_PATH_BATCH_ONLY)
                        ? cfg->path_kernel : VRT_PATH_WAVEFRONT;
   if (!r && s->path_kernel == VRT_PATH_WAVEFRONT) {
-    const int max_waves = 72;
+    const int max_waves = kMaxWaves;
     s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves);
     r = dev_alloc(ctx, &s->wf_mem, s->wf_bytes, &s->bytes);
     if (!r) {
@@ -541,6 +544,7 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
 
 static int parity_of(const VrtSession* s) { return (int)(s->frame_counter & 1u); }
 static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o);
+static CacheLaunch cache_launch_of(VrtSession* s, uint32_t frame);
 
 int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
@@ -781,6 +785,8 @@ struct VrtBatch {
   cudaGraphExec_t gexec = nullptr;
   int graph_waves = -1;
   WavefrontTuning graph_tune;
+  uint64_t graph_cache_sig = 0;
+  uint32_t graph_launches = 0;
   cudaEvent_t ev_start = nullptr, ev_end = nullptr, ev_upload = nullptr;
   bool uploaded = false;
   uint32_t launches = 0;
@@ -910,9 +916,15 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
       if (ss[(size_t)q] == ss[(size_t)i]) return fail(VRT_ERR_INVALID, "session %d listed twice", k);
   }
   int maxB = 0;
+  uint64_t cache_sig = 0x9e3779b97f4a7c15ull;
   for (int i = 0; i < m; i++) {
-    if (int r = check_uniforms(ss[(size_t)i], &u[i])) return r;
-    maxB = std::max(maxB, (int)u[i].params0[1]);
+    VrtSession* s = ss[(size_t)i];
+    if (int r = check_uniforms(s, &u[i])) return r;
+    maxB = std::max(maxB, s->cache_on ? s->cache_cfg.train_bounces : (int)u[i].params0[1]);
+    if (s->cache_on && !s->mlp) return fail(VRT_ERR_STATE, "cache session without a network");
+    // the captured graph bakes each cache job's buffers and sizes in
+    const uint64_t v = s->cache_on ? (s->cache_version * 0x100000001b3ull) ^ (uint64_t)s->scene->dev.N : 0ull;
+    cache_sig = (cache_sig ^ (v + (uint64_t)i)) * 0x100000001b3ull;
   }
   const int waves = maxB + 2;
   if (waves + 1 > b->wf.max_waves) return fail(VRT_ERR_INVALID, "bounce count %d too large for a batch", maxB);
@@ -921,6 +933,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   // the staging tables may still be read by the previous frame's upload
   if (b->uploaded) CUDA_TRY(cudaEventSynchronize(b->ev_upload));
   uint32_t first = 0;
+  std::vector<CacheLaunch> cls;
   for (int i = 0; i < m; i++) {
     VrtSession* s = ss[(size_t)i];
     JobHost& j = b->h_jobs[i];
@@ -933,6 +946,10 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     j.W = s->W; j.H = s->H; j.first = first; j.fclamp = s->fclamp;
     j.acc_prev = s->accum[1 - p]; j.acc_cur = s->accum[p]; j.gbuf_prev = s->gbuf[1 - p];
     j.den0 = s->den[0]; j.den1 = s->den[1]; j.ldr = s->ldr; j.acc_f32 = s->acc_f32 ? 1 : 0;
+    if (s->cache_on) {
+      cls.push_back(cache_launch_of(s, u[i].params0[0]));
+      j.cache = cls.back().cd;
+    }
     b->h_firsts[i] = first;
     first += (uint32_t)(s->W * s->H);
   }
@@ -945,12 +962,14 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   CUDA_TRY(cudaEventRecord(b->ev_start, st));
   b->launches = 0;
   if (b->use_graph && full) {
-    if (!b->gexec || b->graph_waves != waves || !same_tuning(b->graph_tune, b->tune)) {
+    if (!b->gexec || b->graph_waves != waves || !same_tuning(b->graph_tune, b->tune) ||
+        b->graph_cache_sig != cache_sig) {
       batch_drop_graph(b);
       cudaGraph_t graph = nullptr;
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       uint32_t nl = 0;
-      cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl);
+      cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl,
+                                         cls.data(), (int)cls.size());
       cudaError_t e2 = cudaStreamEndCapture(st, &graph);
       if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -964,11 +983,14 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
       }
       b->graph_waves = waves;
       b->graph_tune = b->tune;
+      b->graph_cache_sig = cache_sig;
+      b->graph_launches = nl;
     }
-    b->launches = (uint32_t)(1 + 2 * waves + 5);
+    b->launches = b->graph_launches;
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
-    CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches));
+    CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches,
+                                cls.data(), (int)cls.size()));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
   for (int i = 0; i < m; i++) {
@@ -1006,6 +1028,13 @@ int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out) {
   out->voxel_reads = h[kStatVReads];
   out->pixels = h[kStatPixels];
   out->launches = b->launches;
+  out->cache_queries = h[kStatCacheQueries];
+  out->cache_samples = h[kStatCacheSamples];
+  for (VrtSession* s : b->sessions)
+    if (s->cache_on) {
+      out->cache_on = 1u;
+      if (int r = vrt_mlp_check(s->mlp)) return r;
+    }
   if (b->have_frame) {
     float ms = 0.0f;
     CUDA_TRY(cudaEventElapsedTime(&ms, b->ev_start, b->ev_end));
@@ -1289,9 +1318,9 @@ struct VrtMlp {
   uint16_t* wb = nullptr;   // bf16 copy read by the kernels
   float* partial = nullptr; // per-CTA gradient partials
   float* loss = nullptr;    // per-CTA loss sums
-  int* err = nullptr;
-  int step = 0;
+  int* err = nullptr;        // [0]: a tensor-core wait ran out; [1]: Adam step counter
   int P = 0, ctas = 0;
+  int* step() const { return err + 1; }
 };
 
 // He-normal initial weights from a PCG-hash stream (Box-Muller).
@@ -1353,8 +1382,8 @@ int vrt_mlp_set_params(VrtMlp* m, const float* host) {
   CUDA_TRY(cudaMemsetAsync(m->m, 0, P * 4, st));
   CUDA_TRY(cudaMemsetAsync(m->v, 0, P * 4, st));
   CUDA_TRY(mlp_to_bf16(m->wm, m->wb, st));
+  CUDA_TRY(cudaMemsetAsync(m->step(), 0, 4, st));
   CUDA_TRY(cudaStreamSynchronize(st));
-  m->step = 0;
   return VRT_OK;
 }
 
@@ -1424,10 +1453,12 @@ int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, floa
   return VRT_OK;
 }
 
-static int mlp_grad_impl(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* loss_out) {
+// advance: the reduction advances the Adam step counter (a training step follows).
+static int mlp_grad_impl(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* loss_out,
+                         bool advance) {
   int ctas = 0;
-  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, nullptr, n, 0u, extent, m->partial, m->loss, m->err, m->grad, &ctas,
-                        m->ctx->stream));
+  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, nullptr, n, 0u, advance ? m->step() : nullptr, extent, m->partial,
+                        m->loss, m->err, m->grad, &ctas, m->ctx->stream));
   if (loss_out) {
     std::vector<float> l((size_t)ctas);
     CUDA_TRY(cudaMemcpyAsync(l.data(), m->loss, (size_t)ctas * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
@@ -1443,7 +1474,7 @@ int vrt_mlp_gradient_device(VrtMlp* m, const float* d_q9, const float* d_y3, int
                             float* loss_out) {
   if (!m || n < 1 || !d_q9 || !d_y3 || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
   if (int r = set_dev(m->ctx)) return r;
-  if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, loss_out)) return r;
+  if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, loss_out, false)) return r;
   if (d_grad)
     CUDA_TRY(cudaMemcpyAsync(d_grad, m->grad, (size_t)m->P * 4, cudaMemcpyDeviceToDevice, m->ctx->stream));
   return mlp_check_err(m);
@@ -1455,9 +1486,8 @@ int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n,
     return fail(VRT_ERR_INVALID, "bad argument");
   if (int r = set_dev(m->ctx)) return r;
   for (int i = 0; i < steps; i++) {
-    if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, (loss_out && i == 0) ? loss_out : nullptr)) return r;
-    m->step++;
-    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step, nullptr, m->ctx->stream));
+    if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, (loss_out && i == 0) ? loss_out : nullptr, true)) return r;
+    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step(), nullptr, m->ctx->stream));
   }
   return VRT_OK;
 }
@@ -1480,17 +1510,18 @@ int vrt_session_cache_mlp(VrtSession* s, VrtMlp** out) {
 int vrt_session_set_cache(VrtSession* s, const VrtCacheConfig* cfg_in) {
   if (!s || !cfg_in) return fail(VRT_ERR_INVALID, "NULL argument");
   VrtCacheConfig cfg = *cfg_in;
+  s->cache_version++;
   if (!cfg.enabled) {
     s->cache_on = false;
     return VRT_OK;
   }
-  if (s->path_kernel != VRT_PATH_WAVEFRONT) return fail(VRT_ERR_STATE, "the cache needs the wavefront path kernel");
+  if (s->path_kernel == VRT_PATH_MEGAKERNEL) return fail(VRT_ERR_STATE, "the cache needs the wavefront path kernel");
   if (cfg.train_bounces == 0) cfg.train_bounces = 6;
   if (cfg.train_vertices == 0) cfg.train_vertices = 3;
   if (cfg.train_batch == 0) cfg.train_batch = 65536;
   if (cfg.train_steps == 0) cfg.train_steps = 1;
   if (cfg.learning_rate == 0.0f) cfg.learning_rate = 1e-2f;
-  if (cfg.train_bounces < 1 || cfg.train_bounces + 3 > s->wf.max_waves || cfg.train_vertices < 1 ||
+  if (cfg.train_bounces < 1 || cfg.train_bounces + 3 > kMaxWaves || cfg.train_vertices < 1 ||
       cfg.train_vertices > kCacheMaxRec || cfg.train_batch < 1 || cfg.train_batch > (1 << 22) ||
       cfg.train_steps < 0 || cfg.train_steps > 64 || !(cfg.learning_rate > 0.0f))
     return fail(VRT_ERR_INVALID, "cache configuration out of range");
@@ -1559,34 +1590,32 @@ int vrt_session_read_cache_samples(VrtSession* s, float* q9, float* y3, int cap,
   return VRT_OK;
 }
 
+// The post-wave work description of a cache session for frame `frame`.
+static CacheLaunch cache_launch_of(VrtSession* s, uint32_t frame) {
+  VrtMlp* m = s->mlp;
+  CacheLaunch cl;
+  cl.cd = s->cache;
+  cl.cd.on = 1;
+  cl.cd.phase = (frame * 7u) & 15u;   // 7 is odd: all 16 positions within 16 frames
+  cl.wb = m->wb; cl.wm = m->wm; cl.m = m->m; cl.v = m->v; cl.grad = m->grad;
+  cl.partial = m->partial; cl.loss = m->loss; cl.err = m->err; cl.step = m->step();
+  cl.pred = s->pred;
+  cl.P = s->W * s->H;
+  cl.extent = (float)s->scene->dev.N * 0.0625f;
+  cl.train_batch = s->cache_cfg.train_batch;
+  cl.train_steps = s->cache_cfg.train_steps;
+  cl.lr = s->cache_cfg.learning_rate;
+  return cl;
+}
+
 // One cache-assisted path-trace pass: waves (training + query paths),
 // inference over the queries, resolve, then the frame's training steps.
 static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o) {
-  cudaStream_t st = s->ctx->stream;
-  VrtMlp* m = s->mlp;
-  CacheDev d = s->cache;
-  d.on = 1;
-  const uint32_t frame = u->params0[0];
-  d.phase = (frame * 7u) & 15u;   // 7 is odd: all 16 positions within 16 frames
-  const int P = s->W * s->H;
-  const float extent = (float)s->scene->dev.N * 0.0625f;
-  CUDA_TRY(cudaMemsetAsync(d.qcount, 0, 8, st));
-  CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, st, &s->launches,
-                            s->timing ? s->tev : nullptr, VrtSession::kTimedWaves, &s->timed_waves, &d));
+  const CacheLaunch cl = cache_launch_of(s, u->params0[0]);
   s->cache_timed = s->timing;
-  if (s->timing) CUDA_TRY(cudaEventRecord(s->cev[0], st));
-  CUDA_TRY(mlp_infer(m->wb, d.qbuf, P, d.qcount, extent, s->pred, m->err, st));
-  CUDA_TRY(launch_cache_resolve(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, d, s->pred, st));
-  s->launches += 2;
-  for (int k = 0; k < s->cache_cfg.train_steps; k++) {
-    const uint32_t seed = frame * 0x9e3779b9u + (uint32_t)k * 0x85ebca6bu + 0x1234567u;
-    CUDA_TRY(mlp_gradient(m->wb, d.cand_q9, d.cand_y3, s->cache_cfg.train_batch, d.cand_count, d.cand_cap, seed,
-                          extent, m->partial, m->loss, m->err, m->grad, nullptr, st));
-    m->step++;
-    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, s->cache_cfg.learning_rate, m->step, d.cand_count, st));
-    s->launches += 3;
-  }
-  if (s->timing) CUDA_TRY(cudaEventRecord(s->cev[1], st));
+  CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
+                            &s->launches, s->timing ? s->tev : nullptr, VrtSession::kTimedWaves, &s->timed_waves,
+                            &cl, s->timing ? s->cev : nullptr));
   return VRT_OK;
 }
 

@@ -99,13 +99,34 @@ struct JobHost {
   uint32_t* ldr;
   int acc_f32;
   int pad[3];
+  CacheDev cache;
+};
+
+// Post-wave cache work of one job: its queries, network and training state.
+struct CacheLaunch {
+  CacheDev cd;
+  uint16_t* wb = nullptr;     // bf16 weights
+  float* wm = nullptr;        // fp32 masters
+  float* m = nullptr;
+  float* v = nullptr;
+  float* grad = nullptr;
+  float* partial = nullptr;
+  float* loss = nullptr;
+  int* err = nullptr;
+  int* step = nullptr;        // device Adam step counter
+  float* pred = nullptr;      // [P][3]
+  int P = 0;
+  float extent = 0.0f;
+  int train_batch = 0, train_steps = 0;
+  float lr = 0.0f;
 };
 
 // One batch frame over n jobs of P pixels in total: wavefront path trace
-// (waves = max bounces + 2), temporal, 3x a-trous, present.
+// (waves = max bounces + 2), the cache jobs' post-wave work, temporal,
+// 3x a-trous, present.
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
-                               cudaStream_t st, uint32_t* launches);
+                               cudaStream_t st, uint32_t* launches, const CacheLaunch* cls = nullptr, int ncl = 0);
 
 // Radiance-cache MLP kernels (k_mlp.cu).  q9: n x 9 floats (position in
 // metres, normal, albedo); y3: n x 3 target radiance; weights bf16 row-major.
@@ -119,11 +140,14 @@ cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_d
 // population is min(*n_dev, pop_cap) samples and a step uses min(population,
 // n) of them -- all of them in order when they fit, else n uniform draws
 // (with replacement) keyed by draw_seed.
+// (with replacement) keyed by draw_seed and the device step counter.  The
+// reduction increments *step (the Adam step) unless the step has no samples.
 cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
-                         int pop_cap, uint32_t draw_seed, float extent, float* partial, float* loss_ctas, int* err,
-                         float* grad, int* ctas_used, cudaStream_t st);
-// n_dev (may be null): the step is skipped when *n_dev == 0.
-cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, int step,
+                         int pop_cap, uint32_t draw_seed, int* step, float extent, float* partial, float* loss_ctas,
+                         int* err, float* grad, int* ctas_used, cudaStream_t st);
+// Adam step number *step (bias corrections from it); n_dev (may be null):
+// the step is skipped when *n_dev == 0.
+cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, const int* step,
                      const int* n_dev, cudaStream_t st);
 cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st);
 
@@ -133,16 +157,13 @@ int set_error(int code, const char* msg);
 size_t wavefront_bytes(int W, int H, int max_waves);
 // When trace_ev is non-null, events trace_ev[2w], trace_ev[2w+1] bracket the
 // trace kernel of wave w (w < max_timed_waves); *timed_waves receives the count.
-// cache (may be null): cache-assisted frame (training + query paths).
+// cache (may be null): cache-assisted frame (training + query paths),
+// followed by its post-wave work (events cache_ev[0..1] around it when given).
 cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                              const PathOut& out, const WavefrontBufs& wb, const WavefrontTuning& tune,
                              cudaStream_t st, uint32_t* launches, cudaEvent_t* trace_ev = nullptr,
-                             int max_timed_waves = 0, int* timed_waves = nullptr, const CacheDev* cache = nullptr);
-// Finishes the cache-terminated paths of a cache-assisted frame with the
-// network's predictions pred[3 * query].
-cudaError_t launch_cache_resolve(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
-                                 const PathOut& out, const WavefrontBufs& wb, const CacheDev& cc, const float* pred,
-                                 cudaStream_t st);
+                             int max_timed_waves = 0, int* timed_waves = nullptr, const CacheLaunch* cache = nullptr,
+                             cudaEvent_t* cache_ev = nullptr);
 
 cudaError_t launch_build_bricks(const SceneDev& s, int bx0, int by0, int bz0, int bx1, int by1, int bz1,
                                 cudaStream_t st);

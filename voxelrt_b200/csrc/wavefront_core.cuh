@@ -5,6 +5,7 @@
 #pragma once
 #include "vrt_device.cuh"
 #include "vrt_internal.h"
+#include <algorithm>
 #include <cstring>
 
 namespace vrt {
@@ -223,8 +224,11 @@ struct SingleJob {
   Uni u;
   DScene S;
   JobOut out;
+  CacheDev cc;             // radiance cache (cc.on == 0: plain path)
   float fclamp;
   int W, H;
+  __host__ __device__ bool any_cache() const { return cc.on != 0; }
+  VRT_DI const CacheDev& cache(int) const { return cc; }
   VRT_DI int job_of(uint32_t) const { return 0; }
   VRT_DI const Uni& uni(int) const { return u; }
   VRT_DI DScene scene(int) const { return S; }
@@ -252,6 +256,7 @@ struct JobDev {
   uint32_t* ldr;
   int acc_f32;
   int pad[3];
+  CacheDev cache;          // radiance cache of the job's session (cache.on == 0: plain path)
 };
 
 // Many sessions: job table in device memory, job found by binary search on
@@ -260,6 +265,9 @@ struct MultiJob {
   const JobDev* jobs;
   const uint32_t* firsts;  // n entries, ascending
   int n;
+  int cache_jobs;          // jobs with the cache on
+  __host__ __device__ bool any_cache() const { return cache_jobs != 0; }
+  VRT_DI const CacheDev& cache(int j) const { return jobs[j].cache; }
   VRT_DI int job_of(uint32_t g) const {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
@@ -318,22 +326,35 @@ VRT_DI float cache_target(float rfin, float rk, float tpk, float clampv) {
 // the radiance the path gathered after vertex k's emission pickup per unit
 // of the throughput that reached it, (R_final - R_k) / tp_k -- the reflected
 // radiance estimate at x_k.  Warp-aggregated append; all 32 lanes call.
+// When the warp's lanes belong to different jobs (batches) each lane
+// appends with its own atomic.
 VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nrec = fin ? c.rec_n[ti] : 0;
-  int incl = nrec;
+  const unsigned any = __ballot_sync(full, nrec > 0);
+  if (!any) return;
+  // one job among the lanes with samples?
+  const unsigned long long key = (unsigned long long)c.cand_count;
+  const unsigned grp = __match_any_sync(full, nrec > 0 ? key : 0ull) & any;
+  const bool one_job = nrec > 0 ? grp == any : true;
+  int slot = 0;
+  if (__all_sync(full, one_job)) {
+    int incl = nrec;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    const int leader = __ffs(any) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(c.cand_count, total);
+    base = __shfl_sync(full, base, leader);
+    slot = base + incl - nrec;
+  } else if (nrec > 0) {
+    slot = atomicAdd(c.cand_count, nrec);
   }
-  const int total = __shfl_sync(full, incl, 31);
-  if (total == 0) return;
-  int base = 0;
-  if (lane == 31) base = atomicAdd(c.cand_count, total);
-  base = __shfl_sync(full, base, 31);
-  int slot = base + incl - nrec;
   for (int k = 0; k < nrec && slot < c.cand_cap; k++, slot++) {
     const float4* r = c.rec + ((size_t)ti * kCacheMaxRec + k) * 4;
     const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
@@ -350,7 +371,13 @@ VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin
 
 // Appends a cache query of path g at its vertex 1.  All 32 lanes call.
 VRT_DI void cache_emit_query(const CacheDev& c, bool q, uint32_t g, F3 pos, F3 n, F3 alb) {
-  const uint32_t slot = warp_append(c.qcount, q);
+  const unsigned full = 0xffffffffu;
+  const unsigned any = __ballot_sync(full, q);
+  if (!any) return;
+  const unsigned grp = __match_any_sync(full, q ? (unsigned long long)c.qcount : 0ull) & any;
+  uint32_t slot;
+  if (__all_sync(full, q ? grp == any : true)) slot = warp_append(c.qcount, q);
+  else slot = q ? (uint32_t)atomicAdd(c.qcount, 1) : 0u;
   if (q) {
     float* d = c.qbuf + (size_t)slot * 9;
     d[0] = pos.x; d[1] = pos.y; d[2] = pos.z;
@@ -542,8 +569,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(J jobs, WfDev b, i
 
 // shade(0): primary hits over all pixels.
 template <class J>
-__global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, WfDev b, unsigned long long* stats,
-                                                          CacheDev cc) {
+__global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, WfDev b, unsigned long long* stats) {
+  const bool any_cache = jobs.any_cache();
+  const CacheDev* ccp = nullptr;
   const uint32_t stride = gridDim.x * blockDim.x;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + kStatPixels, (unsigned long long)P);
   for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += stride) {
@@ -577,6 +605,8 @@ __global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, Wf
         uint32_t rng = __float_as_uint(b.S0[g].w);
         F3 radiance = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
         const int W = jobs.width(j);
+        const CacheDev& cc = jobs.cache(j);
+        ccp = &cc;
         const int role = cache_role(cc, lp, W);
         const uint32_t kmax = role == kRolePlain ? u.params0[1] : (role == kRoleTrain ? cc.train_bounces : 1u);
         keep = shade_vertex(u, b, g, 0u, x1, n1, mat1, radiance, tp, rng, h.y, shadow, bounce, kmax,
@@ -588,13 +618,14 @@ __global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, Wf
       }
     }
     emit(b, 1, g, shadow, bounce, keep);
-    if (cc.on) cache_emit_samples(cc, fin_train, ti, rfin);
+    if (any_cache) cache_emit_samples(fin_train ? *ccp : jobs.cache(0), fin_train, ti, rfin);
   }
 }
 
 // shade(k), k >= 1: resolve vertex k-1's shadow ray, then the bounce hit.
 template <class J>
-__global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave, CacheDev cc) {
+__global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave) {
+  const bool any_cache = jobs.any_cache();
   const int n = b.ctr[4 * wave + 2];
   const uint32_t* list = active_of(b, wave);
   const int stride = gridDim.x * blockDim.x;
@@ -605,11 +636,14 @@ __global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave, Cac
     uint32_t ti = 0u;
     F3 rfin = f3(0.0f, 0.0f, 0.0f), qpos = rfin, qn = rfin, qalb = rfin;
     uint32_t g = 0u;
+    int jc = 0;
     if (i < n) {
       g = list[i];
       const int j = jobs.job_of(g);
+      jc = j;
       const uint32_t lp = g - jobs.first(j);
       const int W = jobs.width(j);
+      const CacheDev& cc = jobs.cache(j);
       const int role = cache_role(cc, lp, W);
       const float4 s0 = b.S0[g];
       const float4 s1 = b.S1[g];
@@ -654,10 +688,23 @@ __global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave, Cac
       }
     }
     emit(b, wave + 1, g, shadow, bounce, keep);
-    if (cc.on) {
+    if (any_cache) {
+      const CacheDev& cc = jobs.cache(jc);
       cache_emit_query(cc, query, g, qpos, qn, qalb);
       cache_emit_samples(cc, fin_train, ti, rfin);
     }
+  }
+}
+
+// Zeroes the per-frame query and sample counters of every cache job.
+template <class J>
+__global__ void k_cache_reset(J jobs, int njobs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const CacheDev& c = jobs.cache(j);
+  if (c.on) {
+    *c.qcount = 0;
+    *c.cand_count = 0;
   }
 }
 
@@ -703,6 +750,34 @@ inline int wf_sm_count() {
   return sms > 0 ? sms : 1;
 }
 
+// ---------------------------------------------------------------------------
+// host: post-wave cache work of one job -- inference over its queries, the
+// resolve of its cache-terminated paths, then its training steps.  Every
+// per-frame quantity (counts, Adam step, sample draws) lives on the device,
+// so the sequence can be captured in a CUDA graph and replayed.
+// ---------------------------------------------------------------------------
+template <class J>
+cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch& cl, unsigned long long* stats,
+                              cudaStream_t st, uint32_t* launches) {
+  cudaError_t e = mlp_infer(cl.wb, cl.cd.qbuf, cl.P, cl.cd.qcount, cl.extent, cl.pred, cl.err, st);
+  if (e != cudaSuccess) return e;
+  const int blocks = std::min((cl.P + 255) / 256, wf_sm_count() * 8);
+  k_cache_resolve<J><<<blocks, 256, 0, st>>>(jobs, b, cl.cd, cl.pred, stats);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  uint32_t nl = 2;
+  for (int k = 0; k < cl.train_steps; k++) {
+    e = mlp_gradient(cl.wb, cl.cd.cand_q9, cl.cd.cand_y3, cl.train_batch, cl.cd.cand_count, cl.cd.cand_cap,
+                     0x9e3779b9u * (uint32_t)(k + 1), cl.step, cl.extent, cl.partial, cl.loss, cl.err, cl.grad,
+                     nullptr, st);
+    if (e != cudaSuccess) return e;
+    e = mlp_adam(cl.wm, cl.m, cl.v, cl.grad, cl.wb, cl.lr, cl.step, cl.cd.cand_count, st);
+    if (e != cudaSuccess) return e;
+    nl += 3;
+  }
+  if (launches) *launches += nl;
+  return cudaSuccess;
+}
+
 template <class J, bool kSmem, int kMinBlocks>
 cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms, const WfDev& b, int w,
                             int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
@@ -726,18 +801,19 @@ template <class J>
 cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                             const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
                             uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
-                            const CacheDev* cache = nullptr) {
+                            int njobs = 1) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   const WfDev b = wf_view(wb);
-  CacheDev cc;
-  std::memset(&cc, 0, sizeof cc);
-  if (cache) cc = *cache;
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
   if (e != cudaSuccess) return e;
   const int sms = wf_sm_count();
   const int refill = tune.refill_min > 0 ? tune.refill_min : 12;
   const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 16);
   uint32_t nl = 0;
+  if (jobs.any_cache()) {
+    k_cache_reset<J><<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
+    nl++;
+  }
   k_wf_generate<J><<<(P + 255) / 256, 256, 0, st>>>(jobs, P, b);
   nl++;
   int timed = 0;
@@ -759,8 +835,8 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
     if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
     if (tm) timed++;
     nl++;
-    if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats, cc);
-    else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w, cc);
+    if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
+    else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
     nl++;
   }
   if (launches) *launches += nl;
