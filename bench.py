@@ -522,6 +522,90 @@ def cache_quality(vrt, ctx, scene, spawn, W, H, ref, bounces, cache, warm, K):
             "bias2": round(mk - var / K, 7)}
 
 
+def served_views(vrt, ctx, sc, spawn, flush, args, K, warm_train, views=16):
+    """`views` sessions of one scene at 480x270 (the reference image's view,
+    each with its own frame-index stream): batched with a cache per view
+    (quality + time), batched plain, and plain views one after another."""
+    import numpy as np
+    import torch
+
+    from voxelrt_b200.quality import hdr_image, mse
+    W, H = 480, 270
+    ref = np.load(ROOT / "tests" / "golden" / "cache_reference_256_480x270.npz")["ref"].astype(np.float64)
+    light = vrt.Lighting()
+
+    def uni(i, f, b, flags):
+        return vrt.make_uniforms(spawn, None, light, 100000 * i + f, b, flags, W, H, 1.0, 64.0)
+
+    out = {"views": views, "resolution": f"{W}x{H}"}
+    # batched with caches: quality (pass-level calls, no temporal) then timing (full frames)
+    ss = [vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True, path_kernel="batch_only")
+          for _ in range(views)]
+    for i, s in enumerate(ss):
+        s.set_cache(**dict(CACHE_CFG, seed=i + 1))
+    batch = vrt.Batch(ctx, ss)
+    for f in range(warm_train):
+        batch.frame([uni(i, f, 2, 0) for i in range(views)])
+    acc = [np.zeros_like(ref) for _ in range(views)]
+    for f in range(warm_train, warm_train + K):
+        batch.frame([uni(i, f, 2, 0) for i in range(views)])
+        for i, s in enumerate(ss):
+            acc[i] += hdr_image(s)
+    m = [mse(a / K, ref) for a in acc]
+
+    def time_batch(b, bounces, f0):
+        ms = []
+        for f in range(f0, f0 + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            b.frame([uni(i, f, bounces, 3) for i in range(views)])
+            ms.append(b.stats().ms_total)
+        return float(np.mean(ms))
+
+    ms_c = time_batch(batch, 2, warm_train + K)
+    out["batched_cache"] = {"mse_64frame_mean": round(float(np.mean(m)), 6), "mse_spread": [round(min(m), 6), round(max(m), 6)],
+                            "ms_per_batch": round(ms_c, 4), "views_per_s": round(views * 1e3 / ms_c, 1)}
+    batch.close()
+    for s in ss:
+        s.close()
+    # batched plain 2-bounce
+    ss = [vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, path_kernel="batch_only") for _ in range(views)]
+    batch = vrt.Batch(ctx, ss)
+    for f in range(max(args.warmup, 3)):
+        batch.frame([uni(i, f, 2, 3) for i in range(views)])
+    ms_p = time_batch(batch, 2, 100)
+    out["batched_plain_2bounce"] = {"ms_per_batch": round(ms_p, 4), "views_per_s": round(views * 1e3 / ms_p, 1)}
+    batch.close()
+    for s in ss:
+        s.close()
+    # plain views one after another
+    for b in (2, 6):
+        ss = [vrt.Session(ctx, sc, W, H, firefly_clamp=10.0) for _ in range(views)]
+        for s in ss:
+            s.set_timing(True)
+        for f in range(max(args.warmup, 3)):
+            for i, s in enumerate(ss):
+                s.frame(uni(i, f, b, 3))
+        tot, pt = [], []
+        for f in range(100, 100 + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t_all, p_all = 0.0, 0.0
+            for i, s in enumerate(ss):
+                s.frame(uni(i, f, b, 3))
+                st = s.stats()
+                t_all += st.ms_total
+                p_all += st.ms_pathtrace
+            tot.append(t_all)
+            pt.append(p_all)
+        out[f"sequential_plain_{b}bounce"] = {"ms_per_view": round(float(np.mean(tot)) / views, 4),
+                                              "pathtrace_ms_per_view": round(float(np.mean(pt)) / views, 4),
+                                              "views_per_s": round(views * 1e3 / float(np.mean(tot)), 1)}
+        for s in ss:
+            s.close()
+    return out
+
+
 def run_cache(args, local):
     """Cache-assisted path tracing against plain 2- and 6-bounce tracing.
 
@@ -583,6 +667,10 @@ def run_cache(args, local):
             speed[name]["queries_per_frame"] = round(float(a[:, 5].mean()))
             speed[name]["training_samples_per_frame"] = round(float(a[:, 6].mean()))
         s.close()
+    # served form: 16 views of the 256^3 world at the reference's 480x270, one
+    # batch frame for all of them, each view with its own cache; against the
+    # same views rendered one after another by plain sessions
+    served = served_views(vrt, ctx, sc, spawn, flush, args, K, WARM_TRAIN)
     sc.close()
     ctx.close()
     # matched MSE (256^3 world quality, 1080p speed of the same view)
@@ -599,6 +687,20 @@ def run_cache(args, local):
         ms = s_star * sp["pathtrace_ms"] + (sp["frame_ms"] - sp["pathtrace_ms"])
         matched[name] = {"spp_needed": round(s_star, 3), "frame_ms_at_matched_mse": round(ms, 4),
                          "cache_speedup": round(ms / speed["cache"]["frame_ms"], 3)}
+    # served form at matched MSE: plain views one after another at s* spp
+    sv = served
+    target_b = sv["batched_cache"]["mse_64frame_mean"]
+    for name in ("plain_2bounce", "plain_6bounce"):
+        var, bias2 = q[name]["var"], q[name]["bias2"]
+        seq = sv["sequential_" + name]
+        if target_b <= bias2:
+            sv["matched_" + name] = {"spp_needed": None}
+            continue
+        s_star = max(1.0, var / (K * (target_b - bias2)))
+        per_view = s_star * seq["pathtrace_ms_per_view"] + (seq["ms_per_view"] - seq["pathtrace_ms_per_view"])
+        sv["matched_" + name] = {"spp_needed": round(s_star, 3), "ms_per_view": round(per_view, 4),
+                                 "views_per_s": round(1e3 / per_view, 1),
+                                 "batched_cache_speedup": round(sv["batched_cache"]["views_per_s"] * per_view / 1e3, 3)}
     line = {
         "metric": "1080p frames/s of cache-assisted vs plain path tracing at matched MSE (FP64 4096-spp reference)",
         "mode": "cache", "value": speed["cache"]["fps"], "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
@@ -610,7 +712,7 @@ def run_cache(args, local):
                    "cache": CACHE_CFG, "quality_frames": K, "cache_training_frames_before_quality": WARM_TRAIN,
                    "reference": "plain 6-bounce path, 4096 spp, FP64 accumulation (tests/golden)",
                    "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
-        "quality": quality, "speed_1080p": speed, "matched_mse_64frame": matched,
+        "quality": quality, "speed_1080p": speed, "matched_mse_64frame": matched, "served_16_views": sv,
     }
     print(json.dumps(line), flush=True)
 
