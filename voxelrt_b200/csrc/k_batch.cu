@@ -77,10 +77,8 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   J.cache_jobs = ncl;
   cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n);
   if (e != cudaSuccess) return e;
-  // each cache job's inference, resolve and training, in job order
-  const WfDev b = wf_view(wb);
-  for (int k = 0; k < ncl; k++)
-    if ((e = launch_cache_post(J, b, cls[k], stats, st, launches)) != cudaSuccess) return e;
+  // the cache jobs' inference, resolve and training, all jobs per launch
+  if (ncl > 0 && (e = launch_cache_post(J, wf_view(wb), cls, ncl, stats, st, launches)) != cudaSuccess) return e;
   const unsigned blocks = (P + 255) / 256;
   k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
   for (int it = 0; it < 3; it++) k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);

@@ -346,39 +346,49 @@ __global__ void k_mlp_encode(const float* __restrict__ q9, int n, float extent, 
   for (int j = 0; j < mlp::kIn; j++) out[(size_t)i * mlp::kIn + j] = mlp::f2bf(f[j]);
 }
 
-// Inference: out[i*3 + c] = MLP(encode(q_i)).
-__global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ w, const float* __restrict__ q9,
-                                                   int n, const int* __restrict__ n_dev, float extent,
-                                                   float* __restrict__ out, int* __restrict__ err) {
-  if (n_dev) n = min(*n_dev, n);
+// The task of CTA b: tasks own contiguous CTA ranges [cta0, cta0 + ctas).
+__device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
+  int j = 0;
+  while (j + 1 < ts.n && b >= ts.t[j + 1].cta0) j++;
+  return j;
+}
+
+// Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set; a
+// task's CTAs stride over its 128-query tiles.
+__global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
+  const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
+  int n = tk.n_max;
+  if (tk.n_dev) n = min(*tk.n_dev, n);
+  const int tiles = (n + 127) / 128;
+  const int cb = blockIdx.x - tk.cta0;
+  if (cb >= tiles) return;   // nothing for this CTA (before any TMEM allocation)
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
   if (t == 0) umma::mbar_init(&mbar, 1);
-  mlp::load_weights(smem, w);
+  mlp::load_weights(smem, tk.wb);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   mlp::Ctl c{&mbar, 0u, true};
-  const int tiles = (n + 127) / 128;
-  for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
+  for (int tile = cb; tile < tiles && c.ok; tile += tk.ctas) {
     const int idx = tile * 128 + t;
-    mlp::stage_input(smem + mlp::kIA0, t, q9, n, idx, extent, idx);
+    mlp::stage_input(smem + mlp::kIA0, t, tk.q9, n, idx, tk.extent, idx);
     mlp::publish();
     float o[mlp::kOutPad];
     uint64_t mask[3];
     // activations ping-pong between the two buffers (A1 = IA1, A2 = IA0, A3 = IA1)
     mlp::forward_tile<1>(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, 0, o, mask);
     if (c.ok && idx < n)
-      for (int j = 0; j < mlp::kOut; j++) out[(size_t)idx * 3 + j] = o[j];
+      for (int j = 0; j < mlp::kOut; j++) tk.out3[(size_t)idx * 3 + j] = o[j];
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
   }
-  if (!c.ok && t == 0) atomicExch(err, 1);
+  if (!c.ok && t == 0) atomicExch(tk.err, 1);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 64);
@@ -391,17 +401,18 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const uint16_t* __restrict__ 
 // gradients of both groups accumulate in order into the same TMEM columns.
 // Input gradients dX = dH W^T read the forward weight copy MN-major; weight
 // gradients dW = X^T dH read the activation tiles MN-major (no transposes).
-__global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict__ w, const float* __restrict__ q9,
-                                                     const float* __restrict__ y3, int n_req,
-                                                     const int* __restrict__ n_dev, int pop_cap, uint32_t seed,
-                                                     const int* __restrict__ step, float extent,
-                                                     float* __restrict__ partial, float* __restrict__ loss,
-                                                     int* __restrict__ err) {
+__global__ void __launch_bounds__(256, 1) k_mlp_grad(const __grid_constant__ MlpTaskSet ts) {
   using namespace mlp;
+  const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
+  const int cb = blockIdx.x - tk.cta0;
+  const float* __restrict__ q9 = tk.q9;
+  const float* __restrict__ y3 = tk.y3;
+  const float extent = tk.extent;
   int n, pop;
   bool draw;
-  sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
-  if (step) seed ^= pcg_hash((uint32_t)*step + 0x6a09e667u);
+  sample_counts(tk.n_max, tk.n_dev, tk.pop_cap, n, pop, draw);
+  uint32_t seed = tk.seed;
+  if (tk.step) seed ^= pcg_hash((uint32_t)*tk.step + 0x6a09e667u);
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -409,7 +420,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict_
   const int t = threadIdx.x, warp = t >> 5, g = t >> 7, r = t & 127;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 512);
   if (t == 0) umma::mbar_init(&mbar, 1);
-  load_weights(smem, w);
+  load_weights(smem, tk.wb);
   for (int i = t; i < (kTrainSmem - kGEnd) / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(smem + kGEnd)[i] = 0u;
   umma::fence_before_sync();
   __syncthreads();
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict_
   float lsum = 0.0f;
   const int tiles = (n + 255) / 256;
   bool first = true;
-  for (int tile = blockIdx.x; tile < tiles && c.ok; tile += gridDim.x) {
+  for (int tile = cb; tile < tiles && c.ok; tile += tk.ctas) {
     const int idx = tile * 256 + t;
     const int src = idx < n ? sample_source(idx, pop, draw, seed) : 0;
     stage_input(mine + kGA0, r, q9, n, idx, extent, src);
@@ -479,7 +490,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict_
     first = false;
   }
   // partial gradients of this CTA: TMEM lane = input feature row, columns = outputs
-  float* pc = partial + (size_t)blockIdx.x * kParams;
+  float* pc = tk.partial + (size_t)cb * kParams;
   if (c.ok) {
     const int kin[4] = {kIn, kHid, kHid, kHid};
     const int nout[4] = {kHid, kHid, kHid, kOutPad};
@@ -503,47 +514,51 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const uint16_t* __restrict_
   if (t == 0) {
     float a = 0.0f;
     for (int i = 0; i < 8; i++) a += s_loss[i];
-    loss[blockIdx.x] = a;
-    if (!c.ok) atomicExch(err, 1);
+    tk.loss[cb] = a;
+    if (!c.ok) atomicExch(tk.err, 1);
   }
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 512);
 }
 
-// grad[i] = sum over CTAs of partial[cta][i] / n  (fixed order: deterministic)
-// Thread 0 advances the Adam step counter (when the step has samples).
-__global__ void k_mlp_reduce(const float* __restrict__ partial, int ctas, int n_req, const int* __restrict__ n_dev,
-                             int pop_cap, float* __restrict__ grad, int* __restrict__ step) {
+// grad[i] = sum over the task's CTAs of partial[cta][i] / n (fixed order:
+// deterministic); blockIdx.y = task.  Thread 0 advances the task's Adam step
+// counter when the step has samples.
+__global__ void k_mlp_reduce(const __grid_constant__ MlpTaskSet ts) {
+  const MlpTask& tk = ts.t[blockIdx.y];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
   int n, pop;
   bool draw;
-  mlp::sample_counts(n_req, n_dev, pop_cap, n, pop, draw);
-  if (i == 0 && step && n > 0) *step += 1;
+  mlp::sample_counts(tk.n_max, tk.n_dev, tk.pop_cap, n, pop, draw);
   const float inv_n = n > 0 ? 1.0f / (float)n : 0.0f;
+  if (i == 0 && tk.step && n > 0) *tk.step += 1;
   float s = 0.0f;
-  for (int c = 0; c < ctas; c++) s += partial[(size_t)c * mlp::kParams + i];
-  grad[i] = s * inv_n;
+  for (int c = 0; c < tk.ctas; c++) s += tk.partial[(size_t)c * mlp::kParams + i];
+  tk.grad[i] = s * inv_n;
 }
 
-// Adam on fp32 masters; writes the bf16 copy.  Output columns >= 3 stay 0.
-__global__ void k_mlp_adam(float* __restrict__ wm, float* __restrict__ m, float* __restrict__ v,
-                           const float* __restrict__ grad, uint16_t* __restrict__ wb, float lr, float b1, float b2,
-                           float eps, const int* __restrict__ step, const int* __restrict__ n_dev) {
+// Adam on fp32 masters (step number *step, bias corrections from it); writes
+// the bf16 copy.  Output columns >= 3 stay 0.  Skipped when the step had no
+// samples.  blockIdx.y = task.
+__global__ void k_mlp_adam(const __grid_constant__ MlpTaskSet ts, float b1, float b2, float eps) {
+  const MlpTask& tk = ts.t[blockIdx.y];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
-  if (n_dev && *n_dev <= 0) return;
-  const float t = (float)*step;
-  const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+  if (tk.n_dev && *tk.n_dev <= 0) return;
+  float* __restrict__ wm = tk.wm;
+  uint16_t* __restrict__ wb = tk.wbw;
   if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) { wm[i] = 0.0f; wb[i] = 0; return; }
-  const float g = grad[i];
-  const float mi = b1 * m[i] + (1.0f - b1) * g;
-  const float vi = b2 * v[i] + (1.0f - b2) * g * g;
-  m[i] = mi;
-  v[i] = vi;
+  const float t = (float)*tk.step;
+  const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+  const float g = tk.grad[i];
+  const float mi = b1 * tk.m[i] + (1.0f - b1) * g;
+  const float vi = b2 * tk.v[i] + (1.0f - b2) * g * g;
+  tk.m[i] = mi;
+  tk.v[i] = vi;
   const float mh = mi / bc1, vh = vi / bc2;
-  const float w = wm[i] - lr * mh / (sqrtf(vh) + eps);
+  const float w = wm[i] - tk.lr * mh / (sqrtf(vh) + eps);
   wm[i] = w;
   wb[i] = mlp::f2bf(w);
 }
@@ -574,46 +589,61 @@ cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cuda
   return cudaGetLastError();
 }
 
-cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_dev, float extent, float* out,
-                      int* err, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
+// Splits `total` CTAs over the tasks in proportion to their work (at least
+// one each, at most one per tile) and sets cta0/ctas; returns the grid.
+static int task_work(const MlpTask& t) {
+  const int w = (t.n_dev && t.pop_cap > 0) ? std::min(t.n_max, t.pop_cap) : t.n_max;
+  return std::max(w, 1);
+}
+
+static int assign_ctas(MlpTaskSet& ts, int total, int tile_samples) {
+  double work = 0.0;
+  for (int k = 0; k < ts.n; k++) work += (double)task_work(ts.t[k]);
+  int next = 0;
+  for (int k = 0; k < ts.n; k++) {
+    const int tiles = std::max(1, (task_work(ts.t[k]) + tile_samples - 1) / tile_samples);
+    int c = (int)((double)total * (double)task_work(ts.t[k]) / work);
+    c = std::max(1, std::min(c, tiles));
+    ts.t[k].cta0 = next;
+    ts.t[k].ctas = c;
+    next += c;
+  }
+  return next;
+}
+
+cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st) {
+  if (ts.n <= 0) return cudaSuccess;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kInferSmem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int tiles = (n + 127) / 128;
-  const int grid = std::min(tiles, sm_count_mlp() * 3);   // 3 x 72 KB of shared memory per SM
-  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(wb, q9, n, n_dev, extent, out, err);
+  const int grid = assign_ctas(ts, sm_count_mlp() * 3, 128);   // 3 x 72 KB of shared memory per SM
+  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(ts);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
-                         int pop_cap, uint32_t draw_seed, int* step, float extent, float* partial, float* loss_ctas,
-                         int* err, float* grad, int* ctas_used, cudaStream_t st) {
-  if (n <= 0) return cudaErrorInvalidValue;
+cudaError_t mlp_gradient_tasks(MlpTaskSet& ts, cudaStream_t st) {
+  if (ts.n <= 0) return cudaSuccess;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::kTrainSmem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int tiles = (n + 255) / 256;
-  const int grid = std::min(tiles, sm_count_mlp());
-  k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(wb, q9, y3, n, n_dev, pop_cap, draw_seed, step, extent, partial,
-                                                 loss_ctas, err);
+  // partial buffers hold mlp_max_ctas() rows per network
+  const int grid = assign_ctas(ts, sm_count_mlp(), 256);
+  k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(ts);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_mlp_reduce<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(partial, grid, n, n_dev, pop_cap, grad, step);
-  if (ctas_used) *ctas_used = grid;
+  k_mlp_reduce<<<dim3((mlp::kParams + 255) / 256, ts.n), 256, 0, st>>>(ts);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, const int* step,
-                     const int* n_dev, cudaStream_t st) {
-  const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
-  k_mlp_adam<<<(mlp::kParams + 255) / 256, 256, 0, st>>>(wm, m, v, grad, wb, lr, b1, b2, eps, step, n_dev);
+cudaError_t mlp_adam_tasks(const MlpTaskSet& ts, cudaStream_t st) {
+  if (ts.n <= 0) return cudaSuccess;
+  k_mlp_adam<<<dim3((mlp::kParams + 255) / 256, ts.n), 256, 0, st>>>(ts, 0.9f, 0.99f, 1e-8f);
   return cudaGetLastError();
 }
 

@@ -63,7 +63,7 @@ cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fcl
                                   max_timed_waves, timed_waves);
   if (e != cudaSuccess || !job.cc.on) return e;
   if (cache_ev && (e = cudaEventRecord(cache_ev[0], st)) != cudaSuccess) return e;
-  e = launch_cache_post(job, wf_view(wb), *cache, out.stats, st, launches);
+  e = launch_cache_post(job, wf_view(wb), cache, 1, out.stats, st, launches);
   if (e != cudaSuccess) return e;
   if (cache_ev) e = cudaEventRecord(cache_ev[1], st);
   return e;

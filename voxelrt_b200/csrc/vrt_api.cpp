@@ -1449,7 +1449,12 @@ int vrt_mlp_encode_device(VrtMlp* m, const float* d_q9, int n, float extent, uin
 int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, float* d_out3) {
   if (!m || n < 0 || (n && (!d_q9 || !d_out3)) || !(extent > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
   if (int r = set_dev(m->ctx)) return r;
-  CUDA_TRY(mlp_infer(m->wb, d_q9, n, nullptr, extent, d_out3, m->err, m->ctx->stream));
+  MlpTaskSet ts;
+  std::memset(&ts, 0, sizeof ts);
+  ts.n = 1;
+  MlpTask& t = ts.t[0];
+  t.wb = m->wb; t.q9 = d_q9; t.out3 = d_out3; t.n_max = n; t.extent = extent; t.err = m->err;
+  CUDA_TRY(mlp_infer_tasks(ts, m->ctx->stream));
   return VRT_OK;
 }
 
@@ -1457,8 +1462,15 @@ int vrt_mlp_infer_device(VrtMlp* m, const float* d_q9, int n, float extent, floa
 static int mlp_grad_impl(VrtMlp* m, const float* d_q9, const float* d_y3, int n, float extent, float* loss_out,
                          bool advance) {
   int ctas = 0;
-  CUDA_TRY(mlp_gradient(m->wb, d_q9, d_y3, n, nullptr, n, 0u, advance ? m->step() : nullptr, extent, m->partial,
-                        m->loss, m->err, m->grad, &ctas, m->ctx->stream));
+  MlpTaskSet ts;
+  std::memset(&ts, 0, sizeof ts);
+  ts.n = 1;
+  MlpTask& t = ts.t[0];
+  t.wb = m->wb; t.q9 = d_q9; t.y3 = d_y3; t.n_max = n; t.extent = extent; t.err = m->err;
+  t.step = advance ? m->step() : nullptr;
+  t.partial = m->partial; t.loss = m->loss; t.grad = m->grad;
+  CUDA_TRY(mlp_gradient_tasks(ts, m->ctx->stream));
+  ctas = ts.t[0].ctas;
   if (loss_out) {
     std::vector<float> l((size_t)ctas);
     CUDA_TRY(cudaMemcpyAsync(l.data(), m->loss, (size_t)ctas * 4, cudaMemcpyDeviceToHost, m->ctx->stream));
@@ -1487,7 +1499,12 @@ int vrt_mlp_train_device(VrtMlp* m, const float* d_q9, const float* d_y3, int n,
   if (int r = set_dev(m->ctx)) return r;
   for (int i = 0; i < steps; i++) {
     if (int r = mlp_grad_impl(m, d_q9, d_y3, n, extent, (loss_out && i == 0) ? loss_out : nullptr, true)) return r;
-    CUDA_TRY(mlp_adam(m->wm, m->m, m->v, m->grad, m->wb, lr, m->step(), nullptr, m->ctx->stream));
+    MlpTaskSet ts;
+    std::memset(&ts, 0, sizeof ts);
+    ts.n = 1;
+    MlpTask& t = ts.t[0];
+    t.step = m->step(); t.grad = m->grad; t.wm = m->wm; t.m = m->m; t.v = m->v; t.wbw = m->wb; t.lr = lr;
+    CUDA_TRY(mlp_adam_tasks(ts, m->ctx->stream));
   }
   return VRT_OK;
 }

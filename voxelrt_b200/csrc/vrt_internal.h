@@ -133,22 +133,47 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
 int mlp_num_params();
 int mlp_max_ctas();
 cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cudaStream_t st);
-// n_dev (may be null): the query count is read on the device, n is its upper bound.
-cudaError_t mlp_infer(const uint16_t* wb, const float* q9, int n, const int* n_dev, float extent, float* out,
-                      int* err, cudaStream_t st);
-// Sample selection: with n_dev null the n samples in order; otherwise the
-// population is min(*n_dev, pop_cap) samples and a step uses min(population,
-// n) of them -- all of them in order when they fit, else n uniform draws
-// (with replacement) keyed by draw_seed.
-// (with replacement) keyed by draw_seed and the device step counter.  The
-// reduction increments *step (the Adam step) unless the step has no samples.
-cudaError_t mlp_gradient(const uint16_t* wb, const float* q9, const float* y3, int n, const int* n_dev,
-                         int pop_cap, uint32_t draw_seed, int* step, float extent, float* partial, float* loss_ctas,
-                         int* err, float* grad, int* ctas_used, cudaStream_t st);
-// Adam step number *step (bias corrections from it); n_dev (may be null):
-// the step is skipped when *n_dev == 0.
-cudaError_t mlp_adam(float* wm, float* m, float* v, const float* grad, uint16_t* wb, float lr, const int* step,
-                     const int* n_dev, cudaStream_t st);
+// One network's share of an MLP launch.  A launch serves up to
+// kMaxMlpTasks networks (the sessions of a batch); the task table travels as
+// a kernel parameter, so a captured graph needs no table upload.
+struct MlpTask {
+  const uint16_t* wb;       // bf16 weights
+  const float* q9;          // inputs [n][9]: position (metres), normal, albedo
+  const float* y3;          // training targets [n][3]
+  float* out3;              // inference output [n][3]
+  const int* n_dev;         // count on the device (may be null: n_max is the count)
+  int n_max;                // inference: bound on *n_dev; training: samples per step
+  int pop_cap;              // training: population = min(*n_dev, pop_cap)
+  uint32_t seed;            // training: sample draws (mixed with *step)
+  float extent;             // world size in metres
+  int* step;                // Adam step counter (advanced by the reduction)
+  float* partial;           // per-CTA gradient partials [mlp_max_ctas()][params]
+  float* loss;              // per-CTA loss sums
+  float* grad;              // reduced gradient
+  float* wm;                // fp32 masters
+  float* m;
+  float* v;
+  uint16_t* wbw;            // bf16 copy written by Adam (= wb)
+  float lr;
+  int* err;                 // a bounded tensor-core wait ran out
+  int cta0, ctas;           // CTA range of the task (set by the launcher)
+};
+constexpr int kMaxMlpTasks = 48;
+struct MlpTaskSet {
+  int n;
+  int pad[3];
+  MlpTask t[kMaxMlpTasks];
+};
+// Inference over every task's queries (count *n_dev, bounded by n_max).
+cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st);
+// Gradient of every task (per-CTA partials, then the fixed-order reduction,
+// which advances *step when the step had samples).  Sample selection: with
+// n_dev null the n_max samples in order; otherwise the population is
+// min(*n_dev, pop_cap) samples and the step uses min(population, n_max) of
+// them -- all in order when they fit, else uniform draws with replacement.
+cudaError_t mlp_gradient_tasks(MlpTaskSet& ts, cudaStream_t st);
+// Adam step number *step of every task (skipped when *n_dev == 0).
+cudaError_t mlp_adam_tasks(const MlpTaskSet& ts, cudaStream_t st);
 cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st);
 
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.

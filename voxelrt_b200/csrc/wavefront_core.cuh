@@ -708,23 +708,40 @@ __global__ void k_cache_reset(J jobs, int njobs) {
   }
 }
 
-// Cache-terminated paths: radiance += throughput at vertex 1 * predicted
-// reflected radiance there, then the usual clamp / demodulation / store.
+// Cache-terminated paths of up to kMaxMlpTasks jobs (blockIdx.y = entry):
+// radiance += throughput at vertex 1 * predicted reflected radiance there,
+// then the usual clamp / demodulation / store.
+struct ResolveEntry {
+  const int* qcount;
+  const uint32_t* qpix;
+  const int* cand_count;
+  const float* pred;
+  int cand_cap;
+  int pad;
+};
+struct ResolveSet {
+  int n;
+  int pad[3];
+  ResolveEntry e[kMaxMlpTasks];
+};
+
 template <class J>
-__global__ void __launch_bounds__(256) k_cache_resolve(J jobs, WfDev b, CacheDev cc, const float* __restrict__ pred,
+__global__ void __launch_bounds__(256) k_cache_resolve(J jobs, WfDev b, const __grid_constant__ ResolveSet rs,
                                                        unsigned long long* stats) {
-  const int n = *cc.qcount;
+  const ResolveEntry& r = rs.e[blockIdx.y];
+  const int n = *r.qcount;
   if (stats && blockIdx.x == 0 && threadIdx.x == 0) {
     atomicAdd(stats + kStatCacheQueries, (unsigned long long)n);
-    atomicAdd(stats + kStatCacheSamples, (unsigned long long)min(*cc.cand_count, cc.cand_cap));
+    atomicAdd(stats + kStatCacheSamples, (unsigned long long)min(*r.cand_count, r.cand_cap));
   }
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const uint32_t g = cc.qpix[i];
+    const uint32_t g = r.qpix[i];
     const int j = jobs.job_of(g);
     const float4 s0 = b.S0[g];
     const float4 s1 = b.S1[g];
-    const F3 L = f3(fmax_(pred[3 * i], 0.0f), fmax_(pred[3 * i + 1], 0.0f), fmax_(pred[3 * i + 2], 0.0f));
+    const float* p = r.pred + 3 * (size_t)i;
+    const F3 L = f3(fmax_(p[0], 0.0f), fmax_(p[1], 0.0f), fmax_(p[2], 0.0f));
     const F3 radiance = xyz(s0) + xyz(s1) * L;
     finalize(jobs.outs(j), g - jobs.first(j), radiance, __float_as_uint(s1.w), jobs.clamp(j));
   }
@@ -756,23 +773,75 @@ inline int wf_sm_count() {
 // per-frame quantity (counts, Adam step, sample draws) lives on the device,
 // so the sequence can be captured in a CUDA graph and replayed.
 // ---------------------------------------------------------------------------
+// The MLP task of a cache job: inference (k < 0) or training step k.
+inline MlpTask mlp_task_of(const CacheLaunch& cl, int k) {
+  MlpTask t;
+  std::memset(&t, 0, sizeof t);
+  t.wb = cl.wb;
+  t.extent = cl.extent;
+  t.err = cl.err;
+  if (k < 0) {
+    t.q9 = cl.cd.qbuf;
+    t.out3 = cl.pred;
+    t.n_dev = cl.cd.qcount;
+    t.n_max = cl.P;
+  } else {
+    t.q9 = cl.cd.cand_q9;
+    t.y3 = cl.cd.cand_y3;
+    t.n_dev = cl.cd.cand_count;
+    t.n_max = cl.train_batch;
+    t.pop_cap = cl.cd.cand_cap;
+    t.seed = 0x9e3779b9u * (uint32_t)(k + 1);
+    t.step = cl.step;
+    t.partial = cl.partial;
+    t.loss = cl.loss;
+    t.grad = cl.grad;
+    t.wm = cl.wm;
+    t.m = cl.m;
+    t.v = cl.v;
+    t.wbw = cl.wb;
+    t.lr = cl.lr;
+  }
+  return t;
+}
+
+// Post-wave cache work of `n` jobs, up to kMaxMlpTasks per launch: one
+// inference launch over all their queries, one resolve launch, then per
+// training step one gradient (+ reduction) and one Adam launch serving every
+// job that still has steps to take.
 template <class J>
-cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch& cl, unsigned long long* stats,
-                              cudaStream_t st, uint32_t* launches) {
-  cudaError_t e = mlp_infer(cl.wb, cl.cd.qbuf, cl.P, cl.cd.qcount, cl.extent, cl.pred, cl.err, st);
-  if (e != cudaSuccess) return e;
-  const int blocks = std::min((cl.P + 255) / 256, wf_sm_count() * 8);
-  k_cache_resolve<J><<<blocks, 256, 0, st>>>(jobs, b, cl.cd, cl.pred, stats);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  uint32_t nl = 2;
-  for (int k = 0; k < cl.train_steps; k++) {
-    e = mlp_gradient(cl.wb, cl.cd.cand_q9, cl.cd.cand_y3, cl.train_batch, cl.cd.cand_count, cl.cd.cand_cap,
-                     0x9e3779b9u * (uint32_t)(k + 1), cl.step, cl.extent, cl.partial, cl.loss, cl.err, cl.grad,
-                     nullptr, st);
+cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch* cls, int n,
+                              unsigned long long* stats, cudaStream_t st, uint32_t* launches) {
+  uint32_t nl = 0;
+  for (int c0 = 0; c0 < n; c0 += kMaxMlpTasks) {
+    const int cn = std::min(kMaxMlpTasks, n - c0);
+    MlpTaskSet ts;
+    std::memset(&ts, 0, sizeof ts);
+    ResolveSet rs;
+    std::memset(&rs, 0, sizeof rs);
+    int maxP = 1, steps = 0;
+    for (int k = 0; k < cn; k++) {
+      const CacheLaunch& cl = cls[c0 + k];
+      ts.t[ts.n++] = mlp_task_of(cl, -1);
+      rs.e[rs.n++] = ResolveEntry{cl.cd.qcount, cl.cd.qpix, cl.cd.cand_count, cl.pred, cl.cd.cand_cap, 0};
+      maxP = std::max(maxP, cl.P);
+      steps = std::max(steps, cl.train_steps);
+    }
+    cudaError_t e = mlp_infer_tasks(ts, st);
     if (e != cudaSuccess) return e;
-    e = mlp_adam(cl.wm, cl.m, cl.v, cl.grad, cl.wb, cl.lr, cl.step, cl.cd.cand_count, st);
-    if (e != cudaSuccess) return e;
-    nl += 3;
+    const int bx = std::max(1, std::min((maxP + 255) / 256, wf_sm_count() * 8 / cn));
+    k_cache_resolve<J><<<dim3(bx, rs.n), 256, 0, st>>>(jobs, b, rs, stats);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    nl += 2;
+    for (int k = 0; k < steps; k++) {
+      MlpTaskSet tr;
+      std::memset(&tr, 0, sizeof tr);
+      for (int q = 0; q < cn; q++)
+        if (k < cls[c0 + q].train_steps) tr.t[tr.n++] = mlp_task_of(cls[c0 + q], k);
+      if ((e = mlp_gradient_tasks(tr, st)) != cudaSuccess) return e;
+      if ((e = mlp_adam_tasks(tr, st)) != cudaSuccess) return e;
+      nl += 3;
+    }
   }
   if (launches) *launches += nl;
   return cudaSuccess;
