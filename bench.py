@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--cache", action="store_true", help="serve: also run the sweep with the cache-assisted path")
     return ap.parse_args()
 
 
@@ -766,11 +767,55 @@ def run_serve(args, local):
         return u, [(int(lo[0]), int(lo[1]), int(lo[2]), int(lo[0] + size[0] - 1), int(lo[1] + size[1] - 1),
                     int(lo[2] + size[2] - 1), val)]
 
-    # warm-up: one request per session
-    for k in range(len(sessions)):
-        u, e = make_request(k)
-        server.submit(k, u, e)
-    server.drain()
+    def warm(rounds):
+        for _ in range(rounds):
+            for k in range(len(sessions)):
+                u, e = make_request(k)
+                server.submit(k, u, e)
+            server.drain()
+
+    warm(1)
+    results = sweep(args, server, sessions, make_request, rng)
+    forms = {"plain": results}
+    if args.cache:
+        # the same sessions switched to the cache-assisted path (one network each),
+        # trained on 32 frames per session before the sweep
+        for k, s in enumerate(sessions):
+            s.set_cache(**dict(CACHE_CFG, seed=k + 1))
+        warm(32)
+        forms["cache"] = sweep(args, server, sessions, make_request, rng)
+    px = sum(w * h for _, w, h in meta)
+    line = {
+        "metric": "served frames/s and p50/p99 frame latency under Poisson arrivals"
+                  + (" (plain and cache-assisted path)" if args.cache else " (plain path)"),
+        "mode": "serve", "value": max(r["frames_per_s"] for r in forms["cache" if args.cache else "plain"]),
+        "unit": "frames/s", "n_gpus": 1,
+        "higher_is_better": True, "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded worlds, cameras, edits, arrival times)",
+        "config": {"workload": "32 sessions, 360p 40% / 720p 35% / 1080p 20% / 1440p 5%, grids {128,256}^3, "
+                               "2 bounces, temporal+a-trous+present, one 1-4096 voxel box edit per request",
+                   "sessions": len(sessions), "session_pixels": px, "hbm_budget_gb": 150,
+                   "hbm_in_use_gb": round(ctx.bytes_in_use / 2 ** 30, 2), "max_in_flight": 2,
+                   "duration_s_per_rate": args.duration,
+                   "cache": CACHE_CFG if args.cache else None,
+                   "quality": "per-view MSE of both forms: bench.py --mode cache (FP64 4096-spp references)"},
+        "rates": results,
+    }
+    if args.cache:
+        line["forms"] = forms
+    print(json.dumps(line), flush=True)
+    server.close()
+    for s in sessions:
+        s.close()
+    for sc in scenes:
+        sc.close()
+    ctx.close()
+
+
+def sweep(args, server, sessions, make_request, rng):
+    """One run of Poisson arrivals per rate; latency = device completion -
+    arrival on the server clock."""
+    import numpy as np
     results = []
     for rate in [float(x) for x in args.rates.split(",")]:
         n_req = max(1, int(rate * args.duration))
@@ -797,26 +842,7 @@ def run_serve(args, local):
                         "latency_ms_p50": round(float(np.percentile(lat, 50)), 3),
                         "latency_ms_p99": round(float(np.percentile(lat, 99)), 3),
                         "latency_ms_mean": round(float(lat.mean()), 3)})
-    px = sum(w * h for _, w, h in meta)
-    line = {
-        "metric": "served frames/s and p50/p99 frame latency under Poisson arrivals (plain path)",
-        "mode": "serve", "value": max(r["frames_per_s"] for r in results), "unit": "frames/s", "n_gpus": 1,
-        "higher_is_better": True, "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded worlds, cameras, edits, arrival times)",
-        "config": {"workload": "32 sessions, 360p 40% / 720p 35% / 1080p 20% / 1440p 5%, grids {128,256}^3, "
-                               "2 bounces, temporal+a-trous+present, one 1-4096 voxel box edit per request",
-                   "sessions": len(sessions), "session_pixels": px, "hbm_budget_gb": 150,
-                   "hbm_in_use_gb": round(ctx.bytes_in_use / 2 ** 30, 2), "max_in_flight": 2,
-                   "duration_s_per_rate": args.duration},
-        "rates": results,
-    }
-    print(json.dumps(line), flush=True)
-    server.close()
-    for s in sessions:
-        s.close()
-    for sc in scenes:
-        sc.close()
-    ctx.close()
+    return results
 
 
 def main():
