@@ -45,7 +45,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
-    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache"],
+    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
                          "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
                          "path tracing at matched MSE")
@@ -523,6 +523,41 @@ def cache_quality(vrt, ctx, scene, spawn, W, H, ref, bounces, cache, warm, K):
             "bias2": round(mk - var / K, 7)}
 
 
+def run_cache_frame(args, local):
+    """The cache-assisted 1080p frame of the 256^3 world alone (static spawn
+    camera): `warmup` training frames, then `steps` timed frames.  A small
+    command for profiling the cache kernels."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+    torch.cuda.set_device(local)
+    ctx = vrt.Context(local)
+    vox, spawn = vrt.generate_scene(2, 256, 2)
+    sc = vrt.Scene(ctx, vox, 256)
+    W, H = 1920, 1080
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0)
+    s.set_cache(**CACHE_CFG)
+    s.set_timing(True)
+    light = vrt.Lighting()
+    for f in range(max(args.warmup, 3)):
+        s.frame(vrt.make_uniforms(spawn, None, light, f, 2, 3, W, H, 1.0, 64.0))
+    rows = []
+    for f in range(args.steps):
+        s.frame(vrt.make_uniforms(spawn, None, light, args.warmup + f, 2, 3, W, H, 1.0, 64.0))
+        st = s.stats()
+        rows.append((st.ms_total, st.ms_pathtrace, st.ms_cache, st.rays, st.cache_queries, st.cache_samples,
+                     st.launches))
+    a = np.array(rows, np.float64)
+    print(json.dumps({"mode": "cache-frame", "frame_ms": round(float(a[:, 0].mean()), 4),
+                      "pathtrace_ms": round(float(a[:, 1].mean()), 4), "cache_ms": round(float(a[:, 2].mean()), 4),
+                      "rays": int(a[:, 3].mean()), "queries": int(a[:, 4].mean()), "samples": int(a[:, 5].mean()),
+                      "launches": int(a[:, 6].mean())}), flush=True)
+    s.close()
+    sc.close()
+    ctx.close()
+
+
 def served_views(vrt, ctx, sc, spawn, flush, args, K, warm_train, views=16):
     """`views` sessions of one scene at 480x270 (the reference image's view,
     each with its own frame-index stream): batched with a cache per view
@@ -859,6 +894,9 @@ def main():
     elif args.mode == "cache":
         if rank == 0:
             run_cache(args, local)
+    elif args.mode == "cache-frame":
+        if rank == 0:
+            run_cache_frame(args, local)
     else:
         run_ours(args, world, rank, local)
 
