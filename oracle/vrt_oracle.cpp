@@ -98,10 +98,16 @@ inline void om_sincos(float x, float& s, float& c) {
 // 2^k for integer k in [-126, 127].
 inline float om_pow2i(int k) { return bitsf((uint32_t)(k + 127) << 23); }
 
-// e^r for |r| <= 0.35: Taylor series to r^7.
+// e^r for |r| <= 0.35: Taylor series to r^7, Horner steps as fused
+// multiply-adds (the kernels use the same fused steps).
 inline float om_exp_poly(float r) {
-  return 1.0f + r * (1.0f + r * (0.5f + r * (0.166666672f + r * (0.0416666679f +
-         r * (0.00833333377f + r * (0.00138888892f + r * 0.000198412701f))))));
+  float p = std::fmaf(r, 0.000198412701f, 0.00138888892f);
+  p = std::fmaf(r, p, 0.00833333377f);
+  p = std::fmaf(r, p, 0.0416666679f);
+  p = std::fmaf(r, p, 0.166666672f);
+  p = std::fmaf(r, p, 0.5f);
+  p = std::fmaf(r, p, 1.0f);
+  return std::fmaf(r, p, 1.0f);
 }
 
 // e^x: k = round(x log2 e), r = x - k ln2 (ln2 split into 0x3f317200 + LN2_LO).
@@ -111,8 +117,8 @@ inline float om_exp(float x) {
   const float LOG2E = 1.44269502f;
   const float LN2_HI = 0.693145751953125f;
   const float LN2_LO = 1.42860677e-06f;
-  float kf = std::floor(x * LOG2E + 0.5f);
-  float r = (x - kf * LN2_HI) - kf * LN2_LO;
+  float kf = std::floor(std::fmaf(x, LOG2E, 0.5f));
+  float r = std::fmaf(-kf, LN2_LO, std::fmaf(-kf, LN2_HI, x));
   return om_exp_poly(r) * om_pow2i((int)kf);
 }
 
@@ -137,8 +143,11 @@ inline float om_log2(float x) {
   if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
   float s = (m - 1.0f) / (m + 1.0f);
   float s2 = s * s;
-  float at = s + (s * s2) * (0.333333343f + s2 * (0.200000003f + s2 * (0.142857149f + s2 * 0.111111112f)));
-  return (float)e + at * 2.88539004f;
+  float q = std::fmaf(s2, 0.111111112f, 0.142857149f);
+  q = std::fmaf(s2, q, 0.200000003f);
+  q = std::fmaf(s2, q, 0.333333343f);
+  const float at = std::fmaf(s * s2, q, s);
+  return std::fmaf(at, 2.88539004f, (float)e);
 }
 
 // x^y for x >= 0, y > 0 (the only uses on this path); 0^y = 0.

@@ -125,6 +125,48 @@ VRT_DI float4 atrous_pixel(int W, int H, int px, int py, const void* __restrict_
   return make_float4(sr / den, sg / den, sb / den, center.w);
 }
 
+// atrous_pixel with the input staged in shared memory: sg = G-buffer tile,
+// sc = source tile in fp32 with its luminance in .w, ci = this pixel's index
+// in the tile (rows of RW pixels); taps outside the image hold zeros and
+// drop out through their zero normal weight.  Same arithmetic in the same
+// order as atrous_pixel.
+VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const float4* sc, int ci, int RW,
+                                int step) {
+  if (g.w < 0.0f) return center;
+  const float history = fmax_(center.w, 1.0f);
+  const float lumC = luminance(center.x, center.y, center.z);
+  const float sigmaL = fmax_(0.08f, 2.0f / __fsqrt_rn(history));
+  float sr = (center.x * 0.375f) * 0.375f;
+  float sg_ = (center.y * 0.375f) * 0.375f;
+  float sb = (center.z * 0.375f) * 0.375f;
+  float wSum = 0.140625f;
+  const float invD = 1.0f / (0.05f * g.w + 0.01f);
+  const float invS = 1.0f / sigmaL;
+#pragma unroll
+  for (int dy = -2; dy <= 2; dy++) {
+#pragma unroll
+    for (int dx = -2; dx <= 2; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      const int qi = ci + (dy * step) * RW + dx * step;
+      const float4 gq = sg[qi];
+      if (gq.w < 0.0f) continue;
+      const float nd = fmax_((g.x * gq.x + g.y * gq.y) + g.z * gq.z, 0.0f);
+      const float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;
+      if (n32 == 0.0f) continue;
+      const float4 cq = sc[qi];
+      const float wKernel = b3_weight(dx) * b3_weight(dy);
+      const float e = exp_(-(fabsf(g.w - gq.w) * invD + fabsf(lumC - cq.w) * invS));
+      const float w = (wKernel * n32) * e;
+      sr = sr + cq.x * w;
+      sg_ = sg_ + cq.y * w;
+      sb = sb + cq.z * w;
+      wSum = wSum + w;
+    }
+  }
+  const float den = fmax_(wSum, 1e-6f);
+  return make_float4(sr / den, sg_ / den, sb / den, center.w);
+}
+
 // present.wgsl:40-55 for one pixel: illum * sqrtAlb^2 * exposure -> ACES ->
 // pow(1/2.2), packed rgba8.
 VRT_DI uint32_t present_pixel(float exposure, float4 il, uint32_t a) {

@@ -125,7 +125,7 @@ constexpr int kGBase = kWEnd, kGEnd = kGBase + 2 * kGStride;
 constexpr int kTrainSmem = kGEnd + 1024;   // slack: MN-major views read up to 1 KB past a tile
 // inference kernel: forward weights + two activation buffers
 constexpr int kIA0 = kWEnd, kIA1 = kIA0 + 128 * kIn * 2, kIEnd = kIA1 + 128 * kIn * 2;
-constexpr int kInferSmem = kIEnd + 4096;
+constexpr int kInferSmem = kIEnd;
 
 // TMEM columns (fp32): layer outputs / input gradients of group g at 64 g,
 // weight gradients accumulated over all of a CTA's samples at kTW*
@@ -265,9 +265,9 @@ __device__ __forceinline__ void tmem_row(uint32_t tbase, uint32_t col, float* ou
 
 // Forward of G tiles of 128 samples (thread t: group t / 128, row t % 128):
 // activations written to A1..A3 (bf16) of the thread's group (group g's
-// tiles at +g * gstride), output o[16].  Returns the three hidden layers'
-// ReLU masks.  Thread 0 issues every group's MMAs.
-template <int G>
+// tiles at +g * gstride), output o[16].  With kMasks, returns the three
+// hidden layers' ReLU masks (training).  Thread 0 issues every group's MMAs.
+template <int G, bool kMasks>
 __device__ __forceinline__ void forward_tile(uint8_t* smem, uint32_t tbase, Ctl& c, int a_in, int a1, int a2, int a3,
                                              int gstride, float* o, uint64_t* mask) {
   const uint32_t s0 = umma::smem_u32(smem);
@@ -285,14 +285,17 @@ __device__ __forceinline__ void forward_tile(uint8_t* smem, uint32_t tbase, Ctl&
     sync_mma(c);
     float h[kHid];
     tmem_row<kHid>(tbase, tcol, h);
-    uint64_t m = 0;
+    if (kMasks) {
+      uint32_t lo = 0u, hi = 0u;
 #pragma unroll
-    for (int j = 0; j < kHid; j++) {
-      if (h[j] > 0.0f) m |= 1ull << j;
-      else h[j] = 0.0f;
+      for (int j = 0; j < 32; j++) lo |= (h[j] > 0.0f ? 1u : 0u) << j;
+#pragma unroll
+      for (int j = 0; j < 32; j++) hi |= (h[32 + j] > 0.0f ? 1u : 0u) << j;
+      mask[l] = ((uint64_t)hi << 32) | lo;
     }
+#pragma unroll
+    for (int j = 0; j < kHid; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
     store_row(smem + aout[l] + g * gstride, r, kHid, h);
-    mask[l] = m;
     publish();
   }
   if (t == 0)
@@ -310,6 +313,18 @@ __device__ __forceinline__ void stage_input(uint8_t* tile, int row, const float*
     float q[9];
 #pragma unroll
     for (int j = 0; j < 9; j++) q[j] = q9[(size_t)src * 9 + j];
+    encode(q, extent, f);
+  } else {
+#pragma unroll
+    for (int j = 0; j < kIn; j++) f[j] = 0.0f;
+  }
+  store_row(tile, row, kIn, f);
+}
+
+// As stage_input with the query already in registers (valid: row holds a sample).
+__device__ __forceinline__ void stage_query(uint8_t* tile, int row, const float* q, bool valid, float extent) {
+  float f[kIn];
+  if (valid) {
     encode(q, extent, f);
   } else {
 #pragma unroll
@@ -376,12 +391,17 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTa
   mlp::Ctl c{&mbar, 0u, true};
   for (int tile = cb; tile < tiles && c.ok; tile += tk.ctas) {
     const int idx = tile * 128 + t;
-    mlp::stage_input(smem + mlp::kIA0, t, tk.q9, n, idx, tk.extent, idx);
+    float q[9];
+    if (idx < n) {
+#pragma unroll
+      for (int j = 0; j < 9; j++) q[j] = __ldg(tk.q9 + (size_t)idx * 9 + j);
+    }
+    mlp::stage_query(smem + mlp::kIA0, t, q, idx < n, tk.extent);
     mlp::publish();
     float o[mlp::kOutPad];
     uint64_t mask[3];
     // activations ping-pong between the two buffers (A1 = IA1, A2 = IA0, A3 = IA1)
-    mlp::forward_tile<1>(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, 0, o, mask);
+    mlp::forward_tile<1, false>(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, 0, o, mask);
     if (c.ok && idx < n)
       for (int j = 0; j < mlp::kOut; j++) tk.out3[(size_t)idx * 3 + j] = o[j];
     umma::fence_before_sync();
@@ -433,21 +453,40 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const __grid_constant__ Mlp
   float lsum = 0.0f;
   const int tiles = (n + 255) / 256;
   bool first = true;
+  // the next tile's sample (query + target) is loaded one tile ahead, so its
+  // scattered read overlaps the current tile's tensor-core work
+  float qn[9], yn[3];
+  auto fetch = [&](int tile_) {
+    const int idx_ = tile_ * 256 + t;
+    if (tile_ < tiles && idx_ < n) {
+      const int src_ = sample_source(idx_, pop, draw, seed);
+#pragma unroll
+      for (int j = 0; j < 9; j++) qn[j] = __ldg(q9 + (size_t)src_ * 9 + j);
+#pragma unroll
+      for (int j = 0; j < 3; j++) yn[j] = __ldg(y3 + (size_t)src_ * 3 + j);
+    }
+  };
+  fetch(cb);
   for (int tile = cb; tile < tiles && c.ok; tile += tk.ctas) {
     const int idx = tile * 256 + t;
-    const int src = idx < n ? sample_source(idx, pop, draw, seed) : 0;
-    stage_input(mine + kGA0, r, q9, n, idx, extent, src);
+    float q[9], yv[3];
+#pragma unroll
+    for (int j = 0; j < 9; j++) q[j] = qn[j];
+#pragma unroll
+    for (int j = 0; j < 3; j++) yv[j] = yn[j];
+    fetch(tile + tk.ctas);
+    stage_query(mine + kGA0, r, q, idx < n, extent);
     publish();
     float o[kOutPad];
     uint64_t mask[3];
-    forward_tile<2>(smem, tbase, c, kGBase + kGA0, kGBase + kGA1, kGBase + kGA2, kGBase + kGA3, kGStride, o, mask);
+    forward_tile<2, true>(smem, tbase, c, kGBase + kGA0, kGBase + kGA1, kGBase + kGA2, kGBase + kGA3, kGStride, o, mask);
     // loss gradient dL/do (rows of padding samples are zero)
     float gy[kOutPad];
 #pragma unroll
     for (int j = 0; j < kOutPad; j++) {
       float gv = 0.0f;
       if (idx < n && j < kOut) {
-        const float d = o[j] - y3[(size_t)src * 3 + j];
+        const float d = o[j] - yv[j];
         const float den = o[j] * o[j] + 0.01f;
         gv = 2.0f * d / den;
         lsum += d * d / den;

@@ -587,7 +587,8 @@ int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int it) {
   const void* src = it == 0 ? s->accum[p] : (it == 1 ? s->den[0] : s->den[1]);
   const bool src_f32 = it == 0 && s->acc_f32;
   void* dst = it == 1 ? s->den[1] : s->den[0];
-  CUDA_TRY(launch_atrous(s->W, s->H, src, src_f32, s->gbuf[p], dst, 1 << it, s->ctx->stream));
+  CUDA_TRY(launch_atrous_staged(s->W, s->H, src, src_f32, s->gbuf[p], dst, 1 << it, s->stats + kStatError,
+                                s->ctx->stream));
   s->launches++;
   return VRT_OK;
 }
@@ -654,6 +655,7 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
   out->voxel_reads = h[kStatVReads];
   out->pixels = h[kStatPixels];
   out->launches = s->launches;
+  if (h[kStatError]) return fail(VRT_ERR_TIMEOUT, "a bounded wait for staged image tiles ran out");
   out->cache_on = s->cache_on ? 1u : 0u;
   out->cache_queries = h[kStatCacheQueries];
   out->cache_samples = h[kStatCacheSamples];

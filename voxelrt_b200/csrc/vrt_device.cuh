@@ -98,9 +98,16 @@ VRT_DI void sincos_(float x, float& s, float& c) {
 
 VRT_DI float pow2i_(int k) { return __uint_as_float((uint32_t)(k + 127) << 23); }
 
+// Horner steps as explicit fused multiply-adds (one rounding each; the CPU
+// restatement uses std::fmaf, so both sides round identically).
 VRT_DI float exp_poly_(float r) {
-  return 1.0f + r * (1.0f + r * (0.5f + r * (0.166666672f + r * (0.0416666679f +
-         r * (0.00833333377f + r * (0.00138888892f + r * 0.000198412701f))))));
+  float p = __fmaf_rn(r, 0.000198412701f, 0.00138888892f);
+  p = __fmaf_rn(r, p, 0.00833333377f);
+  p = __fmaf_rn(r, p, 0.0416666679f);
+  p = __fmaf_rn(r, p, 0.166666672f);
+  p = __fmaf_rn(r, p, 0.5f);
+  p = __fmaf_rn(r, p, 1.0f);
+  return __fmaf_rn(r, p, 1.0f);
 }
 
 VRT_DI float exp_(float x) {
@@ -109,8 +116,8 @@ VRT_DI float exp_(float x) {
   const float LOG2E = 1.44269502f;
   const float LN2_HI = 0.693145751953125f;
   const float LN2_LO = 1.42860677e-06f;
-  float kf = floorf(x * LOG2E + 0.5f);
-  float r = (x - kf * LN2_HI) - kf * LN2_LO;
+  float kf = floorf(__fmaf_rn(x, LOG2E, 0.5f));
+  float r = __fmaf_rn(-kf, LN2_LO, __fmaf_rn(-kf, LN2_HI, x));
   return exp_poly_(r) * pow2i_((int)kf);
 }
 
@@ -132,8 +139,11 @@ VRT_DI float log2_(float x) {
   if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
   float s = (m - 1.0f) / (m + 1.0f);
   float s2 = s * s;
-  float at = s + (s * s2) * (0.333333343f + s2 * (0.200000003f + s2 * (0.142857149f + s2 * 0.111111112f)));
-  return (float)e + at * 2.88539004f;
+  float q = __fmaf_rn(s2, 0.111111112f, 0.142857149f);
+  q = __fmaf_rn(s2, q, 0.200000003f);
+  q = __fmaf_rn(s2, q, 0.333333343f);
+  const float at = __fmaf_rn(s * s2, q, s);
+  return __fmaf_rn(at, 2.88539004f, (float)e);
 }
 
 VRT_DI float pow_(float x, float y) {

@@ -21,6 +21,7 @@ inline size_t occ_words(int BG) { return ((size_t)BG * BG * BG + 31) / 32; }
 // Per-frame counters written by the path kernel (u64 each).
 enum StatSlot {
   kStatRays = 0, kStatOuter, kStatInner, kStatVReads, kStatPixels, kStatCacheQueries, kStatCacheSamples,
+  kStatError,   // nonzero: a bounded wait on staged copies ran out
   kStatCount = 8
 };
 
@@ -202,6 +203,11 @@ cudaError_t launch_trace_rays(const SceneDev& s, const float* o, const float* d,
 cudaError_t launch_temporal(const VrtUniforms& u, int W, int H, const void* rad16, const void* gcur,
                             const void* acc_prev, const void* gprev, void* acc_out, bool acc_f32,
                             cudaStream_t st);
+// The a-trous iteration with its input tile staged by TMA (falls back to
+// launch_atrous when the buffers do not meet the copy constraints); err
+// (may be null) is set when a bounded wait for the copies ran out.
+cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
+                                 unsigned long long* err, cudaStream_t st);
 cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
                           cudaStream_t st);
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
