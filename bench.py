@@ -44,6 +44,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cache-compare", action="store_true",
+                    help="frame mode: skip the plain vs batched+cache comparison in the output line")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
@@ -296,11 +298,17 @@ def run_ours(args, world, rank, local):
         line["clocks"] = clk
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(vox, spawn, vrt)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     sess.close()
     scene.close()
     ctx.close()
+    if rank == 0 and world == 1 and not args.no_cache_compare:
+        # the metric's second half: plain vs batched + cache at equal MSE
+        import copy
+        a2 = copy.copy(args)
+        a2.steps = min(args.steps, 10)
+        line["plain_vs_batched_cache"] = cache_summary(cache_comparison(a2, local))
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -643,6 +651,32 @@ def served_views(vrt, ctx, sc, spawn, flush, args, K, warm_train, views=16):
 
 
 def run_cache(args, local):
+    """`--mode cache`: prints cache_comparison's full result."""
+    print(json.dumps(cache_comparison(args, local)), flush=True)
+
+
+def cache_summary(c):
+    """The headline figures of cache_comparison for the default bench line."""
+    q = c["quality"][CACHE_SCENES[1][0]]
+    sv = c["served_16_views"]
+    return {
+        "metric": "frames/s at matched MSE (64-frame accumulation vs a 4096-spp FP64 plain 6-bounce reference), "
+                  "cache-assisted over plain",
+        "mse_64frame_256world_480x270": {k: q[k]["mse_64frame_mean"] for k in ("plain_2bounce", "plain_6bounce",
+                                                                                "cache")},
+        "single_1080p": {"fps": {k: c["speed_1080p"][k]["fps"] for k in c["speed_1080p"]},
+                         "speedup_at_matched_mse": {k: v.get("cache_speedup") for k, v in
+                                                    c["matched_mse_64frame"].items()}},
+        "served_16_views_batched": {"views_per_s": sv["batched_cache"]["views_per_s"],
+                                    "mse_64frame": sv["batched_cache"]["mse_64frame_mean"],
+                                    "speedup_at_matched_mse_vs_views_one_after_another": {
+                                        k: sv["matched_" + k].get("batched_cache_speedup")
+                                        for k in ("plain_2bounce", "plain_6bounce")}},
+        "details": "bench.py --mode cache",
+    }
+
+
+def cache_comparison(args, local):
     """Cache-assisted path tracing against plain 2- and 6-bounce tracing.
 
     Quality: MSE against a 4096-spp FP64 plain 6-bounce reference (committed
@@ -750,7 +784,7 @@ def run_cache(args, local):
                    "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
         "quality": quality, "speed_1080p": speed, "matched_mse_64frame": matched, "served_16_views": sv,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 SERVE_RES = [((640, 360), 0.40), ((1280, 720), 0.35), ((1920, 1080), 0.20), ((2560, 1440), 0.05)]
