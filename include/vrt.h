@@ -98,7 +98,10 @@ typedef struct VrtTuning {
   int refill_min;             /* idle lanes of a warp that trigger a refill    */
   int trace_blocks_per_sm;    /* persistent DDA blocks per SM (0 = max)        */
   int shade_blocks_per_sm;    /* shading kernel blocks per SM                  */
-  int trace_variant;          /* 0: free registers, 1/2: >= 5/6 blocks per SM   */
+  int trace_variant;          /* tracer variant: (DDA iterations per pass of the
+                                 warp bookkeeping, min blocks per SM) =
+                                 0: (8,5) default, 1: (6,5), 2: (6,4), 3: (4,4),
+                                 4: (2,1), 5: (1,1)                              */
 } VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,

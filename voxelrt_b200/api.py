@@ -142,6 +142,15 @@ class Context:
 
     def close(self) -> None:
         if self.h:
+            # objects of this context still open (a test that failed midway, a
+            # caller that forgot one) go first: they need the context to close
+            for kind in ("server", "batch", "cache", "session", "scene"):
+                for obj in list(_LIVE[kind]):
+                    if getattr(obj, "ctx", None) is self:
+                        try:
+                            obj.close()
+                        except Exception:
+                            pass
             lib.vrt_destroy(self.h)
             self.h = None
 

@@ -467,7 +467,7 @@ int vrt_session_get_tuning(VrtSession* s, VrtTuning* t) {
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 2)
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   s->tune.refill_min = t->refill_min ? t->refill_min : 12;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
@@ -489,7 +489,7 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
   if (int r = set_dev(s->ctx)) return r;
   cudaStream_t st = s->ctx->stream;
   static const int refills[] = {4, 8, 12, 16, 24};
-  static const int variants[] = {0, 1};
+  static const int variants[] = {0, 1, 2};
   static const int shades[] = {8, 16, 32};
   const WavefrontTuning keep = s->tune;
   WavefrontTuning win = keep;
@@ -886,7 +886,7 @@ int vrt_batch_set_graph(VrtBatch* b, int enable) {
 int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
   if (!b || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 2)
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   b->tune.refill_min = t->refill_min ? t->refill_min : 12;
   b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
@@ -1048,7 +1048,7 @@ int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out) {
 int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning* best, float* best_ms) {
   if (!b || !u || frames < 1) return fail(VRT_ERR_INVALID, "bad argument");
   static const int refills[] = {4, 8, 12, 16, 24};
-  static const int variants[] = {0, 1};
+  static const int variants[] = {0, 1, 2};
   static const int shades[] = {8, 16, 32};
   const WavefrontTuning keep = b->tune;
   const bool keep_graph = b->use_graph;

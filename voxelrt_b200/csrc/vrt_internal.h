@@ -74,7 +74,8 @@ struct WavefrontTuning {
   int refill_min = 12;          // idle lanes that trigger a warp refill
   int trace_blocks_per_sm = 0;  // 0 = occupancy maximum
   int shade_blocks_per_sm = 16;
-  int trace_variant = 0;        // 0: registers unconstrained, 1: >= 5 blocks/SM, 2: >= 6 blocks/SM
+  int trace_variant = 0;        // (DDA iterations per warp-bookkeeping pass, min blocks/SM):
+                                // 0: (8, 5)  1: (6, 5)  2: (6, 4)  3: (4, 4)  4: (2, 1)  5: (1, 1)
 };
 
 // Host mirror of the device job table entry (JobDev in wavefront_core.cuh):

@@ -490,9 +490,10 @@ __global__ void __launch_bounds__(256) k_wf_generate(J jobs, uint32_t P, WfDev b
 }
 
 // Persistent queue tracer.  kSmem: stage the (single) scene's occupancy
-// bitmap in shared memory.  kMinBlocks > 1 caps registers for occupancy.
-template <class J, bool kSmem, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(J jobs, WfDev b, int wave, int implicit_n,
+// bitmap in shared memory.  kSteps DDA iterations per pass of the warp
+// bookkeeping (idle-lane ballot, refill, drain check).
+template <class J, bool kSmem, int kSteps, int kMinB>
+__global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wave, int implicit_n,
                                                               int refill_min, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
   if (kSmem) {
@@ -539,7 +540,9 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_wf_trace(J jobs, WfDev b, i
       continue;
     }
     if (active) {
-      if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
+#pragma unroll
+      for (int k = 0; k < kSteps; k++)
+        if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
         const uint32_t g = entry & ~kShadowBit;
         uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + g);
@@ -847,10 +850,10 @@ cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch* 
   return cudaSuccess;
 }
 
-template <class J, bool kSmem, int kMinBlocks>
+template <class J, bool kSmem, int kSteps, int kMinB>
 cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms, const WfDev& b, int w,
                             int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
-  auto* fn = k_wf_trace<J, kSmem, kMinBlocks>;
+  auto* fn = k_wf_trace<J, kSmem, kSteps, kMinB>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -862,6 +865,24 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
   }
   fn<<<sms * per, 256, smem, st>>>(jobs, b, w, implicit_n, refill, stats);
   return cudaGetLastError();
+}
+
+// Tracer variants (the autotuner's trace_variant): DDA iterations per pass of
+// the warp bookkeeping x minimum resident blocks per SM (register cap).
+// Measured on the 1080p / 256^3 frame: 8 x 5 (48 registers) 1.66 ms of trace,
+// 6 x 5 1.67, 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98,
+// 1 x 1 2.20 ms.
+template <class J, bool kSmem>
+cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int sms, const WfDev& b, int w, int impl,
+                              int refill, unsigned long long* stats, cudaStream_t st) {
+  switch (variant) {
+    case 1: return wf_launch_trace<J, kSmem, 6, 5>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 2: return wf_launch_trace<J, kSmem, 6, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 3: return wf_launch_trace<J, kSmem, 4, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 4: return wf_launch_trace<J, kSmem, 2, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 5: return wf_launch_trace<J, kSmem, 1, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    default: return wf_launch_trace<J, kSmem, 8, 5>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+  }
 }
 
 // Launches generate + (trace, shade) x waves.  smem > 0 selects the
@@ -891,15 +912,8 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
     if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
     const int impl = w == 0 ? (int)P : 0;
     const int tb = tune.trace_blocks_per_sm;
-    if (smem > 0) {
-      if (tune.trace_variant == 1) e = wf_launch_trace<J, true, 5>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-      else if (tune.trace_variant == 2) e = wf_launch_trace<J, true, 6>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-      else e = wf_launch_trace<J, true, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    } else {
-      if (tune.trace_variant == 1) e = wf_launch_trace<J, false, 5>(jobs, 0, tb, sms, b, w, impl, refill, stats, st);
-      else if (tune.trace_variant == 2) e = wf_launch_trace<J, false, 6>(jobs, 0, tb, sms, b, w, impl, refill, stats, st);
-      else e = wf_launch_trace<J, false, 1>(jobs, 0, tb, sms, b, w, impl, refill, stats, st);
-    }
+    if (smem > 0) e = wf_dispatch_trace<J, true>(tune.trace_variant, jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    else e = wf_dispatch_trace<J, false>(tune.trace_variant, jobs, 0, tb, sms, b, w, impl, refill, stats, st);
     if (e != cudaSuccess) return e;
     if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
     if (tm) timed++;
