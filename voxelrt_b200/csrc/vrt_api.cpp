@@ -469,7 +469,7 @@ int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
       t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
     return fail(VRT_ERR_INVALID, "tuning out of range");
-  s->tune.refill_min = t->refill_min ? t->refill_min : 12;
+  s->tune.refill_min = t->refill_min ? t->refill_min : 8;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   s->tune.trace_variant = t->trace_variant;
@@ -888,7 +888,7 @@ int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
       t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
     return fail(VRT_ERR_INVALID, "tuning out of range");
-  b->tune.refill_min = t->refill_min ? t->refill_min : 12;
+  b->tune.refill_min = t->refill_min ? t->refill_min : 8;
   b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   b->tune.trace_variant = t->trace_variant;

@@ -71,7 +71,7 @@ struct CacheDev {
 
 // Launch-shape knobs of the wavefront tracer (chosen by the autotuner).
 struct WavefrontTuning {
-  int refill_min = 12;          // idle lanes that trigger a warp refill
+  int refill_min = 8;           // idle lanes that trigger a warp refill
   int trace_blocks_per_sm = 0;  // 0 = occupancy maximum
   int shade_blocks_per_sm = 16;
   int trace_variant = 0;        // (DDA iterations per warp-bookkeeping pass, min blocks/SM):

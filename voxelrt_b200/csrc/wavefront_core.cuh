@@ -871,7 +871,9 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 // the warp bookkeeping x minimum resident blocks per SM (register cap).
 // Measured on the 1080p / 256^3 frame: 8 x 5 (48 registers) 1.66 ms of trace,
 // 6 x 5 1.67, 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98,
-// 1 x 1 2.20 ms.
+// 1 x 1 2.20 ms.  (Stepping until enough lanes are idle, with a ballot after
+// every iteration, ran 1.88 ms: the per-iteration ballot costs more than the
+// idle lanes of a fixed pass.)
 template <class J, bool kSmem>
 cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int sms, const WfDev& b, int w, int impl,
                               int refill, unsigned long long* stats, cudaStream_t st) {
@@ -897,7 +899,7 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
   if (e != cudaSuccess) return e;
   const int sms = wf_sm_count();
-  const int refill = tune.refill_min > 0 ? tune.refill_min : 12;
+  const int refill = tune.refill_min > 0 ? tune.refill_min : 8;
   const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 16);
   uint32_t nl = 0;
   if (jobs.any_cache()) {
