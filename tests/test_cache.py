@@ -35,8 +35,8 @@ def test_cache_frame_matches_oracle(vrt, orc, frame, rec):
     den = pix["den"]
     # training paths and cache-terminated paths whose bounce left the scene: plain arithmetic
     plain = (role == 1) | ((role == 2) & (pix["has_query"] == 0))
-    want = np.minimum(pix["radiance"], f32(fclamp)) / den
-    np.testing.assert_allclose(got[plain], want[plain], rtol=1e-4, atol=1e-6)
+    want = np.minimum(pix["radiance"][plain], f32(fclamp)) / den[plain]
+    np.testing.assert_allclose(got[plain], want, rtol=1e-4, atol=1e-6)
     # cache-terminated paths: radiance + tp1 * max(prediction, 0)
     qm = (role == 2) & (pix["has_query"] == 1)
     q9 = pix["q9"][qm]
