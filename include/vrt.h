@@ -358,6 +358,11 @@ int vrt_session_read_cache_samples(VrtSession* s, float* q9, float* y3, int cap,
  * mode 1: D[K x N] = A[128 x K]^T B[128 x N]; mode 2: D[128 x N] = A[128 x K] B[K x N]
  * (B read MN-major).  A, B are bf16 bit patterns. */
 int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint16_t* B, float* D);
+/* No counterpart in the reference.  Exercises the failure path of the
+ * kernels' bounded waits: waits `spins` rounds on an mbarrier that nothing
+ * arrives on, with TMEM held.  Returns VRT_ERR_TIMEOUT (the expected outcome);
+ * the context stays usable. */
+int vrt_selftest_bounded_wait(unsigned int spins);
 
 /* ---- allocation-free denoise ------------------------------------------- */
 /* No counterpart in the reference.  The 3-iteration a-trous chain (steps

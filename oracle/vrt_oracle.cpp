@@ -646,7 +646,7 @@ void bilinear(Fetch fetch, int W, int H, float u, float v, float out[4]) {
   }
 }
 
-inline float luminance(const float* c) { return (c[0] * 0.2126f + c[1] * 0.7152f) + c[2] * 0.0722f; }
+inline float luminance(const float* c) { return std::fmaf(c[2], 0.0722f, std::fmaf(c[1], 0.7152f, c[0] * 0.2126f)); }
 
 }  // namespace
 
@@ -899,12 +899,12 @@ void orc_atrous(const void* uniforms, int Wd, int Hd, const void* src, int src_f
           const float* gq = gbuf + 4 * q;
           if (gq[3] < 0.0f) continue;
           float wKernel = K[std::abs(dx)] * K[std::abs(dy)];
-          float nd = fmaxf_((g[0] * gq[0] + g[1] * gq[1]) + g[2] * gq[2], 0.0f);
+          float nd = fmaxf_(std::fmaf(g[2], gq[2], std::fmaf(g[1], gq[1], g[0] * gq[0])), 0.0f);
           float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;   // pow(., 32)
           if (n32 == 0.0f) continue;   // zero weight: the tap adds nothing
-          float e = om_exp(-(std::fabs(g[3] - gq[3]) * invD + std::fabs(lumC - luminance(cq)) * invS));
+          float e = om_exp(-std::fmaf(std::fabs(g[3] - gq[3]), invD, std::fabs(lumC - luminance(cq)) * invS));
           float w = (wKernel * n32) * e;
-          for (int c = 0; c < 3; c++) sum[c] = sum[c] + cq[c] * w;
+          for (int c = 0; c < 3; c++) sum[c] = std::fmaf(cq[c], w, sum[c]);
           wSum = wSum + w;
         }
       }

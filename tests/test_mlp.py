@@ -170,3 +170,17 @@ def test_mlp_rejects_bad_arguments(vrt, cache):
     assert lib.vrt_mlp_train_device(cache.h, C.c_void_p(q.data_ptr()), C.c_void_p(y.data_ptr()), 0,
                                     C.c_float(16.0), C.c_float(1e-3), 1, None) != 0
     assert lib.vrt_mlp_infer_device(cache.h, C.c_void_p(q.data_ptr()), 1, C.c_float(0.0), C.c_void_p(y.data_ptr())) != 0
+
+
+def test_bounded_wait_runs_out_and_context_survives(vrt, cache):
+    """A wait that nothing completes gives up after its bound, reports
+    VRT_ERR_TIMEOUT through the status code, frees its TMEM, and the device
+    keeps working (an inference afterwards succeeds)."""
+    import torch
+    from voxelrt_b200._lib import lib
+    assert lib.vrt_selftest_bounded_wait(1000) == 6        # VRT_ERR_TIMEOUT
+    assert b"ran out" in lib.vrt_last_error_string()
+    q, _ = _queries(np.random.default_rng(9), 300)
+    out = torch.zeros(900, dtype=torch.float32, device="cuda")
+    cache.infer(_cuda(q), out)
+    assert torch.isfinite(out).all()

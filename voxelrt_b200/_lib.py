@@ -168,6 +168,7 @@ SIGNATURES = {
     "vrt_mlp_gradient_device": (I, [P, P, P, I, C.c_float, P, C.POINTER(C.c_float)]),
     "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
     "vrt_mlp_check": (I, [P]),
+    "vrt_selftest_bounded_wait": (I, [C.c_uint]),
     "vrt_session_set_cache": (I, [P, P]),
     "vrt_session_cache_mlp": (I, [P, C.POINTER(P)]),
     "vrt_session_read_cache_samples": (I, [P, P, P, I, C.POINTER(I)]),

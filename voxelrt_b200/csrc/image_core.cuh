@@ -108,16 +108,16 @@ VRT_DI float4 atrous_pixel(int W, int H, int px, int py, const void* __restrict_
       const size_t q = (size_t)qy * W + qx;
       const float4 gq = __ldg(gbuf + q);
       if (gq.w < 0.0f) continue;
-      const float nd = fmax_((g.x * gq.x + g.y * gq.y) + g.z * gq.z, 0.0f);
+      const float nd = fmax_(__fmaf_rn(g.z, gq.z, __fmaf_rn(g.y, gq.y, g.x * gq.x)), 0.0f);
       const float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;
       if (n32 == 0.0f) continue;
       const float4 cq = load_px(src, srcF32, q);
       const float wKernel = b3_weight(dx) * b3_weight(dy);
-      const float e = exp_(-(fabsf(g.w - gq.w) * invD + fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
+      const float e = exp_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
       const float w = (wKernel * n32) * e;
-      sr = sr + cq.x * w;
-      sg = sg + cq.y * w;
-      sb = sb + cq.z * w;
+      sr = __fmaf_rn(cq.x, w, sr);
+      sg = __fmaf_rn(cq.y, w, sg);
+      sb = __fmaf_rn(cq.z, w, sb);
       wSum = wSum + w;
     }
   }
@@ -150,16 +150,16 @@ VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const
       const int qi = ci + (dy * step) * RW + dx * step;
       const float4 gq = sg[qi];
       if (gq.w < 0.0f) continue;
-      const float nd = fmax_((g.x * gq.x + g.y * gq.y) + g.z * gq.z, 0.0f);
+      const float nd = fmax_(__fmaf_rn(g.z, gq.z, __fmaf_rn(g.y, gq.y, g.x * gq.x)), 0.0f);
       const float n2 = nd * nd, n4 = n2 * n2, n8 = n4 * n4, n16 = n8 * n8, n32 = n16 * n16;
       if (n32 == 0.0f) continue;
       const float4 cq = sc[qi];
       const float wKernel = b3_weight(dx) * b3_weight(dy);
-      const float e = exp_(-(fabsf(g.w - gq.w) * invD + fabsf(lumC - cq.w) * invS));
+      const float e = exp_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - cq.w) * invS));
       const float w = (wKernel * n32) * e;
-      sr = sr + cq.x * w;
-      sg_ = sg_ + cq.y * w;
-      sb = sb + cq.z * w;
+      sr = __fmaf_rn(cq.x, w, sr);
+      sg_ = __fmaf_rn(cq.y, w, sg_);
+      sb = __fmaf_rn(cq.z, w, sb);
       wSum = wSum + w;
     }
   }

@@ -696,6 +696,45 @@ cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st) {
 using namespace vrt;
 
 // Diagnostic of the tensor-core operand layouts (see k_umma_selftest).
+// The failure path of the bounded waits: an mbarrier that nothing arrives on,
+// waited on for `spins` try_wait rounds, with a TMEM allocation held across
+// the wait as the MLP kernels hold one.  The wait runs out, the kernel sets
+// the error flag, frees TMEM and returns.
+__global__ void __launch_bounds__(128) k_wait_selftest(uint32_t spins, int* __restrict__ err) {
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 32);
+  if (t == 0) umma::mbar_init(&mbar, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const bool ok = __syncthreads_and(umma::mbar_wait(&mbar, 0, spins) ? 1 : 0) != 0;
+  if (!ok && t == 0) atomicExch(err, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem_base, 32);
+}
+
+extern "C" int vrt_selftest_bounded_wait(unsigned int spins) {
+  if (spins == 0 || spins > (1u << 20)) return set_error(VRT_ERR_INVALID, "vrt_selftest_bounded_wait: spins out of range");
+  int* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, 4);
+  if (e != cudaSuccess) return set_error(VRT_ERR_OOM, cudaGetErrorString(e));
+  e = cudaMemset(d, 0, 4);
+  if (e == cudaSuccess) {
+    k_wait_selftest<<<1, 128>>>(spins, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, 4, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_error(VRT_ERR_CUDA, cudaGetErrorString(e));
+  if (h) return set_error(VRT_ERR_TIMEOUT, "vrt_selftest_bounded_wait: the wait ran out (expected)");
+  return VRT_OK;
+}
+
 extern "C" int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint16_t* B, float* D) {
   if (!A || !B || !D || mode < 0 || mode > 2 || N < 16 || N > 64 || N % 16 || K < 16 || K > 128 || K % 16)
     return set_error(VRT_ERR_INVALID, "vrt_mlp_selftest_gemm: bad argument");

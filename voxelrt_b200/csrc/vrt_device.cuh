@@ -400,6 +400,6 @@ VRT_DI int face_of(F3 n) {
   return -1;
 }
 
-VRT_DI float luminance(float r, float g, float b) { return (r * 0.2126f + g * 0.7152f) + b * 0.0722f; }
+VRT_DI float luminance(float r, float g, float b) { return __fmaf_rn(b, 0.0722f, __fmaf_rn(g, 0.7152f, r * 0.2126f)); }
 
 }  // namespace vrt
