@@ -655,15 +655,56 @@ def run_cache(args, local):
     print(json.dumps(cache_comparison(args, local)), flush=True)
 
 
+def quality_1080p(vrt, ctx, sc, spawn, forms, K, warm_train, ref_spp=4096):
+    """MSE of each form at the full workload size (1920x1080, 256^3 world,
+    static spawn camera) against a 4096-spp plain 6-bounce reference
+    accumulated in FP64 on the GPU (vrt_hdr_accumulate: bit-identical to the
+    CPU oracle's FP64 accumulation, tests/test_hdr.py).  Errors are summed on
+    the device."""
+    W, H = 1920, 1080
+    light = vrt.Lighting()
+    r = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+    t0 = time.perf_counter()
+    r.hdr_accum_reset()
+    r.hdr_accumulate(vrt.make_uniforms(spawn, None, light, 0, 6, 0, W, H), 1 << 20, ref_spp)
+    ref, count = r.hdr_accum()
+    ref_s = time.perf_counter() - t0
+    r.close()
+    ref32 = ref.astype("float32")
+    out = {"resolution": f"{W}x{H}", "reference": {"spp": count, "bounces": 6, "seconds": round(ref_s, 2)}}
+    for name, b, c in forms:
+        s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+        if c:
+            s.set_cache(**c)
+        s.set_hdr_reference(ref32)
+        w = warm_train if c else 0
+        for f in range(w):
+            s.pathtrace(vrt.make_uniforms(spawn, None, light, f, b, 0, W, H))
+            s.end_frame()
+        s.hdr_accum_reset()
+        per = []
+        for f in range(w, w + K):
+            s.pathtrace(vrt.make_uniforms(spawn, None, light, f, b, 0, W, H))
+            s.end_frame()
+            per.append(s.hdr_frame_mse())
+            s.hdr_accum_add()
+        m1, mk = sum(per) / K, s.hdr_accum_mse()
+        var = max(m1 - mk, 0.0) * K / (K - 1)
+        out[name] = {"mse_1spp": round(m1, 6), f"mse_{K}frame_mean": round(mk, 6), "var": round(var, 6),
+                     "bias2": round(mk - var / K, 7)}
+        s.close()
+    return out
+
+
 def cache_summary(c):
     """The headline figures of cache_comparison for the default bench line."""
-    q = c["quality"][CACHE_SCENES[1][0]]
+    q1 = c["quality"]["256^3 world (seed 2), 1920x1080, GPU FP64 reference"]
     sv = c["served_16_views"]
     return {
         "metric": "frames/s at matched MSE (64-frame accumulation vs a 4096-spp FP64 plain 6-bounce reference), "
-                  "cache-assisted over plain",
-        "mse_64frame_256world_480x270": {k: q[k]["mse_64frame_mean"] for k in ("plain_2bounce", "plain_6bounce",
-                                                                                "cache")},
+                  "cache-assisted over plain; 1080p quality against a GPU-accumulated reference",
+        "mse_64frame_256world_1080p": {k: q1[k]["mse_64frame_mean"] for k in ("plain_2bounce", "plain_6bounce",
+                                                                               "cache")},
         "single_1080p": {"fps": {k: c["speed_1080p"][k]["fps"] for k in c["speed_1080p"]},
                          "speedup_at_matched_mse": {k: v.get("cache_speedup") for k, v in
                                                     c["matched_mse_64frame"].items()}},
@@ -679,13 +720,15 @@ def cache_summary(c):
 def cache_comparison(args, local):
     """Cache-assisted path tracing against plain 2- and 6-bounce tracing.
 
-    Quality: MSE against a 4096-spp FP64 plain 6-bounce reference (committed
-    fixtures) on two scenes.  Speed: full frames (trace + temporal + 3x
-    a-trous + present) of the 256^3 world at 1920x1080 from its spawn pose,
-    after the cache trained on the preceding frames.  Matched MSE: the MSE of
-    a 64-frame accumulation (the temporal history cap) of the cache form; the
-    plain form needs s* = var / (64 (MSE_cache - bias^2)) samples per frame to
-    reach it, i.e. s* times its path-tracing pass per frame."""
+    Quality: MSE against 4096-spp FP64 plain 6-bounce references -- the
+    committed CPU-oracle fixtures of two scenes at small sizes, and the 256^3
+    world at 1920x1080 against a reference accumulated on the GPU.  Speed:
+    full frames (trace + temporal + 3x a-trous + present) of the 256^3 world
+    at 1920x1080 from its spawn pose, after the cache trained on the preceding
+    frames.  Matched MSE: the MSE of a 64-frame accumulation (the temporal
+    history cap) of the cache form; the plain form needs
+    s* = var / (64 (MSE_cache - bias^2)) samples per frame to reach it, i.e.
+    s* times its path-tracing pass per frame."""
     import numpy as np
     import torch
 
@@ -737,14 +780,16 @@ def cache_comparison(args, local):
             speed[name]["queries_per_frame"] = round(float(a[:, 5].mean()))
             speed[name]["training_samples_per_frame"] = round(float(a[:, 6].mean()))
         s.close()
+    q1080 = quality_1080p(vrt, ctx, sc, spawn, forms, K, WARM_TRAIN)
     # served form: 16 views of the 256^3 world at the reference's 480x270, one
     # batch frame for all of them, each view with its own cache; against the
     # same views rendered one after another by plain sessions
     served = served_views(vrt, ctx, sc, spawn, flush, args, K, WARM_TRAIN)
     sc.close()
     ctx.close()
-    # matched MSE (256^3 world quality, 1080p speed of the same view)
-    q = quality[CACHE_SCENES[1][0]]
+    # matched MSE at 1080p: quality and speed of the same view at the same size
+    quality["256^3 world (seed 2), 1920x1080, GPU FP64 reference"] = q1080
+    q = q1080
     target = q["cache"][f"mse_{K}frame_mean"]
     matched = {}
     for name in ("plain_2bounce", "plain_6bounce"):
@@ -758,10 +803,12 @@ def cache_comparison(args, local):
         matched[name] = {"spp_needed": round(s_star, 3), "frame_ms_at_matched_mse": round(ms, 4),
                          "cache_speedup": round(ms / speed["cache"]["frame_ms"], 3)}
     # served form at matched MSE: plain views one after another at s* spp
+    # (the 480x270 views' own statistics)
     sv = served
+    q480 = quality[CACHE_SCENES[1][0]]
     target_b = sv["batched_cache"]["mse_64frame_mean"]
     for name in ("plain_2bounce", "plain_6bounce"):
-        var, bias2 = q[name]["var"], q[name]["bias2"]
+        var, bias2 = q480[name]["var"], q480[name]["bias2"]
         seq = sv["sequential_" + name]
         if target_b <= bias2:
             sv["matched_" + name] = {"spp_needed": None}

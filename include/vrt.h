@@ -292,6 +292,28 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
 
+/* ---- HDR reference pipeline -------------------------------------------- */
+/* The reference's HDR capture (main.js:571-661: final illumination x (albedo
+ * byte / 255)^2) and its converged-reference accumulation (test/bench.mjs
+ * reference(), preset=base with a very long history), done on the device:
+ * per-frame HDR radiance of the path-trace pass (the session must keep fp32
+ * radiance) summed in FP64 -- the same double operations, in the same order,
+ * as a CPU FP64 accumulation, so the sums are bit-identical to it -- plus
+ * squared errors against a reference image, summed on the device. */
+int vrt_hdr_accum_reset(VrtSession* s);
+/* Adds the last path-trace pass's HDR radiance. */
+int vrt_hdr_accum_add(VrtSession* s);
+/* spp path-trace passes of u with frame indices frame0 .. frame0+spp-1, each added. */
+int vrt_hdr_accumulate(VrtSession* s, const VrtUniforms* u, uint32_t frame0, int spp);
+/* The FP64 sums (W*H*3 doubles) and the number of frames added. */
+int vrt_hdr_accum_read(VrtSession* s, double* rgb, size_t bytes, uint32_t* count);
+/* Reference image for the error calls: W*H*3 floats (HDR RGB). */
+int vrt_hdr_set_reference(VrtSession* s, const float* rgb, size_t bytes);
+/* Sum over pixels and channels of (last frame's HDR - reference)^2. */
+int vrt_hdr_frame_error(VrtSession* s, double* sum_sq);
+/* Sum over pixels and channels of (sums / count - reference)^2. */
+int vrt_hdr_accum_error(VrtSession* s, double* sum_sq);
+
 /* ---- radiance cache MLP (no counterpart in the reference) --------------- */
 /* A 4-layer MLP (80 -> 64 -> 64 -> 64 -> 3, ReLU, no biases) mapping an
  * encoded path vertex to outgoing radiance.  Input per query: 9 floats --

@@ -169,6 +169,13 @@ SIGNATURES = {
     "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
     "vrt_mlp_check": (I, [P]),
     "vrt_selftest_bounded_wait": (I, [C.c_uint]),
+    "vrt_hdr_accum_reset": (I, [P]),
+    "vrt_hdr_accum_add": (I, [P]),
+    "vrt_hdr_accumulate": (I, [P, P, U32, I]),
+    "vrt_hdr_accum_read": (I, [P, P, C.c_size_t, C.POINTER(U32)]),
+    "vrt_hdr_set_reference": (I, [P, P, C.c_size_t]),
+    "vrt_hdr_frame_error": (I, [P, C.POINTER(C.c_double)]),
+    "vrt_hdr_accum_error": (I, [P, C.POINTER(C.c_double)]),
     "vrt_session_set_cache": (I, [P, P]),
     "vrt_session_cache_mlp": (I, [P, C.POINTER(P)]),
     "vrt_session_read_cache_samples": (I, [P, P, P, I, C.POINTER(I)]),

@@ -293,6 +293,47 @@ class Session:
         k = min(n.value, cap)
         return q[:k], y[:k], n.value
 
+    # HDR reference pipeline ------------------------------------------------
+    def hdr_accum_reset(self) -> None:
+        check(lib.vrt_hdr_accum_reset(self.h))
+
+    def hdr_accum_add(self) -> None:
+        check(lib.vrt_hdr_accum_add(self.h))
+
+    def hdr_accumulate(self, u: VrtUniforms, frame0: int, spp: int) -> None:
+        """spp path-trace passes (frames frame0..), their HDR radiance summed in FP64."""
+        check(lib.vrt_hdr_accumulate(self.h, C.byref(u), C.c_uint32(frame0), int(spp)))
+
+    def hdr_accum_sums(self):
+        """(FP64 sums H x W x 3, frames added)."""
+        out = np.zeros((self.h_px, self.w, 3), np.float64)
+        n = C.c_uint32()
+        check(lib.vrt_hdr_accum_read(self.h, ptr(out), out.nbytes, C.byref(n)))
+        return out, int(n.value)
+
+    def hdr_accum(self):
+        """(mean HDR image H x W x 3 float64, frames added)."""
+        sums, n = self.hdr_accum_sums()
+        return sums / max(n, 1), n
+
+    def set_hdr_reference(self, img: np.ndarray) -> None:
+        ref = np.ascontiguousarray(img, np.float32)
+        if ref.shape != (self.h_px, self.w, 3):
+            raise ValueError("reference must be H x W x 3")
+        check(lib.vrt_hdr_set_reference(self.h, ptr(ref), ref.nbytes))
+
+    def hdr_frame_mse(self) -> float:
+        """MSE of the last frame's HDR radiance against the reference (on the device)."""
+        v = C.c_double()
+        check(lib.vrt_hdr_frame_error(self.h, C.byref(v)))
+        return v.value / (self.w * self.h_px * 3)
+
+    def hdr_accum_mse(self) -> float:
+        """MSE of the accumulated mean against the reference (on the device)."""
+        v = C.c_double()
+        check(lib.vrt_hdr_accum_error(self.h, C.byref(v)))
+        return v.value / (self.w * self.h_px * 3)
+
     def set_timing(self, on: bool) -> None:
         check(lib.vrt_session_set_timing(self.h, int(bool(on))))
 

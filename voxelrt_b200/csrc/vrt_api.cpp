@@ -108,6 +108,11 @@ struct VrtSession {
   cudaEvent_t cev[2] = {};
   bool cache_timed = false;
   uint64_t cache_version = 0;     // changes with every vrt_session_set_cache
+  // HDR reference pipeline (FP64 sums, reference image, error partials)
+  double* hdr_acc = nullptr;
+  float* hdr_ref = nullptr;
+  double* hdr_part = nullptr;
+  uint32_t hdr_count = 0;
 };
 
 constexpr int kMaxWaves = 72;   // wave counters allocated per wavefront scratch
@@ -354,6 +359,9 @@ int vrt_session_destroy(VrtSession* s) {
   dev_free(c, s->stats, kStatCount * 8, &s->bytes);
   dev_free(c, s->wf_mem, s->wf_bytes, &s->bytes);
   dev_free(c, s->cache_mem, s->cache_bytes, &s->bytes);
+  dev_free(c, s->hdr_acc, P * 24, &s->bytes);
+  dev_free(c, s->hdr_ref, P * 12, &s->bytes);
+  dev_free(c, s->hdr_part, (size_t)hdr_blocks((int)P) * 8, &s->bytes);
   if (s->mlp) vrt_mlp_destroy(s->mlp);
   for (auto& e : s->cev)
     if (e) cudaEventDestroy(e);
@@ -1637,6 +1645,98 @@ static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o) {
                             &cl, s->timing ? s->cev : nullptr));
   return VRT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// HDR reference pipeline
+// ---------------------------------------------------------------------------
+static int hdr_alloc(VrtSession* s) {
+  const size_t P = px(s);
+  if (!s->hdr_acc) {
+    if (int r = dev_alloc(s->ctx, (void**)&s->hdr_acc, P * 24, &s->bytes)) return r;
+    CUDA_TRY(cudaMemsetAsync(s->hdr_acc, 0, P * 24, s->ctx->stream));
+    s->hdr_count = 0;
+  }
+  if (!s->hdr_part) {
+    if (int r = dev_alloc(s->ctx, (void**)&s->hdr_part, (size_t)hdr_blocks((int)P) * 8, &s->bytes)) return r;
+  }
+  return VRT_OK;
+}
+
+int vrt_hdr_accum_reset(VrtSession* s) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = set_dev(s->ctx)) return r;
+  if (int r = hdr_alloc(s)) return r;
+  CUDA_TRY(cudaMemsetAsync(s->hdr_acc, 0, px(s) * 24, s->ctx->stream));
+  s->hdr_count = 0;
+  return VRT_OK;
+}
+
+int vrt_hdr_accum_add(VrtSession* s) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (!s->rad32) return fail(VRT_ERR_STATE, "the session keeps no fp32 radiance (keep_radiance_f32)");
+  if (int r = set_dev(s->ctx)) return r;
+  if (int r = hdr_alloc(s)) return r;
+  CUDA_TRY(launch_hdr_add((int)px(s), s->rad32, s->alb8, s->hdr_acc, s->ctx->stream));
+  s->hdr_count++;
+  return VRT_OK;
+}
+
+int vrt_hdr_accumulate(VrtSession* s, const VrtUniforms* u, uint32_t frame0, int spp) {
+  if (!s || !u || spp < 1) return fail(VRT_ERR_INVALID, "bad argument");
+  VrtUniforms v = *u;
+  for (int k = 0; k < spp; k++) {
+    v.params0[0] = frame0 + (uint32_t)k;
+    if (int r = vrt_pass_pathtrace(s, &v)) return r;
+    if (int r = vrt_hdr_accum_add(s)) return r;
+  }
+  return VRT_OK;
+}
+
+int vrt_hdr_accum_read(VrtSession* s, double* rgb, size_t bytes, uint32_t* count) {
+  if (!s || !rgb) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (!s->hdr_acc) return fail(VRT_ERR_STATE, "nothing accumulated");
+  const size_t P = px(s);
+  if (bytes < P * 24) return fail(VRT_ERR_INVALID, "host buffer %zu bytes < %zu needed", bytes, P * 24);
+  if (int r = set_dev(s->ctx)) return r;
+  CUDA_TRY(cudaMemcpyAsync(rgb, s->hdr_acc, P * 24, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  if (count) *count = s->hdr_count;
+  return VRT_OK;
+}
+
+int vrt_hdr_set_reference(VrtSession* s, const float* rgb, size_t bytes) {
+  if (!s || !rgb) return fail(VRT_ERR_INVALID, "NULL argument");
+  const size_t P = px(s);
+  if (bytes < P * 12) return fail(VRT_ERR_INVALID, "reference %zu bytes < %zu needed", bytes, P * 12);
+  if (int r = set_dev(s->ctx)) return r;
+  if (!s->hdr_ref)
+    if (int r = dev_alloc(s->ctx, (void**)&s->hdr_ref, P * 12, &s->bytes)) return r;
+  if (int r = hdr_alloc(s)) return r;
+  CUDA_TRY(cudaMemcpyAsync(s->hdr_ref, rgb, P * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  return VRT_OK;
+}
+
+static int hdr_error(VrtSession* s, int mode, double* sum_sq) {
+  if (!s || !sum_sq) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (!s->hdr_ref) return fail(VRT_ERR_STATE, "no reference image (vrt_hdr_set_reference)");
+  if (mode == 0 && !s->rad32) return fail(VRT_ERR_STATE, "the session keeps no fp32 radiance (keep_radiance_f32)");
+  if (mode == 1 && s->hdr_count == 0) return fail(VRT_ERR_STATE, "nothing accumulated");
+  if (int r = set_dev(s->ctx)) return r;
+  const int P = (int)px(s), nb = hdr_blocks(P);
+  CUDA_TRY(launch_hdr_sq_err(P, mode, s->rad32, s->alb8, s->hdr_acc, mode == 1 ? 1.0 / (double)s->hdr_count : 0.0,
+                             s->hdr_ref, s->hdr_part, s->ctx->stream));
+  std::vector<double> part((size_t)nb);
+  CUDA_TRY(cudaMemcpyAsync(part.data(), s->hdr_part, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  double acc = 0.0;
+  for (double x : part) acc += x;     // fixed order
+  *sum_sq = acc;
+  return VRT_OK;
+}
+
+int vrt_hdr_frame_error(VrtSession* s, double* sum_sq) { return hdr_error(s, 0, sum_sq); }
+int vrt_hdr_accum_error(VrtSession* s, double* sum_sq) { return hdr_error(s, 1, sum_sq); }
 
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev) {
   if (!s) return fail(VRT_ERR_INVALID, "session is NULL");

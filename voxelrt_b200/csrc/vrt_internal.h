@@ -178,6 +178,14 @@ cudaError_t mlp_gradient_tasks(MlpTaskSet& ts, cudaStream_t st);
 cudaError_t mlp_adam_tasks(const MlpTaskSet& ts, cudaStream_t st);
 cudaError_t mlp_to_bf16(const float* wm, uint16_t* wb, cudaStream_t st);
 
+// HDR reference pipeline (k_hdr.cu): FP64 sums of the capture's HDR value
+// (demodulated radiance x (albedo byte / 255)^2) and per-block partial sums
+// of squared errors (mode 0: last frame vs ref; mode 1: acc * inv_count vs ref).
+int hdr_blocks(int P);
+cudaError_t launch_hdr_add(int P, const void* rad32, const uint32_t* alb8, double* acc, cudaStream_t st);
+cudaError_t launch_hdr_sq_err(int P, int mode, const void* rad32, const uint32_t* alb8, const double* acc,
+                              double inv_count, const float* ref, double* part, cudaStream_t st);
+
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
