@@ -292,6 +292,26 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
 
+/* ---- scene lights -------------------------------------------------------- */
+/* The emissive-face light list, its power alias table and the per-brick
+ * top-16 light grid of the scene (scene.js:58-200, 435-461: `lights`,
+ * `lightAlias`, `lightGrid`), built from the scene's current voxels -- the
+ * list and grid on the device, the O(n) alias pass on the host -- so a host
+ * that edits the world can rebuild them per edit.  Same contents as the
+ * reference's buffers: words (x | y<<9 | z<<18 | face<<27, material) per
+ * light, (q, alias, pdf, 0) floats per light (4 floats when there are no
+ * lights), 34 words per brick cell (count, f32 weight sum, 16 x (index, f32
+ * weight)).  Grids up to 512^3. */
+typedef struct VrtLightStats {
+  uint32_t count;             /* emissive faces                                 */
+  uint32_t pad;
+  double total_weight;        /* sum of the face weights (emitted power proxy)  */
+  float ms_list, ms_alias, ms_grid, pad2;   /* device list / host alias / device grid */
+} VrtLightStats;
+int vrt_scene_build_lights(VrtScene* s, VrtLightStats* stats);
+int vrt_scene_read_lights(VrtScene* s, uint32_t* words, size_t words_bytes, float* alias, size_t alias_bytes,
+                          uint32_t* grid, size_t grid_bytes);
+
 /* ---- HDR reference pipeline -------------------------------------------- */
 /* The reference's HDR capture (main.js:571-661: final illumination x (albedo
  * byte / 255)^2) and its converged-reference accumulation (test/bench.mjs

@@ -196,6 +196,33 @@ def cache_paths(vox, bricks, masks, n, ubytes, w, h, phase: int, train_bounces: 
     return out.reshape(h, w)
 
 
+def light_list(vox, n: int):
+    """(words [k x 2] uint32, weights [k] float64) -- scene.js's emissive-face list."""
+    vox = np.ascontiguousarray(vox, np.uint32)
+    lib().orc_light_list.restype = C.c_long
+    k = lib().orc_light_list(_p(vox), C.c_int(n), None, None, C.c_long(0))
+    words = np.zeros((max(k, 1), 2), np.uint32)
+    weights = np.zeros(max(k, 1), np.float64)
+    lib().orc_light_list(_p(vox), C.c_int(n), _p(words), _p(weights), C.c_long(k))
+    return words[:k], weights[:k]
+
+
+def light_alias(weights):
+    w = np.ascontiguousarray(weights, np.float64)
+    out = np.zeros((max(len(w), 1), 4), np.float32)
+    lib().orc_light_alias(_p(w), C.c_long(len(w)), _p(out))
+    return out
+
+
+def light_grid(n: int, words, weights):
+    words = np.ascontiguousarray(words, np.uint32)
+    w = np.ascontiguousarray(weights, np.float64)
+    bg = n // 8
+    out = np.zeros((bg ** 3, 34), np.uint32)
+    lib().orc_light_grid(C.c_int(n), _p(words), _p(w), C.c_long(len(w)), _p(out))
+    return out
+
+
 def pcg_hash(v: int) -> int:
     f = lib().orc_pcg_hash
     f.restype = C.c_uint32

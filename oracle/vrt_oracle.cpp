@@ -1038,6 +1038,139 @@ void orc_math_eval(int fn, const float* x, float* y, int n) {
 
 uint32_t orc_pcg_hash(uint32_t v) { return pcg_hash(v); }
 
+// ---------------------------------------------------------------------------
+// Emissive-face light list, power alias table and per-brick light grid
+// (scene.js:58-200, 435-461).  JavaScript numbers are doubles and typed-array
+// stores round: the restatement computes in double and rounds where the
+// reference stores into a Float32Array.
+// ---------------------------------------------------------------------------
+static double light_weight(uint32_t m) {   // emissiveFaceWeight, scene.js:58-65
+  const double e = (double)((m >> 24) & 0xffu) / 255.0;
+  if (e <= 0.0) return 0.0;
+  const double r = (double)(m & 0xffu) / 255.0;
+  const double g = (double)((m >> 8) & 0xffu) / 255.0;
+  const double b = (double)((m >> 16) & 0xffu) / 255.0;
+  return e * (((0.2126 * r) * r + (0.7152 * g) * g) + (0.0722 * b) * b);
+}
+
+// Light list (scene.js:435-456): voxels in z, y, x order, faces +x,-x,+y,-y,+z,-z;
+// a face is a light when its neighbour is outside the grid or air.  Writes
+// at most `cap` lights (2 words each) and weights; returns the count.
+long orc_light_list(const uint32_t* vox, int N, uint32_t* words, double* weights, long cap) {
+  static const int D[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  long n = 0;
+  for (int z = 0; z < N; z++)
+    for (int y = 0; y < N; y++)
+      for (int x = 0; x < N; x++) {
+        const uint32_t m = vox[(size_t)x + (size_t)y * N + (size_t)z * N * N];
+        if (((m >> 24) & 0xffu) == 0u || m == 0u) continue;
+        const double w = light_weight(m);
+        for (int f = 0; f < 6; f++) {
+          const int nx = x + D[f][0], ny = y + D[f][1], nz = z + D[f][2];
+          const bool in = nx >= 0 && ny >= 0 && nz >= 0 && nx < N && ny < N && nz < N;
+          if (!in || vox[(size_t)nx + (size_t)ny * N + (size_t)nz * N * N] == 0u) {
+            if (n < cap) {
+              words[2 * n] = (uint32_t)x | ((uint32_t)y << 9) | ((uint32_t)z << 18) | ((uint32_t)f << 27);
+              words[2 * n + 1] = m;
+              weights[n] = w;
+            }
+            n++;
+          }
+        }
+      }
+  return n;
+}
+
+// makeAliasTable (scene.js:67-104): table[4i..4i+3] = (q, alias, prob, 0) as float32.
+void orc_light_alias(const double* weights, long n, float* table) {
+  if (n == 0) { table[0] = 1.0f; table[1] = 0.0f; table[2] = 1.0f; table[3] = 0.0f; return; }
+  double total = 0.0;
+  for (long i = 0; i < n; i++) total += weights[i] > 0.0 ? weights[i] : 0.0;
+  std::vector<double> prob((size_t)n), scaled((size_t)n);
+  for (long i = 0; i < n; i++) {
+    prob[(size_t)i] = total > 0.0 ? (weights[i] > 0.0 ? weights[i] : 0.0) / total : 1.0 / (double)n;
+    scaled[(size_t)i] = prob[(size_t)i] * (double)n;
+  }
+  std::vector<uint32_t> alias((size_t)n, 0u);
+  std::vector<float> q((size_t)n, 0.0f);
+  std::vector<long> small, large;
+  for (long i = 0; i < n; i++) (scaled[(size_t)i] < 1.0 ? small : large).push_back(i);
+  while (!small.empty() && !large.empty()) {
+    const long sidx = small.back(); small.pop_back();
+    const long l = large.back(); large.pop_back();
+    q[(size_t)sidx] = (float)scaled[(size_t)sidx];
+    alias[(size_t)sidx] = (uint32_t)l;
+    scaled[(size_t)l] = (scaled[(size_t)l] + scaled[(size_t)sidx]) - 1.0;
+    (scaled[(size_t)l] < 1.0 ? small : large).push_back(l);
+  }
+  for (long i : large) { q[(size_t)i] = 1.0f; alias[(size_t)i] = (uint32_t)i; }
+  for (long i : small) { q[(size_t)i] = 1.0f; alias[(size_t)i] = (uint32_t)i; }
+  for (long i = 0; i < n; i++) {
+    table[4 * i + 0] = q[(size_t)i];
+    table[4 * i + 1] = (float)alias[(size_t)i];
+    table[4 * i + 2] = (float)(prob[(size_t)i] > 0.0 ? prob[(size_t)i] : 1.0 / (double)n);
+    table[4 * i + 3] = 0.0f;
+  }
+}
+
+// buildLightGrid (scene.js:106-200): per brick cell (BG^3 cells, 34 words
+// each) the top-16 lights by power / max(d^2, 16) with a facing test.
+void orc_light_grid(int N, const uint32_t* words, const double* weights, long n, uint32_t* grid) {
+  const int BG = N / BRICK, K = 16, STRIDE = 2 + 2 * K;
+  std::vector<float> fc((size_t)n * 3), fn((size_t)n * 3);
+  for (long i = 0; i < n; i++) {
+    const uint32_t w0 = words[2 * i];
+    const int x = (int)(w0 & 0x1ffu), y = (int)((w0 >> 9) & 0x1ffu), z = (int)((w0 >> 18) & 0x1ffu);
+    const int face = (int)((w0 >> 27) & 7u), axis = face >> 1, pos = (face & 1) == 0 ? 1 : 0;
+    double c[3] = {x + 0.5, y + 0.5, z + 0.5}, nn[3] = {0, 0, 0};
+    const int v[3] = {x, y, z};
+    c[axis] = v[axis] + pos;
+    nn[axis] = pos ? 1.0 : -1.0;
+    for (int k = 0; k < 3; k++) { fc[3 * i + k] = (float)c[k]; fn[3 * i + k] = (float)nn[k]; }
+  }
+  const double eps = (BRICK / 2.0) * (BRICK / 2.0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int cell = 0; cell < BG * BG * BG; cell++) {
+    const int bx = cell % BG, by = (cell / BG) % BG, bz = cell / (BG * BG);
+    const double ccx = (bx + 0.5) * BRICK, ccy = (by + 0.5) * BRICK, ccz = (bz + 0.5) * BRICK;
+    uint32_t topIdx[16];
+    float topW[16];
+    int count = 0, minAt = 0;
+    double minW = 0.0;
+    for (long i = 0; i < n; i++) {
+      const double dx = ccx - (double)fc[3 * i], dy = ccy - (double)fc[3 * i + 1], dz = ccz - (double)fc[3 * i + 2];
+      if ((dx * (double)fn[3 * i] + dy * (double)fn[3 * i + 1]) + dz * (double)fn[3 * i + 2] <= 0.0) continue;
+      const double d2 = (dx * dx + dy * dy) + dz * dz;
+      const double w = weights[i] / (d2 > eps ? d2 : eps);
+      if (count < K) {
+        topIdx[count] = (uint32_t)i;
+        topW[count] = (float)w;
+        count++;
+        if (count == K) {
+          minW = topW[0]; minAt = 0;
+          for (int k = 1; k < K; k++) if ((double)topW[k] < minW) { minW = topW[k]; minAt = k; }
+        }
+      } else if (w > minW) {
+        topIdx[minAt] = (uint32_t)i;
+        topW[minAt] = (float)w;
+        minW = topW[0]; minAt = 0;
+        for (int k = 1; k < K; k++) if ((double)topW[k] < minW) { minW = topW[k]; minAt = k; }
+      }
+    }
+    uint32_t* g = grid + (size_t)cell * STRIDE;
+    double wSum = 0.0;
+    for (int k = 0; k < count; k++) wSum += (double)topW[k];
+    const float wSumF = (float)wSum;
+    g[0] = (uint32_t)count;
+    std::memcpy(&g[1], &wSumF, 4);
+    for (int k = 0; k < count; k++) {
+      g[2 + 2 * k] = topIdx[k];
+      std::memcpy(&g[3 + 2 * k], &topW[k], 4);
+    }
+    for (int k = count; k < K; k++) { g[2 + 2 * k] = 0u; g[3 + 2 * k] = 0u; }
+  }
+}
+
 // Cache-assisted estimator of every pixel (OrcCachePix per pixel, row-major).
 int orc_cache_pix_bytes(void) { return (int)sizeof(OrcCachePix); }
 

@@ -92,6 +92,11 @@ class VrtFrameStats(C.Structure):
                 ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("pad", C.c_uint32)]
 
 
+class VrtLightStats(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("pad", C.c_uint32), ("total_weight", C.c_double), ("ms_list", C.c_float),
+                ("ms_alias", C.c_float), ("ms_grid", C.c_float), ("pad2", C.c_float)]
+
+
 class VrtCacheConfig(C.Structure):
     _fields_ = [("enabled", C.c_int), ("train_bounces", C.c_int), ("train_vertices", C.c_int),
                 ("train_batch", C.c_int), ("train_steps", C.c_int), ("learning_rate", C.c_float),
@@ -169,6 +174,8 @@ SIGNATURES = {
     "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
     "vrt_mlp_check": (I, [P]),
     "vrt_selftest_bounded_wait": (I, [C.c_uint]),
+    "vrt_scene_build_lights": (I, [P, P]),
+    "vrt_scene_read_lights": (I, [P, P, C.c_size_t, P, C.c_size_t, P, C.c_size_t]),
     "vrt_hdr_accum_reset": (I, [P]),
     "vrt_hdr_accum_add": (I, [P]),
     "vrt_hdr_accumulate": (I, [P, P, U32, I]),

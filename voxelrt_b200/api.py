@@ -15,7 +15,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._lib import (HIT_DTYPE, PATH_BATCH_ONLY, PATH_MEGAKERNEL, PATH_WAVEFRONT, VrtCameraPose, VrtCompletion,
-                   VrtCacheConfig, VrtDeviceConfig, VrtEditBox, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
+                   VrtCacheConfig, VrtDeviceConfig, VrtEditBox, VrtLightStats, VrtFrameStats, VrtLighting, VrtSessionConfig, VrtTuning, VrtUniforms,
                    check, lib, ptr)
 
 # Live handles, closed in dependency order when the interpreter exits (objects
@@ -196,6 +196,28 @@ class Scene:
         out = np.zeros(n, HIT_DTYPE)
         check(lib.vrt_trace_rays(self.h, ptr(o), ptr(d), ptr(t), n, ptr(out)))
         return out
+
+    def build_lights(self):
+        """Rebuild the light list, alias table and light grid from the current
+        voxels (vrt_scene_build_lights); returns the build statistics."""
+        st = VrtLightStats()
+        check(lib.vrt_scene_build_lights(self.h, C.byref(st)))
+        self._lights_n = int(st.count)
+        return st
+
+    def lights(self):
+        """(words [n x 2] uint32, alias [max(n,1) x 4] float32, grid [cells x 34]
+        uint32) of the last build_lights()."""
+        n = getattr(self, "_lights_n", None)
+        if n is None:
+            raise RuntimeError("call build_lights() first")
+        bg = self.n // BRICK
+        words = np.zeros((n, 2), np.uint32)
+        alias = np.zeros((max(n, 1), 4), np.float32)
+        grid = np.zeros((bg ** 3, 34), np.uint32)
+        check(lib.vrt_scene_read_lights(self.h, ptr(words), words.nbytes, ptr(alias), alias.nbytes, ptr(grid),
+                                        grid.nbytes))
+        return words, alias, grid
 
     def close(self) -> None:
         if self.h:

@@ -60,6 +60,16 @@ struct VrtScene {
   VrtCtx* ctx = nullptr;
   SceneDev dev;
   uint64_t bytes = 0;
+  // emissive-face light list, alias table, light grid (vrt_scene_build_lights)
+  uint32_t* light_words = nullptr;   // 2 per light
+  double* light_w = nullptr;         // weight per light
+  float* light_alias = nullptr;      // 4 per light
+  uint32_t* light_grid = nullptr;    // 34 per brick cell
+  uint32_t* light_tmp = nullptr;     // block offsets + count
+  size_t light_cap = 0;              // lights the word/weight buffers hold
+  size_t light_alias_bytes = 0;
+  uint32_t light_count = 0;
+  bool lights_built = false;
 };
 
 struct VrtSession {
@@ -295,6 +305,12 @@ int vrt_scene_destroy(VrtScene* s) {
   dev_free(c, s->dev.bricks, nb * 4, &s->bytes);
   dev_free(c, s->dev.masks, nb * 64, &s->bytes);
   dev_free(c, s->dev.bits, occ_words(s->dev.BG) * 4 + 128, &s->bytes);
+  const size_t cap = s->light_cap;
+  dev_free(c, s->light_words, cap * 8, &s->bytes);
+  dev_free(c, s->light_w, cap * 8, &s->bytes);
+  dev_free(c, s->light_alias, s->light_alias_bytes, &s->bytes);
+  dev_free(c, s->light_grid, nb * 34 * 4, &s->bytes);
+  dev_free(c, s->light_tmp, ((size_t)light_blocks((int)N) + 1) * 4, &s->bytes);
   delete s;
   return VRT_OK;
 }
@@ -1643,6 +1659,144 @@ static int cache_frame(VrtSession* s, const VrtUniforms* u, const PathOut& o) {
   CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
                             &s->launches, s->timing ? s->tev : nullptr, VrtSession::kTimedWaves, &s->timed_waves,
                             &cl, s->timing ? s->cev : nullptr));
+  return VRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// scene lights (scene.js:58-200, 435-461)
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+// Power alias table of the light weights (makeAliasTable, scene.js:67-104):
+// doubles throughout, float32 where the reference stores into a Float32Array.
+static void alias_table(const std::vector<double>& wts, std::vector<float>& table) {
+  const size_t n = wts.size();
+  if (n == 0) { table = {1.0f, 0.0f, 1.0f, 0.0f}; return; }
+  double total = 0.0;
+  for (double w : wts) total += std::max(0.0, w);
+  std::vector<double> prob(n), scaled(n);
+  for (size_t i = 0; i < n; i++) {
+    prob[i] = total > 0.0 ? std::max(0.0, wts[i]) / total : 1.0 / (double)n;
+    scaled[i] = prob[i] * (double)n;
+  }
+  std::vector<uint32_t> alias(n, 0u);
+  std::vector<float> q(n, 0.0f);
+  std::vector<size_t> small, large;
+  for (size_t i = 0; i < n; i++) (scaled[i] < 1.0 ? small : large).push_back(i);
+  while (!small.empty() && !large.empty()) {
+    const size_t a = small.back(), b = large.back();
+    small.pop_back();
+    large.pop_back();
+    q[a] = (float)scaled[a];
+    alias[a] = (uint32_t)b;
+    scaled[b] = (scaled[b] + scaled[a]) - 1.0;
+    (scaled[b] < 1.0 ? small : large).push_back(b);
+  }
+  for (size_t i : large) { q[i] = 1.0f; alias[i] = (uint32_t)i; }
+  for (size_t i : small) { q[i] = 1.0f; alias[i] = (uint32_t)i; }
+  table.assign(n * 4, 0.0f);
+  for (size_t i = 0; i < n; i++) {
+    table[4 * i] = q[i];
+    table[4 * i + 1] = (float)alias[i];
+    table[4 * i + 2] = (float)(prob[i] > 0.0 ? prob[i] : 1.0 / (double)n);
+  }
+}
+
+extern "C" {
+
+int vrt_scene_build_lights(VrtScene* sc, VrtLightStats* st) {
+  if (!sc) return fail(VRT_ERR_INVALID, "scene is NULL");
+  const int N = sc->dev.N, BG = sc->dev.BG;
+  if (N > 512) return fail(VRT_ERR_INVALID, "the light word packing holds grids up to 512^3 (scene.js:437)");
+  if (int r = set_dev(sc->ctx)) return r;
+  VrtCtx* c = sc->ctx;
+  cudaStream_t s = c->stream;
+  const size_t nb = (size_t)light_blocks(N), cells = (size_t)BG * BG * BG;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+  struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]); } } guard{ev};
+  if (!sc->light_tmp)
+    if (int r = dev_alloc(c, (void**)&sc->light_tmp, (nb + 1) * 4, &sc->bytes)) return r;
+  if (!sc->light_grid)
+    if (int r = dev_alloc(c, (void**)&sc->light_grid, cells * 34 * 4, &sc->bytes)) return r;
+  CUDA_TRY(cudaEventRecord(ev[0], s));
+  CUDA_TRY(launch_light_count(sc->dev.vox, N, sc->light_tmp, sc->light_tmp + nb, s));
+  uint32_t n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, sc->light_tmp + nb, 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (n > sc->light_cap) {
+    const size_t cap = sc->light_cap;
+    dev_free(c, sc->light_words, cap * 8, &sc->bytes);
+    dev_free(c, sc->light_w, cap * 8, &sc->bytes);
+    sc->light_words = nullptr; sc->light_w = nullptr;
+    sc->light_cap = 0;
+    const size_t ncap = std::max<size_t>(n, 1);
+    int r = dev_alloc(c, (void**)&sc->light_words, ncap * 8, &sc->bytes);
+    if (!r) r = dev_alloc(c, (void**)&sc->light_w, ncap * 8, &sc->bytes);
+    if (r) return r;
+    sc->light_cap = ncap;
+  }
+  if (n > 0) CUDA_TRY(launch_light_write(sc->dev.vox, N, sc->light_tmp, sc->light_words, sc->light_w, s));
+  CUDA_TRY(cudaEventRecord(ev[1], s));
+  // alias table on the host (a sequential O(n) pass), then uploaded
+  std::vector<double> w(n);
+  if (n > 0) CUDA_TRY(cudaMemcpyAsync(w.data(), sc->light_w, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<float> table;
+  alias_table(w, table);
+  const double alias_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (sc->light_alias_bytes < table.size() * 4) {
+    dev_free(c, sc->light_alias, sc->light_alias_bytes, &sc->bytes);
+    sc->light_alias = nullptr;
+    sc->light_alias_bytes = 0;
+    if (int r = dev_alloc(c, (void**)&sc->light_alias, table.size() * 4, &sc->bytes)) return r;
+    sc->light_alias_bytes = table.size() * 4;
+  }
+  CUDA_TRY(cudaMemcpyAsync(sc->light_alias, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaEventRecord(ev[2], s));
+  CUDA_TRY(launch_light_grid(N, sc->light_words, sc->light_w, (int)n, sc->light_grid, s));
+  CUDA_TRY(cudaEventRecord(ev[3], s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  sc->light_count = n;
+  sc->lights_built = true;
+  if (st) {
+    std::memset(st, 0, sizeof *st);
+    st->count = n;
+    double tot = 0.0;
+    for (double x : w) tot += std::max(0.0, x);
+    st->total_weight = tot;
+    float a = 0, g = 0;
+    CUDA_TRY(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    CUDA_TRY(cudaEventElapsedTime(&g, ev[2], ev[3]));
+    st->ms_list = a;
+    st->ms_alias = (float)alias_ms;
+    st->ms_grid = g;
+  }
+  return VRT_OK;
+}
+
+int vrt_scene_read_lights(VrtScene* sc, uint32_t* words, size_t words_bytes, float* alias, size_t alias_bytes,
+                          uint32_t* grid, size_t grid_bytes) {
+  if (!sc) return fail(VRT_ERR_INVALID, "scene is NULL");
+  if (!sc->lights_built) return fail(VRT_ERR_STATE, "lights not built (vrt_scene_build_lights)");
+  if (int r = set_dev(sc->ctx)) return r;
+  cudaStream_t s = sc->ctx->stream;
+  const size_t n = sc->light_count, cells = (size_t)sc->dev.BG * sc->dev.BG * sc->dev.BG;
+  const size_t alias_need = std::max<size_t>(n, 1) * 16;
+  if (words) {
+    if (words_bytes < n * 8) return fail(VRT_ERR_INVALID, "words buffer too small");
+    if (n) CUDA_TRY(cudaMemcpyAsync(words, sc->light_words, n * 8, cudaMemcpyDeviceToHost, s));
+  }
+  if (alias) {
+    if (alias_bytes < alias_need) return fail(VRT_ERR_INVALID, "alias buffer too small");
+    CUDA_TRY(cudaMemcpyAsync(alias, sc->light_alias, alias_need, cudaMemcpyDeviceToHost, s));
+  }
+  if (grid) {
+    if (grid_bytes < cells * 136) return fail(VRT_ERR_INVALID, "grid buffer too small");
+    CUDA_TRY(cudaMemcpyAsync(grid, sc->light_grid, cells * 136, cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
   return VRT_OK;
 }
 

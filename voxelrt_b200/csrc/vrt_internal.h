@@ -186,6 +186,14 @@ cudaError_t launch_hdr_add(int P, const void* rad32, const uint32_t* alb8, doubl
 cudaError_t launch_hdr_sq_err(int P, int mode, const void* rad32, const uint32_t* alb8, const double* acc,
                               double inv_count, const float* ref, double* part, cudaStream_t st);
 
+// Scene lights (k_lights.cu): ordered light-list compaction and light grid.
+int light_blocks(int N);
+cudaError_t launch_light_count(const uint32_t* vox, int N, uint32_t* bsum, uint32_t* count, cudaStream_t st);
+cudaError_t launch_light_write(const uint32_t* vox, int N, const uint32_t* boff, uint32_t* words, double* weights,
+                               cudaStream_t st);
+cudaError_t launch_light_grid(int N, const uint32_t* words, const double* weights, int n, uint32_t* grid,
+                              cudaStream_t st);
+
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
