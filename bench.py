@@ -47,10 +47,11 @@ def parse_args():
     ap.add_argument("--no-cache-compare", action="store_true",
                     help="frame mode: skip the plain vs batched+cache comparison in the output line")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
-    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame", "lights"],
+    ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame", "lights",
+                                                              "restir"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
                          "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
-                         "path tracing at matched MSE")
+                         "path tracing at matched MSE; restir: the ReSTIR gi preset beside the plain frame")
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
@@ -1010,6 +1011,95 @@ def sweep(args, server, sessions, make_request, rng):
     return results
 
 
+def run_restir(args, local):
+    """`--mode restir`: the reference's ReSTIR `gi` preset (RF_RESTIR |
+    RF_TEMPORAL | RF_SPATIAL: initial candidates, temporal + spatial reservoir
+    reuse, then temporal / a-trous / present) on the full-size workload, timed
+    like the plain frame, with the plain frame measured beside it and the CPU
+    oracle's ReSTIR frame as the CPU baseline."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+
+    torch.cuda.set_device(local)
+    n, W, H = WORKLOAD["n"], WORKLOAD["W"], WORKLOAD["H"]
+    vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
+    ctx = vrt.Context(local)
+    scene = vrt.Scene(ctx, vox, n)
+    sess = vrt.Session(ctx, scene, W, H, firefly_clamp=WORKLOAD["fclamp"], accum_f32=False,
+                       path_kernel=args.path_kernel)
+    sess.set_timing(True)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def uni(f, preset):
+        u = frame_uniforms(vrt, spawn, f)
+        u.params2[0] = vrt.api.preset_flags(preset)
+        return u
+
+    res, clk = {}, None
+    for preset in ("base", "gi"):
+        sess.reset()
+        for i in range(args.warmup):
+            sess.frame(uni(i, preset))
+            sess.stats()
+        ctx.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        fm, pt, ru, rays, launches = [], [], [], 0, 0
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sess.frame(uni(args.warmup + i, preset))
+            st = sess.stats()
+            fm.append(st.ms_total)
+            pt.append(st.ms_pathtrace)
+            ru.append(st.ms_reuse)
+            rays += st.rays
+            launches += st.launches
+        ctx.synchronize()
+        c = clocks.stop()
+        if preset == "gi":
+            clk = c
+        res[preset] = {"frame_ms_mean": round(statistics.mean(fm), 4), "frame_ms_p50": round(statistics.median(fm), 4),
+                       "frame_ms_p99": round(float(np.percentile(fm, 99)), 4),
+                       "pathtrace_ms_mean": round(statistics.mean(pt), 4),
+                       "reuse_ms_mean": round(statistics.mean(ru), 4),
+                       "rays_per_frame": round(rays / args.steps), "launches": launches,
+                       "mrays_s": round(rays / (sum(fm) / 1e3) / 1e6, 2)}
+    sess.close()
+    scene.close()
+    ctx.close()
+    gi = res["gi"]
+    line = {
+        "metric": "ReSTIR gi frame ms at 1080p (initial + temporal/spatial reuse + temporal + a-trous + present)",
+        "value": gi["frame_ms_mean"], "unit": "ms/frame", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": gi["frame_ms_mean"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural voxel world and camera path)",
+        "config": {"workload": "ReSTIR gi preset on " + WORKLOAD_NAME, "preset": "gi (flags 7)", "taps": 3,
+                   "radius_px": 30, "ccap": 20, "path_kernel": args.path_kernel,
+                   "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
+        "gi": gi, "plain": res["base"],
+        "gi_over_plain_frame_ms": round(gi["frame_ms_mean"] / res["base"]["frame_ms_mean"], 3),
+        "gpu_launches": gi["launches"],
+    }
+    if clk:
+        line["clocks"] = clk
+    if not args.no_cpu_baseline:
+        import oracle
+        b, m = oracle.build_bricks(vox, n)
+        u = uni(0, "gi")
+        t0 = time.perf_counter()
+        r = oracle.frame(vox, b, m, n, vrt.uniforms_bytes(u), WORKLOAD["fclamp"], W, H,
+                         np.zeros((H, W, 4), np.uint16), np.zeros((H, W, 4), np.float32))
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(dt * 1e3, 1), "unit": "ms/frame", "cores": oracle.num_threads(),
+                                "kind": "port", "rays": r["stats"]["rays"],
+                                "sample": "1 full ReSTIR gi frame of the workload through the CPU oracle"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_env()
@@ -1030,6 +1120,9 @@ def main():
     elif args.mode == "lights":
         if rank == 0:
             run_lights(args, local)
+    elif args.mode == "restir":
+        if rank == 0:
+            run_restir(args, local)
     else:
         run_ours(args, world, rank, local)
 

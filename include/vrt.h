@@ -66,9 +66,12 @@ typedef struct VrtUniforms {
   uint32_t params0[4];     /* x frame index (RNG stream), y bounces,
                               z flags: bit0 temporal, bit1 denoise             */
   float params1[4];        /* x width, y height, z exposure                    */
-  uint32_t params2[4];     /* x restir flags (must be 0 on this path)          */
-  float params3[4];
-  float params4[4];        /* y = max temporal history (default 64)            */
+  uint32_t params2[4];     /* x restir flags: 0 (preset=base) or a subset of
+                              RF_RESTIR|RF_TEMPORAL|RF_SPATIAL = 1|2|4 with
+                              RF_RESTIR set (preset=gi is 7); z spatial taps  */
+  float params3[4];        /* x = temporal confidence cap (default 20)         */
+  float params4[4];        /* x = spatial disk radius in pixels (default 30),
+                              y = max temporal history (default 64)            */
   float params5[4];
   float params6[4];
 } VrtUniforms;
@@ -132,7 +135,8 @@ typedef struct VrtFrameStats {
   uint64_t cache_queries;     /* paths that ended in a cache query             */
   uint64_t cache_samples;     /* training samples produced by training paths   */
   float ms_cache;             /* cache inference + resolve + training steps    */
-  uint32_t pad;
+  float ms_reuse;             /* ReSTIR frames: reuse passes (inside
+                                 ms_pathtrace, which covers all three)         */
 } VrtFrameStats;
 
 /* Camera pose of the reference's fly camera (camera.js:1-57). */
@@ -194,11 +198,20 @@ int vrt_session_destroy(VrtSession* s);
 int vrt_session_set_scene(VrtSession* s, VrtScene* scene);
 /* Clears history (next frame starts with parity 0 and empty history). */
 int vrt_session_reset(VrtSession* s);
-/* One frame: pathtrace -> temporal -> (if params0.z bit1) a-trous x3 ->
- * present, ping-ponging G-buffer/history by frame parity (main.js:680-772). */
+/* One frame: pathtrace -> [ReSTIR: reuse_temporal (RF_TEMPORAL) ->
+ * reuse_spatial] -> temporal -> (if params0.z bit1) a-trous x3 -> present,
+ * ping-ponging G-buffer/history by frame parity (main.js:680-772). */
 int vrt_frame(VrtSession* s, const VrtUniforms* u);
-/* Individual passes of the same frame (parity of the frame in flight). */
+/* Individual passes of the same frame (parity of the frame in flight).
+ * With RF_RESTIR in params2.x the path-trace pass is the reservoir pass of
+ * pathtrace.wgsl:332-457 (initial candidates -> reservoirs A, pass-through
+ * radiance -> direct); reuse_temporal merges the reprojected history
+ * reservoirs B into A (reuse_temporal.wgsl, no-op without RF_TEMPORAL) and
+ * reuse_spatial merges neighbours, shades the radiance and writes B
+ * (reuse_spatial.wgsl). */
 int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u);
+int vrt_pass_reuse_temporal(VrtSession* s, const VrtUniforms* u);
+int vrt_pass_reuse_spatial(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int iteration /*0,1,2*/);
 int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
@@ -226,6 +239,12 @@ int vrt_read_denoise(VrtSession* s, int index, void* host, size_t bytes); /* rgb
 int vrt_read_final(VrtSession* s, void* host, size_t bytes);         /* rgba16f/32f */
 int vrt_read_ldr(VrtSession* s, void* host, size_t bytes);           /* rgba8   */
 int vrt_read_hdr(VrtSession* s, float* host_rgb, size_t bytes);      /* f32 RGB */
+/* ReSTIR state: reservoirs (which 0 = A, 1 = B; W*H records of 32 bytes in
+ * the layout of restir.wgsl:14-27: posW f32 x 4, data u32 x 4) and the
+ * pass-through radiance (rgba16f).  VRT_ERR_STATE before the first ReSTIR
+ * frame of the session. */
+int vrt_read_reservoirs(VrtSession* s, int which, void* host, size_t bytes);
+int vrt_read_direct(VrtSession* s, void* host, size_t bytes);
 /* Writes history buffers (resume from a saved session state). */
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
 

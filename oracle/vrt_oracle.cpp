@@ -9,6 +9,8 @@
 //   src/shaders/temporal.wgsl:17-77   reprojection + history accumulation
 //   src/shaders/atrous.wgsl:26-83     edge-aware a-trous iteration
 //   src/shaders/present.wgsl:40-55    remodulate, exposure, ACES, gamma
+//   src/shaders/pathtrace.wgsl:199-246, 332-457, restir.wgsl,
+//   reuse_temporal.wgsl, reuse_spatial.wgsl   ReSTIR `gi` preset passes
 //   src/main.js:628-659               HDR capture = illum * (alb8/255)^2
 //   src/scene.js:411-433              brick occupancy words + 16-word masks
 //   src/math.js:3-74, src/camera.js:47-57   view/projection matrices
@@ -648,6 +650,425 @@ void bilinear(Fetch fetch, int W, int H, float u, float v, float out[4]) {
 
 inline float luminance(const float* c) { return std::fmaf(c[2], 0.0722f, std::fmaf(c[1], 0.7152f, c[0] * 0.2126f)); }
 
+
+// ---------------------------------------------------------------------------
+// ReSTIR `gi` preset (RF_RESTIR | RF_TEMPORAL | RF_SPATIAL, main.js:44)
+// ---------------------------------------------------------------------------
+const uint32_t SK_NONE = 0u, SK_POINT = 1u, SK_DIR = 2u;   // restir.wgsl:29-31
+const uint32_t RF_SPATIAL = 4u;                            // common.wgsl:42
+
+// Decoded reservoir sample (restir.wgsl:33-41).
+struct RSample {
+  uint32_t kind;
+  f3 pos, n, rad;
+  float W, c;
+  uint32_t seed;
+};
+
+inline RSample null_sample(float c) {
+  RSample s;
+  s.kind = SK_NONE;
+  s.pos = s.n = s.rad = mk(0, 0, 0);
+  s.W = 0.0f;
+  s.c = c;
+  s.seed = 0u;
+  return s;
+}
+
+// WGSL f32 -> i32: toward zero, saturating, NaN -> 0.
+inline int itrunc(float x) {
+  if (x != x) return 0;
+  if (x >= 2147483648.0f) return 2147483647;
+  if (x < -2147483648.0f) return (-2147483647 - 1);
+  return (int)x;
+}
+
+// pack2x16snorm / unpack2x16snorm, one component (WGSL builtin definitions).
+inline uint32_t snorm16(float v) {
+  float c = fminf_(1.0f, fmaxf_(-1.0f, v));
+  return (uint32_t)(uint16_t)(int16_t)(int)std::floor(0.5f + 32767.0f * c);
+}
+inline float unsnorm16(uint32_t b) { return fmaxf_((float)(int16_t)(uint16_t)b / 32767.0f, -1.0f); }
+inline float sgn_ge0(float x) { return x >= 0.0f ? 1.0f : -1.0f; }
+
+// octEncode (restir.wgsl:43-50)
+inline void oct_encode(f3 nIn, float& ex, float& ey) {
+  float s = (std::fabs(nIn.x) + std::fabs(nIn.y)) + std::fabs(nIn.z);
+  f3 n = mk(nIn.x / s, nIn.y / s, nIn.z / s);
+  ex = n.x; ey = n.y;
+  if (n.z < 0.0f) {
+    ex = (1.0f - std::fabs(n.y)) * sgn_ge0(n.x);
+    ey = (1.0f - std::fabs(n.x)) * sgn_ge0(n.y);
+  }
+}
+
+// octDecode (restir.wgsl:52-59)
+inline f3 oct_decode(float ex, float ey) {
+  f3 n = mk(ex, ey, (1.0f - std::fabs(ex)) - std::fabs(ey));
+  if (n.z < 0.0f) n = mk((1.0f - std::fabs(n.y)) * sgn_ge0(n.x), (1.0f - std::fabs(n.x)) * sgn_ge0(n.y), n.z);
+  return normalize3(n);
+}
+
+// packReservoir (restir.wgsl:61-71): 8 words, posW then data.
+inline void pack_res(const RSample& s, uint32_t* w) {
+  float cf = s.c + 0.5f;
+  uint32_t cq = std::min(cf >= 4294967296.0f ? 4294967295u : (uint32_t)cf, 255u);
+  f3 nn = s.kind != SK_POINT ? mk(0, 1, 0) : s.n;
+  float ex, ey;
+  oct_encode(nn, ex, ey);
+  w[0] = fbits(s.pos.x); w[1] = fbits(s.pos.y); w[2] = fbits(s.pos.z); w[3] = fbits(s.W);
+  w[4] = (uint32_t)f32_to_f16(s.rad.x) | ((uint32_t)f32_to_f16(s.rad.y) << 16);
+  w[5] = ((uint32_t)f32_to_f16(s.rad.z) & 0xffffu) | (s.kind << 16) | (cq << 18);
+  w[6] = snorm16(ex) | (snorm16(ey) << 16);
+  w[7] = s.seed;
+}
+
+// unpackReservoir (restir.wgsl:73-84)
+inline RSample unpack_res(const uint32_t* w) {
+  RSample s;
+  s.pos = mk(bitsf(w[0]), bitsf(w[1]), bitsf(w[2]));
+  s.W = bitsf(w[3]);
+  s.rad = mk(f16_to_f32((uint16_t)(w[4] & 0xffffu)), f16_to_f32((uint16_t)(w[4] >> 16)),
+             f16_to_f32((uint16_t)(w[5] & 0xffffu)));
+  s.kind = (w[5] >> 16) & 3u;
+  s.c = (float)((w[5] >> 18) & 0xffu);
+  s.n = oct_decode(unsnorm16(w[6] & 0xffffu), unsnorm16(w[6] >> 16));
+  s.seed = w[7];
+  return s;
+}
+
+// lum (restir.wgsl:90-92), a dot product summed left to right.
+inline float rlum(f3 c) { return (c.x * 0.2126f + c.y * 0.7152f) + c.z * 0.0722f; }
+
+// evalF (restir.wgsl:143-159); inverseSqrt(r2) = 1 / sqrt(r2).
+inline f3 eval_f(const RSample& s, f3 x1, f3 n1) {
+  if (s.kind == SK_POINT) {
+    f3 d = sub(s.pos, x1);
+    float r2 = fmaxf_(dot3(d, d), 1e-4f);
+    f3 dir = muls(d, 1.0f / std::sqrt(r2));
+    float cos1 = dot3(n1, dir);
+    float cos2 = dot3(s.n, mk(-dir.x, -dir.y, -dir.z));
+    if (cos1 <= 0.0f || cos2 <= 0.0f) return mk(0, 0, 0);
+    return muls(s.rad, ((INV_PI * cos1) * cos2) / r2);
+  }
+  if (s.kind == SK_DIR) {
+    float cos1 = dot3(n1, s.pos);
+    if (cos1 <= 0.0f) return mk(0, 0, 0);
+    return muls(s.rad, INV_PI * cos1);
+  }
+  return mk(0, 0, 0);
+}
+inline float eval_target(const RSample& s, f3 x1, f3 n1) { return rlum(eval_f(s, x1, n1)); }
+
+// receiverPoint (restir.wgsl:127-137); WGSL round() is half-to-even.
+inline f3 receiver_point(f3 ro, f3 rd, float t, f3 n1) {
+  f3 approx = add(ro, muls(rd, t));
+  int ax = std::fabs(n1.x) > 0.5f ? 0 : (std::fabs(n1.y) > 0.5f ? 1 : 2);
+  float ac = ax == 0 ? approx.x : (ax == 1 ? approx.y : approx.z);
+  float roA = ax == 0 ? ro.x : (ax == 1 ? ro.y : ro.z);
+  float rdA = ax == 0 ? rd.x : (ax == 1 ? rd.y : rd.z);
+  if (std::fabs(rdA) < 1e-4f) return approx;
+  float d = std::nearbyint(ac * INV_VOXEL) * VOXEL_SIZE;
+  float tp = (d - roA) / rdA;
+  return tp > 0.0f ? add(ro, muls(rd, tp)) : approx;
+}
+
+// surfaceAt (reuse_spatial.wgsl:111-114)
+inline f3 surface_at(const Uni& u, int qx, int qy, int Wd, int Hd, const float* g) {
+  return receiver_point(mk(u.camPos[0], u.camPos[1], u.camPos[2]),
+                        camera_ray(u, ((float)qx + 0.5f) / (float)Wd, ((float)qy + 0.5f) / (float)Hd), g[3],
+                        mk(g[0], g[1], g[2]));
+}
+
+inline f3 firefly(float fclamp, f3 v) { return fclamp <= 0.0f ? v : min3(v, mk(fclamp, fclamp, fclamp)); }
+
+// estimateLo (pathtrace.wgsl:205-246), unification off.
+f3 estimate_lo(const World& W, const Uni& u, float fclamp, f3 x2, f3 n2, Mat mat2, Rng& rng, PixStats& st) {
+  auto shadowed = [&](f3 o, f3 d, float maxT) {
+    Hit h = trace(W, o, d, maxT);
+    st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+    return h.t >= 0.0f;
+  };
+  f3 Lo = mk(0, 0, 0), tp = mk(1, 1, 1);
+  f3 pos = x2, n = n2;
+  Mat mat = mat2;
+  const uint32_t nB = u.params0[1];
+  f3 sunRad = mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
+  for (uint32_t v = 1u; v <= nB; v++) {
+    if (mat.emissive > 0.0f && v > 1u) Lo = add(Lo, muls(mul(tp, mat.albedo), mat.emissive * EMISSIVE_SCALE));
+    f3 surf = add(pos, muls(n, 1e-3f));
+    f3 l = sample_sun_dir(u, rng);
+    float ndl = dot3(n, l);
+    if (ndl > 0.0f && l.y > 0.0f && !shadowed(surf, l, 1e4f))
+      Lo = add(Lo, mul(muls(muls(mul(tp, mat.albedo), INV_PI), ndl), sunRad));
+    if (v == nB) break;
+    f3 rd = cosine_hemisphere(n, rng);
+    tp = mul(tp, mat.albedo);
+    if (v >= 2u) {
+      float p = clampf(fmaxf_(tp.x, fmaxf_(tp.y, tp.z)), 0.05f, 0.95f);
+      if (rng.next() > p) break;
+      tp = mk(tp.x / p, tp.y / p, tp.z / p);
+    }
+    Hit h = trace(W, surf, rd, 1e4f);
+    st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+    if (h.t < 0.0f) {
+      Lo = add(Lo, mul(tp, sky_color(u, rd, false)));
+      break;
+    }
+    pos = add(surf, muls(rd, h.t));
+    n = h.n;
+    mat = unpack_material(h.mat);
+  }
+  return firefly(fclamp, Lo);
+}
+
+// Initial candidates of one pixel (pathtrace.wgsl:248-284, 332-457,
+// RF_UNIFIED off).  Outputs: rgba16f radiance (sky pixels only), fp32 copy,
+// albedo, G-buffer, reservoir A, rgba16f pass-through radiance.
+void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, int gy, int Wd, int Hd,
+                          uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, uint32_t* resA,
+                          uint16_t* direct16, PixStats& st) {
+  const size_t p = (size_t)gy * Wd + gx;
+  auto count = [&](const Hit& h) { st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads; };
+  Rng rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0]);
+  float jx = rng.next() - 0.5f;
+  float jy = rng.next() - 0.5f;
+  f3 ro = mk(u.camPos[0], u.camPos[1], u.camPos[2]);
+  f3 rd = camera_ray(u, (((float)gx + 0.5f) + jx) / (float)Wd, (((float)gy + 0.5f) + jy) / (float)Hd);
+  Hit h0 = trace(W, ro, rd, 1e4f);
+  count(h0);
+  if (h0.t < 0.0f) {
+    f3 sky = sky_color(u, rd, true);
+    const float v[4] = {sky.x, sky.y, sky.z, 1.0f};
+    for (int c = 0; c < 4; c++) {
+      rad16[4 * p + c] = f32_to_f16(v[c]);
+      if (rad32) rad32[4 * p + c] = v[c];
+      direct16[4 * p + c] = f32_to_f16(v[c]);
+      alb8[4 * p + c] = 255;
+    }
+    gbuf[4 * p] = -rd.x; gbuf[4 * p + 1] = -rd.y; gbuf[4 * p + 2] = -rd.z; gbuf[4 * p + 3] = -1.0f;
+    std::memset(resA + 8 * p, 0, 32);
+    return;
+  }
+  Mat mat1 = unpack_material(h0.mat);
+  f3 x1 = add(ro, muls(rd, h0.t));
+  f3 n1 = h0.n;
+  f3 surf1 = add(x1, muls(n1, fmaxf_(1e-3f, h0.t * 1e-4f)));
+  alb8[4 * p] = unorm8(std::sqrt(mat1.albedo.x));
+  alb8[4 * p + 1] = unorm8(std::sqrt(mat1.albedo.y));
+  alb8[4 * p + 2] = unorm8(std::sqrt(mat1.albedo.z));
+  alb8[4 * p + 3] = 255;
+  gbuf[4 * p] = n1.x; gbuf[4 * p + 1] = n1.y; gbuf[4 * p + 2] = n1.z; gbuf[4 * p + 3] = h0.t;
+
+  float em = mat1.emissive * EMISSIVE_SCALE;
+  f3 direct = mk(em, em, em);
+  float wSum = 0.0f, selP = 0.0f;
+  RSample sel = null_sample(0.0f);
+  {
+    f3 l = sample_sun_dir(u, rng);
+    float ndl = dot3(n1, l);
+    if (ndl > 0.0f && l.y > 0.0f) {
+      Hit hs = trace(W, surf1, l, 1e4f);
+      count(hs);
+      if (!(hs.t >= 0.0f)) direct = add(direct, muls(mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]),
+                                                    INV_PI * ndl));
+    }
+  }
+  if (u.params0[1] > 0u) {
+    f3 brd = cosine_hemisphere(n1, rng);
+    Hit h = trace(W, surf1, brd, 1e4f);
+    count(h);
+    RSample s = null_sample(0.0f);
+    float Wc;
+    if (h.t < 0.0f) {
+      s.kind = SK_DIR;
+      s.pos = brd;
+      s.rad = sky_color(u, brd, false);
+      Wc = PI / fmaxf_(dot3(n1, brd), 1e-4f);
+    } else {
+      f3 x2 = add(surf1, muls(brd, h.t));
+      Mat mat2 = unpack_material(h.mat);
+      f3 Lo = estimate_lo(W, u, fclamp, x2, h.n, mat2, rng, st);
+      if (mat2.emissive > 0.0f) Lo = add(Lo, muls(mat2.albedo, mat2.emissive * EMISSIVE_SCALE));
+      s.kind = SK_POINT;
+      s.pos = x2;
+      s.n = h.n;
+      s.rad = firefly(fclamp, Lo);
+      f3 d = sub(x2, x1);
+      float r2 = fmaxf_(dot3(d, d), 1e-6f);
+      f3 dn = normalize3(d);
+      float cos1 = fmaxf_(dot3(n1, dn), 1e-4f);
+      float cos2 = fmaxf_(dot3(h.n, mk(-dn.x, -dn.y, -dn.z)), 1e-4f);
+      Wc = ((PI / cos1) * r2) / cos2;
+    }
+    float pt = eval_target(s, x1, n1);
+    float w = pt * Wc;
+    if (w > 0.0f) {
+      wSum = wSum + w;
+      if (rng.next() * wSum < w) { sel = s; selP = pt; }
+    }
+  }
+  RSample out = null_sample(0.0f);
+  if (sel.kind != SK_NONE && selP > 0.0f) {
+    out = sel;
+    out.W = wSum / selP;
+  }
+  out.c = 1.0f;
+  out.seed = pcg_hash((uint32_t)p + u.params0[0] * ((uint32_t)Wd * (uint32_t)Hd + 1u));
+  pack_res(out, resA + 8 * p);
+  const float dv[4] = {direct.x, direct.y, direct.z, 1.0f};
+  for (int c = 0; c < 4; c++) direct16[4 * p + c] = f32_to_f16(dv[c]);
+}
+
+// Temporal reuse of one pixel (reuse_temporal.wgsl:38-46, 140-279 without
+// dupmap / rescue / world cache / mutation).
+void restir_temporal_pixel(const Uni& u, int gx, int gy, int Wd, int Hd, const float* gbufCur,
+                           const float* gbufPrev, const uint32_t* resB, uint32_t* resA) {
+  const size_t p = (size_t)gy * Wd + gx;
+  const float* g = gbufCur + 4 * p;
+  if (g[3] <= 0.0f) return;
+  Rng rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x5f356495u);
+  f3 n1 = mk(g[0], g[1], g[2]);
+  f3 x1 = surface_at(u, gx, gy, Wd, Hd, g);
+  const float wp[4] = {x1.x, x1.y, x1.z, 1.0f};
+  float pc[4];
+  matvec4(u.prevViewProj, wp, pc);
+  if (pc[3] <= 0.0f) return;
+  float ndx = pc[0] / pc[3], ndy = pc[1] / pc[3];
+  int ppx = itrunc((ndx * 0.5f + 0.5f) * (float)Wd);
+  int ppy = itrunc(((-ndy) * 0.5f + 0.5f) * (float)Hd);
+  if (ppx < 0 || ppy < 0 || ppx >= Wd || ppy >= Hd) return;
+  const float* pg = gbufPrev + 4 * ((size_t)ppy * Wd + ppx);
+  if (pg[3] <= 0.0f) return;
+  f3 dv = sub(x1, mk(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]));
+  float expectedT = length3(dv);
+  bool depthOk = std::fabs(pg[3] - expectedT) < 0.08f * expectedT + 0.02f;
+  bool normalOk = dot3(mk(pg[0], pg[1], pg[2]), n1) > 0.9f;
+  if (!(depthOk && normalOk)) return;
+  RSample sT = unpack_res(resB + 8 * ((size_t)ppy * Wd + ppx));
+  float cT = fminf_(sT.c, u.params3[0]);
+  RSample sC = unpack_res(resA + 8 * p);
+  float cC = fmaxf_(sC.c, 0.0f);
+  float pC = eval_target(sC, x1, n1), pT = eval_target(sT, x1, n1);
+  float mDen = fmaxf_(cC + cT, 1e-3f);
+  float wC = ((cC / mDen) * pC) * fmaxf_(sC.W, 0.0f);
+  float wT = ((cT / mDen) * pT) * fmaxf_(sT.W, 0.0f);
+  float wSum = wC + wT;
+  if (wSum <= 0.0f) {
+    pack_res(null_sample(cC + cT), resA + 8 * p);
+    return;
+  }
+  RSample sel = sC;
+  float selP = pC;
+  if (rng.next() * wSum >= wC) { sel = sT; selP = pT; }
+  if (selP <= 0.0f) return;
+  sel.W = wSum / selP;
+  sel.c = cC + cT;
+  pack_res(sel, resA + 8 * p);
+}
+
+// Spatial reuse + shading of one pixel (reuse_spatial.wgsl:116-126, 128-354:
+// random disk, generic neighbour test, scalar shading weight).
+void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, int Hd, const float* gbufCur,
+                          const uint32_t* resA, const uint16_t* direct16, uint16_t* rad16, float* rad32,
+                          uint32_t* resB, PixStats& st) {
+  const size_t p = (size_t)gy * Wd + gx;
+  f3 direct = mk(f16_to_f32(direct16[4 * p]), f16_to_f32(direct16[4 * p + 1]), f16_to_f32(direct16[4 * p + 2]));
+  auto out_radiance = [&](f3 v) {
+    const float o[4] = {v.x, v.y, v.z, 1.0f};
+    for (int c = 0; c < 4; c++) {
+      rad16[4 * p + c] = f32_to_f16(o[c]);
+      if (rad32) rad32[4 * p + c] = o[c];
+    }
+  };
+  const float* g = gbufCur + 4 * p;
+  if (g[3] <= 0.0f) {
+    out_radiance(direct);
+    std::memset(resB + 8 * p, 0, 32);
+    return;
+  }
+  Rng rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
+  f3 x1 = surface_at(u, gx, gy, Wd, Hd, g);
+  f3 n1 = mk(g[0], g[1], g[2]);
+  f3 domX1[4], domN1[4];
+  float domC[4];
+  RSample cand[4];
+  uint32_t candDom[4];
+  uint32_t nDom = 1u, nCand = 0u;
+  RSample canonical = unpack_res(resA + 8 * p);
+  domX1[0] = x1; domN1[0] = n1; domC[0] = canonical.c;
+  if (canonical.kind != SK_NONE) { cand[0] = canonical; candDom[0] = 0u; nCand = 1u; }
+  if (u.params2[0] & RF_SPATIAL) {
+    uint32_t taps = std::min(u.params2[2], 3u);
+    for (uint32_t ti = 0u; ti < taps; ti++) {
+      float r = u.params4[0] * std::sqrt(rng.next());
+      float a = TWO_PI * rng.next();
+      float sa, ca;
+      om_sincos(a, sa, ca);
+      int qx = gx + itrunc(ca * r), qy = gy + itrunc(sa * r);
+      if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= Wd || qy >= Hd) continue;
+      size_t q = (size_t)qy * Wd + qx;
+      const float* gq = gbufCur + 4 * q;
+      if (gq[3] <= 0.0f) continue;
+      f3 x1q = surface_at(u, qx, qy, Wd, Hd, gq);
+      f3 nq = mk(gq[0], gq[1], gq[2]);
+      float nDot = dot3(n1, nq);
+      if (!(nDot > 0.9f && std::fabs(gq[3] - g[3]) < 0.1f * g[3] + 0.02f)) continue;
+      RSample rq = unpack_res(resA + 8 * q);
+      domX1[nDom] = x1q; domN1[nDom] = nq; domC[nDom] = rq.c;
+      if (rq.kind != SK_NONE) { cand[nCand] = rq; candDom[nCand] = nDom; nCand++; }
+      nDom++;
+    }
+  }
+  float cTotal = 0.0f;
+  for (uint32_t l = 0u; l < nDom; l++) cTotal = cTotal + domC[l];
+  float wSum = 0.0f, selP = 0.0f;
+  RSample sel = null_sample(0.0f);
+  uint32_t selJ = 0u;
+  for (uint32_t j = 0u; j < nCand; j++) {
+    const RSample& s = cand[j];
+    float denom = 0.0f;
+    for (uint32_t l = 0u; l < nDom; l++) denom = denom + domC[l] * eval_target(s, domX1[l], domN1[l]);
+    if (denom <= 0.0f) continue;
+    uint32_t dj = candDom[j];
+    float m = (domC[dj] * eval_target(s, domX1[dj], domN1[dj])) / denom;
+    float pMe = eval_target(s, x1, n1);
+    float w = (m * pMe) * fmaxf_(s.W, 0.0f);
+    if (w > 0.0f) {
+      wSum = wSum + w;
+      if (rng.next() * wSum < w) { sel = s; selP = pMe; selJ = j; }
+    }
+  }
+  if (nCand == 0u || sel.kind == SK_NONE || selP <= 0.0f || wSum <= 0.0f) {
+    out_radiance(direct);
+    pack_res(null_sample(fminf_(cTotal, 255.0f)), resB + 8 * p);
+    return;
+  }
+  sel.W = wSum / selP;
+  sel.c = fminf_(cTotal, 255.0f);
+  bool vis = true;
+  if (selJ > 0u) {   // sampleVisible (reuse_spatial.wgsl:117-126)
+    f3 surf = add(x1, muls(n1, 1e-3f));
+    Hit h;
+    if (sel.kind == SK_DIR) {
+      h = trace(W, surf, sel.pos, 1e4f);
+      st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+      vis = !(h.t >= 0.0f);
+    } else {
+      f3 d = sub(sel.pos, surf);
+      float r = length3(d);
+      if (!(r < 2e-3f)) {
+        h = trace(W, surf, mk(d.x / r, d.y / r, d.z / r), r - 2e-3f);
+        st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+        vis = !(h.t >= 0.0f);
+      }
+    }
+  }
+  f3 contrib = vis ? muls(eval_f(sel, x1, n1), sel.W) : mk(0, 0, 0);
+  out_radiance(add(direct, contrib));
+  pack_res(sel, resB + 8 * p);
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1216,6 +1637,56 @@ long orc_collect_rays(const uint32_t* vox, const uint32_t* bricks, const uint32_
     total += n;
   }
   return total;
+}
+
+// ReSTIR `gi` passes over whole images (reservoirs: 8 u32 per pixel in the
+// 32-byte record of restir.wgsl:14-27).  stats (optional) receives the rays
+// the pass traced.
+void orc_restir_initial(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                        const void* uniforms, float fclamp, int Wd, int Hd, uint16_t* rad16, float* rad32,
+                        uint8_t* alb8, float* gbuf, uint32_t* resA, uint16_t* direct16, OrcStats* stats) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  uint64_t rays = 0, outer = 0, inner = 0, vreads = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads)
+  for (int y = 0; y < Hd; y++) {
+    PixStats st{0, 0, 0, 0};
+    for (int x = 0; x < Wd; x++)
+      restir_initial_pixel(W, u, fclamp, x, y, Wd, Hd, rad16, rad32, alb8, gbuf, resA, direct16, st);
+    rays += st.rays; outer += st.outer; inner += st.inner; vreads += st.vreads;
+  }
+  if (stats) {
+    stats->rays = rays; stats->outer = outer; stats->inner = inner; stats->vreads = vreads;
+    stats->pixels = (uint64_t)Wd * Hd;
+  }
+}
+
+void orc_restir_temporal(const void* uniforms, int Wd, int Hd, const float* gbufCur, const float* gbufPrev,
+                         const uint32_t* resB, uint32_t* resA) {
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  if (!(u.params2[0] & 1u) || !(u.params2[0] & 2u)) return;   // reuse_temporal.wgsl:144
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < Hd; y++)
+    for (int x = 0; x < Wd; x++) restir_temporal_pixel(u, x, y, Wd, Hd, gbufCur, gbufPrev, resB, resA);
+}
+
+void orc_restir_spatial(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                        const void* uniforms, int Wd, int Hd, const float* gbufCur, const uint32_t* resA,
+                        const uint16_t* direct16, uint16_t* rad16, float* rad32, uint32_t* resB, OrcStats* stats) {
+  World W{vox, bricks, masks, N, N / BRICK};
+  Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  uint64_t rays = 0, outer = 0, inner = 0, vreads = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads)
+  for (int y = 0; y < Hd; y++) {
+    PixStats st{0, 0, 0, 0};
+    for (int x = 0; x < Wd; x++)
+      restir_spatial_pixel(W, u, x, y, Wd, Hd, gbufCur, resA, direct16, rad16, rad32, resB, st);
+    rays += st.rays; outer += st.outer; inner += st.inner; vreads += st.vreads;
+  }
+  if (stats) {
+    stats->rays = rays; stats->outer = outer; stats->inner = inner; stats->vreads = vreads;
+    stats->pixels = 0;
+  }
 }
 
 }  // extern "C"

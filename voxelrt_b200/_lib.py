@@ -89,7 +89,7 @@ class VrtFrameStats(C.Structure):
                 ("ms_temporal", C.c_float), ("ms_atrous", C.c_float), ("ms_present", C.c_float),
                 ("ms_total", C.c_float), ("launches", C.c_uint32), ("trace_launches", C.c_uint32),
                 ("ms_trace", C.c_float), ("cache_on", C.c_uint32), ("cache_queries", C.c_uint64),
-                ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("pad", C.c_uint32)]
+                ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("ms_reuse", C.c_float)]
 
 
 class VrtLightStats(C.Structure):
@@ -142,6 +142,8 @@ SIGNATURES = {
     "vrt_session_reset": (I, [P]),
     "vrt_frame": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_pathtrace": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_reuse_temporal": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_reuse_spatial": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_temporal": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_atrous": (I, [P, C.POINTER(VrtUniforms), I]),
     "vrt_pass_present": (I, [P, C.POINTER(VrtUniforms)]),
@@ -159,6 +161,8 @@ SIGNATURES = {
     "vrt_read_denoise": (I, [P, I, P, SZ]),
     "vrt_read_final": (I, [P, P, SZ]),
     "vrt_read_ldr": (I, [P, P, SZ]),
+    "vrt_read_reservoirs": (I, [P, I, P, SZ]),
+    "vrt_read_direct": (I, [P, P, SZ]),
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),

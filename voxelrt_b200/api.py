@@ -110,12 +110,36 @@ def camera_matrices(pose: CameraPose, aspect: float):
     return vp, ivp
 
 
+# ReSTIR flag bits of params2.x (common.wgsl:40-59) and the presets built from
+# them (main.js:34-62).  This build implements `base` and `gi`.
+RF = {"restir": 1, "treuse": 2, "sreuse": 4, "paired": 8, "dupmap": 16, "footprint": 32, "vector": 64,
+      "unified": 128, "plane": 256, "rescue": 512, "fullv": 1024, "rclamp": 2048, "lightpower": 4096,
+      "mixsigma": 8192, "adaptcand": 16384, "confdenoise": 32768, "lightgrid": 65536, "mutate": 131072,
+      "histisolate": 262144, "worldgi": 524288}
+PRESETS = {"base": [], "gi": ["restir", "treuse", "sreuse"]}
+
+
+def preset_flags(preset: str) -> int:
+    flags = 0
+    for k in PRESETS[preset]:
+        flags |= RF[k]
+    return flags
+
+
 def make_uniforms(cur: CameraPose, prev: CameraPose | None, light: Lighting, frame: int, bounces: int, flags: int,
-                  width: int, height: int, exposure: float = 1.0, max_history: float = 64.0) -> VrtUniforms:
+                  width: int, height: int, exposure: float = 1.0, max_history: float = 64.0, preset: str = "base",
+                  taps: int = 3, ccap: float = 20.0, radius: float = 30.0) -> VrtUniforms:
+    """The 304-byte uniform block (main.js:399-426).  preset selects the
+    reservoir flags of params2.x; taps, ccap and radius are the reference's
+    tuning defaults (main.js:72-76) in params2.z, params3.x, params4.x."""
     u = VrtUniforms()
     check(lib.vrt_make_uniforms(C.byref(cur.c()), C.byref(prev.c()) if prev is not None else None,
                                 C.byref(light.c()), int(frame) & 0xFFFFFFFF, int(bounces), int(flags), int(width),
                                 int(height), float(exposure), float(max_history), C.byref(u)))
+    u.params2[0] = preset_flags(preset)
+    u.params2[2] = int(taps)
+    u.params3[0] = float(ccap)
+    u.params4[0] = float(radius)
     return u
 
 
@@ -252,6 +276,8 @@ class Session:
         check(lib.vrt_frame(self.h, C.byref(u)))
 
     def pathtrace(self, u): check(lib.vrt_pass_pathtrace(self.h, C.byref(u)))
+    def reuse_temporal(self, u): check(lib.vrt_pass_reuse_temporal(self.h, C.byref(u)))
+    def reuse_spatial(self, u): check(lib.vrt_pass_reuse_spatial(self.h, C.byref(u)))
     def temporal(self, u): check(lib.vrt_pass_temporal(self.h, C.byref(u)))
     def atrous(self, u, it): check(lib.vrt_pass_atrous(self.h, C.byref(u), int(it)))
     def present(self, u): check(lib.vrt_pass_present(self.h, C.byref(u)))
@@ -376,6 +402,8 @@ class Session:
     def gbuffer(self): return self._read(lib.vrt_read_gbuffer, np.float32, 4)
     def ldr(self): return self._read(lib.vrt_read_ldr, np.uint8, 4)
     def denoise(self, i): return self._read(lib.vrt_read_denoise, np.uint16, 4, int(i))
+    def reservoirs(self, which: int): return self._read(lib.vrt_read_reservoirs, np.uint32, 8, int(which))
+    def direct(self): return self._read(lib.vrt_read_direct, np.uint16, 4)
 
     def accum(self):
         return self._read(lib.vrt_read_accum, np.float32 if self.accum_f32 else np.uint16, 4)

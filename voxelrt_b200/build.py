@@ -22,9 +22,10 @@ BUILD = PKG / "_build"
 LIB = PKG / "libvrt.so"
 
 CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_atrous_tma.cu", "k_wavefront.cu", "k_noalloc.cu", "k_batch.cu",
-              "k_mlp.cu", "k_hdr.cu", "k_lights.cu"]
+              "k_mlp.cu", "k_hdr.cu", "k_lights.cu", "k_restir.cu"]
 CPP_SOURCES = ["vrt_api.cpp", "scene_gen.cpp"]
-HEADERS = ["vrt_device.cuh", "vrt_internal.h", "wavefront_core.cuh", "image_core.cuh", "umma.cuh"]
+HEADERS = ["vrt_device.cuh", "vrt_internal.h", "wavefront_core.cuh", "image_core.cuh", "umma.cuh",
+           "trace_kernel.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FP_CONTRACT = ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]

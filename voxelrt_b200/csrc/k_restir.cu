@@ -1,0 +1,553 @@
+// k_restir.cu -- the reference's ReSTIR GI preset (`preset=gi`, main.js:44:
+// flags RF_RESTIR | RF_TEMPORAL | RF_SPATIAL): reservoirs for indirect light
+// only, temporal reuse with a confidence cap, random-disk spatial reuse and
+// shading of the selected sample.  Three passes, as the reference dispatches
+// them (main.js:736-739):
+//
+//   initial  (pathtrace.wgsl:248-284, 332-457, RF_UNIFIED off): primary hit,
+//            G-buffer and albedo, pass-through radiance `direct` = emission +
+//            sun-cone NEE, one BSDF bounce candidate whose reconnection vertex
+//            x2 carries Lo(x2) estimated by continuing the path (estimateLo,
+//            pathtrace.wgsl:205-246) -> reservoirs A, direct -> rgba16f
+//   temporal (reuse_temporal.wgsl:140-279, no dupmap / rescue / world cache /
+//            mutation): confidence-weighted merge with the reprojected history
+//            reservoir of B -> A
+//   spatial  (reuse_spatial.wgsl:128-354, random disk, generic neighbour test,
+//            scalar shading weight): balance-heuristic merge over the canonical
+//            and up to three neighbour domains, one visibility ray for a
+//            neighbour's sample, radiance (demodulated) = direct + f W -> rgba16f,
+//            post-reuse reservoir -> B (next frame's history)
+//
+// Reservoirs keep the reference's 32-byte record (restir.wgsl:14-31, 61-84):
+// posW = (position or direction, W); data = (radiance RG as f16 x 2, radiance
+// B f16 | kind << 16 | confidence u8 << 18, octahedral normal as snorm16 x 2,
+// seed), stored as two 16-byte words per pixel (array-of-structures: the
+// spatial pass gathers whole records of random neighbours, one 32-byte sector
+// each).  One thread per pixel; 16 x 16 blocks whose warps cover 8 x 4 tiles;
+// the brick occupancy bitmap is staged in shared memory.  The arithmetic
+// follows the WGSL expression by expression (no contraction), so the CPU
+// restatement reproduces every word bit for bit.
+#include "trace_kernel.cuh"
+
+namespace vrt {
+
+enum : uint32_t { kSkNone = 0u, kSkPoint = 1u, kSkDir = 2u };   // restir.wgsl:29-31
+
+// Decoded reservoir sample (restir.wgsl:33-41).
+struct RSample {
+  uint32_t kind;
+  F3 pos, n, rad;
+  float W, c;
+  uint32_t seed;
+};
+
+VRT_DI RSample null_sample(float c) {
+  RSample s;
+  s.kind = kSkNone;
+  s.pos = s.n = s.rad = f3(0.0f, 0.0f, 0.0f);
+  s.W = 0.0f;
+  s.c = c;
+  s.seed = 0u;
+  return s;
+}
+
+// WGSL f32 -> i32 conversion: toward zero, saturating, NaN -> 0.
+VRT_DI int itrunc_(float x) { return __float2int_rz(x); }
+
+// pack2x16snorm / unpack2x16snorm, one component.
+VRT_DI uint32_t snorm16(float v) {
+  const float c = fmin_(1.0f, fmax_(-1.0f, v));
+  return (uint32_t)(uint16_t)(int16_t)(int)floorf(0.5f + 32767.0f * c);
+}
+VRT_DI float unsnorm16(uint32_t b) { return fmax_((float)(int16_t)(uint16_t)b / 32767.0f, -1.0f); }
+
+VRT_DI float sgn_ge0(float x) { return x >= 0.0f ? 1.0f : -1.0f; }
+
+// octEncode / octDecode (restir.wgsl:43-59).
+VRT_DI void oct_encode(F3 nIn, float& ex, float& ey) {
+  const float s = (fabsf(nIn.x) + fabsf(nIn.y)) + fabsf(nIn.z);
+  const F3 n = f3(nIn.x / s, nIn.y / s, nIn.z / s);
+  ex = n.x;
+  ey = n.y;
+  if (n.z < 0.0f) {
+    ex = (1.0f - fabsf(n.y)) * sgn_ge0(n.x);
+    ey = (1.0f - fabsf(n.x)) * sgn_ge0(n.y);
+  }
+}
+
+VRT_DI F3 oct_decode(float ex, float ey) {
+  F3 n = f3(ex, ey, (1.0f - fabsf(ex)) - fabsf(ey));
+  if (n.z < 0.0f) n = f3((1.0f - fabsf(n.y)) * sgn_ge0(n.x), (1.0f - fabsf(n.x)) * sgn_ge0(n.y), n.z);
+  return normalize3(n);
+}
+
+// packReservoir (restir.wgsl:61-71) into the two 16-byte words of pixel p.
+VRT_DI void store_res(uint4* res, size_t p, const RSample& s) {
+  const uint32_t cq = min((uint32_t)__float2uint_rz(s.c + 0.5f), 255u);
+  const F3 nn = s.kind != kSkPoint ? f3(0.0f, 1.0f, 0.0f) : s.n;
+  float ex, ey;
+  oct_encode(nn, ex, ey);
+  res[2 * p] = make_uint4(__float_as_uint(s.pos.x), __float_as_uint(s.pos.y), __float_as_uint(s.pos.z),
+                          __float_as_uint(s.W));
+  res[2 * p + 1] = make_uint4(h2bits(s.rad.x) | (h2bits(s.rad.y) << 16),
+                              (h2bits(s.rad.z) & 0xffffu) | (s.kind << 16) | (cq << 18),
+                              snorm16(ex) | (snorm16(ey) << 16), s.seed);
+}
+
+// unpackReservoir (restir.wgsl:73-84).
+VRT_DI RSample load_res(const uint4* res, size_t p) {
+  const uint4 a = res[2 * p], d = res[2 * p + 1];
+  RSample s;
+  s.pos = f3(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z));
+  s.W = __uint_as_float(a.w);
+  s.rad = f3(bits2f(d.x & 0xffffu), bits2f(d.x >> 16), bits2f(d.y & 0xffffu));
+  s.kind = (d.y >> 16) & 3u;
+  s.c = (float)((d.y >> 18) & 0xffu);
+  s.n = oct_decode(unsnorm16(d.z & 0xffffu), unsnorm16(d.z >> 16));
+  s.seed = d.w;
+  return s;
+}
+
+VRT_DI float rlum(F3 c) { return (c.x * 0.2126f + c.y * 0.7152f) + c.z * 0.0722f; }   // restir.wgsl:90-92
+
+// evalF (restir.wgsl:143-159): demodulated integrand without visibility;
+// inverseSqrt(r2) is 1 / sqrt(r2).
+VRT_DI F3 eval_f(const RSample& s, F3 x1, F3 n1) {
+  if (s.kind == kSkPoint) {
+    const F3 d = s.pos - x1;
+    const float r2 = fmax_(dot3(d, d), 1e-4f);
+    const F3 dir = d * (1.0f / __fsqrt_rn(r2));
+    const float cos1 = dot3(n1, dir);
+    const float cos2 = dot3(s.n, f3(-dir.x, -dir.y, -dir.z));
+    if (cos1 <= 0.0f || cos2 <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
+    return s.rad * (((kInvPi * cos1) * cos2) / r2);
+  }
+  if (s.kind == kSkDir) {
+    const float cos1 = dot3(n1, s.pos);
+    if (cos1 <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
+    return s.rad * (kInvPi * cos1);
+  }
+  return f3(0.0f, 0.0f, 0.0f);
+}
+VRT_DI float eval_target(const RSample& s, F3 x1, F3 n1) { return rlum(eval_f(s, x1, n1)); }
+
+// receiverPoint (restir.wgsl:127-137): the reconstruction ray meets the voxel
+// face plane recovered by rounding (half to even) the dominant coordinate.
+VRT_DI F3 receiver_point(F3 ro, F3 rd, float t, F3 n1) {
+  const F3 approx = ro + rd * t;
+  const int ax = fabsf(n1.x) > 0.5f ? 0 : (fabsf(n1.y) > 0.5f ? 1 : 2);
+  const float ac = ax == 0 ? approx.x : (ax == 1 ? approx.y : approx.z);
+  const float roA = ax == 0 ? ro.x : (ax == 1 ? ro.y : ro.z);
+  const float rdA = ax == 0 ? rd.x : (ax == 1 ? rd.y : rd.z);
+  if (fabsf(rdA) < 1e-4f) return approx;
+  const float d = rintf(ac * kInvVoxel) * kVoxelSize;
+  const float tp = (d - roA) / rdA;
+  return tp > 0.0f ? ro + rd * tp : approx;
+}
+
+// surfaceAt (reuse_spatial.wgsl:111-114) / the temporal pass's x1.
+VRT_DI F3 surface_at(const Uni& u, int qx, int qy, int W, int H, float4 g) {
+  return receiver_point(f3(u.camPos[0], u.camPos[1], u.camPos[2]),
+                        camera_ray(u, ((float)qx + 0.5f) / (float)W, ((float)qy + 0.5f) / (float)H), g.w,
+                        f3(g.x, g.y, g.z));
+}
+
+struct RestirDev {
+  DScene S;
+  Uni u;
+  int W, H;
+  float fclamp;
+  uint4* resA;              // working reservoirs (initial, then temporal merge)
+  uint4* resB;              // post-spatial reservoirs = next frame's history
+  uint2* direct;            // rgba16f pass-through radiance
+  uint2* rad16;             // rgba16f radiance (demodulated)
+  float4* rad32;            // optional fp32 copy of the radiance
+  uint32_t* alb8;
+  float4* gbuf;             // current G-buffer (n, t)
+  const float4* gprev;      // previous frame's G-buffer
+  unsigned long long* stats;
+};
+
+VRT_DI bool occluded(const RestirDev& R, const uint32_t* occ, F3 o, F3 d, float maxT, DCount& cnt) {
+  return trace<true>(R.S, occ, o, d, maxT, cnt).t >= 0.0f;
+}
+
+VRT_DI F3 fclamp3(const RestirDev& R, F3 v) {
+  return R.fclamp <= 0.0f ? v : min3(v, f3(R.fclamp, R.fclamp, R.fclamp));
+}
+
+// estimateLo (pathtrace.wgsl:205-246) with unification off: emission rides
+// on hits, sun-cone NEE at every vertex, Russian roulette from vertex 2.
+VRT_DI F3 estimate_lo(const RestirDev& R, const uint32_t* occ, F3 x2, F3 n2, Mat mat2, uint32_t& rng,
+                      DCount& cnt) {
+  const Uni& u = R.u;
+  F3 Lo = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
+  F3 pos = x2, n = n2;
+  Mat mat = mat2;
+  const uint32_t nB = u.params0[1];
+  const F3 sunRad = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
+  for (uint32_t v = 1u; v <= nB; v++) {
+    if (mat.emissive > 0.0f && v > 1u) Lo = Lo + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
+    const F3 surf = pos + n * 1e-3f;
+    const F3 l = sample_sun_dir(u, rng);
+    const float ndl = dot3(n, l);
+    if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf, l, 1e4f, cnt))
+      Lo = Lo + (((tp * mat.albedo) * kInvPi) * ndl) * sunRad;
+    if (v == nB) break;
+    const F3 rd = cosine_hemisphere(n, rng);
+    tp = tp * mat.albedo;
+    if (v >= 2u) {
+      const float p = clamp_(fmax_(tp.x, fmax_(tp.y, tp.z)), 0.05f, 0.95f);
+      if (rand_(rng) > p) break;
+      tp = f3(tp.x / p, tp.y / p, tp.z / p);
+    }
+    const DHit h = trace<true>(R.S, occ, surf, rd, 1e4f, cnt);
+    if (h.t < 0.0f) {
+      Lo = Lo + tp * sky_color(u, rd, false);
+      break;
+    }
+    pos = surf + rd * h.t;
+    n = h.n;
+    mat = unpack_material(h.mat);
+  }
+  return fclamp3(R, Lo);
+}
+
+// ---------------------------------------------------------------------------
+// initial candidates (pathtrace.wgsl:248-284, 332-457)
+// ---------------------------------------------------------------------------
+VRT_DI void initial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int gy, DCount& cnt) {
+  const Uni& u = R.u;
+  const size_t p = (size_t)gy * R.W + gx;
+  uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0]);
+  const float jx = rand_(rng) - 0.5f;
+  const float jy = rand_(rng) - 0.5f;
+  const F3 ro = f3(u.camPos[0], u.camPos[1], u.camPos[2]);
+  const F3 rd = camera_ray(u, (((float)gx + 0.5f) + jx) / (float)R.W, (((float)gy + 0.5f) + jy) / (float)R.H);
+  const DHit h0 = trace<true>(R.S, occ, ro, rd, 1e4f, cnt);
+  if (h0.t < 0.0f) {
+    const F3 sky = sky_color(u, rd, true);
+    const uint2 sk = pack_h4(sky.x, sky.y, sky.z, 1.0f);
+    R.rad16[p] = sk;
+    if (R.rad32) R.rad32[p] = make_float4(sky.x, sky.y, sky.z, 1.0f);
+    R.direct[p] = sk;
+    R.alb8[p] = 0xffffffffu;
+    R.gbuf[p] = make_float4(-rd.x, -rd.y, -rd.z, -1.0f);
+    R.resA[2 * p] = make_uint4(0u, 0u, 0u, 0u);
+    R.resA[2 * p + 1] = make_uint4(0u, 0u, 0u, 0u);
+    return;
+  }
+  const Mat mat1 = unpack_material(h0.mat);
+  const F3 x1 = ro + rd * h0.t;
+  const F3 n1 = h0.n;
+  const F3 surf1 = x1 + n1 * fmax_(1e-3f, h0.t * 1e-4f);
+  R.alb8[p] = unorm8_(__fsqrt_rn(mat1.albedo.x)) | (unorm8_(__fsqrt_rn(mat1.albedo.y)) << 8) |
+              (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
+  R.gbuf[p] = make_float4(n1.x, n1.y, n1.z, h0.t);
+
+  const float em = mat1.emissive * kEmissiveScale;
+  F3 direct = f3(em, em, em);
+  float wSum = 0.0f, selP = 0.0f;
+  RSample sel = null_sample(0.0f);
+  {   // sun-cone NEE at x1: pass-through radiance when unification is off
+    const F3 l = sample_sun_dir(u, rng);
+    const float ndl = dot3(n1, l);
+    if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf1, l, 1e4f, cnt))
+      direct = direct + f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
+  }
+  if (u.params0[1] > 0u) {   // BSDF bounce candidate: reconnection vertex x2 carries Lo
+    const F3 brd = cosine_hemisphere(n1, rng);
+    const DHit h = trace<true>(R.S, occ, surf1, brd, 1e4f, cnt);
+    RSample s = null_sample(0.0f);
+    float Wc;
+    if (h.t < 0.0f) {
+      s.kind = kSkDir;
+      s.pos = brd;
+      s.rad = sky_color(u, brd, false);
+      Wc = kPi / fmax_(dot3(n1, brd), 1e-4f);
+    } else {
+      const F3 x2 = surf1 + brd * h.t;
+      const Mat mat2 = unpack_material(h.mat);
+      F3 Lo = estimate_lo(R, occ, x2, h.n, mat2, rng, cnt);
+      if (mat2.emissive > 0.0f) Lo = Lo + mat2.albedo * (mat2.emissive * kEmissiveScale);
+      s.kind = kSkPoint;
+      s.pos = x2;
+      s.n = h.n;
+      s.rad = fclamp3(R, Lo);
+      const F3 d = x2 - x1;
+      const float r2 = fmax_(dot3(d, d), 1e-6f);
+      const F3 dn = normalize3(d);
+      const float cos1 = fmax_(dot3(n1, dn), 1e-4f);
+      const float cos2 = fmax_(dot3(h.n, f3(-dn.x, -dn.y, -dn.z)), 1e-4f);
+      Wc = ((kPi / cos1) * r2) / cos2;
+    }
+    const float pt = eval_target(s, x1, n1);
+    const float w = pt * Wc;
+    if (w > 0.0f) {
+      wSum = wSum + w;
+      if (rand_(rng) * wSum < w) { sel = s; selP = pt; }
+    }
+  }
+  RSample out = null_sample(0.0f);
+  if (sel.kind != kSkNone && selP > 0.0f) {
+    out = sel;
+    out.W = wSum / selP;
+  }
+  out.c = 1.0f;   // a failed candidate is a zero-valued outcome, confidence 1
+  out.seed = pcg_hash((uint32_t)p + u.params0[0] * ((uint32_t)R.W * (uint32_t)R.H + 1u));
+  store_res(R.resA, p, out);
+  R.direct[p] = pack_h4(direct.x, direct.y, direct.z, 1.0f);
+}
+
+template <bool kSmem>
+__global__ void __launch_bounds__(256) k_restir_initial(const __grid_constant__ RestirDev R) {
+  extern __shared__ uint32_t s_occ[];
+  const uint32_t* occ = stage_occupancy<kSmem>(R.S, s_occ);
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
+  DCount cnt{0u, 0u, 0u, 0u};
+  uint32_t pix = 0u;
+  if (gx < R.W && gy < R.H) {
+    initial_pixel(R, occ, gx, gy, cnt);
+    pix = 1u;
+  }
+  if (R.stats) warp_flush_stats(R.stats, cnt, pix);
+}
+
+// ---------------------------------------------------------------------------
+// temporal reuse (reuse_temporal.wgsl:38-46, 140-279)
+// ---------------------------------------------------------------------------
+VRT_DI bool valid_prev(const RestirDev& R, int px, int py, F3 wp, F3 n1) {
+  if (px < 0 || py < 0 || px >= R.W || py >= R.H) return false;
+  const float4 pg = R.gprev[(size_t)py * R.W + px];
+  if (pg.w <= 0.0f) return false;
+  const F3 dv = wp - f3(R.u.prevCamPos[0], R.u.prevCamPos[1], R.u.prevCamPos[2]);
+  const float expectedT = __fsqrt_rn(dot3(dv, dv));
+  const bool depthOk = fabsf(pg.w - expectedT) < 0.08f * expectedT + 0.02f;
+  const bool normalOk = dot3(f3(pg.x, pg.y, pg.z), n1) > 0.9f;
+  return depthOk && normalOk;
+}
+
+__global__ void __launch_bounds__(256) k_restir_temporal(const __grid_constant__ RestirDev R) {
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
+  if (gx >= R.W || gy >= R.H) return;
+  const Uni& u = R.u;
+  const size_t p = (size_t)gy * R.W + gx;
+  const float4 g = R.gbuf[p];
+  if (g.w <= 0.0f) return;
+  uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x5f356495u);
+  const F3 n1 = f3(g.x, g.y, g.z);
+  const F3 x1 = surface_at(u, gx, gy, R.W, R.H, g);
+  float pc[4];
+  matvec4(u.prevViewProj, x1.x, x1.y, x1.z, 1.0f, pc);
+  if (pc[3] <= 0.0f) return;
+  const float ndx = pc[0] / pc[3], ndy = pc[1] / pc[3];
+  const int ppx = itrunc_((ndx * 0.5f + 0.5f) * (float)R.W);
+  const int ppy = itrunc_(((-ndy) * 0.5f + 0.5f) * (float)R.H);
+  if (!valid_prev(R, ppx, ppy, x1, n1)) return;   // disocclusion: keep the fresh reservoir
+  const RSample st = load_res(R.resB, (size_t)ppy * R.W + ppx);
+  const float cT = fmin_(st.c, u.params3[0]);
+  const RSample sc = load_res(R.resA, p);
+  const float cC = fmax_(sc.c, 0.0f);
+  const float pC = eval_target(sc, x1, n1), pT = eval_target(st, x1, n1);
+  const float mDen = fmax_(cC + cT, 1e-3f);
+  const float wC = ((cC / mDen) * pC) * fmax_(sc.W, 0.0f);
+  const float wT = ((cT / mDen) * pT) * fmax_(st.W, 0.0f);
+  const float wSum = wC + wT;
+  if (wSum <= 0.0f) {   // pooled null keeps the merged confidence
+    store_res(R.resA, p, null_sample(cC + cT));
+    return;
+  }
+  RSample sel = sc;
+  float selP = pC;
+  if (rand_(rng) * wSum >= wC) { sel = st; selP = pT; }
+  if (selP <= 0.0f) return;
+  sel.W = wSum / selP;
+  sel.c = cC + cT;
+  store_res(R.resA, p, sel);
+}
+
+// ---------------------------------------------------------------------------
+// spatial reuse + shading (reuse_spatial.wgsl:116-126, 128-354)
+// ---------------------------------------------------------------------------
+VRT_DI bool sample_visible(const RestirDev& R, const uint32_t* occ, const RSample& s, F3 x1, F3 n1, DCount& cnt) {
+  const F3 surf = x1 + n1 * 1e-3f;
+  if (s.kind == kSkDir) return !occluded(R, occ, surf, s.pos, 1e4f, cnt);
+  const F3 d = s.pos - surf;
+  const float r = __fsqrt_rn(dot3(d, d));
+  if (r < 2e-3f) return true;
+  return !occluded(R, occ, surf, f3(d.x / r, d.y / r, d.z / r), r - 2e-3f, cnt);
+}
+
+VRT_DI void spatial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int gy, DCount& cnt) {
+  const Uni& u = R.u;
+  const size_t p = (size_t)gy * R.W + gx;
+  const float4 dr = unpack_h4(R.direct[p]);
+  const F3 direct = f3(dr.x, dr.y, dr.z);
+  const float4 g = R.gbuf[p];
+  auto out_radiance = [&](F3 v) {
+    R.rad16[p] = pack_h4(v.x, v.y, v.z, 1.0f);
+    if (R.rad32) R.rad32[p] = make_float4(v.x, v.y, v.z, 1.0f);
+  };
+  if (g.w <= 0.0f) {   // sky: direct carries the analytic sky radiance
+    out_radiance(direct);
+    R.resB[2 * p] = make_uint4(0u, 0u, 0u, 0u);
+    R.resB[2 * p + 1] = make_uint4(0u, 0u, 0u, 0u);
+    return;
+  }
+  uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
+  const F3 x1 = surface_at(u, gx, gy, R.W, R.H, g);
+  const F3 n1 = f3(g.x, g.y, g.z);
+
+  // Domains: the canonical pixel plus every validated neighbour, null
+  // reservoirs included (their confidence stays in the MIS denominators).
+  F3 domX1[4], domN1[4];
+  float domC[4];
+  RSample cand[4];
+  uint32_t candDom[4];
+  uint32_t nDom = 1u, nCand = 0u;
+  const RSample canonical = load_res(R.resA, p);
+  domX1[0] = x1;
+  domN1[0] = n1;
+  domC[0] = canonical.c;
+  if (canonical.kind != kSkNone) {
+    cand[0] = canonical;
+    candDom[0] = 0u;
+    nCand = 1u;
+  }
+  if (u.params2[0] & kRfSpatial) {
+    const uint32_t taps = min(u.params2[2], 3u);
+    for (uint32_t ti = 0u; ti < taps; ti++) {
+      // classic random neighbour in a uniform disk of radius params4.x
+      const float r = u.params4[0] * __fsqrt_rn(rand_(rng));
+      const float a = kTwoPi * rand_(rng);
+      float sa, ca;
+      sincos_(a, sa, ca);
+      const int qx = gx + itrunc_(ca * r), qy = gy + itrunc_(sa * r);
+      if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
+      const size_t q = (size_t)qy * R.W + qx;
+      const float4 gq = R.gbuf[q];
+      if (gq.w <= 0.0f) continue;
+      const F3 x1q = surface_at(u, qx, qy, R.W, R.H, gq);
+      const F3 nq = f3(gq.x, gq.y, gq.z);
+      const float nDot = dot3(n1, nq);
+      if (!(nDot > 0.9f && fabsf(gq.w - g.w) < 0.1f * g.w + 0.02f)) continue;
+      const RSample rq = load_res(R.resA, q);
+      domX1[nDom] = x1q;
+      domN1[nDom] = nq;
+      domC[nDom] = rq.c;
+      if (rq.kind != kSkNone) {
+        cand[nCand] = rq;
+        candDom[nCand] = nDom;
+        nCand++;
+      }
+      nDom++;
+    }
+  }
+  float cTotal = 0.0f;
+  for (uint32_t l = 0u; l < nDom; l++) cTotal = cTotal + domC[l];
+
+  float wSum = 0.0f, selP = 0.0f;
+  RSample sel = null_sample(0.0f);
+  uint32_t selJ = 0u;
+  for (uint32_t j = 0u; j < nCand; j++) {
+    const RSample& s = cand[j];
+    float denom = 0.0f;   // balance heuristic over all domains
+    for (uint32_t l = 0u; l < nDom; l++) denom = denom + domC[l] * eval_target(s, domX1[l], domN1[l]);
+    if (denom <= 0.0f) continue;
+    const uint32_t dj = candDom[j];
+    const float m = (domC[dj] * eval_target(s, domX1[dj], domN1[dj])) / denom;
+    const float pMe = eval_target(s, x1, n1);
+    const float w = (m * pMe) * fmax_(s.W, 0.0f);
+    if (w > 0.0f) {
+      wSum = wSum + w;
+      if (rand_(rng) * wSum < w) { sel = s; selP = pMe; selJ = j; }
+    }
+  }
+  if (nCand == 0u || sel.kind == kSkNone || selP <= 0.0f || wSum <= 0.0f) {   // pooled null
+    out_radiance(direct);
+    store_res(R.resB, p, null_sample(fmin_(cTotal, 255.0f)));
+    return;
+  }
+  sel.W = wSum / selP;
+  sel.c = fmin_(cTotal, 255.0f);
+  F3 contrib = f3(0.0f, 0.0f, 0.0f);
+  // the canonical sample's visibility was established when it was traced
+  const bool vis = selJ == 0u || sample_visible(R, occ, sel, x1, n1, cnt);
+  if (vis) contrib = eval_f(sel, x1, n1) * sel.W;
+  out_radiance(direct + contrib);
+  store_res(R.resB, p, sel);
+}
+
+template <bool kSmem>
+__global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ RestirDev R) {
+  extern __shared__ uint32_t s_occ[];
+  const uint32_t* occ = stage_occupancy<kSmem>(R.S, s_occ);
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
+  DCount cnt{0u, 0u, 0u, 0u};
+  if (gx < R.W && gy < R.H) spatial_pixel(R, occ, gx, gy, cnt);
+  if (R.stats) warp_flush_stats(R.stats, cnt, 0u);
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+static RestirDev restir_dev(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H, const PathOut& out,
+                            const RestirBufs& rb) {
+  RestirDev R;
+  R.S = to_dscene(s);
+  R.u = to_uni(u);
+  R.W = W;
+  R.H = H;
+  R.fclamp = fclamp;
+  R.resA = (uint4*)rb.resA;
+  R.resB = (uint4*)rb.resB;
+  R.direct = (uint2*)rb.direct;
+  R.rad16 = (uint2*)out.rad16;
+  R.rad32 = (float4*)out.rad32;
+  R.alb8 = out.alb8;
+  R.gbuf = (float4*)out.gbuf;
+  R.gprev = (const float4*)rb.gbuf_prev;
+  R.stats = out.stats;
+  return R;
+}
+
+template <typename K>
+static cudaError_t launch_occ_kernel(K kern_smem, K kern_glob, const SceneDev& s, int W, int H, const RestirDev& R,
+                                     cudaStream_t st) {
+  const size_t smem = occ_words(s.BG) * sizeof(uint32_t);
+  const dim3 grid((W + 15) / 16, (H + 15) / 16);
+  if (smem <= kMaxSmemOccBytes) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(kern_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    kern_smem<<<grid, 256, smem, st>>>(R);
+  } else {
+    kern_glob<<<grid, 256, 0, st>>>(R);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                                  const PathOut& out, const RestirBufs& rb, cudaStream_t st) {
+  const RestirDev R = restir_dev(s, u, fclamp, W, H, out, rb);
+  return launch_occ_kernel(k_restir_initial<true>, k_restir_initial<false>, s, W, H, R, st);
+}
+
+cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                   const RestirBufs& rb, cudaStream_t st) {
+  const RestirDev R = restir_dev(s, u, 0.0f, W, H, out, rb);
+  k_restir_temporal<<<dim3((W + 15) / 16, (H + 15) / 16), 256, 0, st>>>(R);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                  const RestirBufs& rb, cudaStream_t st) {
+  const RestirDev R = restir_dev(s, u, 0.0f, W, H, out, rb);
+  return launch_occ_kernel(k_restir_spatial<true>, k_restir_spatial<false>, s, W, H, R, st);
+}
+
+}  // namespace vrt

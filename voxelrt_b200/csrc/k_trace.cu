@@ -6,39 +6,9 @@
 // per 8^3 brick, 4 KB at 256^3, 32 KB at 512^3) is staged once per block in
 // shared memory; brick masks and voxels are read through the read-only path
 // (L1/L2 resident: 2 MB + 64 MB at 256^3 fit the 126 MB L2).
-#include "vrt_device.cuh"
-#include "vrt_internal.h"
-#include <cstring>
+#include "trace_kernel.cuh"
 
 namespace vrt {
-
-// Largest occupancy bitmap staged in shared memory (512^3 grid = 32 KB).
-constexpr size_t kMaxSmemOccBytes = 64 * 1024;
-
-template <bool kSmem>
-VRT_DI const uint32_t* stage_occupancy(const DScene& S, uint32_t* s_occ) {
-  if (!kSmem) return S.bits;
-  const int nwords = (S.BG * S.BG * S.BG + 31) >> 5;
-  for (int i = threadIdx.x; i < nwords; i += blockDim.x) s_occ[i] = __ldg(S.bits + i);
-  __syncthreads();
-  return s_occ;
-}
-
-VRT_DI void warp_flush_stats(unsigned long long* stats, const DCount& c, uint32_t pix) {
-  const unsigned full = 0xffffffffu;
-  uint32_t r = __reduce_add_sync(full, c.rays);
-  uint32_t o = __reduce_add_sync(full, c.outer);
-  uint32_t i = __reduce_add_sync(full, c.inner);
-  uint32_t v = __reduce_add_sync(full, c.vreads);
-  uint32_t p = __reduce_add_sync(full, pix);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(stats + kStatRays, (unsigned long long)r);
-    atomicAdd(stats + kStatOuter, (unsigned long long)o);
-    atomicAdd(stats + kStatInner, (unsigned long long)i);
-    atomicAdd(stats + kStatVReads, (unsigned long long)v);
-    atomicAdd(stats + kStatPixels, (unsigned long long)p);
-  }
-}
 
 // One pixel of the plain path (pathtrace.wgsl:248-330).
 VRT_DI void path_pixel(const DScene& S, const uint32_t* occ, const Uni& u, float fclamp, uint32_t gx, uint32_t gy,
@@ -107,9 +77,8 @@ template <bool kSmem>
 __global__ void __launch_bounds__(256) k_pathtrace(DScene S, Uni u, float fclamp, int W, int H, PathOut out) {
   extern __shared__ uint32_t s_occ[];
   const uint32_t* occ = stage_occupancy<kSmem>(S, s_occ);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gx = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-  const int gy = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
   DCount cnt{0u, 0u, 0u, 0u};
   uint32_t pix = 0;
   if (gx < W && gy < H) {
@@ -145,19 +114,6 @@ __global__ void __launch_bounds__(256) k_trace_rays(DScene S, const float* __res
   r.bytes = 4u * (cnt.outer + cnt.inner + cnt.vreads);
   r.pad = 0u;
   out[i] = r;
-}
-
-static DScene to_dscene(const SceneDev& s) {
-  DScene d;
-  d.vox = s.vox; d.masks = s.masks; d.bits = s.bits; d.N = s.N; d.BG = s.BG;
-  return d;
-}
-
-static Uni to_uni(const VrtUniforms& u) {
-  Uni r;
-  static_assert(sizeof(Uni) == sizeof(VrtUniforms), "uniform layouts differ");
-  std::memcpy(&r, &u, sizeof(Uni));
-  return r;
 }
 
 cudaError_t launch_pathtrace(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,

@@ -445,7 +445,8 @@ int vrt_make_uniforms(const VrtCameraPose* cur, const VrtCameraPose* prev, const
   out->params1[0] = (float)width;
   out->params1[1] = (float)height;
   out->params1[2] = exposure;
-  // reference defaults of the (unused here) ReSTIR tuning slots, main.js:71-89
+  // reference defaults of the ReSTIR tuning slots (main.js:71-89); params2.x
+  // (the preset flags) stays 0 = preset=base
   out->params2[0] = 0u;
   out->params2[2] = 3u;
   out->params3[0] = 20.0f; out->params3[1] = 1.0f; out->params3[2] = 0.1f; out->params3[3] = 0.0008f;

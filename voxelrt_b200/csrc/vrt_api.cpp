@@ -123,6 +123,12 @@ struct VrtSession {
   float* hdr_ref = nullptr;
   double* hdr_part = nullptr;
   uint32_t hdr_count = 0;
+  // ReSTIR reservoirs A and B (32 B per pixel each) + pass-through radiance
+  // (8 B per pixel), allocated by the first frame with reservoir flags
+  void* restir_mem = nullptr;
+  size_t restir_bytes = 0;
+  bool restir_timed = false;      // ev[5] marks the end of the initial pass
+  uint64_t events_frame = ~0ull;  // frame whose pass events vrt_frame recorded
 };
 
 constexpr int kMaxWaves = 72;   // wave counters allocated per wavefront scratch
@@ -378,6 +384,7 @@ int vrt_session_destroy(VrtSession* s) {
   dev_free(c, s->hdr_acc, P * 24, &s->bytes);
   dev_free(c, s->hdr_ref, P * 12, &s->bytes);
   dev_free(c, s->hdr_part, (size_t)hdr_blocks((int)P) * 8, &s->bytes);
+  dev_free(c, s->restir_mem, s->restir_bytes, &s->bytes);
   if (s->mlp) vrt_mlp_destroy(s->mlp);
   for (auto& e : s->cev)
     if (e) cudaEventDestroy(e);
@@ -404,8 +411,11 @@ int vrt_session_reset(VrtSession* s) {
   CUDA_TRY(cudaMemsetAsync(s->alb8, 0, P * 4, st));
   CUDA_TRY(cudaMemsetAsync(s->ldr, 0, P * 4, st));
   CUDA_TRY(cudaMemsetAsync(s->stats, 0, kStatCount * 8, st));
+  // a fresh history reservoir B decodes as "no sample" (main.js:350-352)
+  if (s->restir_mem) CUDA_TRY(cudaMemsetAsync(s->restir_mem, 0, s->restir_bytes, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   s->frame_counter = 0;
+  s->events_frame = ~0ull;
   s->have_frame = false;
   s->last_parity = 0;
   return VRT_OK;
@@ -501,6 +511,7 @@ int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
 }
 
 static int check_uniforms(const VrtSession* s, const VrtUniforms* u);
+static bool restir_on(const VrtUniforms* u) { return (u->params2[0] & kRfRestir) != 0u; }
 
 // Autotuner: renders `frames` path-trace passes of `u` per candidate launch
 // shape (refill threshold x occupancy variant x shading grid) and keeps the
@@ -510,6 +521,7 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
   if (!s || !u || frames < 1) return fail(VRT_ERR_INVALID, "bad argument");
   if (s->path_kernel != VRT_PATH_WAVEFRONT) return fail(VRT_ERR_STATE, "autotune needs the wavefront path kernel");
   if (int r = check_uniforms(s, u)) return r;
+  if (restir_on(u)) return fail(VRT_ERR_INVALID, "autotune tunes the plain path's tracer (restir flags set)");
   if (int r = set_dev(s->ctx)) return r;
   cudaStream_t st = s->ctx->stream;
   static const int refills[] = {4, 8, 12, 16, 24};
@@ -560,10 +572,35 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
   if ((int)u->params1[0] != s->W || (int)u->params1[1] != s->H)
     return fail(VRT_ERR_INVALID, "uniform render size %gx%g does not match session %dx%d", u->params1[0],
                 u->params1[1], s->W, s->H);
-  if (u->params2[0] != 0u)
-    return fail(VRT_ERR_INVALID, "restir flags 0x%x set: only the plain path (preset=base) is implemented",
-                u->params2[0]);
+  const uint32_t f = u->params2[0];
+  if (f & ~kRestirFlagsImplemented)
+    return fail(VRT_ERR_INVALID,
+                "restir flags 0x%x: only RF_RESTIR|RF_TEMPORAL|RF_SPATIAL (preset=gi) and 0 (preset=base) are "
+                "implemented", f);
+  if (f != 0u && !(f & kRfRestir))
+    return fail(VRT_ERR_INVALID, "restir flags 0x%x set without RF_RESTIR", f);
   return VRT_OK;
+}
+
+
+// Reservoir buffers of the session, allocated (zeroed) on first use.
+static int ensure_restir(VrtSession* s) {
+  if (s->restir_mem) return VRT_OK;
+  const size_t bytes = px(s) * (32 + 32 + 8);
+  if (int r = dev_alloc(s->ctx, &s->restir_mem, bytes, &s->bytes)) return r;
+  s->restir_bytes = bytes;
+  CUDA_TRY(cudaMemsetAsync(s->restir_mem, 0, bytes, s->ctx->stream));
+  return VRT_OK;
+}
+
+static RestirBufs restir_bufs(const VrtSession* s, int parity) {
+  RestirBufs rb;
+  char* m = (char*)s->restir_mem;
+  rb.resA = m;
+  rb.resB = m + px(s) * 32;
+  rb.direct = m + px(s) * 64;
+  rb.gbuf_prev = s->gbuf[1 - parity];
+  return rb;
 }
 
 static int parity_of(const VrtSession* s) { return (int)(s->frame_counter & 1u); }
@@ -578,6 +615,14 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[parity_of(s)]; o.stats = s->stats;
   if (s->path_kernel == VRT_PATH_BATCH_ONLY)
     return fail(VRT_ERR_STATE, "session was created for batches only (VRT_PATH_BATCH_ONLY)");
+  if (restir_on(u)) {
+    if (s->cache_on) return fail(VRT_ERR_STATE, "the radiance cache serves the plain path only (restir flags set)");
+    if (int r = ensure_restir(s)) return r;
+    CUDA_TRY(launch_restir_initial(s->scene->dev, *u, s->fclamp, s->W, s->H, o, restir_bufs(s, parity_of(s)),
+                                   s->ctx->stream));
+    s->launches++;
+    return VRT_OK;
+  }
   if (s->cache_on) return cache_frame(s, u, o);
   if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
     CUDA_TRY(launch_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, s->wf, s->tune, s->ctx->stream,
@@ -589,6 +634,28 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   }
   return VRT_OK;
 }
+
+static int restir_pass(VrtSession* s, const VrtUniforms* u, bool spatial) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (!restir_on(u)) return fail(VRT_ERR_STATE, "reservoir reuse needs RF_RESTIR in params2.x");
+  if (!s->restir_mem) return fail(VRT_ERR_STATE, "reservoir reuse before the initial pass of a ReSTIR frame");
+  if (int r = set_dev(s->ctx)) return r;
+  const int p = parity_of(s);
+  PathOut o;
+  o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[p]; o.stats = s->stats;
+  if (spatial) {
+    CUDA_TRY(launch_restir_spatial(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->ctx->stream));
+  } else {
+    if (!(u->params2[0] & kRfTemporal)) return VRT_OK;   // reuse_temporal.wgsl:144
+    CUDA_TRY(launch_restir_temporal(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->ctx->stream));
+  }
+  s->launches++;
+  return VRT_OK;
+}
+
+int vrt_pass_reuse_temporal(VrtSession* s, const VrtUniforms* u) { return restir_pass(s, u, false); }
+int vrt_pass_reuse_spatial(VrtSession* s, const VrtUniforms* u) { return restir_pass(s, u, true); }
 
 int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u) {
   if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
@@ -653,6 +720,13 @@ int vrt_frame(VrtSession* s, const VrtUniforms* u) {
   CUDA_TRY(cudaMemsetAsync(s->stats, 0, kStatCount * 8, st));
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[0], st));
   if (int r = vrt_pass_pathtrace(s, u)) return r;
+  s->restir_timed = restir_on(u) && s->timing;
+  if (restir_on(u)) {   // main.js:737-739
+    if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[5], st));
+    if (u->params2[0] & kRfTemporal)
+      if (int r = vrt_pass_reuse_temporal(s, u)) return r;
+    if (int r = vrt_pass_reuse_spatial(s, u)) return r;
+  }
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[1], st));
   if (int r = vrt_pass_temporal(s, u)) return r;
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[2], st));
@@ -662,7 +736,10 @@ int vrt_frame(VrtSession* s, const VrtUniforms* u) {
       if (int r = vrt_pass_atrous(s, u, it)) return r;
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[3], st));
   if (int r = vrt_pass_present(s, u)) return r;
-  if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[4], st));
+  if (s->timing) {
+    CUDA_TRY(cudaEventRecord(s->ev[4], st));
+    s->events_frame = s->frame_counter;
+  }
   return vrt_end_frame(s);
 }
 
@@ -687,7 +764,8 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
     if (int r = vrt_mlp_check(s->mlp)) return r;
   }
   if (s->timing && s->have_frame && s->cache_timed) CUDA_TRY(cudaEventElapsedTime(&out->ms_cache, s->cev[0], s->cev[1]));
-  if (s->timing && s->have_frame) {
+  // pass timings exist only for a frame rendered by vrt_frame with timing on
+  if (s->timing && s->have_frame && s->events_frame + 1 == s->frame_counter) {
     float a = 0, b = 0, c = 0, d = 0;
     CUDA_TRY(cudaEventElapsedTime(&a, s->ev[0], s->ev[1]));
     CUDA_TRY(cudaEventElapsedTime(&b, s->ev[1], s->ev[2]));
@@ -703,6 +781,7 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
     }
     out->ms_trace = tr;
     out->trace_launches = (uint32_t)s->timed_waves;
+    if (s->restir_timed) CUDA_TRY(cudaEventElapsedTime(&out->ms_reuse, s->ev[5], s->ev[1]));
   }
   return VRT_OK;
 }
@@ -742,6 +821,16 @@ int vrt_read_final(VrtSession* s, void* h, size_t b) {
   return read_buf(s, fin, px(s) * (f32 ? 16 : 8), h, b);
 }
 int vrt_read_ldr(VrtSession* s, void* h, size_t b) { return read_buf(s, s ? s->ldr : nullptr, s ? px(s) * 4 : 0, h, b); }
+int vrt_read_reservoirs(VrtSession* s, int which, void* h, size_t b) {
+  if (which < 0 || which > 1) return fail(VRT_ERR_INVALID, "reservoir set %d (0 = A, 1 = B)", which);
+  if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
+  return read_buf(s, s ? (const char*)s->restir_mem + (size_t)which * px(s) * 32 : nullptr, s ? px(s) * 32 : 0, h,
+                  b);
+}
+int vrt_read_direct(VrtSession* s, void* h, size_t b) {
+  if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
+  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 64 : nullptr, s ? px(s) * 8 : 0, h, b);
+}
 
 static float half_to_float(uint16_t hbits) {
   const uint32_t sign = (uint32_t)(hbits & 0x8000u) << 16;
@@ -946,6 +1035,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   for (int i = 0; i < m; i++) {
     VrtSession* s = ss[(size_t)i];
     if (int r = check_uniforms(s, &u[i])) return r;
+    if (restir_on(&u[i])) return fail(VRT_ERR_INVALID, "batched frames render the plain path (restir flags set)");
     maxB = std::max(maxB, s->cache_on ? s->cache_cfg.train_bounces : (int)u[i].params0[1]);
     if (s->cache_on && !s->mlp) return fail(VRT_ERR_STATE, "cache session without a network");
     // the captured graph bakes each cache job's buffers and sizes in
@@ -1275,6 +1365,7 @@ int vrt_server_submit(VrtServer* sv, int session, const VrtUniforms* u, const Vr
   if (!sv || !u || session < 0 || session >= sv->n || n_edits < 0 || (n_edits && !edits))
     return fail(VRT_ERR_INVALID, "bad argument");
   if (int r = check_uniforms(sv->batch->sessions[(size_t)session], u)) return r;
+  if (restir_on(u)) return fail(VRT_ERR_INVALID, "served frames render the plain path (restir flags set)");
   VrtServer::Req r;
   r.ticket = sv->next_ticket++;
   r.session = session;
@@ -1837,6 +1928,9 @@ int vrt_hdr_accum_add(VrtSession* s) {
 
 int vrt_hdr_accumulate(VrtSession* s, const VrtUniforms* u, uint32_t frame0, int spp) {
   if (!s || !u || spp < 1) return fail(VRT_ERR_INVALID, "bad argument");
+  // independent path-trace passes: the reference convention (preset=base);
+  // a reservoir chain is accumulated frame by frame with vrt_hdr_accum_add
+  if (restir_on(u)) return fail(VRT_ERR_INVALID, "reference accumulation renders the plain path (restir flags set)");
   VrtUniforms v = *u;
   for (int k = 0; k < spp; k++) {
     v.params0[0] = frame0 + (uint32_t)k;

@@ -230,4 +230,24 @@ cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const voi
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
                            const uint32_t* alb8, uint32_t* ldr, cudaStream_t st);
 
+// Reservoir flags of params2.x (common.wgsl:40-42) this build implements:
+// the `gi` preset (main.js:44).
+constexpr uint32_t kRfRestir = 1u, kRfTemporal = 2u, kRfSpatial = 4u;
+constexpr uint32_t kRestirFlagsImplemented = kRfRestir | kRfTemporal | kRfSpatial;
+
+// ReSTIR reservoirs of one session (32 bytes per pixel each, the reference's
+// record layout) and the pass-through radiance of the initial pass.
+struct RestirBufs {
+  void* resA = nullptr;             // working set: initial, then temporal merge
+  void* resB = nullptr;             // post-spatial = next frame's history
+  void* direct = nullptr;           // rgba16f
+  const void* gbuf_prev = nullptr;  // previous frame's G-buffer
+};
+cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                                  const PathOut& out, const RestirBufs& rb, cudaStream_t st);
+cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                   const RestirBufs& rb, cudaStream_t st);
+cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                  const RestirBufs& rb, cudaStream_t st);
+
 }  // namespace vrt
