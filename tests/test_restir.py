@@ -42,7 +42,8 @@ def _eq(a, b, what):
 
 
 def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=2, fclamp=10.0, preset="gi",
-                move=True, taps=3, ccap=20.0, radius=30.0, pose=None, restir_flags=None, check_stages=True):
+                move=True, taps=3, ccap=20.0, radius=30.0, pose=None, restir_flags=None, check_stages=True,
+                kernel="wavefront"):
     """Renders `frames` frames pass by pass on the device and with the oracle;
     asserts every stage of every frame.  Returns the device stats of the
     last frame and the oracle's last frame."""
@@ -50,7 +51,7 @@ def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=
     spawn = pose or spawn
     b, m = orc.build_bricks(vox, n)
     sc = vrt.Scene(ctx, vox, n)
-    s = vrt.Session(ctx, sc, W, H, firefly_clamp=fclamp, keep_radiance_f32=True)
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=fclamp, keep_radiance_f32=True, path_kernel=kernel)
     s.set_timing(True)
     light = vrt.Lighting()
     acc_prev = np.zeros((H, W, 4), np.uint16)
@@ -111,8 +112,9 @@ def _conf(res):
     return (res[..., 5] >> 18) & 0xFF
 
 
-def test_restir_gi_moving_camera(ctx, vrt, orc):
-    _, ref = _run_restir(ctx, vrt, orc, 1, 64, 1, 160, 90, 5)
+@pytest.mark.parametrize("kernel", ["wavefront", "megakernel"])
+def test_restir_gi_moving_camera(ctx, vrt, orc, kernel):
+    _, ref = _run_restir(ctx, vrt, orc, 1, 64, 1, 160, 90, 5, kernel=kernel)
     # the chain did real work: point and direction samples, reuse confidence > 1
     k = _kinds(ref["resB"])
     assert (k == 1).any() and (k == 2).any()
@@ -131,9 +133,10 @@ def test_restir_flag_subsets(ctx, vrt, orc, restir_flags):
     _run_restir(ctx, vrt, orc, 1, 64, 1, 128, 72, 3, restir_flags=restir_flags)
 
 
-@pytest.mark.parametrize("bounces", [0, 1, 4])
-def test_restir_bounce_counts(ctx, vrt, orc, bounces):
-    _run_restir(ctx, vrt, orc, 1, 64, 1, 128, 72, 3, bounces=bounces)
+@pytest.mark.parametrize("kernel", ["wavefront", "megakernel"])
+@pytest.mark.parametrize("bounces", [0, 1, 4, 6])
+def test_restir_bounce_counts(ctx, vrt, orc, bounces, kernel):
+    _run_restir(ctx, vrt, orc, 1, 64, 1, 128, 72, 3, bounces=bounces, kernel=kernel)
 
 
 @pytest.mark.parametrize("taps,radius,ccap", [(0, 30.0, 20.0), (1, 2.0, 1.0), (3, 120.0, 255.0), (7, 5.5, 0.0)])
@@ -151,9 +154,10 @@ def test_restir_odd_sizes(ctx, vrt, orc, W, H):
                 pose=vrt.CameraPose((4.0, 3.0, 1.0), 0.3, -0.1, math.radians(70)))
 
 
-def test_restir_full_size(ctx, vrt, orc):
+@pytest.mark.parametrize("kernel", ["wavefront", "megakernel"])
+def test_restir_full_size(ctx, vrt, orc, kernel):
     """1920x1080 on the 256^3 world, two frames, every stage against the oracle."""
-    _run_restir(ctx, vrt, orc, 2, 256, 2, 1920, 1080, 2)
+    _run_restir(ctx, vrt, orc, 2, 256, 2, 1920, 1080, 2, kernel=kernel)
 
 
 def test_restir_frame_equals_passes(ctx, vrt):

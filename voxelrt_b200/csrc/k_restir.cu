@@ -28,6 +28,7 @@
 // follows the WGSL expression by expression (no contraction), so the CPU
 // restatement reproduces every word bit for bit.
 #include "trace_kernel.cuh"
+#include "wavefront_core.cuh"
 
 namespace vrt {
 
@@ -216,6 +217,55 @@ VRT_DI F3 estimate_lo(const RestirDev& R, const uint32_t* occ, F3 x2, F3 n2, Mat
 // ---------------------------------------------------------------------------
 // initial candidates (pathtrace.wgsl:248-284, 332-457)
 // ---------------------------------------------------------------------------
+// The bounce candidate when its ray escapes: a sky direction, W = 1/pdf_omega.
+VRT_DI void cand_dir(const Uni& u, F3 n1, F3 brd, RSample& s, float& Wc) {
+  s = null_sample(0.0f);
+  s.kind = kSkDir;
+  s.pos = brd;
+  s.rad = sky_color(u, brd, false);
+  Wc = kPi / fmax_(dot3(n1, brd), 1e-4f);
+}
+
+// The bounce candidate at reconnection vertex x2 carrying Lo (already
+// clamped), W = 1/pdf in area measure.
+VRT_DI void cand_point(F3 x1, F3 n1, F3 x2, F3 n2, F3 Lo, RSample& s, float& Wc) {
+  s = null_sample(0.0f);
+  s.kind = kSkPoint;
+  s.pos = x2;
+  s.n = n2;
+  s.rad = Lo;
+  const F3 d = x2 - x1;
+  const float r2 = fmax_(dot3(d, d), 1e-6f);
+  const F3 dn = normalize3(d);
+  const float cos1 = fmax_(dot3(n1, dn), 1e-4f);
+  const float cos2 = fmax_(dot3(n2, f3(-dn.x, -dn.y, -dn.z)), 1e-4f);
+  Wc = ((kPi / cos1) * r2) / cos2;
+}
+
+// Initial RIS over the (at most one) candidate and the reservoir record of
+// pixel p (pathtrace.wgsl:434-455).
+VRT_DI void store_initial(uint4* resA, size_t p, const Uni& u, int W, int H, bool has, const RSample& s, float Wc,
+                          F3 x1, F3 n1, uint32_t& rng) {
+  float wSum = 0.0f, selP = 0.0f;
+  RSample sel = null_sample(0.0f);
+  if (has) {
+    const float pt = eval_target(s, x1, n1);
+    const float w = pt * Wc;
+    if (w > 0.0f) {
+      wSum = wSum + w;
+      if (rand_(rng) * wSum < w) { sel = s; selP = pt; }
+    }
+  }
+  RSample out = null_sample(0.0f);
+  if (sel.kind != kSkNone && selP > 0.0f) {
+    out = sel;
+    out.W = wSum / selP;
+  }
+  out.c = 1.0f;   // a failed candidate is a zero-valued outcome, confidence 1
+  out.seed = pcg_hash((uint32_t)p + u.params0[0] * ((uint32_t)W * (uint32_t)H + 1u));
+  store_res(resA, p, out);
+}
+
 VRT_DI void initial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int gy, DCount& cnt) {
   const Uni& u = R.u;
   const size_t p = (size_t)gy * R.W + gx;
@@ -247,55 +297,29 @@ VRT_DI void initial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int g
 
   const float em = mat1.emissive * kEmissiveScale;
   F3 direct = f3(em, em, em);
-  float wSum = 0.0f, selP = 0.0f;
-  RSample sel = null_sample(0.0f);
   {   // sun-cone NEE at x1: pass-through radiance when unification is off
     const F3 l = sample_sun_dir(u, rng);
     const float ndl = dot3(n1, l);
     if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf1, l, 1e4f, cnt))
       direct = direct + f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
   }
-  if (u.params0[1] > 0u) {   // BSDF bounce candidate: reconnection vertex x2 carries Lo
+  RSample s = null_sample(0.0f);
+  float Wc = 0.0f;
+  const bool has = u.params0[1] > 0u;
+  if (has) {   // BSDF bounce candidate: reconnection vertex x2 carries Lo
     const F3 brd = cosine_hemisphere(n1, rng);
     const DHit h = trace<true>(R.S, occ, surf1, brd, 1e4f, cnt);
-    RSample s = null_sample(0.0f);
-    float Wc;
     if (h.t < 0.0f) {
-      s.kind = kSkDir;
-      s.pos = brd;
-      s.rad = sky_color(u, brd, false);
-      Wc = kPi / fmax_(dot3(n1, brd), 1e-4f);
+      cand_dir(u, n1, brd, s, Wc);
     } else {
       const F3 x2 = surf1 + brd * h.t;
       const Mat mat2 = unpack_material(h.mat);
       F3 Lo = estimate_lo(R, occ, x2, h.n, mat2, rng, cnt);
       if (mat2.emissive > 0.0f) Lo = Lo + mat2.albedo * (mat2.emissive * kEmissiveScale);
-      s.kind = kSkPoint;
-      s.pos = x2;
-      s.n = h.n;
-      s.rad = fclamp3(R, Lo);
-      const F3 d = x2 - x1;
-      const float r2 = fmax_(dot3(d, d), 1e-6f);
-      const F3 dn = normalize3(d);
-      const float cos1 = fmax_(dot3(n1, dn), 1e-4f);
-      const float cos2 = fmax_(dot3(h.n, f3(-dn.x, -dn.y, -dn.z)), 1e-4f);
-      Wc = ((kPi / cos1) * r2) / cos2;
-    }
-    const float pt = eval_target(s, x1, n1);
-    const float w = pt * Wc;
-    if (w > 0.0f) {
-      wSum = wSum + w;
-      if (rand_(rng) * wSum < w) { sel = s; selP = pt; }
+      cand_point(x1, n1, x2, h.n, fclamp3(R, Lo), s, Wc);
     }
   }
-  RSample out = null_sample(0.0f);
-  if (sel.kind != kSkNone && selP > 0.0f) {
-    out = sel;
-    out.W = wSum / selP;
-  }
-  out.c = 1.0f;   // a failed candidate is a zero-valued outcome, confidence 1
-  out.seed = pcg_hash((uint32_t)p + u.params0[0] * ((uint32_t)R.W * (uint32_t)R.H + 1u));
-  store_res(R.resA, p, out);
+  store_initial(R.resA, p, u, R.W, R.H, has, s, Wc, x1, n1, rng);
   R.direct[p] = pack_h4(direct.x, direct.y, direct.z, 1.0f);
 }
 
@@ -492,6 +516,224 @@ __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------------------
+// wavefront form of the initial pass.  The candidate path has the plain
+// path's ray structure -- primary hit x1, sun shadow + bounce at x1, then
+// estimateLo's vertices x2, x3, ... with a sun shadow each -- so it runs on
+// the wavefront tracer's waves with its own shading kernels:
+//   shade(0): G-buffer, albedo, x1's sun sample (pass-through radiance) and
+//             bounce direction;
+//   shade(1): x1's shadow resolves the pass-through radiance (stored); the
+//             bounce hit is x2 (stored with its normal) or the sky (a
+//             direction candidate, finished here); x2 is shaded as
+//             estimateLo's vertex 1 (no emission pickup there);
+//   shade(k): estimateLo's vertex k (shade_vertex: emission, sun sample,
+//             Russian roulette from vertex 2, bounce);
+// and a finished path builds its candidate and writes reservoir A.  Per-path
+// state lives in the tracer's buffers (Lo in the radiance slot, throughput,
+// RNG); x1 is rebuilt from the G-buffer and the primary ray (recomputed from
+// the pixel's RNG stream).  Every draw and sum is the megakernel's, in the
+// same order, so the records are bit-identical to it.
+// ---------------------------------------------------------------------------
+struct RestirWf {
+  uint4* resA;
+  uint2* direct;
+  float4* x2;     // per path: reconnection vertex x2 (xyz), code of its normal (w bits)
+  int W, H;
+};
+
+// Exact code of a DDA normal (components +-0 or +-1): sign and magnitude
+// bits per component, so that signed zeros survive the round trip.
+VRT_DI uint32_t normal_code(F3 n) {
+  const float c[3] = {n.x, n.y, n.z};
+  uint32_t code = 0u;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    code |= ((__float_as_uint(c[i]) >> 31) | ((c[i] != 0.0f ? 1u : 0u) << 1)) << (2 * i);
+  return code;
+}
+VRT_DI F3 normal_decode(uint32_t code) {
+  float c[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const uint32_t b = (code >> (2 * i)) & 3u;
+    c[i] = __uint_as_float(((b & 1u) << 31) | ((b & 2u) ? 0x3f800000u : 0u));
+  }
+  return f3(c[0], c[1], c[2]);
+}
+
+// Primary ray direction of pixel (gx, gy): the first two draws of its stream
+// are the sub-pixel jitter (pathtrace.wgsl:255-262).
+VRT_DI F3 primary_dir(const Uni& u, uint32_t gx, uint32_t gy, int W, int H) {
+  uint32_t rng = init_rng(gx, gy, u.params0[0]);
+  const float jx = rand_(rng) - 0.5f;
+  const float jy = rand_(rng) - 0.5f;
+  return camera_ray(u, (((float)gx + 0.5f) + jx) / (float)W, (((float)gy + 0.5f) + jy) / (float)H);
+}
+
+// Candidate at the end of estimateLo: Lo (unclamped), x2's material; x1
+// from the G-buffer.
+VRT_DI void finish_point(const SingleJob& job, const RestirWf& r, uint32_t g, F3 Lo, uint32_t mat2bits, F3 x2, F3 n2,
+                         uint32_t& rng) {
+  const Uni& u = job.u;
+  const float fc = job.fclamp;
+  auto clampf3 = [&](F3 v) { return fc <= 0.0f ? v : min3(v, f3(fc, fc, fc)); };
+  Lo = clampf3(Lo);
+  const Mat mat2 = unpack_material(mat2bits);
+  if (mat2.emissive > 0.0f) Lo = Lo + mat2.albedo * (mat2.emissive * kEmissiveScale);
+  const float4 gb = job.out.gbuf[g];
+  const F3 n1 = f3(gb.x, gb.y, gb.z);
+  const uint32_t gx = g % (uint32_t)r.W, gy = g / (uint32_t)r.W;
+  const F3 x1 = f3(u.camPos[0], u.camPos[1], u.camPos[2]) + primary_dir(u, gx, gy, r.W, r.H) * gb.w;
+  RSample s;
+  float Wc;
+  cand_point(x1, n1, x2, n2, clampf3(Lo), s, Wc);
+  store_initial(r.resA, g, u, r.W, r.H, true, s, Wc, x1, n1, rng);
+}
+
+__global__ void __launch_bounds__(256) k_wf_restir_primary(const __grid_constant__ SingleJob job, RestirWf r,
+                                                           uint32_t P, WfDev b, unsigned long long* stats) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  if (stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(stats + kStatPixels, (unsigned long long)P);
+  const Uni& u = job.u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += stride) {
+    const uint32_t g = base + threadIdx.x;
+    bool shadow = false, bounce = false, keep = false;
+    if (g < P) {
+      const uint4 h = b.hit[g];
+      const F3 rd = xyz(b.R1[g]);
+      const float t = __uint_as_float(h.x);
+      if (t < 0.0f) {
+        const F3 sky = sky_color(u, rd, true);
+        const uint2 sk = pack_h4(sky.x, sky.y, sky.z, 1.0f);
+        job.out.rad16[g] = sk;
+        if (job.out.rad32) job.out.rad32[g] = make_float4(sky.x, sky.y, sky.z, 1.0f);
+        r.direct[g] = sk;
+        job.out.alb8[g] = 0xffffffffu;
+        job.out.gbuf[g] = make_float4(-rd.x, -rd.y, -rd.z, -1.0f);
+        r.resA[2 * (size_t)g] = make_uint4(0u, 0u, 0u, 0u);
+        r.resA[2 * (size_t)g + 1] = make_uint4(0u, 0u, 0u, 0u);
+      } else {
+        const Mat mat1 = unpack_material(h.y);
+        const F3 x1 = f3(u.camPos[0], u.camPos[1], u.camPos[2]) + rd * t;
+        const F3 n1 = hit_normal((int)h.z, rd);
+        job.out.alb8[g] = unorm8_(__fsqrt_rn(mat1.albedo.x)) | (unorm8_(__fsqrt_rn(mat1.albedo.y)) << 8) |
+                          (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
+        job.out.gbuf[g] = make_float4(n1.x, n1.y, n1.z, t);
+        uint32_t rng = __float_as_uint(b.S0[g].w);
+        const F3 surf1 = x1 + n1 * fmax_(1e-3f, t * 1e-4f);
+        const F3 l = sample_sun_dir(u, rng);
+        const float ndl = dot3(n1, l);
+        shadow = ndl > 0.0f && l.y > 0.0f;
+        F3 sunc = f3(0.0f, 0.0f, 0.0f);
+        uint32_t flags = 0u;
+        if (shadow) {
+          sunc = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
+          flags |= kFlagShadow;
+          b.R2[g] = make_float4(l.x, l.y, l.z, 0.0f);
+        }
+        bounce = u.params0[1] > 0u;
+        if (bounce) {
+          const F3 brd = cosine_hemisphere(n1, rng);
+          b.R1[g] = make_float4(brd.x, brd.y, brd.z, 0.0f);
+        } else {
+          flags |= kFlagTerminal;
+        }
+        keep = shadow || bounce;
+        if (keep) {
+          b.R0[g] = make_float4(surf1.x, surf1.y, surf1.z, 0.0f);
+          b.S0[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
+          b.S1[g] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(h.y));
+          b.S2[g] = make_float4(sunc.x, sunc.y, sunc.z, __uint_as_float(flags));
+        } else {   // no sun sample, no bounce: emission only, null reservoir
+          const float em = mat1.emissive * kEmissiveScale;
+          r.direct[g] = pack_h4(em, em, em, 1.0f);
+          store_initial(r.resA, g, u, r.W, r.H, false, null_sample(0.0f), 0.0f, x1, n1, rng);
+        }
+      }
+    }
+    emit(b, 1, g, shadow, bounce, keep);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wf_restir_wave(const __grid_constant__ SingleJob job, RestirWf r, WfDev b,
+                                                        int wave) {
+  const int n = b.ctr[4 * wave + 2];
+  const uint32_t* list = active_of(b, wave);
+  const Uni& u = job.u;
+  const uint32_t nB = u.params0[1];
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int i = base + threadIdx.x;
+    bool shadow = false, bounce = false, keep = false;
+    uint32_t g = 0u;
+    if (i < n) {
+      g = list[i];
+      const float4 s0 = b.S0[g];
+      const float4 s1 = b.S1[g];
+      const float4 s2 = b.S2[g];
+      const uint4 h = b.hit[g];
+      F3 Lo = xyz(s0), tp = xyz(s1);
+      uint32_t rng = __float_as_uint(s0.w);
+      const uint32_t flags = __float_as_uint(s2.w);
+      const bool lit = (flags & kFlagShadow) && h.w == 0u;
+      const bool terminal = (flags & kFlagTerminal) != 0u;
+      if (wave == 1) {
+        // x1's sun shadow resolved: the pass-through radiance is complete
+        const float em = unpack_material(__float_as_uint(s1.w)).emissive * kEmissiveScale;
+        F3 direct = f3(em, em, em);
+        if (lit) direct = direct + xyz(s2);
+        r.direct[g] = pack_h4(direct.x, direct.y, direct.z, 1.0f);
+        const float4 gb = job.out.gbuf[g];
+        const F3 n1 = f3(gb.x, gb.y, gb.z);
+        if (terminal) {   // no bounce candidate (0 bounces)
+          store_initial(r.resA, g, u, r.W, r.H, false, null_sample(0.0f), 0.0f, f3(0.0f, 0.0f, 0.0f), n1, rng);
+        } else {
+          const F3 brd = xyz(b.R1[g]);
+          const float t = __uint_as_float(h.x);
+          if (t < 0.0f) {   // escaped: a sky direction candidate (x1 unused by its target)
+            RSample s;
+            float Wc;
+            cand_dir(u, n1, brd, s, Wc);
+            store_initial(r.resA, g, u, r.W, r.H, true, s, Wc, f3(0.0f, 0.0f, 0.0f), n1, rng);
+          } else {
+            const F3 x2 = xyz(b.R0[g]) + brd * t;
+            const F3 n2 = hit_normal((int)h.z, brd);
+            r.x2[g] = make_float4(x2.x, x2.y, x2.z, __uint_as_float(normal_code(n2)));
+            Mat m2 = unpack_material(h.y);
+            m2.emissive = 0.0f;   // estimateLo picks up emission from vertex 2 on
+            Lo = f3(0.0f, 0.0f, 0.0f);
+            tp = f3(1.0f, 1.0f, 1.0f);
+            keep = shade_vertex(u, b, g, 1u, x2, n2, m2, Lo, tp, rng, h.y, shadow, bounce, nB, nullptr);
+            if (!keep) finish_point(job, r, g, Lo, h.y, x2, n2, rng);
+          }
+        }
+      } else {
+        if (lit) Lo = Lo + xyz(s2);
+        bool done = terminal;
+        if (!done) {
+          const F3 rd = xyz(b.R1[g]);
+          const float t = __uint_as_float(h.x);
+          if (t < 0.0f) {
+            Lo = Lo + tp * sky_color(u, rd, false);
+            done = true;
+          } else {
+            const F3 pos = xyz(b.R0[g]) + rd * t;
+            keep = shade_vertex(u, b, g, (uint32_t)wave, pos, hit_normal((int)h.z, rd), unpack_material(h.y), Lo,
+                                tp, rng, __float_as_uint(s1.w), shadow, bounce, nB, nullptr);
+            done = !keep;
+          }
+        }
+        if (done) {
+          const float4 x2c = r.x2[g];
+          finish_point(job, r, g, Lo, __float_as_uint(s1.w), xyz(x2c), normal_decode(__float_as_uint(x2c.w)), rng);
+        }
+      }
+    }
+    emit(b, wave + 1, g, shadow, bounce, keep);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
 static RestirDev restir_dev(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H, const PathOut& out,
@@ -535,6 +777,34 @@ cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float
                                   const PathOut& out, const RestirBufs& rb, cudaStream_t st) {
   const RestirDev R = restir_dev(s, u, fclamp, W, H, out, rb);
   return launch_occ_kernel(k_restir_initial<true>, k_restir_initial<false>, s, W, H, R, st);
+}
+
+cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
+                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
+                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
+  SingleJob job;
+  std::memset(&job, 0, sizeof job);
+  job.u = to_uni(uu);
+  job.S = to_dscene(s);
+  job.out.rad16 = (uint2*)out.rad16;
+  job.out.rad32 = (float4*)out.rad32;
+  job.out.alb8 = out.alb8;
+  job.out.gbuf = (float4*)out.gbuf;
+  job.fclamp = fclamp;
+  job.W = W;
+  job.H = H;
+  const RestirWf r{(uint4*)rb.resA, (uint2*)rb.direct, (float4*)rb.scratch, W, H};
+  const uint32_t P = (uint32_t)W * (uint32_t)H;
+  const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
+  const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
+  unsigned long long* stats = out.stats;
+  return wf_run_waves(job, P, (int)job.u.params0[1] + 2, smem, wb, tune, stats, st, launches, trace_ev,
+                      max_timed_waves, timed_waves, [&](const WfDev& b, int w, int sblocks) {
+                        if (w == 0) k_wf_restir_primary<<<sblocks, 256, 0, st>>>(job, r, P, b, stats);
+                        else k_wf_restir_wave<<<sblocks, 256, 0, st>>>(job, r, b, w);
+                        return cudaGetLastError();
+                      });
 }
 
 cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,

@@ -586,7 +586,7 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
 // Reservoir buffers of the session, allocated (zeroed) on first use.
 static int ensure_restir(VrtSession* s) {
   if (s->restir_mem) return VRT_OK;
-  const size_t bytes = px(s) * (32 + 32 + 8);
+  const size_t bytes = px(s) * (32 + 32 + 8 + 16);
   if (int r = dev_alloc(s->ctx, &s->restir_mem, bytes, &s->bytes)) return r;
   s->restir_bytes = bytes;
   CUDA_TRY(cudaMemsetAsync(s->restir_mem, 0, bytes, s->ctx->stream));
@@ -598,7 +598,8 @@ static RestirBufs restir_bufs(const VrtSession* s, int parity) {
   char* m = (char*)s->restir_mem;
   rb.resA = m;
   rb.resB = m + px(s) * 32;
-  rb.direct = m + px(s) * 64;
+  rb.scratch = m + px(s) * 64;   // 16-byte records before the 8-byte ones: every
+  rb.direct = m + px(s) * 80;    // region starts on a 16-byte boundary for any P
   rb.gbuf_prev = s->gbuf[1 - parity];
   return rb;
 }
@@ -618,9 +619,15 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (restir_on(u)) {
     if (s->cache_on) return fail(VRT_ERR_STATE, "the radiance cache serves the plain path only (restir flags set)");
     if (int r = ensure_restir(s)) return r;
-    CUDA_TRY(launch_restir_initial(s->scene->dev, *u, s->fclamp, s->W, s->H, o, restir_bufs(s, parity_of(s)),
-                                   s->ctx->stream));
-    s->launches++;
+    const RestirBufs rb = restir_bufs(s, parity_of(s));
+    if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
+      CUDA_TRY(launch_restir_initial_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
+                                               s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,
+                                               VrtSession::kTimedWaves, &s->timed_waves));
+    } else {
+      CUDA_TRY(launch_restir_initial(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->ctx->stream));
+      s->launches++;
+    }
     return VRT_OK;
   }
   if (s->cache_on) return cache_frame(s, u, o);
@@ -829,7 +836,7 @@ int vrt_read_reservoirs(VrtSession* s, int which, void* h, size_t b) {
 }
 int vrt_read_direct(VrtSession* s, void* h, size_t b) {
   if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
-  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 64 : nullptr, s ? px(s) * 8 : 0, h, b);
+  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 80 : nullptr, s ? px(s) * 8 : 0, h, b);
 }
 
 static float half_to_float(uint16_t hbits) {

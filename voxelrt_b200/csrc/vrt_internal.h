@@ -242,9 +242,15 @@ struct RestirBufs {
   void* resB = nullptr;             // post-spatial = next frame's history
   void* direct = nullptr;           // rgba16f
   const void* gbuf_prev = nullptr;  // previous frame's G-buffer
+  void* scratch = nullptr;          // 16 B per pixel: wavefront path state (x2)
 };
 cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                                   const PathOut& out, const RestirBufs& rb, cudaStream_t st);
+// The initial pass on the wavefront tracer (bit-identical to launch_restir_initial).
+cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
+                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves);
 cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
                                    const RestirBufs& rb, cudaStream_t st);
 cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,

@@ -887,13 +887,13 @@ cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int 
   }
 }
 
-// Launches generate + (trace, shade) x waves.  smem > 0 selects the
-// shared-memory bitmap tracer (single scene only).
-template <class J>
-cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
-                            const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
-                            uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
-                            int njobs = 1) {
+// Launches generate + (trace, shade) x waves; shade(b, w, blocks) launches
+// the shading kernel of wave w.  smem > 0 selects the shared-memory bitmap
+// tracer (single scene only).
+template <class J, class ShadeFn>
+cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
+                         const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st, uint32_t* launches,
+                         cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves, ShadeFn shade) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   const WfDev b = wf_view(wb);
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
@@ -902,10 +902,6 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
   const int refill = tune.refill_min > 0 ? tune.refill_min : 8;
   const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 16);
   uint32_t nl = 0;
-  if (jobs.any_cache()) {
-    k_cache_reset<J><<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
-    nl++;
-  }
   k_wf_generate<J><<<(P + 255) / 256, 256, 0, st>>>(jobs, P, b);
   nl++;
   int timed = 0;
@@ -920,13 +916,32 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
     if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
     if (tm) timed++;
     nl++;
-    if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
-    else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
+    if ((e = shade(b, w, sblocks)) != cudaSuccess) return e;
     nl++;
   }
   if (launches) *launches += nl;
   if (timed_waves) *timed_waves = timed;
   return cudaGetLastError();
+}
+
+// The plain path's wave sequence (with the radiance cache's counter reset
+// when any job has the cache on).
+template <class J>
+cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
+                            const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
+                            uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
+                            int njobs = 1) {
+  if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
+  if (jobs.any_cache()) {
+    k_cache_reset<J><<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
+    if (launches) (*launches)++;
+  }
+  return wf_run_waves(jobs, P, waves, smem, wb, tune, stats, st, launches, trace_ev, max_timed_waves, timed_waves,
+                      [&](const WfDev& b, int w, int sblocks) {
+                        if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
+                        else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
+                        return cudaGetLastError();
+                      });
 }
 
 }  // namespace vrt
