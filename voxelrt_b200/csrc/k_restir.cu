@@ -394,116 +394,166 @@ __global__ void __launch_bounds__(256) k_restir_temporal(const __grid_constant__
 
 // ---------------------------------------------------------------------------
 // spatial reuse + shading (reuse_spatial.wgsl:116-126, 128-354)
+//
+// Domains and candidates sit in fixed slots -- 0 the canonical pixel, k the
+// k-th tap -- with validity flags instead of the reference's compacted
+// arrays; every loop runs over the slots in increasing order and skips the
+// invalid ones, so sums and RNG draws happen in the reference's order, and
+// the arrays stay in registers.  A candidate's position in the compacted
+// list (`rank`) decides whether its visibility is tested (rank > 0).  Each
+// target evaluation serves the denominator, the MIS numerator (its own
+// domain's term) and p-hat at the receiver (the canonical domain's term).
 // ---------------------------------------------------------------------------
-VRT_DI bool sample_visible(const RestirDev& R, const uint32_t* occ, const RSample& s, F3 x1, F3 n1, DCount& cnt) {
-  const F3 surf = x1 + n1 * 1e-3f;
-  if (s.kind == kSkDir) return !occluded(R, occ, surf, s.pos, 1e4f, cnt);
-  const F3 d = s.pos - surf;
-  const float r = __fsqrt_rn(dot3(d, d));
-  if (r < 2e-3f) return true;
-  return !occluded(R, occ, surf, f3(d.x / r, d.y / r, d.z / r), r - 2e-3f, cnt);
-}
+struct SpatialPick {
+  bool ok;          // a sample was selected (else: pooled null)
+  bool vis_test;    // its visibility must be tested (a neighbour's sample)
+  RSample sel;      // the selected sample with W and pooled confidence
+  float cTotal;
+};
 
-VRT_DI void spatial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int gy, DCount& cnt) {
+VRT_DI SpatialPick spatial_pick(const RestirDev& R, int gx, int gy, float4 g, F3 x1, F3 n1) {
   const Uni& u = R.u;
   const size_t p = (size_t)gy * R.W + gx;
-  const float4 dr = unpack_h4(R.direct[p]);
-  const F3 direct = f3(dr.x, dr.y, dr.z);
-  const float4 g = R.gbuf[p];
-  auto out_radiance = [&](F3 v) {
-    R.rad16[p] = pack_h4(v.x, v.y, v.z, 1.0f);
-    if (R.rad32) R.rad32[p] = make_float4(v.x, v.y, v.z, 1.0f);
-  };
-  if (g.w <= 0.0f) {   // sky: direct carries the analytic sky radiance
-    out_radiance(direct);
-    R.resB[2 * p] = make_uint4(0u, 0u, 0u, 0u);
-    R.resB[2 * p + 1] = make_uint4(0u, 0u, 0u, 0u);
-    return;
-  }
   uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
-  const F3 x1 = surface_at(u, gx, gy, R.W, R.H, g);
-  const F3 n1 = f3(g.x, g.y, g.z);
-
-  // Domains: the canonical pixel plus every validated neighbour, null
-  // reservoirs included (their confidence stays in the MIS denominators).
-  F3 domX1[4], domN1[4];
-  float domC[4];
-  RSample cand[4];
-  uint32_t candDom[4];
-  uint32_t nDom = 1u, nCand = 0u;
-  const RSample canonical = load_res(R.resA, p);
-  domX1[0] = x1;
-  domN1[0] = n1;
-  domC[0] = canonical.c;
-  if (canonical.kind != kSkNone) {
-    cand[0] = canonical;
-    candDom[0] = 0u;
-    nCand = 1u;
+  F3 dx[4], dn[4];
+  float dc[4];
+  uint32_t qi[4];
+  bool dok[4], cok[4];
+  dx[0] = x1;
+  dn[0] = n1;
+  qi[0] = (uint32_t)p;
+  {
+    const uint4 d0 = R.resA[2 * p + 1];
+    dc[0] = (float)((d0.y >> 18) & 0xffu);
+    dok[0] = true;
+    cok[0] = ((d0.y >> 16) & 3u) != kSkNone;
   }
-  if (u.params2[0] & kRfSpatial) {
-    const uint32_t taps = min(u.params2[2], 3u);
-    for (uint32_t ti = 0u; ti < taps; ti++) {
-      // classic random neighbour in a uniform disk of radius params4.x
-      const float r = u.params4[0] * __fsqrt_rn(rand_(rng));
-      const float a = kTwoPi * rand_(rng);
-      float sa, ca;
-      sincos_(a, sa, ca);
-      const int qx = gx + itrunc_(ca * r), qy = gy + itrunc_(sa * r);
-      if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
-      const size_t q = (size_t)qy * R.W + qx;
-      const float4 gq = R.gbuf[q];
-      if (gq.w <= 0.0f) continue;
-      const F3 x1q = surface_at(u, qx, qy, R.W, R.H, gq);
-      const F3 nq = f3(gq.x, gq.y, gq.z);
-      const float nDot = dot3(n1, nq);
-      if (!(nDot > 0.9f && fabsf(gq.w - g.w) < 0.1f * g.w + 0.02f)) continue;
-      const RSample rq = load_res(R.resA, q);
-      domX1[nDom] = x1q;
-      domN1[nDom] = nq;
-      domC[nDom] = rq.c;
-      if (rq.kind != kSkNone) {
-        cand[nCand] = rq;
-        candDom[nCand] = nDom;
-        nCand++;
-      }
-      nDom++;
-    }
+  const uint32_t taps = (u.params2[0] & kRfSpatial) ? min(u.params2[2], 3u) : 0u;
+#pragma unroll
+  for (int k = 1; k < 4; k++) {
+    dok[k] = cok[k] = false;
+    dc[k] = 0.0f;
+    qi[k] = 0u;
+    dx[k] = dn[k] = f3(0.0f, 0.0f, 0.0f);
+    if ((uint32_t)k > taps) continue;
+    // classic random neighbour in a uniform disk of radius params4.x
+    const float r = u.params4[0] * __fsqrt_rn(rand_(rng));
+    const float a = kTwoPi * rand_(rng);
+    float sa, ca;
+    sincos_(a, sa, ca);
+    const int qx = gx + itrunc_(ca * r), qy = gy + itrunc_(sa * r);
+    if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
+    const size_t q = (size_t)qy * R.W + qx;
+    const float4 gq = R.gbuf[q];
+    if (gq.w <= 0.0f) continue;
+    const F3 nq = f3(gq.x, gq.y, gq.z);
+    const float nDot = dot3(n1, nq);
+    if (!(nDot > 0.9f && fabsf(gq.w - g.w) < 0.1f * g.w + 0.02f)) continue;
+    const uint4 dq = R.resA[2 * q + 1];
+    dx[k] = surface_at(u, qx, qy, R.W, R.H, gq);
+    dn[k] = nq;
+    dc[k] = (float)((dq.y >> 18) & 0xffu);
+    qi[k] = (uint32_t)q;
+    dok[k] = true;
+    cok[k] = ((dq.y >> 16) & 3u) != kSkNone;
   }
-  float cTotal = 0.0f;
-  for (uint32_t l = 0u; l < nDom; l++) cTotal = cTotal + domC[l];
-
+  SpatialPick pk;
+  pk.cTotal = 0.0f;
+#pragma unroll
+  for (int l = 0; l < 4; l++)
+    if (dok[l]) pk.cTotal = pk.cTotal + dc[l];
   float wSum = 0.0f, selP = 0.0f;
-  RSample sel = null_sample(0.0f);
-  uint32_t selJ = 0u;
-  for (uint32_t j = 0u; j < nCand; j++) {
-    const RSample& s = cand[j];
-    float denom = 0.0f;   // balance heuristic over all domains
-    for (uint32_t l = 0u; l < nDom; l++) denom = denom + domC[l] * eval_target(s, domX1[l], domN1[l]);
-    if (denom <= 0.0f) continue;
-    const uint32_t dj = candDom[j];
-    const float m = (domC[dj] * eval_target(s, domX1[dj], domN1[dj])) / denom;
-    const float pMe = eval_target(s, x1, n1);
-    const float w = (m * pMe) * fmax_(s.W, 0.0f);
-    if (w > 0.0f) {
-      wSum = wSum + w;
-      if (rand_(rng) * wSum < w) { sel = s; selP = pMe; selJ = j; }
+  int rank = 0, selRank = 0;
+  pk.sel = null_sample(0.0f);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (!cok[j]) continue;
+    const RSample s = load_res(R.resA, qi[j]);
+    float denom = 0.0f, num = 0.0f, pMe = 0.0f;   // balance heuristic over all domains
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      if (!dok[l]) continue;
+      const float e = eval_target(s, dx[l], dn[l]);
+      const float term = dc[l] * e;
+      denom = denom + term;
+      if (l == j) num = term;
+      if (l == 0) pMe = e;
     }
+    if (denom > 0.0f) {
+      const float m = num / denom;
+      const float w = (m * pMe) * fmax_(s.W, 0.0f);
+      if (w > 0.0f) {
+        wSum = wSum + w;
+        if (rand_(rng) * wSum < w) { pk.sel = s; selP = pMe; selRank = rank; }
+      }
+    }
+    rank++;
   }
-  if (nCand == 0u || sel.kind == kSkNone || selP <= 0.0f || wSum <= 0.0f) {   // pooled null
-    out_radiance(direct);
-    store_res(R.resB, p, null_sample(fmin_(cTotal, 255.0f)));
-    return;
+  pk.ok = pk.sel.kind != kSkNone && selP > 0.0f && wSum > 0.0f;
+  pk.vis_test = selRank > 0;
+  if (pk.ok) {
+    pk.sel.W = wSum / selP;
+    pk.sel.c = fmin_(pk.cTotal, 255.0f);
   }
-  sel.W = wSum / selP;
-  sel.c = fmin_(cTotal, 255.0f);
-  F3 contrib = f3(0.0f, 0.0f, 0.0f);
-  // the canonical sample's visibility was established when it was traced
-  const bool vis = selJ == 0u || sample_visible(R, occ, sel, x1, n1, cnt);
-  if (vis) contrib = eval_f(sel, x1, n1) * sel.W;
-  out_radiance(direct + contrib);
-  store_res(R.resB, p, sel);
+  return pk;
 }
 
+// The shadow ray of sampleVisible (reuse_spatial.wgsl:117-126); false when
+// the sample is closer than 2 mm (visible without a ray).
+VRT_DI bool visibility_ray(const RSample& s, F3 x1, F3 n1, F3& o, F3& d, float& maxT) {
+  o = x1 + n1 * 1e-3f;
+  if (s.kind == kSkDir) {
+    d = s.pos;
+    maxT = 1e4f;
+    return true;
+  }
+  const F3 v = s.pos - o;
+  const float r = __fsqrt_rn(dot3(v, v));
+  if (r < 2e-3f) return false;
+  d = f3(v.x / r, v.y / r, v.z / r);
+  maxT = r - 2e-3f;
+  return true;
+}
+
+VRT_DI void out_radiance(const RestirDev& R, size_t p, F3 v) {
+  R.rad16[p] = pack_h4(v.x, v.y, v.z, 1.0f);
+  if (R.rad32) R.rad32[p] = make_float4(v.x, v.y, v.z, 1.0f);
+}
+
+VRT_DI F3 load_direct(const RestirDev& R, size_t p) {
+  const float4 dr = unpack_h4(R.direct[p]);
+  return f3(dr.x, dr.y, dr.z);
+}
+
+// Selection, record and (without a pending ray) radiance of pixel (gx, gy).
+// Returns whether a visibility ray is pending; then o / d / maxT describe
+// it and contrib is the contribution it gates.
+VRT_DI bool spatial_pixel(const RestirDev& R, int gx, int gy, F3& o, F3& d, float& maxT, F3& contrib) {
+  const size_t p = (size_t)gy * R.W + gx;
+  const F3 direct = load_direct(R, p);
+  const float4 g = R.gbuf[p];
+  if (g.w <= 0.0f) {   // sky: direct carries the analytic sky radiance
+    out_radiance(R, p, direct);
+    R.resB[2 * p] = make_uint4(0u, 0u, 0u, 0u);
+    R.resB[2 * p + 1] = make_uint4(0u, 0u, 0u, 0u);
+    return false;
+  }
+  const F3 x1 = surface_at(R.u, gx, gy, R.W, R.H, g);
+  const F3 n1 = f3(g.x, g.y, g.z);
+  const SpatialPick pk = spatial_pick(R, gx, gy, g, x1, n1);
+  if (!pk.ok) {   // pooled null
+    out_radiance(R, p, direct);
+    store_res(R.resB, p, null_sample(fmin_(pk.cTotal, 255.0f)));
+    return false;
+  }
+  store_res(R.resB, p, pk.sel);
+  contrib = eval_f(pk.sel, x1, n1) * pk.sel.W;
+  if (pk.vis_test && visibility_ray(pk.sel, x1, n1, o, d, maxT)) return true;
+  out_radiance(R, p, direct + contrib);
+  return false;
+}
+
+// Fused form (megakernel sessions): the visibility ray traced in place.
 template <bool kSmem>
 __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ RestirDev R) {
   extern __shared__ uint32_t s_occ[];
@@ -511,8 +561,49 @@ __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ 
   int gx, gy;
   block_pixel_16x16(gx, gy);
   DCount cnt{0u, 0u, 0u, 0u};
-  if (gx < R.W && gy < R.H) spatial_pixel(R, occ, gx, gy, cnt);
+  if (gx < R.W && gy < R.H) {
+    F3 o, d, contrib;
+    float maxT;
+    if (spatial_pixel(R, gx, gy, o, d, maxT, contrib)) {
+      const size_t p = (size_t)gy * R.W + gx;
+      const bool vis = !occluded(R, occ, o, d, maxT, cnt);
+      out_radiance(R, p, load_direct(R, p) + (vis ? contrib : f3(0.0f, 0.0f, 0.0f)));
+    }
+  }
   if (R.stats) warp_flush_stats(R.stats, cnt, 0u);
+}
+
+// Split form (wavefront sessions): selection here, the pending visibility
+// rays appended to a queue of the wavefront tracer (origin R0, direction and
+// maxT in R2, contribution in S1, pass-through radiance in S0), traced by the
+// persistent tracer, then k_restir_spatial_resolve.
+__global__ void __launch_bounds__(256) k_restir_spatial_select(const __grid_constant__ RestirDev R, WfDev b,
+                                                               int wave) {
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
+  F3 o, d, contrib;
+  float maxT;
+  const bool ray = gx < R.W && gy < R.H && spatial_pixel(R, gx, gy, o, d, maxT, contrib);
+  const uint32_t g = ray ? (uint32_t)gy * (uint32_t)R.W + (uint32_t)gx : 0u;
+  const uint32_t slot = warp_append(b.ctr + 4 * wave, ray);
+  if (ray) {
+    queue_of(b, wave)[slot] = g | kShadowBit;
+    b.R0[g] = make_float4(o.x, o.y, o.z, 0.0f);
+    b.R2[g] = make_float4(d.x, d.y, d.z, maxT);
+    b.S1[g] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_constant__ RestirDev R, WfDev b,
+                                                                int wave) {
+  const int n = b.ctr[4 * wave];
+  const uint32_t* q = queue_of(b, wave);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t g = q[i] & ~kShadowBit;
+    const bool vis = b.hit[g].w == 0u;
+    const float4 c = b.S1[g];
+    out_radiance(R, g, load_direct(R, g) + (vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -629,7 +720,7 @@ __global__ void __launch_bounds__(256) k_wf_restir_primary(const __grid_constant
         if (shadow) {
           sunc = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
           flags |= kFlagShadow;
-          b.R2[g] = make_float4(l.x, l.y, l.z, 0.0f);
+          b.R2[g] = make_float4(l.x, l.y, l.z, 1e4f);
         }
         bounce = u.params0[1] > 0u;
         if (bounce) {
@@ -779,10 +870,7 @@ cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float
   return launch_occ_kernel(k_restir_initial<true>, k_restir_initial<false>, s, W, H, R, st);
 }
 
-cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
-                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
-                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
-                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
+static SingleJob restir_job(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H, const PathOut& out) {
   SingleJob job;
   std::memset(&job, 0, sizeof job);
   job.u = to_uni(uu);
@@ -794,10 +882,22 @@ cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms
   job.fclamp = fclamp;
   job.W = W;
   job.H = H;
+  return job;
+}
+
+static int occ_smem(const SceneDev& s) {
+  const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
+  return smem_occ <= (int)kMaxSmemOccBytes ? smem_occ : 0;
+}
+
+cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
+                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
+                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
+  const SingleJob job = restir_job(s, uu, fclamp, W, H, out);
   const RestirWf r{(uint4*)rb.resA, (uint2*)rb.direct, (float4*)rb.scratch, W, H};
   const uint32_t P = (uint32_t)W * (uint32_t)H;
-  const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
-  const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
+  const int smem = occ_smem(s);
   unsigned long long* stats = out.stats;
   return wf_run_waves(job, P, (int)job.u.params0[1] + 2, smem, wb, tune, stats, st, launches, trace_ev,
                       max_timed_waves, timed_waves, [&](const WfDev& b, int w, int sblocks) {
@@ -818,6 +918,32 @@ cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W
                                   const RestirBufs& rb, cudaStream_t st) {
   const RestirDev R = restir_dev(s, u, 0.0f, W, H, out, rb);
   return launch_occ_kernel(k_restir_spatial<true>, k_restir_spatial<false>, s, W, H, R, st);
+}
+
+cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                            const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches) {
+  const RestirDev R = restir_dev(s, u, 0.0f, W, H, out, rb);
+  const SingleJob job = restir_job(s, u, 0.0f, W, H, out);
+  const WfDev b = wf_view(wb);
+  const int wave = 0;   // the initial pass's waves are complete: reuse slot 0
+  cudaError_t e = cudaMemsetAsync(wb.ctr, 0, 16, st);
+  if (e != cudaSuccess) return e;
+  k_restir_spatial_select<<<dim3((W + 15) / 16, (H + 15) / 16), 256, 0, st>>>(R, b, wave);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int sms = wf_sm_count();
+  const int smem = occ_smem(s);
+  const int refill = tune.refill_min > 0 ? tune.refill_min : 8;
+  if (smem > 0)
+    e = wf_dispatch_trace<SingleJob, true>(tune.trace_variant, job, smem, tune.trace_blocks_per_sm, sms, b, wave, 0,
+                                           refill, out.stats, st);
+  else
+    e = wf_dispatch_trace<SingleJob, false>(tune.trace_variant, job, 0, tune.trace_blocks_per_sm, sms, b, wave, 0,
+                                            refill, out.stats, st);
+  if (e != cudaSuccess) return e;
+  k_restir_spatial_resolve<<<sms * 8, 256, 0, st>>>(R, b, wave);
+  if (launches) *launches += 3;
+  return cudaGetLastError();
 }
 
 }  // namespace vrt

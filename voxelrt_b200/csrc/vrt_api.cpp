@@ -651,6 +651,11 @@ static int restir_pass(VrtSession* s, const VrtUniforms* u, bool spatial) {
   const int p = parity_of(s);
   PathOut o;
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[p]; o.stats = s->stats;
+  if (spatial && s->path_kernel == VRT_PATH_WAVEFRONT) {
+    CUDA_TRY(launch_restir_spatial_wavefront(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->wf, s->tune,
+                                             s->ctx->stream, &s->launches));
+    return VRT_OK;
+  }
   if (spatial) {
     CUDA_TRY(launch_restir_spatial(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->ctx->stream));
   } else {

@@ -255,5 +255,10 @@ cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int 
                                    const RestirBufs& rb, cudaStream_t st);
 cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
                                   const RestirBufs& rb, cudaStream_t st);
+// The spatial pass with its visibility rays on the wavefront tracer (select,
+// trace, resolve; bit-identical to launch_restir_spatial).
+cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
+                                            const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches);
 
 }  // namespace vrt

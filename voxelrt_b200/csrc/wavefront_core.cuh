@@ -18,7 +18,7 @@ constexpr uint32_t kShadowBit = 0x80000000u;
 struct WfDev {
   float4* R0;      // ray origin: camera position (primary) or surf = pos + n*1e-3
   float4* R1;      // primary / bounce direction
-  float4* R2;      // sun direction of the pending shadow ray
+  float4* R2;      // direction (xyz) and maxT (w) of the pending shadow ray
   float4* S0;      // radiance xyz, w = RNG state bits
   float4* S1;      // throughput xyz, w = primary material bits
   float4* S2;      // pending sun contribution xyz, w = flags
@@ -424,7 +424,7 @@ VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, uint32_t g, uint32_t k, F
     const F3 sunRad = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
     sunc = (((tp * mat.albedo) * kInvPi) * ndl) * sunRad;
     flags |= kFlagShadow;
-    b.R2[g] = make_float4(l.x, l.y, l.z, 0.0f);
+    b.R2[g] = make_float4(l.x, l.y, l.z, 1e4f);
   }
   want_bounce = false;
   if (k == kmax) {
@@ -528,9 +528,16 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
           const uint32_t g = entry & ~kShadowBit;
           S = jobs.scene(jobs.job_of(g));
           const F3 ro = xyz(b.R0[g]);
-          rd = (entry & kShadowBit) ? xyz(b.R2[g]) : xyz(b.R1[g]);
+          float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w
+          if (entry & kShadowBit) {
+            const float4 r2 = b.R2[g];
+            rd = xyz(r2);
+            maxT = r2.w;
+          } else {
+            rd = xyz(b.R1[g]);
+          }
           c.rays++;
-          d.init(S, ro, rd, 1e4f);
+          d.init(S, ro, rd, maxT);
           active = true;
         }
       }
