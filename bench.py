@@ -1011,12 +1011,22 @@ def sweep(args, server, sessions, make_request, rng):
     return results
 
 
+RESTIR_RUNS = [   # (label, preset, bounces, params0.z flags: bit0 temporal, bit1 denoise)
+    ("plain", "base", 2, 3),
+    ("gi", "gi", 2, 3),
+    ("ours", "ours", 2, 3),
+    ("ours_b6_nodenoise", "ours", 6, 1),
+]
+
+
 def run_restir(args, local):
-    """`--mode restir`: the reference's ReSTIR `gi` preset (RF_RESTIR |
-    RF_TEMPORAL | RF_SPATIAL: initial candidates, temporal + spatial reservoir
-    reuse, then temporal / a-trous / present) on the full-size workload, timed
-    like the plain frame, with the plain frame measured beside it and the CPU
-    oracle's ReSTIR frame as the CPU baseline."""
+    """`--mode restir`: the reference's ReSTIR presets -- `gi` (RF_RESTIR |
+    RF_TEMPORAL | RF_SPATIAL) and its default `ours` (paired reuse, duplication
+    map, vector weights, unified light-list NEE with power sampling, plane,
+    rescue, full visibility, clamp) -- on the full-size workload, timed like
+    the plain frame, with the plain frame measured beside them.  `value` is
+    `ours` at 6 bounces with the denoiser off, the configuration of the
+    reference's published GPU timings (docs/STATUS.md:79-81, RTX 3080)."""
     import numpy as np
     import torch
 
@@ -1027,21 +1037,24 @@ def run_restir(args, local):
     vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
     ctx = vrt.Context(local)
     scene = vrt.Scene(ctx, vox, n)
+    nlights = int(scene.build_lights().count)
     sess = vrt.Session(ctx, scene, W, H, firefly_clamp=WORKLOAD["fclamp"], accum_f32=False,
                        path_kernel=args.path_kernel)
     sess.set_timing(True)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
 
-    def uni(f, preset):
-        u = frame_uniforms(vrt, spawn, f)
-        u.params2[0] = vrt.api.preset_flags(preset)
-        return u
+    def uni(f, preset, bounces, flags):
+        k = f % WORKLOAD["path_frames"]
+        pose = vrt.camera_spline(spawn, k)
+        prev = vrt.camera_spline(spawn, k - 1) if k > 0 else None
+        return vrt.make_uniforms(pose, prev, vrt.Lighting(), f, bounces, flags, W, H, 1.0, WORKLOAD["maxhist"],
+                                 preset=preset, light_count=nlights)
 
     res, clk = {}, None
-    for preset in ("base", "gi"):
+    for label, preset, bounces, flags in RESTIR_RUNS:
         sess.reset()
         for i in range(args.warmup):
-            sess.frame(uni(i, preset))
+            sess.frame(uni(i, preset, bounces, flags))
             sess.stats()
         ctx.synchronize()
         clocks = ClockSampler(local)
@@ -1050,7 +1063,7 @@ def run_restir(args, local):
         for i in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            sess.frame(uni(args.warmup + i, preset))
+            sess.frame(uni(args.warmup + i, preset, bounces, flags))
             st = sess.stats()
             fm.append(st.ms_total)
             pt.append(st.ms_pathtrace)
@@ -1059,44 +1072,47 @@ def run_restir(args, local):
             launches += st.launches
         ctx.synchronize()
         c = clocks.stop()
-        if preset == "gi":
+        if label == RESTIR_RUNS[-1][0]:
             clk = c
-        res[preset] = {"frame_ms_mean": round(statistics.mean(fm), 4), "frame_ms_p50": round(statistics.median(fm), 4),
-                       "frame_ms_p99": round(float(np.percentile(fm, 99)), 4),
-                       "pathtrace_ms_mean": round(statistics.mean(pt), 4),
-                       "reuse_ms_mean": round(statistics.mean(ru), 4),
-                       "rays_per_frame": round(rays / args.steps), "launches": launches,
-                       "mrays_s": round(rays / (sum(fm) / 1e3) / 1e6, 2)}
+        res[label] = {"preset": preset, "bounces": bounces, "denoise": bool(flags & 2),
+                      "frame_ms_mean": round(statistics.mean(fm), 4), "frame_ms_p50": round(statistics.median(fm), 4),
+                      "frame_ms_p99": round(float(np.percentile(fm, 99)), 4),
+                      "pathtrace_ms_mean": round(statistics.mean(pt), 4),
+                      "reuse_ms_mean": round(statistics.mean(ru), 4),
+                      "rays_per_frame": round(rays / args.steps), "launches": launches,
+                      "mrays_s": round(rays / (sum(fm) / 1e3) / 1e6, 2)}
     sess.close()
     scene.close()
     ctx.close()
-    gi = res["gi"]
+    head = res[RESTIR_RUNS[-1][0]]
     line = {
-        "metric": "ReSTIR gi frame ms at 1080p (initial + temporal/spatial reuse + temporal + a-trous + present)",
-        "value": gi["frame_ms_mean"], "unit": "ms/frame", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": gi["frame_ms_mean"], "higher_is_better": False,
+        "metric": "ReSTIR `ours` frame ms at 1080p, 6 bounces, denoiser off (initial + reuse + temporal + present)",
+        "value": head["frame_ms_mean"], "unit": "ms/frame", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["frame_ms_mean"], "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded procedural voxel world and camera path)",
-        "config": {"workload": "ReSTIR gi preset on " + WORKLOAD_NAME, "preset": "gi (flags 7)", "taps": 3,
-                   "radius_px": 30, "ccap": 20, "path_kernel": args.path_kernel,
+        "config": {"workload": "ReSTIR presets on " + WORKLOAD_NAME, "lights": nlights, "taps": 3, "radius_px": 30,
+                   "ccap": 20, "pairing_sigma": 16, "path_kernel": args.path_kernel,
                    "l2": "flushed before every timed frame (256 MB write), outside the timed events"},
-        "gi": gi, "plain": res["base"],
-        "gi_over_plain_frame_ms": round(gi["frame_ms_mean"] / res["base"]["frame_ms_mean"], 3),
-        "gpu_launches": gi["launches"],
+        "runs": res,
+        "reference_published_ms": {"ours_b6_nodenoise_1080p_rtx3080_webgpu": {
+            "exterior": 22.56, "lamps": 33.31, "interior": 33.96,
+            "note": "other hardware and scenes (docs/STATUS.md:79-81); context, not a like-for-like ratio"}},
+        "gpu_launches": head["launches"],
     }
     if clk:
         line["clocks"] = clk
     if not args.no_cpu_baseline:
         import oracle
         b, m = oracle.build_bricks(vox, n)
-        u = uni(0, "gi")
+        u = uni(0, "gi", 2, 3)
         t0 = time.perf_counter()
         r = oracle.frame(vox, b, m, n, vrt.uniforms_bytes(u), WORKLOAD["fclamp"], W, H,
                          np.zeros((H, W, 4), np.uint16), np.zeros((H, W, 4), np.float32))
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": round(dt * 1e3, 1), "unit": "ms/frame", "cores": oracle.num_threads(),
                                 "kind": "port", "rays": r["stats"]["rays"],
-                                "sample": "1 full ReSTIR gi frame of the workload through the CPU oracle"}
+                                "sample": "1 full ReSTIR gi frame (2 bounces) of the workload through the CPU oracle"}
     print(json.dumps(line), flush=True)
 
 

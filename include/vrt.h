@@ -66,9 +66,14 @@ typedef struct VrtUniforms {
   uint32_t params0[4];     /* x frame index (RNG stream), y bounces,
                               z flags: bit0 temporal, bit1 denoise             */
   float params1[4];        /* x width, y height, z exposure                    */
-  uint32_t params2[4];     /* x restir flags: 0 (preset=base) or a subset of
-                              RF_RESTIR|RF_TEMPORAL|RF_SPATIAL = 1|2|4 with
-                              RF_RESTIR set (preset=gi is 7); z spatial taps  */
+  uint32_t params2[4];     /* x restir flags (common.wgsl:40-59): 0 = preset
+                              base; with RF_RESTIR (1) any of TEMPORAL 2,
+                              SPATIAL 4, PAIRED 8, DUPMAP 16, FOOTPRINT 32,
+                              VECTOR 64, UNIFIED 128, PLANE 256, RESCUE 512,
+                              FULLV 1024, CLAMP 2048, LIGHTPOWER 4096,
+                              MIXSIGMA 8192, ADAPTCAND 16384, LIGHTGRID
+                              65536, HISTISOLATE 262144; y light count;
+                              z spatial taps                                  */
   float params3[4];        /* x = temporal confidence cap (default 20)         */
   float params4[4];        /* x = spatial disk radius in pixels (default 30),
                               y = max temporal history (default 64)            */
@@ -212,6 +217,15 @@ int vrt_frame(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_reuse_temporal(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_reuse_spatial(VrtSession* s, const VrtUniforms* u);
+/* dupmap.wgsl: the duplication map of reservoirs B (no-op without
+ * RF_DUPMAP); vrt_frame runs it after reuse_spatial (main.js:741). */
+int vrt_pass_dupmap(VrtSession* s, const VrtUniforms* u);
+/* Base sigma of the pairing textures of RF_PAIRED (main.js:73 `sigma`,
+ * default 16); the wide tap's sigma under RF_MIXSIGMA is params5.x. */
+int vrt_session_set_pairing_sigma(VrtSession* s, float sigma);
+/* The pairing buffer itself (pairing.js:80-89, seeds 0xc0ffee + 7919 i):
+ * 254^2 + 230^2 + 210^2 words for sigmas[0..2]; host only. */
+int vrt_make_pairing(const double* sigmas, uint32_t* out, size_t words);
 int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u);
 int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int iteration /*0,1,2*/);
 int vrt_pass_present(VrtSession* s, const VrtUniforms* u);
@@ -245,6 +259,7 @@ int vrt_read_hdr(VrtSession* s, float* host_rgb, size_t bytes);      /* f32 RGB 
  * frame of the session. */
 int vrt_read_reservoirs(VrtSession* s, int which, void* host, size_t bytes);
 int vrt_read_direct(VrtSession* s, void* host, size_t bytes);
+int vrt_read_dupmap(VrtSession* s, void* host, size_t bytes);       /* f32 per pixel */
 /* Writes history buffers (resume from a saved session state). */
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
 

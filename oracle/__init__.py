@@ -229,8 +229,16 @@ def pcg_hash(v: int) -> int:
     return int(f(C.c_uint32(v)))
 
 
-def restir_initial(vox, bricks, masks, n, ubytes, fclamp: float, w: int, h: int):
-    """ReSTIR initial-candidate pass (pathtrace.wgsl:332-457, unification off).
+PAIRING_WORDS = 254 * 254 + 230 * 230 + 210 * 210
+
+
+def _ptr_or_none(a):
+    return _p(np.ascontiguousarray(a)) if a is not None else None
+
+
+def restir_initial(vox, bricks, masks, n, ubytes, fclamp: float, w: int, h: int, lights=None):
+    """ReSTIR initial-candidate pass (pathtrace.wgsl:332-457).  lights: dict
+    with "words", "alias", "grid" (the scene's light data) for RF_UNIFIED.
     Returns rad16, rad32 (sky pixels only), alb8, gbuf, resA (u32 HxWx8, the
     32-byte reservoir records), direct (rgba16f bits), stats."""
     ub = np.frombuffer(ubytes, np.uint8).copy()
@@ -241,23 +249,32 @@ def restir_initial(vox, bricks, masks, n, ubytes, fclamp: float, w: int, h: int)
     res_a = np.zeros((h, w, 8), np.uint32)
     direct = np.zeros((h, w, 4), np.uint16)
     st = OrcStats()
+    lw = la = lg = None
+    if lights is not None:
+        lw = np.ascontiguousarray(lights["words"], np.uint32)
+        la = np.ascontiguousarray(lights["alias"], np.float32)
+        lg = np.ascontiguousarray(lights["grid"], np.uint32)
     lib().orc_restir_initial(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_float(fclamp), C.c_int(w),
-                             C.c_int(h), _p(rad16), _p(rad32), _p(alb8), _p(gbuf), _p(res_a), _p(direct), C.byref(st))
+                             C.c_int(h), _ptr_or_none(lw), _ptr_or_none(la), _ptr_or_none(lg), _p(rad16), _p(rad32),
+                             _p(alb8), _p(gbuf), _p(res_a), _p(direct), C.byref(st))
     return {"rad16": rad16, "rad32": rad32, "alb8": alb8, "gbuf": gbuf, "resA": res_a, "direct": direct,
             "stats": {k: int(getattr(st, k)) for k, _ in OrcStats._fields_}}
 
 
-def restir_temporal(ubytes, w: int, h: int, gcur, gprev, res_b, res_a):
-    """Temporal reservoir reuse (reuse_temporal.wgsl); returns the merged A."""
+def restir_temporal(ubytes, w: int, h: int, gcur, gprev, res_b, res_a, dup=None):
+    """Temporal reservoir reuse (reuse_temporal.wgsl); dup = the previous
+    frame's duplication map (RF_DUPMAP).  Returns the merged A."""
     ub = np.frombuffer(ubytes, np.uint8).copy()
     out = np.array(res_a, np.uint32, copy=True, order="C")
+    d = np.zeros((h, w), np.float32) if dup is None else np.ascontiguousarray(dup, np.float32)
     lib().orc_restir_temporal(_p(ub), C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(gcur, np.float32)),
                               _p(np.ascontiguousarray(gprev, np.float32)), _p(np.ascontiguousarray(res_b, np.uint32)),
-                              _p(out))
+                              _p(d), _p(out))
     return out
 
 
-def restir_spatial(vox, bricks, masks, n, ubytes, w: int, h: int, gcur, res_a, direct, rad16=None, rad32=None):
+def restir_spatial(vox, bricks, masks, n, ubytes, w: int, h: int, gcur, res_a, direct, rad16=None, rad32=None,
+                   pairing=None):
     """Spatial reuse + shading (reuse_spatial.wgsl).  Returns rad16, rad32,
     resB (next frame's history) and the visibility rays traced."""
     ub = np.frombuffer(ubytes, np.uint8).copy()
@@ -265,42 +282,67 @@ def restir_spatial(vox, bricks, masks, n, ubytes, w: int, h: int, gcur, res_a, d
     rad32 = np.zeros((h, w, 4), np.float32) if rad32 is None else np.array(rad32, np.float32, copy=True)
     res_b = np.zeros((h, w, 8), np.uint32)
     st = OrcStats()
+    pr = None if pairing is None else np.ascontiguousarray(pairing, np.uint32)
     lib().orc_restir_spatial(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_int(w), C.c_int(h),
                              _p(np.ascontiguousarray(gcur, np.float32)), _p(np.ascontiguousarray(res_a, np.uint32)),
-                             _p(np.ascontiguousarray(direct, np.uint16)), _p(rad16), _p(rad32), _p(res_b), C.byref(st))
+                             _p(np.ascontiguousarray(direct, np.uint16)), _ptr_or_none(pr), _p(rad16), _p(rad32),
+                             _p(res_b), C.byref(st))
     return {"rad16": rad16, "rad32": rad32, "resB": res_b,
             "stats": {k: int(getattr(st, k)) for k, _ in OrcStats._fields_}}
 
 
-def restir_path(vox, bricks, masks, n, ubytes, fclamp, w, h, gprev, res_b_prev):
-    """The ReSTIR passes of one frame (main.js:736-739): initial -> temporal
-    reuse (RF_TEMPORAL) -> spatial reuse.  Returns every intermediate; "resA0"
-    is A after the initial pass, "resA" after temporal reuse."""
-    pt = restir_initial(vox, bricks, masks, n, ubytes, fclamp, w, h)
+def restir_dupmap(w: int, h: int, res_b):
+    """dupmap.wgsl: duplication score per pixel from reservoirs B."""
+    out = np.zeros((h, w), np.float32)
+    lib().orc_restir_dupmap(C.c_int(w), C.c_int(h), _p(np.ascontiguousarray(res_b, np.uint32)), _p(out))
+    return out
+
+
+def pairing_buffer(sigmas):
+    """makePairingBuffer (pairing.js:80-89) for three sigmas."""
+    sg = np.ascontiguousarray(sigmas, np.float64)
+    out = np.zeros(PAIRING_WORDS, np.uint32)
+    lib().orc_pairing_buffer(_p(sg), _p(out))
+    return out
+
+
+def restir_path(vox, bricks, masks, n, ubytes, fclamp, w, h, gprev, res_b_prev, dup_prev=None, lights=None,
+                pairing=None):
+    """The ReSTIR passes of one frame (main.js:736-741): initial -> temporal
+    reuse (RF_TEMPORAL) -> spatial reuse -> duplication map (RF_DUPMAP).
+    Returns every intermediate; "resA0" is A after the initial pass, "resA"
+    after temporal reuse, "dup" the map this frame leaves for the next."""
+    pt = restir_initial(vox, bricks, masks, n, ubytes, fclamp, w, h, lights)
     res = dict(pt)
     res["resA0"] = pt["resA"]
     flags = int(np.frombuffer(ubytes, np.uint32)[56])
     res_a = pt["resA"]
     if flags & 1 and flags & 2:
-        res_a = restir_temporal(ubytes, w, h, pt["gbuf"], gprev, res_b_prev, res_a)
+        res_a = restir_temporal(ubytes, w, h, pt["gbuf"], gprev, res_b_prev, res_a, dup_prev)
     res["resA"] = res_a
-    sp = restir_spatial(vox, bricks, masks, n, ubytes, w, h, pt["gbuf"], res_a, pt["direct"], pt["rad16"], pt["rad32"])
+    sp = restir_spatial(vox, bricks, masks, n, ubytes, w, h, pt["gbuf"], res_a, pt["direct"], pt["rad16"], pt["rad32"],
+                        pairing)
     res["rad16"], res["rad32"], res["resB"] = sp["rad16"], sp["rad32"], sp["resB"]
+    res["dup"] = restir_dupmap(w, h, sp["resB"]) if flags & (16 | 131072) else dup_prev
     res["stats"] = dict(pt["stats"])
     for k in ("rays", "outer", "inner", "vreads"):
         res["stats"][k] += sp["stats"][k]
     return res
 
 
-def frame(vox, bricks, masks, n, ubytes, fclamp, w, h, acc_prev, gprev, acc_f32=False, res_b_prev=None):
+def frame(vox, bricks, masks, n, ubytes, fclamp, w, h, acc_prev, gprev, acc_f32=False, res_b_prev=None,
+          dup_prev=None, lights=None, pairing=None):
     """One full oracle frame: pathtrace (or the ReSTIR passes when params2.x
-    has RF_RESTIR; res_b_prev = the previous frame's reservoirs B) ->
-    temporal -> a-trous x3 (if the denoise flag is set) -> present.  Returns
-    every intermediate."""
+    has RF_RESTIR; res_b_prev / dup_prev = the previous frame's reservoirs B
+    and duplication map, lights / pairing as for restir_path) -> temporal ->
+    a-trous x3 (if the denoise flag is set) -> present.  Returns every
+    intermediate."""
     if int(np.frombuffer(ubytes, np.uint32)[56]) & 1:
         if res_b_prev is None:
             res_b_prev = np.zeros((h, w, 8), np.uint32)
-        pt = restir_path(vox, bricks, masks, n, ubytes, fclamp, w, h, gprev, res_b_prev)
+        if dup_prev is None:
+            dup_prev = np.zeros((h, w), np.float32)
+        pt = restir_path(vox, bricks, masks, n, ubytes, fclamp, w, h, gprev, res_b_prev, dup_prev, lights, pairing)
     else:
         pt = pathtrace(vox, bricks, masks, n, ubytes, fclamp, w, h)
     flags = np.frombuffer(ubytes, np.uint32)[48 + 2]

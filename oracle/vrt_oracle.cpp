@@ -10,7 +10,9 @@
 //   src/shaders/atrous.wgsl:26-83     edge-aware a-trous iteration
 //   src/shaders/present.wgsl:40-55    remodulate, exposure, ACES, gamma
 //   src/shaders/pathtrace.wgsl:199-246, 332-457, restir.wgsl,
-//   reuse_temporal.wgsl, reuse_spatial.wgsl   ReSTIR `gi` preset passes
+//   reuse_temporal.wgsl, reuse_spatial.wgsl, dupmap.wgsl, pairing.js
+//                                     ReSTIR passes (all flags but the world
+//                                     cache, mutation and the quality signal)
 //   src/main.js:628-659               HDR capture = illum * (alb8/255)^2
 //   src/scene.js:411-433              brick occupancy words + 16-word masks
 //   src/math.js:3-74, src/camera.js:47-57   view/projection matrices
@@ -652,10 +654,25 @@ inline float luminance(const float* c) { return std::fmaf(c[2], 0.0722f, std::fm
 
 
 // ---------------------------------------------------------------------------
-// ReSTIR `gi` preset (RF_RESTIR | RF_TEMPORAL | RF_SPATIAL, main.js:44)
+// ReSTIR pipeline (pathtrace.wgsl:1-246, 332-457, restir.wgsl,
+// reuse_temporal.wgsl, reuse_spatial.wgsl, dupmap.wgsl, pairing.js)
 // ---------------------------------------------------------------------------
 const uint32_t SK_NONE = 0u, SK_POINT = 1u, SK_DIR = 2u;   // restir.wgsl:29-31
-const uint32_t RF_SPATIAL = 4u;                            // common.wgsl:42
+// common.wgsl:40-59
+const uint32_t RF_TEMPORAL = 2u, RF_SPATIAL = 4u, RF_PAIRED = 8u, RF_DUPMAP = 16u, RF_FOOTPRINT = 32u,
+               RF_VECTOR = 64u, RF_UNIFIED = 128u, RF_PLANE = 256u, RF_RESCUE = 512u, RF_FULLV = 1024u,
+               RF_CLAMP = 2048u, RF_LIGHTPOWER = 4096u, RF_MIXSIGMA = 8192u, RF_ADAPTCAND = 16384u,
+               RF_LIGHTGRID = 65536u, RF_MUTATE = 131072u, RF_HISTISOLATE = 262144u;
+inline bool rflag(const Uni& u, uint32_t f) { return (u.params2[0] & f) != 0u; }
+
+// Scene light data and reuse inputs (main.js:223-263).
+struct RestirAux {
+  const uint32_t* lights;    // 2 words per emissive face
+  const float* alias;        // 4 floats per face
+  const uint32_t* grid;      // 34 words per brick cell
+  const uint32_t* pairing;   // 254^2 + 230^2 + 210^2 words
+  const float* dup;          // previous frame's duplication map
+};
 
 // Decoded reservoir sample (restir.wgsl:33-41).
 struct RSample {
@@ -675,12 +692,17 @@ inline RSample null_sample(float c) {
   return s;
 }
 
-// WGSL f32 -> i32: toward zero, saturating, NaN -> 0.
+// WGSL f32 -> i32 / u32: toward zero, saturating, NaN -> 0.
 inline int itrunc(float x) {
   if (x != x) return 0;
   if (x >= 2147483648.0f) return 2147483647;
   if (x < -2147483648.0f) return (-2147483647 - 1);
   return (int)x;
+}
+inline uint32_t utrunc(float x) {
+  if (!(x > 0.0f)) return 0u;
+  if (x >= 4294967296.0f) return 4294967295u;
+  return (uint32_t)x;
 }
 
 // pack2x16snorm / unpack2x16snorm, one component (WGSL builtin definitions).
@@ -711,8 +733,7 @@ inline f3 oct_decode(float ex, float ey) {
 
 // packReservoir (restir.wgsl:61-71): 8 words, posW then data.
 inline void pack_res(const RSample& s, uint32_t* w) {
-  float cf = s.c + 0.5f;
-  uint32_t cq = std::min(cf >= 4294967296.0f ? 4294967295u : (uint32_t)cf, 255u);
+  uint32_t cq = std::min(utrunc(s.c + 0.5f), 255u);
   f3 nn = s.kind != SK_POINT ? mk(0, 1, 0) : s.n;
   float ex, ey;
   oct_encode(nn, ex, ey);
@@ -760,6 +781,17 @@ inline f3 eval_f(const RSample& s, f3 x1, f3 n1) {
 }
 inline float eval_target(const RSample& s, f3 x1, f3 n1) { return rlum(eval_f(s, x1, n1)); }
 
+// footprintOK (restir.wgsl:172-180)
+inline bool footprint_ok(const Uni& u, const RSample& s, f3 x1, f3 n1, float tPrim, float cosView) {
+  if (s.kind != SK_POINT) return true;
+  f3 d = sub(s.pos, x1);
+  float r2 = dot3(d, d);
+  f3 dir = muls(d, 1.0f / std::sqrt(fmaxf_(r2, 1e-8f)));
+  float cos1 = fmaxf_(dot3(n1, dir), 0.0f);
+  float cos2 = fmaxf_(dot3(s.n, mk(-dir.x, -dir.y, -dir.z)), 0.0f);
+  return r2 >= u.params3[3] * tPrim * tPrim * cos1 * cos2 / fmaxf_(cosView, 0.05f);
+}
+
 // receiverPoint (restir.wgsl:127-137); WGSL round() is half-to-even.
 inline f3 receiver_point(f3 ro, f3 rd, float t, f3 n1) {
   f3 approx = add(ro, muls(rd, t));
@@ -782,25 +814,156 @@ inline f3 surface_at(const Uni& u, int qx, int qy, int Wd, int Hd, const float* 
 
 inline f3 firefly(float fclamp, f3 v) { return fclamp <= 0.0f ? v : min3(v, mk(fclamp, fclamp, fclamp)); }
 
-// estimateLo (pathtrace.wgsl:205-246), unification off.
-f3 estimate_lo(const World& W, const Uni& u, float fclamp, f3 x2, f3 n2, Mat mat2, Rng& rng, PixStats& st) {
-  auto shadowed = [&](f3 o, f3 d, float maxT) {
-    Hit h = trace(W, o, d, maxT);
-    st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
-    return h.t >= 0.0f;
-  };
+inline bool shadow_ray(const World& W, f3 o, f3 d, float maxT, PixStats& st) {
+  Hit h = trace(W, o, d, maxT);
+  st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+  return h.t >= 0.0f;
+}
+
+// ---- emissive-face sampling (pathtrace.wgsl:37-199) -------------------------
+struct LightPoint { f3 pos, n, Le; float pdfA; };
+
+// sampleGlobalLightIndex (pathtrace.wgsl:49-60)
+uint32_t global_light_index(const Uni& u, const RestirAux& ax, Rng& rng) {
+  uint32_t count = u.params2[1];
+  if (rflag(u, RF_LIGHTPOWER)) {
+    float uLight = rng.next() * (float)count;
+    uint32_t base = std::min(utrunc(uLight), count - 1u);
+    float frac = uLight - (float)base;
+    const float* rec = ax.alias + 4 * (size_t)base;
+    uint32_t aliasLi = std::min(utrunc(rec[1] + 0.5f), count - 1u);
+    return frac >= rec[0] ? aliasLi : base;
+  }
+  return std::min(utrunc(rng.next() * (float)count), count - 1u);
+}
+
+// globalLightPdf (pathtrace.wgsl:62-65)
+float global_light_pdf(const Uni& u, const RestirAux& ax, uint32_t li) {
+  if (rflag(u, RF_LIGHTPOWER)) return fmaxf_(ax.alias[4 * (size_t)li + 2], 1e-8f);
+  return 1.0f / (float)u.params2[1];
+}
+
+// pickLightIndex (pathtrace.wgsl:80-121)
+uint32_t pick_light_index(const Uni& u, const RestirAux& ax, int BG, f3 pos, Rng& rng, float& pdf) {
+  if (!rflag(u, RF_LIGHTGRID)) {
+    uint32_t li = global_light_index(u, ax, rng);
+    pdf = global_light_pdf(u, ax, li);
+    return li;
+  }
+  const float k = INV_VOXEL / (float)BRICK;
+  int bx = iclamp(ifloor(pos.x * k), 0, BG - 1), by = iclamp(ifloor(pos.y * k), 0, BG - 1),
+      bz = iclamp(ifloor(pos.z * k), 0, BG - 1);
+  const uint32_t* cell = ax.grid + (size_t)(uint32_t)(bx + by * BG + bz * BG * BG) * 34u;
+  uint32_t n = std::min(cell[0], 16u);
+  float wSum = bitsf(cell[1]);
+  if (n == 0u || wSum <= 0.0f) {
+    uint32_t li = global_light_index(u, ax, rng);
+    pdf = global_light_pdf(u, ax, li);
+    return li;
+  }
+  uint32_t li;
+  if (rng.next() < 0.75f) {
+    float r = rng.next() * wSum;
+    li = cell[2];
+    for (uint32_t i = 0; i < n; i++) {
+      li = cell[2 + 2 * i];
+      r -= bitsf(cell[3 + 2 * i]);
+      if (r <= 0.0f) break;
+    }
+  } else {
+    li = global_light_index(u, ax, rng);
+  }
+  float pCell = 0.0f;
+  for (uint32_t i = 0; i < n; i++)
+    if (cell[2 + 2 * i] == li) { pCell = bitsf(cell[3 + 2 * i]) / wSum; break; }
+  pdf = 0.75f * pCell + (1.0f - 0.75f) * global_light_pdf(u, ax, li);
+  return li;
+}
+
+// sampleLightFace (pathtrace.wgsl:123-144)
+LightPoint sample_light_face(const Uni& u, const RestirAux& ax, int BG, f3 shadePos, Rng& rng) {
+  float pdfSelect;
+  uint32_t li = pick_light_index(u, ax, BG, shadePos, rng, pdfSelect);
+  uint32_t lx = ax.lights[2 * (size_t)li], lm = ax.lights[2 * (size_t)li + 1];
+  f3 v = mk((float)(lx & 0x1ffu), (float)((lx >> 9) & 0x1ffu), (float)((lx >> 18) & 0x1ffu));
+  uint32_t face = (lx >> 27) & 7u, axis = face >> 1;
+  float pos = (face & 1u) == 0u ? 1.0f : 0.0f;
+  float r0 = rng.next();
+  float r1 = rng.next();
+  float r2 = rng.next();
+  f3 q = add(v, mk(r0, r1, r2));
+  f3 n = mk(0, 0, 0);
+  if (axis == 0u) { q.x = v.x + pos; n.x = pos > 0.5f ? 1.0f : -1.0f; }
+  else if (axis == 1u) { q.y = v.y + pos; n.y = pos > 0.5f ? 1.0f : -1.0f; }
+  else { q.z = v.z + pos; n.z = pos > 0.5f ? 1.0f : -1.0f; }
+  Mat mat = unpack_material(lm);
+  LightPoint lp;
+  lp.pos = muls(q, VOXEL_SIZE);
+  lp.n = n;
+  lp.Le = muls(mat.albedo, mat.emissive * EMISSIVE_SCALE);
+  lp.pdfA = pdfSelect / (VOXEL_SIZE * VOXEL_SIZE);
+  return lp;
+}
+
+// emissiveCandCount (pathtrace.wgsl:155-159)
+uint32_t emissive_cand_count(const Uni& u, uint32_t bounce) {
+  if (!rflag(u, RF_ADAPTCAND)) return bounce == 0u ? 4u : 1u;
+  float n0 = clampf(std::nearbyint(u.params5[1] * 4.0f * (1.0f + om_log2(1.0f + (float)u.params2[1] / 256.0f))),
+                    1.0f, 16.0f);
+  return std::max(utrunc(n0) >> std::min(bounce, 31u), 1u);
+}
+
+// emissiveNEE (pathtrace.wgsl:167-199)
+f3 emissive_nee(const World& W, const Uni& u, const RestirAux& ax, f3 pos, f3 n, f3 albedo, uint32_t nCand, Rng& rng,
+                PixStats& st) {
+  if (u.params2[1] == 0u) return mk(0, 0, 0);
+  f3 surf = add(pos, muls(n, 1e-3f));
+  float invM = 1.0f / (float)nCand;
+  float wSum = 0.0f, selLum = 0.0f, selR2 = 0.0f;
+  f3 sel = mk(0, 0, 0), selDir = mk(0, 0, 0);
+  for (uint32_t k = 0; k < nCand; k++) {
+    LightPoint lp = sample_light_face(u, ax, W.BG, pos, rng);
+    f3 d = sub(lp.pos, surf);
+    float r2 = fmaxf_(dot3(d, d), 1e-6f);
+    f3 dir = muls(d, 1.0f / std::sqrt(r2));
+    float cos1 = dot3(n, dir);
+    float cos2 = dot3(lp.n, mk(-dir.x, -dir.y, -dir.z));
+    if (cos1 <= 0.0f || cos2 <= 0.0f) continue;
+    // albedo * INV_PI * cos1 * cos2 / r2 * lp.Le / lp.pdfA, left to right
+    f3 v = muls(muls(muls(albedo, INV_PI), cos1), cos2);
+    v = mk(v.x / r2, v.y / r2, v.z / r2);
+    v = mul(v, lp.Le);
+    v = mk(v.x / lp.pdfA, v.y / lp.pdfA, v.z / lp.pdfA);
+    float w = rlum(v) * invM;
+    if (w <= 0.0f) continue;
+    bool first = wSum == 0.0f;
+    wSum += w;
+    if (first || rng.next() * wSum < w) { sel = v; selLum = rlum(v); selDir = dir; selR2 = r2; }
+  }
+  if (wSum <= 0.0f) return mk(0, 0, 0);
+  float r = std::sqrt(selR2);
+  if (shadow_ray(W, surf, selDir, r - 2e-3f, st)) return mk(0, 0, 0);
+  return muls(sel, wSum / selLum);
+}
+
+// estimateLo (pathtrace.wgsl:205-246)
+f3 estimate_lo(const World& W, const Uni& u, const RestirAux& ax, float fclamp, f3 x2, f3 n2, Mat mat2, Rng& rng,
+               PixStats& st) {
+  const bool unified = rflag(u, RF_UNIFIED);
   f3 Lo = mk(0, 0, 0), tp = mk(1, 1, 1);
   f3 pos = x2, n = n2;
   Mat mat = mat2;
   const uint32_t nB = u.params0[1];
   f3 sunRad = mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
   for (uint32_t v = 1u; v <= nB; v++) {
-    if (mat.emissive > 0.0f && v > 1u) Lo = add(Lo, muls(mul(tp, mat.albedo), mat.emissive * EMISSIVE_SCALE));
+    if (!unified && mat.emissive > 0.0f && v > 1u)
+      Lo = add(Lo, muls(mul(tp, mat.albedo), mat.emissive * EMISSIVE_SCALE));
     f3 surf = add(pos, muls(n, 1e-3f));
     f3 l = sample_sun_dir(u, rng);
     float ndl = dot3(n, l);
-    if (ndl > 0.0f && l.y > 0.0f && !shadowed(surf, l, 1e4f))
+    if (ndl > 0.0f && l.y > 0.0f && !shadow_ray(W, surf, l, 1e4f, st))
       Lo = add(Lo, mul(muls(muls(mul(tp, mat.albedo), INV_PI), ndl), sunRad));
+    if (unified) Lo = add(Lo, mul(tp, emissive_nee(W, u, ax, pos, n, mat.albedo, emissive_cand_count(u, v), rng, st)));
     if (v == nB) break;
     f3 rd = cosine_hemisphere(n, rng);
     tp = mul(tp, mat.albedo);
@@ -822,21 +985,20 @@ f3 estimate_lo(const World& W, const Uni& u, float fclamp, f3 x2, f3 n2, Mat mat
   return firefly(fclamp, Lo);
 }
 
-// Initial candidates of one pixel (pathtrace.wgsl:248-284, 332-457,
-// RF_UNIFIED off).  Outputs: rgba16f radiance (sky pixels only), fp32 copy,
-// albedo, G-buffer, reservoir A, rgba16f pass-through radiance.
-void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, int gy, int Wd, int Hd,
-                          uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, uint32_t* resA,
+// Initial candidates of one pixel (pathtrace.wgsl:248-284, 332-457).
+// Outputs: rgba16f radiance (sky pixels only), fp32 copy, albedo, G-buffer,
+// reservoir A, rgba16f pass-through radiance.
+void restir_initial_pixel(const World& W, const Uni& u, const RestirAux& ax, float fclamp, int gx, int gy, int Wd,
+                          int Hd, uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, uint32_t* resA,
                           uint16_t* direct16, PixStats& st) {
   const size_t p = (size_t)gy * Wd + gx;
-  auto count = [&](const Hit& h) { st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads; };
   Rng rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0]);
   float jx = rng.next() - 0.5f;
   float jy = rng.next() - 0.5f;
   f3 ro = mk(u.camPos[0], u.camPos[1], u.camPos[2]);
   f3 rd = camera_ray(u, (((float)gx + 0.5f) + jx) / (float)Wd, (((float)gy + 0.5f) + jy) / (float)Hd);
   Hit h0 = trace(W, ro, rd, 1e4f);
-  count(h0);
+  st.rays++; st.outer += h0.outer; st.inner += h0.inner; st.vreads += h0.vreads;
   if (h0.t < 0.0f) {
     f3 sky = sky_color(u, rd, true);
     const float v[4] = {sky.x, sky.y, sky.z, 1.0f};
@@ -860,24 +1022,69 @@ void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, in
   alb8[4 * p + 3] = 255;
   gbuf[4 * p] = n1.x; gbuf[4 * p + 1] = n1.y; gbuf[4 * p + 2] = n1.z; gbuf[4 * p + 3] = h0.t;
 
+  const bool unified = rflag(u, RF_UNIFIED);
   float em = mat1.emissive * EMISSIVE_SCALE;
   f3 direct = mk(em, em, em);
   float wSum = 0.0f, selP = 0.0f;
   RSample sel = null_sample(0.0f);
+  // Candidate: sun cone NEE at x1.
   {
     f3 l = sample_sun_dir(u, rng);
     float ndl = dot3(n1, l);
-    if (ndl > 0.0f && l.y > 0.0f) {
-      Hit hs = trace(W, surf1, l, 1e4f);
-      count(hs);
-      if (!(hs.t >= 0.0f)) direct = add(direct, muls(mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]),
-                                                    INV_PI * ndl));
+    if (ndl > 0.0f && l.y > 0.0f && !shadow_ray(W, surf1, l, 1e4f, st)) {
+      if (unified) {
+        float coneSA = 2.0f * PI * (1.0f - u.sunDir[3]);
+        RSample s = null_sample(0.0f);
+        s.kind = SK_DIR;
+        s.pos = l;
+        float den = fmaxf_(coneSA, 1e-5f);
+        s.rad = mk(u.sunRadiance[0] / den, u.sunRadiance[1] / den, u.sunRadiance[2] / den);
+        float pt = eval_target(s, x1, n1);
+        float w = pt * coneSA;
+        if (w > 0.0f) {
+          wSum += w;
+          if (rng.next() * wSum < w) { sel = s; selP = pt; }
+        }
+      } else {
+        direct = add(direct, muls(mk(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]), INV_PI * ndl));
+      }
     }
   }
+  // Candidate: light-list NEE at x1, RIS over emissiveCandCount(0) faces.
+  if (unified && u.params2[1] > 0u) {
+    uint32_t nCand = emissive_cand_count(u, 0u);
+    float eSum = 0.0f, eSelP = 0.0f;
+    RSample eSel = null_sample(0.0f);
+    for (uint32_t k = 0; k < nCand; k++) {
+      LightPoint lp = sample_light_face(u, ax, W.BG, x1, rng);
+      RSample s = null_sample(0.0f);
+      s.kind = SK_POINT;
+      s.pos = lp.pos;
+      s.n = lp.n;
+      s.rad = lp.Le;
+      float pt = eval_target(s, x1, n1);
+      float w = pt / ((float)nCand * lp.pdfA);
+      if (w > 0.0f) {
+        eSum += w;
+        if (rng.next() * eSum < w) { eSel = s; eSelP = pt; }
+      }
+    }
+    if (eSel.kind != SK_NONE && eSelP > 0.0f) {
+      f3 d = sub(eSel.pos, surf1);
+      float r = length3(d);
+      if (!shadow_ray(W, surf1, mk(d.x / r, d.y / r, d.z / r), r - 2e-3f, st)) {
+        float We = eSum / eSelP;
+        float w = eSelP * We;
+        wSum += w;
+        if (rng.next() * wSum < w) { sel = eSel; selP = eSelP; }
+      }
+    }
+  }
+  // Candidate: BSDF bounce path, reconnection vertex x2 carries Lo.
   if (u.params0[1] > 0u) {
     f3 brd = cosine_hemisphere(n1, rng);
     Hit h = trace(W, surf1, brd, 1e4f);
-    count(h);
+    st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
     RSample s = null_sample(0.0f);
     float Wc;
     if (h.t < 0.0f) {
@@ -888,8 +1095,8 @@ void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, in
     } else {
       f3 x2 = add(surf1, muls(brd, h.t));
       Mat mat2 = unpack_material(h.mat);
-      f3 Lo = estimate_lo(W, u, fclamp, x2, h.n, mat2, rng, st);
-      if (mat2.emissive > 0.0f) Lo = add(Lo, muls(mat2.albedo, mat2.emissive * EMISSIVE_SCALE));
+      f3 Lo = estimate_lo(W, u, ax, fclamp, x2, h.n, mat2, rng, st);
+      if (!unified && mat2.emissive > 0.0f) Lo = add(Lo, muls(mat2.albedo, mat2.emissive * EMISSIVE_SCALE));
       s.kind = SK_POINT;
       s.pos = x2;
       s.n = h.n;
@@ -899,12 +1106,12 @@ void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, in
       f3 dn = normalize3(d);
       float cos1 = fmaxf_(dot3(n1, dn), 1e-4f);
       float cos2 = fmaxf_(dot3(h.n, mk(-dn.x, -dn.y, -dn.z)), 1e-4f);
-      Wc = ((PI / cos1) * r2) / cos2;
+      Wc = PI / cos1 * r2 / cos2;
     }
     float pt = eval_target(s, x1, n1);
     float w = pt * Wc;
     if (w > 0.0f) {
-      wSum = wSum + w;
+      wSum += w;
       if (rng.next() * wSum < w) { sel = s; selP = pt; }
     }
   }
@@ -920,9 +1127,21 @@ void restir_initial_pixel(const World& W, const Uni& u, float fclamp, int gx, in
   for (int c = 0; c < 4; c++) direct16[4 * p + c] = f32_to_f16(dv[c]);
 }
 
-// Temporal reuse of one pixel (reuse_temporal.wgsl:38-46, 140-279 without
-// dupmap / rescue / world cache / mutation).
-void restir_temporal_pixel(const Uni& u, int gx, int gy, int Wd, int Hd, const float* gbufCur,
+// validPrev (reuse_temporal.wgsl:38-46)
+inline bool valid_prev(const Uni& u, int px, int py, int Wd, int Hd, const float* gbufPrev, f3 wp, f3 n1) {
+  if (px < 0 || py < 0 || px >= Wd || py >= Hd) return false;
+  const float* pg = gbufPrev + 4 * ((size_t)py * Wd + px);
+  if (pg[3] <= 0.0f) return false;
+  f3 dv = sub(wp, mk(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]));
+  float expectedT = length3(dv);
+  bool depthOk = std::fabs(pg[3] - expectedT) < 0.08f * expectedT + 0.02f;
+  bool normalOk = dot3(mk(pg[0], pg[1], pg[2]), n1) > 0.9f;
+  return depthOk && normalOk;
+}
+
+// Temporal reuse of one pixel (reuse_temporal.wgsl:140-279 without the world
+// cache and mutation).
+void restir_temporal_pixel(const Uni& u, const RestirAux& ax, int gx, int gy, int Wd, int Hd, const float* gbufCur,
                            const float* gbufPrev, const uint32_t* resB, uint32_t* resA) {
   const size_t p = (size_t)gy * Wd + gx;
   const float* g = gbufCur + 4 * p;
@@ -937,22 +1156,31 @@ void restir_temporal_pixel(const Uni& u, int gx, int gy, int Wd, int Hd, const f
   float ndx = pc[0] / pc[3], ndy = pc[1] / pc[3];
   int ppx = itrunc((ndx * 0.5f + 0.5f) * (float)Wd);
   int ppy = itrunc(((-ndy) * 0.5f + 0.5f) * (float)Hd);
-  if (ppx < 0 || ppy < 0 || ppx >= Wd || ppy >= Hd) return;
-  const float* pg = gbufPrev + 4 * ((size_t)ppy * Wd + ppx);
-  if (pg[3] <= 0.0f) return;
-  f3 dv = sub(x1, mk(u.prevCamPos[0], u.prevCamPos[1], u.prevCamPos[2]));
-  float expectedT = length3(dv);
-  bool depthOk = std::fabs(pg[3] - expectedT) < 0.08f * expectedT + 0.02f;
-  bool normalOk = dot3(mk(pg[0], pg[1], pg[2]), n1) > 0.9f;
-  if (!(depthOk && normalOk)) return;
-  RSample sT = unpack_res(resB + 8 * ((size_t)ppy * Wd + ppx));
-  float cT = fminf_(sT.c, u.params3[0]);
+  bool found = valid_prev(u, ppx, ppy, Wd, Hd, gbufPrev, x1, n1);
+  if (!found && rflag(u, RF_RESCUE)) {
+    for (int dy = -1; dy <= 1 && !found; dy++)
+      for (int dx = -1; dx <= 1 && !found; dx++) {
+        int qx = ppx + dx, qy = ppy + dy;
+        if ((dx != 0 || dy != 0) && valid_prev(u, qx, qy, Wd, Hd, gbufPrev, x1, n1)) {
+          ppx = qx; ppy = qy;
+          found = true;
+        }
+      }
+  }
+  if (!found) return;
+  const size_t prevIdx = (size_t)ppy * Wd + ppx;
+  RSample sT = unpack_res(resB + 8 * prevIdx);
+  float dupScore = 0.0f;
+  if (rflag(u, RF_DUPMAP) || rflag(u, RF_MUTATE)) dupScore = clampf(ax.dup[prevIdx], 0.0f, 1.0f);
+  float cap = u.params3[0];
+  if (rflag(u, RF_DUPMAP)) cap = mixf(u.params3[0], u.params3[1], om_pow(dupScore, u.params3[2]));
+  float cT = fminf_(sT.c, cap);
   RSample sC = unpack_res(resA + 8 * p);
   float cC = fmaxf_(sC.c, 0.0f);
   float pC = eval_target(sC, x1, n1), pT = eval_target(sT, x1, n1);
   float mDen = fmaxf_(cC + cT, 1e-3f);
-  float wC = ((cC / mDen) * pC) * fmaxf_(sC.W, 0.0f);
-  float wT = ((cT / mDen) * pT) * fmaxf_(sT.W, 0.0f);
+  float wC = (cC / mDen) * pC * fmaxf_(sC.W, 0.0f);
+  float wT = (cT / mDen) * pT * fmaxf_(sT.W, 0.0f);
   float wSum = wC + wT;
   if (wSum <= 0.0f) {
     pack_res(null_sample(cC + cT), resA + 8 * p);
@@ -967,11 +1195,49 @@ void restir_temporal_pixel(const Uni& u, int gx, int gy, int Wd, int Hd, const f
   pack_res(sel, resA + 8 * p);
 }
 
-// Spatial reuse + shading of one pixel (reuse_spatial.wgsl:116-126, 128-354:
-// random disk, generic neighbour test, scalar shading weight).
-void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, int Hd, const float* gbufCur,
-                          const uint32_t* resA, const uint16_t* direct16, uint16_t* rad16, float* rad32,
-                          uint32_t* resB, PixStats& st) {
+// pairSize / pairOff / wrapMod / pairedPartner (reuse_spatial.wgsl:65-109)
+inline int pair_size(uint32_t ti) { return ti == 0u ? 254 : (ti == 1u ? 230 : 210); }
+inline uint32_t pair_off(uint32_t ti) { return ti == 0u ? 0u : (ti == 1u ? 64516u : 117416u); }
+inline int wrap_mod(int v, int s) { return ((v % s) + s) % s; }
+
+void paired_partner(const Uni& u, const RestirAux& ax, int px, int py, uint32_t ti, int& qx, int& qy) {
+  int s = pair_size(ti);
+  uint32_t h = pcg_hash(u.params0[0] * 2654435761u + ti * 0x68bc21ebu + 0x9e3779b9u);
+  uint32_t h2 = pcg_hash(h);
+  int offx = (int)(h % (uint32_t)s), offy = (int)(h2 % (uint32_t)s);
+  bool mx = (h & 0x40000000u) != 0u, my = (h & 0x20000000u) != 0u, sw = (h & 0x10000000u) != 0u;
+  int p0 = wrap_mod(px + offx, s), p1 = wrap_mod(py + offy, s);
+  if (sw) std::swap(p0, p1);
+  if (mx) p0 = s - 1 - p0;
+  if (my) p1 = s - 1 - p1;
+  uint32_t word = ax.pairing[pair_off(ti) + (uint32_t)(p1 * s + p0)];
+  int dTx = (int32_t)(word << 16u) >> 16, dTy = (int32_t)word >> 16;
+  int q0 = wrap_mod(p0 + dTx, s), q1 = wrap_mod(p1 + dTy, s);
+  if (mx) q0 = s - 1 - q0;
+  if (my) q1 = s - 1 - q1;
+  if (sw) std::swap(q0, q1);
+  int dx = wrap_mod(q0 - offx - px, s), dy = wrap_mod(q1 - offy - py, s);
+  if (dx > s / 2) dx -= s;
+  if (dy > s / 2) dy -= s;
+  qx = px + dx;
+  qy = py + dy;
+}
+
+// sampleVisible (reuse_spatial.wgsl:117-126)
+bool sample_visible(const World& W, const RSample& s, f3 x1, f3 n1, PixStats& st) {
+  f3 surf = add(x1, muls(n1, 1e-3f));
+  if (s.kind == SK_DIR) return !shadow_ray(W, surf, s.pos, 1e4f, st);
+  f3 d = sub(s.pos, surf);
+  float r = length3(d);
+  if (r < 2e-3f) return true;
+  return !shadow_ray(W, surf, mk(d.x / r, d.y / r, d.z / r), r - 2e-3f, st);
+}
+
+// Spatial reuse + shading of one pixel (reuse_spatial.wgsl:128-354 without
+// the world cache and the quality signal).
+void restir_spatial_pixel(const World& W, const Uni& u, const RestirAux& ax, int gx, int gy, int Wd, int Hd,
+                          const float* gbufCur, const uint32_t* resA, const uint16_t* direct16, uint16_t* rad16,
+                          float* rad32, uint32_t* resB, PixStats& st) {
   const size_t p = (size_t)gy * Wd + gx;
   f3 direct = mk(f16_to_f32(direct16[4 * p]), f16_to_f32(direct16[4 * p + 1]), f16_to_f32(direct16[4 * p + 2]));
   auto out_radiance = [&](f3 v) {
@@ -980,6 +1246,10 @@ void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, 
       rad16[4 * p + c] = f32_to_f16(o[c]);
       if (rad32) rad32[4 * p + c] = o[c];
     }
+  };
+  auto write_history = [&](const RSample& s) {
+    if (rflag(u, RF_HISTISOLATE)) std::memcpy(resB + 8 * p, resA + 8 * p, 32);
+    else pack_res(s, resB + 8 * p);
   };
   const float* g = gbufCur + 4 * p;
   if (g[3] <= 0.0f) {
@@ -990,6 +1260,8 @@ void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, 
   Rng rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
   f3 x1 = surface_at(u, gx, gy, Wd, Hd, g);
   f3 n1 = mk(g[0], g[1], g[2]);
+  float tPrim = g[3];
+  float cosView = fmaxf_(dot3(n1, normalize3(sub(mk(u.camPos[0], u.camPos[1], u.camPos[2]), x1))), 0.0f);
   f3 domX1[4], domN1[4];
   float domC[4];
   RSample cand[4];
@@ -998,14 +1270,23 @@ void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, 
   RSample canonical = unpack_res(resA + 8 * p);
   domX1[0] = x1; domN1[0] = n1; domC[0] = canonical.c;
   if (canonical.kind != SK_NONE) { cand[0] = canonical; candDom[0] = 0u; nCand = 1u; }
-  if (u.params2[0] & RF_SPATIAL) {
-    uint32_t taps = std::min(u.params2[2], 3u);
+  const bool paired = rflag(u, RF_PAIRED), planeExact = rflag(u, RF_PLANE);
+  uint32_t taps = std::min(u.params2[2], 3u);
+  if (rflag(u, RF_SPATIAL)) {
     for (uint32_t ti = 0u; ti < taps; ti++) {
-      float r = u.params4[0] * std::sqrt(rng.next());
-      float a = TWO_PI * rng.next();
-      float sa, ca;
-      om_sincos(a, sa, ca);
-      int qx = gx + itrunc(ca * r), qy = gy + itrunc(sa * r);
+      int qx, qy;
+      if (paired) {
+        uint32_t tex = ti;
+        if (rflag(u, RF_MIXSIGMA)) tex = ti + 1u == taps ? 0u : ti + 1u;
+        paired_partner(u, ax, gx, gy, tex, qx, qy);
+      } else {
+        float r = u.params4[0] * std::sqrt(rng.next());
+        float a = 2.0f * PI * rng.next();
+        float sa, ca;
+        om_sincos(a, sa, ca);
+        qx = gx + itrunc(ca * r);
+        qy = gy + itrunc(sa * r);
+      }
       if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= Wd || qy >= Hd) continue;
       size_t q = (size_t)qy * Wd + qx;
       const float* gq = gbufCur + 4 * q;
@@ -1013,60 +1294,137 @@ void restir_spatial_pixel(const World& W, const Uni& u, int gx, int gy, int Wd, 
       f3 x1q = surface_at(u, qx, qy, Wd, Hd, gq);
       f3 nq = mk(gq[0], gq[1], gq[2]);
       float nDot = dot3(n1, nq);
-      if (!(nDot > 0.9f && std::fabs(gq[3] - g[3]) < 0.1f * g[3] + 0.02f)) continue;
+      bool genericOk = nDot > 0.9f && std::fabs(gq[3] - g[3]) < 0.1f * g[3] + 0.02f;
+      bool samePlane = nDot > 0.99f && std::fabs(dot3(n1, sub(x1q, x1))) < 0.02f;
+      bool ok = planeExact ? (genericOk || samePlane) : genericOk;
+      if (!ok) continue;
       RSample rq = unpack_res(resA + 8 * q);
+      bool reconnectable = rq.kind == SK_NONE || !rflag(u, RF_FOOTPRINT) || footprint_ok(u, rq, x1, n1, tPrim, cosView);
+      if (!reconnectable) continue;
       domX1[nDom] = x1q; domN1[nDom] = nq; domC[nDom] = rq.c;
       if (rq.kind != SK_NONE) { cand[nCand] = rq; candDom[nCand] = nDom; nCand++; }
       nDom++;
     }
   }
   float cTotal = 0.0f;
-  for (uint32_t l = 0u; l < nDom; l++) cTotal = cTotal + domC[l];
+  for (uint32_t l = 0u; l < nDom; l++) cTotal += domC[l];
+  if (nCand == 0u) {
+    out_radiance(direct);
+    write_history(null_sample(fminf_(cTotal, 255.0f)));
+    return;
+  }
+  const bool vector = rflag(u, RF_VECTOR), fullV = rflag(u, RF_FULLV);
   float wSum = 0.0f, selP = 0.0f;
+  f3 contrib = mk(0, 0, 0);
   RSample sel = null_sample(0.0f);
   uint32_t selJ = 0u;
   for (uint32_t j = 0u; j < nCand; j++) {
-    const RSample& s = cand[j];
+    const RSample s = cand[j];
     float denom = 0.0f;
-    for (uint32_t l = 0u; l < nDom; l++) denom = denom + domC[l] * eval_target(s, domX1[l], domN1[l]);
+    for (uint32_t l = 0u; l < nDom; l++) denom += domC[l] * eval_target(s, domX1[l], domN1[l]);
     if (denom <= 0.0f) continue;
     uint32_t dj = candDom[j];
-    float m = (domC[dj] * eval_target(s, domX1[dj], domN1[dj])) / denom;
+    float m = domC[dj] * eval_target(s, domX1[dj], domN1[dj]) / denom;
     float pMe = eval_target(s, x1, n1);
-    float w = (m * pMe) * fmaxf_(s.W, 0.0f);
+    float w = m * pMe * fmaxf_(s.W, 0.0f);
     if (w > 0.0f) {
-      wSum = wSum + w;
+      wSum += w;
       if (rng.next() * wSum < w) { sel = s; selP = pMe; selJ = j; }
     }
+    if (vector && w > 0.0f) {
+      bool vis = true;
+      if (j > 0u || fullV) vis = sample_visible(W, s, x1, n1, st);
+      if (vis) contrib = add(contrib, muls(eval_f(s, x1, n1), m * fmaxf_(s.W, 0.0f)));
+    }
   }
-  if (nCand == 0u || sel.kind == SK_NONE || selP <= 0.0f || wSum <= 0.0f) {
+  if (sel.kind == SK_NONE || selP <= 0.0f || wSum <= 0.0f) {
     out_radiance(direct);
-    pack_res(null_sample(fminf_(cTotal, 255.0f)), resB + 8 * p);
+    write_history(null_sample(fminf_(cTotal, 255.0f)));
     return;
   }
   sel.W = wSum / selP;
   sel.c = fminf_(cTotal, 255.0f);
-  bool vis = true;
-  if (selJ > 0u) {   // sampleVisible (reuse_spatial.wgsl:117-126)
-    f3 surf = add(x1, muls(n1, 1e-3f));
-    Hit h;
-    if (sel.kind == SK_DIR) {
-      h = trace(W, surf, sel.pos, 1e4f);
-      st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
-      vis = !(h.t >= 0.0f);
-    } else {
-      f3 d = sub(sel.pos, surf);
-      float r = length3(d);
-      if (!(r < 2e-3f)) {
-        h = trace(W, surf, mk(d.x / r, d.y / r, d.z / r), r - 2e-3f);
-        st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
-        vis = !(h.t >= 0.0f);
-      }
-    }
+  if (!vector) {
+    bool vis = true;
+    if (selJ > 0u || fullV) vis = sample_visible(W, sel, x1, n1, st);
+    if (vis) contrib = muls(eval_f(sel, x1, n1), sel.W);
   }
-  f3 contrib = vis ? muls(eval_f(sel, x1, n1), sel.W) : mk(0, 0, 0);
+  if (rflag(u, RF_CLAMP)) {
+    float l = rlum(contrib);
+    if (l > u.params4[2]) contrib = muls(contrib, u.params4[2] / l);
+  }
   out_radiance(add(direct, contrib));
-  pack_res(sel, resB + 8 * p);
+  write_history(sel);
+}
+
+// dupmap.wgsl:17-46 for one pixel.
+float dupmap_pixel(int gx, int gy, int Wd, int Hd, const uint32_t* resB) {
+  const uint32_t* mine = resB + 8 * ((size_t)gy * Wd + gx);
+  if (((mine[5] >> 16) & 3u) == SK_NONE) return 0.0f;
+  int count = 0;
+  for (int dy = -4; dy <= 4; dy++)
+    for (int dx = -4; dx <= 4; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      int qx = gx + dx, qy = gy + dy;
+      if (qx < 0 || qy < 0 || qx >= Wd || qy >= Hd) continue;
+      const uint32_t* r = resB + 8 * ((size_t)qy * Wd + qx);
+      if (((r[5] >> 16) & 3u) != SK_NONE && r[7] == mine[7]) count++;
+    }
+  return (float)count / (float)((2 * 4 + 1) * (2 * 4 + 1) - 1);
+}
+
+// ---- pairing.js -------------------------------------------------------------
+// mulberry32 (pairing.js:9-17) on 32-bit integers as JavaScript's imul / >>>.
+struct Mulberry {
+  uint32_t a;
+  double operator()() {
+    a += 0x6d2b79f5u;
+    uint32_t t = (a ^ (a >> 15)) * (1u | a);
+    t = (t + ((t ^ (t >> 7)) * (61u | t))) ^ t;
+    return (double)(t ^ (t >> 14)) / 4294967296.0;
+  }
+};
+
+// makePairingTexture (pairing.js:26-70)
+void pairing_texture(int S, double sigma, uint32_t seed, uint32_t* out) {
+  Mulberry rand{seed};
+  std::vector<int> link((size_t)S * S);
+  for (int y = 0; y < S; y++)
+    for (int x = 0; x < S; x++) link[(size_t)y * S + x] = (x >> 1) + (S >> 1) * y;
+  // shuffleCount (pairing.js:20-24)
+  int n = std::max(1, (int)std::floor((sigma * sigma) / 2 + 1.46 / sigma + 1.76 / (sigma * sigma) +
+                                      0.656 / std::pow(sigma, 3.0) + 0.5));
+  int cell[4];
+  for (int it = 0; it < n; it++) {
+    int o = it & 1;
+    for (int by = 0; by < S; by += 2)
+      for (int bx = 0; bx < S; bx += 2) {
+        int xs[2] = {(bx + o) % S, (bx + o + 1) % S};
+        int ys[2] = {(by + o) % S, (by + o + 1) % S};
+        cell[0] = ys[0] * S + xs[0]; cell[1] = ys[0] * S + xs[1];
+        cell[2] = ys[1] * S + xs[0]; cell[3] = ys[1] * S + xs[1];
+        for (int i = 3; i > 0; i--) {
+          int j = (int)(rand() * (i + 1));
+          std::swap(link[(size_t)cell[i]], link[(size_t)cell[j]]);
+        }
+      }
+  }
+  std::vector<int> first(((size_t)S * S) >> 1, -1);
+  auto wrap = [S](int d) {
+    int w = d % S;
+    if (w > S / 2) w -= S;
+    if (w < -S / 2) w += S;
+    return w;
+  };
+  for (int i = 0; i < S * S; i++) {
+    int l = link[(size_t)i];
+    if (first[(size_t)l] < 0) { first[(size_t)l] = i; continue; }
+    int a = first[(size_t)l], b = i;
+    int dx = wrap((b % S) - (a % S));
+    int dy = wrap(b / S - a / S);
+    out[a] = ((uint32_t)(dy & 0xffff) << 16) | (uint32_t)(dx & 0xffff);
+    out[b] = ((uint32_t)(-dy & 0xffff) << 16) | (uint32_t)(-dx & 0xffff);
+  }
 }
 
 }  // namespace
@@ -1639,20 +1997,24 @@ long orc_collect_rays(const uint32_t* vox, const uint32_t* bricks, const uint32_
   return total;
 }
 
-// ReSTIR `gi` passes over whole images (reservoirs: 8 u32 per pixel in the
-// 32-byte record of restir.wgsl:14-27).  stats (optional) receives the rays
-// the pass traced.
+// ReSTIR passes over whole images (reservoirs: 8 u32 per pixel in the 32-byte
+// record of restir.wgsl:14-27).  lights / alias / grid: the scene's light
+// data (orc_light_*), read with RF_UNIFIED; dup: the previous frame's
+// duplication map (RF_DUPMAP); pairing: the pairing buffer (RF_PAIRED).  stats
+// (optional) receives the rays the pass traced.
 void orc_restir_initial(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
-                        const void* uniforms, float fclamp, int Wd, int Hd, uint16_t* rad16, float* rad32,
-                        uint8_t* alb8, float* gbuf, uint32_t* resA, uint16_t* direct16, OrcStats* stats) {
+                        const void* uniforms, float fclamp, int Wd, int Hd, const uint32_t* lights,
+                        const float* alias, const uint32_t* grid, uint16_t* rad16, float* rad32, uint8_t* alb8,
+                        float* gbuf, uint32_t* resA, uint16_t* direct16, OrcStats* stats) {
   World W{vox, bricks, masks, N, N / BRICK};
   Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  RestirAux ax{lights, alias, grid, nullptr, nullptr};
   uint64_t rays = 0, outer = 0, inner = 0, vreads = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads)
   for (int y = 0; y < Hd; y++) {
     PixStats st{0, 0, 0, 0};
     for (int x = 0; x < Wd; x++)
-      restir_initial_pixel(W, u, fclamp, x, y, Wd, Hd, rad16, rad32, alb8, gbuf, resA, direct16, st);
+      restir_initial_pixel(W, u, ax, fclamp, x, y, Wd, Hd, rad16, rad32, alb8, gbuf, resA, direct16, st);
     rays += st.rays; outer += st.outer; inner += st.inner; vreads += st.vreads;
   }
   if (stats) {
@@ -1662,30 +2024,49 @@ void orc_restir_initial(const uint32_t* vox, const uint32_t* bricks, const uint3
 }
 
 void orc_restir_temporal(const void* uniforms, int Wd, int Hd, const float* gbufCur, const float* gbufPrev,
-                         const uint32_t* resB, uint32_t* resA) {
+                         const uint32_t* resB, const float* dup, uint32_t* resA) {
   Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
-  if (!(u.params2[0] & 1u) || !(u.params2[0] & 2u)) return;   // reuse_temporal.wgsl:144
+  if (!(u.params2[0] & 1u) || !(u.params2[0] & RF_TEMPORAL)) return;   // reuse_temporal.wgsl:144
+  RestirAux ax{nullptr, nullptr, nullptr, nullptr, dup};
 #pragma omp parallel for schedule(dynamic, 4)
   for (int y = 0; y < Hd; y++)
-    for (int x = 0; x < Wd; x++) restir_temporal_pixel(u, x, y, Wd, Hd, gbufCur, gbufPrev, resB, resA);
+    for (int x = 0; x < Wd; x++) restir_temporal_pixel(u, ax, x, y, Wd, Hd, gbufCur, gbufPrev, resB, resA);
 }
 
 void orc_restir_spatial(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
                         const void* uniforms, int Wd, int Hd, const float* gbufCur, const uint32_t* resA,
-                        const uint16_t* direct16, uint16_t* rad16, float* rad32, uint32_t* resB, OrcStats* stats) {
+                        const uint16_t* direct16, const uint32_t* pairing, uint16_t* rad16, float* rad32,
+                        uint32_t* resB, OrcStats* stats) {
   World W{vox, bricks, masks, N, N / BRICK};
   Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
+  RestirAux ax{nullptr, nullptr, nullptr, pairing, nullptr};
   uint64_t rays = 0, outer = 0, inner = 0, vreads = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads)
   for (int y = 0; y < Hd; y++) {
     PixStats st{0, 0, 0, 0};
     for (int x = 0; x < Wd; x++)
-      restir_spatial_pixel(W, u, x, y, Wd, Hd, gbufCur, resA, direct16, rad16, rad32, resB, st);
+      restir_spatial_pixel(W, u, ax, x, y, Wd, Hd, gbufCur, resA, direct16, rad16, rad32, resB, st);
     rays += st.rays; outer += st.outer; inner += st.inner; vreads += st.vreads;
   }
   if (stats) {
     stats->rays = rays; stats->outer = outer; stats->inner = inner; stats->vreads = vreads;
     stats->pixels = 0;
+  }
+}
+
+void orc_restir_dupmap(int Wd, int Hd, const uint32_t* resB, float* dup) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < Hd; y++)
+    for (int x = 0; x < Wd; x++) dup[(size_t)y * Wd + x] = dupmap_pixel(x, y, Wd, Hd, resB);
+}
+
+// makePairingBuffer (pairing.js:80-89) for sigmas[3].
+void orc_pairing_buffer(const double* sigmas, uint32_t* out) {
+  const int sizes[3] = {254, 230, 210};
+  size_t off = 0;
+  for (int i = 0; i < 3; i++) {
+    pairing_texture(sizes[i], sigmas[i], 0xc0ffeeu + (uint32_t)i * 7919u, out + off);
+    off += (size_t)sizes[i] * sizes[i];
   }
 }
 

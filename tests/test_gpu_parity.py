@@ -319,7 +319,7 @@ def test_invalid_calls_fail_on_host(ctx, vrt):
     with pytest.raises(vrt.VrtError):
         s.frame(u)                            # size mismatch
     u = vrt.make_uniforms(spawn, None, vrt.Lighting(), 0, 2, 3, 64, 36)
-    u.params2[0] = 1 | 128                    # RF_UNIFIED: not implemented
+    u.params2[0] = 1 | 32768                  # RF_CONFDENOISE: not implemented
     with pytest.raises(vrt.VrtError):
         s.frame(u)
     u.params2[0] = 2                          # RF_TEMPORAL without RF_RESTIR

@@ -108,3 +108,48 @@ def test_plain_preset_unchanged(vrt, orc):
 @pytest.mark.parametrize("preset,flags", [("base", 0), ("gi", 7)])
 def test_preset_flags(vrt, preset, flags):
     assert vrt.api.preset_flags(preset) == flags
+
+
+@pytest.mark.parametrize("sigmas", [(16.0, 16.0, 16.0), (48.0, 16.0, 16.0), (0.8, 3.0, 100.0)])
+def test_pairing_textures(vrt, orc, sigmas):
+    """The library's pairing buffer equals the oracle's restatement of
+    pairing.js; partners are mutual and spread with about the target sigma."""
+    a = vrt.api.make_pairing(sigmas)
+    b = orc.pairing_buffer(sigmas)
+    assert np.array_equal(a, b)
+    off = 0
+    for S, sg in zip((254, 230, 210), sigmas):
+        tex = a[off:off + S * S].reshape(S, S)
+        off += S * S
+        dx = (tex & 0xFFFF).astype(np.uint16).view(np.int16).astype(np.int64)
+        dy = (tex >> 16).astype(np.uint16).view(np.int16).astype(np.int64)
+        ys, xs = np.mgrid[0:S, 0:S]
+        px, py = (xs + dx) % S, (ys + dy) % S
+        assert np.array_equal((px + dx[py, px]) % S, xs) and np.array_equal((py + dy[py, px]) % S, ys)
+        assert not ((dx == 0) & (dy == 0)).any()
+        if 2.0 <= sg <= 20.0:
+            assert abs(dx.std() / sg - 1.0) < 0.1
+
+
+def test_ours_chain_invariants(vrt, orc):
+    """The `ours` preset through the oracle: unified NEE produces light-face
+    samples, the duplication map stays in [0, 1], confidence stays capped."""
+    W, H = 64, 36
+    vox, spawn = vrt.generate_scene(0, 128, 1337)
+    b, m = orc.build_bricks(vox, 128)
+    words, weights = orc.light_list(vox, 128)
+    lights = {"words": words, "alias": orc.light_alias(weights), "grid": orc.light_grid(128, words, weights)}
+    pairing = orc.pairing_buffer([16.0, 16.0, 16.0])
+    acc = np.zeros((H, W, 4), np.uint16)
+    g = np.zeros((H, W, 4), np.float32)
+    rb = np.zeros((H, W, 8), np.uint32)
+    dup = np.zeros((H, W), np.float32)
+    for f in range(4):
+        u = vrt.make_uniforms(spawn, spawn if f else None, vrt.Lighting(), f, 2, 3, W, H, preset="ours",
+                              light_count=len(words))
+        r = orc.frame(vox, b, m, 128, vrt.uniforms_bytes(u), 10.0, W, H, acc, g, False, rb, dup, lights, pairing)
+        acc, g, rb, dup = r["accum"], r["gbuf"], r["resB"], r["dup"]
+        assert (dup >= 0).all() and (dup <= 1).all()
+        assert np.isfinite(_f16(r["rad16"])).all()
+    assert (_kind(rb) == 1).any() and (_kind(rb) == 2).any()
+    assert dup.max() > 0

@@ -43,7 +43,7 @@ def _eq(a, b, what):
 
 def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=2, fclamp=10.0, preset="gi",
                 move=True, taps=3, ccap=20.0, radius=30.0, pose=None, restir_flags=None, check_stages=True,
-                kernel="wavefront"):
+                kernel="wavefront", extra_flags=0, sigma=16.0, tweak=None):
     """Renders `frames` frames pass by pass on the device and with the oracle;
     asserts every stage of every frame.  Returns the device stats of the
     last frame and the oracle's last frame."""
@@ -53,21 +53,37 @@ def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=
     sc = vrt.Scene(ctx, vox, n)
     s = vrt.Session(ctx, sc, W, H, firefly_clamp=fclamp, keep_radiance_f32=True, path_kernel=kernel)
     s.set_timing(True)
+    if sigma != 16.0:
+        s.set_pairing_sigma(sigma)
     light = vrt.Lighting()
     acc_prev = np.zeros((H, W, 4), np.uint16)
     gprev = np.zeros((H, W, 4), np.float32)
     res_b = np.zeros((H, W, 8), np.uint32)
+    dup = np.zeros((H, W), np.float32)
+    lights, nlights = None, 0
+    rf0 = (vrt.api.preset_flags(preset) if restir_flags is None else restir_flags) | extra_flags
+    if rf0 & 128:
+        sc.build_lights()
+        words, alias, grid = sc.lights()
+        lights = {"words": words, "alias": alias, "grid": grid}
+        nlights = len(words)
     prev = None
     st = ref = None
     tot = {"rays": 0, "outer": 0, "inner": 0, "vreads": 0}
     for f in range(frames):
         p = vrt.camera_spline(spawn, f) if move else spawn
         u = vrt.make_uniforms(p, prev, light, f, bounces, flags, W, H, preset=preset, taps=taps, ccap=ccap,
-                              radius=radius)
-        if restir_flags is not None:
-            u.params2[0] = restir_flags
+                              radius=radius, light_count=nlights)
+        u.params2[0] = rf0
+        if tweak:
+            tweak(u)
         rf = int(u.params2[0])
-        ref = orc.frame(vox, b, m, n, vrt.uniforms_bytes(u), fclamp, W, H, acc_prev, gprev, False, res_b)
+        pairing = None
+        if rf & 8:
+            wide = max(0.8, float(np.float32(u.params5[0]))) if rf & 8192 else max(0.8, sigma)
+            pairing = orc.pairing_buffer([wide, max(0.8, sigma), max(0.8, sigma)])
+        ref = orc.frame(vox, b, m, n, vrt.uniforms_bytes(u), fclamp, W, H, acc_prev, gprev, False, res_b, dup,
+                        lights, pairing)
         s.pathtrace(u)
         if check_stages:
             _eq(s.reservoirs(0), ref["resA0"], f"frame {f} reservoirs A (initial)")
@@ -77,6 +93,9 @@ def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=
         if check_stages:
             _eq(s.reservoirs(0), ref["resA"], f"frame {f} reservoirs A (temporal reuse)")
         s.reuse_spatial(u)
+        s.dupmap(u)
+        if rf & 16:
+            _eq(s.dupmap_image().view(np.uint32), ref["dup"].view(np.uint32), f"frame {f} dupmap")
         s.temporal(u)
         if flags & 2:
             for it in range(3):
@@ -99,7 +118,7 @@ def _run_restir(ctx, vrt, orc, kind, n, seed, W, H, frames, *, flags=3, bounces=
         assert st.rays == tot["rays"], f"frame {f} rays"
         assert st.dda_outer == tot["outer"] and st.dda_inner == tot["inner"] and st.voxel_reads == tot["vreads"]
         assert st.pixels == W * H * (f + 1)
-        acc_prev, gprev, res_b, prev = ref["accum"], ref["gbuf"], ref["resB"], p
+        acc_prev, gprev, res_b, dup, prev = ref["accum"], ref["gbuf"], ref["resB"], ref["dup"], p
     s.close(); sc.close()
     return st, ref
 
@@ -160,6 +179,38 @@ def test_restir_full_size(ctx, vrt, orc, kernel):
     _run_restir(ctx, vrt, orc, 2, 256, 2, 1920, 1080, 2, kernel=kernel)
 
 
+@pytest.mark.parametrize("preset", ["lin", "ours", "ours_motion"])
+def test_restir_reference_presets(ctx, vrt, orc, preset):
+    """The reference's presets (main.js:40-62) on a moving camera."""
+    _, ref = _run_restir(ctx, vrt, orc, 0, 128, 1337, 160, 90, 4, preset=preset)
+    assert (_kinds(ref["resB"]) == 1).any()
+
+
+@pytest.mark.parametrize("extra", [8, 8 | 8192, 16, 64, 64 | 1024, 1024, 128, 128 | 4096, 128 | 65536,
+                                   128 | 16384, 256, 512, 32, 2048, 262144, 8 | 16 | 256 | 512 | 2048])
+def test_restir_flags(ctx, vrt, orc, extra):
+    """Each flag (and a few combinations) on top of `gi`, every stage against
+    the oracle: paired (8), mixsigma (8192), dupmap (16), vector (64), fullv
+    (1024), unified (128) with lightpower (4096) / lightgrid (65536) /
+    adaptcand (16384), plane (256), rescue (512), footprint (32), rclamp
+    (2048), histisolate (262144)."""
+    _run_restir(ctx, vrt, orc, 1, 64, 1, 128, 72, 4, extra_flags=extra)
+
+
+def test_restir_ours_bounces_and_sizes(ctx, vrt, orc):
+    """`ours` with 6 bounces (the reference's published configuration), an
+    odd size and the megakernel, and a second pairing sigma."""
+    _run_restir(ctx, vrt, orc, 0, 128, 1337, 97, 61, 3, preset="ours", bounces=6)
+    _run_restir(ctx, vrt, orc, 3, 128, 4, 128, 72, 3, preset="ours", kernel="megakernel", sigma=6.0)
+    _run_restir(ctx, vrt, orc, 1, 64, 1, 128, 72, 3, preset="gi", extra_flags=8 | 8192,
+                tweak=lambda u: u.params5.__setitem__(0, 24.0))
+
+
+def test_restir_ours_full_size(ctx, vrt, orc):
+    """`ours` at 1920x1080 on the 256^3 world, two frames."""
+    _run_restir(ctx, vrt, orc, 2, 256, 2, 1920, 1080, 2, preset="ours", bounces=6)
+
+
 def test_restir_frame_equals_passes(ctx, vrt):
     """vrt_frame runs exactly the pass sequence of main.js:736-749."""
     W, H, n = 128, 72, 64
@@ -206,9 +257,10 @@ def test_restir_reset_and_invalid_calls(ctx, vrt):
     with pytest.raises(vrt.VrtError):
         s.reservoirs(2)
     bad = vrt.make_uniforms(spawn, None, vrt.Lighting(), 0, 2, 3, W, H, preset="gi")
-    bad.params2[0] = 7 | 8                    # RF_PAIRED: not implemented
-    with pytest.raises(vrt.VrtError):
-        s.frame(bad)
+    for unbuilt in (32768, 131072, 524288):   # confdenoise, mutate, worldgi: not implemented
+        bad.params2[0] = 7 | unbuilt
+        with pytest.raises(vrt.VrtError):
+            s.frame(bad)
     s.close()
     bs = vrt.Session(ctx, sc, W, H, path_kernel="batch_only")
     batch = vrt.Batch(ctx, [bs])

@@ -144,6 +144,9 @@ SIGNATURES = {
     "vrt_pass_pathtrace": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_reuse_temporal": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_reuse_spatial": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_pass_dupmap": (I, [P, C.POINTER(VrtUniforms)]),
+    "vrt_session_set_pairing_sigma": (I, [P, C.c_float]),
+    "vrt_make_pairing": (I, [P, P, SZ]),
     "vrt_pass_temporal": (I, [P, C.POINTER(VrtUniforms)]),
     "vrt_pass_atrous": (I, [P, C.POINTER(VrtUniforms), I]),
     "vrt_pass_present": (I, [P, C.POINTER(VrtUniforms)]),
@@ -163,6 +166,7 @@ SIGNATURES = {
     "vrt_read_ldr": (I, [P, P, SZ]),
     "vrt_read_reservoirs": (I, [P, I, P, SZ]),
     "vrt_read_direct": (I, [P, P, SZ]),
+    "vrt_read_dupmap": (I, [P, P, SZ]),
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),

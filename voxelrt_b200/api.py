@@ -116,7 +116,23 @@ RF = {"restir": 1, "treuse": 2, "sreuse": 4, "paired": 8, "dupmap": 16, "footpri
       "unified": 128, "plane": 256, "rescue": 512, "fullv": 1024, "rclamp": 2048, "lightpower": 4096,
       "mixsigma": 8192, "adaptcand": 16384, "confdenoise": 32768, "lightgrid": 65536, "mutate": 131072,
       "histisolate": 262144, "worldgi": 524288}
-PRESETS = {"base": [], "gi": ["restir", "treuse", "sreuse"]}
+PRESETS = {
+    "base": [],
+    "gi": ["restir", "treuse", "sreuse"],
+    "lin": ["restir", "treuse", "sreuse", "paired", "dupmap", "vector", "unified"],
+    "ours": ["restir", "treuse", "sreuse", "paired", "dupmap", "vector", "unified", "plane", "rescue", "fullv",
+             "rclamp", "lightpower"],
+    "ours_motion": ["restir", "treuse", "sreuse", "paired", "dupmap", "vector", "unified", "plane", "rescue", "fullv",
+                    "rclamp", "lightpower", "histisolate"],
+}
+
+
+def make_pairing(sigmas) -> np.ndarray:
+    """The pairing textures of paired spatial reuse (pairing.js:80-89)."""
+    sg = np.ascontiguousarray(sigmas, np.float64)
+    out = np.zeros(254 * 254 + 230 * 230 + 210 * 210, np.uint32)
+    check(lib.vrt_make_pairing(ptr(sg), ptr(out), out.size))
+    return out
 
 
 def preset_flags(preset: str) -> int:
@@ -128,15 +144,18 @@ def preset_flags(preset: str) -> int:
 
 def make_uniforms(cur: CameraPose, prev: CameraPose | None, light: Lighting, frame: int, bounces: int, flags: int,
                   width: int, height: int, exposure: float = 1.0, max_history: float = 64.0, preset: str = "base",
-                  taps: int = 3, ccap: float = 20.0, radius: float = 30.0) -> VrtUniforms:
+                  taps: int = 3, ccap: float = 20.0, radius: float = 30.0, light_count: int = 0) -> VrtUniforms:
     """The 304-byte uniform block (main.js:399-426).  preset selects the
     reservoir flags of params2.x; taps, ccap and radius are the reference's
-    tuning defaults (main.js:72-76) in params2.z, params3.x, params4.x."""
+    tuning defaults (main.js:72-76) in params2.z, params3.x, params4.x;
+    light_count is the scene's emissive-face count (params2.y, read by
+    unified NEE)."""
     u = VrtUniforms()
     check(lib.vrt_make_uniforms(C.byref(cur.c()), C.byref(prev.c()) if prev is not None else None,
                                 C.byref(light.c()), int(frame) & 0xFFFFFFFF, int(bounces), int(flags), int(width),
                                 int(height), float(exposure), float(max_history), C.byref(u)))
     u.params2[0] = preset_flags(preset)
+    u.params2[1] = int(light_count)
     u.params2[2] = int(taps)
     u.params3[0] = float(ccap)
     u.params4[0] = float(radius)
@@ -278,6 +297,8 @@ class Session:
     def pathtrace(self, u): check(lib.vrt_pass_pathtrace(self.h, C.byref(u)))
     def reuse_temporal(self, u): check(lib.vrt_pass_reuse_temporal(self.h, C.byref(u)))
     def reuse_spatial(self, u): check(lib.vrt_pass_reuse_spatial(self.h, C.byref(u)))
+    def dupmap(self, u): check(lib.vrt_pass_dupmap(self.h, C.byref(u)))
+    def set_pairing_sigma(self, sigma: float): check(lib.vrt_session_set_pairing_sigma(self.h, float(sigma)))
     def temporal(self, u): check(lib.vrt_pass_temporal(self.h, C.byref(u)))
     def atrous(self, u, it): check(lib.vrt_pass_atrous(self.h, C.byref(u), int(it)))
     def present(self, u): check(lib.vrt_pass_present(self.h, C.byref(u)))
@@ -404,6 +425,7 @@ class Session:
     def denoise(self, i): return self._read(lib.vrt_read_denoise, np.uint16, 4, int(i))
     def reservoirs(self, which: int): return self._read(lib.vrt_read_reservoirs, np.uint32, 8, int(which))
     def direct(self): return self._read(lib.vrt_read_direct, np.uint16, 4)
+    def dupmap_image(self): return self._read(lib.vrt_read_dupmap, np.float32, 1)[..., 0]
 
     def accum(self):
         return self._read(lib.vrt_read_accum, np.float32 if self.accum_f32 else np.uint16, 4)

@@ -167,7 +167,17 @@ struct RestirDev {
   float4* gbuf;             // current G-buffer (n, t)
   const float4* gprev;      // previous frame's G-buffer
   unsigned long long* stats;
+  float* dup;               // duplication score (dupmap.wgsl), read at the reprojected pixel
+  const uint32_t* pairing;  // pairing textures (RF_PAIRED)
+  const uint2* lights;      // emissive faces: x|y<<9|z<<18|face<<27, material (RF_UNIFIED)
+  const float4* lightAlias; // acceptance, alias index, selection pdf, 0
+  const uint32_t* lightGrid;// 34 words per brick cell (RF_LIGHTGRID)
 };
+
+VRT_DI bool rflag(const Uni& u, uint32_t f) { return (u.params2[0] & f) != 0u; }
+
+// WGSL f32 -> u32 conversion: toward zero, saturating, NaN -> 0.
+VRT_DI uint32_t utrunc_(float x) { return __float2uint_rz(x); }
 
 VRT_DI bool occluded(const RestirDev& R, const uint32_t* occ, F3 o, F3 d, float maxT, DCount& cnt) {
   return trace<true>(R.S, occ, o, d, maxT, cnt).t >= 0.0f;
@@ -177,10 +187,156 @@ VRT_DI F3 fclamp3(const RestirDev& R, F3 v) {
   return R.fclamp <= 0.0f ? v : min3(v, f3(R.fclamp, R.fclamp, R.fclamp));
 }
 
-// estimateLo (pathtrace.wgsl:205-246) with unification off: emission rides
-// on hits, sun-cone NEE at every vertex, Russian roulette from vertex 2.
+// ---------------------------------------------------------------------------
+// emissive-face sampling for unified NEE (pathtrace.wgsl:37-199)
+// ---------------------------------------------------------------------------
+constexpr uint32_t kLgK = 16u, kLgStride = 2u + 2u * kLgK;
+constexpr float kLgPCell = 0.75f;
+
+struct LightPoint {
+  F3 pos, n, Le;
+  float pdfA;
+};
+
+// sampleGlobalLightIndex / globalLightPdf (pathtrace.wgsl:49-65)
+VRT_DI uint32_t global_light_index(const RestirDev& R, uint32_t& rng) {
+  const uint32_t count = R.u.params2[1];
+  if (rflag(R.u, kRfLightPower)) {
+    const float uLight = rand_(rng) * (float)count;
+    const uint32_t base = min(utrunc_(uLight), count - 1u);
+    const float frac = uLight - (float)base;
+    const float4 rec = R.lightAlias[base];
+    const uint32_t aliasLi = min(utrunc_(rec.y + 0.5f), count - 1u);
+    return frac >= rec.x ? aliasLi : base;
+  }
+  return min(utrunc_(rand_(rng) * (float)count), count - 1u);
+}
+VRT_DI float global_light_pdf(const RestirDev& R, uint32_t li) {
+  if (rflag(R.u, kRfLightPower)) return fmax_(R.lightAlias[li].z, 1e-8f);
+  return 1.0f / (float)R.u.params2[1];
+}
+
+// pickLightIndex (pathtrace.wgsl:80-121): global distribution, or with
+// RF_LIGHTGRID the 0.75 / 0.25 mixture of the receiver cell's top-K table and
+// the global distribution, with its exact mixture pdf.
+VRT_DI uint32_t pick_light(const RestirDev& R, F3 pos, uint32_t& rng, float& pdf) {
+  if (!rflag(R.u, kRfLightGrid)) {
+    const uint32_t li = global_light_index(R, rng);
+    pdf = global_light_pdf(R, li);
+    return li;
+  }
+  const int BG = R.S.BG;
+  const float sc = kInvVoxel / (float)kBrick;
+  const int bx = iclamp_(ifloor_(pos.x * sc), 0, BG - 1), by = iclamp_(ifloor_(pos.y * sc), 0, BG - 1),
+            bz = iclamp_(ifloor_(pos.z * sc), 0, BG - 1);
+  const uint32_t base = (uint32_t)(bx + by * BG + bz * BG * BG) * kLgStride;
+  const uint32_t n = min(R.lightGrid[base], kLgK);
+  const float wSum = __uint_as_float(R.lightGrid[base + 1u]);
+  if (n == 0u || wSum <= 0.0f) {
+    const uint32_t li = global_light_index(R, rng);
+    pdf = global_light_pdf(R, li);
+    return li;
+  }
+  uint32_t li;
+  if (rand_(rng) < kLgPCell) {   // by cumulative weight over the cell's entries
+    float r = rand_(rng) * wSum;
+    li = R.lightGrid[base + 2u];
+    for (uint32_t k = 0u; k < n; k++) {
+      li = R.lightGrid[base + 2u + 2u * k];
+      r = r - __uint_as_float(R.lightGrid[base + 3u + 2u * k]);
+      if (r <= 0.0f) break;
+    }
+  } else {
+    li = global_light_index(R, rng);
+  }
+  float pCell = 0.0f;
+  for (uint32_t k = 0u; k < n; k++) {
+    if (R.lightGrid[base + 2u + 2u * k] == li) {
+      pCell = __uint_as_float(R.lightGrid[base + 3u + 2u * k]) / wSum;
+      break;
+    }
+  }
+  pdf = kLgPCell * pCell + (1.0f - kLgPCell) * global_light_pdf(R, li);
+  return li;
+}
+
+// sampleLightFace (pathtrace.wgsl:123-144): a uniform point on the face.
+VRT_DI LightPoint sample_light_face(const RestirDev& R, F3 shadePos, uint32_t& rng) {
+  float pdfSelect;
+  const uint32_t li = pick_light(R, shadePos, rng, pdfSelect);
+  const uint2 l = R.lights[li];
+  const F3 v = f3((float)(l.x & 0x1ffu), (float)((l.x >> 9) & 0x1ffu), (float)((l.x >> 18) & 0x1ffu));
+  const uint32_t face = (l.x >> 27) & 7u, axis = face >> 1;
+  const float side = (face & 1u) == 0u ? 1.0f : 0.0f;   // +side faces sit at v+1
+  const float j0 = rand_(rng);
+  const float j1 = rand_(rng);
+  const float j2 = rand_(rng);
+  F3 q = v + f3(j0, j1, j2);
+  F3 n = f3(0.0f, 0.0f, 0.0f);
+  const float sg = side > 0.5f ? 1.0f : -1.0f;
+  if (axis == 0u) { q.x = v.x + side; n.x = sg; }
+  else if (axis == 1u) { q.y = v.y + side; n.y = sg; }
+  else { q.z = v.z + side; n.z = sg; }
+  const Mat mat = unpack_material(l.y);
+  LightPoint lp;
+  lp.pos = q * kVoxelSize;
+  lp.n = n;
+  lp.Le = mat.albedo * (mat.emissive * kEmissiveScale);
+  lp.pdfA = pdfSelect / (kVoxelSize * kVoxelSize);
+  return lp;
+}
+
+// emissiveCandCount (pathtrace.wgsl:155-159)
+VRT_DI uint32_t emissive_cand_count(const Uni& u, uint32_t bounce) {
+  if (!rflag(u, kRfAdaptCand)) return bounce == 0u ? 4u : 1u;
+  const float n0 =
+      clamp_(rintf((u.params5[1] * 4.0f) * (1.0f + log2_(1.0f + (float)u.params2[1] / 256.0f))), 1.0f, 16.0f);
+  return max(utrunc_(n0) >> min(bounce, 31u), 1u);
+}
+
+// emissiveNEE (pathtrace.wgsl:167-199): RIS over nCand light-face samples,
+// one shadow ray on the survivor; the first valid candidate is taken
+// without a draw.
+VRT_DI F3 emissive_nee(const RestirDev& R, const uint32_t* occ, F3 pos, F3 n, F3 albedo, uint32_t nCand,
+                       uint32_t& rng, DCount& cnt) {
+  if (R.u.params2[1] == 0u) return f3(0.0f, 0.0f, 0.0f);
+  const F3 surf = pos + n * 1e-3f;
+  const float invM = 1.0f / (float)nCand;
+  float wSum = 0.0f, selLum = 0.0f, selR2 = 0.0f;
+  F3 sel = f3(0.0f, 0.0f, 0.0f), selDir = sel;
+  for (uint32_t k = 0u; k < nCand; k++) {
+    const LightPoint lp = sample_light_face(R, pos, rng);
+    const F3 d = lp.pos - surf;
+    const float r2 = fmax_(dot3(d, d), 1e-6f);
+    const F3 dir = d * (1.0f / __fsqrt_rn(r2));
+    const float cos1 = dot3(n, dir);
+    const float cos2 = dot3(lp.n, f3(-dir.x, -dir.y, -dir.z));
+    if (cos1 <= 0.0f || cos2 <= 0.0f) continue;
+    const F3 a = ((albedo * kInvPi) * cos1) * cos2;
+    const F3 v = f3((a.x / r2) * lp.Le.x / lp.pdfA, (a.y / r2) * lp.Le.y / lp.pdfA, (a.z / r2) * lp.Le.z / lp.pdfA);
+    const float w = rlum(v) * invM;
+    if (w <= 0.0f) continue;
+    const bool first = wSum == 0.0f;
+    wSum = wSum + w;
+    if (first || rand_(rng) * wSum < w) {
+      sel = v;
+      selLum = rlum(v);
+      selDir = dir;
+      selR2 = r2;
+    }
+  }
+  if (wSum <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
+  const float r = __fsqrt_rn(selR2);
+  if (occluded(R, occ, surf, selDir, r - 2e-3f, cnt)) return f3(0.0f, 0.0f, 0.0f);
+  return sel * (wSum / selLum);
+}
+
+// estimateLo (pathtrace.wgsl:205-246): sun-cone NEE at every vertex,
+// Russian roulette from vertex 2; emission rides on hits (unification off)
+// or comes from light-list NEE at every vertex (RF_UNIFIED).
 VRT_DI F3 estimate_lo(const RestirDev& R, const uint32_t* occ, F3 x2, F3 n2, Mat mat2, uint32_t& rng,
                       DCount& cnt) {
+  const bool unified = rflag(R.u, kRfUnified);
   const Uni& u = R.u;
   F3 Lo = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
   F3 pos = x2, n = n2;
@@ -188,12 +344,13 @@ VRT_DI F3 estimate_lo(const RestirDev& R, const uint32_t* occ, F3 x2, F3 n2, Mat
   const uint32_t nB = u.params0[1];
   const F3 sunRad = f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
   for (uint32_t v = 1u; v <= nB; v++) {
-    if (mat.emissive > 0.0f && v > 1u) Lo = Lo + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
+    if (!unified && mat.emissive > 0.0f && v > 1u) Lo = Lo + (tp * mat.albedo) * (mat.emissive * kEmissiveScale);
     const F3 surf = pos + n * 1e-3f;
     const F3 l = sample_sun_dir(u, rng);
     const float ndl = dot3(n, l);
     if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf, l, 1e4f, cnt))
       Lo = Lo + (((tp * mat.albedo) * kInvPi) * ndl) * sunRad;
+    if (unified) Lo = Lo + tp * emissive_nee(R, occ, pos, n, mat.albedo, emissive_cand_count(u, v), rng, cnt);
     if (v == nB) break;
     const F3 rd = cosine_hemisphere(n, rng);
     tp = tp * mat.albedo;
@@ -242,28 +399,40 @@ VRT_DI void cand_point(F3 x1, F3 n1, F3 x2, F3 n2, F3 Lo, RSample& s, float& Wc)
   Wc = ((kPi / cos1) * r2) / cos2;
 }
 
-// Initial RIS over the (at most one) candidate and the reservoir record of
-// pixel p (pathtrace.wgsl:434-455).
-VRT_DI void store_initial(uint4* resA, size_t p, const Uni& u, int W, int H, bool has, const RSample& s, float Wc,
-                          F3 x1, F3 n1, uint32_t& rng) {
+// Streaming RIS of the initial candidates (pathtrace.wgsl:340-440).
+struct Ris {
   float wSum = 0.0f, selP = 0.0f;
-  RSample sel = null_sample(0.0f);
-  if (has) {
-    const float pt = eval_target(s, x1, n1);
-    const float w = pt * Wc;
+  RSample sel;
+  VRT_DI void add(const RSample& s, float p, float w, uint32_t& rng) {
     if (w > 0.0f) {
       wSum = wSum + w;
-      if (rand_(rng) * wSum < w) { sel = s; selP = pt; }
+      if (rand_(rng) * wSum < w) { sel = s; selP = p; }
     }
   }
+};
+
+// The reservoir record of pixel p after the initial RIS (pathtrace.wgsl:442-455).
+VRT_DI void store_ris(uint4* resA, size_t p, const Uni& u, int W, int H, const Ris& ris) {
   RSample out = null_sample(0.0f);
-  if (sel.kind != kSkNone && selP > 0.0f) {
-    out = sel;
-    out.W = wSum / selP;
+  if (ris.sel.kind != kSkNone && ris.selP > 0.0f) {
+    out = ris.sel;
+    out.W = ris.wSum / ris.selP;
   }
   out.c = 1.0f;   // a failed candidate is a zero-valued outcome, confidence 1
   out.seed = pcg_hash((uint32_t)p + u.params0[0] * ((uint32_t)W * (uint32_t)H + 1u));
   store_res(resA, p, out);
+}
+
+// Initial RIS over the (at most one) bounce candidate (unification off).
+VRT_DI void store_initial(uint4* resA, size_t p, const Uni& u, int W, int H, bool has, const RSample& s, float Wc,
+                          F3 x1, F3 n1, uint32_t& rng) {
+  Ris ris;
+  ris.sel = null_sample(0.0f);
+  if (has) {
+    const float pt = eval_target(s, x1, n1);
+    ris.add(s, pt, pt * Wc, rng);
+  }
+  store_ris(resA, p, u, W, H, ris);
 }
 
 VRT_DI void initial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int gy, DCount& cnt) {
@@ -295,31 +464,74 @@ VRT_DI void initial_pixel(const RestirDev& R, const uint32_t* occ, int gx, int g
               (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
   R.gbuf[p] = make_float4(n1.x, n1.y, n1.z, h0.t);
 
+  const bool unified = rflag(u, kRfUnified);
   const float em = mat1.emissive * kEmissiveScale;
-  F3 direct = f3(em, em, em);
-  {   // sun-cone NEE at x1: pass-through radiance when unification is off
+  F3 direct = f3(em, em, em);   // radiance that bypasses the reservoir
+  Ris ris;
+  ris.sel = null_sample(0.0f);
+  {   // sun-cone NEE at x1: a direction candidate (unified) or pass-through radiance
     const F3 l = sample_sun_dir(u, rng);
     const float ndl = dot3(n1, l);
-    if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf1, l, 1e4f, cnt))
-      direct = direct + f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
+    if (ndl > 0.0f && l.y > 0.0f && !occluded(R, occ, surf1, l, 1e4f, cnt)) {
+      if (unified) {
+        const float coneSA = kTwoPi * (1.0f - u.sunDir[3]);
+        RSample s = null_sample(0.0f);
+        s.kind = kSkDir;
+        s.pos = l;
+        const float den = fmax_(coneSA, 1e-5f);
+        s.rad = f3(u.sunRadiance[0] / den, u.sunRadiance[1] / den, u.sunRadiance[2] / den);
+        const float pt = eval_target(s, x1, n1);
+        ris.add(s, pt, pt * coneSA, rng);   // W = 1/pdf = cone solid angle
+      } else {
+        direct = direct + f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]) * (kInvPi * ndl);
+      }
+    }
   }
-  RSample s = null_sample(0.0f);
-  float Wc = 0.0f;
-  const bool has = u.params0[1] > 0u;
-  if (has) {   // BSDF bounce candidate: reconnection vertex x2 carries Lo
+  if (unified && u.params2[1] > 0u) {   // light-list NEE at x1: RIS over emissive faces
+    const uint32_t nCand = emissive_cand_count(u, 0u);
+    float eSum = 0.0f, eSelP = 0.0f;
+    RSample eSel = null_sample(0.0f);
+    for (uint32_t k = 0u; k < nCand; k++) {
+      const LightPoint lp = sample_light_face(R, x1, rng);
+      RSample s = null_sample(0.0f);
+      s.kind = kSkPoint;
+      s.pos = lp.pos;
+      s.n = lp.n;
+      s.rad = lp.Le;
+      const float pt = eval_target(s, x1, n1);
+      const float w = pt / ((float)nCand * lp.pdfA);
+      if (w > 0.0f) {
+        eSum = eSum + w;
+        if (rand_(rng) * eSum < w) { eSel = s; eSelP = pt; }
+      }
+    }
+    if (eSel.kind != kSkNone && eSelP > 0.0f) {
+      const F3 d = eSel.pos - surf1;
+      const float r = __fsqrt_rn(dot3(d, d));
+      if (!occluded(R, occ, surf1, f3(d.x / r, d.y / r, d.z / r), r - 2e-3f, cnt)) {
+        const float We = eSum / eSelP;
+        ris.add(eSel, eSelP, eSelP * We, rng);
+      }
+    }
+  }
+  if (u.params0[1] > 0u) {   // BSDF bounce candidate: reconnection vertex x2 carries Lo
     const F3 brd = cosine_hemisphere(n1, rng);
     const DHit h = trace<true>(R.S, occ, surf1, brd, 1e4f, cnt);
+    RSample s;
+    float Wc;
     if (h.t < 0.0f) {
       cand_dir(u, n1, brd, s, Wc);
     } else {
       const F3 x2 = surf1 + brd * h.t;
       const Mat mat2 = unpack_material(h.mat);
       F3 Lo = estimate_lo(R, occ, x2, h.n, mat2, rng, cnt);
-      if (mat2.emissive > 0.0f) Lo = Lo + mat2.albedo * (mat2.emissive * kEmissiveScale);
+      if (!unified && mat2.emissive > 0.0f) Lo = Lo + mat2.albedo * (mat2.emissive * kEmissiveScale);
       cand_point(x1, n1, x2, h.n, fclamp3(R, Lo), s, Wc);
     }
+    const float pt = eval_target(s, x1, n1);
+    ris.add(s, pt, pt * Wc, rng);
   }
-  store_initial(R.resA, p, u, R.W, R.H, has, s, Wc, x1, n1, rng);
+  store_ris(R.resA, p, u, R.W, R.H, ris);
   R.direct[p] = pack_h4(direct.x, direct.y, direct.z, 1.0f);
 }
 
@@ -367,11 +579,26 @@ __global__ void __launch_bounds__(256) k_restir_temporal(const __grid_constant__
   matvec4(u.prevViewProj, x1.x, x1.y, x1.z, 1.0f, pc);
   if (pc[3] <= 0.0f) return;
   const float ndx = pc[0] / pc[3], ndy = pc[1] / pc[3];
-  const int ppx = itrunc_((ndx * 0.5f + 0.5f) * (float)R.W);
-  const int ppy = itrunc_(((-ndy) * 0.5f + 0.5f) * (float)R.H);
-  if (!valid_prev(R, ppx, ppy, x1, n1)) return;   // disocclusion: keep the fresh reservoir
+  int ppx = itrunc_((ndx * 0.5f + 0.5f) * (float)R.W);
+  int ppy = itrunc_(((-ndy) * 0.5f + 0.5f) * (float)R.H);
+  bool found = valid_prev(R, ppx, ppy, x1, n1);
+  if (!found && rflag(u, kRfRescue)) {   // disocclusion rescue: first validating 3x3 neighbour
+    for (int dy = -1; dy <= 1 && !found; dy++)
+      for (int dx = -1; dx <= 1 && !found; dx++)
+        if ((dx != 0 || dy != 0) && valid_prev(R, ppx + dx, ppy + dy, x1, n1)) {
+          ppx += dx;
+          ppy += dy;
+          found = true;
+        }
+  }
+  if (!found) return;   // disocclusion: keep the fresh reservoir
   const RSample st = load_res(R.resB, (size_t)ppy * R.W + ppx);
-  const float cT = fmin_(st.c, u.params3[0]);
+  float cap = u.params3[0];
+  if (rflag(u, kRfDupmap)) {   // duplication-adaptive confidence cap (Lin 2026 section 5)
+    const float dupScore = clamp_(R.dup[(size_t)ppy * R.W + ppx], 0.0f, 1.0f);
+    cap = mix_(u.params3[0], u.params3[1], pow_(dupScore, u.params3[2]));
+  }
+  const float cT = fmin_(st.c, cap);
   const RSample sc = load_res(R.resA, p);
   const float cC = fmax_(sc.c, 0.0f);
   const float pC = eval_target(sc, x1, n1), pT = eval_target(st, x1, n1);
@@ -406,15 +633,89 @@ __global__ void __launch_bounds__(256) k_restir_temporal(const __grid_constant__
 // ---------------------------------------------------------------------------
 struct SpatialPick {
   bool ok;          // a sample was selected (else: pooled null)
-  bool vis_test;    // its visibility must be tested (a neighbour's sample)
+  bool vis_test;    // its visibility must be tested (a neighbour's sample, or RF_FULLV)
   RSample sel;      // the selected sample with W and pooled confidence
   float cTotal;
+  F3 vcontrib;      // RF_VECTOR: the summed per-candidate contributions
 };
 
-VRT_DI SpatialPick spatial_pick(const RestirDev& R, int gx, int gy, float4 g, F3 x1, F3 n1) {
+// pairSize / pairOff / wrapMod / pairedPartner (reuse_spatial.wgsl:65-109):
+// the mutual partner of pixel (px, py) in pairing texture ti, varied per
+// frame by a hashed offset, mirror and swap; the pixel itself when the
+// partner falls off the image (rejected by the caller's bounds test).
+VRT_DI int wrap_mod(int v, int sz) { return ((v % sz) + sz) % sz; }
+
+VRT_DI void paired_partner(const RestirDev& R, int px, int py, uint32_t ti, int& qx, int& qy) {
+  const int sz = ti == 0u ? 254 : (ti == 1u ? 230 : 210);
+  const uint32_t off = ti == 0u ? 0u : (ti == 1u ? 64516u : 117416u);
+  const uint32_t h = pcg_hash(R.u.params0[0] * 2654435761u + ti * 0x68bc21ebu + 0x9e3779b9u);
+  const uint32_t h2 = pcg_hash(h);
+  const int ox = (int)(h % (uint32_t)sz), oy = (int)(h2 % (uint32_t)sz);
+  const bool mx = (h & 0x40000000u) != 0u, my = (h & 0x20000000u) != 0u, sw = (h & 0x10000000u) != 0u;
+  int ax = wrap_mod(px + ox, sz), ay = wrap_mod(py + oy, sz);
+  if (sw) { const int t = ax; ax = ay; ay = t; }
+  if (mx) ax = sz - 1 - ax;
+  if (my) ay = sz - 1 - ay;
+  const uint32_t word = R.pairing[off + (uint32_t)(ay * sz + ax)];
+  const int dtx = (int)(word << 16) >> 16, dty = (int)word >> 16;
+  int bx = wrap_mod(ax + dtx, sz), by = wrap_mod(ay + dty, sz);
+  if (mx) bx = sz - 1 - bx;
+  if (my) by = sz - 1 - by;
+  if (sw) { const int t = bx; bx = by; by = t; }
+  int dx = wrap_mod(bx - ox - px, sz), dy = wrap_mod(by - oy - py, sz);
+  if (dx > sz / 2) dx -= sz;
+  if (dy > sz / 2) dy -= sz;
+  qx = px + dx;
+  qy = py + dy;
+}
+
+// footprintOK (restir.wgsl:172-180)
+VRT_DI bool footprint_ok(const Uni& u, const RSample& s, F3 x1, F3 n1, float tPrim, float cosView) {
+  if (s.kind != kSkPoint) return true;
+  const F3 d = s.pos - x1;
+  const float r2 = dot3(d, d);
+  const F3 dir = d * (1.0f / __fsqrt_rn(fmax_(r2, 1e-8f)));
+  const float cos1 = fmax_(dot3(n1, dir), 0.0f);
+  const float cos2 = fmax_(dot3(s.n, f3(-dir.x, -dir.y, -dir.z)), 0.0f);
+  return r2 >= ((((u.params3[3] * tPrim) * tPrim) * cos1) * cos2) / fmax_(cosView, 0.05f);
+}
+
+// The shadow ray of sampleVisible (reuse_spatial.wgsl:117-126); false when
+// the sample is closer than 2 mm (visible without a ray).
+VRT_DI bool visibility_ray(const RSample& s, F3 x1, F3 n1, F3& o, F3& d, float& maxT) {
+  o = x1 + n1 * 1e-3f;
+  if (s.kind == kSkDir) {
+    d = s.pos;
+    maxT = 1e4f;
+    return true;
+  }
+  const F3 v = s.pos - o;
+  const float r = __fsqrt_rn(dot3(v, v));
+  if (r < 2e-3f) return false;
+  d = f3(v.x / r, v.y / r, v.z / r);
+  maxT = r - 2e-3f;
+  return true;
+}
+
+VRT_DI bool sample_visible(const RestirDev& R, const uint32_t* occ, const RSample& s, F3 x1, F3 n1, DCount& cnt) {
+  F3 o, d;
+  float maxT;
+  if (!visibility_ray(s, x1, n1, o, d, maxT)) return true;
+  return !occluded(R, occ, o, d, maxT, cnt);
+}
+
+// Neighbour selection, confidence-weighted balance-heuristic resampling and
+// (RF_VECTOR, kTraceHere only) the vector-valued shading sum of pixel (gx, gy).
+template <bool kTraceHere>
+VRT_DI SpatialPick spatial_pick(const RestirDev& R, const uint32_t* occ, DCount& cnt, int gx, int gy, float4 g, F3 x1,
+                                F3 n1) {
   const Uni& u = R.u;
   const size_t p = (size_t)gy * R.W + gx;
   uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
+  const float tPrim = g.w;
+  const bool footprint = rflag(u, kRfFootprint);
+  float cosView = 0.0f;
+  if (footprint) cosView = fmax_(dot3(n1, normalize3(f3(u.camPos[0], u.camPos[1], u.camPos[2]) - x1)), 0.0f);
   F3 dx[4], dn[4];
   float dc[4];
   uint32_t qi[4];
@@ -428,40 +729,62 @@ VRT_DI SpatialPick spatial_pick(const RestirDev& R, int gx, int gy, float4 g, F3
     dok[0] = true;
     cok[0] = ((d0.y >> 16) & 3u) != kSkNone;
   }
-  const uint32_t taps = (u.params2[0] & kRfSpatial) ? min(u.params2[2], 3u) : 0u;
+  const uint32_t taps = rflag(u, kRfSpatial) ? min(u.params2[2], 3u) : 0u;
+  const bool paired = rflag(u, kRfPaired), plane = rflag(u, kRfPlane);
 #pragma unroll
   for (int k = 1; k < 4; k++) {
     dok[k] = cok[k] = false;
     dc[k] = 0.0f;
     qi[k] = 0u;
     dx[k] = dn[k] = f3(0.0f, 0.0f, 0.0f);
-    if ((uint32_t)k > taps) continue;
-    // classic random neighbour in a uniform disk of radius params4.x
-    const float r = u.params4[0] * __fsqrt_rn(rand_(rng));
-    const float a = kTwoPi * rand_(rng);
-    float sa, ca;
-    sincos_(a, sa, ca);
-    const int qx = gx + itrunc_(ca * r), qy = gy + itrunc_(sa * r);
+    const uint32_t ti = (uint32_t)k - 1u;
+    if (ti >= taps) continue;
+    int qx, qy;
+    if (paired) {
+      // RF_MIXSIGMA: the last tap reads the wide-sigma texture 0, the others shift up
+      uint32_t tex = ti;
+      if (rflag(u, kRfMixSigma)) tex = ti + 1u == taps ? 0u : ti + 1u;
+      paired_partner(R, gx, gy, tex, qx, qy);
+    } else {   // classic random neighbour in a uniform disk of radius params4.x
+      const float r = u.params4[0] * __fsqrt_rn(rand_(rng));
+      const float a = kTwoPi * rand_(rng);
+      float sa, ca;
+      sincos_(a, sa, ca);
+      qx = gx + itrunc_(ca * r);
+      qy = gy + itrunc_(sa * r);
+    }
     if ((qx == gx && qy == gy) || qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
     const size_t q = (size_t)qy * R.W + qx;
     const float4 gq = R.gbuf[q];
     if (gq.w <= 0.0f) continue;
     const F3 nq = f3(gq.x, gq.y, gq.z);
     const float nDot = dot3(n1, nq);
-    if (!(nDot > 0.9f && fabsf(gq.w - g.w) < 0.1f * g.w + 0.02f)) continue;
+    const bool genericOk = nDot > 0.9f && fabsf(gq.w - g.w) < 0.1f * g.w + 0.02f;
+    F3 x1q = f3(0.0f, 0.0f, 0.0f);
+    bool ok = genericOk;
+    if (plane) {   // same voxel face plane, regardless of depth
+      x1q = surface_at(u, qx, qy, R.W, R.H, gq);
+      ok = genericOk || (nDot > 0.99f && fabsf(dot3(n1, x1q - x1)) < 0.02f);
+    }
+    if (!ok) continue;
     const uint4 dq = R.resA[2 * q + 1];
-    dx[k] = surface_at(u, qx, qy, R.W, R.H, gq);
+    const bool nonnull = ((dq.y >> 16) & 3u) != kSkNone;
+    if (footprint && nonnull && !footprint_ok(u, load_res(R.resA, q), x1, n1, tPrim, cosView)) continue;
+    dx[k] = plane ? x1q : surface_at(u, qx, qy, R.W, R.H, gq);
     dn[k] = nq;
     dc[k] = (float)((dq.y >> 18) & 0xffu);
     qi[k] = (uint32_t)q;
     dok[k] = true;
-    cok[k] = ((dq.y >> 16) & 3u) != kSkNone;
+    cok[k] = nonnull;
   }
   SpatialPick pk;
   pk.cTotal = 0.0f;
+  pk.vcontrib = f3(0.0f, 0.0f, 0.0f);
 #pragma unroll
   for (int l = 0; l < 4; l++)
     if (dok[l]) pk.cTotal = pk.cTotal + dc[l];
+  const bool vector = kTraceHere && rflag(u, kRfVector);
+  const bool fullV = rflag(u, kRfFullV);
   float wSum = 0.0f, selP = 0.0f;
   int rank = 0, selRank = 0;
   pk.sel = null_sample(0.0f);
@@ -486,33 +809,21 @@ VRT_DI SpatialPick spatial_pick(const RestirDev& R, int gx, int gy, float4 g, F3
         wSum = wSum + w;
         if (rand_(rng) * wSum < w) { pk.sel = s; selP = pMe; selRank = rank; }
       }
+      if (vector && w > 0.0f) {   // vector-valued shading weight with per-candidate visibility
+        bool vis = true;
+        if (rank > 0 || fullV) vis = sample_visible(R, occ, s, x1, n1, cnt);
+        if (vis) pk.vcontrib = pk.vcontrib + eval_f(s, x1, n1) * (m * fmax_(s.W, 0.0f));
+      }
     }
     rank++;
   }
   pk.ok = pk.sel.kind != kSkNone && selP > 0.0f && wSum > 0.0f;
-  pk.vis_test = selRank > 0;
+  pk.vis_test = selRank > 0 || fullV;
   if (pk.ok) {
     pk.sel.W = wSum / selP;
     pk.sel.c = fmin_(pk.cTotal, 255.0f);
   }
   return pk;
-}
-
-// The shadow ray of sampleVisible (reuse_spatial.wgsl:117-126); false when
-// the sample is closer than 2 mm (visible without a ray).
-VRT_DI bool visibility_ray(const RSample& s, F3 x1, F3 n1, F3& o, F3& d, float& maxT) {
-  o = x1 + n1 * 1e-3f;
-  if (s.kind == kSkDir) {
-    d = s.pos;
-    maxT = 1e4f;
-    return true;
-  }
-  const F3 v = s.pos - o;
-  const float r = __fsqrt_rn(dot3(v, v));
-  if (r < 2e-3f) return false;
-  d = f3(v.x / r, v.y / r, v.z / r);
-  maxT = r - 2e-3f;
-  return true;
 }
 
 VRT_DI void out_radiance(const RestirDev& R, size_t p, F3 v) {
@@ -525,10 +836,31 @@ VRT_DI F3 load_direct(const RestirDev& R, size_t p) {
   return f3(dr.x, dr.y, dr.z);
 }
 
-// Selection, record and (without a pending ray) radiance of pixel (gx, gy).
-// Returns whether a visibility ray is pending; then o / d / maxT describe
-// it and contrib is the contribution it gates.
-VRT_DI bool spatial_pixel(const RestirDev& R, int gx, int gy, F3& o, F3& d, float& maxT, F3& contrib) {
+// RF_CLAMP: luminance clamp of the reservoir contribution (params4.z).
+VRT_DI F3 clamp_contrib(const Uni& u, F3 c) {
+  if (!rflag(u, kRfClamp)) return c;
+  const float l = rlum(c);
+  return l > u.params4[2] ? c * (u.params4[2] / l) : c;
+}
+
+// Next frame's history record: the post-spatial sample, or with
+// RF_HISTISOLATE the pre-spatial (temporal) reservoir.
+VRT_DI void store_history(const RestirDev& R, size_t p, const RSample& s) {
+  if (rflag(R.u, kRfHistIsolate)) {
+    R.resB[2 * p] = R.resA[2 * p];
+    R.resB[2 * p + 1] = R.resA[2 * p + 1];
+  } else {
+    store_res(R.resB, p, s);
+  }
+}
+
+// Selection, record and (unless a visibility ray is left pending) radiance of
+// pixel (gx, gy).  kTraceHere: every visibility ray is traced in place.
+// Otherwise returns whether a ray is pending; then o / d / maxT describe it
+// and contrib is the contribution it gates (clamped after the test).
+template <bool kTraceHere>
+VRT_DI bool spatial_pixel(const RestirDev& R, const uint32_t* occ, DCount& cnt, int gx, int gy, F3& o, F3& d,
+                          float& maxT, F3& contrib) {
   const size_t p = (size_t)gy * R.W + gx;
   const F3 direct = load_direct(R, p);
   const float4 g = R.gbuf[p];
@@ -540,20 +872,27 @@ VRT_DI bool spatial_pixel(const RestirDev& R, int gx, int gy, F3& o, F3& d, floa
   }
   const F3 x1 = surface_at(R.u, gx, gy, R.W, R.H, g);
   const F3 n1 = f3(g.x, g.y, g.z);
-  const SpatialPick pk = spatial_pick(R, gx, gy, g, x1, n1);
+  const SpatialPick pk = spatial_pick<kTraceHere>(R, occ, cnt, gx, gy, g, x1, n1);
   if (!pk.ok) {   // pooled null
     out_radiance(R, p, direct);
-    store_res(R.resB, p, null_sample(fmin_(pk.cTotal, 255.0f)));
+    store_history(R, p, null_sample(fmin_(pk.cTotal, 255.0f)));
     return false;
   }
-  store_res(R.resB, p, pk.sel);
+  store_history(R, p, pk.sel);
+  if (kTraceHere && rflag(R.u, kRfVector)) {
+    out_radiance(R, p, direct + clamp_contrib(R.u, pk.vcontrib));
+    return false;
+  }
   contrib = eval_f(pk.sel, x1, n1) * pk.sel.W;
-  if (pk.vis_test && visibility_ray(pk.sel, x1, n1, o, d, maxT)) return true;
-  out_radiance(R, p, direct + contrib);
+  if (pk.vis_test && visibility_ray(pk.sel, x1, n1, o, d, maxT)) {
+    if (!kTraceHere) return true;
+    if (occluded(R, occ, o, d, maxT, cnt)) contrib = f3(0.0f, 0.0f, 0.0f);
+  }
+  out_radiance(R, p, direct + clamp_contrib(R.u, contrib));
   return false;
 }
 
-// Fused form (megakernel sessions): the visibility ray traced in place.
+// Fused form (megakernel sessions, and RF_VECTOR): rays traced in place.
 template <bool kSmem>
 __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ RestirDev R) {
   extern __shared__ uint32_t s_occ[];
@@ -564,18 +903,14 @@ __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ 
   if (gx < R.W && gy < R.H) {
     F3 o, d, contrib;
     float maxT;
-    if (spatial_pixel(R, gx, gy, o, d, maxT, contrib)) {
-      const size_t p = (size_t)gy * R.W + gx;
-      const bool vis = !occluded(R, occ, o, d, maxT, cnt);
-      out_radiance(R, p, load_direct(R, p) + (vis ? contrib : f3(0.0f, 0.0f, 0.0f)));
-    }
+    spatial_pixel<true>(R, occ, cnt, gx, gy, o, d, maxT, contrib);
   }
   if (R.stats) warp_flush_stats(R.stats, cnt, 0u);
 }
 
-// Split form (wavefront sessions): selection here, the pending visibility
-// rays appended to a queue of the wavefront tracer (origin R0, direction and
-// maxT in R2, contribution in S1, pass-through radiance in S0), traced by the
+// Split form (wavefront sessions, scalar shading weight): selection here, the
+// pending visibility rays appended to a queue of the wavefront tracer (origin
+// R0, direction and maxT in R2, gated contribution in S1), traced by the
 // persistent tracer, then k_restir_spatial_resolve.
 __global__ void __launch_bounds__(256) k_restir_spatial_select(const __grid_constant__ RestirDev R, WfDev b,
                                                                int wave) {
@@ -583,7 +918,8 @@ __global__ void __launch_bounds__(256) k_restir_spatial_select(const __grid_cons
   block_pixel_16x16(gx, gy);
   F3 o, d, contrib;
   float maxT;
-  const bool ray = gx < R.W && gy < R.H && spatial_pixel(R, gx, gy, o, d, maxT, contrib);
+  DCount cnt{0u, 0u, 0u, 0u};
+  const bool ray = gx < R.W && gy < R.H && spatial_pixel<false>(R, nullptr, cnt, gx, gy, o, d, maxT, contrib);
   const uint32_t g = ray ? (uint32_t)gy * (uint32_t)R.W + (uint32_t)gx : 0u;
   const uint32_t slot = warp_append(b.ctr + 4 * wave, ray);
   if (ray) {
@@ -602,8 +938,32 @@ __global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_con
     const uint32_t g = q[i] & ~kShadowBit;
     const bool vis = b.hit[g].w == 0u;
     const float4 c = b.S1[g];
-    out_radiance(R, g, load_direct(R, g) + (vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
+    out_radiance(R, g, load_direct(R, g) + clamp_contrib(R.u, vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
   }
+}
+
+// dupmap.wgsl: share of the 9x9 window (centre excluded) whose reservoirs B
+// carry the same initial candidate (seed) as this pixel's.
+__global__ void __launch_bounds__(256) k_restir_dupmap(const __grid_constant__ RestirDev R) {
+  int gx, gy;
+  block_pixel_16x16(gx, gy);
+  if (gx >= R.W || gy >= R.H) return;
+  const size_t p = (size_t)gy * R.W + gx;
+  const uint4 mine = R.resB[2 * p + 1];
+  if (((mine.y >> 16) & 3u) == kSkNone) {
+    R.dup[p] = 0.0f;
+    return;
+  }
+  int count = 0;
+  for (int dy = -4; dy <= 4; dy++)
+    for (int dx = -4; dx <= 4; dx++) {
+      if (dx == 0 && dy == 0) continue;
+      const int qx = gx + dx, qy = gy + dy;
+      if (qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
+      const uint4 r = R.resB[2 * ((size_t)qy * R.W + qx) + 1];
+      if (((r.y >> 16) & 3u) != kSkNone && r.w == mine.w) count++;
+    }
+  R.dup[p] = (float)count / 80.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -844,6 +1204,11 @@ static RestirDev restir_dev(const SceneDev& s, const VrtUniforms& u, float fclam
   R.gbuf = (float4*)out.gbuf;
   R.gprev = (const float4*)rb.gbuf_prev;
   R.stats = out.stats;
+  R.dup = rb.dup;
+  R.pairing = rb.pairing;
+  R.lights = (const uint2*)rb.light_words;
+  R.lightAlias = (const float4*)rb.light_alias;
+  R.lightGrid = rb.light_grid;
   return R;
 }
 
@@ -918,6 +1283,14 @@ cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W
                                   const RestirBufs& rb, cudaStream_t st) {
   const RestirDev R = restir_dev(s, u, 0.0f, W, H, out, rb);
   return launch_occ_kernel(k_restir_spatial<true>, k_restir_spatial<false>, s, W, H, R, st);
+}
+
+cudaError_t launch_restir_dupmap(const VrtUniforms& u, int W, int H, const RestirBufs& rb, cudaStream_t st) {
+  SceneDev none;
+  PathOut out;
+  const RestirDev R = restir_dev(none, u, 0.0f, W, H, out, rb);
+  k_restir_dupmap<<<dim3((W + 15) / 16, (H + 15) / 16), 256, 0, st>>>(R);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,

@@ -127,6 +127,9 @@ struct VrtSession {
   // (8 B per pixel), allocated by the first frame with reservoir flags
   void* restir_mem = nullptr;
   size_t restir_bytes = 0;
+  uint32_t* pairing = nullptr;    // pairing textures (RF_PAIRED), built on first use
+  double pairing_built[3] = {0.0, 0.0, 0.0};   // their sigmas
+  double pairing_sigma = 16.0;    // base sigma (main.js:73 `sigma`)
   bool restir_timed = false;      // ev[5] marks the end of the initial pass
   uint64_t events_frame = ~0ull;  // frame whose pass events vrt_frame recorded
 };
@@ -385,6 +388,7 @@ int vrt_session_destroy(VrtSession* s) {
   dev_free(c, s->hdr_ref, P * 12, &s->bytes);
   dev_free(c, s->hdr_part, (size_t)hdr_blocks((int)P) * 8, &s->bytes);
   dev_free(c, s->restir_mem, s->restir_bytes, &s->bytes);
+  dev_free(c, s->pairing, (size_t)kPairingWords * 4, &s->bytes);
   if (s->mlp) vrt_mlp_destroy(s->mlp);
   for (auto& e : s->cev)
     if (e) cudaEventDestroy(e);
@@ -586,7 +590,7 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
 // Reservoir buffers of the session, allocated (zeroed) on first use.
 static int ensure_restir(VrtSession* s) {
   if (s->restir_mem) return VRT_OK;
-  const size_t bytes = px(s) * (32 + 32 + 8 + 16);
+  const size_t bytes = px(s) * (32 + 32 + 16 + 8 + 4);
   if (int r = dev_alloc(s->ctx, &s->restir_mem, bytes, &s->bytes)) return r;
   s->restir_bytes = bytes;
   CUDA_TRY(cudaMemsetAsync(s->restir_mem, 0, bytes, s->ctx->stream));
@@ -598,10 +602,47 @@ static RestirBufs restir_bufs(const VrtSession* s, int parity) {
   char* m = (char*)s->restir_mem;
   rb.resA = m;
   rb.resB = m + px(s) * 32;
-  rb.scratch = m + px(s) * 64;   // 16-byte records before the 8-byte ones: every
-  rb.direct = m + px(s) * 80;    // region starts on a 16-byte boundary for any P
+  rb.scratch = m + px(s) * 64;   // 16-byte records before the 8- and 4-byte ones:
+  rb.direct = m + px(s) * 80;    // every region starts on its own alignment for any P
+  rb.dup = (float*)(m + px(s) * 88);
   rb.gbuf_prev = s->gbuf[1 - parity];
+  rb.pairing = s->pairing;
+  const VrtScene* sc = s->scene;
+  rb.light_words = sc->light_words;
+  rb.light_alias = sc->light_alias;
+  rb.light_grid = sc->light_grid;
   return rb;
+}
+
+// Pairing textures for the frame's sigmas (main.js:252-263): texture 0 takes
+// the wide sigma (params5.x) under RF_MIXSIGMA, the others the base sigma.
+static int ensure_pairing(VrtSession* s, const VrtUniforms* u) {
+  if (!(u->params2[0] & kRfPaired)) return VRT_OK;
+  const double base = std::max(0.8, s->pairing_sigma);
+  const double wide = (u->params2[0] & kRfMixSigma) ? std::max(0.8, (double)u->params5[0]) : base;
+  const double want[3] = {wide, base, base};
+  if (s->pairing && std::equal(want, want + 3, s->pairing_built)) return VRT_OK;
+  if (!s->pairing)
+    if (int r = dev_alloc(s->ctx, (void**)&s->pairing, (size_t)kPairingWords * 4, &s->bytes)) return r;
+  std::vector<uint32_t> host(kPairingWords);
+  make_pairing_buffer(want, host.data());
+  CUDA_TRY(cudaMemcpyAsync(s->pairing, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  std::copy(want, want + 3, s->pairing_built);
+  return VRT_OK;
+}
+
+// Unified NEE reads the scene's light list (built on first use; an edited
+// scene's lights are rebuilt by vrt_scene_build_lights).
+static int ensure_lights(VrtSession* s, const VrtUniforms* u) {
+  if (!(u->params2[0] & kRfUnified) || u->params2[1] == 0u) return VRT_OK;
+  if (!s->scene->lights_built)
+    if (int r = vrt_scene_build_lights(s->scene, nullptr)) return r;
+  if (u->params2[1] > s->scene->light_count)
+    return fail(VRT_ERR_INVALID, "params2.y = %u lights, the scene has %u", u->params2[1], s->scene->light_count);
+  if ((u->params2[0] & kRfLightGrid) && !s->scene->light_grid)
+    return fail(VRT_ERR_STATE, "light grid not built");
+  return VRT_OK;
 }
 
 static int parity_of(const VrtSession* s) { return (int)(s->frame_counter & 1u); }
@@ -619,8 +660,11 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
   if (restir_on(u)) {
     if (s->cache_on) return fail(VRT_ERR_STATE, "the radiance cache serves the plain path only (restir flags set)");
     if (int r = ensure_restir(s)) return r;
+    if (int r = ensure_lights(s, u)) return r;
     const RestirBufs rb = restir_bufs(s, parity_of(s));
-    if (s->path_kernel == VRT_PATH_WAVEFRONT && (int)u->params0[1] + 3 <= s->wf.max_waves) {
+    // unified NEE adds a second shadow ray per vertex: the per-pixel kernel
+    if (s->path_kernel == VRT_PATH_WAVEFRONT && !(u->params2[0] & kRfUnified) &&
+        (int)u->params0[1] + 3 <= s->wf.max_waves) {
       CUDA_TRY(launch_restir_initial_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
                                                s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,
                                                VrtSession::kTimedWaves, &s->timed_waves));
@@ -651,7 +695,10 @@ static int restir_pass(VrtSession* s, const VrtUniforms* u, bool spatial) {
   const int p = parity_of(s);
   PathOut o;
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[p]; o.stats = s->stats;
-  if (spatial && s->path_kernel == VRT_PATH_WAVEFRONT) {
+  if (spatial)
+    if (int r = ensure_pairing(s, u)) return r;
+  // vector-valued weights test every candidate's visibility: traced in place
+  if (spatial && s->path_kernel == VRT_PATH_WAVEFRONT && !(u->params2[0] & kRfVector)) {
     CUDA_TRY(launch_restir_spatial_wavefront(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->wf, s->tune,
                                              s->ctx->stream, &s->launches));
     return VRT_OK;
@@ -668,6 +715,23 @@ static int restir_pass(VrtSession* s, const VrtUniforms* u, bool spatial) {
 
 int vrt_pass_reuse_temporal(VrtSession* s, const VrtUniforms* u) { return restir_pass(s, u, false); }
 int vrt_pass_reuse_spatial(VrtSession* s, const VrtUniforms* u) { return restir_pass(s, u, true); }
+
+int vrt_pass_dupmap(VrtSession* s, const VrtUniforms* u) {
+  if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
+  if (int r = check_uniforms(s, u)) return r;
+  if (!restir_on(u) || !(u->params2[0] & (kRfDupmap | kRfMutate))) return VRT_OK;   // main.js:741
+  if (!s->restir_mem) return fail(VRT_ERR_STATE, "duplication map before the initial pass of a ReSTIR frame");
+  if (int r = set_dev(s->ctx)) return r;
+  CUDA_TRY(launch_restir_dupmap(*u, s->W, s->H, restir_bufs(s, parity_of(s)), s->ctx->stream));
+  s->launches++;
+  return VRT_OK;
+}
+
+int vrt_session_set_pairing_sigma(VrtSession* s, float sigma) {
+  if (!s || !(sigma > 0.0f)) return fail(VRT_ERR_INVALID, "bad argument");
+  s->pairing_sigma = (double)sigma;
+  return VRT_OK;
+}
 
 int vrt_pass_temporal(VrtSession* s, const VrtUniforms* u) {
   if (!s) return fail(VRT_ERR_INVALID, "session is NULL");
@@ -738,6 +802,7 @@ int vrt_frame(VrtSession* s, const VrtUniforms* u) {
     if (u->params2[0] & kRfTemporal)
       if (int r = vrt_pass_reuse_temporal(s, u)) return r;
     if (int r = vrt_pass_reuse_spatial(s, u)) return r;
+    if (int r = vrt_pass_dupmap(s, u)) return r;
   }
   if (s->timing) CUDA_TRY(cudaEventRecord(s->ev[1], st));
   if (int r = vrt_pass_temporal(s, u)) return r;
@@ -838,6 +903,10 @@ int vrt_read_reservoirs(VrtSession* s, int which, void* h, size_t b) {
   if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
   return read_buf(s, s ? (const char*)s->restir_mem + (size_t)which * px(s) * 32 : nullptr, s ? px(s) * 32 : 0, h,
                   b);
+}
+int vrt_read_dupmap(VrtSession* s, void* h, size_t b) {
+  if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
+  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 88 : nullptr, s ? px(s) * 4 : 0, h, b);
 }
 int vrt_read_direct(VrtSession* s, void* h, size_t b) {
   if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");

@@ -230,10 +230,25 @@ cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const voi
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
                            const uint32_t* alb8, uint32_t* ldr, cudaStream_t st);
 
-// Reservoir flags of params2.x (common.wgsl:40-42) this build implements:
-// the `gi` preset (main.js:44).
-constexpr uint32_t kRfRestir = 1u, kRfTemporal = 2u, kRfSpatial = 4u;
-constexpr uint32_t kRestirFlagsImplemented = kRfRestir | kRfTemporal | kRfSpatial;
+// Reservoir flags of params2.x (common.wgsl:40-59).
+constexpr uint32_t kRfRestir = 1u, kRfTemporal = 2u, kRfSpatial = 4u, kRfPaired = 8u, kRfDupmap = 16u,
+                   kRfFootprint = 32u, kRfVector = 64u, kRfUnified = 128u, kRfPlane = 256u, kRfRescue = 512u,
+                   kRfFullV = 1024u, kRfClamp = 2048u, kRfLightPower = 4096u, kRfMixSigma = 8192u,
+                   kRfAdaptCand = 16384u, kRfConfDenoise = 32768u, kRfLightGrid = 65536u, kRfMutate = 131072u,
+                   kRfHistIsolate = 262144u, kRfWorldGi = 524288u;
+// The flags this build implements: every flag of the `gi`, `lin`, `ours` and
+// `ours_motion` presets (main.js:40-62) plus footprint, mixed sigma, adaptive
+// candidate counts and the light grid.
+constexpr uint32_t kRestirFlagsImplemented =
+    kRfRestir | kRfTemporal | kRfSpatial | kRfPaired | kRfDupmap | kRfFootprint | kRfVector | kRfUnified | kRfPlane |
+    kRfRescue | kRfFullV | kRfClamp | kRfLightPower | kRfMixSigma | kRfAdaptCand | kRfLightGrid | kRfHistIsolate;
+
+// Pairing textures of paired spatial reuse (pairing.js:74): sizes and offsets.
+constexpr int kPairSizes[3] = {254, 230, 210};
+constexpr uint32_t kPairingWords = 254u * 254u + 230u * 230u + 210u * 210u;
+// pairing.js:26-70 restated: the three textures for sigmas[0..2] (uint32
+// words of two i16 coordinate deltas), into out[kPairingWords].
+void make_pairing_buffer(const double sigmas[3], uint32_t* out);
 
 // ReSTIR reservoirs of one session (32 bytes per pixel each, the reference's
 // record layout) and the pass-through radiance of the initial pass.
@@ -243,6 +258,11 @@ struct RestirBufs {
   void* direct = nullptr;           // rgba16f
   const void* gbuf_prev = nullptr;  // previous frame's G-buffer
   void* scratch = nullptr;          // 16 B per pixel: wavefront path state (x2)
+  float* dup = nullptr;             // duplication score per pixel (dupmap.wgsl)
+  const uint32_t* pairing = nullptr;      // kPairingWords (RF_PAIRED)
+  const uint32_t* light_words = nullptr;  // 2 per light (RF_UNIFIED)
+  const float* light_alias = nullptr;     // 4 per light
+  const uint32_t* light_grid = nullptr;   // 34 per brick cell
 };
 cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                                   const PathOut& out, const RestirBufs& rb, cudaStream_t st);
@@ -255,6 +275,8 @@ cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int 
                                    const RestirBufs& rb, cudaStream_t st);
 cudaError_t launch_restir_spatial(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
                                   const RestirBufs& rb, cudaStream_t st);
+// dupmap.wgsl: duplication score of every pixel from reservoirs B.
+cudaError_t launch_restir_dupmap(const VrtUniforms& u, int W, int H, const RestirBufs& rb, cudaStream_t st);
 // The spatial pass with its visibility rays on the wavefront tracer (select,
 // trace, resolve; bit-identical to launch_restir_spatial).
 cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
