@@ -935,7 +935,7 @@ __global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_con
   const int n = b.ctr[4 * wave];
   const uint32_t* q = queue_of(b, wave);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t g = q[i] & ~kShadowBit;
+    const uint32_t g = q[i] & kEntryIndex;
     const bool vis = b.hit[g].w == 0u;
     const float4 c = b.S1[g];
     out_radiance(R, g, load_direct(R, g) + clamp_contrib(R.u, vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
@@ -988,8 +988,13 @@ __global__ void __launch_bounds__(256) k_restir_dupmap(const __grid_constant__ R
 struct RestirWf {
   uint4* resA;
   uint2* direct;
-  float4* x2;     // per path: reconnection vertex x2 (xyz), code of its normal (w bits)
+  float4* x2;     // per path: reconnection vertex x2 (xyz), code of its normal (w bits; unified: + state bits)
   int W, H;
+  // unified (RF_UNIFIED) path state: the initial RIS at x1 across its waves
+  float4* selPW;  // selected candidate's position / direction, RIS weight sum
+  float4* selRP;  // its radiance, its target p-hat
+  float4* aux;    // light-list candidate's position and weight sum (x1), or the pending NEE term (x2...)
+  float4* aux2;   // light-list candidate's radiance and p-hat
 };
 
 // Exact code of a DDA normal (components +-0 or +-1): sign and magnitude
@@ -1185,6 +1190,369 @@ __global__ void __launch_bounds__(256) k_wf_restir_wave(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------------------
+// wavefront form of the unified initial pass (RF_UNIFIED).  At x1 the RNG
+// stream depends on each visibility result (a candidate that survives its
+// shadow ray draws its RIS number), so x1's rays run one per wave:
+//   kStSun    sun-cone shadow ray -> sun direction candidate
+//   kStLight  light-list RIS over emissive faces -> its shadow ray -> candidate
+//   kStBounce bounce ray -> x2 (or a sky direction candidate)
+// then every estimateLo vertex issues its sun shadow ray, its light-list NEE
+// shadow ray (the tracer's second shadow slot) and its bounce ray in one wave
+// (kStLo): no draw depends on their results.  The RIS state at x1 (weight
+// sum, selected candidate, p-hat) is kept per path between waves.
+// ---------------------------------------------------------------------------
+enum : uint32_t { kStSun = 0u, kStLight = 1u, kStBounce = 2u, kStLo = 3u };
+
+// State bits (x2.w): x2's normal code 0-5, selected kind 6-7, its normal
+// code 8-13, stage 14-15, light candidate's normal code 16-21, estimateLo
+// vertex index 22-29 (paths reach x2 in different waves).
+VRT_DI uint32_t bits_get(uint32_t b, int at, int n) { return (b >> at) & ((1u << n) - 1u); }
+VRT_DI uint32_t bits_set(uint32_t b, int at, int n, uint32_t v) {
+  const uint32_t m = ((1u << n) - 1u) << at;
+  return (b & ~m) | ((v << at) & m);
+}
+
+VRT_DI void ris_save(const RestirWf& r, uint32_t g, const Ris& q, uint32_t& bits) {
+  r.selPW[g] = make_float4(q.sel.pos.x, q.sel.pos.y, q.sel.pos.z, q.wSum);
+  r.selRP[g] = make_float4(q.sel.rad.x, q.sel.rad.y, q.sel.rad.z, q.selP);
+  bits = bits_set(bits, 6, 2, q.sel.kind);
+  bits = bits_set(bits, 8, 6, normal_code(q.sel.n));
+}
+
+VRT_DI Ris ris_load(const RestirWf& r, uint32_t g, uint32_t bits) {
+  const float4 a = r.selPW[g], c = r.selRP[g];
+  Ris q;
+  q.sel = null_sample(0.0f);
+  q.sel.kind = bits_get(bits, 6, 2);
+  q.sel.pos = f3(a.x, a.y, a.z);
+  q.sel.n = normal_decode(bits_get(bits, 8, 6));
+  q.sel.rad = f3(c.x, c.y, c.z);
+  q.wSum = a.w;
+  q.selP = c.w;
+  return q;
+}
+
+// x1 and n1 of path g from the G-buffer and the recomputed primary ray.
+VRT_DI void x1_of(const RestirDev& R, uint32_t g, F3& x1, F3& n1, F3& surf1) {
+  const float4 gb = R.gbuf[g];
+  n1 = f3(gb.x, gb.y, gb.z);
+  const uint32_t gx = g % (uint32_t)R.W, gy = g / (uint32_t)R.W;
+  x1 = f3(R.u.camPos[0], R.u.camPos[1], R.u.camPos[2]) + primary_dir(R.u, gx, gy, R.W, R.H) * gb.w;
+  surf1 = x1 + n1 * fmax_(1e-3f, gb.w * 1e-4f);
+}
+
+struct URays {
+  bool shadow = false, shadow2 = false, bounce = false;
+};
+
+// The path's candidate is final: reservoir A.
+VRT_DI void unified_finish(const RestirDev& R, uint32_t g, const Ris& ris) { store_ris(R.resA, g, R.u, R.W, R.H, ris); }
+
+// Runs x1's stages from the start of stage `st` (earlier stages resolved)
+// until a ray is pending (returned in rays, state saved) or the candidate
+// path ends.
+VRT_DI void x1_run(const RestirDev& R, const RestirWf& r, const WfDev& b, uint32_t g, uint32_t st, Ris& ris,
+                   uint32_t& bits, uint32_t& rng, F3 x1, F3 n1, F3 surf1, URays& rays) {
+  const Uni& u = R.u;
+  if (st == kStLight) {   // light-list NEE at x1: RIS over emissive faces
+    if (u.params2[1] > 0u) {
+      const uint32_t nCand = emissive_cand_count(u, 0u);
+      float eSum = 0.0f, eSelP = 0.0f;
+      RSample eSel = null_sample(0.0f);
+      for (uint32_t k = 0u; k < nCand; k++) {
+        const LightPoint lp = sample_light_face(R, x1, rng);
+        RSample s = null_sample(0.0f);
+        s.kind = kSkPoint;
+        s.pos = lp.pos;
+        s.n = lp.n;
+        s.rad = lp.Le;
+        const float pt = eval_target(s, x1, n1);
+        const float w = pt / ((float)nCand * lp.pdfA);
+        if (w > 0.0f) {
+          eSum = eSum + w;
+          if (rand_(rng) * eSum < w) { eSel = s; eSelP = pt; }
+        }
+      }
+      if (eSel.kind != kSkNone && eSelP > 0.0f) {
+        const F3 d = eSel.pos - surf1;
+        const float rr = __fsqrt_rn(dot3(d, d));
+        b.R0[g] = make_float4(surf1.x, surf1.y, surf1.z, 0.0f);
+        b.R2[g] = make_float4(d.x / rr, d.y / rr, d.z / rr, rr - 2e-3f);
+        r.aux[g] = make_float4(eSel.pos.x, eSel.pos.y, eSel.pos.z, eSum);
+        r.aux2[g] = make_float4(eSel.rad.x, eSel.rad.y, eSel.rad.z, eSelP);
+        bits = bits_set(bits, 16, 6, normal_code(eSel.n));
+        bits = bits_set(bits, 14, 2, kStLight);
+        rays.shadow = true;
+      }
+    }
+    if (!rays.shadow) st = kStBounce;
+  }
+  if (st == kStBounce) {
+    if (u.params0[1] > 0u) {
+      const F3 brd = cosine_hemisphere(n1, rng);
+      b.R0[g] = make_float4(surf1.x, surf1.y, surf1.z, 0.0f);
+      b.R1[g] = make_float4(brd.x, brd.y, brd.z, 1e4f);
+      bits = bits_set(bits, 14, 2, kStBounce);
+      rays.bounce = true;
+    } else {
+      unified_finish(R, g, ris);
+      return;
+    }
+  }
+  ris_save(r, g, ris, bits);
+  b.S0[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
+  r.x2[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(bits));
+}
+
+// estimateLo's vertex v with unification (pathtrace.wgsl:213-244): sun shadow,
+// light-list NEE shadow and bounce rays issued together.  Returns whether the
+// path stays active.
+VRT_DI bool lo_vertex(const RestirDev& R, const WfDev& b, const RestirWf& r, uint32_t g, uint32_t v, F3 pos, F3 n,
+                      Mat mat, F3 Lo, F3 tp, uint32_t& rng, URays& rays) {
+  const Uni& u = R.u;
+  const uint32_t nB = u.params0[1];
+  const F3 surf = pos + n * 1e-3f;
+  uint32_t flags = 0u;
+  const F3 l = sample_sun_dir(u, rng);
+  const float ndl = dot3(n, l);
+  F3 sunc = f3(0.0f, 0.0f, 0.0f);
+  if (ndl > 0.0f && l.y > 0.0f) {
+    sunc = (((tp * mat.albedo) * kInvPi) * ndl) * f3(u.sunRadiance[0], u.sunRadiance[1], u.sunRadiance[2]);
+    b.R2[g] = make_float4(l.x, l.y, l.z, 1e4f);
+    flags |= kFlagShadow;
+    rays.shadow = true;
+  }
+  // light-list NEE: the candidate RIS of emissiveNEE; its shadow ray pending
+  F3 neeC = f3(0.0f, 0.0f, 0.0f);
+  if (u.params2[1] > 0u) {
+    const uint32_t nCand = emissive_cand_count(u, v);
+    const float invM = 1.0f / (float)nCand;
+    float wSum = 0.0f, selLum = 0.0f, selR2 = 0.0f;
+    F3 sel = f3(0.0f, 0.0f, 0.0f), selDir = sel;
+    for (uint32_t k = 0u; k < nCand; k++) {
+      const LightPoint lp = sample_light_face(R, pos, rng);
+      const F3 d = lp.pos - surf;
+      const float r2 = fmax_(dot3(d, d), 1e-6f);
+      const F3 dir = d * (1.0f / __fsqrt_rn(r2));
+      const float cos1 = dot3(n, dir);
+      const float cos2 = dot3(lp.n, f3(-dir.x, -dir.y, -dir.z));
+      if (cos1 <= 0.0f || cos2 <= 0.0f) continue;
+      const F3 a = ((mat.albedo * kInvPi) * cos1) * cos2;
+      const F3 vv =
+          f3((a.x / r2) * lp.Le.x / lp.pdfA, (a.y / r2) * lp.Le.y / lp.pdfA, (a.z / r2) * lp.Le.z / lp.pdfA);
+      const float w = rlum(vv) * invM;
+      if (w <= 0.0f) continue;
+      const bool first = wSum == 0.0f;
+      wSum = wSum + w;
+      if (first || rand_(rng) * wSum < w) {
+        sel = vv;
+        selLum = rlum(vv);
+        selDir = dir;
+        selR2 = r2;
+      }
+    }
+    if (wSum > 0.0f) {
+      neeC = tp * (sel * (wSum / selLum));
+      b.R3[g] = make_float4(selDir.x, selDir.y, selDir.z, __fsqrt_rn(selR2) - 2e-3f);
+      flags |= kFlagShadow2;
+      rays.shadow2 = true;
+    }
+  }
+  if (v == nB) {
+    flags |= kFlagTerminal;
+  } else {
+    const F3 rd = cosine_hemisphere(n, rng);
+    tp = tp * mat.albedo;
+    bool alive = true;
+    if (v >= 2u) {
+      const float p = clamp_(fmax_(tp.x, fmax_(tp.y, tp.z)), 0.05f, 0.95f);
+      if (rand_(rng) > p) alive = false;
+      else tp = f3(tp.x / p, tp.y / p, tp.z / p);
+    }
+    if (alive) {
+      b.R1[g] = make_float4(rd.x, rd.y, rd.z, 1e4f);
+      rays.bounce = true;
+    } else {
+      flags |= kFlagTerminal;
+    }
+  }
+  b.R0[g] = make_float4(surf.x, surf.y, surf.z, 0.0f);
+  b.S0[g] = make_float4(Lo.x, Lo.y, Lo.z, __uint_as_float(rng));
+  b.S1[g] = make_float4(tp.x, tp.y, tp.z, 0.0f);
+  b.S2[g] = make_float4(sunc.x, sunc.y, sunc.z, __uint_as_float(flags));
+  r.aux[g] = make_float4(neeC.x, neeC.y, neeC.z, 0.0f);
+  return rays.shadow || rays.shadow2 || rays.bounce;
+}
+
+// The end of estimateLo: the bounce candidate at x2, then the final RIS.
+VRT_DI void lo_finish(const RestirDev& R, const RestirWf& r, uint32_t g, F3 Lo, uint32_t bits, uint32_t& rng) {
+  F3 x1, n1, surf1;
+  x1_of(R, g, x1, n1, surf1);
+  const float4 x2c = r.x2[g];
+  RSample s;
+  float Wc;
+  cand_point(x1, n1, xyz(x2c), normal_decode(bits_get(bits, 0, 6)), fclamp3(R, fclamp3(R, Lo)), s, Wc);
+  Ris ris = ris_load(r, g, bits);
+  const float pt = eval_target(s, x1, n1);
+  ris.add(s, pt, pt * Wc, rng);
+  unified_finish(R, g, ris);
+}
+
+__global__ void __launch_bounds__(256) k_wf_unified_primary(const __grid_constant__ RestirDev R, RestirWf r,
+                                                            uint32_t P, WfDev b) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  if (R.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(R.stats + kStatPixels, (unsigned long long)P);
+  const Uni& u = R.u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P; base += stride) {
+    const uint32_t g = base + threadIdx.x;
+    URays rays;
+    if (g < P) {
+      const uint4 h = b.hit[g];
+      const F3 rd = xyz(b.R1[g]);
+      const float t = __uint_as_float(h.x);
+      if (t < 0.0f) {
+        const F3 sky = sky_color(u, rd, true);
+        const uint2 sk = pack_h4(sky.x, sky.y, sky.z, 1.0f);
+        R.rad16[g] = sk;
+        if (R.rad32) R.rad32[g] = make_float4(sky.x, sky.y, sky.z, 1.0f);
+        R.direct[g] = sk;
+        R.alb8[g] = 0xffffffffu;
+        R.gbuf[g] = make_float4(-rd.x, -rd.y, -rd.z, -1.0f);
+        R.resA[2 * (size_t)g] = make_uint4(0u, 0u, 0u, 0u);
+        R.resA[2 * (size_t)g + 1] = make_uint4(0u, 0u, 0u, 0u);
+      } else {
+        const Mat mat1 = unpack_material(h.y);
+        const F3 x1 = f3(u.camPos[0], u.camPos[1], u.camPos[2]) + rd * t;
+        const F3 n1 = hit_normal((int)h.z, rd);
+        R.alb8[g] = unorm8_(__fsqrt_rn(mat1.albedo.x)) | (unorm8_(__fsqrt_rn(mat1.albedo.y)) << 8) |
+                    (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
+        R.gbuf[g] = make_float4(n1.x, n1.y, n1.z, t);
+        const float em = mat1.emissive * kEmissiveScale;   // unified: the sun goes through the reservoir
+        R.direct[g] = pack_h4(em, em, em, 1.0f);
+        uint32_t rng = __float_as_uint(b.S0[g].w);
+        const F3 surf1 = x1 + n1 * fmax_(1e-3f, t * 1e-4f);
+        Ris ris;
+        ris.sel = null_sample(0.0f);
+        uint32_t bits = 0u;
+        const F3 l = sample_sun_dir(u, rng);
+        const float ndl = dot3(n1, l);
+        if (ndl > 0.0f && l.y > 0.0f) {   // sun-cone shadow ray first
+          b.R0[g] = make_float4(surf1.x, surf1.y, surf1.z, 0.0f);
+          b.R2[g] = make_float4(l.x, l.y, l.z, 1e4f);
+          ris_save(r, g, ris, bits);
+          b.S0[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
+          r.x2[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(bits_set(bits, 14, 2, kStSun)));
+          rays.shadow = true;
+        } else {
+          x1_run(R, r, b, g, kStLight, ris, bits, rng, x1, n1, surf1, rays);
+        }
+      }
+    }
+    const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
+    emit2(b, 1, g, rays.shadow, rays.shadow2, rays.bounce, keep);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wf_unified_wave(const __grid_constant__ RestirDev R, RestirWf r, WfDev b,
+                                                         int wave) {
+  const int n = b.ctr[4 * wave + 2];
+  const uint32_t* list = active_of(b, wave);
+  const Uni& u = R.u;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int i = base + threadIdx.x;
+    URays rays;
+    uint32_t g = 0u;
+    if (i < n) {
+      g = list[i];
+      const float4 s0 = b.S0[g];
+      uint32_t rng = __float_as_uint(s0.w);
+      uint32_t bits = __float_as_uint(r.x2[g].w);
+      const uint32_t st = bits_get(bits, 14, 2);
+      const uint4 h = b.hit[g];
+      if (st != kStLo) {
+        F3 x1, n1, surf1;
+        x1_of(R, g, x1, n1, surf1);
+        Ris ris = ris_load(r, g, bits);
+        if (st == kStSun) {   // the sun-cone shadow ray resolved
+          if (h.w == 0u) {
+            const float4 l = b.R2[g];
+            const float coneSA = kTwoPi * (1.0f - u.sunDir[3]);
+            RSample s = null_sample(0.0f);
+            s.kind = kSkDir;
+            s.pos = f3(l.x, l.y, l.z);
+            const float den = fmax_(coneSA, 1e-5f);
+            s.rad = f3(u.sunRadiance[0] / den, u.sunRadiance[1] / den, u.sunRadiance[2] / den);
+            const float pt = eval_target(s, x1, n1);
+            ris.add(s, pt, pt * coneSA, rng);
+          }
+          x1_run(R, r, b, g, kStLight, ris, bits, rng, x1, n1, surf1, rays);
+        } else if (st == kStLight) {   // the light-list candidate's shadow ray resolved
+          if (h.w == 0u) {
+            const float4 a = r.aux[g], a2 = r.aux2[g];
+            RSample eSel = null_sample(0.0f);
+            eSel.kind = kSkPoint;
+            eSel.pos = f3(a.x, a.y, a.z);
+            eSel.n = normal_decode(bits_get(bits, 16, 6));
+            eSel.rad = f3(a2.x, a2.y, a2.z);
+            const float We = a.w / a2.w;
+            ris.add(eSel, a2.w, a2.w * We, rng);
+          }
+          x1_run(R, r, b, g, kStBounce, ris, bits, rng, x1, n1, surf1, rays);
+        } else {   // the bounce ray resolved: x2, or a sky direction candidate
+          const F3 brd = xyz(b.R1[g]);
+          const float t = __uint_as_float(h.x);
+          if (t < 0.0f) {
+            RSample s;
+            float Wc;
+            cand_dir(u, n1, brd, s, Wc);
+            const float pt = eval_target(s, x1, n1);
+            ris.add(s, pt, pt * Wc, rng);
+            unified_finish(R, g, ris);
+          } else {
+            const F3 x2 = surf1 + brd * t;
+            const F3 n2 = hit_normal((int)h.z, brd);
+            bits = bits_set(bits, 0, 6, normal_code(n2));
+            bits = bits_set(bits, 14, 2, kStLo);
+            bits = bits_set(bits, 22, 8, 1u);
+            ris_save(r, g, ris, bits);
+            r.x2[g] = make_float4(x2.x, x2.y, x2.z, __uint_as_float(bits));
+            if (!lo_vertex(R, b, r, g, 1u, x2, n2, unpack_material(h.y), f3(0.0f, 0.0f, 0.0f),
+                           f3(1.0f, 1.0f, 1.0f), rng, rays))
+              lo_finish(R, r, g, f3(0.0f, 0.0f, 0.0f), bits, rng);
+          }
+        }
+      } else {   // estimateLo vertex (wave - 3) resolved: shadows, then the bounce hit
+        const float4 s1 = b.S1[g], s2 = b.S2[g];
+        const uint32_t flags = __float_as_uint(s2.w);
+        F3 Lo = xyz(s0), tp = xyz(s1);
+        if ((flags & kFlagShadow) && h.w == 0u) Lo = Lo + xyz(s2);
+        if ((flags & kFlagShadow2) && b.occ2[g] == 0u) Lo = Lo + xyz(r.aux[g]);
+        bool done = (flags & kFlagTerminal) != 0u;
+        if (!done) {
+          const F3 rd = xyz(b.R1[g]);
+          const float t = __uint_as_float(h.x);
+          if (t < 0.0f) {
+            Lo = Lo + tp * sky_color(u, rd, false);
+            done = true;
+          } else {
+            const uint32_t v = bits_get(bits, 22, 8) + 1u;
+            bits = bits_set(bits, 22, 8, v);
+            const float4 x2c = r.x2[g];
+            r.x2[g] = make_float4(x2c.x, x2c.y, x2c.z, __uint_as_float(bits));
+            const F3 pos = xyz(b.R0[g]) + rd * t;
+            done = !lo_vertex(R, b, r, g, v, pos, hit_normal((int)h.z, rd), unpack_material(h.y), Lo, tp, rng, rays);
+          }
+        }
+        if (done) lo_finish(R, r, g, Lo, bits, rng);
+      }
+    }
+    const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
+    emit2(b, wave + 1, g, rays.shadow, rays.shadow2, rays.bounce, keep);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
 static RestirDev restir_dev(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H, const PathOut& out,
@@ -1260,7 +1628,7 @@ cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms
                                             const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
                                             cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
   const SingleJob job = restir_job(s, uu, fclamp, W, H, out);
-  const RestirWf r{(uint4*)rb.resA, (uint2*)rb.direct, (float4*)rb.scratch, W, H};
+  const RestirWf r{(uint4*)rb.resA, (uint2*)rb.direct, (float4*)rb.scratch, W, H, nullptr, nullptr, nullptr, nullptr};
   const uint32_t P = (uint32_t)W * (uint32_t)H;
   const int smem = occ_smem(s);
   unsigned long long* stats = out.stats;
@@ -1268,6 +1636,26 @@ cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms
                       max_timed_waves, timed_waves, [&](const WfDev& b, int w, int sblocks) {
                         if (w == 0) k_wf_restir_primary<<<sblocks, 256, 0, st>>>(job, r, P, b, stats);
                         else k_wf_restir_wave<<<sblocks, 256, 0, st>>>(job, r, b, w);
+                        return cudaGetLastError();
+                      });
+}
+
+cudaError_t launch_restir_unified_wavefront(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H,
+                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
+                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves) {
+  const SingleJob job = restir_job(s, uu, fclamp, W, H, out);
+  const RestirDev R = restir_dev(s, uu, fclamp, W, H, out, rb);
+  const uint32_t P = (uint32_t)W * (uint32_t)H;
+  float4* sc = (float4*)rb.scratch;
+  const RestirWf r{(uint4*)rb.resA, (uint2*)rb.direct, sc, W, H, sc + P, sc + 2 * (size_t)P, sc + 3 * (size_t)P,
+                   sc + 4 * (size_t)P};
+  const int smem = occ_smem(s);
+  // x1's three sequential rays, then one wave per estimateLo vertex
+  return wf_run_waves(job, P, (int)job.u.params0[1] + 4, smem, wb, tune, out.stats, st, launches, trace_ev,
+                      max_timed_waves, timed_waves, [&](const WfDev& b, int w, int sblocks) {
+                        if (w == 0) k_wf_unified_primary<<<sblocks, 256, 0, st>>>(R, r, P, b);
+                        else k_wf_unified_wave<<<sblocks, 256, 0, st>>>(R, r, b, w);
                         return cudaGetLastError();
                       });
 }

@@ -31,7 +31,19 @@ namespace vrt {
 
 size_t wavefront_bytes(int W, int H, int max_waves) {
   const size_t P = (size_t)W * H;
-  return P * 16 * 7 + P * 4 * 2 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
+  return P * 16 * 8 + P * 12 * 2 + P * 4 * 2 + P * 4 + (size_t)max_waves * 16;
+}
+
+void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb) {
+  char* m = (char*)mem;
+  void** f4[8] = {&wb.R0, &wb.R1, &wb.R2, &wb.R3, &wb.S0, &wb.S1, &wb.S2, &wb.hit};
+  for (auto* f : f4) { *f = m; m += P * 16; }
+  for (int i = 0; i < 2; i++) { wb.q[i] = (uint32_t*)m; m += P * 12; }
+  for (int i = 0; i < 2; i++) { wb.act[i] = (uint32_t*)m; m += P * 4; }
+  wb.occ2 = (uint32_t*)m;
+  m += P * 4;
+  wb.ctr = (int*)m;
+  wb.max_waves = max_waves;
 }
 
 static SingleJob make_job(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H, const PathOut& out) {

@@ -457,15 +457,7 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
     const int max_waves = kMaxWaves;
     s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves);
     r = dev_alloc(ctx, &s->wf_mem, s->wf_bytes, &s->bytes);
-    if (!r) {
-      char* m = (char*)s->wf_mem;
-      void** f4[7] = {&s->wf.R0, &s->wf.R1, &s->wf.R2, &s->wf.S0, &s->wf.S1, &s->wf.S2, &s->wf.hit};
-      for (auto* f : f4) { *f = m; m += P * 16; }
-      for (int i = 0; i < 2; i++) { s->wf.q[i] = (uint32_t*)m; m += P * 8; }
-      for (int i = 0; i < 2; i++) { s->wf.act[i] = (uint32_t*)m; m += P * 4; }
-      s->wf.ctr = (int*)m;
-      s->wf.max_waves = max_waves;
-    }
+    if (!r) carve_wavefront(s->wf_mem, P, max_waves, s->wf);
   }
   if (!r) {
     for (auto& e : s->ev) {
@@ -590,7 +582,7 @@ static int check_uniforms(const VrtSession* s, const VrtUniforms* u) {
 // Reservoir buffers of the session, allocated (zeroed) on first use.
 static int ensure_restir(VrtSession* s) {
   if (s->restir_mem) return VRT_OK;
-  const size_t bytes = px(s) * (32 + 32 + 16 + 8 + 4);
+  const size_t bytes = px(s) * (32 + 32 + 80 + 8 + 4);
   if (int r = dev_alloc(s->ctx, &s->restir_mem, bytes, &s->bytes)) return r;
   s->restir_bytes = bytes;
   CUDA_TRY(cudaMemsetAsync(s->restir_mem, 0, bytes, s->ctx->stream));
@@ -603,8 +595,8 @@ static RestirBufs restir_bufs(const VrtSession* s, int parity) {
   rb.resA = m;
   rb.resB = m + px(s) * 32;
   rb.scratch = m + px(s) * 64;   // 16-byte records before the 8- and 4-byte ones:
-  rb.direct = m + px(s) * 80;    // every region starts on its own alignment for any P
-  rb.dup = (float*)(m + px(s) * 88);
+  rb.direct = m + px(s) * 144;   // every region starts on its own alignment for any P
+  rb.dup = (float*)(m + px(s) * 152);
   rb.gbuf_prev = s->gbuf[1 - parity];
   rb.pairing = s->pairing;
   const VrtScene* sc = s->scene;
@@ -662,9 +654,13 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
     if (int r = ensure_restir(s)) return r;
     if (int r = ensure_lights(s, u)) return r;
     const RestirBufs rb = restir_bufs(s, parity_of(s));
-    // unified NEE adds a second shadow ray per vertex: the per-pixel kernel
-    if (s->path_kernel == VRT_PATH_WAVEFRONT && !(u->params2[0] & kRfUnified) &&
-        (int)u->params0[1] + 3 <= s->wf.max_waves) {
+    if (s->path_kernel == VRT_PATH_WAVEFRONT && (u->params2[0] & kRfUnified) &&
+        (int)u->params0[1] + 5 <= s->wf.max_waves) {
+      CUDA_TRY(launch_restir_unified_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
+                                               s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,
+                                               VrtSession::kTimedWaves, &s->timed_waves));
+    } else if (s->path_kernel == VRT_PATH_WAVEFRONT && !(u->params2[0] & kRfUnified) &&
+               (int)u->params0[1] + 3 <= s->wf.max_waves) {
       CUDA_TRY(launch_restir_initial_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
                                                s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,
                                                VrtSession::kTimedWaves, &s->timed_waves));
@@ -906,11 +902,11 @@ int vrt_read_reservoirs(VrtSession* s, int which, void* h, size_t b) {
 }
 int vrt_read_dupmap(VrtSession* s, void* h, size_t b) {
   if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
-  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 88 : nullptr, s ? px(s) * 4 : 0, h, b);
+  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 152 : nullptr, s ? px(s) * 4 : 0, h, b);
 }
 int vrt_read_direct(VrtSession* s, void* h, size_t b) {
   if (s && !s->restir_mem) return fail(VRT_ERR_STATE, "no ReSTIR frame rendered by this session");
-  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 80 : nullptr, s ? px(s) * 8 : 0, h, b);
+  return read_buf(s, s ? (const char*)s->restir_mem + px(s) * 144 : nullptr, s ? px(s) * 8 : 0, h, b);
 }
 
 static float half_to_float(uint16_t hbits) {
@@ -1049,14 +1045,7 @@ int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch**
     g_err = keep;
     return r;
   }
-  const size_t Pz = b->P;
-  char* m = (char*)b->wf_mem;
-  void** f4[7] = {&b->wf.R0, &b->wf.R1, &b->wf.R2, &b->wf.S0, &b->wf.S1, &b->wf.S2, &b->wf.hit};
-  for (auto* f : f4) { *f = m; m += Pz * 16; }
-  for (int i = 0; i < 2; i++) { b->wf.q[i] = (uint32_t*)m; m += Pz * 8; }
-  for (int i = 0; i < 2; i++) { b->wf.act[i] = (uint32_t*)m; m += Pz * 4; }
-  b->wf.ctr = (int*)m;
-  b->wf.max_waves = max_waves;
+  carve_wavefront(b->wf_mem, b->P, max_waves, b->wf);
   std::vector<uint32_t> firsts((size_t)n);
   uint32_t acc = 0;
   for (int i = 0; i < n; i++) { firsts[(size_t)i] = acc; acc += (uint32_t)(sessions[i]->W * sessions[i]->H); }

@@ -38,10 +38,12 @@ struct PathOut {
 // allocation): per-pixel path state, ray queues, active lists, counters.
 struct WavefrontBufs {
   void *R0 = nullptr, *R1 = nullptr, *R2 = nullptr;   // float4 per pixel
+  void* R3 = nullptr;                                 // float4 per pixel: a path's second shadow ray
   void *S0 = nullptr, *S1 = nullptr, *S2 = nullptr;   // float4 per pixel
   void* hit = nullptr;                                // uint4 per pixel
-  uint32_t* q[2] = {nullptr, nullptr};                // 2P entries each
+  uint32_t* q[2] = {nullptr, nullptr};                // 3P entries each
   uint32_t* act[2] = {nullptr, nullptr};              // P entries each
+  uint32_t* occ2 = nullptr;                           // P: second shadow ray's result
   int* ctr = nullptr;                                 // 4 ints per wave
   int max_waves = 0;
 };
@@ -198,6 +200,8 @@ cudaError_t launch_light_grid(int N, const uint32_t* words, const double* weight
 int set_error(int code, const char* msg);
 
 size_t wavefront_bytes(int W, int H, int max_waves);
+// Lays the wavefront scratch of P pixels out in mem (wavefront_bytes(P, 1, max_waves) bytes).
+void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb);
 // When trace_ev is non-null, events trace_ev[2w], trace_ev[2w+1] bracket the
 // trace kernel of wave w (w < max_timed_waves); *timed_waves receives the count.
 // cache (may be null): cache-assisted frame (training + query paths),
@@ -257,7 +261,7 @@ struct RestirBufs {
   void* resB = nullptr;             // post-spatial = next frame's history
   void* direct = nullptr;           // rgba16f
   const void* gbuf_prev = nullptr;  // previous frame's G-buffer
-  void* scratch = nullptr;          // 16 B per pixel: wavefront path state (x2)
+  void* scratch = nullptr;          // 80 B per pixel: wavefront path state (x2, RIS state)
   float* dup = nullptr;             // duplication score per pixel (dupmap.wgsl)
   const uint32_t* pairing = nullptr;      // kPairingWords (RF_PAIRED)
   const uint32_t* light_words = nullptr;  // 2 per light (RF_UNIFIED)
@@ -268,6 +272,11 @@ cudaError_t launch_restir_initial(const SceneDev& s, const VrtUniforms& u, float
                                   const PathOut& out, const RestirBufs& rb, cudaStream_t st);
 // The initial pass on the wavefront tracer (bit-identical to launch_restir_initial).
 cudaError_t launch_restir_initial_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
+                                            const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
+                                            const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
+                                            cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves);
+// The unified (RF_UNIFIED) initial pass on the wavefront tracer.
+cudaError_t launch_restir_unified_wavefront(const SceneDev& s, const VrtUniforms& u, float fclamp, int W, int H,
                                             const PathOut& out, const RestirBufs& rb, const WavefrontBufs& wb,
                                             const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches,
                                             cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves);

@@ -14,20 +14,25 @@ namespace vrt {
 constexpr uint32_t kFlagShadow = 1u;     // a shadow ray of the previous vertex is pending
 constexpr uint32_t kFlagTerminal = 2u;   // no bounce ray: finalize after the shadow ray
 constexpr uint32_t kShadowBit = 0x80000000u;
+constexpr uint32_t kShadow2Bit = 0x40000000u;   // with kShadowBit: the path's second shadow ray (R3, occ2)
+constexpr uint32_t kEntryIndex = 0x3fffffffu;   // path index of a queue entry
+constexpr uint32_t kFlagShadow2 = 4u;           // a second shadow ray of the previous vertex is pending
 
 struct WfDev {
   float4* R0;      // ray origin: camera position (primary) or surf = pos + n*1e-3
   float4* R1;      // primary / bounce direction
   float4* R2;      // direction (xyz) and maxT (w) of the pending shadow ray
+  float4* R3;      // direction and maxT of a second pending shadow ray (same origin R0)
   float4* S0;      // radiance xyz, w = RNG state bits
   float4* S1;      // throughput xyz, w = primary material bits
   float4* S2;      // pending sun contribution xyz, w = flags
   uint4* hit;      // x = t bits, y = material, z = entry axis, w = shadow occluded
-  uint32_t* q0;    // ray queues (entry = pixel | kShadowBit for shadow rays), capacity 2P
+  uint32_t* q0;    // ray queues (entry = pixel | kShadowBit [| kShadow2Bit] for shadow rays), capacity 3P
   uint32_t* q1;
   uint32_t* a0;    // active path lists, capacity P
   uint32_t* a1;
   int* ctr;        // per wave k: [4k] queue count, [4k+1] queue head, [4k+2] active count
+  uint32_t* occ2;  // result of the second shadow ray (1 = occluded)
 };
 
 VRT_DI uint32_t* queue_of(const WfDev& b, int wave) { return (wave & 1) ? b.q1 : b.q0; }
@@ -465,6 +470,15 @@ VRT_DI void emit(const WfDev& b, int next, uint32_t g, bool shadow, bool bounce,
   if (keep) a[s3] = g;
 }
 
+// emit() with a second shadow ray (R3) of the path.
+VRT_DI void emit2(const WfDev& b, int next, uint32_t g, bool shadow, bool shadow2, bool bounce, bool keep) {
+  uint32_t* q = queue_of(b, next);
+  int* c = b.ctr + 4 * next;
+  const uint32_t s0 = warp_append(c, shadow2);
+  if (shadow2) q[s0] = g | kShadowBit | kShadow2Bit;
+  emit(b, next, g, shadow, bounce, keep);
+}
+
 // ---------------------------------------------------------------------------
 // kernels (templated on the job policy)
 // ---------------------------------------------------------------------------
@@ -525,12 +539,12 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
         const int slot = base + __popc(idle & ((1u << lane) - 1u));
         if (slot < n) {
           entry = implicit_n > 0 ? (uint32_t)slot : queue[slot];
-          const uint32_t g = entry & ~kShadowBit;
+          const uint32_t g = entry & kEntryIndex;
           S = jobs.scene(jobs.job_of(g));
           const F3 ro = xyz(b.R0[g]);
-          float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w
+          float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w / R3.w
           if (entry & kShadowBit) {
-            const float4 r2 = b.R2[g];
+            const float4 r2 = (entry & kShadow2Bit) ? b.R3[g] : b.R2[g];
             rd = xyz(r2);
             maxT = r2.w;
           } else {
@@ -551,9 +565,11 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       for (int k = 0; k < kSteps; k++)
         if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
-        const uint32_t g = entry & ~kShadowBit;
+        const uint32_t g = entry & kEntryIndex;
         uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + g);
-        if (entry & kShadowBit) {
+        if (entry & kShadow2Bit) {
+          b.occ2[g] = d.tHit >= 0.0f ? 1u : 0u;
+        } else if (entry & kShadowBit) {
           h[3] = d.tHit >= 0.0f ? 1u : 0u;
         } else {
           *reinterpret_cast<uint2*>(h) = make_uint2(__float_as_uint(d.tHit), d.mat);
@@ -762,7 +778,8 @@ __global__ void __launch_bounds__(256) k_cache_resolve(J jobs, WfDev b, const __
 // ---------------------------------------------------------------------------
 inline WfDev wf_view(const WavefrontBufs& w) {
   WfDev d;
-  d.R0 = (float4*)w.R0; d.R1 = (float4*)w.R1; d.R2 = (float4*)w.R2;
+  d.R0 = (float4*)w.R0; d.R1 = (float4*)w.R1; d.R2 = (float4*)w.R2; d.R3 = (float4*)w.R3;
+  d.occ2 = w.occ2;
   d.S0 = (float4*)w.S0; d.S1 = (float4*)w.S1; d.S2 = (float4*)w.S2;
   d.hit = (uint4*)w.hit;
   d.q0 = w.q[0]; d.q1 = w.q[1]; d.a0 = w.act[0]; d.a1 = w.act[1];
