@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--cache", action="store_true", help="serve: also run the sweep with the cache-assisted path")
+    ap.add_argument("--runs", default="", help="restir: comma-separated subset of plain,gi,ours,ours_b6_nodenoise")
     return ap.parse_args()
 
 
@@ -1051,7 +1052,8 @@ def run_restir(args, local):
                                  preset=preset, light_count=nlights)
 
     res, clk = {}, None
-    for label, preset, bounces, flags in RESTIR_RUNS:
+    runs = [r for r in RESTIR_RUNS if not args.runs or r[0] in args.runs.split(",")]
+    for label, preset, bounces, flags in runs:
         sess.reset()
         for i in range(args.warmup):
             sess.frame(uni(i, preset, bounces, flags))
@@ -1072,7 +1074,7 @@ def run_restir(args, local):
             launches += st.launches
         ctx.synchronize()
         c = clocks.stop()
-        if label == RESTIR_RUNS[-1][0]:
+        if label == runs[-1][0]:
             clk = c
         res[label] = {"preset": preset, "bounces": bounces, "denoise": bool(flags & 2),
                       "frame_ms_mean": round(statistics.mean(fm), 4), "frame_ms_p50": round(statistics.median(fm), 4),
@@ -1084,7 +1086,7 @@ def run_restir(args, local):
     sess.close()
     scene.close()
     ctx.close()
-    head = res[RESTIR_RUNS[-1][0]]
+    head = res[runs[-1][0]]
     line = {
         "metric": "ReSTIR `ours` frame ms at 1080p, 6 bounces, denoiser off (initial + reuse + temporal + present)",
         "value": head["frame_ms_mean"], "unit": "ms/frame", "n_gpus": 1, "steps": args.steps,

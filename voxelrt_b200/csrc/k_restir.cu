@@ -935,7 +935,7 @@ __global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_con
   const int n = b.ctr[4 * wave];
   const uint32_t* q = queue_of(b, wave);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t g = q[i] & kEntryIndex;
+    const uint32_t g = q[i] & ~kShadowBit;
     const bool vis = b.hit[g].w == 0u;
     const float4 c = b.S1[g];
     out_radiance(R, g, load_direct(R, g) + clamp_contrib(R.u, vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
@@ -1353,7 +1353,9 @@ VRT_DI bool lo_vertex(const RestirDev& R, const WfDev& b, const RestirWf& r, uin
     }
     if (wSum > 0.0f) {
       neeC = tp * (sel * (wSum / selLum));
-      b.R3[g] = make_float4(selDir.x, selDir.y, selDir.z, __fsqrt_rn(selR2) - 2e-3f);
+      const uint32_t g2 = g + (uint32_t)r.W * (uint32_t)r.H;   // the second shadow ray's path index
+      b.R0[g2] = make_float4(surf.x, surf.y, surf.z, 0.0f);
+      b.R2[g2] = make_float4(selDir.x, selDir.y, selDir.z, __fsqrt_rn(selR2) - 2e-3f);
       flags |= kFlagShadow2;
       rays.shadow2 = true;
     }
@@ -1449,7 +1451,7 @@ __global__ void __launch_bounds__(256) k_wf_unified_primary(const __grid_constan
       }
     }
     const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
-    emit2(b, 1, g, rays.shadow, rays.shadow2, rays.bounce, keep);
+    emit2(b, 1, g, P, rays.shadow, rays.shadow2, rays.bounce, keep);
   }
 }
 
@@ -1527,7 +1529,7 @@ __global__ void __launch_bounds__(256) k_wf_unified_wave(const __grid_constant__
         const uint32_t flags = __float_as_uint(s2.w);
         F3 Lo = xyz(s0), tp = xyz(s1);
         if ((flags & kFlagShadow) && h.w == 0u) Lo = Lo + xyz(s2);
-        if ((flags & kFlagShadow2) && b.occ2[g] == 0u) Lo = Lo + xyz(r.aux[g]);
+        if ((flags & kFlagShadow2) && b.hit[g + (uint32_t)r.W * (uint32_t)r.H].w == 0u) Lo = Lo + xyz(r.aux[g]);
         bool done = (flags & kFlagTerminal) != 0u;
         if (!done) {
           const F3 rd = xyz(b.R1[g]);
@@ -1548,7 +1550,7 @@ __global__ void __launch_bounds__(256) k_wf_unified_wave(const __grid_constant__
       }
     }
     const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
-    emit2(b, wave + 1, g, rays.shadow, rays.shadow2, rays.bounce, keep);
+    emit2(b, wave + 1, g, (uint32_t)r.W * (uint32_t)r.H, rays.shadow, rays.shadow2, rays.bounce, keep);
   }
 }
 
@@ -1652,12 +1654,13 @@ cudaError_t launch_restir_unified_wavefront(const SceneDev& s, const VrtUniforms
                    sc + 4 * (size_t)P};
   const int smem = occ_smem(s);
   // x1's three sequential rays, then one wave per estimateLo vertex
-  return wf_run_waves(job, P, (int)job.u.params0[1] + 4, smem, wb, tune, out.stats, st, launches, trace_ev,
-                      max_timed_waves, timed_waves, [&](const WfDev& b, int w, int sblocks) {
-                        if (w == 0) k_wf_unified_primary<<<sblocks, 256, 0, st>>>(R, r, P, b);
-                        else k_wf_unified_wave<<<sblocks, 256, 0, st>>>(R, r, b, w);
-                        return cudaGetLastError();
-                      });
+  auto shade = [&](const WfDev& b, int w, int sblocks) {
+    if (w == 0) k_wf_unified_primary<<<sblocks, 256, 0, st>>>(R, r, P, b);
+    else k_wf_unified_wave<<<sblocks, 256, 0, st>>>(R, r, b, w);
+    return cudaGetLastError();
+  };
+  return wf_run_waves<SingleJob, decltype(shade), true>(job, P, (int)job.u.params0[1] + 4, smem, wb, tune, out.stats,
+                                                        st, launches, trace_ev, max_timed_waves, timed_waves, shade);
 }
 
 cudaError_t launch_restir_temporal(const SceneDev& s, const VrtUniforms& u, int W, int H, const PathOut& out,
@@ -1696,11 +1699,11 @@ cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms
   const int smem = occ_smem(s);
   const int refill = tune.refill_min > 0 ? tune.refill_min : 8;
   if (smem > 0)
-    e = wf_dispatch_trace<SingleJob, true>(tune.trace_variant, job, smem, tune.trace_blocks_per_sm, sms, b, wave, 0,
-                                           refill, out.stats, st);
+    e = wf_dispatch_trace<SingleJob, true, true>(tune.trace_variant, job, smem, tune.trace_blocks_per_sm, sms, b, wave,
+                                                 0, refill, out.stats, st);
   else
-    e = wf_dispatch_trace<SingleJob, false>(tune.trace_variant, job, 0, tune.trace_blocks_per_sm, sms, b, wave, 0,
-                                            refill, out.stats, st);
+    e = wf_dispatch_trace<SingleJob, false, true>(tune.trace_variant, job, 0, tune.trace_blocks_per_sm, sms, b, wave,
+                                                  0, refill, out.stats, st);
   if (e != cudaSuccess) return e;
   k_restir_spatial_resolve<<<sms * 8, 256, 0, st>>>(R, b, wave);
   if (launches) *launches += 3;

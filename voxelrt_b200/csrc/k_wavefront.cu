@@ -29,21 +29,25 @@
 
 namespace vrt {
 
-size_t wavefront_bytes(int W, int H, int max_waves) {
+size_t wavefront_bytes(int W, int H, int max_waves, bool dual) {
   const size_t P = (size_t)W * H;
-  return P * 16 * 8 + P * 12 * 2 + P * 4 * 2 + P * 4 + (size_t)max_waves * 16;
+  return P * 16 * (dual ? 10 : 7) + P * 12 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
 }
 
-void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb) {
+void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, bool dual) {
   char* m = (char*)mem;
-  void** f4[8] = {&wb.R0, &wb.R1, &wb.R2, &wb.R3, &wb.S0, &wb.S1, &wb.S2, &wb.hit};
-  for (auto* f : f4) { *f = m; m += P * 16; }
+  const size_t big = dual ? 2 * P : P;
+  void** f4[7] = {&wb.R0, &wb.R1, &wb.R2, &wb.S0, &wb.S1, &wb.S2, &wb.hit};
+  for (auto* f : f4) {
+    const bool twice = f == &wb.R0 || f == &wb.R2 || f == &wb.hit;
+    *f = m;
+    m += (twice ? big : P) * 16;
+  }
   for (int i = 0; i < 2; i++) { wb.q[i] = (uint32_t*)m; m += P * 12; }
   for (int i = 0; i < 2; i++) { wb.act[i] = (uint32_t*)m; m += P * 4; }
-  wb.occ2 = (uint32_t*)m;
-  m += P * 4;
   wb.ctr = (int*)m;
   wb.max_waves = max_waves;
+  wb.dual = dual;
 }
 
 static SingleJob make_job(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H, const PathOut& out) {

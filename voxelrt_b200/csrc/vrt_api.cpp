@@ -455,9 +455,9 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
                        ? cfg->path_kernel : VRT_PATH_WAVEFRONT;
   if (!r && s->path_kernel == VRT_PATH_WAVEFRONT) {
     const int max_waves = kMaxWaves;
-    s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves);
+    s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves, true);
     r = dev_alloc(ctx, &s->wf_mem, s->wf_bytes, &s->bytes);
-    if (!r) carve_wavefront(s->wf_mem, P, max_waves, s->wf);
+    if (!r) carve_wavefront(s->wf_mem, P, max_waves, s->wf, true);
   }
   if (!r) {
     for (auto& e : s->ev) {
@@ -654,7 +654,7 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
     if (int r = ensure_restir(s)) return r;
     if (int r = ensure_lights(s, u)) return r;
     const RestirBufs rb = restir_bufs(s, parity_of(s));
-    if (s->path_kernel == VRT_PATH_WAVEFRONT && (u->params2[0] & kRfUnified) &&
+    if (s->path_kernel == VRT_PATH_WAVEFRONT && (u->params2[0] & kRfUnified) && s->wf.dual &&
         (int)u->params0[1] + 5 <= s->wf.max_waves) {
       CUDA_TRY(launch_restir_unified_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
                                                s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,

@@ -14,25 +14,22 @@ namespace vrt {
 constexpr uint32_t kFlagShadow = 1u;     // a shadow ray of the previous vertex is pending
 constexpr uint32_t kFlagTerminal = 2u;   // no bounce ray: finalize after the shadow ray
 constexpr uint32_t kShadowBit = 0x80000000u;
-constexpr uint32_t kShadow2Bit = 0x40000000u;   // with kShadowBit: the path's second shadow ray (R3, occ2)
-constexpr uint32_t kEntryIndex = 0x3fffffffu;   // path index of a queue entry
 constexpr uint32_t kFlagShadow2 = 4u;           // a second shadow ray of the previous vertex is pending
 
 struct WfDev {
   float4* R0;      // ray origin: camera position (primary) or surf = pos + n*1e-3
   float4* R1;      // primary / bounce direction
   float4* R2;      // direction (xyz) and maxT (w) of the pending shadow ray
-  float4* R3;      // direction and maxT of a second pending shadow ray (same origin R0)
   float4* S0;      // radiance xyz, w = RNG state bits
   float4* S1;      // throughput xyz, w = primary material bits
   float4* S2;      // pending sun contribution xyz, w = flags
   uint4* hit;      // x = t bits, y = material, z = entry axis, w = shadow occluded
-  uint32_t* q0;    // ray queues (entry = pixel | kShadowBit [| kShadow2Bit] for shadow rays), capacity 3P
+  uint32_t* q0;    // ray queues (entry = path | kShadowBit for shadow rays), capacity 3P; a path's second
+                   // shadow ray uses path index g + P (R0, R2 and hit hold 2P entries where it is used)
   uint32_t* q1;
   uint32_t* a0;    // active path lists, capacity P
   uint32_t* a1;
   int* ctr;        // per wave k: [4k] queue count, [4k+1] queue head, [4k+2] active count
-  uint32_t* occ2;  // result of the second shadow ray (1 = occluded)
 };
 
 VRT_DI uint32_t* queue_of(const WfDev& b, int wave) { return (wave & 1) ? b.q1 : b.q0; }
@@ -470,12 +467,13 @@ VRT_DI void emit(const WfDev& b, int next, uint32_t g, bool shadow, bool bounce,
   if (keep) a[s3] = g;
 }
 
-// emit() with a second shadow ray (R3) of the path.
-VRT_DI void emit2(const WfDev& b, int next, uint32_t g, bool shadow, bool shadow2, bool bounce, bool keep) {
+// emit() with a second shadow ray of the path, traced as path g + P.
+VRT_DI void emit2(const WfDev& b, int next, uint32_t g, uint32_t P, bool shadow, bool shadow2, bool bounce,
+                  bool keep) {
   uint32_t* q = queue_of(b, next);
   int* c = b.ctr + 4 * next;
   const uint32_t s0 = warp_append(c, shadow2);
-  if (shadow2) q[s0] = g | kShadowBit | kShadow2Bit;
+  if (shadow2) q[s0] = (g + P) | kShadowBit;
   emit(b, next, g, shadow, bounce, keep);
 }
 
@@ -505,8 +503,10 @@ __global__ void __launch_bounds__(256) k_wf_generate(J jobs, uint32_t P, WfDev b
 
 // Persistent queue tracer.  kSmem: stage the (single) scene's occupancy
 // bitmap in shared memory.  kSteps DDA iterations per pass of the warp
-// bookkeeping (idle-lane ballot, refill, drain check).
-template <class J, bool kSmem, int kSteps, int kMinB>
+// bookkeeping (idle-lane ballot, refill, drain check).  kVarMaxT: shadow rays
+// carry their own maxT in R2.w (otherwise every ray ends at 1e4 m, the plain
+// path's bound, and the tracer keeps its register budget).
+template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT>
 __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wave, int implicit_n,
                                                               int refill_min, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
@@ -539,19 +539,24 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
         const int slot = base + __popc(idle & ((1u << lane) - 1u));
         if (slot < n) {
           entry = implicit_n > 0 ? (uint32_t)slot : queue[slot];
-          const uint32_t g = entry & kEntryIndex;
+          const uint32_t g = entry & ~kShadowBit;
           S = jobs.scene(jobs.job_of(g));
           const F3 ro = xyz(b.R0[g]);
-          float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w / R3.w
-          if (entry & kShadowBit) {
-            const float4 r2 = (entry & kShadow2Bit) ? b.R3[g] : b.R2[g];
-            rd = xyz(r2);
-            maxT = r2.w;
+          if (kVarMaxT) {
+            float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w
+            if (entry & kShadowBit) {
+              const float4 r2 = b.R2[g];
+              rd = xyz(r2);
+              maxT = r2.w;
+            } else {
+              rd = xyz(b.R1[g]);
+            }
+            d.init(S, ro, rd, maxT);
           } else {
-            rd = xyz(b.R1[g]);
+            rd = (entry & kShadowBit) ? xyz(b.R2[g]) : xyz(b.R1[g]);
+            d.init(S, ro, rd, 1e4f);
           }
           c.rays++;
-          d.init(S, ro, rd, maxT);
           active = true;
         }
       }
@@ -565,11 +570,9 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       for (int k = 0; k < kSteps; k++)
         if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
-        const uint32_t g = entry & kEntryIndex;
+        const uint32_t g = entry & ~kShadowBit;
         uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + g);
-        if (entry & kShadow2Bit) {
-          b.occ2[g] = d.tHit >= 0.0f ? 1u : 0u;
-        } else if (entry & kShadowBit) {
+        if (entry & kShadowBit) {
           h[3] = d.tHit >= 0.0f ? 1u : 0u;
         } else {
           *reinterpret_cast<uint2*>(h) = make_uint2(__float_as_uint(d.tHit), d.mat);
@@ -778,8 +781,7 @@ __global__ void __launch_bounds__(256) k_cache_resolve(J jobs, WfDev b, const __
 // ---------------------------------------------------------------------------
 inline WfDev wf_view(const WavefrontBufs& w) {
   WfDev d;
-  d.R0 = (float4*)w.R0; d.R1 = (float4*)w.R1; d.R2 = (float4*)w.R2; d.R3 = (float4*)w.R3;
-  d.occ2 = w.occ2;
+  d.R0 = (float4*)w.R0; d.R1 = (float4*)w.R1; d.R2 = (float4*)w.R2;
   d.S0 = (float4*)w.S0; d.S1 = (float4*)w.S1; d.S2 = (float4*)w.S2;
   d.hit = (uint4*)w.hit;
   d.q0 = w.q[0]; d.q1 = w.q[1]; d.a0 = w.act[0]; d.a1 = w.act[1];
@@ -874,10 +876,10 @@ cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch* 
   return cudaSuccess;
 }
 
-template <class J, bool kSmem, int kSteps, int kMinB>
+template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT>
 cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms, const WfDev& b, int w,
                             int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
-  auto* fn = k_wf_trace<J, kSmem, kSteps, kMinB>;
+  auto* fn = k_wf_trace<J, kSmem, kSteps, kMinB, kVarMaxT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -898,23 +900,25 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 // 1 x 1 2.20 ms.  (Stepping until enough lanes are idle, with a ballot after
 // every iteration, ran 1.88 ms: the per-iteration ballot costs more than the
 // idle lanes of a fixed pass.)
-template <class J, bool kSmem>
+template <class J, bool kSmem, bool kVarMaxT = false>
 cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int sms, const WfDev& b, int w, int impl,
                               int refill, unsigned long long* stats, cudaStream_t st) {
+  if (kVarMaxT)   // the ReSTIR passes: the default shape only
+    return wf_launch_trace<J, kSmem, 8, 5, kVarMaxT>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
   switch (variant) {
-    case 1: return wf_launch_trace<J, kSmem, 6, 5>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    case 2: return wf_launch_trace<J, kSmem, 6, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    case 3: return wf_launch_trace<J, kSmem, 4, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    case 4: return wf_launch_trace<J, kSmem, 2, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    case 5: return wf_launch_trace<J, kSmem, 1, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    default: return wf_launch_trace<J, kSmem, 8, 5>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 1: return wf_launch_trace<J, kSmem, 6, 5, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 2: return wf_launch_trace<J, kSmem, 6, 4, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 3: return wf_launch_trace<J, kSmem, 4, 4, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 4: return wf_launch_trace<J, kSmem, 2, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 5: return wf_launch_trace<J, kSmem, 1, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    default: return wf_launch_trace<J, kSmem, 8, 5, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
   }
 }
 
 // Launches generate + (trace, shade) x waves; shade(b, w, blocks) launches
 // the shading kernel of wave w.  smem > 0 selects the shared-memory bitmap
 // tracer (single scene only).
-template <class J, class ShadeFn>
+template <class J, class ShadeFn, bool kVarMaxT = false>
 cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                          const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st, uint32_t* launches,
                          cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves, ShadeFn shade) {
@@ -934,8 +938,10 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
     if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
     const int impl = w == 0 ? (int)P : 0;
     const int tb = tune.trace_blocks_per_sm;
-    if (smem > 0) e = wf_dispatch_trace<J, true>(tune.trace_variant, jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    else e = wf_dispatch_trace<J, false>(tune.trace_variant, jobs, 0, tb, sms, b, w, impl, refill, stats, st);
+    if (smem > 0)
+      e = wf_dispatch_trace<J, true, kVarMaxT>(tune.trace_variant, jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    else
+      e = wf_dispatch_trace<J, false, kVarMaxT>(tune.trace_variant, jobs, 0, tb, sms, b, w, impl, refill, stats, st);
     if (e != cudaSuccess) return e;
     if (tm && (e = cudaEventRecord(trace_ev[2 * w + 1], st)) != cudaSuccess) return e;
     if (tm) timed++;
