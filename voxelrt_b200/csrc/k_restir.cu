@@ -636,7 +636,18 @@ struct SpatialPick {
   bool vis_test;    // its visibility must be tested (a neighbour's sample, or RF_FULLV)
   RSample sel;      // the selected sample with W and pooled confidence
   float cTotal;
-  F3 vcontrib;      // RF_VECTOR: the summed per-candidate contributions
+  F3 vcontrib;      // RF_VECTOR: the summed per-candidate contributions (deferred: those without a ray)
+  int nrays;        // RF_VECTOR, deferred: visibility rays left pending
+};
+
+// Deferred RF_VECTOR terms of path g: term j (candidate slot j) in
+// T[j][g] = (contribution, code): code 0 no term, 1 visible without a ray,
+// 2 + k visible iff ray slot k (path g + k P) is unoccluded.
+struct VecSink {
+  float4* T[4];     // S0, S1, S2, R1 of the wavefront scratch
+  float4* R0;
+  float4* R2;
+  uint32_t g, P;
 };
 
 // pairSize / pairOff / wrapMod / pairedPartner (reuse_spatial.wgsl:65-109):
@@ -706,9 +717,9 @@ VRT_DI bool sample_visible(const RestirDev& R, const uint32_t* occ, const RSampl
 
 // Neighbour selection, confidence-weighted balance-heuristic resampling and
 // (RF_VECTOR, kTraceHere only) the vector-valued shading sum of pixel (gx, gy).
-template <bool kTraceHere>
+template <bool kTraceHere, bool kVector>
 VRT_DI SpatialPick spatial_pick(const RestirDev& R, const uint32_t* occ, DCount& cnt, int gx, int gy, float4 g, F3 x1,
-                                F3 n1) {
+                                F3 n1, const VecSink* sink) {
   const Uni& u = R.u;
   const size_t p = (size_t)gy * R.W + gx;
   uint32_t rng = init_rng((uint32_t)gx, (uint32_t)gy, u.params0[0] ^ 0x2c1b3c6du);
@@ -783,39 +794,60 @@ VRT_DI SpatialPick spatial_pick(const RestirDev& R, const uint32_t* occ, DCount&
 #pragma unroll
   for (int l = 0; l < 4; l++)
     if (dok[l]) pk.cTotal = pk.cTotal + dc[l];
-  const bool vector = kTraceHere && rflag(u, kRfVector);
+  const bool vector = kVector;
   const bool fullV = rflag(u, kRfFullV);
   float wSum = 0.0f, selP = 0.0f;
   int rank = 0, selRank = 0;
   pk.sel = null_sample(0.0f);
+  pk.nrays = 0;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    if (!cok[j]) continue;
-    const RSample s = load_res(R.resA, qi[j]);
-    float denom = 0.0f, num = 0.0f, pMe = 0.0f;   // balance heuristic over all domains
+    F3 vterm = f3(0.0f, 0.0f, 0.0f);
+    uint32_t vcode = 0u;
+    if (cok[j]) {
+      const RSample s = load_res(R.resA, qi[j]);
+      float denom = 0.0f, num = 0.0f, pMe = 0.0f;   // balance heuristic over all domains
 #pragma unroll
-    for (int l = 0; l < 4; l++) {
-      if (!dok[l]) continue;
-      const float e = eval_target(s, dx[l], dn[l]);
-      const float term = dc[l] * e;
-      denom = denom + term;
-      if (l == j) num = term;
-      if (l == 0) pMe = e;
-    }
-    if (denom > 0.0f) {
-      const float m = num / denom;
-      const float w = (m * pMe) * fmax_(s.W, 0.0f);
-      if (w > 0.0f) {
-        wSum = wSum + w;
-        if (rand_(rng) * wSum < w) { pk.sel = s; selP = pMe; selRank = rank; }
+      for (int l = 0; l < 4; l++) {
+        if (!dok[l]) continue;
+        const float e = eval_target(s, dx[l], dn[l]);
+        const float term = dc[l] * e;
+        denom = denom + term;
+        if (l == j) num = term;
+        if (l == 0) pMe = e;
       }
-      if (vector && w > 0.0f) {   // vector-valued shading weight with per-candidate visibility
-        bool vis = true;
-        if (rank > 0 || fullV) vis = sample_visible(R, occ, s, x1, n1, cnt);
-        if (vis) pk.vcontrib = pk.vcontrib + eval_f(s, x1, n1) * (m * fmax_(s.W, 0.0f));
+      if (denom > 0.0f) {
+        const float m = num / denom;
+        const float w = (m * pMe) * fmax_(s.W, 0.0f);
+        if (w > 0.0f) {
+          wSum = wSum + w;
+          if (rand_(rng) * wSum < w) { pk.sel = s; selP = pMe; selRank = rank; }
+        }
+        if (vector && w > 0.0f) {   // vector-valued shading weight with per-candidate visibility
+          const bool test = rank > 0 || fullV;
+          if (kTraceHere) {
+            if (!test || sample_visible(R, occ, s, x1, n1, cnt))
+              pk.vcontrib = pk.vcontrib + eval_f(s, x1, n1) * (m * fmax_(s.W, 0.0f));
+          } else {
+            vterm = eval_f(s, x1, n1) * (m * fmax_(s.W, 0.0f));
+            vcode = 1u;
+            F3 o, d;
+            float mt;
+            if (test && visibility_ray(s, x1, n1, o, d, mt)) {
+              const uint32_t gk = sink->g + (uint32_t)pk.nrays * sink->P;
+              sink->R0[gk] = make_float4(o.x, o.y, o.z, 0.0f);
+              sink->R2[gk] = make_float4(d.x, d.y, d.z, mt);
+              vcode = 2u + (uint32_t)pk.nrays;
+              pk.nrays++;
+            } else {
+              pk.vcontrib = pk.vcontrib + vterm;
+            }
+          }
+        }
       }
+      rank++;
     }
-    rank++;
+    if (!kTraceHere && vector) sink->T[j][sink->g] = make_float4(vterm.x, vterm.y, vterm.z, __uint_as_float(vcode));
   }
   pk.ok = pk.sel.kind != kSkNone && selP > 0.0f && wSum > 0.0f;
   pk.vis_test = selRank > 0 || fullV;
@@ -854,13 +886,14 @@ VRT_DI void store_history(const RestirDev& R, size_t p, const RSample& s) {
   }
 }
 
-// Selection, record and (unless a visibility ray is left pending) radiance of
-// pixel (gx, gy).  kTraceHere: every visibility ray is traced in place.
-// Otherwise returns whether a ray is pending; then o / d / maxT describe it
-// and contrib is the contribution it gates (clamped after the test).
-template <bool kTraceHere>
-VRT_DI bool spatial_pixel(const RestirDev& R, const uint32_t* occ, DCount& cnt, int gx, int gy, F3& o, F3& d,
-                          float& maxT, F3& contrib) {
+// Selection, record and (unless visibility rays are left pending) radiance
+// of pixel (gx, gy).  kTraceHere: every visibility ray is traced in place.
+// Otherwise returns the number of pending rays: the scalar weight's single ray
+// in o / d / maxT gating contrib (clamped after the test), or RF_VECTOR's
+// rays and terms written through `sink`.
+template <bool kTraceHere, bool kVector>
+VRT_DI int spatial_pixel(const RestirDev& R, const uint32_t* occ, DCount& cnt, int gx, int gy, F3& o, F3& d,
+                         float& maxT, F3& contrib, const VecSink* sink) {
   const size_t p = (size_t)gy * R.W + gx;
   const F3 direct = load_direct(R, p);
   const float4 g = R.gbuf[p];
@@ -868,31 +901,32 @@ VRT_DI bool spatial_pixel(const RestirDev& R, const uint32_t* occ, DCount& cnt, 
     out_radiance(R, p, direct);
     R.resB[2 * p] = make_uint4(0u, 0u, 0u, 0u);
     R.resB[2 * p + 1] = make_uint4(0u, 0u, 0u, 0u);
-    return false;
+    return 0;
   }
   const F3 x1 = surface_at(R.u, gx, gy, R.W, R.H, g);
   const F3 n1 = f3(g.x, g.y, g.z);
-  const SpatialPick pk = spatial_pick<kTraceHere>(R, occ, cnt, gx, gy, g, x1, n1);
+  const SpatialPick pk = spatial_pick<kTraceHere, kVector>(R, occ, cnt, gx, gy, g, x1, n1, sink);
   if (!pk.ok) {   // pooled null
     out_radiance(R, p, direct);
     store_history(R, p, null_sample(fmin_(pk.cTotal, 255.0f)));
-    return false;
+    return 0;
   }
   store_history(R, p, pk.sel);
-  if (kTraceHere && rflag(R.u, kRfVector)) {
+  if (kVector) {
+    if (!kTraceHere && pk.nrays > 0) return pk.nrays;
     out_radiance(R, p, direct + clamp_contrib(R.u, pk.vcontrib));
-    return false;
+    return 0;
   }
   contrib = eval_f(pk.sel, x1, n1) * pk.sel.W;
   if (pk.vis_test && visibility_ray(pk.sel, x1, n1, o, d, maxT)) {
-    if (!kTraceHere) return true;
+    if (!kTraceHere) return 1;
     if (occluded(R, occ, o, d, maxT, cnt)) contrib = f3(0.0f, 0.0f, 0.0f);
   }
   out_radiance(R, p, direct + clamp_contrib(R.u, contrib));
-  return false;
+  return 0;
 }
 
-// Fused form (megakernel sessions, and RF_VECTOR): rays traced in place.
+// Fused form (megakernel sessions): rays traced in place.
 template <bool kSmem>
 __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ RestirDev R) {
   extern __shared__ uint32_t s_occ[];
@@ -903,67 +937,104 @@ __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ 
   if (gx < R.W && gy < R.H) {
     F3 o, d, contrib;
     float maxT;
-    spatial_pixel<true>(R, occ, cnt, gx, gy, o, d, maxT, contrib);
+    if (rflag(R.u, kRfVector)) spatial_pixel<true, true>(R, occ, cnt, gx, gy, o, d, maxT, contrib, nullptr);
+    else spatial_pixel<true, false>(R, occ, cnt, gx, gy, o, d, maxT, contrib, nullptr);
   }
   if (R.stats) warp_flush_stats(R.stats, cnt, 0u);
 }
 
-// Split form (wavefront sessions, scalar shading weight): selection here, the
-// pending visibility rays appended to a queue of the wavefront tracer (origin
-// R0, direction and maxT in R2, gated contribution in S1), traced by the
-// persistent tracer, then k_restir_spatial_resolve.
+// Split form (wavefront sessions): selection here; the pending visibility
+// rays (ray k of pixel g traced as path g + k P: origin R0, direction and
+// maxT R2) go to the persistent tracer's queue, the pixels with rays to the
+// active list; k_restir_spatial_resolve then sums the terms whose rays were
+// unoccluded.  Terms: the scalar weight's gated contribution in S1 (code 2),
+// RF_VECTOR's per-candidate terms in S0, S1, S2, R1 (VecSink codes).
+template <bool kVector>
 __global__ void __launch_bounds__(256) k_restir_spatial_select(const __grid_constant__ RestirDev R, WfDev b,
                                                                int wave) {
   int gx, gy;
   block_pixel_16x16(gx, gy);
+  const uint32_t P = (uint32_t)R.W * (uint32_t)R.H;
+  const bool in = gx < R.W && gy < R.H;
+  const uint32_t g = in ? (uint32_t)gy * (uint32_t)R.W + (uint32_t)gx : 0u;
+  const VecSink sink{{b.S0, b.S1, b.S2, b.R1}, b.R0, b.R2, g, P};
   F3 o, d, contrib;
   float maxT;
   DCount cnt{0u, 0u, 0u, 0u};
-  const bool ray = gx < R.W && gy < R.H && spatial_pixel<false>(R, nullptr, cnt, gx, gy, o, d, maxT, contrib);
-  const uint32_t g = ray ? (uint32_t)gy * (uint32_t)R.W + (uint32_t)gx : 0u;
-  const uint32_t slot = warp_append(b.ctr + 4 * wave, ray);
-  if (ray) {
-    queue_of(b, wave)[slot] = g | kShadowBit;
+  const int nr = in ? spatial_pixel<false, kVector>(R, nullptr, cnt, gx, gy, o, d, maxT, contrib, &sink) : 0;
+  if (nr > 0 && !kVector) {   // the scalar weight's ray, slot 0
     b.R0[g] = make_float4(o.x, o.y, o.z, 0.0f);
     b.R2[g] = make_float4(d.x, d.y, d.z, maxT);
-    b.S1[g] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+    b.S1[g] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(2u));
   }
+  uint32_t* q = queue_of(b, wave);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t slot = warp_append(b.ctr + 4 * wave, k < nr);
+    if (k < nr) q[slot] = (g + (uint32_t)k * P) | kShadowBit;
+  }
+  const uint32_t a = warp_append(b.ctr + 4 * wave + 2, nr > 0);
+  if (nr > 0) active_of(b, wave)[a] = g;
 }
 
 __global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_constant__ RestirDev R, WfDev b,
                                                                 int wave) {
-  const int n = b.ctr[4 * wave];
-  const uint32_t* q = queue_of(b, wave);
+  const int n = b.ctr[4 * wave + 2];
+  const uint32_t* list = active_of(b, wave);
+  const uint32_t P = (uint32_t)R.W * (uint32_t)R.H;
+  const bool vector = rflag(R.u, kRfVector);
+  const float4* T[4] = {b.S0, b.S1, b.S2, b.R1};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t g = q[i] & ~kShadowBit;
-    const bool vis = b.hit[g].w == 0u;
-    const float4 c = b.S1[g];
-    out_radiance(R, g, load_direct(R, g) + clamp_contrib(R.u, vis ? f3(c.x, c.y, c.z) : f3(0.0f, 0.0f, 0.0f)));
+    const uint32_t g = list[i];
+    F3 contrib = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (!vector && j != 1) continue;   // the scalar weight keeps its single term in S1
+      const float4 t = T[j][g];
+      const uint32_t code = __float_as_uint(t.w);
+      if (code == 1u || (code >= 2u && b.hit[g + (code - 2u) * P].w == 0u)) contrib = contrib + f3(t.x, t.y, t.z);
+    }
+    out_radiance(R, g, load_direct(R, g) + clamp_contrib(R.u, contrib));
   }
 }
 
 // dupmap.wgsl: share of the 9x9 window (centre excluded) whose reservoirs B
-// carry the same initial candidate (seed) as this pixel's.
+// carry the same initial candidate (seed) as this pixel's.  The block's
+// 16 x 16 tile and its 4-pixel halo are staged in shared memory as (seed,
+// non-null) pairs; the count is an integer, so the window order is free.
 __global__ void __launch_bounds__(256) k_restir_dupmap(const __grid_constant__ RestirDev R) {
+  constexpr int kHalo = 4, kT = 16 + 2 * kHalo;
+  __shared__ uint32_t s_seed[kT * kT];
+  __shared__ uint8_t s_live[kT * kT];
+  const int x0 = blockIdx.x * 16 - kHalo, y0 = blockIdx.y * 16 - kHalo;
+  for (int i = threadIdx.x; i < kT * kT; i += blockDim.x) {
+    const int qx = x0 + i % kT, qy = y0 + i / kT;
+    uint32_t seed = 0u, live = 0u;
+    if (qx >= 0 && qy >= 0 && qx < R.W && qy < R.H) {
+      const uint4 d = R.resB[2 * ((size_t)qy * R.W + qx) + 1];
+      seed = d.w;
+      live = ((d.y >> 16) & 3u) != kSkNone ? 1u : 0u;
+    }
+    s_seed[i] = seed;
+    s_live[i] = (uint8_t)live;
+  }
+  __syncthreads();
   int gx, gy;
   block_pixel_16x16(gx, gy);
   if (gx >= R.W || gy >= R.H) return;
-  const size_t p = (size_t)gy * R.W + gx;
-  const uint4 mine = R.resB[2 * p + 1];
-  if (((mine.y >> 16) & 3u) == kSkNone) {
-    R.dup[p] = 0.0f;
-    return;
+  const int c = (gy - y0) * kT + (gx - x0);
+  float score = 0.0f;
+  if (s_live[c]) {
+    const uint32_t mine = s_seed[c];
+    int count = 0;
+    for (int dy = -kHalo; dy <= kHalo; dy++)
+      for (int dx = -kHalo; dx <= kHalo; dx++) {
+        const int k = c + dy * kT + dx;
+        count += ((dx | dy) != 0 && s_live[k] && s_seed[k] == mine) ? 1 : 0;
+      }
+    score = (float)count / 80.0f;
   }
-  int count = 0;
-  for (int dy = -4; dy <= 4; dy++)
-    for (int dx = -4; dx <= 4; dx++) {
-      if (dx == 0 && dy == 0) continue;
-      const int qx = gx + dx, qy = gy + dy;
-      if (qx < 0 || qy < 0 || qx >= R.W || qy >= R.H) continue;
-      const uint4 r = R.resB[2 * ((size_t)qy * R.W + qx) + 1];
-      if (((r.y >> 16) & 3u) != kSkNone && r.w == mine.w) count++;
-    }
-  R.dup[p] = (float)count / 80.0f;
+  R.dup[(size_t)gy * R.W + gx] = score;
 }
 
 // ---------------------------------------------------------------------------
@@ -1455,7 +1526,7 @@ __global__ void __launch_bounds__(256) k_wf_unified_primary(const __grid_constan
   }
 }
 
-__global__ void __launch_bounds__(256) k_wf_unified_wave(const __grid_constant__ RestirDev R, RestirWf r, WfDev b,
+__global__ void __launch_bounds__(256, 3) k_wf_unified_wave(const __grid_constant__ RestirDev R, RestirWf r, WfDev b,
                                                          int wave) {
   const int n = b.ctr[4 * wave + 2];
   const uint32_t* list = active_of(b, wave);
@@ -1693,7 +1764,9 @@ cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms
   const int wave = 0;   // the initial pass's waves are complete: reuse slot 0
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, 16, st);
   if (e != cudaSuccess) return e;
-  k_restir_spatial_select<<<dim3((W + 15) / 16, (H + 15) / 16), 256, 0, st>>>(R, b, wave);
+  const dim3 grid((W + 15) / 16, (H + 15) / 16);
+  if (u.params2[0] & kRfVector) k_restir_spatial_select<true><<<grid, 256, 0, st>>>(R, b, wave);
+  else k_restir_spatial_select<false><<<grid, 256, 0, st>>>(R, b, wave);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int sms = wf_sm_count();
   const int smem = occ_smem(s);

@@ -29,25 +29,29 @@
 
 namespace vrt {
 
-size_t wavefront_bytes(int W, int H, int max_waves, bool dual) {
+// Queue capacity: a plain path appends at most a shadow and a bounce ray per
+// wave; with several slots a path (or the spatial pass's pixel) up to four.
+static size_t queue_entries(size_t P, int slots) { return (slots > 1 ? 4 : 2) * P; }
+
+size_t wavefront_bytes(int W, int H, int max_waves, int slots) {
   const size_t P = (size_t)W * H;
-  return P * 16 * (dual ? 10 : 7) + P * 12 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
+  return P * 16 * (4 + 3 * (size_t)slots) + queue_entries(P, slots) * 4 * 2 + P * 4 * 2 + (size_t)max_waves * 16;
 }
 
-void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, bool dual) {
+void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, int slots) {
   char* m = (char*)mem;
-  const size_t big = dual ? 2 * P : P;
+  const size_t big = (size_t)slots * P;
   void** f4[7] = {&wb.R0, &wb.R1, &wb.R2, &wb.S0, &wb.S1, &wb.S2, &wb.hit};
   for (auto* f : f4) {
     const bool twice = f == &wb.R0 || f == &wb.R2 || f == &wb.hit;
     *f = m;
     m += (twice ? big : P) * 16;
   }
-  for (int i = 0; i < 2; i++) { wb.q[i] = (uint32_t*)m; m += P * 12; }
+  for (int i = 0; i < 2; i++) { wb.q[i] = (uint32_t*)m; m += queue_entries(P, slots) * 4; }
   for (int i = 0; i < 2; i++) { wb.act[i] = (uint32_t*)m; m += P * 4; }
   wb.ctr = (int*)m;
   wb.max_waves = max_waves;
-  wb.dual = dual;
+  wb.slots = slots;
 }
 
 static SingleJob make_job(const SceneDev& s, const VrtUniforms& uu, float fclamp, int W, int H, const PathOut& out) {

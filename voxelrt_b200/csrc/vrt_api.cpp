@@ -455,9 +455,9 @@ int vrt_session_create(VrtCtx* ctx, VrtScene* scene, const VrtSessionConfig* cfg
                        ? cfg->path_kernel : VRT_PATH_WAVEFRONT;
   if (!r && s->path_kernel == VRT_PATH_WAVEFRONT) {
     const int max_waves = kMaxWaves;
-    s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves, true);
+    s->wf_bytes = wavefront_bytes(s->W, s->H, max_waves, 4);
     r = dev_alloc(ctx, &s->wf_mem, s->wf_bytes, &s->bytes);
-    if (!r) carve_wavefront(s->wf_mem, P, max_waves, s->wf, true);
+    if (!r) carve_wavefront(s->wf_mem, P, max_waves, s->wf, 4);
   }
   if (!r) {
     for (auto& e : s->ev) {
@@ -654,7 +654,7 @@ int vrt_pass_pathtrace(VrtSession* s, const VrtUniforms* u) {
     if (int r = ensure_restir(s)) return r;
     if (int r = ensure_lights(s, u)) return r;
     const RestirBufs rb = restir_bufs(s, parity_of(s));
-    if (s->path_kernel == VRT_PATH_WAVEFRONT && (u->params2[0] & kRfUnified) && s->wf.dual &&
+    if (s->path_kernel == VRT_PATH_WAVEFRONT && (u->params2[0] & kRfUnified) && s->wf.slots >= 2 &&
         (int)u->params0[1] + 5 <= s->wf.max_waves) {
       CUDA_TRY(launch_restir_unified_wavefront(s->scene->dev, *u, s->fclamp, s->W, s->H, o, rb, s->wf, s->tune,
                                                s->ctx->stream, &s->launches, s->timing ? s->tev : nullptr,
@@ -693,8 +693,8 @@ static int restir_pass(VrtSession* s, const VrtUniforms* u, bool spatial) {
   o.rad16 = s->rad16; o.rad32 = s->rad32; o.alb8 = s->alb8; o.gbuf = s->gbuf[p]; o.stats = s->stats;
   if (spatial)
     if (int r = ensure_pairing(s, u)) return r;
-  // vector-valued weights test every candidate's visibility: traced in place
-  if (spatial && s->path_kernel == VRT_PATH_WAVEFRONT && !(u->params2[0] & kRfVector)) {
+  // visibility rays (up to four per pixel with vector weights) on the wavefront tracer
+  if (spatial && s->path_kernel == VRT_PATH_WAVEFRONT && s->wf.slots >= 4) {
     CUDA_TRY(launch_restir_spatial_wavefront(s->scene->dev, *u, s->W, s->H, o, restir_bufs(s, p), s->wf, s->tune,
                                              s->ctx->stream, &s->launches));
     return VRT_OK;

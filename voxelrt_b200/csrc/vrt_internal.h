@@ -37,14 +37,15 @@ struct PathOut {
 // Scratch of the wavefront path tracer (per session, carved from one
 // allocation): per-pixel path state, ray queues, active lists, counters.
 struct WavefrontBufs {
-  void *R0 = nullptr, *R1 = nullptr, *R2 = nullptr;   // float4 per pixel (R0, R2: 2P with dual shadows)
+  void *R0 = nullptr, *R1 = nullptr, *R2 = nullptr;   // float4 per pixel (R0, R2: slots x P)
   void *S0 = nullptr, *S1 = nullptr, *S2 = nullptr;   // float4 per pixel
-  void* hit = nullptr;                                // uint4 per pixel (2P with dual shadows)
-  uint32_t* q[2] = {nullptr, nullptr};                // 3P entries each
+  void* hit = nullptr;                                // uint4 per pixel (slots x P)
+  uint32_t* q[2] = {nullptr, nullptr};                // 2P entries each (4P with several slots)
   uint32_t* act[2] = {nullptr, nullptr};              // P entries each
   int* ctr = nullptr;                                 // 4 ints per wave
   int max_waves = 0;
-  bool dual = false;                                  // paths may have two shadow rays per wave
+  int slots = 1;                                      // shadow-ray slots per path: ray k of path g is
+                                                      // traced as path g + k P
 };
 
 // Radiance-cache state of one cache-assisted wavefront frame (device
@@ -198,10 +199,11 @@ cudaError_t launch_light_grid(int N, const uint32_t* words, const double* weight
 // Records `msg` as the calling thread's vrt_last_error_string(); returns code.
 int set_error(int code, const char* msg);
 
-// dual: room for a second shadow ray per path (path index g + P in R0, R2, hit).
-size_t wavefront_bytes(int W, int H, int max_waves, bool dual = false);
-// Lays the wavefront scratch of P pixels out in mem (wavefront_bytes(P, 1, max_waves, dual) bytes).
-void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, bool dual = false);
+// slots: shadow-ray slots per path (1 for the plain path; the ReSTIR passes
+// use up to 4: ray k of path g is traced as path g + k P in R0, R2 and hit).
+size_t wavefront_bytes(int W, int H, int max_waves, int slots = 1);
+// Lays the wavefront scratch of P pixels out in mem (wavefront_bytes(P, 1, max_waves, slots) bytes).
+void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, int slots = 1);
 // When trace_ev is non-null, events trace_ev[2w], trace_ev[2w+1] bracket the
 // trace kernel of wave w (w < max_timed_waves); *timed_waves receives the count.
 // cache (may be null): cache-assisted frame (training + query paths),
