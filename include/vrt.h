@@ -263,6 +263,47 @@ int vrt_read_dupmap(VrtSession* s, void* host, size_t bytes);       /* f32 per p
 /* Writes history buffers (resume from a saved session state). */
 int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_prev);
 
+/* ---- VoxelBench technique adapter (VoxelBench/pipeline/technique.h:8-14) --
+ * A VoxelBench Technique estimates the indirect radiance of every G-buffer
+ * pixel of the harness under a per-frame ray budget.  This object holds the
+ * harness's world on the device and runs the estimator of its baseline
+ * technique (techniques/pt.h: NEE paths, exponential history, edge-aware 5x5
+ * filter) on this library's DDA.  Units are the harness's (voxels). */
+typedef struct VrtVb VrtVb;
+
+typedef struct VrtVbWorld {
+  int nx, ny, nz;                /* grid size (core.h:64), any size up to 1024     */
+  const uint8_t* grid;           /* material ids 0..15, index (z*ny + y)*nx + x    */
+  float albedo[16][3];           /* MAT[m].alb                                     */
+  float emission[16][3];         /* MAT[m].emi (emissive when the sum is > 0)      */
+  const int32_t* emitters;       /* 5 per exposed emissive face: x, y, z, face, m  */
+  int n_emitters;                /* (collectEmitters, core.cpp:133-141)            */
+  int sky_enabled;               /* SKY (core.h:85-95)                             */
+  float sun_dir[3], sun_e[3], zenith[3], horizon[3];
+} VrtVbWorld;
+
+typedef struct VrtVbPixel {      /* one GPix (core.h:119)                           */
+  float pos[3];                  /* hit point (voxels)                              */
+  float depth;
+  float n[3];                    /* face normal                                     */
+  uint32_t flags;                /* bit0 hit, bit1 the hit material is emissive     */
+  float albedo[3];
+  uint32_t pad;
+} VrtVbPixel;
+
+int vrt_vb_create(VrtCtx* ctx, int width, int height, VrtVb** out);
+int vrt_vb_destroy(VrtVb* vb);
+/* Uploads the world (Technique::init, and after a geometry or light event). */
+int vrt_vb_set_world(VrtVb* vb, const VrtVbWorld* world);
+/* Uploads the harness's G-buffer (width*height pixels, row-major). */
+int vrt_vb_set_gbuffer(VrtVb* vb, const VrtVbPixel* pixels);
+/* Clears the history (the next frame starts the estimate afresh). */
+int vrt_vb_reset(VrtVb* vb);
+/* Technique::frame(budget): one frame within `budget` rays; out_rgb (may be
+ * NULL) receives width*height indirect radiances (RGB f32), *rays the rays
+ * traced. */
+int vrt_vb_frame(VrtVb* vb, long long budget, float* out_rgb, uint64_t* rays);
+
 /* ---- batched frames (no counterpart in the reference) ------------------ */
 /* A batch renders one frame for each of n sessions of one context in a
  * single launch sequence: one wavefront path trace over all sessions' pixels

@@ -26,11 +26,16 @@ class OrcStats(C.Structure):
                 ("pixels", C.c_uint64)]
 
 
+VB_VRT = HERE / "_ref" / "vb_vrt"
+
+
 def build(ref: bool | None = None) -> None:
-    """make -C oracle (and the reference traversal when its sources exist)."""
+    """make -C oracle (and, when the reference sources exist, the reference
+    traversal library and the VoxelBench harness driver vb_vrt, which links
+    voxelrt_b200/libvrt.so)."""
     targets = ["all"]
     if ref or (ref is None and REF_SRC.exists()):
-        targets.append("ref")
+        targets += ["ref", "vbvrt"]
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 
 

@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libvrt.so"
 
 CU_SOURCES = ["k_trace.cu", "k_image.cu", "k_atrous_tma.cu", "k_wavefront.cu", "k_noalloc.cu", "k_batch.cu",
-              "k_mlp.cu", "k_hdr.cu", "k_lights.cu", "k_restir.cu"]
+              "k_mlp.cu", "k_hdr.cu", "k_lights.cu", "k_restir.cu", "k_vb.cu"]
 CPP_SOURCES = ["vrt_api.cpp", "scene_gen.cpp", "pairing.cpp"]
 HEADERS = ["vrt_device.cuh", "vrt_internal.h", "wavefront_core.cuh", "image_core.cuh", "umma.cuh",
            "trace_kernel.cuh"]

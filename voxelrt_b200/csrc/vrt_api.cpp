@@ -2068,3 +2068,193 @@ int vrt_write_history(VrtSession* s, const void* accum_prev, const float* gbuf_p
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// VoxelBench technique adapter (VoxelBench/pipeline/technique.h:8-14): the
+// harness's grid, palette, emitters and sky on the device, its G-buffer per
+// frame, and its baseline estimator (techniques/pt.h) on this library's DDA.
+// ---------------------------------------------------------------------------
+struct VrtVb {
+  VrtCtx* ctx = nullptr;
+  int W = 0, H = 0;
+  VrtScene* scene = nullptr;     // the harness's grid embedded in an N^3 packed grid
+  int nx = 0, ny = 0, nz = 0;
+  uint64_t bytes = 0;
+  void* px = nullptr;            // 48 B per pixel (VrtVbPixel)
+  void* hist = nullptr;          // float4 per pixel
+  void* out = nullptr;           // float4 per pixel
+  int* emitters = nullptr;       // int4 per emissive face
+  size_t em_cap = 0;
+  int n_em = 0;
+  unsigned long long* rays = nullptr;
+  float albedo[16][3] = {}, emission[16][3] = {};
+  int sky = 0;
+  float sun_dir[3] = {}, sun_e[3] = {}, zenith[3] = {}, horizon[3] = {};
+  uint32_t fcount = 0;
+  bool have_world = false, have_gbuf = false;
+};
+
+static_assert(sizeof(VrtVbPixel) == 48, "VrtVbPixel is 3 float4");
+
+extern "C" {
+
+int vrt_vb_create(VrtCtx* ctx, int width, int height, VrtVb** out) {
+  if (!ctx || !out || width < 1 || height < 1 || (long long)width * height > (1ll << 26))
+    return fail(VRT_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  if (int r = set_dev(ctx)) return r;
+  VrtVb* v = new VrtVb();
+  v->ctx = ctx;
+  v->W = width;
+  v->H = height;
+  const size_t P = (size_t)width * height;
+  int r = dev_alloc(ctx, &v->px, P * 48, &v->bytes);
+  if (!r) r = dev_alloc(ctx, &v->hist, P * 16, &v->bytes);
+  if (!r) r = dev_alloc(ctx, &v->out, P * 16, &v->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&v->rays, 8, &v->bytes);
+  if (!r) r = vrt_vb_reset(v);
+  if (r) {
+    std::string keep = g_err;
+    vrt_vb_destroy(v);
+    g_err = keep;
+    return r;
+  }
+  *out = v;
+  return VRT_OK;
+}
+
+int vrt_vb_destroy(VrtVb* v) {
+  if (!v) return VRT_OK;
+  VrtCtx* c = v->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  const size_t P = (size_t)v->W * v->H;
+  dev_free(c, v->px, P * 48, &v->bytes);
+  dev_free(c, v->hist, P * 16, &v->bytes);
+  dev_free(c, v->out, P * 16, &v->bytes);
+  dev_free(c, v->rays, 8, &v->bytes);
+  dev_free(c, v->emitters, v->em_cap * 16, &v->bytes);
+  if (v->scene) vrt_scene_destroy(v->scene);
+  delete v;
+  return VRT_OK;
+}
+
+int vrt_vb_reset(VrtVb* v) {
+  if (!v) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(v->ctx)) return r;
+  CUDA_TRY(cudaMemsetAsync(v->hist, 0, (size_t)v->W * v->H * 16, v->ctx->stream));
+  CUDA_TRY(cudaMemsetAsync(v->out, 0, (size_t)v->W * v->H * 16, v->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(v->ctx->stream));
+  v->fcount = 0;
+  return VRT_OK;
+}
+
+int vrt_vb_set_world(VrtVb* v, const VrtVbWorld* w) {
+  if (!v || !w || !w->grid || w->nx < 1 || w->ny < 1 || w->nz < 1 || w->n_emitters < 0 ||
+      (w->n_emitters > 0 && !w->emitters))
+    return fail(VRT_ERR_INVALID, "bad world");
+  const int N = ((std::max(w->nx, std::max(w->ny, w->nz)) + 7) / 8) * 8;
+  if (N > 1024) return fail(VRT_ERR_INVALID, "grid %dx%dx%d larger than 1024", w->nx, w->ny, w->nz);
+  for (size_t i = 0; i < (size_t)w->nx * w->ny * w->nz; i++)
+    if (w->grid[i] >= 16) return fail(VRT_ERR_INVALID, "material id %u >= 16", (unsigned)w->grid[i]);
+  if (int r = set_dev(v->ctx)) return r;
+  // the harness's grid (index (z*ny + y)*nx + x) at the origin of an N^3 grid
+  std::vector<uint32_t> vox((size_t)N * N * N, 0u);
+  for (int z = 0; z < w->nz; z++)
+    for (int y = 0; y < w->ny; y++)
+      for (int x = 0; x < w->nx; x++)
+        vox[(size_t)x + (size_t)y * N + (size_t)z * N * N] = w->grid[((size_t)z * w->ny + y) * w->nx + x];
+  if (v->scene) {
+    vrt_scene_destroy(v->scene);
+    v->scene = nullptr;
+  }
+  if (int r = vrt_scene_upload(v->ctx, vox.data(), N, &v->scene)) return r;
+  if ((size_t)w->n_emitters > v->em_cap) {
+    dev_free(v->ctx, v->emitters, v->em_cap * 16, &v->bytes);
+    v->emitters = nullptr;
+    v->em_cap = 0;
+    if (int r = dev_alloc(v->ctx, (void**)&v->emitters, (size_t)w->n_emitters * 16, &v->bytes)) return r;
+    v->em_cap = (size_t)w->n_emitters;
+  }
+  std::vector<int> em((size_t)w->n_emitters * 4);
+  for (int i = 0; i < w->n_emitters; i++) {
+    const int32_t* e = w->emitters + 5 * (size_t)i;
+    if (e[3] < 0 || e[3] > 5 || e[4] < 0 || e[4] >= 16) return fail(VRT_ERR_INVALID, "bad emitter %d", i);
+    em[4 * (size_t)i] = e[0];
+    em[4 * (size_t)i + 1] = e[1];
+    em[4 * (size_t)i + 2] = e[2];
+    em[4 * (size_t)i + 3] = e[3] | (e[4] << 8);
+  }
+  if (!em.empty())
+    CUDA_TRY(cudaMemcpyAsync(v->emitters, em.data(), em.size() * 4, cudaMemcpyHostToDevice, v->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(v->ctx->stream));
+  v->n_em = w->n_emitters;
+  v->nx = w->nx; v->ny = w->ny; v->nz = w->nz;
+  std::memcpy(v->albedo, w->albedo, sizeof v->albedo);
+  std::memcpy(v->emission, w->emission, sizeof v->emission);
+  v->sky = w->sky_enabled;
+  std::memcpy(v->sun_dir, w->sun_dir, 12);
+  std::memcpy(v->sun_e, w->sun_e, 12);
+  std::memcpy(v->zenith, w->zenith, 12);
+  std::memcpy(v->horizon, w->horizon, 12);
+  v->have_world = true;
+  return VRT_OK;
+}
+
+int vrt_vb_set_gbuffer(VrtVb* v, const VrtVbPixel* pixels) {
+  if (!v || !pixels) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (int r = set_dev(v->ctx)) return r;
+  CUDA_TRY(cudaMemcpyAsync(v->px, pixels, (size_t)v->W * v->H * 48, cudaMemcpyHostToDevice, v->ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(v->ctx->stream));
+  v->have_gbuf = true;
+  return VRT_OK;
+}
+
+int vrt_vb_frame(VrtVb* v, long long budget, float* out_rgb, uint64_t* rays) {
+  if (!v || budget < 0) return fail(VRT_ERR_INVALID, "bad argument");
+  if (!v->have_world || !v->have_gbuf) return fail(VRT_ERR_STATE, "set the world and the G-buffer first");
+  if (int r = set_dev(v->ctx)) return r;
+  cudaStream_t st = v->ctx->stream;
+  // paths per pixel from the ray budget (techniques/pt.h:25-28): 5 rays a path
+  const double ppp = (double)budget / ((double)v->W * v->H * 5.0);
+  VbLaunch L;
+  L.scene = v->scene->dev;
+  L.nx = v->nx; L.ny = v->ny; L.nz = v->nz;
+  L.W = v->W; L.H = v->H;
+  L.px = v->px; L.hist = v->hist; L.out = v->out;
+  L.emitters = v->emitters;
+  L.n_emitters = v->n_em;
+  std::memcpy(L.albedo, v->albedo, sizeof L.albedo);
+  std::memcpy(L.emission, v->emission, sizeof L.emission);
+  L.sky = v->sky;
+  std::memcpy(L.sun_dir, v->sun_dir, 12);
+  std::memcpy(L.sun_e, v->sun_e, 12);
+  std::memcpy(L.zenith, v->zenith, 12);
+  std::memcpy(L.horizon, v->horizon, 12);
+  L.rays = v->rays;
+  L.fcount = v->fcount;
+  L.base_paths = (int)std::max(1.0, std::floor(ppp));
+  L.frac_p = ppp > 1.0 ? ppp - std::floor(ppp) : 0.0;
+  L.stride = ppp < 1.0 ? (int)std::lround(1.0 / std::max(ppp, 1e-9)) : 1;
+  CUDA_TRY(cudaMemsetAsync(v->rays, 0, 8, st));
+  CUDA_TRY(launch_vb_frame(L, st));
+  v->fcount++;
+  unsigned long long n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, v->rays, 8, cudaMemcpyDeviceToHost, st));
+  std::vector<float> o4;
+  if (out_rgb) {
+    o4.resize((size_t)v->W * v->H * 4);
+    CUDA_TRY(cudaMemcpyAsync(o4.data(), v->out, o4.size() * 4, cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (out_rgb)
+    for (size_t i = 0; i < (size_t)v->W * v->H; i++) {
+      out_rgb[3 * i] = o4[4 * i];
+      out_rgb[3 * i + 1] = o4[4 * i + 1];
+      out_rgb[3 * i + 2] = o4[4 * i + 2];
+    }
+  if (rays) *rays = n;
+  return VRT_OK;
+}
+
+}  // extern "C"

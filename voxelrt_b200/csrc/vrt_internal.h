@@ -294,4 +294,25 @@ cudaError_t launch_restir_spatial_wavefront(const SceneDev& s, const VrtUniforms
                                             const RestirBufs& rb, const WavefrontBufs& wb,
                                             const WavefrontTuning& tune, cudaStream_t st, uint32_t* launches);
 
+// One frame of the VoxelBench technique adapter (k_vb.cu).
+struct VbLaunch {
+  SceneDev scene;            // the harness's grid in the packed layout (material id in the low byte)
+  int nx, ny, nz;            // the harness's grid size
+  int W, H;
+  const void* px;            // 3 float4 per pixel (VrtVbPixel)
+  void* hist;                // float4 per pixel
+  void* out;                 // float4 per pixel
+  const int* emitters;       // 4 ints per emissive face
+  int n_emitters;
+  float albedo[16][3], emission[16][3];
+  int sky;
+  float sun_dir[3], sun_e[3], zenith[3], horizon[3];
+  unsigned long long* rays;
+  uint32_t fcount;
+  int base_paths;
+  double frac_p;
+  int stride;
+};
+cudaError_t launch_vb_frame(const VbLaunch& L, cudaStream_t st);
+
 }  // namespace vrt
