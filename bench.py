@@ -48,7 +48,7 @@ def parse_args():
                     help="frame mode: skip the plain vs batched+cache comparison in the output line")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame", "lights",
-                                                              "restir"],
+                                                              "restir", "voxelbench"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
                          "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
                          "path tracing at matched MSE; restir: the ReSTIR gi preset beside the plain frame")
@@ -1118,6 +1118,55 @@ def run_restir(args, local):
     print(json.dumps(line), flush=True)
 
 
+VB_SCENES = ["bunker", "cavern", "courtyard", "town"]
+VB_PUBLISHED_PT_MS = {"bunker": 115.7, "cavern": 123.5, "courtyard": 36.4, "town": 34.6}
+
+
+def run_voxelbench(args, local):
+    """`--mode voxelbench`: the VoxelBench harness protocol (240x135, ray budget
+    4*W*H per frame, the reference's scenes and metrics) with the library's
+    Technique adapter MethodVRT on the GPU beside the reference's own baseline
+    MethodPT on the CPU (the harness's 2 OpenMP threads), same estimator and
+    budget.  Runs oracle/_ref/vb_vrt (built from the reference sources)."""
+    import oracle
+
+    if not oracle.VB_VRT.exists():
+        print(json.dumps({"mode": "voxelbench", "unavailable": "oracle/_ref/vb_vrt not built (needs the "
+                          "reference sources at build time)"}), flush=True)
+        return
+    frames = max(args.steps, 5)
+    out = {}
+    for sc in VB_SCENES:
+        r = subprocess.run([str(oracle.VB_VRT), sc, "1.0", str(frames), "64", "2"], capture_output=True, text=True,
+                           timeout=1800, env={**os.environ, "CUDA_VISIBLE_DEVICES": os.environ.get(
+                               "CUDA_VISIBLE_DEVICES", str(local))})
+        if r.returncode != 0:
+            raise RuntimeError(f"vb_vrt {sc}: {r.stderr[-2000:]}")
+        rows = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+        summ = {x["summary"]: x for x in rows if "summary" in x}
+        ref = [x for x in rows if "reference" in x][0]
+        vrt_ms = [x["ms"] for x in rows if x.get("method") == "VRT"][1:]   # the first frame uploads
+        out[sc] = {"vrt_ms": round(statistics.mean(vrt_ms), 4), "pt_ms": round(summ["PT"]["mean_ms"], 2),
+                   "speedup": round(summ["PT"]["mean_ms"] / statistics.mean(vrt_ms), 1),
+                   "rays_per_frame": round(summ["VRT"]["rays_per_frame"]),
+                   "psnr": [summ["PT"]["psnr"], summ["VRT"]["psnr"]], "ssim": [summ["PT"]["ssim"], summ["VRT"]["ssim"]],
+                   "gpsnr": [summ["PT"]["gpsnr"], summ["VRT"]["gpsnr"]],
+                   "mean_luma": [summ["PT"]["mean_luma"], summ["VRT"]["mean_luma"], ref["mean_luma"]],
+                   "published_pt_ms_author_cpu": VB_PUBLISHED_PT_MS[sc]}
+    line = {
+        "metric": "VoxelBench PT@1.0x frame ms (240x135, budget 4*W*H rays): MethodVRT (GPU) vs the reference MethodPT",
+        "value": round(statistics.mean(v["vrt_ms"] for v in out.values()), 4), "unit": "ms/frame", "n_gpus": 1,
+        "steps": frames, "warmup": 1, "ms_per_step": round(statistics.mean(v["vrt_ms"] for v in out.values()), 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "the reference's procedural VoxelBench scenes (pre-event state)",
+        "config": {"workload": "VoxelBench harness run protocol, 4 scenes", "frames": frames, "ref_spp": 64,
+                   "pt_threads": 1, "note": "host wall clock per Technique::frame (upload of the G-buffer excluded "
+                   "after the first frame); quality pairs are [PT, VRT] against the same reference"},
+        "scenes": out,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_env()
@@ -1141,6 +1190,9 @@ def main():
     elif args.mode == "restir":
         if rank == 0:
             run_restir(args, local)
+    elif args.mode == "voxelbench":
+        if rank == 0:
+            run_voxelbench(args, local)
     else:
         run_ours(args, world, rank, local)
 

@@ -13,7 +13,9 @@
 // oracle/_ref/vb_vrt, linked against voxelrt_b200/libvrt.so.
 //
 // usage: vb_vrt <scene> <mult> <frames> <ref_spp> [threads] [event_frame]
-// prints one JSON line per technique and frame, then a summary line each.
+// threads: OpenMP threads of the techniques (the harness uses 2,
+// harness.cpp:201); the references use every host thread.  Prints one JSON
+// line per technique and frame, then a summary line each.
 #include "core.h"
 #include "scenes.h"
 #include "technique.h"
@@ -49,9 +51,9 @@ int main(int argc, char** argv) {
   const std::string sc = argv[1];
   const float mult = (float)atof(argv[2]);
   const int frames = atoi(argv[3]), ref_spp = atoi(argv[4]);
-  const int threads = argc > 5 ? atoi(argv[5]) : omp_get_max_threads();
+  const int all_threads = omp_get_max_threads();
+  const int threads = argc > 5 && atoi(argv[5]) > 0 ? atoi(argv[5]) : all_threads;
   const int event_frame = argc > 6 ? atoi(argv[6]) : -1;
-  omp_set_num_threads(threads);
   std::unique_ptr<Scene> s(makeScene(sc));
   if (!s) { fprintf(stderr, "unknown scene %s\n", sc.c_str()); return 2; }
   const long budget = (long)(4L * W * H * mult);
@@ -66,7 +68,8 @@ int main(int argc, char** argv) {
   renderReference(refPre, ref_spp, 7919u * 1u);
   const double ref_s = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
   printf("{\"reference\": \"%s\", \"spp\": %d, \"seconds\": %.3f, \"mean_luma\": %.6f, \"threads\": %d}\n",
-         sc.c_str(), ref_spp, ref_s, mean_luma(refPre), threads);
+         sc.c_str(), ref_spp, ref_s, mean_luma(refPre), all_threads);
+  omp_set_num_threads(threads);
 
   for (int which = 0; which < 2; which++) {
     s.reset(makeScene(sc));
@@ -98,9 +101,9 @@ int main(int argc, char** argv) {
     }
     printf("{\"summary\": \"%s\", \"scene\": \"%s\", \"mult\": %.2f, \"budget\": %ld, \"frames\": %d, "
            "\"mean_ms\": %.4f, \"rays_per_frame\": %.1f, \"psnr\": %.4f, \"ssim\": %.5f, \"gpsnr\": %.4f, "
-           "\"mean_luma\": %.6f}\n",
+           "\"mean_luma\": %.6f, \"threads\": %d}\n",
            m->name(), sc.c_str(), mult, budget, frames, ms_sum / frames, (double)rays_sum / frames, last_psnr,
-           last_ssim, last_gpsnr, mean_luma(m->out));
+           last_ssim, last_gpsnr, mean_luma(m->out), threads);
     fflush(stdout);
   }
   return 0;
