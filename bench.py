@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--cache", action="store_true", help="serve: also run the sweep with the cache-assisted path")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="frame mode: skip the ReSTIR and VoxelBench summaries in the output line")
     ap.add_argument("--runs", default="", help="restir: comma-separated subset of plain,gi,ours,ours_b6_nodenoise")
     return ap.parse_args()
 
@@ -309,6 +311,26 @@ def run_ours(args, world, rank, local):
         a2 = copy.copy(args)
         a2.steps = min(args.steps, 10)
         line["plain_vs_batched_cache"] = cache_summary(cache_comparison(a2, local))
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the survey's "next" rows measured on the same box: ReSTIR presets and the VoxelBench adapter
+        import copy
+        a3 = copy.copy(args)
+        a3.steps, a3.warmup, a3.no_cpu_baseline, a3.runs = 10, 3, True, "gi,ours_b6_nodenoise"
+        try:
+            r = restir_line(a3, local)
+            line["restir"] = {k: {"preset": v["preset"], "bounces": v["bounces"], "frame_ms": v["frame_ms_mean"],
+                                  "rays_per_frame": v["rays_per_frame"]} for k, v in r["runs"].items()}
+            line["restir"]["details"] = "bench.py --mode restir"
+        except Exception as e:   # the headline line must still print
+            line["restir"] = {"error": str(e)[:300]}
+        try:
+            v = voxelbench_line(a3, local, 10, 32)
+            line["voxelbench"] = {sc: {"vrt_ms": x["vrt_ms"], "pt_ms": x["pt_ms"], "psnr_pt_vrt": x["psnr"]}
+                                  for sc, x in v.get("scenes", {}).items()} or v
+            if v.get("scenes"):
+                line["voxelbench"]["details"] = "bench.py --mode voxelbench"
+        except Exception as e:
+            line["voxelbench"] = {"error": str(e)[:300]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -1021,6 +1043,10 @@ RESTIR_RUNS = [   # (label, preset, bounces, params0.z flags: bit0 temporal, bit
 
 
 def run_restir(args, local):
+    print(json.dumps(restir_line(args, local)), flush=True)
+
+
+def restir_line(args, local):
     """`--mode restir`: the reference's ReSTIR presets -- `gi` (RF_RESTIR |
     RF_TEMPORAL | RF_SPATIAL) and its default `ours` (paired reuse, duplication
     map, vector weights, unified light-list NEE with power sampling, plane,
@@ -1115,7 +1141,7 @@ def run_restir(args, local):
         line["cpu_baseline"] = {"value": round(dt * 1e3, 1), "unit": "ms/frame", "cores": oracle.num_threads(),
                                 "kind": "port", "rays": r["stats"]["rays"],
                                 "sample": "1 full ReSTIR gi frame (2 bounces) of the workload through the CPU oracle"}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 VB_SCENES = ["bunker", "cavern", "courtyard", "town"]
@@ -1123,6 +1149,10 @@ VB_PUBLISHED_PT_MS = {"bunker": 115.7, "cavern": 123.5, "courtyard": 36.4, "town
 
 
 def run_voxelbench(args, local):
+    print(json.dumps(voxelbench_line(args, local, max(args.steps, 5), 64)), flush=True)
+
+
+def voxelbench_line(args, local, frames, ref_spp):
     """`--mode voxelbench`: the VoxelBench harness protocol (240x135, ray budget
     4*W*H per frame, the reference's scenes and metrics) with the library's
     Technique adapter MethodVRT on the GPU beside the reference's own baseline
@@ -1131,13 +1161,11 @@ def run_voxelbench(args, local):
     import oracle
 
     if not oracle.VB_VRT.exists():
-        print(json.dumps({"mode": "voxelbench", "unavailable": "oracle/_ref/vb_vrt not built (needs the "
-                          "reference sources at build time)"}), flush=True)
-        return
-    frames = max(args.steps, 5)
+        return {"mode": "voxelbench", "unavailable": "oracle/_ref/vb_vrt not built (needs the reference sources "
+                "at build time)"}
     out = {}
     for sc in VB_SCENES:
-        r = subprocess.run([str(oracle.VB_VRT), sc, "1.0", str(frames), "64", "2"], capture_output=True, text=True,
+        r = subprocess.run([str(oracle.VB_VRT), sc, "1.0", str(frames), str(ref_spp), "1"], capture_output=True, text=True,
                            timeout=1800, env={**os.environ, "CUDA_VISIBLE_DEVICES": os.environ.get(
                                "CUDA_VISIBLE_DEVICES", str(local))})
         if r.returncode != 0:
@@ -1159,12 +1187,12 @@ def run_voxelbench(args, local):
         "steps": frames, "warmup": 1, "ms_per_step": round(statistics.mean(v["vrt_ms"] for v in out.values()), 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "the reference's procedural VoxelBench scenes (pre-event state)",
-        "config": {"workload": "VoxelBench harness run protocol, 4 scenes", "frames": frames, "ref_spp": 64,
+        "config": {"workload": "VoxelBench harness run protocol, 4 scenes", "frames": frames, "ref_spp": ref_spp,
                    "pt_threads": 1, "note": "host wall clock per Technique::frame (upload of the G-buffer excluded "
                    "after the first frame); quality pairs are [PT, VRT] against the same reference"},
         "scenes": out,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
