@@ -76,7 +76,7 @@ VRT_DI F3 hit_normal(int vax, F3 rd) {
 // Counters follow the oracle: outer = brick iterations entered, inner =
 // voxel iterations entered, vreads = voxel words read.
 // ---------------------------------------------------------------------------
-enum : int { kLevelVoxel = 1, kPending = 2, kDone = 4 };
+enum : int { kLevelVoxel = 1, kPending = 2, kDone = 4, kHitCell = 8 };
 
 struct FlatDDA {
   F3 ro, invRd;
@@ -93,9 +93,24 @@ struct FlatDDA {
 
   VRT_DI bool done() const { return (state & kDone) != 0; }
 
-  VRT_DI void init(const DScene& S, F3 roW, F3 rd, float maxTW) {
+  // The walk's result once done(): at an occupied voxel the voxel word is read
+  // and the hit kept unless it lies beyond maxT (voxel.wgsl:128-137).  Kept
+  // out of step() so that the unrolled steps carry neither the read nor the
+  // result registers.
+  VRT_DI void finish(const DScene& S, DCount& c) {
     tHit = -1.0f;
     mat = 0u;
+    if (state & kHitCell) {
+      const uint32_t vx = (uint32_t)(bx * kBrick + lx), vy = (uint32_t)(by * kBrick + ly),
+                     vz = (uint32_t)(bz * kBrick + lz);
+      mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
+      c.vreads++;
+      if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
+      else mat = 0u;
+    }
+  }
+
+  VRT_DI void init(const DScene& S, F3 roW, F3 rd, float maxTW) {
     vax = 0;
     ro = roW * kInvVoxel;
     maxT = maxTW * kInvVoxel;
@@ -128,6 +143,23 @@ struct FlatDDA {
     bz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
     tMaxB = ((f3((float)bx, (float)by, (float)bz) + stepGE) * 8.0f - ro) * invRd;
     state = 0;   // brick level, test first
+  }
+
+  // Enters the occupied brick (bx, by, bz) at t: the entry voxel from
+  // t + 1e-4 (voxel.wgsl:104-109), its tMax, and a test without stepping next.
+  VRT_DI void descend(const DScene& S, F3 rd) {
+    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
+    const F3 p = ro + rd * (t + 1e-4f);
+    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
+    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
+    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
+    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
+    tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
+    lx = vx - mnx; ly = vy - mny; lz = vz - mnz;
+    tCur = t;
+    vax = ax;
+    j = 0;
+    state = kLevelVoxel;
   }
 
   VRT_DI void step(const DScene& S, const uint32_t* occ, F3 rd, DCount& c) {
@@ -183,28 +215,10 @@ struct FlatDDA {
       return;
     }
     if (lv) {
-      const uint32_t vx = (uint32_t)(bx * kBrick + lx), vy = (uint32_t)(by * kBrick + ly),
-                     vz = (uint32_t)(bz * kBrick + lz);
-      mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
-      c.vreads++;
-      if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
-      else mat = 0u;
-      state = kDone;
+      state = kDone | kHitCell;   // finish() reads the voxel
       return;
     }
-    // descend into the occupied brick
-    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
-    const F3 p = ro + rd * (t + 1e-4f);
-    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
-    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
-    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
-    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
-    tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
-    lx = vx - mnx; ly = vy - mny; lz = vz - mnz;
-    tCur = t;
-    vax = ax;
-    j = 0;
-    state = kLevelVoxel;
+    descend(S, rd);
   }
 };
 
@@ -570,6 +584,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       for (int k = 0; k < kSteps; k++)
         if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
+        d.finish(S, c);
         const uint32_t g = entry & ~kShadowBit;
         uint32_t* h = reinterpret_cast<uint32_t*>(b.hit + g);
         if (entry & kShadowBit) {
@@ -899,7 +914,15 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 // 6 x 5 1.67, 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98,
 // 1 x 1 2.20 ms.  (Stepping until enough lanes are idle, with a ballot after
 // every iteration, ran 1.88 ms: the per-iteration ballot costs more than the
-// idle lanes of a fixed pass.)
+// idle lanes of a fixed pass.)  Also measured and dropped, each bit-identical:
+// a step with every outcome selected instead of branched (only the descent
+// branched) 2.02 ms; descents parked until the end of each pass, so that a
+// warp runs the descent block once per pass, 1.71 (4 x 5) - 1.80 ms (8 x 5);
+// an exact empty-space skip (brick distance field and 4^3 sub-block masks,
+// the skipped steps replayed in closed form per axis: 41% fewer step calls on
+// this frame) 2.2 - 3.3 ms, because a warp runs the ~100-instruction replay in
+// nearly every step in which one of its lanes needs it.  The frame with the
+// 8 x 5 default: 1.60 ms of trace.
 template <class J, bool kSmem, bool kVarMaxT = false>
 cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int sms, const WfDev& b, int w, int impl,
                               int refill, unsigned long long* stats, cudaStream_t st) {
