@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(256) k_restir_initial(const __grid_constant__ 
     initial_pixel(R, occ, gx, gy, cnt);
     pix = 1u;
   }
-  if (R.stats) warp_flush_stats(R.stats, cnt, pix);
+  if (R.stats) block_flush_stats(R.stats, cnt, pix);
 }
 
 // ---------------------------------------------------------------------------
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(256) k_restir_spatial(const __grid_constant__ 
     if (rflag(R.u, kRfVector)) spatial_pixel<true, true>(R, occ, cnt, gx, gy, o, d, maxT, contrib, nullptr);
     else spatial_pixel<true, false>(R, occ, cnt, gx, gy, o, d, maxT, contrib, nullptr);
   }
-  if (R.stats) warp_flush_stats(R.stats, cnt, 0u);
+  if (R.stats) block_flush_stats(R.stats, cnt, 0u);
 }
 
 // Split form (wavefront sessions): selection here; the pending visibility
@@ -967,14 +967,11 @@ __global__ void __launch_bounds__(256) k_restir_spatial_select(const __grid_cons
     b.R2[g] = make_float4(d.x, d.y, d.z, maxT);
     b.S1[g] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(2u));
   }
+  uint32_t rs, as;
+  block_append(b.ctr + 4 * wave, b.ctr + 4 * wave + 2, nr, nr > 0, rs, as);
   uint32_t* q = queue_of(b, wave);
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const uint32_t slot = warp_append(b.ctr + 4 * wave, k < nr);
-    if (k < nr) q[slot] = (g + (uint32_t)k * P) | kShadowBit;
-  }
-  const uint32_t a = warp_append(b.ctr + 4 * wave + 2, nr > 0);
-  if (nr > 0) active_of(b, wave)[a] = g;
+  for (int k = 0; k < nr; k++) q[rs + (uint32_t)k] = (g + (uint32_t)k * P) | kShadowBit;
+  if (nr > 0) active_of(b, wave)[as] = g;
 }
 
 __global__ void __launch_bounds__(256) k_restir_spatial_resolve(const __grid_constant__ RestirDev R, WfDev b,
@@ -1178,7 +1175,7 @@ __global__ void __launch_bounds__(256) k_wf_restir_primary(const __grid_constant
         }
       }
     }
-    emit(b, 1, g, shadow, bounce, keep);
+    emit_block(b, 1, g, shadow, bounce, keep);
   }
 }
 
@@ -1256,7 +1253,7 @@ __global__ void __launch_bounds__(256) k_wf_restir_wave(const __grid_constant__ 
         }
       }
     }
-    emit(b, wave + 1, g, shadow, bounce, keep);
+    emit_block(b, wave + 1, g, shadow, bounce, keep);
   }
 }
 
@@ -1522,7 +1519,7 @@ __global__ void __launch_bounds__(256) k_wf_unified_primary(const __grid_constan
       }
     }
     const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
-    emit2(b, 1, g, P, rays.shadow, rays.shadow2, rays.bounce, keep);
+    emit2_block(b, 1, g, P, rays.shadow, rays.shadow2, rays.bounce, keep);
   }
 }
 
@@ -1621,7 +1618,7 @@ __global__ void __launch_bounds__(256, 3) k_wf_unified_wave(const __grid_constan
       }
     }
     const bool keep = rays.shadow || rays.shadow2 || rays.bounce;
-    emit2(b, wave + 1, g, (uint32_t)r.W * (uint32_t)r.H, rays.shadow, rays.shadow2, rays.bounce, keep);
+    emit2_block(b, wave + 1, g, (uint32_t)r.W * (uint32_t)r.H, rays.shadow, rays.shadow2, rays.bounce, keep);
   }
 }
 

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_pathtrace(DScene S, Uni u, float fclamp
     reinterpret_cast<float4*>(out.gbuf)[p] = gb;
     pix = 1;
   }
-  if (out.stats) warp_flush_stats(out.stats, cnt, pix);
+  if (out.stats) block_flush_stats(out.stats, cnt, pix);
 }
 
 template <bool kSmem>

@@ -21,22 +21,6 @@ VRT_DI const uint32_t* stage_occupancy(const DScene& S, uint32_t* s_occ) {
   return s_occ;
 }
 
-// Warp-reduced traversal counters, one atomic per counter per warp.
-VRT_DI void warp_flush_stats(unsigned long long* stats, const DCount& c, uint32_t pix) {
-  const unsigned full = 0xffffffffu;
-  uint32_t r = __reduce_add_sync(full, c.rays);
-  uint32_t o = __reduce_add_sync(full, c.outer);
-  uint32_t i = __reduce_add_sync(full, c.inner);
-  uint32_t v = __reduce_add_sync(full, c.vreads);
-  uint32_t p = __reduce_add_sync(full, pix);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(stats + kStatRays, (unsigned long long)r);
-    atomicAdd(stats + kStatOuter, (unsigned long long)o);
-    atomicAdd(stats + kStatInner, (unsigned long long)i);
-    atomicAdd(stats + kStatVReads, (unsigned long long)v);
-    atomicAdd(stats + kStatPixels, (unsigned long long)p);
-  }
-}
 
 inline DScene to_dscene(const SceneDev& s) {
   DScene d;

@@ -272,6 +272,30 @@ struct DCount {
   uint32_t rays, outer, inner, vreads;
 };
 
+// Block-reduced traversal counters: stats[0..4] += rays, brick iterations,
+// voxel iterations, voxel reads, pixels of the block (the frame counters'
+// first five slots); one atomic per counter per block of 256 threads, since
+// every block adds to the same counters.  All threads of the block call it.
+VRT_DI void block_flush_stats(unsigned long long* stats, const DCount& c, uint32_t pix) {
+  __shared__ uint32_t s_part[8][5];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t v[5] = {__reduce_add_sync(full, c.rays), __reduce_add_sync(full, c.outer),
+                         __reduce_add_sync(full, c.inner), __reduce_add_sync(full, c.vreads),
+                         __reduce_add_sync(full, pix)};
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) s_part[w][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    unsigned long long tot = 0ull;
+#pragma unroll
+    for (int q = 0; q < 8; q++) tot += s_part[q][threadIdx.x];
+    if (tot) atomicAdd(stats + threadIdx.x, tot);
+  }
+}
+
 // Brick occupancy bit of brick bi from the bitmap `occ` (shared memory when
 // the kernel staged it, global otherwise).
 VRT_DI bool brick_occupied(const uint32_t* occ, uint32_t bi) {

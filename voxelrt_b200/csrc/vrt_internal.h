@@ -24,6 +24,8 @@ enum StatSlot {
   kStatError,   // nonzero: a bounded wait on staged copies ran out
   kStatCount = 8
 };
+static_assert(kStatRays == 0 && kStatOuter == 1 && kStatInner == 2 && kStatVReads == 3 && kStatPixels == 4,
+              "block_flush_stats adds to the first five counters in this order");
 
 // Device pointers of one frame's path-trace outputs.
 struct PathOut {

@@ -1,6 +1,6 @@
 // wavefront.cuh -- building blocks of the wavefront path tracer shared by the
 // single-session kernels (k_wavefront.cu) and the batched kernels
-// (k_batch.cu): path-state layout, warp-aggregated queue appends, the flat
+// (k_batch.cu): path-state layout, block-aggregated queue appends, the flat
 // two-level DDA, and per-vertex shading.
 #pragma once
 #include "vrt_device.cuh"
@@ -468,27 +468,65 @@ VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, uint32_t g, uint32_t k, F
   return want_shadow || want_bounce;
 }
 
-// Appends this warp's new rays / active paths for wave `next`.
-VRT_DI void emit(const WfDev& b, int next, uint32_t g, bool shadow, bool bounce, bool keep) {
-  uint32_t* q = queue_of(b, next);
-  uint32_t* a = active_of(b, next);
-  int* c = b.ctr + 4 * next;
-  const uint32_t s1 = warp_append(c, shadow);
-  if (shadow) q[s1] = g | kShadowBit;
-  const uint32_t s2 = warp_append(c, bounce);
-  if (bounce) q[s2] = g;
-  const uint32_t s3 = warp_append(c + 2, keep);
-  if (keep) a[s3] = g;
+// Block-aggregated appends: each thread of a block of 256 adds nr entries to
+// the ray queue counted by c_rays and, if act, one to the list counted by
+// c_act; one atomicAdd per counter per block, since every block of the grid
+// appends to the same counters.  Returns the thread's first ray slot (its nr
+// slots are consecutive) and its list slot.  All threads of the block call it
+// (block-uniform control flow).  Entries of a block are in thread order; a
+// path's results do not depend on the order of the queues.
+VRT_DI void block_append(int* c_rays, int* c_act, int nr, bool act, uint32_t& rslot, uint32_t& aslot) {
+  __shared__ int s_cnt[2][8];
+  __shared__ int s_base[2];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = nr;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const unsigned ma = __ballot_sync(full, act);
+  if (lane == 31) s_cnt[0][w] = incl;
+  if (lane == 0) s_cnt[1][w] = __popc(ma);
+  __syncthreads();
+  if (threadIdx.x < 2) {   // thread 0: rays, thread 1: list
+    int tot = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int v = s_cnt[threadIdx.x][k];
+      s_cnt[threadIdx.x][k] = tot;
+      tot += v;
+    }
+    s_base[threadIdx.x] = tot ? atomicAdd(threadIdx.x == 0 ? c_rays : c_act, tot) : 0;
+  }
+  __syncthreads();
+  rslot = (uint32_t)(s_base[0] + s_cnt[0][w] + incl - nr);
+  aslot = (uint32_t)(s_base[1] + s_cnt[1][w]) + (uint32_t)__popc(ma & ((1u << lane) - 1u));
+  __syncthreads();   // s_cnt / s_base are rewritten by the block's next call
 }
 
-// emit() with a second shadow ray of the path, traced as path g + P.
-VRT_DI void emit2(const WfDev& b, int next, uint32_t g, uint32_t P, bool shadow, bool shadow2, bool bounce,
-                  bool keep) {
+// Appends the new rays (shadow ray of path g, its bounce ray) and the active
+// path of wave `next`.  Block-uniform, see block_append.
+VRT_DI void emit_block(const WfDev& b, int next, uint32_t g, bool shadow, bool bounce, bool keep) {
+  uint32_t rs, as;
+  block_append(b.ctr + 4 * next, b.ctr + 4 * next + 2, (int)shadow + (int)bounce, keep, rs, as);
   uint32_t* q = queue_of(b, next);
-  int* c = b.ctr + 4 * next;
-  const uint32_t s0 = warp_append(c, shadow2);
-  if (shadow2) q[s0] = (g + P) | kShadowBit;
-  emit(b, next, g, shadow, bounce, keep);
+  if (shadow) q[rs++] = g | kShadowBit;
+  if (bounce) q[rs] = g;
+  if (keep) active_of(b, next)[as] = g;
+}
+
+// emit_block() with a second shadow ray of the path, traced as path g + P.
+VRT_DI void emit2_block(const WfDev& b, int next, uint32_t g, uint32_t P, bool shadow, bool shadow2, bool bounce,
+                        bool keep) {
+  uint32_t rs, as;
+  block_append(b.ctr + 4 * next, b.ctr + 4 * next + 2, (int)shadow2 + (int)shadow + (int)bounce, keep, rs, as);
+  uint32_t* q = queue_of(b, next);
+  if (shadow2) q[rs++] = (g + P) | kShadowBit;
+  if (shadow) q[rs++] = g | kShadowBit;
+  if (bounce) q[rs] = g;
+  if (keep) active_of(b, next)[as] = g;
 }
 
 // ---------------------------------------------------------------------------
@@ -597,18 +635,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       }
     }
   }
-  if (stats) {
-    const uint32_t r = __reduce_add_sync(full, c.rays);
-    const uint32_t o = __reduce_add_sync(full, c.outer);
-    const uint32_t in = __reduce_add_sync(full, c.inner);
-    const uint32_t v = __reduce_add_sync(full, c.vreads);
-    if (lane == 0) {
-      atomicAdd(stats + kStatRays, (unsigned long long)r);
-      atomicAdd(stats + kStatOuter, (unsigned long long)o);
-      atomicAdd(stats + kStatInner, (unsigned long long)in);
-      atomicAdd(stats + kStatVReads, (unsigned long long)v);
-    }
-  }
+  if (stats) block_flush_stats(stats, c, 0u);   // kStatRays..kStatVReads
 }
 
 // shade(0): primary hits over all pixels.
@@ -661,7 +688,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_primary(J jobs, uint32_t P, Wf
         }
       }
     }
-    emit(b, 1, g, shadow, bounce, keep);
+    emit_block(b, 1, g, shadow, bounce, keep);
     if (any_cache) cache_emit_samples(fin_train ? *ccp : jobs.cache(0), fin_train, ti, rfin);
   }
 }
@@ -731,7 +758,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(J jobs, WfDev b, int wave) {
         if (role == kRoleTrain) { fin_train = true; ti = train_index(cc, lp, W); rfin = radiance; }
       }
     }
-    emit(b, wave + 1, g, shadow, bounce, keep);
+    emit_block(b, wave + 1, g, shadow, bounce, keep);
     if (any_cache) {
       const CacheDev& cc = jobs.cache(jc);
       cache_emit_query(cc, query, g, qpos, qn, qalb);
