@@ -338,38 +338,88 @@ VRT_DI float cache_target(float rfin, float rk, float tpk, float clampv) {
   return v;
 }
 
+// The counter that every thread of the block with want set appends to, when
+// it is one counter (a single job's), or null when no thread appends; false
+// when the threads append to different counters (several jobs of a batch in
+// one block).  All threads of the block call it.
+VRT_DI bool block_common_counter(int* mine, bool want, int*& common) {
+  __shared__ int* s_c;
+  if (threadIdx.x == 0) s_c = nullptr;
+  __syncthreads();
+  if (want) s_c = mine;   // any of the writers
+  __syncthreads();
+  common = s_c;
+  return __syncthreads_and(!want || mine == common) != 0;
+}
+
+// One atomicAdd on ctr for the n entries of every thread of the block; the
+// thread's first slot (its n slots are consecutive).  All threads call it.
+VRT_DI uint32_t block_append1(int* ctr, int n) {
+  __shared__ int s_cnt[8];
+  __shared__ int s_base;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) s_cnt[w] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int v = s_cnt[k];
+      s_cnt[k] = tot;
+      tot += v;
+    }
+    s_base = tot ? atomicAdd(ctr, tot) : 0;
+  }
+  __syncthreads();
+  const uint32_t slot = (uint32_t)(s_base + s_cnt[w] + incl - n);
+  __syncthreads();   // s_cnt / s_base are rewritten by the block's next call
+  return slot;
+}
+
 // Training samples of finished training paths: for each recorded vertex k,
 // the radiance the path gathered after vertex k's emission pickup per unit
 // of the throughput that reached it, (R_final - R_k) / tp_k -- the reflected
-// radiance estimate at x_k.  Warp-aggregated append; all 32 lanes call.
-// When the warp's lanes belong to different jobs (batches) each lane
-// appends with its own atomic.
+// radiance estimate at x_k.  All threads of the block call it: one atomic per
+// block when its samples go to one job's buffer; otherwise per warp, or per
+// lane when a warp's lanes belong to different jobs.
 VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nrec = fin ? c.rec_n[ti] : 0;
-  const unsigned any = __ballot_sync(full, nrec > 0);
-  if (!any) return;
-  // one job among the lanes with samples?
-  const unsigned long long key = (unsigned long long)c.cand_count;
-  const unsigned grp = __match_any_sync(full, nrec > 0 ? key : 0ull) & any;
-  const bool one_job = nrec > 0 ? grp == any : true;
+  int* common = nullptr;
   int slot = 0;
-  if (__all_sync(full, one_job)) {
-    int incl = nrec;
+  if (block_common_counter(c.cand_count, nrec > 0, common)) {
+    if (!common) return;
+    slot = (int)block_append1(common, nrec);
+  } else {
+    const unsigned any = __ballot_sync(full, nrec > 0);
+    if (!any) return;
+    const unsigned long long key = (unsigned long long)c.cand_count;
+    const unsigned grp = __match_any_sync(full, nrec > 0 ? key : 0ull) & any;
+    const bool one_job = nrec > 0 ? grp == any : true;
+    if (__all_sync(full, one_job)) {
+      int incl = nrec;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(full, incl, o);
-      if (lane >= o) incl += v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(full, incl, 31);
+      const int leader = __ffs(any) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(c.cand_count, total);
+      base = __shfl_sync(full, base, leader);
+      slot = base + incl - nrec;
+    } else if (nrec > 0) {
+      slot = atomicAdd(c.cand_count, nrec);
     }
-    const int total = __shfl_sync(full, incl, 31);
-    const int leader = __ffs(any) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(c.cand_count, total);
-    base = __shfl_sync(full, base, leader);
-    slot = base + incl - nrec;
-  } else if (nrec > 0) {
-    slot = atomicAdd(c.cand_count, nrec);
   }
   for (int k = 0; k < nrec && slot < c.cand_cap; k++, slot++) {
     const float4* r = c.rec + ((size_t)ti * kCacheMaxRec + k) * 4;
@@ -385,15 +435,22 @@ VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin
   }
 }
 
-// Appends a cache query of path g at its vertex 1.  All 32 lanes call.
+// Appends a cache query of path g at its vertex 1.  All threads of the block
+// call it; one atomic per block when its queries go to one job's buffer.
 VRT_DI void cache_emit_query(const CacheDev& c, bool q, uint32_t g, F3 pos, F3 n, F3 alb) {
   const unsigned full = 0xffffffffu;
-  const unsigned any = __ballot_sync(full, q);
-  if (!any) return;
-  const unsigned grp = __match_any_sync(full, q ? (unsigned long long)c.qcount : 0ull) & any;
-  uint32_t slot;
-  if (__all_sync(full, q ? grp == any : true)) slot = warp_append(c.qcount, q);
-  else slot = q ? (uint32_t)atomicAdd(c.qcount, 1) : 0u;
+  int* common = nullptr;
+  uint32_t slot = 0u;
+  if (block_common_counter(c.qcount, q, common)) {
+    if (!common) return;
+    slot = block_append1(common, q ? 1 : 0);
+  } else {
+    const unsigned any = __ballot_sync(full, q);
+    if (!any) return;
+    const unsigned grp = __match_any_sync(full, q ? (unsigned long long)c.qcount : 0ull) & any;
+    if (__all_sync(full, q ? grp == any : true)) slot = warp_append(c.qcount, q);
+    else slot = q ? (uint32_t)atomicAdd(c.qcount, 1) : 0u;
+  }
   if (q) {
     float* d = c.qbuf + (size_t)slot * 9;
     d[0] = pos.x; d[1] = pos.y; d[2] = pos.z;
