@@ -48,6 +48,12 @@ VRT_DI int iclamp_(int x, int lo, int hi) { return min(max(x, lo), hi); }
 // floor to int with saturation (NaN -> 0): cvt.rmi.s32.f32.
 VRT_DI int ifloor_(float x) { return __float2int_rd(x); }
 
+// safeInv (voxel.wgsl:65-71): sg / max(|v|, 1e-8) with sg = +-1, evaluated as
+// sg times the correctly rounded reciprocal (__frcp_rn, IEEE round to
+// nearest): multiplying by +-1 is exact, so the value equals the IEEE
+// quotient for every input, NaN and infinity included.
+VRT_DI float safe_inv(float sg, float v) { return sg * __frcp_rn(fmax_(fabsf(v), 1e-8f)); }
+
 struct F3 { float x, y, z; };
 VRT_DI F3 f3(float x, float y, float z) { return F3{x, y, z}; }
 VRT_DI F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -330,8 +336,7 @@ VRT_DI DHit trace(const DScene& S, const uint32_t* occ, F3 roW, F3 rd, float max
   const float sgx = rd.x >= 0.0f ? 1.0f : -1.0f;
   const float sgy = rd.y >= 0.0f ? 1.0f : -1.0f;
   const float sgz = rd.z >= 0.0f ? 1.0f : -1.0f;
-  const F3 invRd = f3(sgx / fmax_(fabsf(rd.x), 1e-8f), sgy / fmax_(fabsf(rd.y), 1e-8f),
-                      sgz / fmax_(fabsf(rd.z), 1e-8f));
+  const F3 invRd = f3(safe_inv(sgx, rd.x), safe_inv(sgy, rd.y), safe_inv(sgz, rd.z));
   const int sx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
   const int sy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
   const int sz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);

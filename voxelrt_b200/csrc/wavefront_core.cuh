@@ -64,8 +64,8 @@ VRT_DI F3 hit_normal(int vax, F3 rd) {
 // Two-level DDA as one resumable iteration shared by both levels
 // (voxel.wgsl:73-153).  Each call performs
 //   [pending step at the current level] + [test of the current cell],
-// so lanes walking bricks and lanes walking voxels execute the same code
-// with level-selected operands.  Transitions reproduce the nested loops:
+// so lanes walking bricks and lanes walking voxels execute the same code.
+// Transitions reproduce the nested loops:
 //   brick test occupied  -> descend (entry voxel from t + 1e-4, next call
 //                           tests it without stepping)
 //   voxel test occupied  -> hit (voxel read, maxT check)
@@ -78,46 +78,53 @@ VRT_DI F3 hit_normal(int vax, F3 rd) {
 // ---------------------------------------------------------------------------
 enum : int { kLevelVoxel = 1, kPending = 2, kDone = 4, kHitCell = 8 };
 
+// Register layout: tm / (cx, cy, cz) / t / ax hold the current level's state
+// -- the brick level's tMaxB, brick cell, t and ax while walking bricks, the
+// voxel level's tMaxV, local cell, tCur and vax while walking voxels -- so the
+// step reads no level-selected operands; the brick level's tMax and cell are
+// saved in tmB / (bx, by, bz) on descent and restored when the voxel walk ends
+// (t and ax need no restore: the brick step that follows rewrites them).  The
+// step's scale (8 or 1) and coordinate bound (BG - 1 or 7) are per-level
+// registers, and only the stepped coordinate is bounds-checked (the others did
+// not move).  The entry axis left in ax after a miss is not meaningful; every
+// consumer reads it for hits only.  Against a layout with both levels' state
+// and per-operand level selects: 1.61 -> 1.48 ms of trace on the 1080p frame.
 struct FlatDDA {
   F3 ro, invRd;
   float maxT, tExit;
-  float t, tCur;                // brick-level t, voxel-level t
-  F3 tMaxB, tMaxV;
-  int bx, by, bz;               // brick cell
-  int lx, ly, lz;               // voxel cell, local to the brick (0..7)
+  F3 tm, tmB;
+  int cx, cy, cz;               // current cell (brick, or voxel local to the brick)
+  int bx, by, bz;               // brick cell while walking voxels
   int sx, sy, sz;
-  int ax, vax, iter, j;
-  int state;
+  float t, sc;
+  int lim, ax, iter, j, state;
+  uint32_t bi;                  // brick index while walking voxels
   float tHit;
   uint32_t mat;
 
   VRT_DI bool done() const { return (state & kDone) != 0; }
+  VRT_DI int hit_axis() const { return ax; }
 
-  // The walk's result once done(): at an occupied voxel the voxel word is read
-  // and the hit kept unless it lies beyond maxT (voxel.wgsl:128-137).  Kept
-  // out of step() so that the unrolled steps carry neither the read nor the
-  // result registers.
   VRT_DI void finish(const DScene& S, DCount& c) {
     tHit = -1.0f;
     mat = 0u;
     if (state & kHitCell) {
-      const uint32_t vx = (uint32_t)(bx * kBrick + lx), vy = (uint32_t)(by * kBrick + ly),
-                     vz = (uint32_t)(bz * kBrick + lz);
+      const uint32_t vx = (uint32_t)(bx * kBrick + cx), vy = (uint32_t)(by * kBrick + cy),
+                     vz = (uint32_t)(bz * kBrick + cz);
       mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
       c.vreads++;
-      if (!(tCur > maxT)) tHit = tCur * kVoxelSize;
+      if (!(t > maxT)) tHit = t * kVoxelSize;
       else mat = 0u;
     }
   }
 
   VRT_DI void init(const DScene& S, F3 roW, F3 rd, float maxTW) {
-    vax = 0;
     ro = roW * kInvVoxel;
     maxT = maxTW * kInvVoxel;
     const float sgx = rd.x >= 0.0f ? 1.0f : -1.0f;
     const float sgy = rd.y >= 0.0f ? 1.0f : -1.0f;
     const float sgz = rd.z >= 0.0f ? 1.0f : -1.0f;
-    invRd = f3(sgx / fmax_(fabsf(rd.x), 1e-8f), sgy / fmax_(fabsf(rd.y), 1e-8f), sgz / fmax_(fabsf(rd.z), 1e-8f));
+    invRd = f3(safe_inv(sgx, rd.x), safe_inv(sgy, rd.y), safe_inv(sgz, rd.z));
     sx = rd.x > 0.0f ? 1 : (rd.x < 0.0f ? -1 : 0);
     sy = rd.y > 0.0f ? 1 : (rd.y < 0.0f ? -1 : 0);
     sz = rd.z > 0.0f ? 1 : (rd.z < 0.0f ? -1 : 0);
@@ -131,75 +138,54 @@ struct FlatDDA {
     tExit = fmin_(fmin_(tmax3.x, tmax3.y), fmin_(tmax3.z, maxT));
     iter = 0;
     j = 0;
-    lx = ly = lz = 0;
+    ax = 0;
     if (tEnter > tExit) { state = kDone; return; }
     if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) ax = 0;
     else if (tmin3.y >= tmin3.z) ax = 1;
     else ax = 2;
     t = tEnter;
     const F3 sp = ro + rd * (t + 1e-4f);
-    bx = iclamp_(ifloor_(sp.x / 8.0f), 0, S.BG - 1);
-    by = iclamp_(ifloor_(sp.y / 8.0f), 0, S.BG - 1);
-    bz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
-    tMaxB = ((f3((float)bx, (float)by, (float)bz) + stepGE) * 8.0f - ro) * invRd;
+    cx = iclamp_(ifloor_(sp.x / 8.0f), 0, S.BG - 1);
+    cy = iclamp_(ifloor_(sp.y / 8.0f), 0, S.BG - 1);
+    cz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
+    tm = ((f3((float)cx, (float)cy, (float)cz) + stepGE) * 8.0f - ro) * invRd;
+    sc = 8.0f;
+    lim = S.BG - 1;
     state = 0;   // brick level, test first
   }
 
-  // Enters the occupied brick (bx, by, bz) at t: the entry voxel from
-  // t + 1e-4 (voxel.wgsl:104-109), its tMax, and a test without stepping next.
-  VRT_DI void descend(const DScene& S, F3 rd) {
-    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
-    const F3 p = ro + rd * (t + 1e-4f);
-    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
-    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
-    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
-    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
-    tMaxV = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
-    lx = vx - mnx; ly = vy - mny; lz = vz - mnz;
-    tCur = t;
-    vax = ax;
-    j = 0;
-    state = kLevelVoxel;
+  // The voxel walk of the current brick ends: brick step next.
+  VRT_DI void leave_brick(const DScene& S) {
+    cx = bx; cy = by; cz = bz;
+    tm = tmB;
+    sc = 8.0f;
+    lim = S.BG - 1;
+    state = kPending;
   }
 
   VRT_DI void step(const DScene& S, const uint32_t* occ, F3 rd, DCount& c) {
     const bool lv = (state & kLevelVoxel) != 0;
     if (state & kPending) {
-      // ---- one DDA step at the current level --------------------------
-      const float mx = lv ? tMaxV.x : tMaxB.x;
-      const float my = lv ? tMaxV.y : tMaxB.y;
-      const float mz = lv ? tMaxV.z : tMaxB.z;
-      const bool cx = mx <= my && mx <= mz;
-      const bool cy = !cx && my <= mz;
-      const bool cz = !cx && !cy;
-      const float tn = cx ? mx : (cy ? my : mz);
-      const float ia = fabsf(cx ? invRd.x : (cy ? invRd.y : invRd.z));
-      const float nv = __fmaf_rn(ia, lv ? 1.0f : 8.0f, tn);
-      const F3 m = f3(cx ? nv : mx, cy ? nv : my, cz ? nv : mz);
-      const int a = cx ? 0 : (cy ? 1 : 2);
-      const int dx = cx ? sx : 0, dy = cy ? sy : 0, dz = cz ? sz : 0;
-      if (lv) {
-        tMaxV = m; tCur = tn; vax = a;
-        lx += dx; ly += dy; lz += dz;
-        if ((unsigned)(lx | ly | lz) > 7u) {
-          state = kPending;                  // left the brick: brick step next
-          return;
-        }
-      } else {
-        tMaxB = m; t = tn; ax = a;
-        bx += dx; by += dy; bz += dz;
-        if ((unsigned)bx >= (unsigned)S.BG || (unsigned)by >= (unsigned)S.BG || (unsigned)bz >= (unsigned)S.BG) {
-          state = kDone;
-          return;
-        }
+      const bool px = tm.x <= tm.y && tm.x <= tm.z;
+      const bool py = !px && tm.y <= tm.z;
+      const float tn = px ? tm.x : (py ? tm.y : tm.z);
+      const float ia = fabsf(px ? invRd.x : (py ? invRd.y : invRd.z));
+      const float nv = __fmaf_rn(ia, sc, tn);
+      int cn;
+      if (px) { tm.x = nv; cx += sx; cn = cx; }
+      else if (py) { tm.y = nv; cy += sy; cn = cy; }
+      else { tm.z = nv; cz += sz; cn = cz; }
+      t = tn;
+      ax = px ? 0 : (py ? 1 : 2);
+      if ((unsigned)cn > (unsigned)lim) {   // left the brick (voxel walk) or the grid (brick walk)
+        if (lv) leave_brick(S);
+        else state = kDone;
+        return;
       }
       state &= ~kPending;
     }
-    // ---- test the current cell ------------------------------------------
-    const uint32_t bi = (uint32_t)bx + (uint32_t)by * (uint32_t)S.BG + (uint32_t)bz * (uint32_t)(S.BG * S.BG);
-    const uint32_t lbit = (uint32_t)(lx + ly * 8 + lz * 64);
     if (lv) {
-      if (j >= 3 * kBrick) { state = kPending; return; }   // voxel loop exhausted
+      if (j >= 3 * kBrick) { leave_brick(S); return; }   // voxel loop exhausted
       j++;
       c.inner++;
     } else {
@@ -207,10 +193,11 @@ struct FlatDDA {
       iter++;
       c.outer++;
     }
-    const uint32_t* wp = lv ? (S.masks + (size_t)bi * 16u + (lbit >> 5)) : (occ + (bi >> 5));
-    const uint32_t sh = lv ? (lbit & 31u) : (bi & 31u);
-    const bool hitcell = ((*wp >> sh) & 1u) != 0u;
-    if (!hitcell) {
+    const uint32_t bidx = lv ? bi : (uint32_t)cx + (uint32_t)cy * (uint32_t)S.BG + (uint32_t)cz * (uint32_t)(S.BG * S.BG);
+    const uint32_t lbit = (uint32_t)(cx + cy * 8 + cz * 64);
+    const uint32_t* wp = lv ? (S.masks + (size_t)bidx * 16u + (lbit >> 5)) : (occ + (bidx >> 5));
+    const uint32_t sh = lv ? (lbit & 31u) : (bidx & 31u);
+    if (!((*wp >> sh) & 1u)) {
       state |= kPending;
       return;
     }
@@ -218,7 +205,22 @@ struct FlatDDA {
       state = kDone | kHitCell;   // finish() reads the voxel
       return;
     }
-    descend(S, rd);
+    // descend into the occupied brick (voxel.wgsl:104-109); t and ax carry over as tCur and vax
+    bx = cx; by = cy; bz = cz;
+    bi = bidx;
+    tmB = tm;
+    const int mnx = bx * kBrick, mny = by * kBrick, mnz = bz * kBrick;
+    const F3 p = ro + rd * (t + 1e-4f);
+    const int vx = iclamp_(ifloor_(p.x), mnx, mnx + 7);
+    const int vy = iclamp_(ifloor_(p.y), mny, mny + 7);
+    const int vz = iclamp_(ifloor_(p.z), mnz, mnz + 7);
+    const F3 stepGE = f3(rd.x >= 0.0f ? 1.0f : 0.0f, rd.y >= 0.0f ? 1.0f : 0.0f, rd.z >= 0.0f ? 1.0f : 0.0f);
+    tm = ((f3((float)vx, (float)vy, (float)vz) + stepGE) - ro) * invRd;
+    cx = vx - mnx; cy = vy - mny; cz = vz - mnz;
+    j = 0;
+    sc = 1.0f;
+    lim = 7;
+    state = kLevelVoxel;
   }
 };
 
@@ -686,7 +688,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
           h[3] = d.tHit >= 0.0f ? 1u : 0u;
         } else {
           *reinterpret_cast<uint2*>(h) = make_uint2(__float_as_uint(d.tHit), d.mat);
-          h[2] = (uint32_t)d.vax;
+          h[2] = (uint32_t)d.hit_axis();
         }
         active = false;
       }
@@ -994,19 +996,20 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 
 // Tracer variants (the autotuner's trace_variant): DDA iterations per pass of
 // the warp bookkeeping x minimum resident blocks per SM (register cap).
-// Measured on the 1080p / 256^3 frame: 8 x 5 (48 registers) 1.66 ms of trace,
-// 6 x 5 1.67, 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98,
-// 1 x 1 2.20 ms.  (Stepping until enough lanes are idle, with a ballot after
-// every iteration, ran 1.88 ms: the per-iteration ballot costs more than the
-// idle lanes of a fixed pass.)  Also measured and dropped, each bit-identical:
-// a step with every outcome selected instead of branched (only the descent
-// branched) 2.02 ms; descents parked until the end of each pass, so that a
-// warp runs the descent block once per pass, 1.71 (4 x 5) - 1.80 ms (8 x 5);
-// an exact empty-space skip (brick distance field and 4^3 sub-block masks,
-// the skipped steps replayed in closed form per axis: 41% fewer step calls on
-// this frame) 2.2 - 3.3 ms, because a warp runs the ~100-instruction replay in
-// nearly every step in which one of its lanes needs it.  The frame with the
-// 8 x 5 default: 1.60 ms of trace.
+// Measured on the 1080p / 256^3 frame with FlatDDA's current-level register
+// layout: 8 x 5 (48 registers) 1.48 ms of trace, 6 x 5 1.49, 12 x 5 1.63,
+// 16 x 5 1.69 ms; with the earlier layout 8 x 5 1.60-1.66, 6 x 5 1.67,
+// 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98, 1 x 1 2.20 ms.
+// (Stepping until enough lanes are idle, with a ballot after every iteration,
+// ran 1.88 ms: the per-iteration ballot costs more than the idle lanes of a
+// fixed pass.)  Also measured with the earlier layout and dropped, each
+// bit-identical: a step with every outcome selected instead of branched (only
+// the descent branched) 2.02 ms; descents parked until the end of each pass,
+// so that a warp runs the descent block once per pass, 1.71 (4 x 5) - 1.80 ms
+// (8 x 5); an exact empty-space skip (brick distance field and 4^3 sub-block
+// masks, the skipped steps replayed in closed form per axis: 41% fewer step
+// calls on this frame) 2.2 - 3.3 ms, because a warp runs the ~100-instruction
+// replay in nearly every step in which one of its lanes needs it.
 template <class J, bool kSmem, bool kVarMaxT = false>
 cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int sms, const WfDev& b, int w, int impl,
                               int refill, unsigned long long* stats, cudaStream_t st) {
