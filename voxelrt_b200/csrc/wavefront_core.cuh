@@ -105,10 +105,15 @@ struct FlatDDA {
   VRT_DI bool done() const { return (state & kDone) != 0; }
   VRT_DI int hit_axis() const { return ax; }
 
+  // Counters: brick iterations entered = iter at the end of the walk; voxel
+  // iterations = the sum of j over the bricks walked (added as each voxel
+  // walk ends), so the steps count nothing.
   VRT_DI void finish(const DScene& S, DCount& c) {
     tHit = -1.0f;
     mat = 0u;
+    c.outer += (uint32_t)iter;
     if (state & kHitCell) {
+      c.inner += (uint32_t)j;
       const uint32_t vx = (uint32_t)(bx * kBrick + cx), vy = (uint32_t)(by * kBrick + cy),
                      vz = (uint32_t)(bz * kBrick + cz);
       mat = __ldg(S.vox + (vx + vy * (uint32_t)S.N + vz * (uint32_t)(S.N * S.N)));
@@ -155,7 +160,8 @@ struct FlatDDA {
   }
 
   // The voxel walk of the current brick ends: brick step next.
-  VRT_DI void leave_brick(const DScene& S) {
+  VRT_DI void leave_brick(const DScene& S, DCount& c) {
+    c.inner += (uint32_t)j;
     cx = bx; cy = by; cz = bz;
     tm = tmB;
     sc = 8.0f;
@@ -178,20 +184,18 @@ struct FlatDDA {
       t = tn;
       ax = px ? 0 : (py ? 1 : 2);
       if ((unsigned)cn > (unsigned)lim) {   // left the brick (voxel walk) or the grid (brick walk)
-        if (lv) leave_brick(S);
+        if (lv) leave_brick(S, c);
         else state = kDone;
         return;
       }
       state &= ~kPending;
     }
     if (lv) {
-      if (j >= 3 * kBrick) { leave_brick(S); return; }   // voxel loop exhausted
+      if (j >= 3 * kBrick) { leave_brick(S, c); return; }   // voxel loop exhausted
       j++;
-      c.inner++;
     } else {
       if (iter >= 3 * S.BG + 2 || t > tExit) { state = kDone; return; }
       iter++;
-      c.outer++;
     }
     const uint32_t bidx = lv ? bi : (uint32_t)cx + (uint32_t)cy * (uint32_t)S.BG + (uint32_t)cz * (uint32_t)(S.BG * S.BG);
     const uint32_t lbit = (uint32_t)(cx + cy * 8 + cz * 64);
