@@ -113,7 +113,7 @@ VRT_DI float4 atrous_pixel(int W, int H, int px, int py, const void* __restrict_
       if (n32 == 0.0f) continue;
       const float4 cq = load_px(src, srcF32, q);
       const float wKernel = b3_weight(dx) * b3_weight(dy);
-      const float e = exp_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
+      const float e = exp_nonpos_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
       const float w = (wKernel * n32) * e;
       sr = __fmaf_rn(cq.x, w, sr);
       sg = __fmaf_rn(cq.y, w, sg);
@@ -155,7 +155,7 @@ VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const
       if (n32 == 0.0f) continue;
       const float4 cq = sc[qi];
       const float wKernel = b3_weight(dx) * b3_weight(dy);
-      const float e = exp_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - cq.w) * invS));
+      const float e = exp_nonpos_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - cq.w) * invS));
       const float w = (wKernel * n32) * e;
       sr = __fmaf_rn(cq.x, w, sr);
       sg_ = __fmaf_rn(cq.y, w, sg_);

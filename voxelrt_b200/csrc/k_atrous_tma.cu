@@ -7,7 +7,10 @@
 // side -- completing on one mbarrier; pixels outside the image arrive as zeros
 // (a zero normal gives a zero edge weight, the same as skipping the tap).
 // The threads then convert the staged source to fp32 once per pixel, with its
-// luminance in .w, and evaluate the 24 taps from shared memory.  The per-tap
+// luminance in .w, over the copied tile itself (each thread reads its pixels
+// before the block rewrites them: 32 bytes of shared memory per staged pixel,
+// 49 KB at step 4), read their centre pixel with its history alpha from global
+// memory, and evaluate the 24 taps from shared memory.  The per-tap
 // arithmetic and its order are those of atrous_pixel (image_core.cuh), so the
 // output is bit-identical to the plain kernel's.
 //
@@ -30,9 +33,11 @@ constexpr uint32_t kTmaSpin = 1u << 22;      // bounded wait for the copies (try
 
 __host__ __device__ constexpr int align128(int x) { return (x + 127) & ~127; }
 __host__ __device__ constexpr int tile_px(int step) { return (kTX + 4 * step) * (kTY + 4 * step); }
-__host__ __device__ constexpr int tile_smem(int step, bool src_f32) {
-  return align128(tile_px(step) * 16) + align128(tile_px(step) * (src_f32 ? 16 : 8)) + tile_px(step) * 16;
-}
+// G-buffer tile + source tile (rgba16f or rgba32f as copied, expanded in place
+// to fp32 with its luminance); the steps are 1, 2, 4.
+__host__ __device__ constexpr int tile_smem(int step) { return align128(tile_px(step) * 16) + tile_px(step) * 16; }
+constexpr int kMaxTilePx = tile_px(4);
+static_assert(kMaxTilePx % 256 == 0, "staged pixels per thread");
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_u32(mbar)), "r"(bytes)
@@ -59,14 +64,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, in
 template <bool kSrcF32>
 __global__ void __launch_bounds__(256) k_atrous_tma(const __grid_constant__ CUtensorMap tm_src,
                                                     const __grid_constant__ CUtensorMap tm_g, int W, int H,
-                                                    uint2* __restrict__ dst, int step, unsigned long long* err) {
+                                                    const void* __restrict__ src, uint2* __restrict__ dst, int step,
+                                                    unsigned long long* err) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ uint64_t mbar;
   const int hx = 2 * step;
   const int RW = kTX + 2 * hx, RH = kTY + 2 * hx, npx = RW * RH;
   float4* sg = reinterpret_cast<float4*>(smem);
-  uint8_t* ssrc = smem + align128(npx * 16);
-  float4* sc = reinterpret_cast<float4*>(ssrc + align128(npx * (kSrcF32 ? 16 : 8)));
+  uint8_t* ssrc = smem + align128(npx * 16);          // the source tile as copied, expanded in place below
+  float4* sc = reinterpret_cast<float4*>(ssrc);
   const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
   const int t = threadIdx.x;
   if (t == 0) umma::mbar_init(&mbar, 1);
@@ -83,11 +89,32 @@ __global__ void __launch_bounds__(256) k_atrous_tma(const __grid_constant__ CUte
     umma::mbar_wait(&mbar, 0, kTmaSpin);
     return;
   }
-  // fp32 source with its luminance in .w, once per staged pixel
-  for (int i = t; i < npx; i += 256) {
-    float4 c = kSrcF32 ? reinterpret_cast<const float4*>(ssrc)[i] : unpack_h4(reinterpret_cast<const uint2*>(ssrc)[i]);
-    c.w = luminance(c.x, c.y, c.z);
-    sc[i] = c;
+  // fp32 source with its luminance in .w, once per staged pixel, written over
+  // the copied tile: an rgba32f pixel in its own slot; rgba16f pixels (half
+  // the size) are read by every thread before the block rewrites them.
+  if (kSrcF32) {
+    for (int i = t; i < npx; i += 256) {
+      float4 c = sc[i];
+      c.w = luminance(c.x, c.y, c.z);
+      sc[i] = c;
+    }
+  } else {
+    uint2 raw[kMaxTilePx / 256];
+#pragma unroll
+    for (int k = 0; k < kMaxTilePx / 256; k++) {
+      const int i = t + 256 * k;
+      if (i < npx) raw[k] = reinterpret_cast<const uint2*>(ssrc)[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kMaxTilePx / 256; k++) {
+      const int i = t + 256 * k;
+      if (i < npx) {
+        float4 c = unpack_h4(raw[k]);
+        c.w = luminance(c.x, c.y, c.z);
+        sc[i] = c;
+      }
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -96,10 +123,11 @@ __global__ void __launch_bounds__(256) k_atrous_tma(const __grid_constant__ CUte
     const int px = x0 + lx, py = y0 + ly;
     if (px >= W || py >= H) continue;
     const int ci = (ly + hx) * RW + (lx + hx);
-    const float4 center = kSrcF32 ? reinterpret_cast<const float4*>(ssrc)[ci]
-                                  : unpack_h4(reinterpret_cast<const uint2*>(ssrc)[ci]);
+    const size_t p = (size_t)py * W + px;
+    const float4 center = kSrcF32 ? __ldg(reinterpret_cast<const float4*>(src) + p)
+                                  : unpack_h4(__ldg(reinterpret_cast<const uint2*>(src) + p));
     const float4 v = atrous_pixel_tile(center, sg[ci], sg, sc, ci, RW, step);
-    dst[(size_t)py * W + px] = pack_h4(v.x, v.y, v.z, v.w);
+    dst[p] = pack_h4(v.x, v.y, v.z, v.w);
   }
 }
 
@@ -155,17 +183,17 @@ cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, co
   const bool enc = map_f32x4(&tg, gbuf, W, H, bw, bh) &&
                    (src_f32 ? map_f32x4(&ts, src, W, H, bw, bh) : map_h4(&ts, src, W, H, bw, bh));
   if (!enc) return launch_atrous(W, H, src, src_f32, gbuf, dst, step, st);
-  const int smem = tile_smem(step, src_f32);
+  const int smem = tile_smem(step);
   dim3 grid((W + kTX - 1) / kTX, (H + kTY - 1) / kTY);
   cudaError_t e;
   if (src_f32) {
-    e = cudaFuncSetAttribute(k_atrous_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4, true));
+    e = cudaFuncSetAttribute(k_atrous_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4));
     if (e != cudaSuccess) return e;
-    k_atrous_tma<true><<<grid, 256, smem, st>>>(ts, tg, W, H, (uint2*)dst, step, err);
+    k_atrous_tma<true><<<grid, 256, smem, st>>>(ts, tg, W, H, src, (uint2*)dst, step, err);
   } else {
-    e = cudaFuncSetAttribute(k_atrous_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4, false));
+    e = cudaFuncSetAttribute(k_atrous_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4));
     if (e != cudaSuccess) return e;
-    k_atrous_tma<false><<<grid, 256, smem, st>>>(ts, tg, W, H, (uint2*)dst, step, err);
+    k_atrous_tma<false><<<grid, 256, smem, st>>>(ts, tg, W, H, src, (uint2*)dst, step, err);
   }
   return cudaGetLastError();
 }

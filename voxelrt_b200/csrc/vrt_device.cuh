@@ -127,6 +127,21 @@ VRT_DI float exp_(float x) {
   return exp_poly_(r) * pow2i_((int)kf);
 }
 
+// exp_ for x <= 0 (and NaN), as the a-trous weights use it: the same
+// reduction and polynomial, with the scaling by 2^k done by adding k to the
+// exponent field.  That equals exp_'s multiplication exactly because every
+// result for x in (-87, 0] is normal: the polynomial p lies in [0.707, 1.415)
+// and k >= -126, with p > 1 whenever k = -126 (x < -86.988).
+VRT_DI float exp_nonpos_(float x) {
+  if (!(x > -87.0f)) return 0.0f;
+  const float LOG2E = 1.44269502f;
+  const float LN2_HI = 0.693145751953125f;
+  const float LN2_LO = 1.42860677e-06f;
+  const float kf = floorf(__fmaf_rn(x, LOG2E, 0.5f));
+  const float r = __fmaf_rn(-kf, LN2_LO, __fmaf_rn(-kf, LN2_HI, x));
+  return __int_as_float(__float_as_int(exp_poly_(r)) + ((int)kf << 23));
+}
+
 VRT_DI float exp2_(float z) {
   if (!(z > -126.0f)) return 0.0f;
   if (z > 127.0f) return __int_as_float(0x7f800000);
