@@ -199,9 +199,11 @@ struct FlatDDA {
     }
     const uint32_t bidx = lv ? bi : (uint32_t)cx + (uint32_t)cy * (uint32_t)S.BG + (uint32_t)cz * (uint32_t)(S.BG * S.BG);
     const uint32_t lbit = (uint32_t)(cx + cy * 8 + cz * 64);
-    const uint32_t* wp = lv ? (S.masks + (size_t)bidx * 16u + (lbit >> 5)) : (occ + (bidx >> 5));
+    // two typed loads (the bitmap may be in shared memory, the masks are in
+    // global memory) rather than one load through a selected pointer
+    const uint32_t word = lv ? __ldg(S.masks + (size_t)bidx * 16u + (lbit >> 5)) : occ[bidx >> 5];
     const uint32_t sh = lv ? (lbit & 31u) : (bidx & 31u);
-    if (!((*wp >> sh) & 1u)) {
+    if (!((word >> sh) & 1u)) {
       state |= kPending;
       return;
     }
@@ -1002,7 +1004,8 @@ cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms,
 // the warp bookkeeping x minimum resident blocks per SM (register cap).
 // Measured on the 1080p / 256^3 frame with FlatDDA's current-level register
 // layout: 8 x 5 (48 registers) 1.48 ms of trace, 6 x 5 1.49, 12 x 5 1.63,
-// 16 x 5 1.69 ms; with the earlier layout 8 x 5 1.60-1.66, 6 x 5 1.67,
+// 16 x 5 1.69 ms; with the typed test loads 8 x 5 1.436, 8 x 6 (40 registers,
+// spilling) 1.491, 8 x 4 (59 registers) 1.497 ms; with the earlier layout 8 x 5 1.60-1.66, 6 x 5 1.67,
 // 6 x 4 (57 registers) 1.71, 4 x 4 1.74, 2 x 1 (69) 1.98, 1 x 1 2.20 ms.
 // (Stepping until enough lanes are idle, with a ballot after every iteration,
 // ran 1.88 ms: the per-iteration ballot costs more than the idle lanes of a
