@@ -88,7 +88,10 @@ def profiled_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks + throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks + throttle reasons sampled every 20 ms while the timed
+    region runs.  start() returns once the sampler has produced its first line
+    (nvidia-smi's own startup can outlast a short timed region); stop() keeps
+    the samples taken between start() and stop()."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -96,27 +99,48 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []
+        self.t0 = 0.0
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.perf_counter(), line))
 
     def start(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                          "-lms", "20", "-i", str(self.device)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+        deadline = time.perf_counter() + 5.0
+        while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.t0 = time.perf_counter()
 
     def stop(self):
         if self.proc is None:
             return None
+        t1 = time.perf_counter()
+        time.sleep(0.03)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+            self.proc.wait()
+        self.th.join(timeout=5)
+        inside = [ln for t, ln in self.lines if self.t0 <= t <= t1 + 0.03]
+        if not inside and self.lines:
+            inside = [self.lines[-1][1]]
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in inside:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
