@@ -656,28 +656,37 @@ struct VecSink {
 // partner falls off the image (rejected by the caller's bounds test).
 VRT_DI int wrap_mod(int v, int sz) { return ((v % sz) + sz) % sz; }
 
-VRT_DI void paired_partner(const RestirDev& R, int px, int py, uint32_t ti, int& qx, int& qy) {
-  const int sz = ti == 0u ? 254 : (ti == 1u ? 230 : 210);
-  const uint32_t off = ti == 0u ? 0u : (ti == 1u ? 64516u : 117416u);
+// Texture ti of size kSz at word offset kOff; the sizes are compile-time
+// constants so that the modulos reduce to multiplies.
+template <int kSz, uint32_t kOff>
+VRT_DI void paired_partner_sz(const RestirDev& R, int px, int py, uint32_t ti, int& qx, int& qy) {
   const uint32_t h = pcg_hash(R.u.params0[0] * 2654435761u + ti * 0x68bc21ebu + 0x9e3779b9u);
   const uint32_t h2 = pcg_hash(h);
-  const int ox = (int)(h % (uint32_t)sz), oy = (int)(h2 % (uint32_t)sz);
+  const int ox = (int)(h % (uint32_t)kSz), oy = (int)(h2 % (uint32_t)kSz);
   const bool mx = (h & 0x40000000u) != 0u, my = (h & 0x20000000u) != 0u, sw = (h & 0x10000000u) != 0u;
-  int ax = wrap_mod(px + ox, sz), ay = wrap_mod(py + oy, sz);
+  int ax = wrap_mod(px + ox, kSz), ay = wrap_mod(py + oy, kSz);
   if (sw) { const int t = ax; ax = ay; ay = t; }
-  if (mx) ax = sz - 1 - ax;
-  if (my) ay = sz - 1 - ay;
-  const uint32_t word = R.pairing[off + (uint32_t)(ay * sz + ax)];
+  if (mx) ax = kSz - 1 - ax;
+  if (my) ay = kSz - 1 - ay;
+  const uint32_t word = R.pairing[kOff + (uint32_t)(ay * kSz + ax)];
   const int dtx = (int)(word << 16) >> 16, dty = (int)word >> 16;
-  int bx = wrap_mod(ax + dtx, sz), by = wrap_mod(ay + dty, sz);
-  if (mx) bx = sz - 1 - bx;
-  if (my) by = sz - 1 - by;
+  int bx = wrap_mod(ax + dtx, kSz), by = wrap_mod(ay + dty, kSz);
+  if (mx) bx = kSz - 1 - bx;
+  if (my) by = kSz - 1 - by;
   if (sw) { const int t = bx; bx = by; by = t; }
-  int dx = wrap_mod(bx - ox - px, sz), dy = wrap_mod(by - oy - py, sz);
-  if (dx > sz / 2) dx -= sz;
-  if (dy > sz / 2) dy -= sz;
+  int dx = wrap_mod(bx - ox - px, kSz), dy = wrap_mod(by - oy - py, kSz);
+  if (dx > kSz / 2) dx -= kSz;
+  if (dy > kSz / 2) dy -= kSz;
   qx = px + dx;
   qy = py + dy;
+}
+
+// The texture index is the same for every pixel of a pass (it depends on
+// the tap and the flags only), so the branch is uniform.
+VRT_DI void paired_partner(const RestirDev& R, int px, int py, uint32_t ti, int& qx, int& qy) {
+  if (ti == 0u) paired_partner_sz<254, 0u>(R, px, py, ti, qx, qy);
+  else if (ti == 1u) paired_partner_sz<230, 64516u>(R, px, py, ti, qx, qy);
+  else paired_partner_sz<210, 117416u>(R, px, py, ti, qx, qy);
 }
 
 // footprintOK (restir.wgsl:172-180)
