@@ -48,10 +48,11 @@ def parse_args():
                     help="frame mode: skip the plain vs batched+cache comparison in the output line")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame", "lights",
-                                                              "restir", "voxelbench"],
+                                                        "restir", "restir-scenes", "voxelbench"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
                          "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
-                         "path tracing at matched MSE; restir: the ReSTIR gi preset beside the plain frame")
+                         "path tracing at matched MSE; restir: the ReSTIR presets beside the plain frame; "
+                         "restir-scenes: `ours` on the reference's own scenarios with its capture settings")
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
@@ -1168,6 +1169,96 @@ def restir_line(args, local):
     return line
 
 
+# The scenarios of the reference's published `ours` timings
+# (test/eval/claim-manifest.v1.json: poses in metres / radians; the moving runs
+# strafe along x by sin(0.07 frame) * 0.6 m, main.js:687-691; capture 1920x1080,
+# 6 bounces, denoiser off, firefly clamp 0, rgba32f history) on the reference's
+# world (scene.js generateScene(256, 'default' or 'lamps'), noise seed 1337).
+REF_SCENARIOS = {
+    "exterior": {"pos": (8.0, 4.9, 4.6), "yaw": 0.85, "pitch": -0.1, "world": 0, "published_ms": 22.56},
+    "lamps": {"pos": (6.6, 4.9, 6.9), "yaw": 0.55, "pitch": 0.0, "world": 4, "published_ms": 33.31},
+    "interior": {"pos": (8.8, 4.7, 7.0), "yaw": -0.45, "pitch": 0.02, "world": 0, "published_ms": 33.96},
+}
+REF_SCENARIO_FRAMES = 96
+REF_SCENARIO_MOVE = (0.6, 0.07)
+
+
+def run_restir_scenes(args, local):
+    print(json.dumps(restir_scenes_line(args, local)), flush=True)
+
+
+def restir_scenes_line(args, local):
+    """`--mode restir-scenes`: the reference's `ours` preset on its own default
+    world and the exterior / interior scenario poses, with the capture settings
+    of its published GPU timings (docs/STATUS.md:75-81: median GPU ms of the
+    96-frame moving runs, RTX 3080, Chromium WebGPU): 1920x1080, 6 bounces,
+    denoiser off, firefly clamp 0, rgba32f history, the reference's sun and
+    70-degree camera.  Frames 1..96 of the strafe are rendered; the first
+    `--warmup` are untimed; the median and mean of the rest are reported."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+
+    torch.cuda.set_device(local)
+    n, W, H = 256, 1920, 1080
+    ctx = vrt.Context(local)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    light = vrt.Lighting.reference_default()
+    amp, step = REF_SCENARIO_MOVE
+
+    def pose_at(sc, f):
+        x, y, z = sc["pos"]
+        return vrt.CameraPose((x + math.sin(f * step) * amp, y, z), sc["yaw"], sc["pitch"])
+
+    out, clk, lights = {}, None, {}
+    warm = max(args.warmup, 3)
+    for name, sc in REF_SCENARIOS.items():
+        vox, _ = vrt.generate_scene(sc["world"], n, 1337)
+        scene = vrt.Scene(ctx, vox, n)
+        nlights = int(scene.build_lights().count)
+        lights[name] = nlights
+        sess = vrt.Session(ctx, scene, W, H, firefly_clamp=0.0, accum_f32=True, path_kernel=args.path_kernel)
+        sess.set_timing(True)
+        fm, rays = [], 0
+        clocks = None
+        for f in range(REF_SCENARIO_FRAMES):
+            if f == warm:
+                ctx.synchronize()
+                clocks = ClockSampler(local)
+                clocks.start()
+            u = vrt.make_uniforms(pose_at(sc, f), pose_at(sc, f - 1) if f > 0 else None, light, f, 6, 1, W, H,
+                                  1.0, 64.0, preset="ours", light_count=nlights)
+            flush.zero_()
+            torch.cuda.synchronize()
+            sess.frame(u)
+            st = sess.stats()
+            if f >= warm:
+                fm.append(st.ms_total)
+                rays += st.rays
+        ctx.synchronize()
+        c = clocks.stop() if clocks else None
+        clk = c or clk
+        sess.close()
+        scene.close()
+        out[name] = {"frame_ms_p50": round(statistics.median(fm), 4), "frame_ms_mean": round(statistics.mean(fm), 4),
+                     "frame_ms_p99": round(float(np.percentile(fm, 99)), 4), "frames_timed": len(fm),
+                     "rays_per_frame": round(rays / len(fm)),
+                     "reference_published_ms": sc["published_ms"],
+                     "ratio_published_over_ours": round(sc["published_ms"] / statistics.median(fm), 2)}
+    ctx.close()
+    line = {"mode": "restir-scenes", "metric": "ReSTIR `ours` median frame ms on the reference's scenarios "
+            "(1920x1080, 6 bounces, denoiser off, fclamp 0)", "unit": "ms/frame", "higher_is_better": False,
+            "lights": lights, "world": "scene.js world ('default', or 'lamps' for the lamps scenario), 256^3, "
+                                        "noise seed 1337",
+            "scenarios": out,
+            "note": "the published numbers are an RTX 3080 in Chromium WebGPU (docs/STATUS.md:75-81); same scene, "
+                    "pose, resolution, bounces and preset, different hardware and runtime."}
+    if clk:
+        line["clocks"] = clk
+    return line
+
+
 VB_SCENES = ["bunker", "cavern", "courtyard", "town"]
 VB_PUBLISHED_PT_MS = {"bunker": 115.7, "cavern": 123.5, "courtyard": 36.4, "town": 34.6}
 
@@ -1242,6 +1333,9 @@ def main():
     elif args.mode == "restir":
         if rank == 0:
             run_restir(args, local)
+    elif args.mode == "restir-scenes":
+        if rank == 0:
+            run_restir_scenes(args, local)
     elif args.mode == "voxelbench":
         if rank == 0:
             run_voxelbench(args, local)

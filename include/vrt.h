@@ -164,7 +164,8 @@ enum {
   VRT_SCENE_VOXELRT = 0,      /* scene.js 'default' world (noise seed = seed)  */
   VRT_SCENE_SMALL = 1,        /* 64^3 terrain + 24^3 Cornell box              */
   VRT_SCENE_FULL = 2,         /* terrain, room, 40 trees, RGB lanterns        */
-  VRT_SCENE_RANDOM = 3        /* terrain + boxes, 0.1% emissive U(1,20)       */
+  VRT_SCENE_RANDOM = 3,       /* terrain + boxes, 0.1% emissive U(1,20)       */
+  VRT_SCENE_VOXELRT_LAMPS = 4 /* scene.js 'lamps' variant (scene.js:303-409)  */
 };
 
 /* ---- context ----------------------------------------------------------- */

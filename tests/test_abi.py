@@ -37,6 +37,39 @@ def test_no_device_is_reported_without_gpu(vrt):
     assert e.value.code == 4  # VRT_ERR_NO_DEVICE
 
 
+def test_scene_lamps_variant(vrt):
+    """scene.js generateScene(N, 'lamps') (scene.js:303-409): the default world
+    with the room's ceiling strip replaced by dim strips, coloured panels,
+    occluders and small bright lamps, dimmed exterior lanterns and no corner
+    lamp -- every other voxel as in the default world."""
+    n = 256
+    d, sd = vrt.generate_scene(vrt.VRT_SCENE_VOXELRT, n, 1337)
+    a, sa = vrt.generate_scene(vrt.VRT_SCENE_VOXELRT_LAMPS, n, 1337)
+    b, _ = vrt.generate_scene(vrt.VRT_SCENE_VOXELRT_LAMPS, n, 1337)
+    assert np.array_equal(a, b) and sa == sd
+    # differences only in the room (walls 2 voxels thick) and at the three lanterns
+    room_w = min(80, n * 45 // 100)
+    cx, cz = n // 2, int(n * 0.55)
+    x0, x1, z0, z1 = cx - room_w // 2, cx + room_w // 2, cz - room_w // 2, cz + room_w // 2
+    z, y, x = np.unravel_index(np.nonzero(a != d)[0], (n, n, n))
+    in_room = (x >= x0 - 2) & (x <= x1 + 2) & (z >= z0 - 2) & (z <= z1 + 2)
+    lanterns = [(int(n * 0.35), int(n * 0.25)), (int(n * 0.68), int(n * 0.30)), (int(n * 0.25), int(n * 0.65))]
+    at_lantern = np.zeros_like(in_room)
+    for lx, lz in lanterns:
+        at_lantern |= (np.abs(x - lx) <= 1) & (np.abs(z - lz) <= 1)
+    assert x.size > 0 and np.all(in_room | at_lantern)
+    # the variant's emitters: hot lamps (E 255), four panels, dim strips (E 45), dimmed lanterns (E 64)
+    emis = {int(v) for v in np.unique(a[(a >> 24) != 0])}
+    def m(r, g, bl, e):
+        return r | g << 8 | bl << 16 | e << 24
+    for want in (m(255, 214, 150, 255), m(255, 140, 40, 200), m(40, 220, 200, 165), m(190, 80, 255, 245),
+                 m(150, 255, 60, 125), m(140, 180, 255, 45), m(255, 190, 110, 64), m(90, 220, 255, 64),
+                 m(255, 90, 200, 64)):
+        assert want in emis, hex(want)
+    assert m(255, 240, 220, 210) not in emis          # no ceiling strip
+    assert m(255, 190, 110, 255) not in emis          # no full-power warm lantern or corner lamp
+
+
 def test_scene_generate_deterministic(vrt):
     for kind, n, seed in [(0, 64, 1337), (1, 64, 1), (2, 64, 2), (3, 64, 3)]:
         a, sa = vrt.generate_scene(kind, n, seed)

@@ -19,6 +19,7 @@ VRT_SCENE_VOXELRT = 0
 VRT_SCENE_SMALL = 1
 VRT_SCENE_FULL = 2
 VRT_SCENE_RANDOM = 3
+VRT_SCENE_VOXELRT_LAMPS = 4
 
 
 class VrtError(RuntimeError):

@@ -133,6 +133,13 @@ const uint32_t boxTall = M(200, 200, 210), boxShort = M(210, 170, 90), trunk = M
 uint32_t leaf(int v) { return M(50 + v, 120 + v, 45); }
 const uint32_t lampPost = M(60, 60, 65), lampWarm = M(255, 190, 110, 255), lampCyan = M(90, 220, 255, 255);
 const uint32_t lampMagenta = M(255, 90, 200, 255), ceilLight = M(255, 240, 220, 210);
+// the 'lamps' variant's emitters and occluders (scene.js:38-56)
+const uint32_t lampHot = M(255, 214, 150, 255);
+const uint32_t panelOrange = M(255, 140, 40, 200), panelTeal = M(40, 220, 200, 165);
+const uint32_t panelViolet = M(190, 80, 255, 245), panelLime = M(150, 255, 60, 125);
+const uint32_t dimStrip = M(140, 180, 255, 45), pillar = M(118, 116, 126), shelf = M(140, 105, 70);
+const uint32_t lampWarmDim = M(255, 190, 110, 64), lampCyanDim = M(90, 220, 255, 64);
+const uint32_t lampMagentaDim = M(255, 90, 200, 64);
 }  // namespace mat
 
 // Emissive byte for a radiance intensity I: Le = alb^2 (E/255) 24.
@@ -169,8 +176,54 @@ void terrain_voxelrt(World& w, const Noise& noise) {
     }
 }
 
-// scene.js:267-301 room + 363-366 ceiling strip + 368-374 boxes.
-Room room_voxelrt(World& w) {
+// The 'lamps' variant's interior lighting in place of the ceiling strip
+// (scene.js:303-360): dim cool strips, four coloured wall panels, two pillars
+// and a shelf as occluders, and small very bright lamps (ceiling pendants,
+// standing lamps, two wall lamps), all placed by room-coordinate arithmetic.
+void lamps_interior(Grid& g, const Room& r) {
+  const int cx = r.cx, cz = r.cz, x0 = r.x0, x1 = r.x1, z0 = r.z0, z1 = r.z1, floorY = r.floorY, y1 = r.y1;
+  const int roomW = r.roomW, roomH = r.roomH;
+  const int stripLen = ifl(roomW * 0.5);
+  const int sx0 = cx - (stripLen >> 1), sx1 = sx0 + stripLen - 1;
+  const int stripDz = ifl(roomW * 0.22);
+  for (const int dz : {-stripDz, 0, stripDz}) g.box(sx0, y1, cz + dz - 1, sx1, y1, cz + dz + 1, mat::dimStrip);
+  g.box(sx0, y1 - 4, z1, sx1, y1 - 3, z1, mat::dimStrip);
+  const int pW = 5, pH = 3;
+  const int pMidY = floorY + ifl(roomH * 0.35);
+  g.box(x0, pMidY, cz - 9, x0, pMidY + pH, cz - 9 + pW, mat::panelOrange);
+  const int tealY = floorY + ifl(roomH * 0.2);
+  g.box(x1, tealY, cz - 22, x1, tealY + pH, cz - 22 + pW, mat::panelTeal);
+  const int violetY = floorY + ifl(roomH * 0.5);
+  g.box(cx + 10, violetY, z1, cx + 10 + pW, violetY + pH, z1, mat::panelViolet);
+  const int limeY = floorY + ifl(roomH * 0.4);
+  g.box(x0 + 6, limeY, z0, x0 + 6 + pW, limeY + pH, z0, mat::panelLime);
+  const int pAx = cx - ifl(roomW * 0.12), pAz = cz + ifl(roomW * 0.15);
+  g.box(pAx - 1, floorY + 1, pAz - 1, pAx + 2, y1, pAz + 2, mat::pillar);
+  const int pBx = cx + ifl(roomW * 0.22), pBz = cz - ifl(roomW * 0.12);
+  g.box(pBx - 1, floorY + 1, pBz - 1, pBx + 2, floorY + ifl(roomH * 0.75), pBz + 2, mat::pillar);
+  const int shelfY = floorY + ifl(roomH * 0.3);
+  g.box(x1 - 10, shelfY, cz + 10, x1 - 1, shelfY + 1, cz + 26, mat::shelf);
+  auto pendant = [&](int lx, int lz) {
+    for (int y = y1 - 2; y <= y1; y++) g.set(lx, y, lz, mat::lampPost);
+    g.box(lx, y1 - 4, lz, lx, y1 - 3, lz, mat::lampHot);
+  };
+  pendant(cx + ifl(roomW * 0.19), cz - ifl(roomW * 0.16));
+  pendant(cx - ifl(roomW * 0.3), cz + ifl(roomW * 0.3));
+  auto standing = [&](int lx, int lz) {
+    g.set(lx, floorY + 1, lz, mat::lampPost);
+    g.box(lx, floorY + 2, lz, lx, floorY + 3, lz, mat::lampHot);
+  };
+  standing(x1 - 5, cz + 18);
+  standing(pAx - 4, z1 - 4);
+  standing(pBx + 4, pBz - 4);
+  standing(x0 + 3, z1 - 3);
+  g.box(cx - 24, y1 - 6, z0, cx - 24, y1 - 5, z0, mat::lampHot);
+  g.box(cx - 6, floorY + 8, z1, cx - 6, floorY + 9, z1, mat::lampHot);
+}
+
+// scene.js:267-301 room + 363-366 ceiling strip (or the 'lamps' interior,
+// 303-360) + 368-374 boxes.
+Room room_voxelrt(World& w, bool lamps = false) {
   const int N = w.g.N;
   Grid& g = w.g;
   Room r;
@@ -197,8 +250,12 @@ Room room_voxelrt(World& w) {
   g.box(cx - doorHalf, floorY + 1, z0 - T, cx + doorHalf, y1 - 2, z0 - 1, 0);
   const int winY0 = floorY + ifl(roomH * 0.45), winY1 = floorY + ifl(roomH * 0.8);
   g.box(x1 + 1, winY0, cz - ifl(roomW * 0.3), x1 + T, winY1, cz + ifl(roomW * 0.3), 0);
-  const int lHalf = ifl(roomW * 0.18);
-  g.box(cx - lHalf, y1, cz - lHalf, cx + lHalf, y1, cz + lHalf, mat::ceilLight);
+  if (lamps) {
+    lamps_interior(g, r);
+  } else {
+    const int lHalf = ifl(roomW * 0.18);
+    g.box(cx - lHalf, y1, cz - lHalf, cx + lHalf, y1, cz + lHalf, mat::ceilLight);
+  }
   const int tallW = ifl(roomW * 0.16), tallH = ifl(roomH * 0.55);
   g.box(cx - ifl(roomW * 0.28) - tallW, floorY + 1, cz + ifl(roomW * 0.05), cx - ifl(roomW * 0.28), floorY + tallH,
         cz + ifl(roomW * 0.05) + tallW, mat::boxTall);
@@ -234,18 +291,20 @@ void lantern(World& w, int lx, int lz, uint32_t m) {
   w.g.box(lx - 1, gr + h + 1, lz - 1, lx + 1, gr + h + 3, lz + 1, m);
 }
 
-void gen_voxelrt(Grid g, uint32_t seed, VrtCameraPose* spawn) {
+// scene.js generateScene(N, variant): 'default' or 'lamps' (dimmed exterior
+// lanterns, no corner lamp: scene.js:402-409).
+void gen_voxelrt(Grid g, uint32_t seed, VrtCameraPose* spawn, bool lamps = false) {
   World w{g, {}};
   const int N = g.N;
   Noise noise{(int64_t)seed};
   terrain_voxelrt(w, noise);
-  Room r = room_voxelrt(w);
+  Room r = room_voxelrt(w, lamps);
   const double spots[6][2] = {{0.15, 0.2}, {0.82, 0.25}, {0.2, 0.8}, {0.86, 0.78}, {0.12, 0.55}, {0.65, 0.12}};
   for (auto& s : spots) tree(w, ifl(N * s[0]), ifl(N * s[1]));
-  lantern(w, ifl(N * 0.35), ifl(N * 0.25), mat::lampWarm);
-  lantern(w, ifl(N * 0.68), ifl(N * 0.30), mat::lampCyan);
-  lantern(w, ifl(N * 0.25), ifl(N * 0.65), mat::lampMagenta);
-  w.g.box(r.x0 + 2, r.floorY + 1, r.z1 - 4, r.x0 + 4, r.floorY + 3, r.z1 - 2, mat::lampWarm);
+  lantern(w, ifl(N * 0.35), ifl(N * 0.25), lamps ? mat::lampWarmDim : mat::lampWarm);
+  lantern(w, ifl(N * 0.68), ifl(N * 0.30), lamps ? mat::lampCyanDim : mat::lampCyan);
+  lantern(w, ifl(N * 0.25), ifl(N * 0.65), lamps ? mat::lampMagentaDim : mat::lampMagenta);
+  if (!lamps) w.g.box(r.x0 + 2, r.floorY + 1, r.z1 - 4, r.x0 + 4, r.floorY + 3, r.z1 - 2, mat::lampWarm);
   if (spawn) {
     spawn->pos[0] = r.cx * kVS;
     spawn->pos[1] = (w.groundAt(r.cx, r.z0 - V(3)) + 1) * kVS + 1.65;
@@ -474,7 +533,7 @@ int vrt_camera_spline(const VrtCameraPose* spawn, int frame, VrtCameraPose* out)
 
 int vrt_scene_generate(int kind, int N, uint32_t seed, uint32_t* out_voxels, VrtCameraPose* spawn) {
   if (!out_voxels || N < 8 || N % 8 != 0 || N > 2048) return VRT_ERR_INVALID;
-  if (kind < VRT_SCENE_VOXELRT || kind > VRT_SCENE_RANDOM) return VRT_ERR_INVALID;
+  if (kind < VRT_SCENE_VOXELRT || kind > VRT_SCENE_VOXELRT_LAMPS) return VRT_ERR_INVALID;
   std::memset(out_voxels, 0, (size_t)N * N * N * sizeof(uint32_t));
   Grid g{N, out_voxels};
   switch (kind) {
@@ -482,6 +541,7 @@ int vrt_scene_generate(int kind, int N, uint32_t seed, uint32_t* out_voxels, Vrt
     case VRT_SCENE_SMALL: gen_small(g, seed, spawn); break;
     case VRT_SCENE_FULL: gen_full(g, seed, spawn); break;
     case VRT_SCENE_RANDOM: gen_random(g, seed, spawn); break;
+    case VRT_SCENE_VOXELRT_LAMPS: gen_voxelrt(g, seed, spawn, true); break;
     default: return VRT_ERR_INVALID;
   }
   return VRT_OK;
