@@ -349,6 +349,14 @@ def run_ours(args, world, rank, local):
         except Exception as e:   # the headline line must still print
             line["restir"] = {"error": str(e)[:300]}
         try:
+            rs = restir_scenes_line(a3, local)
+            line["restir_reference_scenarios"] = {
+                k: {"frame_ms_p50": v["frame_ms_p50"], "reference_published_ms": v["reference_published_ms"]}
+                for k, v in rs["scenarios"].items()}
+            line["restir_reference_scenarios"]["details"] = "bench.py --mode restir-scenes"
+        except Exception as e:
+            line["restir_reference_scenarios"] = {"error": str(e)[:300]}
+        try:
             v = voxelbench_line(a3, local, 10, 32)
             line["voxelbench"] = {sc: {"vrt_ms": x["vrt_ms"], "pt_ms": x["pt_ms"], "psnr_pt_vrt": x["psnr"]}
                                   for sc, x in v.get("scenes", {}).items()} or v
