@@ -981,10 +981,11 @@ __global__ void __launch_bounds__(256, 3) k_restir_spatial_select(const __grid_c
     b.R2[g] = make_float4(d.x, d.y, d.z, maxT);
     b.S1[g] = make_float4(contrib.x, contrib.y, contrib.z, __uint_as_float(2u));
   }
-  uint32_t rs, as;
-  block_append(b.ctr + 4 * wave, b.ctr + 4 * wave + 2, nr, nr > 0, rs, as);
+  uint32_t fs, bs, as;
+  int* c = b.ctr + 4 * wave;
+  block_append(c, c + 3, c + 2, nr, 0, nr > 0, fs, bs, as);
   uint32_t* q = queue_of(b, wave);
-  for (int k = 0; k < nr; k++) q[rs + (uint32_t)k] = (g + (uint32_t)k * P) | kShadowBit;
+  for (int k = 0; k < nr; k++) q[fs + (uint32_t)k] = (g + (uint32_t)k * P) | kShadowBit;
   if (nr > 0) active_of(b, wave)[as] = g;
 }
 

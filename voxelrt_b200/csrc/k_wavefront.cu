@@ -48,6 +48,7 @@ void carve_wavefront(void* mem, size_t P, int max_waves, WavefrontBufs& wb, int 
     m += (twice ? big : P) * 16;
   }
   for (int i = 0; i < 2; i++) { wb.q[i] = (uint32_t*)m; m += queue_entries(P, slots) * 4; }
+  wb.qcap = queue_entries(P, slots);
   for (int i = 0; i < 2; i++) { wb.act[i] = (uint32_t*)m; m += P * 4; }
   wb.ctr = (int*)m;
   wb.max_waves = max_waves;

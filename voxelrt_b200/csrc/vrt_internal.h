@@ -45,6 +45,7 @@ struct WavefrontBufs {
   uint32_t* q[2] = {nullptr, nullptr};                // 2P entries each (4P with several slots)
   uint32_t* act[2] = {nullptr, nullptr};              // P entries each
   int* ctr = nullptr;                                 // 4 ints per wave
+  size_t qcap = 0;                                    // entries per queue
   int max_waves = 0;
   int slots = 1;                                      // shadow-ray slots per path: ray k of path g is
                                                       // traced as path g + k P

@@ -29,8 +29,15 @@ struct WfDev {
   uint32_t* q1;
   uint32_t* a0;    // active path lists, capacity P
   uint32_t* a1;
-  int* ctr;        // per wave k: [4k] queue count, [4k+1] queue head, [4k+2] active count
+  int* ctr;        // per wave k: [4k] shadow rays (queue front), [4k+1] queue head, [4k+2] active count,
+                   // [4k+3] bounce rays (queue back)
+  uint32_t qcap;   // queue capacity in entries: bounce ray i of a wave sits at qcap - 1 - i
 };
+
+// Ray queues: a wave's shadow rays are appended from the front, its bounce
+// rays from the back (bounce ray i at qcap - 1 - i), so a tracer warp takes
+// runs of one kind -- shadow rays of neighbouring paths share the sun
+// direction and much of their walks.
 
 VRT_DI uint32_t* queue_of(const WfDev& b, int wave) { return (wave & 1) ? b.q1 : b.q0; }
 VRT_DI uint32_t* active_of(const WfDev& b, int wave) { return (wave & 1) ? b.a1 : b.a0; }
@@ -533,29 +540,31 @@ VRT_DI bool shade_vertex(const Uni& u, const WfDev& b, uint32_t g, uint32_t k, F
   return want_shadow || want_bounce;
 }
 
-// Block-aggregated appends: each thread of a block of 256 adds nr entries to
-// the ray queue counted by c_rays and, if act, one to the list counted by
-// c_act; one atomicAdd per counter per block, since every block of the grid
-// appends to the same counters.  Returns the thread's first ray slot (its nr
-// slots are consecutive) and its list slot.  All threads of the block call it
-// (block-uniform control flow).  Entries of a block are in thread order; a
-// path's results do not depend on the order of the queues.
-VRT_DI void block_append(int* c_rays, int* c_act, int nr, bool act, uint32_t& rslot, uint32_t& aslot) {
-  __shared__ int s_cnt[2][8];
-  __shared__ int s_base[2];
+// Block-aggregated appends: each thread of a block of 256 adds nf entries to
+// the list counted by c_front, nb to the list counted by c_back and, if act,
+// one to the list counted by c_act; one atomicAdd per counter per block, since
+// every block of the grid appends to the same counters.  Returns the thread's
+// first slot in each (its nf / nb slots are consecutive).  All threads of the
+// block call it (block-uniform control flow).  Entries of a block are in
+// thread order; a path's results do not depend on the order of the queues.
+VRT_DI void block_append(int* c_front, int* c_back, int* c_act, int nf, int nb, bool act, uint32_t& fslot,
+                         uint32_t& bslot, uint32_t& aslot) {
+  __shared__ int s_cnt[3][8];
+  __shared__ int s_base[3];
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int incl = nr;
+  int incf = nf, incb = nb;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
+    const int vf = __shfl_up_sync(full, incf, o);
+    const int vb = __shfl_up_sync(full, incb, o);
+    if (lane >= o) { incf += vf; incb += vb; }
   }
   const unsigned ma = __ballot_sync(full, act);
-  if (lane == 31) s_cnt[0][w] = incl;
-  if (lane == 0) s_cnt[1][w] = __popc(ma);
+  if (lane == 31) { s_cnt[0][w] = incf; s_cnt[1][w] = incb; }
+  if (lane == 0) s_cnt[2][w] = __popc(ma);
   __syncthreads();
-  if (threadIdx.x < 2) {   // thread 0: rays, thread 1: list
+  if (threadIdx.x < 3) {   // thread 0: front, 1: back, 2: list
     int tot = 0;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -563,34 +572,38 @@ VRT_DI void block_append(int* c_rays, int* c_act, int nr, bool act, uint32_t& rs
       s_cnt[threadIdx.x][k] = tot;
       tot += v;
     }
-    s_base[threadIdx.x] = tot ? atomicAdd(threadIdx.x == 0 ? c_rays : c_act, tot) : 0;
+    int* c = threadIdx.x == 0 ? c_front : (threadIdx.x == 1 ? c_back : c_act);
+    s_base[threadIdx.x] = tot ? atomicAdd(c, tot) : 0;
   }
   __syncthreads();
-  rslot = (uint32_t)(s_base[0] + s_cnt[0][w] + incl - nr);
-  aslot = (uint32_t)(s_base[1] + s_cnt[1][w]) + (uint32_t)__popc(ma & ((1u << lane) - 1u));
+  fslot = (uint32_t)(s_base[0] + s_cnt[0][w] + incf - nf);
+  bslot = (uint32_t)(s_base[1] + s_cnt[1][w] + incb - nb);
+  aslot = (uint32_t)(s_base[2] + s_cnt[2][w]) + (uint32_t)__popc(ma & ((1u << lane) - 1u));
   __syncthreads();   // s_cnt / s_base are rewritten by the block's next call
 }
 
 // Appends the new rays (shadow ray of path g, its bounce ray) and the active
 // path of wave `next`.  Block-uniform, see block_append.
 VRT_DI void emit_block(const WfDev& b, int next, uint32_t g, bool shadow, bool bounce, bool keep) {
-  uint32_t rs, as;
-  block_append(b.ctr + 4 * next, b.ctr + 4 * next + 2, (int)shadow + (int)bounce, keep, rs, as);
+  uint32_t fs, bs, as;
+  int* c = b.ctr + 4 * next;
+  block_append(c, c + 3, c + 2, (int)shadow, (int)bounce, keep, fs, bs, as);
   uint32_t* q = queue_of(b, next);
-  if (shadow) q[rs++] = g | kShadowBit;
-  if (bounce) q[rs] = g;
+  if (shadow) q[fs] = g | kShadowBit;
+  if (bounce) q[b.qcap - 1u - bs] = g;
   if (keep) active_of(b, next)[as] = g;
 }
 
 // emit_block() with a second shadow ray of the path, traced as path g + P.
 VRT_DI void emit2_block(const WfDev& b, int next, uint32_t g, uint32_t P, bool shadow, bool shadow2, bool bounce,
                         bool keep) {
-  uint32_t rs, as;
-  block_append(b.ctr + 4 * next, b.ctr + 4 * next + 2, (int)shadow2 + (int)shadow + (int)bounce, keep, rs, as);
+  uint32_t fs, bs, as;
+  int* c = b.ctr + 4 * next;
+  block_append(c, c + 3, c + 2, (int)shadow2 + (int)shadow, (int)bounce, keep, fs, bs, as);
   uint32_t* q = queue_of(b, next);
-  if (shadow2) q[rs++] = (g + P) | kShadowBit;
-  if (shadow) q[rs++] = g | kShadowBit;
-  if (bounce) q[rs] = g;
+  if (shadow2) q[fs++] = (g + P) | kShadowBit;
+  if (shadow) q[fs] = g | kShadowBit;
+  if (bounce) q[b.qcap - 1u - bs] = g;
   if (keep) active_of(b, next)[as] = g;
 }
 
@@ -635,7 +648,8 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
   }
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int n = implicit_n > 0 ? implicit_n : b.ctr[4 * wave];
+  const int nf = implicit_n > 0 ? 0 : b.ctr[4 * wave];   // shadow rays at the queue's front
+  const int n = implicit_n > 0 ? implicit_n : nf + b.ctr[4 * wave + 3];
   int* head = b.ctr + 4 * wave + 1;
   const uint32_t* queue = queue_of(b, wave);
   DCount c{0u, 0u, 0u, 0u};
@@ -655,7 +669,8 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       if (!active) {
         const int slot = base + __popc(idle & ((1u << lane) - 1u));
         if (slot < n) {
-          entry = implicit_n > 0 ? (uint32_t)slot : queue[slot];
+          entry = implicit_n > 0 ? (uint32_t)slot
+                                 : (slot < nf ? queue[slot] : queue[b.qcap - 1u - (uint32_t)(slot - nf)]);
           const uint32_t g = entry & ~kShadowBit;
           S = jobs.scene(jobs.job_of(g));
           const F3 ro = xyz(b.R0[g]);
@@ -896,6 +911,7 @@ inline WfDev wf_view(const WavefrontBufs& w) {
   d.hit = (uint4*)w.hit;
   d.q0 = w.q[0]; d.q1 = w.q[1]; d.a0 = w.act[0]; d.a1 = w.act[1];
   d.ctr = w.ctr;
+  d.qcap = (uint32_t)w.qcap;
   return d;
 }
 
