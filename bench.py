@@ -337,7 +337,7 @@ def run_ours(args, world, rank, local):
         a2.steps = min(args.steps, 10)
         line["plain_vs_batched_cache"] = cache_summary(cache_comparison(a2, local))
     if rank == 0 and world == 1 and not args.no_extras:
-        # the survey's "next" rows measured on the same box: ReSTIR presets and the VoxelBench adapter
+        # measured on the same box: the ReSTIR presets, `ours` on the reference's scenarios, the VoxelBench adapter
         import copy
         a3 = copy.copy(args)
         a3.steps, a3.warmup, a3.no_cpu_baseline, a3.runs = 10, 3, True, "gi,ours_b6_nodenoise"

@@ -111,7 +111,9 @@ def camera_matrices(pose: CameraPose, aspect: float):
 
 
 # ReSTIR flag bits of params2.x (common.wgsl:40-59) and the presets built from
-# them (main.js:34-62).  This build implements `base` and `gi`.
+# them (main.js:34-62).  The library implements every flag of these presets,
+# plus footprint, mixed sigma, adaptive candidate counts and the light grid;
+# frames with confdenoise, mutate or worldgi set are rejected.
 RF = {"restir": 1, "treuse": 2, "sreuse": 4, "paired": 8, "dupmap": 16, "footprint": 32, "vector": 64,
       "unified": 128, "plane": 256, "rescue": 512, "fullv": 1024, "rclamp": 2048, "lightpower": 4096,
       "mixsigma": 8192, "adaptcand": 16384, "confdenoise": 32768, "lightgrid": 65536, "mutate": 131072,

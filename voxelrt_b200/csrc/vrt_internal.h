@@ -245,7 +245,7 @@ constexpr uint32_t kRfRestir = 1u, kRfTemporal = 2u, kRfSpatial = 4u, kRfPaired 
                    kRfFullV = 1024u, kRfClamp = 2048u, kRfLightPower = 4096u, kRfMixSigma = 8192u,
                    kRfAdaptCand = 16384u, kRfConfDenoise = 32768u, kRfLightGrid = 65536u, kRfMutate = 131072u,
                    kRfHistIsolate = 262144u, kRfWorldGi = 524288u;
-// The flags this build implements: every flag of the `gi`, `lin`, `ours` and
+// The flags the library implements: every flag of the `gi`, `lin`, `ours` and
 // `ours_motion` presets (main.js:40-62) plus footprint, mixed sigma, adaptive
 // candidate counts and the light grid.
 constexpr uint32_t kRestirFlagsImplemented =
