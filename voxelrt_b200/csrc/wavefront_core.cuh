@@ -741,6 +741,7 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade_primary(J jobs, uint32_t P,
       const uint32_t lp = g - jobs.first(j);
       const uint4 h = b.hit[g];
       const F3 rd = xyz(b.R1[g]);
+      const float s0w = b.S0[g].w;   // RNG state, loaded with the hit rather than after the sky test
       const float t = __uint_as_float(h.x);
       if (t < 0.0f) {
         const F3 sky = sky_color(u, rd, true);
@@ -756,7 +757,7 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade_primary(J jobs, uint32_t P,
         out.alb8[lp] = unorm8_(__fsqrt_rn(mat1.albedo.x)) | (unorm8_(__fsqrt_rn(mat1.albedo.y)) << 8) |
                        (unorm8_(__fsqrt_rn(mat1.albedo.z)) << 16) | (255u << 24);
         out.gbuf[lp] = make_float4(n1.x, n1.y, n1.z, t);
-        uint32_t rng = __float_as_uint(b.S0[g].w);
+        uint32_t rng = __float_as_uint(s0w);
         F3 radiance = f3(0.0f, 0.0f, 0.0f), tp = f3(1.0f, 1.0f, 1.0f);
         const int W = jobs.width(j);
         const CacheDev& cc = jobs.cache(j);
@@ -803,6 +804,10 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
       const float4 s1 = b.S1[g];
       const float4 s2 = b.S2[g];
       const uint4 h = b.hit[g];
+      // loaded with the state above rather than after the terminal check, so a
+      // path's reads are one round trip instead of two
+      const float4 r1 = b.R1[g];
+      const float4 r0 = b.R0[g];
       F3 radiance = xyz(s0);
       F3 tp = xyz(s1);
       uint32_t rng = __float_as_uint(s0.w);
@@ -812,8 +817,8 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
       bool done = (flags & kFlagTerminal) != 0u;
       if (!done) {
         const Uni& u = jobs.uni(j);
-        const F3 rd = xyz(b.R1[g]);
-        const F3 surf = xyz(b.R0[g]);
+        const F3 rd = xyz(r1);
+        const F3 surf = xyz(r0);
         const float t = __uint_as_float(h.x);
         if (t < 0.0f) {
           radiance = radiance + tp * sky_color(u, rd, false);
