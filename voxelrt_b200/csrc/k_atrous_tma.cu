@@ -1,7 +1,8 @@
 // k_atrous_tma.cu -- the a-trous iteration (atrous.wgsl:26-83) with its
 // input tile staged in shared memory by TMA (cp.async.bulk.tensor).
 //
-// A CTA of 256 threads produces a 32 x 16 tile of output pixels.  One thread
+// A CTA of 256 threads produces a 32 x 16 tile of output pixels (32 x 8 at
+// step 4, whose halo is widest).  One thread
 // issues two tiled bulk copies -- the G-buffer (rgba32f) and the source image
 // (rgba16f or rgba32f) of the tile plus a halo of 2 * step pixels on each
 // side -- completing on one mbarrier; pixels outside the image arrive as zeros
@@ -28,15 +29,19 @@
 
 namespace vrt {
 
-constexpr int kTX = 32, kTY = 16;            // output tile
+constexpr int kTX = 32;                      // output tile width; height kTY: 16, or 8 at step 4
 constexpr uint32_t kTmaSpin = 1u << 22;      // bounded wait for the copies (try_wait iterations)
 
 __host__ __device__ constexpr int align128(int x) { return (x + 127) & ~127; }
-__host__ __device__ constexpr int tile_px(int step) { return (kTX + 4 * step) * (kTY + 4 * step); }
+__host__ __device__ constexpr int tile_px(int step, int ty) { return (kTX + 4 * step) * (ty + 4 * step); }
+__host__ __device__ constexpr int tile_rows(int step) { return step >= 4 ? 8 : 16; }
 // G-buffer tile + source tile (rgba16f or rgba32f as copied, expanded in place
 // to fp32 with its luminance); the steps are 1, 2, 4.
-__host__ __device__ constexpr int tile_smem(int step) { return align128(tile_px(step) * 16) + tile_px(step) * 16; }
-constexpr int kMaxTilePx = tile_px(4);
+__host__ __device__ constexpr int tile_smem(int step) {
+  return align128(tile_px(step, tile_rows(step)) * 16) + tile_px(step, tile_rows(step)) * 16;
+}
+constexpr int kMaxTilePx = 1280;   // staged pixels of the largest tile (step 4, 8 rows: 1,152), rounded to 256
+static_assert(tile_px(1, 16) <= kMaxTilePx && tile_px(2, 16) <= kMaxTilePx && tile_px(4, 8) <= kMaxTilePx, "tile");
 static_assert(kMaxTilePx % 256 == 0, "staged pixels per thread");
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
@@ -61,7 +66,9 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, in
       : "memory");
 }
 
-template <bool kSrcF32>
+// kTY: output rows per CTA (16, or 8 at step 4, where the halo is widest: 49 KB of
+// shared memory per CTA at 16 rows, 37 KB at 8).
+template <bool kSrcF32, int kTY>
 __global__ void __launch_bounds__(256) k_atrous_tma(const __grid_constant__ CUtensorMap tm_src,
                                                     const __grid_constant__ CUtensorMap tm_g, int W, int H,
                                                     const void* __restrict__ src, uint2* __restrict__ dst, int step,
@@ -118,7 +125,7 @@ __global__ void __launch_bounds__(256) k_atrous_tma(const __grid_constant__ CUte
   }
   __syncthreads();
 #pragma unroll
-  for (int half = 0; half < 2; half++) {
+  for (int half = 0; half < kTY / 8; half++) {
     const int lx = t & 31, ly = (t >> 5) + 8 * half;
     const int px = x0 + lx, py = y0 + ly;
     if (px >= W || py >= H) continue;
@@ -178,23 +185,24 @@ cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, co
   const bool aligned = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(gbuf)) & 15u) == 0u;
   const bool ok = encode_fn() && aligned && (src_f32 || W % 2 == 0) && step >= 1 && step <= 4 && W > 0 && H > 0;
   if (!ok) return launch_atrous(W, H, src, src_f32, gbuf, dst, step, st);
-  const int hx = 2 * step, bw = kTX + 2 * hx, bh = kTY + 2 * hx;
+  const int ty = tile_rows(step);
+  const int hx = 2 * step, bw = kTX + 2 * hx, bh = ty + 2 * hx;
   CUtensorMap tg, ts;
   const bool enc = map_f32x4(&tg, gbuf, W, H, bw, bh) &&
                    (src_f32 ? map_f32x4(&ts, src, W, H, bw, bh) : map_h4(&ts, src, W, H, bw, bh));
   if (!enc) return launch_atrous(W, H, src, src_f32, gbuf, dst, step, st);
   const int smem = tile_smem(step);
-  dim3 grid((W + kTX - 1) / kTX, (H + kTY - 1) / kTY);
+  dim3 grid((W + kTX - 1) / kTX, (H + ty - 1) / ty);
+  auto run = [&](auto* fn) -> cudaError_t {
+    cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (r != cudaSuccess) return r;
+    fn<<<grid, 256, smem, st>>>(ts, tg, W, H, src, (uint2*)dst, step, err);
+    return cudaGetLastError();
+  };
   cudaError_t e;
-  if (src_f32) {
-    e = cudaFuncSetAttribute(k_atrous_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4));
-    if (e != cudaSuccess) return e;
-    k_atrous_tma<true><<<grid, 256, smem, st>>>(ts, tg, W, H, src, (uint2*)dst, step, err);
-  } else {
-    e = cudaFuncSetAttribute(k_atrous_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile_smem(4));
-    if (e != cudaSuccess) return e;
-    k_atrous_tma<false><<<grid, 256, smem, st>>>(ts, tg, W, H, src, (uint2*)dst, step, err);
-  }
+  if (src_f32) e = ty == 8 ? run(k_atrous_tma<true, 8>) : run(k_atrous_tma<true, 16>);
+  else e = ty == 8 ? run(k_atrous_tma<false, 8>) : run(k_atrous_tma<false, 16>);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
