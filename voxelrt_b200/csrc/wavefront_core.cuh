@@ -17,7 +17,7 @@ constexpr uint32_t kShadowBit = 0x80000000u;
 constexpr uint32_t kFlagShadow2 = 4u;           // a second shadow ray of the previous vertex is pending
 
 struct WfDev {
-  float4* R0;      // ray origin: camera position (primary) or surf = pos + n*1e-3
+  float4* R0;      // ray origin of waves 1..: surf = pos + n*1e-3 (primary rays start at the camera)
   float4* R1;      // primary / bounce direction
   float4* R2;      // direction (xyz) and maxT (w) of the pending shadow ray
   float4* S0;      // radiance xyz, w = RNG state bits
@@ -626,7 +626,6 @@ __global__ void __launch_bounds__(256) k_wf_generate(J jobs, uint32_t P, WfDev b
   const float uvx = (((float)gx + 0.5f) + jx) / (float)W;
   const float uvy = (((float)gy + 0.5f) + jy) / (float)H;
   const F3 rd = camera_ray(u, uvx, uvy);
-  b.R0[g] = make_float4(u.camPos[0], u.camPos[1], u.camPos[2], 0.0f);
   b.R1[g] = make_float4(rd.x, rd.y, rd.z, 0.0f);
   b.S0[g] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
 }
@@ -673,7 +672,11 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
                                  : (slot < nf ? queue[slot] : queue[b.qcap - 1u - (uint32_t)(slot - nf)]);
           const uint32_t g = entry & ~kShadowBit;
           S = jobs.scene(jobs.job_of(g));
-          const F3 ro = xyz(b.R0[g]);
+          // primary rays start at the camera: its position comes from the job's
+          // uniforms (k_wf_generate writes no R0); later waves read the origin
+          // their shading stored
+          const Uni& uj = jobs.uni(jobs.job_of(g));
+          const F3 ro = implicit_n > 0 ? f3(uj.camPos[0], uj.camPos[1], uj.camPos[2]) : xyz(b.R0[g]);
           if (kVarMaxT) {
             float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w
             if (entry & kShadowBit) {
