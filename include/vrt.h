@@ -489,11 +489,13 @@ int vrt_selftest_bounded_wait(unsigned int spins);
  * its own allocator/budget, or a frame loop that must not call cudaMalloc,
  * which synchronizes the device).  d_accum: history, rgba16f (accum_f32 = 0)
  * or rgba32f (1); d_gbuf: rgba32f normal + distance; d_out: rgba16f result.
- * At most 1920x1080 pixels (VRT_ERR_INVALID above that).  The intermediate
+ * At most 1920x1080 pixels, and d_out may not overlap d_accum or d_gbuf
+ * (VRT_ERR_INVALID otherwise, before anything is queued).  The intermediate
  * image lives in a fixed 16,588,800-byte device array of the library, held on
- * every GPU that loads it; the first call on a device looks up that array's
- * address (make the first call before any stream capture).  Calls share the
- * array: calls that overlap on the GPU race and must be ordered by the
+ * every GPU that loads it; each call looks up that array's address on the
+ * current device, and the first call on a device also loads the library's
+ * kernels there (make the first call before any stream capture).  Calls share
+ * the array: calls that overlap on the GPU race and must be ordered by the
  * caller.  Work is queued on `stream` (a cudaStream_t, NULL = legacy default);
  * nothing is allocated or freed. */
 int vrt_denoise_atrous_noalloc(const void* d_accum, int accum_f32, const float* d_gbuf, void* d_out, int width,

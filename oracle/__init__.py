@@ -7,6 +7,7 @@ this package; the product (voxelrt_b200) never does.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -15,7 +16,10 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libvbref.so"
-REF_SRC = Path("/root/reference/VoxelBench/pipeline")
+# The reference checkout, when it is available (it is only needed to build
+# the reference traversal library and the golden fixtures).
+REF_ROOT = Path(os.environ["VRT_REFERENCE_ROOT"]) if os.environ.get("VRT_REFERENCE_ROOT") else None
+REF_SRC = REF_ROOT / "VoxelBench" / "pipeline" if REF_ROOT else None
 
 HIT_DTYPE = np.dtype([("t", "<f4"), ("n", "<f4", 3), ("mat", "<u4"), ("voxel", "<i4", 3), ("face", "<i4"),
                       ("steps", "<u4"), ("bytes", "<u4"), ("pad", "<u4")])
@@ -34,7 +38,9 @@ def build(ref: bool | None = None) -> None:
     traversal library and the VoxelBench harness driver vb_vrt, which links
     voxelrt_b200/libvrt.so)."""
     targets = ["all"]
-    if ref or (ref is None and REF_SRC.exists()):
+    if ref and REF_SRC is None:
+        raise RuntimeError("oracle.build(ref=True): set VRT_REFERENCE_ROOT to the reference checkout")
+    if ref or (ref is None and REF_SRC is not None and REF_SRC.exists()):
         targets += ["ref", "vbvrt"]
     subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
 

@@ -155,3 +155,21 @@ def test_invalid_arguments(vrt):
     assert vrt.lib.vrt_scene_generate(9, 8, 0, C.c_void_p(vox.ctypes.data), None) == 1
     assert vrt.lib.vrt_trace_rays(None, None, None, None, 1, None) == 1
     assert "bad argument" in vrt.lib.vrt_last_error_string().decode()
+
+
+def test_noalloc_denoise_rejects_overlapping_output(vrt):
+    """vrt_denoise_atrous_noalloc checks its buffers before it touches a
+    device: an output that overlaps the history or the G-buffer (an in-place
+    denoise, whose first iteration would read neighbours other threads are
+    overwriting) is rejected with VRT_ERR_INVALID.  The pointers here are
+    never dereferenced."""
+    lib = vrt.lib
+    W, H = 64, 32
+    px = W * H
+    base = 1 << 20
+    acc, gb = base, base + px * 16 * 4
+    for acc_f32, out in [(0, acc), (0, acc + px * 8 - 8), (1, acc + px * 16 - 8), (0, gb), (0, gb + px * 16 - 8),
+                         (0, acc - px * 8 + 8)]:
+        code = lib.vrt_denoise_atrous_noalloc(C.c_void_p(acc), acc_f32, C.c_void_p(gb), C.c_void_p(out), W, H, None)
+        assert code == 1, (acc_f32, out - base)
+        assert "overlaps" in lib.vrt_last_error_string().decode()

@@ -673,10 +673,15 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
           const uint32_t g = entry & ~kShadowBit;
           S = jobs.scene(jobs.job_of(g));
           // primary rays start at the camera: its position comes from the job's
-          // uniforms (k_wf_generate writes no R0); later waves read the origin
-          // their shading stored
-          const Uni& uj = jobs.uni(jobs.job_of(g));
-          const F3 ro = implicit_n > 0 ? f3(uj.camPos[0], uj.camPos[1], uj.camPos[2]) : xyz(b.R0[g]);
+          // uniforms (k_wf_generate writes no R0, so no wave-0 shading kernel
+          // may read R0 either); later waves read the origin their shading stored
+          F3 ro;
+          if (implicit_n > 0) {
+            const Uni& uj = jobs.uni(jobs.job_of(g));
+            ro = f3(uj.camPos[0], uj.camPos[1], uj.camPos[2]);
+          } else {
+            ro = xyz(b.R0[g]);
+          }
           if (kVarMaxT) {
             float maxT = 1e4f;   // bounce rays; shadow rays carry theirs in R2.w
             if (entry & kShadowBit) {
