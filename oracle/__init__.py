@@ -6,6 +6,7 @@ this package; the product (voxelrt_b200) never does.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -15,6 +16,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
+LITERAL_LIB = HERE / "liboracle_literal.so"
 REF_LIB = HERE / "_ref" / "libvbref.so"
 # The reference checkout, when it is available (it is only needed to build
 # the reference traversal library and the golden fixtures).
@@ -56,6 +58,66 @@ def lib() -> C.CDLL:
             build(ref=False)
         _lib = C.CDLL(str(LIB))
     return _lib
+
+
+_literal = None
+
+
+@contextlib.contextmanager
+def literal_wgsl():
+    """Within the block, the oracle's functions run the literal restatement of
+    the shaders (liboracle_literal.so): C-library transcendentals, dot
+    products and a-trous weights as written, none of the kernels'
+    reformulations.  Kernels agree with it within the specification's
+    tolerances, not bit for bit."""
+    global _lib, _literal
+    if _literal is None:
+        if not LITERAL_LIB.exists():
+            build(ref=False)
+        _literal = C.CDLL(str(LITERAL_LIB))
+    saved = lib()
+    _lib = _literal
+    try:
+        yield
+    finally:
+        _lib = saved
+
+
+def _host_isa_level() -> int:
+    """The x86-64 micro-architecture level of this host (1..4) from
+    /proc/cpuinfo's flags."""
+    try:
+        flags = set()
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+    except OSError:
+        return 1
+    v3 = {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "movbe", "xsave", "abm"}
+    v4 = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}
+    if not v3 <= flags:
+        return 1
+    return 4 if v4 <= flags else 3
+
+
+def ref_lib_best():
+    """The reference traversal built for the highest ISA level this host
+    supports (VoxelBench's own build uses -march=native), with a label of
+    the build; (None, None) when it was not built."""
+    global _ref
+    level = _host_isa_level()
+    for lv, name, label in [(4, "libvbref_v4.so", "-O2 -march=x86-64-v4 -fopenmp"),
+                            (3, "libvbref_v3.so", "-O2 -march=x86-64-v3 -fopenmp"),
+                            (1, "libvbref.so", "-O2 -fopenmp")]:
+        path = HERE / "_ref" / name
+        if lv <= level and path.exists():
+            if _ref is None:
+                _ref = C.CDLL(str(path))
+                _ref.vb_time_trace.restype = C.c_double
+                _ref.vb_copy_grid.restype = C.c_long
+            return _ref, label + " (the host's ISA level)"
+    return None, None
 
 
 def ref_lib() -> C.CDLL | None:
@@ -120,6 +182,24 @@ def pathtrace(vox, bricks, masks, n, ubytes: bytes, fclamp: float, w: int, h: in
                         C.byref(st))
     return {"rad16": rad16, "rad32": rad32, "alb8": alb8, "gbuf": gbuf,
             "stats": {k: int(getattr(st, k)) for k, _ in OrcStats._fields_}}
+
+
+def path_signatures(vox, bricks, masks, n, ubytes: bytes, fclamp: float, w: int, h: int, row0=0, row1=None,
+                    row_step=1):
+    """pathtrace() plus sig: per pixel a hash of its discrete path (every trace
+    in order with its outcome: miss, or hit voxel and face)."""
+    row1 = h if row1 is None else row1
+    ub = np.frombuffer(ubytes, np.uint8).copy()
+    rad16 = np.zeros((h, w, 4), np.uint16)
+    rad32 = np.zeros((h, w, 4), np.float32)
+    alb8 = np.zeros((h, w, 4), np.uint8)
+    gbuf = np.zeros((h, w, 4), np.float32)
+    sig = np.zeros((h, w), np.uint32)
+    st = OrcStats()
+    lib().orc_pathtrace_sig(_p(vox), _p(bricks), _p(masks), C.c_int(n), _p(ub), C.c_float(fclamp), C.c_int(w),
+                            C.c_int(h), C.c_int(row0), C.c_int(row1), C.c_int(row_step), _p(rad16), _p(rad32),
+                            _p(alb8), _p(gbuf), C.byref(st), _p(sig))
+    return {"rad16": rad16, "rad32": rad32, "alb8": alb8, "gbuf": gbuf, "sig": sig, "rays": int(st.rays)}
 
 
 def temporal(ubytes, w, h, rad16, gcur, acc_prev, gprev, acc_f32: bool):
@@ -372,3 +452,75 @@ def frame(vox, bricks, masks, n, ubytes, fclamp, w, h, acc_prev, gprev, acc_f32=
     res["ldr"] = present(ubytes, w, h, fin, fin_f32, pt["alb8"])
     res["hdr"] = hdr(w, h, fin, fin_f32, pt["alb8"])
     return res
+
+
+# ---------------------------------------------------------------------------
+# Inputs of the plain-frame workload without the product library: the world
+# (restated from scene.js), the benchmark camera path and the uniform block
+# (main.js:399-426), so the CPU reference arm runs in a process that loads
+# only oracle libraries.
+# ---------------------------------------------------------------------------
+def generate_scene(kind: int, n: int, seed: int):
+    """kind 0: scene.js's world with noise seed `seed`; kind 2: the benchmark
+    world.  Returns (voxels u32[n^3], spawn dict: pos, yaw, pitch, fov_y,
+    near_z, far_z)."""
+    vox = np.zeros(n * n * n, np.uint32)
+    sp = np.zeros(8, np.float64)
+    r = lib().orc_scene_generate(C.c_int(kind), C.c_int(n), C.c_uint32(seed), _p(vox), _p(sp))
+    if r != 0:
+        raise ValueError(f"orc_scene_generate: unsupported kind {kind} / size {n}")
+    return vox, {"pos": (sp[0], sp[1], sp[2]), "yaw": sp[3], "pitch": sp[4], "fov_y": sp[5], "near_z": sp[6],
+                 "far_z": sp[7]}
+
+
+def camera_spline(spawn: dict, frame: int) -> dict:
+    """The benchmark camera path: yaw advances 0.5 degree per frame and the
+    camera moves 0.05 m per frame along its horizontal heading."""
+    import math
+    x, y, z = spawn["pos"]
+    dyaw = 0.5 * math.pi / 180.0
+    for f in range(frame):
+        yaw = spawn["yaw"] + f * dyaw
+        x += 0.05 * math.sin(yaw)
+        z += 0.05 * math.cos(yaw)
+    out = dict(spawn)
+    out["pos"] = (x, y, z)
+    out["yaw"] = spawn["yaw"] + frame * dyaw
+    return out
+
+
+def uniforms(pose: dict, prev: dict | None, frame: int, bounces: int, flags: int, w: int, h: int,
+             exposure: float = 1.0, max_history: float = 64.0, sun_dir=(0.3, 0.8, 0.5),
+             sun_cos_radius: float | None = None, sun_irradiance=(3.0, 3.0, 3.0), sky: float = 1.0) -> bytes:
+    """The 304-byte uniform block of main.js writeUniforms (399-426) for the
+    plain path (params2.x = 0, the reference's ReSTIR tuning defaults in the
+    other slots)."""
+    import math
+    aspect = w / h
+
+    def mats(p):
+        return camera_matrices(p["pos"], p["yaw"], p["pitch"], p["fov_y"], aspect, p["near_z"], p["far_z"])
+
+    vp, ivp = mats(pose)
+    pvp = mats(prev)[0] if prev is not None else vp
+    pp = prev if prev is not None else pose
+    f = np.zeros(76, np.float32)
+    u = f.view(np.uint32)
+    f[0:16] = ivp
+    f[16:32] = pvp
+    f[32:35] = np.asarray(pose["pos"], np.float64).astype(np.float32)
+    f[36:39] = np.asarray(pp["pos"], np.float64).astype(np.float32)
+    sx, sy, sz = (float(np.float32(v)) for v in sun_dir)   # the host API carries the direction as f32
+    sl = math.sqrt(sx * sx + sy * sy + sz * sz)
+    f[40:43] = (sx / sl, sy / sl, sz / sl)
+    f[43] = math.cos(math.radians(0.27)) if sun_cos_radius is None else sun_cos_radius
+    f[44:47] = sun_irradiance
+    f[47] = sky
+    u[48], u[49], u[50] = frame & 0xFFFFFFFF, bounces, flags
+    f[52], f[53], f[54] = w, h, exposure
+    u[56], u[58] = 0, 3
+    f[60:64] = (20.0, 1.0, 0.1, 0.0008)
+    f[64:67] = (30.0, max_history, 24.0)
+    f[68:72] = (48.0, 1.0, 1.0, 0.5)
+    f[72] = 8.0
+    return f.tobytes()

@@ -34,6 +34,15 @@
 // (absolute error up to 2^-11 for sin/cos).  The oracle and the kernels both
 // use the project's own definitions below (Cody-Waite reduction + Taylor
 // series), so both sides compute identical bits.
+//
+// Literal mode (compiled with -DORC_LITERAL into liboracle_literal.so): the
+// shader text as written, with none of the kernels' reformulations --
+// sin/cos/exp/log2/pow from the C library's binary32 functions, pow(x, 8) and
+// pow(x, 32) as pow, dot products as (x*x' + y*y') + z*z', and the a-trous
+// weight as the product of its two exps with every tap summed (no skip of
+// zero-weight taps, no fused multiply-adds).  The kernels are held to this
+// mode at the specification's tolerances (per-sample radiance 1e-4 relative,
+// temporal and denoised output 2e-3), not bit for bit.
 // ============================================================================
 #include <cstdint>
 #include <cstring>
@@ -45,6 +54,12 @@
 #endif
 
 namespace {
+
+#ifdef ORC_LITERAL
+constexpr bool kLiteral = true;
+#else
+constexpr bool kLiteral = false;
+#endif
 
 // ---------------------------------------------------------------------------
 // scalar helpers
@@ -80,6 +95,7 @@ inline f3 mix3(f3 a, f3 b, float t) { return mk(mixf(a.x, b.x, t), mixf(a.y, b.y
 // formed Cody-Waite style with pi/2 = 201/128 + PIO2_LO, then evaluated by the
 // Taylor series of sin (to r^9) and cos (to r^10) about zero.
 inline void om_sincos(float x, float& s, float& c) {
+  if (kLiteral) { s = std::sin(x); c = std::cos(x); return; }
   const float TWO_OVER_PI = 0.636619747f;
   const float PIO2_HI = 1.5703125f;
   const float PIO2_LO = 0.000483826792f;
@@ -116,6 +132,7 @@ inline float om_exp_poly(float r) {
 
 // e^x: k = round(x log2 e), r = x - k ln2 (ln2 split into 0x3f317200 + LN2_LO).
 inline float om_exp(float x) {
+  if (kLiteral) return std::exp(x);
   if (!(x > -87.0f)) return 0.0f;        // also maps NaN/-inf to 0
   if (x > 88.0f) return INFINITY;
   const float LOG2E = 1.44269502f;
@@ -138,6 +155,7 @@ inline float om_exp2(float z) {
 // log2(x) for finite x > 0: x = m 2^e with m in [sqrt(1/2), sqrt(2)],
 // log2(m) = (2/ln2) atanh(s), s = (m-1)/(m+1), atanh by its series to s^9.
 inline float om_log2(float x) {
+  if (kLiteral) return std::log2(x);
   uint32_t b = fbits(x);
   int e = (int)(b >> 23) - 127;
   if ((b >> 23) == 0) {                    // subnormal input
@@ -156,6 +174,7 @@ inline float om_log2(float x) {
 
 // x^y for x >= 0, y > 0 (the only uses on this path); 0^y = 0.
 inline float om_pow(float x, float y) {
+  if (kLiteral) return std::pow(x, y);
   if (!(x > 0.0f)) return 0.0f;
   return om_exp2(y * om_log2(x));
 }
@@ -417,6 +436,7 @@ inline f3 sky_color(const Uni& u, f3 rd, bool withSunDisc) {
   f3 sd = mk(u.sunDir[0], u.sunDir[1], u.sunDir[2]);
   float sunAmt = fmaxf_(dot3(rd, sd), 0.0f);
   float s2 = sunAmt * sunAmt, s4 = s2 * s2, s8 = s4 * s4;   // pow(sunAmt, 8)
+  if (kLiteral) s8 = std::pow(sunAmt, 8.0f);
   sky = add(sky, muls(muls(mk(1.0f, 0.75f, 0.5f), s8), 0.2f));
   if (withSunDisc && sunAmt > u.sunDir[3]) {
     float solidAngle = TWO_PI * (1.0f - u.sunDir[3]);
@@ -453,7 +473,10 @@ inline f3 cosine_hemisphere(f3 n, Rng& rng) {
   return normalize3(d);
 }
 
-struct PixStats { uint64_t rays, outer, inner, vreads; };
+// sig: a hash of the pixel's discrete path -- every trace issued, in order, by
+// its outcome (miss, or hit voxel and face) -- so two restatements that differ
+// in their last bits can be compared wherever they took the same path.
+struct PixStats { uint64_t rays, outer, inner, vreads; uint32_t sig; };
 
 // When set, every trace() issued by path_pixel appends (origin, direction,
 // maxT) in voxel units -- the ray workload replayed by the reference
@@ -482,7 +505,13 @@ void path_pixel(const World& W, const Uni& u, float fclamp, uint32_t gx, uint32_
   f3 ro = mk(u.camPos[0], u.camPos[1], u.camPos[2]);
   f3 rd = camera_ray(u, uvx, uvy);
 
-  auto count = [&](const Hit& h) { st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads; };
+  auto count = [&](const Hit& h) {
+    st.rays++; st.outer += h.outer; st.inner += h.inner; st.vreads += h.vreads;
+    const uint32_t code = h.t < 0.0f ? 0x9e3779b9u
+                                     : ((uint32_t)h.vx * 73856093u) ^ ((uint32_t)h.vy * 19349663u) ^
+                                           ((uint32_t)h.vz * 83492791u) ^ ((uint32_t)face_of(h.n) << 28);
+    st.sig = pcg_hash(st.sig ^ code);
+  };
   Hit h0 = trace_logged(W, ro, rd, 1e4f);
   count(h0);
   if (h0.t < 0.0f) {
@@ -650,7 +679,10 @@ void bilinear(Fetch fetch, int W, int H, float u, float v, float out[4]) {
   }
 }
 
-inline float luminance(const float* c) { return std::fmaf(c[2], 0.0722f, std::fmaf(c[1], 0.7152f, c[0] * 0.2126f)); }
+inline float luminance(const float* c) {
+  if (kLiteral) return (c[0] * 0.2126f + c[1] * 0.7152f) + c[2] * 0.0722f;   // dot(c, weights) (atrous.wgsl:22-24)
+  return std::fmaf(c[2], 0.0722f, std::fmaf(c[1], 0.7152f, c[0] * 0.2126f));
+}
 
 
 // ---------------------------------------------------------------------------
@@ -1545,9 +1577,21 @@ void orc_trace_naive(const uint32_t* vox, int N, const float* o, const float* d,
 // pathtrace.wgsl:248-330 (plain branch) for rows [row0, row1) stepping row_step.
 // rad16: rgba16f bits W*H*4; rad32 (optional): fp32 radiance W*H*4;
 // alb8: rgba8 W*H*4; gbuf: rgba32f W*H*4.  Rows not visited are untouched.
+void orc_pathtrace_sig(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                       const void* uniforms, float fclamp, int Wd, int Hd, int row0, int row1, int row_step,
+                       uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, OrcStats* stats, uint32_t* sig);
+
 void orc_pathtrace(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
                    const void* uniforms, float fclamp, int Wd, int Hd, int row0, int row1, int row_step,
                    uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, OrcStats* stats) {
+  orc_pathtrace_sig(vox, bricks, masks, N, uniforms, fclamp, Wd, Hd, row0, row1, row_step, rad16, rad32, alb8, gbuf,
+                    stats, nullptr);
+}
+
+// orc_pathtrace plus, when sig is given, the per-pixel path signature (W*H u32).
+void orc_pathtrace_sig(const uint32_t* vox, const uint32_t* bricks, const uint32_t* masks, int N,
+                       const void* uniforms, float fclamp, int Wd, int Hd, int row0, int row1, int row_step,
+                       uint16_t* rad16, float* rad32, uint8_t* alb8, float* gbuf, OrcStats* stats, uint32_t* sig) {
   World W{vox, bricks, masks, N, N / BRICK};
   Uni u; std::memcpy(&u, uniforms, sizeof(Uni));
   if (row_step < 1) row_step = 1;
@@ -1557,11 +1601,13 @@ void orc_pathtrace(const uint32_t* vox, const uint32_t* bricks, const uint32_t* 
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : rays, outer, inner, vreads, pix)
   for (int ri = 0; ri < (int)rows.size(); ri++) {
     int y = rows[ri];
-    PixStats st{0, 0, 0, 0};
+    PixStats st{0, 0, 0, 0, 0};
     for (int x = 0; x < Wd; x++) {
       float rad[4], gb[4]; uint8_t al[4];
+      st.sig = 0u;
       path_pixel(W, u, fclamp, (uint32_t)x, (uint32_t)y, (uint32_t)Wd, (uint32_t)Hd, rad, al, gb, st);
       size_t p = (size_t)y * Wd + x;
+      if (sig) sig[p] = st.sig;
       for (int c = 0; c < 4; c++) {
         if (rad16) rad16[4 * p + c] = f32_to_f16(rad[c]);
         if (rad32) rad32[4 * p + c] = rad[c];
@@ -1668,6 +1714,30 @@ void orc_atrous(const void* uniforms, int Wd, int Hd, const void* src, int src_f
       float k00 = K[0] * K[0];
       float sum[3] = {(center[0] * K[0]) * K[0], (center[1] * K[0]) * K[0], (center[2] * K[0]) * K[0]};
       float wSum = k00;
+      if (kLiteral) {   // atrous.wgsl:60-79 as written
+        for (int dy = -2; dy <= 2; dy++) {
+          for (int dx = -2; dx <= 2; dx++) {
+            if (dx == 0 && dy == 0) continue;
+            int qx = px + dx * step, qy = py + dy * step;
+            if (qx < 0 || qy < 0 || qx >= Wd || qy >= Hd) continue;
+            size_t q = (size_t)qy * Wd + qx;
+            float cq[4]; fetch(q, cq);
+            const float* gq = gbuf + 4 * q;
+            if (gq[3] < 0.0f) continue;
+            float wKernel = K[std::abs(dx)] * K[std::abs(dy)];
+            float wNormal = std::pow(fmaxf_((g[0] * gq[0] + g[1] * gq[1]) + g[2] * gq[2], 0.0f), 32.0f);
+            float wDepth = std::exp(-std::fabs(g[3] - gq[3]) / (0.05f * g[3] + 0.01f));
+            float wLum = std::exp(-std::fabs(lumC - luminance(cq)) / sigmaL);
+            float w = ((wKernel * wNormal) * wDepth) * wLum;
+            for (int c = 0; c < 3; c++) sum[c] = sum[c] + cq[c] * w;
+            wSum = wSum + w;
+          }
+        }
+        float den = fmaxf_(wSum, 1e-6f);
+        float v[4] = {sum[0] / den, sum[1] / den, sum[2] / den, center[3]};
+        for (int c = 0; c < 4; c++) dst[4 * p + c] = f32_to_f16(v[c]);
+        continue;
+      }
       for (int dy = -2; dy <= 2; dy++) {
         for (int dx = -2; dx <= 2; dx++) {
           if (dx == 0 && dy == 0) continue;
@@ -1796,6 +1866,186 @@ void orc_camera_matrices(const double pos[3], double yaw, double pitch, double f
                    (float)-dt(rt, pos), (float)-dt(up, pos), (float)-dt(z, pos), 1.0f};
   js_mul(P, W2C, viewProj);
   js_mul(C2W, IP, invViewProj);
+}
+
+// World generator, restated from scene.js generateScene(N, 'default')
+// (scene.js:203-222 noise, 232-264 terrain, 266-301 room, 362-374 light strip
+// and boxes, 376-408 trees, lanterns and corner lamp) with the noise seed as a
+// parameter (the reference fixes it at 1337), plus the benchmark world of the
+// plain-frame workload: the same terrain and room, 40 trees placed by a PCG
+// hash chain outside the room and the camera corridor, and red / green / blue
+// lanterns of intensity 15.  JavaScript's doubles and int32 wrap-around are
+// reproduced with double and 32-bit unsigned arithmetic.  The bench's CPU
+// reference arm uses it so that its process loads no product library.
+}  // extern "C"
+
+namespace world {
+constexpr double kVS = 1.0 / 16.0;
+inline uint32_t M(int r, int g, int b, int e = 0) {
+  return (uint32_t)r | ((uint32_t)g << 8) | ((uint32_t)b << 16) | ((uint32_t)e << 24);
+}
+inline int V(double m) { return (int)std::floor(m / kVS + 0.5); }
+inline int fl(double x) { return (int)std::floor(x); }
+struct Gen {
+  int N; uint32_t* vox; int64_t seed;
+  std::vector<int> heights;
+  int cx, cz, x0, x1, z0, z1, floorY, y1, roomW, roomH;
+  void set(int x, int y, int z, uint32_t m) {
+    if (x >= 0 && y >= 0 && z >= 0 && x < N && y < N && z < N) vox[(size_t)x + (size_t)y * N + (size_t)z * N * N] = m;
+  }
+  template <class F> void boxf(int ax, int ay, int az, int bx, int by, int bz, F f) {
+    for (int z = az; z <= bz; z++) for (int y = ay; y <= by; y++) for (int x = ax; x <= bx; x++) set(x, y, z, f(x, z));
+  }
+  void box(int ax, int ay, int az, int bx, int by, int bz, uint32_t m) {
+    boxf(ax, ay, az, bx, by, bz, [m](int, int) { return m; });
+  }
+  double hash(int64_t x, int64_t y) const {        // (x*374761393 + y*668265263 + seed*1442695041) | 0, Math.imul
+    uint32_t h = (uint32_t)((uint64_t)x * 374761393ull + (uint64_t)y * 668265263ull + (uint64_t)seed * 1442695041ull);
+    h = (h ^ (h >> 13)) * 1274126177u;
+    return (double)(h ^ (h >> 16)) / 4294967296.0;
+  }
+  double noise(double x, double y) const {
+    double v = 0.0, amp = 0.5, f = 1.0;
+    for (int o = 0; o < 4; o++) {
+      const double px = x * f, py = y * f, xi = std::floor(px), yi = std::floor(py);
+      auto sm = [](double t) { return t * t * (3 - 2 * t); };
+      const double xf = sm(px - xi), yf = sm(py - yi);
+      const int64_t X = (int64_t)xi, Y = (int64_t)yi;
+      const double a = hash(X, Y), b = hash(X + 1, Y), c = hash(X, Y + 1), d = hash(X + 1, Y + 1);
+      v += (a + (b - a) * xf + (c - a) * yf + (a - b - c + d) * xf * yf) * amp;
+      amp *= 0.5; f *= 2.0;
+    }
+    return v;
+  }
+  int ground(int x, int z) const { return heights[std::max(0, std::min(N - 1, x)) + std::max(0, std::min(N - 1, z)) * N]; }
+  void terrain() {
+    const int baseH = fl(N * 0.16);
+    heights.assign((size_t)N * N, 0);
+    for (int z = 0; z < N; z++)
+      for (int x = 0; x < N; x++) {
+        const int h = baseH + fl(noise(x * 0.02, z * 0.02) * N * 0.10);
+        heights[x + z * N] = h;
+        for (int y = 0; y <= h && y < N; y++) {
+          const int v = (x * 7 + y * 13 + z * 5) % 9;
+          vox[(size_t)x + (size_t)y * N + (size_t)z * N * N] =
+              y == h ? M(88 + v, 130 + v, 60) : (y > h - 4 ? M(110 + v, 82 + v, 58) : M(120 + v, 120 + v, 125 + v));
+        }
+      }
+  }
+  void room() {
+    roomW = std::min(V(5), fl(N * 0.45));
+    roomH = std::min(V(3.2), fl(N * 0.3));
+    cx = fl(N * 0.5); cz = fl(N * 0.55);
+    x0 = cx - (roomW >> 1); x1 = cx + (roomW >> 1); z0 = cz - (roomW >> 1); z1 = cz + (roomW >> 1);
+    floorY = ground(cx, cz) + 1; y1 = floorY + roomH;
+    const int T = 2;
+    boxf(x0 - T, floorY, z0 - T, x1 + T, floorY, z1 + T, [](int x, int z) { const int v = (x + z) % 9; return M(110 + v, 82 + v, 58); });
+    box(x0 - T, floorY + 1, z0 - T, x1 + T, y1 + T + 4, z1 + T, 0);
+    boxf(x0 - T, floorY, z0 - T, x1 + T, floorY, z1 + T,
+         [](int x, int z) { return ((x >> 3) + (z >> 3)) % 2 ? M(180, 150, 110) : M(150, 118, 84); });
+    const uint32_t white = M(225, 222, 215);
+    box(x0 - T, floorY + 1, z1 + 1, x1 + T, y1, z1 + T, white);
+    box(x0 - T, floorY + 1, z0 - T, x1 + T, y1, z0 - 1, white);
+    box(x0 - T, floorY + 1, z0 - T, x0 - 1, y1, z1 + T, M(200, 45, 40));
+    box(x1 + 1, floorY + 1, z0 - T, x1 + T, y1, z1 + T, M(55, 175, 60));
+    box(x0 - T, y1 + 1, z0 - T, x1 + T, y1 + T, z1 + T, white);
+    const int doorHalf = fl(roomW * 0.28);
+    box(cx - doorHalf, floorY + 1, z0 - T, cx + doorHalf, y1 - 2, z0 - 1, 0);
+    box(x1 + 1, floorY + fl(roomH * 0.45), cz - fl(roomW * 0.3), x1 + T, floorY + fl(roomH * 0.8), cz + fl(roomW * 0.3), 0);
+    const int lHalf = fl(roomW * 0.18);
+    box(cx - lHalf, y1, cz - lHalf, cx + lHalf, y1, cz + lHalf, M(255, 240, 220, 210));
+    const int tallW = fl(roomW * 0.16), tallH = fl(roomH * 0.55);
+    box(cx - fl(roomW * 0.28) - tallW, floorY + 1, cz + fl(roomW * 0.05), cx - fl(roomW * 0.28), floorY + tallH,
+        cz + fl(roomW * 0.05) + tallW, M(200, 200, 210));
+    const int shortW = fl(roomW * 0.18), shortH = fl(roomH * 0.28);
+    box(cx + fl(roomW * 0.10), floorY + 1, cz - fl(roomW * 0.25), cx + fl(roomW * 0.10) + shortW, floorY + shortH,
+        cz - fl(roomW * 0.25) + shortW, M(210, 170, 90));
+  }
+  void tree(int tx, int tz) {
+    const int g = ground(tx, tz);
+    const int trunkH = V(1.4) + ((tx * 31 + tz * 17) % V(0.8));
+    for (int y = g + 1; y <= g + trunkH; y++) { set(tx, y, tz, M(95, 68, 42)); set(tx + 1, y, tz, M(95, 68, 42)); }
+    const int cy = g + trunkH + V(0.35), r = V(0.7) + ((tx + tz) % 3);
+    for (int dz = -r; dz <= r; dz++)
+      for (int dy = -r; dy <= r; dy++)
+        for (int dx = -r; dx <= r; dx++) {
+          const double d2 = dx * dx + dy * dy * 1.6 + dz * dz;
+          if (d2 <= r * r && ((dx * 13 + dy * 7 + dz * 11) % 5 != 0 || d2 < r * r * 0.5)) {
+            const int v = (dx * 3 + dy * 5 + dz * 7) % 12 + ((dx + dy + dz) % 2) * 6;
+            set(tx + dx, cy + dy, tz + dz, M(50 + v, 120 + v, 45));
+          }
+        }
+  }
+  void lantern(int lx, int lz, uint32_t m) {
+    const int g = ground(lx, lz), h = V(1.1);
+    for (int y = g + 1; y <= g + h; y++) set(lx, y, lz, M(60, 60, 65));
+    box(lx - 1, g + h + 1, lz - 1, lx + 1, g + h + 3, lz + 1, m);
+  }
+};
+inline uint32_t pcg_step(uint32_t v) {
+  v = v * 747796405u + 2891336453u;
+  const uint32_t w = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+}  // namespace world
+
+extern "C" {
+
+// kind 0: the reference world (scene.js 'default'); kind 2: the benchmark
+// world.  spawn (8 doubles): x, y, z, yaw, pitch, vertical fov, near, far.
+int orc_scene_generate(int kind, int N, uint32_t seed, uint32_t* vox, double* spawn) {
+  using namespace world;
+  if ((kind != 0 && kind != 2) || N < 8 || N % 8 != 0) return 1;
+  std::memset(vox, 0, (size_t)N * N * N * sizeof(uint32_t));
+  Gen g{N, vox, (int64_t)seed, {}, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  g.terrain();
+  g.room();
+  const uint32_t lampWarm = M(255, 190, 110, 255);
+  if (kind == 0) {
+    const double spots[6][2] = {{0.15, 0.2}, {0.82, 0.25}, {0.2, 0.8}, {0.86, 0.78}, {0.12, 0.55}, {0.65, 0.12}};
+    for (auto& sp : spots) g.tree(fl(N * sp[0]), fl(N * sp[1]));
+    g.lantern(fl(N * 0.35), fl(N * 0.25), lampWarm);
+    g.lantern(fl(N * 0.68), fl(N * 0.30), M(90, 220, 255, 255));
+    g.lantern(fl(N * 0.25), fl(N * 0.65), M(255, 90, 200, 255));
+    g.box(g.x0 + 2, g.floorY + 1, g.z1 - 4, g.x0 + 4, g.floorY + 3, g.z1 - 2, lampWarm);
+    if (spawn) {
+      const double s[8] = {g.cx * kVS, (g.ground(g.cx, g.z0 - V(3)) + 1) * kVS + 1.65, (g.z0 - V(3.5)) * kVS, 0.0,
+                           -0.05, 70.0 * M_PI / 180.0, 0.05, 400.0};
+      std::memcpy(spawn, s, sizeof s);
+    }
+    return 0;
+  }
+  // benchmark world: seeded trees outside the room and the camera corridor
+  const int corX0 = g.cx - 24, corX1 = g.cx + 24;
+  uint32_t st = pcg_step(seed * 2654435761u + 17u);
+  auto uni = [&]() { st = pcg_step(st); return (double)st / 4294967296.0; };
+  int placed = 0;
+  for (int attempt = 0; attempt < 4000 && placed < 40; attempt++) {
+    const int tx = fl(N * (0.05 + 0.90 * uni()));
+    const int tz = fl(N * (0.05 + 0.90 * uni()));
+    const int margin = V(0.7) + 3;
+    const bool inRoom = tx >= g.x0 - 2 - margin && tx <= g.x1 + 2 + margin && tz >= g.z0 - 2 - margin &&
+                        tz <= g.z1 + 2 + margin;
+    const bool inCorridor = tx >= corX0 - margin && tx <= corX1 + margin && tz < g.z0;
+    if (inRoom || inCorridor) continue;
+    g.tree(tx, tz);
+    placed++;
+  }
+  const int E = std::min(255, std::max(1, (int)std::floor(15.0 * 255.0 / 24.0 + 0.5)));
+  g.lantern(fl(N * 0.35), fl(N * 0.25), M(255, 40, 40, E));
+  g.lantern(fl(N * 0.68), fl(N * 0.30), M(40, 255, 40, E));
+  g.lantern(fl(N * 0.25), fl(N * 0.65), M(40, 40, 255, E));
+  g.box(g.x0 + 2, g.floorY + 1, g.z1 - 4, g.x0 + 4, g.floorY + 3, g.z1 - 2, lampWarm);
+  if (spawn) {
+    const int zStart = std::max(2, g.z0 - 60);
+    int gmax = g.floorY - 1;
+    for (int z = zStart; z <= g.z0; z++)
+      for (int x = g.cx - 16; x <= g.cx + 16; x++) gmax = std::max(gmax, g.ground(x, z));
+    const double s[8] = {g.cx * kVS, (gmax + 1) * kVS + 1.65, zStart * kVS, -30.0 * M_PI / 180.0, -0.05,
+                         60.0 * M_PI / 180.0, 0.05, 400.0};
+    std::memcpy(spawn, s, sizeof s);
+  }
+  return 0;
 }
 
 // Scalar checks of the project transcendentals and storage conversions.

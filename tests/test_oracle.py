@@ -162,3 +162,28 @@ def test_temporal_history_grows_and_caps(orc, vrt):
     assert hist[geo].max() == 4.0
     assert (hist[~geo] == 1.0).all()
     assert np.median(hist[geo]) == 4.0
+
+
+@pytest.mark.parametrize("kind,n,seed", [(0, 256, 1337), (2, 256, 2), (2, 128, 5), (0, 64, 9)])
+def test_oracle_world_matches_library(vrt, orc, kind, n, seed):
+    """The oracle's restatement of the world generator (scene.js, seeded) and
+    of the benchmark world gives the library's voxels and spawn pose."""
+    vox, sp = orc.generate_scene(kind, n, seed)
+    want, wsp = vrt.generate_scene(kind, n, seed)
+    assert np.array_equal(vox, want.ravel())
+    assert tuple(sp["pos"]) == tuple(wsp.pos) and sp["yaw"] == wsp.yaw and sp["pitch"] == wsp.pitch
+    assert sp["fov_y"] == wsp.fov_y
+
+
+@pytest.mark.parametrize("frame", [0, 1, 57, 119])
+def test_oracle_uniforms_match_library(vrt, orc, frame):
+    """Benchmark camera path and uniform block restated without the library."""
+    _, sp = orc.generate_scene(2, 256, 2)
+    _, wsp = vrt.generate_scene(2, 256, 2)
+    pose = orc.camera_spline(sp, frame)
+    prev = orc.camera_spline(sp, frame - 1) if frame else None
+    wpose = vrt.camera_spline(wsp, frame)
+    wprev = vrt.camera_spline(wsp, frame - 1) if frame else None
+    got = orc.uniforms(pose, prev, frame, 2, 3, 1920, 1080, 1.0, 64.0)
+    want = vrt.uniforms_bytes(vrt.make_uniforms(wpose, wprev, vrt.Lighting(), frame, 2, 3, 1920, 1080, 1.0, 64.0))
+    assert got == want
