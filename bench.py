@@ -90,6 +90,17 @@ def profiled_traffic(kernel: str):
     return float(m.group(1)) if m else None
 
 
+def profiled_l2(kernel: str):
+    """L2 throughput of `kernel` as a fraction of its peak, from the committed
+    ncu summary (profiles/<kernel>_1080p_256.md, `l2_throughput_pct:` line)."""
+    p = ROOT / "profiles" / f"{kernel}_1080p_256.md"
+    if not p.exists():
+        return None
+    m = re.search(r"l2_throughput_pct:\s*([0-9.eE+]+)", p.read_text())
+    return {"frac": round(float(m.group(1)) / 100.0, 4),
+            "source": f"ncu lts__t_sectors throughput, % of peak (profiles/{p.name})"} if m else None
+
+
 class ClockSampler:
     """nvidia-smi clocks + throttle reasons sampled every 20 ms while the timed
     region runs.  start() returns once the sampler has produced its first line
@@ -245,7 +256,7 @@ def run_ours(args, world, rank, local):
     clocks = ClockSampler(local)
     clocks.start()
     frame_ms, pt_ms, rays, dda_bytes, pixels, launches = [], [], 0, 0, 0, 0
-    trace_ms, trace_launches = 0.0, 0
+    trace_ms, trace_launches, lane_steps, step_slots = 0.0, 0, 0, 0
     for i in range(args.steps):
         f = args.warmup + i
         u = frame_uniforms(vrt, spawn, f)
@@ -261,6 +272,8 @@ def run_ours(args, world, rank, local):
         launches += st.launches
         trace_ms += st.ms_trace
         trace_launches += st.trace_launches
+        lane_steps += st.dda_outer + st.dda_inner
+        step_slots += st.trace_step_slots
     ctx.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -326,6 +339,11 @@ def run_ours(args, world, rank, local):
                      "traffic": traffic,
                      "algorithmic_bytes_per_launch": round(alg_bytes / n_launch),
                      "launch_ms_mean": round(kernel_ms / n_launch, 4), "launches": n_launch,
+                     "warp_exec_efficiency": round(lane_steps / step_slots, 4) if step_slots else None,
+                     "warp_exec_efficiency_note": "brick + voxel iterations of all rays over the tracer's lane "
+                                                  "slots (32 x DDA steps per pass x warp passes), counted in the "
+                                                  "kernel",
+                     "l2": profiled_l2(kernel),
                      "note": alg_note + "; the DDA working set (2 MB masks, 64 MB voxels) is L2-resident, "
                              "so the kernel is issue-bound, not HBM-bound"},
         "e2e": {"value": round(e2e_rays / e2e_s / 1e6, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 304,
@@ -345,7 +363,24 @@ def run_ours(args, world, rank, local):
         import copy
         a2 = copy.copy(args)
         a2.steps = min(args.steps, 10)
-        line["plain_vs_batched_cache"] = cache_summary(cache_comparison(a2, local))
+        cc = cache_comparison(a2, local)
+        line["plain_vs_batched_cache"] = cache_summary(cc)
+        try:
+            line["served_c5"] = served_summary(served_comparison(a2, local), cc)
+        except Exception as e:   # the headline line must still print
+            line["served_c5"] = {"error": str(e)[:300]}
+        try:
+            a4 = copy.copy(args)
+            a4.steps, a4.warmup, a4.jobs = 5, 3, 64
+            bl = batched_line(a4, local)
+            line["batched_c3"] = {"metric": bl["metric"], "batched_mrays_s": bl["value"],
+                                  "sequential_mrays_s": bl["sequential"]["value"],
+                                  "speedup_vs_sequential": bl["speedup_vs_sequential"],
+                                  "batch_frame_ms": bl["frame_ms"], "sequential_ms_per_step":
+                                      bl["sequential"]["ms_per_step"], "pixels_per_step": bl["config"]["pixels_per_step"],
+                                  "tuning": bl["config"]["tuning"], "details": "bench.py --mode batched"}
+        except Exception as e:
+            line["batched_c3"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_extras:
         # measured on the same box: the ReSTIR presets, `ours` on the reference's scenarios, the VoxelBench adapter
         import copy
@@ -478,6 +513,10 @@ def batched_jobs(n_jobs: int, seed: int = 3):
 
 
 def run_batched(args, local):
+    print(json.dumps(batched_line(args, local)), flush=True)
+
+
+def batched_line(args, local):
     """64 independent jobs rendered (a) in one batch frame (one launch
     sequence, CUDA graph, autotuned launch shape) and (b) as 64 sequential
     plain frames, one session after another.  Device time from CUDA events;
@@ -560,14 +599,15 @@ def run_batched(args, local):
         "speedup_vs_sequential": round(b_val / s_val, 3),
         "rays_per_step": round(b_rays / args.steps),
         "frame_ms": {"p50": round(statistics.median(b_ms), 3), "p99": round(float(np.percentile(b_ms, 99)), 3)},
+        "gpu_launches_per_step": batch.stats().launches,
     }
-    print(json.dumps(line), flush=True)
     batch.close()
     for s in alone + inb:
         s.close()
     for sc, _ in worlds.values():
         sc.close()
     ctx.close()
+    return line
 
 
 CACHE_SCENES = [
@@ -791,6 +831,35 @@ def cache_summary(c):
                                         for k in ("plain_2bounce", "plain_6bounce")}},
         "details": "bench.py --mode cache",
     }
+
+
+def served_summary(sc, cc):
+    """The serving block of the default line: each form's capacity and
+    latency, its 64-frame MSE against the 4096-spp FP64 reference (the 1080p
+    statistics of the same estimators), and the cache-assisted served form
+    against the plain form, raw and at matched MSE (the plain form at the
+    samples per frame that reach the cache form's MSE)."""
+    f = sc["forms"]
+    q = cc["quality"]["256^3 world (seed 2), 1920x1080, GPU FP64 reference"]
+    sp, m = cc["speed_1080p"]["plain_2bounce"], cc["matched_mse_64frame"]["plain_2bounce"]
+    cost = (m["frame_ms_at_matched_mse"] / sp["frame_ms"]) if m.get("frame_ms_at_matched_mse") else None
+    seq = f["plain_sequential"]["capacity"]["frames_per_s"]
+    cb = f["cache_batched"]["capacity"]["frames_per_s"]
+    out = {"metric": "served frames/s (capacity, queue never empty) and p50/p99 latency under Poisson arrivals; "
+                     "cache-assisted continuous batching vs the plain form (requests one after another, unbatched)",
+           "sessions": sc["sessions"], "session_pixels": sc["session_pixels"],
+           "mse_64frame_vs_4096spp": {"plain": q["plain_2bounce"]["mse_64frame_mean"],
+                                      "cache": q["cache"]["mse_64frame_mean"]},
+           "forms": {k: {"frames_per_s": v["capacity"]["frames_per_s"],
+                         "latency_ms": {str(int(r["rate_rps"])): [r["latency_ms_p50"], r["latency_ms_p99"]]
+                                        for r in v["poisson"]}} for k, v in f.items()},
+           "speedup_cache_batched_vs_plain_sequential": round(cb / seq, 3),
+           "speedup_plain_batched_vs_plain_sequential": round(f["plain_batched"]["capacity"]["frames_per_s"] / seq, 3),
+           "plain_cost_factor_at_matched_mse": round(cost, 3) if cost else None,
+           "speedup_at_matched_mse": round(cb / seq * cost, 3) if cost else None,
+           "latency_note": "latency_ms: rate (req/s) -> [p50, p99]",
+           "details": "bench.py --mode serve"}
+    return out
 
 
 def cache_comparison(args, local):
@@ -1051,6 +1120,117 @@ def run_serve(args, local):
     for sc in scenes:
         sc.close()
     ctx.close()
+
+
+def serve_mix(vrt, ctx, rng, path_kernel="batch_only", count=32):
+    """The serving workload's sessions: grids 128^3 or 256^3 (seeded benchmark
+    worlds), resolutions 360p 40% / 720p 35% / 1080p 20% / 1440p 5%, each
+    session with its own scene (its requests edit it); stops at the first
+    session the context's HBM budget refuses."""
+    sessions, scenes, spawns, meta = [], [], [], []
+    for k in range(count):
+        n = 128 if rng.random() < 0.5 else 256
+        (w, h), = [SERVE_RES[int(rng.choice(4, p=[p for _, p in SERVE_RES]))][0]]
+        vox, spawn = vrt.generate_scene(vrt.VRT_SCENE_FULL, n, 100 + k)
+        try:
+            sc = vrt.Scene(ctx, vox, n)
+            s = vrt.Session(ctx, sc, w, h, firefly_clamp=10.0, path_kernel=path_kernel)
+        except vrt.VrtError as e:      # admission refused by the budget
+            if e.code != 5:
+                raise
+            break
+        scenes.append(sc)
+        sessions.append(s)
+        spawns.append(spawn)
+        meta.append((n, w, h))
+    return sessions, scenes, spawns, meta
+
+
+def serve_requests(vrt, rng, spawns, meta, frames):
+    """make_request(k): the next frame of session k on its camera path with one
+    seeded voxel-box edit of 1..16^3 voxels (carve or fill)."""
+    light = vrt.Lighting()
+
+    def make_request(k):
+        n, w, h = meta[k]
+        f = frames[k]
+        frames[k] += 1
+        pose = vrt.camera_spline(spawns[k], f % 120)
+        prev = vrt.camera_spline(spawns[k], (f - 1) % 120) if f % 120 else None
+        u = vrt.make_uniforms(pose, prev, light, f, 2, 3, w, h)
+        size = rng.integers(1, 17, 3)
+        lo = rng.integers(0, n - 16, 3)
+        val = 0 if rng.random() < 0.5 else int(rng.integers(1, 1 << 24))
+        return u, [(int(lo[0]), int(lo[1]), int(lo[2]), int(lo[0] + size[0] - 1), int(lo[1] + size[1] - 1),
+                    int(lo[2] + size[2] - 1), val)]
+    return make_request
+
+
+def capacity(server, n_sessions, make_request, rng, n_req):
+    """Frames/s with the queue never empty: n_req requests (uniform over the
+    sessions) submitted at once, served to completion; device completion
+    times on the server clock."""
+    import numpy as np
+    t0 = server.now()
+    for _ in range(n_req):
+        k = int(rng.integers(0, n_sessions))
+        u, e = make_request(k)
+        server.submit(k, u, e, t_arrival=t0)
+    done = server.drain()
+    t_end = max(td for *_, td in done)
+    lat = np.array([(td - ta) * 1e3 for _, _, ta, td in done])
+    return {"requests": n_req, "frames_per_s": round(n_req / (t_end - t0), 1),
+            "mean_frame_ms": round((t_end - t0) * 1e3 / n_req, 4), "queue_drain_ms_p99": round(float(np.percentile(lat, 99)), 2)}
+
+
+def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320):
+    """The serving mix (32 sessions, edits between frames) served three ways
+    over the same device-resident sessions: `plain_sequential`, the plain
+    form -- requests one after another through each session's own frame path,
+    unbatched; `plain_batched` -- continuous batching; `cache_batched` --
+    continuous batching with each session's radiance cache (trained on 32
+    frames per session first).  Per form: capacity (the queue never empty)
+    and p50/p99 latency under Poisson arrivals at each rate."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(5)
+    ctx = vrt.Context(local, hbm_budget_bytes=150 * (1 << 30))
+    sessions, scenes, spawns, meta = serve_mix(vrt, ctx, rng, path_kernel="wavefront")
+    server = vrt.Server(ctx, sessions, max_in_flight=2)
+    frames = [0] * len(sessions)
+    make_request = serve_requests(vrt, rng, spawns, meta, frames)
+    a2 = argparse.Namespace(**vars(args))
+    a2.rates, a2.duration = ",".join(str(r) for r in rates), duration
+
+    def warm(rounds):
+        for _ in range(rounds):
+            for k in range(len(sessions)):
+                u, e = make_request(k)
+                server.submit(k, u, e)
+            server.drain()
+
+    out = {}
+    for form in ("plain_sequential", "plain_batched", "cache_batched"):
+        server.set_sequential(form == "plain_sequential")
+        if form == "cache_batched":
+            for k, s in enumerate(sessions):
+                s.set_cache(**dict(CACHE_CFG, seed=k + 1))
+            warm(32)
+        else:
+            warm(1)
+        out[form] = {"capacity": capacity(server, len(sessions), make_request, rng, n_sat),
+                     "poisson": sweep(a2, server, sessions, make_request, rng)}
+    px = sum(w * h for _, w, h in meta)
+    server.close()
+    for s_ in sessions:
+        s_.close()
+    for sc in scenes:
+        sc.close()
+    ctx.close()
+    return {"sessions": len(sessions), "session_pixels": px, "forms": out}
 
 
 def sweep(args, server, sessions, make_request, rng):

@@ -142,6 +142,10 @@ typedef struct VrtFrameStats {
   float ms_cache;             /* cache inference + resolve + training steps    */
   float ms_reuse;             /* ReSTIR frames: reuse passes (inside
                                  ms_pathtrace, which covers all three)         */
+  uint64_t trace_step_slots;  /* wavefront tracer: lane slots of its DDA steps
+                                 (32 x steps per pass x warp passes); the
+                                 brick + voxel iterations over this is the
+                                 tracer's SIMT (warp execution) efficiency     */
 } VrtFrameStats;
 
 /* Camera pose of the reference's fly camera (camera.js:1-57). */
@@ -367,6 +371,31 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 /* Blocks until every submitted request completed (or out[] is full). */
 int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out);
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight);
+/* No counterpart in the reference (a browser renderer serves one view).
+ * A server whose sessions come and go: `max_sessions` slots and a scratch
+ * pool for `max_pixels` pixels per batch launch (a launch takes the oldest
+ * request of each idle session while their pixels fit).  Sessions enter
+ * through the admission queue below. */
+int vrt_server_create_dynamic(VrtCtx* ctx, int max_sessions, long long max_pixels, int max_in_flight,
+                              VrtServer** out);
+/* Admission by the context's HBM budget: queues a session (scene, config)
+ * and creates it as soon as a slot is free and the budget has room for its
+ * buffers, in arrival order -- immediately when it fits.  The server owns
+ * the session.  *ticket names the open request. */
+int vrt_server_open_session(VrtServer* sv, VrtScene* scene, const VrtSessionConfig* cfg, uint64_t* ticket);
+/* The slot of an admitted session (VRT_ERR_STATE while it still waits). */
+int vrt_server_session_of(VrtServer* sv, uint64_t ticket, int* slot);
+/* Closes the session in `slot`: no new requests; once its queued and
+ * in-flight requests are done it is destroyed (if the server created it),
+ * its memory returns to the budget and waiting sessions are admitted. */
+int vrt_server_close_session(VrtServer* sv, int slot);
+/* Open sessions and sessions waiting for admission. */
+int vrt_server_sessions(VrtServer* sv, int* open, int* waiting);
+/* Sequential mode (on = 1): each launch renders the single oldest request
+ * through its session's own frame path (vrt_frame), one after another --
+ * the unbatched form the batched server is measured against.  Every session
+ * needs its own path scratch (not VRT_PATH_BATCH_ONLY).  Only while idle. */
+int vrt_server_set_sequential(VrtServer* sv, int on);
 
 /* ---- scene lights -------------------------------------------------------- */
 /* The emissive-face light list, its power alias table and the per-brick

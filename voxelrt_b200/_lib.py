@@ -90,7 +90,8 @@ class VrtFrameStats(C.Structure):
                 ("ms_temporal", C.c_float), ("ms_atrous", C.c_float), ("ms_present", C.c_float),
                 ("ms_total", C.c_float), ("launches", C.c_uint32), ("trace_launches", C.c_uint32),
                 ("ms_trace", C.c_float), ("cache_on", C.c_uint32), ("cache_queries", C.c_uint64),
-                ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("ms_reuse", C.c_float)]
+                ("cache_samples", C.c_uint64), ("ms_cache", C.c_float), ("ms_reuse", C.c_float),
+                ("trace_step_slots", C.c_uint64)]
 
 
 class VrtLightStats(C.Structure):
@@ -203,6 +204,12 @@ SIGNATURES = {
     "vrt_server_poll": (I, [P, C.POINTER(VrtCompletion), I, C.POINTER(I)]),
     "vrt_server_drain": (I, [P, C.POINTER(VrtCompletion), I, C.POINTER(I)]),
     "vrt_server_pending": (I, [P, C.POINTER(I), C.POINTER(I)]),
+    "vrt_server_create_dynamic": (I, [P, I, C.c_longlong, I, C.POINTER(P)]),
+    "vrt_server_open_session": (I, [P, P, C.POINTER(VrtSessionConfig), C.POINTER(C.c_uint64)]),
+    "vrt_server_session_of": (I, [P, C.c_uint64, C.POINTER(I)]),
+    "vrt_server_close_session": (I, [P, I]),
+    "vrt_server_sessions": (I, [P, C.POINTER(I), C.POINTER(I)]),
+    "vrt_server_set_sequential": (I, [P, I]),
     "vrt_batch_create": (I, [P, C.POINTER(P), I, C.POINTER(P)]),
     "vrt_batch_destroy": (I, [P]),
     "vrt_batch_frame": (I, [P, C.POINTER(VrtUniforms)]),

@@ -507,13 +507,51 @@ class Batch:
 class Server:
     """Continuous batching over device-resident sessions (vrt_server_*)."""
 
-    def __init__(self, ctx: Context, sessions: list, max_in_flight: int = 2):
-        arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
+    def __init__(self, ctx: Context, sessions: list | None, max_in_flight: int = 2, max_sessions: int = 0,
+                 max_pixels: int = 0):
+        """sessions: the fixed set of served sessions; or None for a server whose
+        sessions come and go through open_session / close_session, with
+        `max_sessions` slots and a launch pool of `max_pixels` pixels."""
         h = C.c_void_p()
-        check(lib.vrt_server_create(ctx.h, arr, len(sessions), int(max_in_flight), C.byref(h)))
-        self.h, self.ctx, self.sessions = h, ctx, list(sessions)
+        if sessions is None:
+            check(lib.vrt_server_create_dynamic(ctx.h, int(max_sessions), int(max_pixels), int(max_in_flight),
+                                                C.byref(h)))
+        else:
+            arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
+            check(lib.vrt_server_create(ctx.h, arr, len(sessions), int(max_in_flight), C.byref(h)))
+        self.h, self.ctx, self.sessions = h, ctx, list(sessions or [])
         self._buf = (VrtCompletion * 4096)()
         _track("server", self)
+
+    def open_session(self, scene: Scene, width: int, height: int, firefly_clamp: float = 48.0,
+                     accum_f32: bool = False, path_kernel: str = "batch_only") -> int:
+        """Queues a session for admission by the HBM budget; returns its ticket."""
+        pk = {"wavefront": PATH_WAVEFRONT, "megakernel": PATH_MEGAKERNEL, "batch_only": PATH_BATCH_ONLY}[path_kernel]
+        cfg = VrtSessionConfig(int(width), int(height), float(firefly_clamp), int(bool(accum_f32)), 0, pk)
+        t = C.c_uint64()
+        check(lib.vrt_server_open_session(self.h, scene.h, C.byref(cfg), C.byref(t)))
+        return int(t.value)
+
+    def session_of(self, ticket: int):
+        """The slot of an admitted session, or None while it waits for admission."""
+        k = C.c_int()
+        code = lib.vrt_server_session_of(self.h, C.c_uint64(ticket), C.byref(k))
+        if code == 7:      # VRT_ERR_STATE: still waiting
+            return None
+        check(code)
+        return int(k.value)
+
+    def close_session(self, slot: int) -> None:
+        check(lib.vrt_server_close_session(self.h, int(slot)))
+
+    def session_counts(self) -> tuple:
+        """(open sessions, sessions waiting for admission)."""
+        o, w = C.c_int(), C.c_int()
+        check(lib.vrt_server_sessions(self.h, C.byref(o), C.byref(w)))
+        return int(o.value), int(w.value)
+
+    def set_sequential(self, on: bool) -> None:
+        check(lib.vrt_server_set_sequential(self.h, int(bool(on))))
 
     def now(self) -> float:
         return float(lib.vrt_server_now(self.h))

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <deque>
+#include <unordered_map>
 #include "vrt_internal.h"
 
 using namespace vrt;
@@ -828,6 +829,7 @@ int vrt_session_last_stats(VrtSession* s, VrtFrameStats* out) {
   out->dda_inner = h[kStatInner];
   out->voxel_reads = h[kStatVReads];
   out->pixels = h[kStatPixels];
+  out->trace_step_slots = h[kStatTraceSlots];
   out->launches = s->launches;
   if (h[kStatError]) return fail(VRT_ERR_TIMEOUT, "a bounded wait for staged image tiles ran out");
   out->cache_on = s->cache_on ? 1u : 0u;
@@ -961,8 +963,8 @@ int vrt_read_hdr(VrtSession* s, float* rgb, size_t bytes) {
 
 struct VrtBatch {
   VrtCtx* ctx = nullptr;
-  std::vector<VrtSession*> sessions;
-  uint32_t P = 0;
+  std::vector<VrtSession*> sessions;   // job slots (a server's free slots are NULL)
+  uint32_t P = 0;                      // pixel capacity of the scratch pool
   uint64_t bytes = 0;
   JobHost* h_jobs = nullptr;          // pinned staging of the job table
   uint32_t* h_firsts = nullptr;       // pinned staging of the jobs' first pixels
@@ -1011,21 +1013,18 @@ int vrt_batch_destroy(VrtBatch* b) {
   return VRT_OK;
 }
 
-int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch** out) {
-  if (!ctx || !sessions || n < 1 || !out) return fail(VRT_ERR_INVALID, "bad argument");
-  *out = nullptr;
-  uint64_t P = 0;
-  for (int i = 0; i < n; i++) {
-    if (!sessions[i] || sessions[i]->ctx != ctx) return fail(VRT_ERR_INVALID, "session %d is NULL or of another context", i);
-    for (int k = 0; k < i; k++)
-      if (sessions[k] == sessions[i]) return fail(VRT_ERR_INVALID, "session %d appears twice", i);
-    P += (uint64_t)sessions[i]->W * sessions[i]->H;
-  }
+}  // extern "C"
+
+// A batch with n job slots and a scratch pool for P pixels per launch; the
+// slots are filled from `sessions` (NULL: all slots free).
+static int batch_create_capacity(VrtCtx* ctx, VrtSession* const* sessions, int n, uint64_t P, VrtBatch** out) {
   if (P >= (1ull << 31)) return fail(VRT_ERR_INVALID, "batch of %llu pixels exceeds 2^31", (unsigned long long)P);
+  if (P < 1 || n < 1) return fail(VRT_ERR_INVALID, "empty batch");
   if (int r = set_dev(ctx)) return r;
   VrtBatch* b = new VrtBatch();
   b->ctx = ctx;
-  b->sessions.assign(sessions, sessions + n);
+  if (sessions) b->sessions.assign(sessions, sessions + n);
+  else b->sessions.assign((size_t)n, nullptr);
   b->P = (uint32_t)P;
   const int max_waves = 72;
   b->wf_bytes = wavefront_bytes((int)b->P, 1, max_waves);
@@ -1046,17 +1045,23 @@ int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch**
     return r;
   }
   carve_wavefront(b->wf_mem, b->P, max_waves, b->wf);
-  std::vector<uint32_t> firsts((size_t)n);
-  uint32_t acc = 0;
-  for (int i = 0; i < n; i++) { firsts[(size_t)i] = acc; acc += (uint32_t)(sessions[i]->W * sessions[i]->H); }
-  cudaError_t e = cudaMemcpyAsync(b->d_firsts, firsts.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) {
-    vrt_batch_destroy(b);
-    return fail(VRT_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));
-  }
   *out = b;
   return VRT_OK;
+}
+
+extern "C" {
+
+int vrt_batch_create(VrtCtx* ctx, VrtSession* const* sessions, int n, VrtBatch** out) {
+  if (!ctx || !sessions || n < 1 || !out) return fail(VRT_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  uint64_t P = 0;
+  for (int i = 0; i < n; i++) {
+    if (!sessions[i] || sessions[i]->ctx != ctx) return fail(VRT_ERR_INVALID, "session %d is NULL or of another context", i);
+    for (int k = 0; k < i; k++)
+      if (sessions[k] == sessions[i]) return fail(VRT_ERR_INVALID, "session %d appears twice", i);
+    P += (uint64_t)sessions[i]->W * sessions[i]->H;
+  }
+  return batch_create_capacity(ctx, sessions, n, P, out);
 }
 
 int vrt_batch_set_graph(VrtBatch* b, int enable) {
@@ -1097,6 +1102,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     const int k = idx ? idx[i] : i;
     if (k < 0 || k >= n) return fail(VRT_ERR_INVALID, "job index %d out of range", k);
     ss[(size_t)i] = b->sessions[(size_t)k];
+    if (!ss[(size_t)i]) return fail(VRT_ERR_INVALID, "job slot %d holds no session", k);
     for (int q = 0; q < i; q++)
       if (ss[(size_t)q] == ss[(size_t)i]) return fail(VRT_ERR_INVALID, "session %d listed twice", k);
   }
@@ -1140,6 +1146,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     first += (uint32_t)(s->W * s->H);
   }
   const uint32_t P = first;
+  if (P > b->P) return fail(VRT_ERR_INVALID, "batch frame of %u pixels exceeds the pool's %u", P, b->P);
   CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, (size_t)m * sizeof(JobHost), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(b->d_firsts, b->h_firsts, (size_t)m * 4, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(b->ev_upload, st));
@@ -1213,11 +1220,12 @@ int vrt_batch_last_stats(VrtBatch* b, VrtFrameStats* out) {
   out->dda_inner = h[kStatInner];
   out->voxel_reads = h[kStatVReads];
   out->pixels = h[kStatPixels];
+  out->trace_step_slots = h[kStatTraceSlots];
   out->launches = b->launches;
   out->cache_queries = h[kStatCacheQueries];
   out->cache_samples = h[kStatCacheSamples];
   for (VrtSession* s : b->sessions)
-    if (s->cache_on) {
+    if (s && s->cache_on) {
       out->cache_on = 1u;
       if (int r = vrt_mlp_check(s->mlp)) return r;
     }
@@ -1291,13 +1299,25 @@ struct VrtServer {
     cudaEvent_t done = nullptr;
     std::vector<Req> reqs;
   };
+  // a session waiting for admission: created once the HBM budget has room
+  struct Open {
+    uint64_t ticket = 0;
+    VrtScene* scene = nullptr;
+    VrtSessionConfig cfg;
+  };
   VrtCtx* ctx = nullptr;
-  VrtBatch* batch = nullptr;
-  int n = 0;
+  VrtBatch* batch = nullptr;     // batch->sessions is the slot table (NULL = free slot)
+  int n = 0;                     // slots
   int max_in_flight = 2;
+  bool sequential = false;       // one request per launch through the session's own frame path
   std::deque<Req> pending;
   std::deque<Flight> flights;
-  std::vector<char> busy;
+  std::vector<int> busy;         // requests of the slot in flight
+  std::vector<int> queued;       // requests of the slot pending
+  std::vector<char> owned;       // session created by the server (destroyed when closed)
+  std::vector<char> closing;     // close requested: destroyed once idle
+  std::deque<Open> opens;        // admission queue, FIFO
+  std::unordered_map<uint64_t, int> open_result;   // ticket -> slot (>= 0) or -error code
   std::vector<cudaEvent_t> spare_events;
   uint64_t next_ticket = 1;
   std::chrono::steady_clock::time_point t0;
@@ -1309,20 +1329,73 @@ struct VrtServer {
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
+  VrtSession* at(int k) const { return batch->sessions[(size_t)k]; }
 };
 
-static int server_launch(VrtServer* sv) {
-  // oldest pending request of every idle session, in arrival order
-  std::vector<char> picked((size_t)sv->n, 0);
-  std::vector<VrtServer::Req> take;
-  for (auto it = sv->pending.begin(); it != sv->pending.end();) {
-    const int k = it->session;
-    if (!sv->busy[(size_t)k] && !picked[(size_t)k]) {
-      picked[(size_t)k] = 1;
-      take.push_back(std::move(*it));
-      it = sv->pending.erase(it);
+// Destroys closed sessions that went idle, then admits queued sessions in
+// arrival order while the budget has room (the first that does not fit
+// waits, so later, smaller ones cannot overtake it).
+static int server_admit(VrtServer* sv) {
+  for (int k = 0; k < sv->n; k++) {
+    if (sv->closing[(size_t)k] && !sv->busy[(size_t)k] && !sv->queued[(size_t)k]) {
+      VrtSession* s = sv->at(k);
+      if (sv->owned[(size_t)k] && s) vrt_session_destroy(s);
+      sv->batch->sessions[(size_t)k] = nullptr;
+      sv->closing[(size_t)k] = 0;
+      sv->owned[(size_t)k] = 0;
+    }
+  }
+  while (!sv->opens.empty()) {
+    VrtServer::Open& o = sv->opens.front();
+    int slot = -1;
+    for (int k = 0; k < sv->n && slot < 0; k++)
+      if (!sv->at(k)) slot = k;
+    if (slot < 0) break;                              // every slot in use: wait for a close
+    if ((uint64_t)o.cfg.width * (uint64_t)o.cfg.height > sv->batch->P && !sv->sequential) {
+      sv->open_result[o.ticket] = -VRT_ERR_INVALID;   // larger than the launch pool: never admissible
+      sv->opens.pop_front();
+      continue;
+    }
+    VrtSession* s = nullptr;
+    const std::string keep = g_err;
+    const int r = vrt_session_create(sv->ctx, o.scene, &o.cfg, &s);
+    if (r == VRT_ERR_BUDGET) { g_err = keep; break; }   // wait until memory frees
+    if (r) {
+      sv->open_result[o.ticket] = -r;
     } else {
-      ++it;
+      sv->batch->sessions[(size_t)slot] = s;
+      sv->owned[(size_t)slot] = 1;
+      sv->open_result[o.ticket] = slot;
+    }
+    sv->opens.pop_front();
+  }
+  return VRT_OK;
+}
+
+static int server_launch(VrtServer* sv) {
+  std::vector<VrtServer::Req> take;
+  if (sv->sequential) {
+    // the plain form: the oldest request alone, through its session's frame path
+    if (sv->pending.empty()) return VRT_OK;
+    take.push_back(std::move(sv->pending.front()));
+    sv->pending.pop_front();
+  } else {
+    // oldest pending request of every idle session, in arrival order, while
+    // their pixels fit the pool
+    std::vector<char> picked((size_t)sv->n, 0);
+    uint64_t pix = 0;
+    for (auto it = sv->pending.begin(); it != sv->pending.end();) {
+      const int k = it->session;
+      VrtSession* s = sv->at(k);
+      const uint64_t p = (uint64_t)s->W * s->H;
+      if (!sv->busy[(size_t)k] && !picked[(size_t)k] && pix + p <= sv->batch->P) {
+        picked[(size_t)k] = 1;
+        pix += p;
+        take.push_back(std::move(*it));
+        it = sv->pending.erase(it);
+      } else {
+        ++it;
+      }
     }
   }
   if (take.empty()) return VRT_OK;
@@ -1330,18 +1403,23 @@ static int server_launch(VrtServer* sv) {
   std::vector<int> idx;
   std::vector<VrtUniforms> us;
   for (auto& r : take) {
-    VrtSession* s = sv->batch->sessions[(size_t)r.session];
+    VrtSession* s = sv->at(r.session);
+    sv->queued[(size_t)r.session]--;
     for (const VrtEditBox& e : r.edits)
       if (int rc = vrt_scene_edit_box(s->scene, e.x0, e.y0, e.z0, e.x1, e.y1, e.z1, e.value)) return rc;
     idx.push_back(r.session);
     us.push_back(r.u);
   }
-  if (int rc = batch_frame_impl(sv->batch, idx.data(), (int)idx.size(), us.data())) return rc;
+  if (sv->sequential) {
+    if (int rc = vrt_frame(sv->at(idx[0]), &us[0])) return rc;
+  } else {
+    if (int rc = batch_frame_impl(sv->batch, idx.data(), (int)idx.size(), us.data())) return rc;
+  }
   for (auto& r : take) {
-    VrtSession* s = sv->batch->sessions[(size_t)r.session];
+    VrtSession* s = sv->at(r.session);
     if (r.ldr_out)
       CUDA_TRY(cudaMemcpyAsync(r.ldr_out, s->ldr, px(s) * 4, cudaMemcpyDeviceToHost, st));
-    sv->busy[(size_t)r.session] = 1;
+    sv->busy[(size_t)r.session]++;
   }
   VrtServer::Flight f;
   if (!sv->spare_events.empty()) {
@@ -1377,7 +1455,7 @@ static int server_retire(VrtServer* sv, VrtCompletion* out, int max_out, bool bl
       out[k].t_arrival = r.t_arrival;
       out[k].t_done = t_done;
       k++;
-      sv->busy[(size_t)r.session] = 0;
+      sv->busy[(size_t)r.session]--;
       sv->completed++;
     }
     sv->spare_events.push_back(f.done);
@@ -1386,32 +1464,64 @@ static int server_retire(VrtServer* sv, VrtCompletion* out, int max_out, bool bl
   return k;
 }
 
+static int server_new(VrtCtx* ctx, int max_in_flight, VrtServer** out) {
+  VrtServer* sv = new VrtServer();
+  sv->ctx = ctx;
+  sv->max_in_flight = max_in_flight;
+  sv->t0 = std::chrono::steady_clock::now();
+  *out = sv;
+  return VRT_OK;
+}
+
+static int server_setup(VrtServer* sv) {
+  sv->n = (int)sv->batch->sessions.size();
+  sv->busy.assign((size_t)sv->n, 0);
+  sv->queued.assign((size_t)sv->n, 0);
+  sv->owned.assign((size_t)sv->n, 0);
+  sv->closing.assign((size_t)sv->n, 0);
+  sv->batch->use_graph = false;
+  cudaError_t e = cudaEventCreate(&sv->ref);
+  if (e == cudaSuccess) e = cudaEventRecord(sv->ref, sv->ctx->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(sv->ref);
+  if (e != cudaSuccess) return fail(VRT_ERR_CUDA, "server setup: %s", cudaGetErrorString(e));
+  sv->ref_host = sv->now();
+  return VRT_OK;
+}
+
 extern "C" {
 
 int vrt_server_create(VrtCtx* ctx, VrtSession* const* sessions, int n, int max_in_flight, VrtServer** out) {
   if (!ctx || !sessions || n < 1 || !out || max_in_flight < 1 || max_in_flight > 8)
     return fail(VRT_ERR_INVALID, "bad argument");
   *out = nullptr;
-  VrtServer* sv = new VrtServer();
-  sv->ctx = ctx;
-  sv->n = n;
-  sv->max_in_flight = max_in_flight;
-  sv->busy.assign((size_t)n, 0);
-  sv->t0 = std::chrono::steady_clock::now();
-  if (int r = vrt_batch_create(ctx, sessions, n, &sv->batch)) {
+  VrtServer* sv = nullptr;
+  server_new(ctx, max_in_flight, &sv);
+  int r = vrt_batch_create(ctx, sessions, n, &sv->batch);
+  if (!r) r = server_setup(sv);
+  if (r) {
+    if (sv->batch) vrt_batch_destroy(sv->batch);
     delete sv;
     return r;
   }
-  sv->batch->use_graph = false;
-  cudaError_t e = cudaEventCreate(&sv->ref);
-  if (e == cudaSuccess) e = cudaEventRecord(sv->ref, ctx->stream);
-  if (e == cudaSuccess) e = cudaEventSynchronize(sv->ref);
-  if (e != cudaSuccess) {
-    vrt_batch_destroy(sv->batch);
+  *out = sv;
+  return VRT_OK;
+}
+
+int vrt_server_create_dynamic(VrtCtx* ctx, int max_sessions, long long max_pixels, int max_in_flight,
+                              VrtServer** out) {
+  if (!ctx || !out || max_sessions < 1 || max_sessions > 4096 || max_pixels < 1 || max_in_flight < 1 ||
+      max_in_flight > 8)
+    return fail(VRT_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  VrtServer* sv = nullptr;
+  server_new(ctx, max_in_flight, &sv);
+  int r = batch_create_capacity(ctx, nullptr, max_sessions, (uint64_t)max_pixels, &sv->batch);
+  if (!r) r = server_setup(sv);
+  if (r) {
+    if (sv->batch) vrt_batch_destroy(sv->batch);
     delete sv;
-    return fail(VRT_ERR_CUDA, "server setup: %s", cudaGetErrorString(e));
+    return r;
   }
-  sv->ref_host = sv->now();
   *out = sv;
   return VRT_OK;
 }
@@ -1423,6 +1533,8 @@ int vrt_server_destroy(VrtServer* sv) {
   for (auto& f : sv->flights) cudaEventDestroy(f.done);
   for (cudaEvent_t e : sv->spare_events) cudaEventDestroy(e);
   if (sv->ref) cudaEventDestroy(sv->ref);
+  for (int k = 0; k < sv->n; k++)
+    if (sv->owned[(size_t)k] && sv->at(k)) vrt_session_destroy(sv->at(k));
   vrt_batch_destroy(sv->batch);
   delete sv;
   return VRT_OK;
@@ -1430,11 +1542,70 @@ int vrt_server_destroy(VrtServer* sv) {
 
 double vrt_server_now(VrtServer* sv) { return sv ? sv->now() : 0.0; }
 
+int vrt_server_set_sequential(VrtServer* sv, int on) {
+  if (!sv) return fail(VRT_ERR_INVALID, "server is NULL");
+  if (!sv->pending.empty() || !sv->flights.empty()) return fail(VRT_ERR_STATE, "server has requests in progress");
+  if (on)
+    for (int k = 0; k < sv->n; k++)
+      if (sv->at(k) && sv->at(k)->path_kernel == VRT_PATH_BATCH_ONLY)
+        return fail(VRT_ERR_STATE, "session %d has no path scratch of its own (VRT_PATH_BATCH_ONLY)", k);
+  sv->sequential = on != 0;
+  return VRT_OK;
+}
+
+int vrt_server_open_session(VrtServer* sv, VrtScene* scene, const VrtSessionConfig* cfg, uint64_t* ticket) {
+  if (!sv || !scene || !cfg || !ticket) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (scene->ctx != sv->ctx) return fail(VRT_ERR_INVALID, "scene belongs to another context");
+  if (sv->sequential && cfg->path_kernel == VRT_PATH_BATCH_ONLY)
+    return fail(VRT_ERR_INVALID, "a sequential server's sessions need their own path scratch");
+  VrtServer::Open o;
+  o.ticket = sv->next_ticket++;
+  o.scene = scene;
+  o.cfg = *cfg;
+  sv->opens.push_back(o);
+  *ticket = o.ticket;
+  if (int r = set_dev(sv->ctx)) return r;
+  return server_admit(sv);
+}
+
+int vrt_server_session_of(VrtServer* sv, uint64_t ticket, int* slot) {
+  if (!sv || !slot) return fail(VRT_ERR_INVALID, "NULL argument");
+  auto it = sv->open_result.find(ticket);
+  if (it == sv->open_result.end()) {
+    for (const auto& o : sv->opens)
+      if (o.ticket == ticket) return fail(VRT_ERR_STATE, "session of ticket %llu is waiting for admission",
+                                          (unsigned long long)ticket);
+    return fail(VRT_ERR_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
+  }
+  if (it->second < 0) return fail(-it->second, "opening the session of ticket %llu failed",
+                                  (unsigned long long)ticket);
+  *slot = it->second;
+  return VRT_OK;
+}
+
+int vrt_server_close_session(VrtServer* sv, int slot) {
+  if (!sv || slot < 0 || slot >= sv->n || !sv->at(slot)) return fail(VRT_ERR_INVALID, "no session in slot %d", slot);
+  sv->closing[(size_t)slot] = 1;
+  if (int r = set_dev(sv->ctx)) return r;
+  return server_admit(sv);
+}
+
+int vrt_server_sessions(VrtServer* sv, int* open, int* waiting) {
+  if (!sv) return fail(VRT_ERR_INVALID, "server is NULL");
+  int k = 0;
+  for (int i = 0; i < sv->n; i++) k += sv->at(i) && !sv->closing[(size_t)i] ? 1 : 0;
+  if (open) *open = k;
+  if (waiting) *waiting = (int)sv->opens.size();
+  return VRT_OK;
+}
+
 int vrt_server_submit(VrtServer* sv, int session, const VrtUniforms* u, const VrtEditBox* edits, int n_edits,
                       double t_arrival, void* ldr_out, uint64_t* ticket) {
   if (!sv || !u || session < 0 || session >= sv->n || n_edits < 0 || (n_edits && !edits))
     return fail(VRT_ERR_INVALID, "bad argument");
-  if (int r = check_uniforms(sv->batch->sessions[(size_t)session], u)) return r;
+  if (!sv->at(session) || sv->closing[(size_t)session])
+    return fail(VRT_ERR_INVALID, "slot %d holds no open session", session);
+  if (int r = check_uniforms(sv->at(session), u)) return r;
   if (restir_on(u)) return fail(VRT_ERR_INVALID, "served frames render the plain path (restir flags set)");
   VrtServer::Req r;
   r.ticket = sv->next_ticket++;
@@ -1444,6 +1615,7 @@ int vrt_server_submit(VrtServer* sv, int session, const VrtUniforms* u, const Vr
   r.t_arrival = t_arrival >= 0.0 ? t_arrival : sv->now();
   r.ldr_out = ldr_out;
   sv->pending.push_back(std::move(r));
+  sv->queued[(size_t)session]++;
   if (ticket) *ticket = sv->pending.back().ticket;
   return VRT_OK;
 }
@@ -1455,6 +1627,7 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out) 
   int err = VRT_OK;
   *n_out = server_retire(sv, out, max_out, false, &err);
   if (err) return err;
+  if (int r = server_admit(sv)) return r;
   while ((int)sv->flights.size() < sv->max_in_flight && !sv->pending.empty()) {
     const size_t before = sv->flights.size();
     if (int r = server_launch(sv)) return r;
@@ -1474,13 +1647,11 @@ int vrt_server_drain(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out)
     if (sv->flights.empty()) continue;
     if ((int)sv->flights.front().reqs.size() > max_out - *n_out) break;   // caller's buffer is full
     int err = VRT_OK;
-    VrtServer::Flight& f = sv->flights.front();
-    (void)f;
     const int got = server_retire(sv, out + *n_out, max_out - *n_out, true, &err);
     if (err) return err;
     *n_out += got;
   }
-  return VRT_OK;
+  return server_admit(sv);
 }
 
 int vrt_server_pending(VrtServer* sv, int* queued, int* in_flight) {

@@ -317,6 +317,21 @@ VRT_DI void block_flush_stats(unsigned long long* stats, const DCount& c, uint32
   }
 }
 
+// Block-reduced single counter: *dst += the sum of v over the block (one
+// atomic per block).  All threads of the block call it.
+VRT_DI void block_flush_one(unsigned long long* dst, uint32_t v) {
+  __shared__ uint32_t s_one[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t r = __reduce_add_sync(0xffffffffu, v);
+  if (lane == 0) s_one[w] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0ull;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) tot += s_one[q];
+    if (tot) atomicAdd(dst, tot);
+  }
+}
+
 // Brick occupancy bit of brick bi from the bitmap `occ` (shared memory when
 // the kernel staged it, global otherwise).
 VRT_DI bool brick_occupied(const uint32_t* occ, uint32_t bi) {

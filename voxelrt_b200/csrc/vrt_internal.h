@@ -22,7 +22,8 @@ inline size_t occ_words(int BG) { return ((size_t)BG * BG * BG + 31) / 32; }
 enum StatSlot {
   kStatRays = 0, kStatOuter, kStatInner, kStatVReads, kStatPixels, kStatCacheQueries, kStatCacheSamples,
   kStatError,   // nonzero: a bounded wait on staged copies ran out
-  kStatCount = 8
+  kStatTraceSlots,   // lane step slots of the queue tracer: 32 x steps per pass x passes, per warp
+  kStatCount = 9
 };
 static_assert(kStatRays == 0 && kStatOuter == 1 && kStatInner == 2 && kStatVReads == 3 && kStatPixels == 4,
               "block_flush_stats adds to the first five counters in this order");

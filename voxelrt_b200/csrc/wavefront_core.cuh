@@ -656,6 +656,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
   DScene S = jobs.scene(0);
   F3 rd = f3(0.0f, 0.0f, 0.0f);
   uint32_t entry = 0u;
+  uint32_t passes = 0u;   // passes of the step loop with a lane walking (warp-uniform)
   bool active = false, drained = false;
   while (true) {
     const unsigned idle = __ballot_sync(full, !active);
@@ -705,6 +706,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       if (drained) break;
       continue;
     }
+    passes++;
     if (active) {
 #pragma unroll
       for (int k = 0; k < kSteps; k++)
@@ -723,7 +725,10 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
       }
     }
   }
-  if (stats) block_flush_stats(stats, c, 0u);   // kStatRays..kStatVReads
+  if (stats) {
+    block_flush_stats(stats, c, 0u);   // kStatRays..kStatVReads
+    block_flush_one(stats + kStatTraceSlots, lane == 0 ? passes * (uint32_t)(32 * kSteps) : 0u);
+  }
 }
 
 // shade(0): primary hits over all pixels.  The shading kernels stream the path
