@@ -1115,11 +1115,13 @@ def run_serve(args, local):
         line["forms"] = forms
     print(json.dumps(line), flush=True)
     server.close()
-    for s in sessions:
-        s.close()
+    for s_ in sessions:
+        s_.close()
     for sc in scenes:
         sc.close()
     ctx.close()
+    line["churn"] = churn_line(args, local)
+    print(json.dumps({"mode": "serve-churn", **line["churn"]}), flush=True)
 
 
 def serve_mix(vrt, ctx, rng, path_kernel="batch_only", count=32):
@@ -1231,6 +1233,115 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
         sc.close()
     ctx.close()
     return {"sessions": len(sessions), "session_pixels": px, "forms": out}
+
+
+def churn_line(args, local, slots=32, close_p=0.02):
+    """Serving with sessions that come and go: a dynamic server with 32
+    session slots and a launch pool for 32 sessions of the largest size, under
+    the 150 GB HBM budget.  Sessions open through the admission queue; after
+    each request its session closes with probability close_p and a new session
+    (new world, resolution from the mix) asks for admission, waiting until a
+    slot and memory free up -- the old session's requests drain first.
+    Poisson arrivals over the open sessions at each rate."""
+    import numpy as np
+    import torch
+
+    import voxelrt_b200 as vrt
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(11)
+    ctx = vrt.Context(local, hbm_budget_bytes=150 * (1 << 30))
+    max_px = SERVE_RES[-1][0][0] * SERVE_RES[-1][0][1]
+    server = vrt.Server(ctx, None, max_in_flight=2, max_sessions=slots, max_pixels=slots * max_px)
+    light = vrt.Lighting()
+    state = {}            # slot -> dict(n, w, h, spawn, frame)
+    waiting = {}          # ticket -> (t_open, n, w, h, spawn)
+    scenes = []
+    opened = [0]
+    waits = []
+
+    def open_one():
+        k = opened[0]
+        opened[0] += 1
+        n = 128 if rng.random() < 0.5 else 256
+        (w, h), = [SERVE_RES[int(rng.choice(4, p=[p_ for _, p_ in SERVE_RES]))][0]]
+        vox, spawn = vrt.generate_scene(vrt.VRT_SCENE_FULL, n, 500 + k)
+        sc = vrt.Scene(ctx, vox, n)
+        scenes.append(sc)
+        t = server.open_session(sc, w, h, firefly_clamp=10.0)
+        waiting[t] = (server.now(), n, w, h, spawn)
+
+    def admit():
+        for t in list(waiting):
+            slot = server.session_of(t)
+            if slot is None:
+                continue
+            t0, n, w, h, spawn = waiting.pop(t)
+            waits.append((server.now() - t0) * 1e3)
+            state[slot] = dict(n=n, w=w, h=h, spawn=spawn, frame=0)
+
+    def request(slot):
+        st = state[slot]
+        f = st["frame"]
+        st["frame"] += 1
+        pose = vrt.camera_spline(st["spawn"], f % 120)
+        prev = vrt.camera_spline(st["spawn"], (f - 1) % 120) if f % 120 else None
+        u = vrt.make_uniforms(pose, prev, light, f, 2, 3, st["w"], st["h"])
+        n = st["n"]
+        size = rng.integers(1, 17, 3)
+        lo = rng.integers(0, n - 16, 3)
+        val = 0 if rng.random() < 0.5 else int(rng.integers(1, 1 << 24))
+        return u, [(int(lo[0]), int(lo[1]), int(lo[2]), int(lo[0] + size[0] - 1), int(lo[1] + size[1] - 1),
+                    int(lo[2] + size[2] - 1), val)]
+
+    for _ in range(slots):
+        open_one()
+    admit()
+    results = []
+    closes = 0
+    for rate in [float(x) for x in args.rates.split(",")]:
+        n_req = max(1, int(rate * args.duration))
+        gaps = rng.exponential(1.0 / rate, n_req)
+        t_start = server.now() + 0.01
+        arrivals = t_start + np.cumsum(gaps)
+        done, i = [], 0
+        while i < n_req:
+            now = server.now()
+            while i < n_req and arrivals[i] <= now:
+                admit()
+                slot = int(rng.choice(list(state)))
+                u, e = request(slot)
+                server.submit(slot, u, e, t_arrival=float(arrivals[i]))
+                i += 1
+                if rng.random() < close_p and len(state) > 1:
+                    server.close_session(slot)
+                    del state[slot]
+                    closes += 1
+                    open_one()
+            done += server.poll()
+            admit()
+            if i < n_req and arrivals[i] > server.now():
+                time.sleep(min(2e-4, max(0.0, arrivals[i] - server.now())))
+        done += server.drain()
+        admit()
+        lat = np.array([(td - ta) * 1e3 for _, _, ta, td in done])
+        t_end = max(td for *_, td in done)
+        results.append({"rate_rps": rate, "requests": n_req, "frames_per_s": round(n_req / (t_end - t_start), 1),
+                        "latency_ms_p50": round(float(np.percentile(lat, 50)), 3),
+                        "latency_ms_p99": round(float(np.percentile(lat, 99)), 3)})
+    open_, wait_ = server.session_counts()
+    out = {"rates": results, "sessions_opened": opened[0], "sessions_closed": closes, "open_at_end": open_,
+           "waiting_at_end": wait_,
+           "admission_wait_ms": {"p50": round(float(np.percentile(waits, 50)), 3) if waits else None,
+                                  "p99": round(float(np.percentile(waits, 99)), 3) if waits else None,
+                                  "admitted": len(waits)},
+           "hbm_in_use_gb": round(ctx.bytes_in_use / 2 ** 30, 2),
+           "note": "dynamic server: a session closes after a request with probability 0.02 and a new one waits "
+                   "in the admission queue for a slot and memory (150 GB budget)"}
+    server.close()
+    for sc in scenes:
+        sc.close()
+    ctx.close()
+    return out
 
 
 def sweep(args, server, sessions, make_request, rng):

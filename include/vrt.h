@@ -511,6 +511,23 @@ int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint1
  * the context stays usable. */
 int vrt_selftest_bounded_wait(unsigned int spins);
 
+/* ---- session checkpoint / resume ----------------------------------------- */
+/* No counterpart in the browser renderer; VoxelBench resumes its reference
+ * accumulations from disk (VoxelBench/pipeline/harness.cpp:241-256).  A
+ * checkpoint holds what the session's next frames depend on: the scene's
+ * voxels, both history and G-buffer parities and the frame parity, the
+ * radiance cache's network (fp32 weights, Adam moments and step), the ReSTIR
+ * history (reservoirs, duplication map) and the HDR reference accumulation.
+ * vrt_session_restore loads one into a session of the same size, history
+ * format and scene size (the scene's bricks, masks and bitmap are rebuilt;
+ * its lights are rebuilt on next use); the session then renders the same
+ * frames the checkpointed one would, bit for bit.  Host buffers; the calls
+ * synchronize the context's stream.  VRT_ERR_INVALID for a buffer that is
+ * not a checkpoint of a matching session. */
+int vrt_session_checkpoint_size(VrtSession* s, uint64_t* bytes);
+int vrt_session_checkpoint(VrtSession* s, void* host, uint64_t bytes);
+int vrt_session_restore(VrtSession* s, const void* host, uint64_t bytes);
+
 /* ---- allocation-free denoise ------------------------------------------- */
 /* No counterpart in the reference.  The 3-iteration a-trous chain (steps
  * 1, 2, 4) on caller-owned device buffers, for callers that cannot allocate

@@ -172,6 +172,9 @@ SIGNATURES = {
     "vrt_read_hdr": (I, [P, P, SZ]),
     "vrt_write_history": (I, [P, P, P]),
     "vrt_denoise_atrous_noalloc": (I, [P, I, P, P, I, I, P]),
+    "vrt_session_checkpoint_size": (I, [P, C.POINTER(C.c_uint64)]),
+    "vrt_session_checkpoint": (I, [P, P, C.c_uint64]),
+    "vrt_session_restore": (I, [P, P, C.c_uint64]),
     "vrt_mlp_selftest_gemm": (I, [I, I, I, P, P, P]),
     "vrt_mlp_create": (I, [P, U32, C.POINTER(P)]),
     "vrt_mlp_destroy": (I, [P]),

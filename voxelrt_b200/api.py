@@ -441,6 +441,19 @@ class Session:
         check(lib.vrt_read_hdr(self.h, ptr(a), a.nbytes))
         return a
 
+    def checkpoint(self) -> bytes:
+        """The session's state as bytes (vrt_session_checkpoint)."""
+        n = C.c_uint64()
+        check(lib.vrt_session_checkpoint_size(self.h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        check(lib.vrt_session_checkpoint(self.h, ptr(buf), n.value))
+        return buf.tobytes()
+
+    def restore(self, state: bytes) -> None:
+        """Loads a checkpoint of a session of the same size (vrt_session_restore)."""
+        buf = np.frombuffer(state, np.uint8)
+        check(lib.vrt_session_restore(self.h, ptr(buf), buf.size))
+
     def write_history(self, accum_prev: np.ndarray | None, gbuf_prev: np.ndarray | None) -> None:
         a = None if accum_prev is None else np.ascontiguousarray(accum_prev)
         g = None if gbuf_prev is None else np.ascontiguousarray(gbuf_prev, np.float32)

@@ -123,9 +123,11 @@ constexpr int kGA0 = 0, kGA1 = kGA0 + 128 * kIn * 2, kGA2 = kGA1 + 128 * kHid * 
 constexpr int kGDY = kGA3 + 128 * kHid * 2, kGStride = kGDY + 128 * kHid * 2;   // 84 KB per group
 constexpr int kGBase = kWEnd, kGEnd = kGBase + 2 * kGStride;
 constexpr int kTrainSmem = kGEnd + 1024;   // slack: MN-major views read up to 1 KB past a tile
-// inference kernel: forward weights + two activation buffers
-constexpr int kIA0 = kWEnd, kIA1 = kIA0 + 128 * kIn * 2, kIEnd = kIA1 + 128 * kIn * 2;
-constexpr int kInferSmem = kIEnd;
+// inference kernel: forward weights + per tile (two in flight) an input tile
+// X (80 columns, later the 64-column layer-2 input) and a 64-column tile Y
+constexpr int kIX0 = kWEnd, kIY0 = kIX0 + 128 * kIn * 2, kIX1 = kIY0 + 128 * kHid * 2,
+              kIY1 = kIX1 + 128 * kIn * 2, kIEnd = kIY1 + 128 * kHid * 2;
+constexpr int kInferSmem = kIEnd;   // 100 KB: two CTAs per SM
 
 // TMEM columns (fp32): layer outputs / input gradients of group g at 64 g,
 // weight gradients accumulated over all of a CTA's samples at kTW*
@@ -184,21 +186,28 @@ __device__ __forceinline__ void store_row(uint8_t* tile, int row, int C, const f
     *reinterpret_cast<uint4*>(tile + umma::canon_off(row, 8 * cg, C)) = pack8(v + 8 * cg);
 }
 
-// Loads bf16 weights (row-major [K_in x N_out]) into the canonical smem
-// layout W^T: rows N_out, columns K_in.  Read K-major it is the B operand of
-// the forward GEMMs; read MN-major it is the B operand W of the input-gradient
-// GEMMs dX = dH W^T.
-__device__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w) {
-  for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-    int l, kin, nout, off;
-    if (i < kOff1) { l = 0; kin = kIn; nout = kHid; off = kOff0; }
-    else if (i < kOff2) { l = 1; kin = kHid; nout = kHid; off = kOff1; }
-    else if (i < kOff3) { l = 2; kin = kHid; nout = kHid; off = kOff2; }
-    else { l = 3; kin = kHid; nout = kOutPad; off = kOff3; }
-    const int k = (i - off) / nout, n = (i - off) % nout;
-    const int fbase = l == 0 ? kWf0 : (l == 1 ? kWf1 : (l == 2 ? kWf2 : kWf3));
-    *reinterpret_cast<uint16_t*>(smem + fbase + umma::canon_off(n, k, kin)) = w[i];
-  }
+// The bf16 weight copy is kept in global memory as the kernels' shared-memory
+// image of the weights: for each layer W^T (rows N_out, columns K_in) in the
+// canonical no-swizzle layout at byte offset kWf<l>, kWEnd bytes in all.
+// Read K-major it is the B operand of the forward GEMMs; read MN-major it is
+// the B operand W of the input-gradient GEMMs dX = dH W^T.  image_index maps
+// parameter i (row-major W_l[K_in x N_out]) to its u16 position in the image.
+__device__ __forceinline__ int image_index(int i) {
+  int kin, nout, off, fbase;
+  if (i < kOff1) { kin = kIn; nout = kHid; off = kOff0; fbase = kWf0; }
+  else if (i < kOff2) { kin = kHid; nout = kHid; off = kOff1; fbase = kWf1; }
+  else if (i < kOff3) { kin = kHid; nout = kHid; off = kOff2; fbase = kWf2; }
+  else { kin = kHid; nout = kOutPad; off = kOff3; fbase = kWf3; }
+  const int k = (i - off) / nout, n = (i - off) % nout;
+  return (int)((fbase + umma::canon_off(n, k, kin)) >> 1);
+}
+static_assert(kWEnd == kParams * 2, "the weight image holds every parameter once");
+
+// Copies the weight image (kWEnd bytes) into shared memory, 16 bytes per access.
+__device__ __forceinline__ void load_weights(uint8_t* smem, const uint16_t* __restrict__ w) {
+  const uint4* src = reinterpret_cast<const uint4*>(w);
+  uint4* dst = reinterpret_cast<uint4*>(smem);
+  for (int i = threadIdx.x; i < kWEnd / 16; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
 struct Ctl {
@@ -247,6 +256,16 @@ __device__ __forceinline__ void publish() {
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
+}
+
+// publish() that also agrees on `ok` across the block (false if any thread's
+// bounded wait ran out).
+__device__ __forceinline__ bool publish_and(bool ok) {
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  const bool all = __syncthreads_and(ok ? 1 : 0) != 0;
+  umma::fence_after_sync();
+  return all;
 }
 
 // Reads `n` (16 or 64) fp32 columns [col, col+n) of this thread's TMEM lane:
@@ -368,9 +387,15 @@ __device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
   return j;
 }
 
-// Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set; a
-// task's CTAs stride over its 128-query tiles.
+// Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set.
+// A CTA of 128 threads keeps two 128-query tiles in flight, each with its own
+// TMEM accumulator (columns 64u..64u+63), its own activation tiles and its own
+// mbarrier: while the tensor core runs one tile's layer, the threads unpack
+// the other tile's previous layer (TMEM load, ReLU, bf16 pack into the next
+// operand tile), so the MMA latency hides behind the epilogue work.  Thread r
+// owns row r of both tiles.  A task's CTAs stride over its tile pairs.
 __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
+  using namespace mlp;
   const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
   int n = tk.n_max;
   if (tk.n_dev) n = min(*tk.n_dev, n);
@@ -378,40 +403,94 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTa
   const int cb = blockIdx.x - tk.cta0;
   if (cb >= tiles) return;   // nothing for this CTA (before any TMEM allocation)
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   const int t = threadIdx.x, warp = t >> 5;
-  if (warp == 0) umma::tmem_alloc(&tmem_base, 64);
-  if (t == 0) umma::mbar_init(&mbar, 1);
-  mlp::load_weights(smem, tk.wb);
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
+  if (t == 0) { umma::mbar_init(&mbar[0], 1); umma::mbar_init(&mbar[1], 1); }
+  load_weights(smem, tk.wb);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
-  mlp::Ctl c{&mbar, 0u, true};
-  for (int tile = cb; tile < tiles && c.ok; tile += tk.ctas) {
-    const int idx = tile * 128 + t;
-    float q[9];
-    if (idx < n) {
+  const uint32_t s0 = umma::smem_u32(smem);
+  // per tile: X (input, 80 columns; later the layer-2 input, 64 columns) and Y
+  const int X[2] = {kIX0, kIX1}, Y[2] = {kIY0, kIY1};
+  uint32_t phase[2] = {0u, 0u};
+  bool ok = true;
+  const int stride = 2 * tk.ctas;          // a CTA's pairs: tiles (pt, pt + ctas), pt = cb + k stride
+  float q[2][9];
+  auto fetch = [&](int pair_tile) {
 #pragma unroll
-      for (int j = 0; j < 9; j++) q[j] = __ldg(tk.q9 + (size_t)idx * 9 + j);
+    for (int u = 0; u < 2; u++) {
+      const int idx = (pair_tile + u * tk.ctas) * 128 + t;
+      if (idx < n) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) q[u][j] = __ldg(tk.q9 + (size_t)idx * 9 + j);
+      }
     }
-    mlp::stage_query(smem + mlp::kIA0, t, q, idx < n, tk.extent);
-    mlp::publish();
-    float o[mlp::kOutPad];
-    uint64_t mask[3];
-    // activations ping-pong between the two buffers (A1 = IA1, A2 = IA0, A3 = IA1)
-    mlp::forward_tile<1, false>(smem, tbase, c, mlp::kIA0, mlp::kIA1, mlp::kIA0, mlp::kIA1, 0, o, mask);
-    if (c.ok && idx < n)
-      for (int j = 0; j < mlp::kOut; j++) tk.out3[(size_t)idx * 3 + j] = o[j];
-    umma::fence_before_sync();
-    __syncthreads();
+  };
+  // tensor-core work of layer l of tile u (thread 0), completion on mbar[u]
+  auto issue = [&](int u, int l) {
+    if (t != 0) return;
+    const uint32_t acc = tbase + 64u * (uint32_t)u;
+    if (l == 0) issue_fwd(acc, s0 + X[u], s0 + kWf0, kIn, kHid, false);
+    else if (l == 1) issue_fwd(acc, s0 + Y[u], s0 + kWf1, kHid, kHid, false);
+    else if (l == 2) issue_fwd(acc, s0 + X[u], s0 + kWf2, kHid, kHid, false);
+    else issue_fwd(acc, s0 + Y[u], s0 + kWf3, kHid, kOutPad, false);
+    umma::commit(&mbar[u]);
+  };
+  auto wait = [&](int u) {
+    ok = umma::mbar_wait(&mbar[u], phase[u], kMbarSpin) && ok;
+    phase[u] ^= 1u;
     umma::fence_after_sync();
+  };
+  fetch(cb);
+  for (int pt = cb; pt < tiles && ok; pt += stride) {
+    int idx[2];
+    float qq[2][9];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      idx[u] = (pt + u * tk.ctas) * 128 + t;
+#pragma unroll
+      for (int j = 0; j < 9; j++) qq[u][j] = q[u][j];
+    }
+    // stage tile 0 and start its first layer; stage tile 1 while it runs
+    stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
+    ok = publish_and(ok);
+    if (ok) issue(0, 0);
+    stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
+    ok = publish_and(ok);
+    if (ok) issue(1, 0);
+    fetch(pt + stride);                    // the next pair's queries, in flight during this pair
+#pragma unroll 1
+    for (int l = 0; l < 4 && ok; l++) {
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        wait(u);
+        if (l < 3) {
+          float h[kHid];
+          tmem_row<kHid>(tbase, 64u * (uint32_t)u, h);
+#pragma unroll
+          for (int j = 0; j < kHid; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
+          store_row(smem + ((l & 1) ? X[u] : Y[u]), t, kHid, h);
+          ok = publish_and(ok);
+          if (ok) issue(u, l + 1);
+        } else {
+          float o[kOutPad];
+          tmem_row<kOutPad>(tbase, 64u * (uint32_t)u, o);
+          if (ok && idx[u] < n)
+            for (int j = 0; j < kOut; j++) tk.out3[(size_t)idx[u] * 3 + j] = o[j];
+        }
+      }
+    }
+    // every thread has read this pair's last TMEM rows before the next pair's MMAs
+    ok = publish_and(ok);
   }
-  if (!c.ok && t == 0) atomicExch(tk.err, 1);
+  if (!ok && t == 0) atomicExch(tk.err, 1);
   umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_free(tbase, 64);
+  if (warp == 0) umma::tmem_free(tbase, 128);
 }
 
 // One gradient pass: per-CTA partial dW (sum over the CTA's samples) of the
@@ -561,10 +640,26 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const __grid_constant__ Mlp
   if (warp == 0) umma::tmem_free(tbase, 512);
 }
 
-// grad[i] = sum over the task's CTAs of partial[cta][i] / n (fixed order:
-// deterministic); blockIdx.y = task.  Thread 0 advances the task's Adam step
-// counter when the step has samples.
+// grad[i] = sum over the task's CTAs of partial[cta][i] / n, in two stages
+// with a fixed order (deterministic): k_mlp_reduce sums each run of
+// kReduceRows partial rows into the run's first row (blockIdx.y = run,
+// blockIdx.z = task); k_mlp_reduce_final sums the runs' first rows in order
+// and scales by 1/n (blockIdx.y = task).  Thread 0 of the final stage
+// advances the task's Adam step counter when the step has samples.
+constexpr int kReduceRows = 16;
+
 __global__ void k_mlp_reduce(const __grid_constant__ MlpTaskSet ts) {
+  const MlpTask& tk = ts.t[blockIdx.z];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c0 = blockIdx.y * kReduceRows;
+  if (i >= mlp::kParams || c0 >= tk.ctas) return;
+  const int c1 = min(c0 + kReduceRows, tk.ctas);
+  float s = 0.0f;
+  for (int c = c0; c < c1; c++) s += tk.partial[(size_t)c * mlp::kParams + i];
+  tk.partial[(size_t)c0 * mlp::kParams + i] = s;
+}
+
+__global__ void k_mlp_reduce_final(const __grid_constant__ MlpTaskSet ts) {
   const MlpTask& tk = ts.t[blockIdx.y];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= mlp::kParams) return;
@@ -574,7 +669,7 @@ __global__ void k_mlp_reduce(const __grid_constant__ MlpTaskSet ts) {
   const float inv_n = n > 0 ? 1.0f / (float)n : 0.0f;
   if (i == 0 && tk.step && n > 0) *tk.step += 1;
   float s = 0.0f;
-  for (int c = 0; c < tk.ctas; c++) s += tk.partial[(size_t)c * mlp::kParams + i];
+  for (int c = 0; c < tk.ctas; c += kReduceRows) s += tk.partial[(size_t)c * mlp::kParams + i];
   tk.grad[i] = s * inv_n;
 }
 
@@ -588,7 +683,11 @@ __global__ void k_mlp_adam(const __grid_constant__ MlpTaskSet ts, float b1, floa
   if (tk.n_dev && *tk.n_dev <= 0) return;
   float* __restrict__ wm = tk.wm;
   uint16_t* __restrict__ wb = tk.wbw;
-  if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) { wm[i] = 0.0f; wb[i] = 0; return; }
+  if (i >= mlp::kOff3 && ((i - mlp::kOff3) % mlp::kOutPad) >= mlp::kOut) {
+    wm[i] = 0.0f;
+    wb[mlp::image_index(i)] = 0;
+    return;
+  }
   const float t = (float)*tk.step;
   const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
   const float g = tk.grad[i];
@@ -599,12 +698,12 @@ __global__ void k_mlp_adam(const __grid_constant__ MlpTaskSet ts, float b1, floa
   const float mh = mi / bc1, vh = vi / bc2;
   const float w = wm[i] - tk.lr * mh / (sqrtf(vh) + eps);
   wm[i] = w;
-  wb[i] = mlp::f2bf(w);
+  wb[mlp::image_index(i)] = mlp::f2bf(w);
 }
 
 __global__ void k_mlp_to_bf16(const float* __restrict__ wm, uint16_t* __restrict__ wb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < mlp::kParams) wb[i] = mlp::f2bf(wm[i]);
+  if (i < mlp::kParams) wb[mlp::image_index(i)] = mlp::f2bf(wm[i]);
 }
 
 
@@ -658,7 +757,7 @@ cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = assign_ctas(ts, sm_count_mlp() * 3, 128);   // 3 x 72 KB of shared memory per SM
+  const int grid = assign_ctas(ts, sm_count_mlp() * 2, 256);   // 2 x 100 KB of shared memory per SM
   k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(ts);
   return cudaGetLastError();
 }
@@ -676,7 +775,11 @@ cudaError_t mlp_gradient_tasks(MlpTaskSet& ts, cudaStream_t st) {
   k_mlp_grad<<<grid, 256, mlp::kTrainSmem, st>>>(ts);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_mlp_reduce<<<dim3((mlp::kParams + 255) / 256, ts.n), 256, 0, st>>>(ts);
+  const int runs = (sm_count_mlp() + kReduceRows - 1) / kReduceRows;   // partial rows per network: one per CTA
+  k_mlp_reduce<<<dim3((mlp::kParams + 255) / 256, runs, ts.n), 256, 0, st>>>(ts);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_mlp_reduce_final<<<dim3((mlp::kParams + 255) / 256, ts.n), 256, 0, st>>>(ts);
   return cudaGetLastError();
 }
 

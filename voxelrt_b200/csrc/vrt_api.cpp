@@ -1947,6 +1947,161 @@ int vrt_session_set_cache(VrtSession* s, const VrtCacheConfig* cfg_in) {
   return VRT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Session checkpoint: everything the next frames depend on -- the scene's
+// voxels (bricks, masks and the occupancy bitmap are rebuilt from them), both
+// history / G-buffer parities and the frame parity, the radiance cache's
+// network (fp32 masters, Adam moments, step), the ReSTIR history (reservoirs
+// and duplication map) and the HDR reference accumulation.  A session
+// restored into a fresh session of the same size renders the same frames
+// bit for bit.  The layout is a header followed by the sections in order.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+struct CkptHeader {
+  char magic[8];              // "VRTCKPT1"
+  uint32_t version, flags;    // flags: 1 cache network, 2 ReSTIR history, 4 HDR accumulation
+  int32_t W, H, N, acc_f32;
+  uint64_t frame_counter;
+  int32_t last_parity, have_frame, last_denoise, hdr_count;
+  VrtCacheConfig cache_cfg;
+  uint64_t restir_bytes, total_bytes;
+};
+constexpr uint32_t kCkptCache = 1u, kCkptRestir = 2u, kCkptHdr = 4u;
+
+uint64_t ckpt_size(const VrtSession* s, uint32_t flags) {
+  const uint64_t P = px(s), N = (uint64_t)s->scene->dev.N;
+  uint64_t b = sizeof(CkptHeader) + N * N * N * 4 + 2 * P * acc_bpp(s) + 2 * P * 16;
+  if (flags & kCkptCache) b += 3ull * (uint64_t)s->mlp->P * 4 + 4;
+  if (flags & kCkptRestir) b += s->restir_bytes;
+  if (flags & kCkptHdr) b += P * 3 * 8;
+  return b;
+}
+
+uint32_t ckpt_flags(const VrtSession* s) {
+  return (s->mlp ? kCkptCache : 0u) | (s->restir_mem ? kCkptRestir : 0u) | (s->hdr_acc ? kCkptHdr : 0u);
+}
+}  // namespace
+
+extern "C" {
+
+int vrt_session_checkpoint_size(VrtSession* s, uint64_t* bytes) {
+  if (!s || !bytes) return fail(VRT_ERR_INVALID, "NULL argument");
+  *bytes = ckpt_size(s, ckpt_flags(s));
+  return VRT_OK;
+}
+
+int vrt_session_checkpoint(VrtSession* s, void* host, uint64_t bytes) {
+  if (!s || !host) return fail(VRT_ERR_INVALID, "NULL argument");
+  const uint32_t flags = ckpt_flags(s);
+  const uint64_t need = ckpt_size(s, flags);
+  if (bytes < need) return fail(VRT_ERR_INVALID, "checkpoint buffer %llu bytes < %llu needed",
+                                (unsigned long long)bytes, (unsigned long long)need);
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  CkptHeader h;
+  std::memset(&h, 0, sizeof h);
+  std::memcpy(h.magic, "VRTCKPT1", 8);
+  h.version = 1;
+  h.flags = flags;
+  h.W = s->W; h.H = s->H; h.N = s->scene->dev.N; h.acc_f32 = s->acc_f32 ? 1 : 0;
+  h.frame_counter = s->frame_counter;
+  h.last_parity = s->last_parity; h.have_frame = s->have_frame ? 1 : 0; h.last_denoise = s->last_denoise ? 1 : 0;
+  h.hdr_count = (int32_t)s->hdr_count;
+  h.cache_cfg = s->cache_cfg;
+  h.cache_cfg.enabled = s->cache_on ? 1 : 0;
+  h.restir_bytes = (flags & kCkptRestir) ? s->restir_bytes : 0;
+  h.total_bytes = need;
+  char* o = (char*)host;
+  std::memcpy(o, &h, sizeof h);
+  o += sizeof h;
+  const uint64_t P = px(s), N = (uint64_t)h.N;
+  auto d2h = [&](const void* src, uint64_t n) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(o, src, n, cudaMemcpyDeviceToHost, st);
+    o += n;
+    return e;
+  };
+  CUDA_TRY(d2h(s->scene->dev.vox, N * N * N * 4));
+  for (int i = 0; i < 2; i++) CUDA_TRY(d2h(s->accum[i], P * acc_bpp(s)));
+  for (int i = 0; i < 2; i++) CUDA_TRY(d2h(s->gbuf[i], P * 16));
+  if (flags & kCkptCache) {
+    const uint64_t np = (uint64_t)s->mlp->P * 4;
+    CUDA_TRY(d2h(s->mlp->wm, np));
+    CUDA_TRY(d2h(s->mlp->m, np));
+    CUDA_TRY(d2h(s->mlp->v, np));
+    CUDA_TRY(d2h(s->mlp->step(), 4));
+  }
+  if (flags & kCkptRestir) CUDA_TRY(d2h(s->restir_mem, s->restir_bytes));
+  if (flags & kCkptHdr) CUDA_TRY(d2h(s->hdr_acc, P * 3 * 8));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return VRT_OK;
+}
+
+int vrt_session_restore(VrtSession* s, const void* host, uint64_t bytes) {
+  if (!s || !host) return fail(VRT_ERR_INVALID, "NULL argument");
+  if (bytes < sizeof(CkptHeader)) return fail(VRT_ERR_INVALID, "checkpoint shorter than its header");
+  CkptHeader h;
+  std::memcpy(&h, host, sizeof h);
+  if (std::memcmp(h.magic, "VRTCKPT1", 8) != 0 || h.version != 1)
+    return fail(VRT_ERR_INVALID, "not a session checkpoint (bad magic or version)");
+  if (h.W != s->W || h.H != s->H || h.N != s->scene->dev.N || h.acc_f32 != (s->acc_f32 ? 1 : 0))
+    return fail(VRT_ERR_INVALID, "checkpoint of a %dx%d session on a %d^3 scene (history %s) does not fit this "
+                "session", h.W, h.H, h.N, h.acc_f32 ? "rgba32f" : "rgba16f");
+  if (h.total_bytes != bytes) return fail(VRT_ERR_INVALID, "checkpoint size %llu != its header's %llu",
+                                         (unsigned long long)bytes, (unsigned long long)h.total_bytes);
+  if (int r = set_dev(s->ctx)) return r;
+  cudaStream_t st = s->ctx->stream;
+  // state the sections need on this side before anything is copied
+  if ((h.flags & kCkptCache) && !s->mlp) {
+    VrtCacheConfig cfg = h.cache_cfg;
+    cfg.enabled = 1;
+    if (int r = vrt_session_set_cache(s, &cfg)) return r;
+  }
+  if ((h.flags & kCkptRestir) && (!s->restir_mem || s->restir_bytes != h.restir_bytes))
+    return fail(VRT_ERR_STATE, "restore the ReSTIR history into a session that rendered a ReSTIR frame");
+  if ((h.flags & kCkptHdr) && !s->hdr_acc) {
+    if (int r = vrt_hdr_accum_reset(s)) return r;
+  }
+  if (ckpt_size(s, h.flags) != bytes) return fail(VRT_ERR_INVALID, "checkpoint sections do not match this session");
+  const char* o = (const char*)host + sizeof h;
+  const uint64_t P = px(s), N = (uint64_t)h.N;
+  auto h2d = [&](void* dst, uint64_t n) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(dst, o, n, cudaMemcpyHostToDevice, st);
+    o += n;
+    return e;
+  };
+  CUDA_TRY(h2d(s->scene->dev.vox, N * N * N * 4));
+  const int BG = s->scene->dev.BG;
+  CUDA_TRY(launch_build_bricks(s->scene->dev, 0, 0, 0, BG - 1, BG - 1, BG - 1, st));
+  CUDA_TRY(launch_build_bits(s->scene->dev, st));
+  s->scene->lights_built = false;
+  for (int i = 0; i < 2; i++) CUDA_TRY(h2d(s->accum[i], P * acc_bpp(s)));
+  for (int i = 0; i < 2; i++) CUDA_TRY(h2d(s->gbuf[i], P * 16));
+  if (h.flags & kCkptCache) {
+    VrtMlp* m = s->mlp;
+    const uint64_t np = (uint64_t)m->P * 4;
+    CUDA_TRY(h2d(m->wm, np));
+    CUDA_TRY(h2d(m->m, np));
+    CUDA_TRY(h2d(m->v, np));
+    CUDA_TRY(h2d(m->step(), 4));
+    CUDA_TRY(mlp_to_bf16(m->wm, m->wb, st));
+    s->cache_cfg = h.cache_cfg;
+    s->cache_cfg.enabled = 1;
+    s->cache_on = h.cache_cfg.enabled != 0;
+    s->cache_version++;
+  }
+  if (h.flags & kCkptRestir) CUDA_TRY(h2d(s->restir_mem, s->restir_bytes));
+  if (h.flags & kCkptHdr) CUDA_TRY(h2d(s->hdr_acc, P * 3 * 8));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  s->frame_counter = h.frame_counter;
+  s->last_parity = h.last_parity;
+  s->have_frame = h.have_frame != 0;
+  s->last_denoise = h.last_denoise != 0;
+  s->hdr_count = (uint32_t)h.hdr_count;
+  return VRT_OK;
+}
+
 int vrt_session_read_cache_samples(VrtSession* s, float* q9, float* y3, int cap, int* count) {
   if (!s || !count || cap < 0 || (cap > 0 && (!q9 || !y3))) return fail(VRT_ERR_INVALID, "bad argument");
   if (!s->cache_mem) return fail(VRT_ERR_STATE, "the cache was never enabled on this session");

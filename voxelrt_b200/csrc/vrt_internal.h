@@ -145,7 +145,7 @@ cudaError_t mlp_encode(const float* q9, int n, float extent, uint16_t* out, cuda
 // kMaxMlpTasks networks (the sessions of a batch); the task table travels as
 // a kernel parameter, so a captured graph needs no table upload.
 struct MlpTask {
-  const uint16_t* wb;       // bf16 weights
+  const uint16_t* wb;       // bf16 weights as the kernels' shared-memory image (k_mlp.cu)
   const float* q9;          // inputs [n][9]: position (metres), normal, albedo
   const float* y3;          // training targets [n][3]
   float* out3;              // inference output [n][3]

@@ -1013,7 +1013,7 @@ cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch* 
         if (k < cls[c0 + q].train_steps) tr.t[tr.n++] = mlp_task_of(cls[c0 + q], k);
       if ((e = mlp_gradient_tasks(tr, st)) != cudaSuccess) return e;
       if ((e = mlp_adam_tasks(tr, st)) != cudaSuccess) return e;
-      nl += 3;
+      nl += 4;   // gradient, the reduction's two stages, Adam
     }
   }
   if (launches) *launches += nl;
