@@ -110,6 +110,8 @@ typedef struct VrtTuning {
                                  warp bookkeeping, min blocks per SM) =
                                  0: (8,5) default, 1: (6,5), 2: (6,4), 3: (4,4),
                                  4: (2,1), 5: (1,1)                              */
+  int atrous_tile_rows;       /* a-trous output tile rows: 0 = 16 at steps 1-2
+                                 and 8 at step 4 (default), 8 = 8 at every step  */
 } VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,

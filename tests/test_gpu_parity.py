@@ -360,3 +360,26 @@ def test_autotune_picks_a_candidate_and_keeps_results(ctx, vrt):
     s.frame(u)                                  # history was reset: same first frame again
     assert np.array_equal(s.radiance_f32().view(np.uint32), before.view(np.uint32))
     s.close(); sc.close()
+
+
+def test_atrous_tile_shape_invariant(ctx, vrt):
+    """The autotuner's a-trous tile shapes (16/16/8 and 8/8/8 output rows per
+    tile) give the same denoised image bit for bit."""
+    W, H, n = 320, 180, 64
+    vox, spawn = vrt.generate_scene(1, n, 1)
+    sc = vrt.Scene(ctx, vox, n)
+    outs = []
+    for rows in (0, 8):
+        s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0)
+        s.set_tuning(0, 0, 0, 0, rows)
+        assert s.get_tuning()[4] == rows
+        prev = None
+        for f in range(3):
+            pose = vrt.camera_spline(spawn, f)
+            s.frame(vrt.make_uniforms(pose, prev, vrt.Lighting(), f, 2, 3, W, H))
+            prev = pose
+        outs.append((s.denoise(0).copy(), s.denoise(1).copy(), s.ldr().copy()))
+        s.close()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    sc.close()

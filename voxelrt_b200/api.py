@@ -312,21 +312,24 @@ class Session:
         self.scene = scene
 
     def set_tuning(self, refill_min: int = 0, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
-                   trace_variant: int = 0) -> None:
-        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant))
+                   trace_variant: int = 0, atrous_tile_rows: int = 0) -> None:
+        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant),
+                      int(atrous_tile_rows))
         check(lib.vrt_session_set_tuning(self.h, C.byref(t)))
 
     def autotune(self, u: VrtUniforms, frames: int = 3):
-        """Picks the fastest wavefront launch shape for frames like `u`; resets history."""
+        """Picks the fastest wavefront launch shape and a-trous tile shape for
+        frames like `u`; resets history."""
         t = VrtTuning()
         ms = C.c_float()
         check(lib.vrt_session_autotune(self.h, C.byref(u), int(frames), C.byref(t), C.byref(ms)))
-        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant), float(ms.value)
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant,
+                t.atrous_tile_rows), float(ms.value)
 
     def get_tuning(self) -> tuple:
         t = VrtTuning()
         check(lib.vrt_session_get_tuning(self.h, C.byref(t)))
-        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant)
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant, t.atrous_tile_rows)
 
     def set_cache(self, enabled: bool = True, train_bounces: int = 6, train_vertices: int = 3,
                   train_batch: int = 65536, train_steps: int = 1, learning_rate: float = 1e-2, seed: int = 1) -> None:

@@ -37,8 +37,8 @@ __host__ __device__ constexpr int tile_px(int step, int ty) { return (kTX + 4 * 
 __host__ __device__ constexpr int tile_rows(int step) { return step >= 4 ? 8 : 16; }
 // G-buffer tile + source tile (rgba16f or rgba32f as copied, expanded in place
 // to fp32 with its luminance); the steps are 1, 2, 4.
-__host__ __device__ constexpr int tile_smem(int step) {
-  return align128(tile_px(step, tile_rows(step)) * 16) + tile_px(step, tile_rows(step)) * 16;
+__host__ __device__ constexpr int tile_smem(int step, int ty) {
+  return align128(tile_px(step, ty) * 16) + tile_px(step, ty) * 16;
 }
 constexpr int kMaxTilePx = 1280;   // staged pixels of the largest tile (step 4, 8 rows: 1,152), rounded to 256
 static_assert(tile_px(1, 16) <= kMaxTilePx && tile_px(2, 16) <= kMaxTilePx && tile_px(4, 8) <= kMaxTilePx, "tile");
@@ -181,17 +181,17 @@ static bool map_h4(CUtensorMap* m, const void* base, int W, int H, int bw, int b
 }
 
 cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
-                                 unsigned long long* err, cudaStream_t st) {
+                                 unsigned long long* err, cudaStream_t st, int rows) {
   const bool aligned = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(gbuf)) & 15u) == 0u;
   const bool ok = encode_fn() && aligned && (src_f32 || W % 2 == 0) && step >= 1 && step <= 4 && W > 0 && H > 0;
   if (!ok) return launch_atrous(W, H, src, src_f32, gbuf, dst, step, st);
-  const int ty = tile_rows(step);
+  const int ty = rows == 8 ? 8 : tile_rows(step);   // rows: 0 = 16 at steps 1-2 and 8 at step 4, 8 = 8 everywhere
   const int hx = 2 * step, bw = kTX + 2 * hx, bh = ty + 2 * hx;
   CUtensorMap tg, ts;
   const bool enc = map_f32x4(&tg, gbuf, W, H, bw, bh) &&
                    (src_f32 ? map_f32x4(&ts, src, W, H, bw, bh) : map_h4(&ts, src, W, H, bw, bh));
   if (!enc) return launch_atrous(W, H, src, src_f32, gbuf, dst, step, st);
-  const int smem = tile_smem(step);
+  const int smem = tile_smem(step, ty);
   dim3 grid((W + kTX - 1) / kTX, (H + ty - 1) / ty);
   auto run = [&](auto* fn) -> cudaError_t {
     cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -492,18 +492,21 @@ int vrt_session_get_tuning(VrtSession* s, VrtTuning* t) {
   t->trace_blocks_per_sm = s->tune.trace_blocks_per_sm;
   t->shade_blocks_per_sm = s->tune.shade_blocks_per_sm;
   t->trace_variant = s->tune.trace_variant;
+  t->atrous_tile_rows = s->tune.atrous_rows;
   return VRT_OK;
 }
 
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5 ||
+      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8))
     return fail(VRT_ERR_INVALID, "tuning out of range");
   s->tune.refill_min = t->refill_min ? t->refill_min : 8;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   s->tune.trace_variant = t->trace_variant;
+  s->tune.atrous_rows = t->atrous_tile_rows;
   return VRT_OK;
 }
 
@@ -548,11 +551,35 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
         if (med < win_ms) { win_ms = med; win = s->tune; }
       }
   s->tune = win;
+  // the a-trous tile shape: the three iterations of a frame timed per shape
+  if (u->params0[2] & 2u) {
+    if (int r = vrt_pass_temporal(s, u)) { s->tune = keep; return r; }
+    float best_atrous = 1e30f;
+    int best_rows = win.atrous_rows;
+    for (int rows : {0, 8}) {
+      s->tune.atrous_rows = rows;
+      for (int it = 0; it < 3; it++)
+        if (int r = vrt_pass_atrous(s, u, it)) { s->tune = keep; return r; }   // warm-up
+      for (int f = 0; f < frames; f++) {
+        CUDA_TRY(cudaEventRecord(s->ev[0], st));
+        for (int it = 0; it < 3; it++)
+          if (int r = vrt_pass_atrous(s, u, it)) { s->tune = keep; return r; }
+        CUDA_TRY(cudaEventRecord(s->ev[1], st));
+        CUDA_TRY(cudaEventSynchronize(s->ev[1]));
+        CUDA_TRY(cudaEventElapsedTime(&ms[(size_t)f], s->ev[0], s->ev[1]));
+      }
+      std::sort(ms.begin(), ms.end());
+      if (ms[(size_t)frames / 2] < best_atrous) { best_atrous = ms[(size_t)frames / 2]; best_rows = rows; }
+    }
+    s->tune.atrous_rows = best_rows;
+    win = s->tune;
+  }
   if (best) {
     best->refill_min = win.refill_min;
     best->trace_blocks_per_sm = win.trace_blocks_per_sm;
     best->shade_blocks_per_sm = win.shade_blocks_per_sm;
     best->trace_variant = win.trace_variant;
+    best->atrous_tile_rows = win.atrous_rows;
   }
   if (best_ms) *best_ms = win_ms;
   return vrt_session_reset(s);
@@ -752,7 +779,7 @@ int vrt_pass_atrous(VrtSession* s, const VrtUniforms* u, int it) {
   const bool src_f32 = it == 0 && s->acc_f32;
   void* dst = it == 1 ? s->den[1] : s->den[0];
   CUDA_TRY(launch_atrous_staged(s->W, s->H, src, src_f32, s->gbuf[p], dst, 1 << it, s->stats + kStatError,
-                                s->ctx->stream));
+                                s->ctx->stream, s->tune.atrous_rows));
   s->launches++;
   return VRT_OK;
 }
@@ -1274,6 +1301,7 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
     best->trace_blocks_per_sm = win.trace_blocks_per_sm;
     best->shade_blocks_per_sm = win.shade_blocks_per_sm;
     best->trace_variant = win.trace_variant;
+    best->atrous_tile_rows = 0;   // batch frames run the unstaged a-trous kernel over all jobs
   }
   if (best_ms) *best_ms = win_ms;
   for (VrtSession* s : b->sessions)

@@ -82,6 +82,7 @@ struct WavefrontTuning {
   int shade_blocks_per_sm = 16;
   int trace_variant = 0;        // (DDA iterations per warp-bookkeeping pass, min blocks/SM):
                                 // 0: (8, 5)  1: (6, 5)  2: (6, 4)  3: (4, 4)  4: (2, 1)  5: (1, 1)
+  int atrous_rows = 0;          // a-trous output tile rows: 0 = 16 at steps 1-2 and 8 at step 4, 8 = 8 at all steps
 };
 
 // Host mirror of the device job table entry (JobDev in wavefront_core.cuh):
@@ -234,7 +235,7 @@ cudaError_t launch_temporal(const VrtUniforms& u, int W, int H, const void* rad1
 // launch_atrous when the buffers do not meet the copy constraints); err
 // (may be null) is set when a bounded wait for the copies ran out.
 cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
-                                 unsigned long long* err, cudaStream_t st);
+                                 unsigned long long* err, cudaStream_t st, int rows = 0);
 cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
                           cudaStream_t st);
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
