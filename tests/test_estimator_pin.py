@@ -15,9 +15,11 @@ camera, RNG streams and capture) and compared with those records:
     maxChannelMeanRelativeDelta), for the reference capture and the test
     capture of each configuration;
   * the HDR MSE between this library's test and reference captures within
-    25% of the MSE the reference recorded between its own two captures.
-The reference renders the same per-pixel RNG streams, so the channel means
-agree far more closely than the 1% gate: the achieved deltas are printed.
+    5% (plain path) or 25% (ReSTIR) of the MSE the reference recorded between
+    its own two captures.
+The reference renders the same per-pixel RNG streams, so the plain path's
+channel means agree far more closely than the 1% gate (within 0.5% is
+asserted); the achieved deltas are printed.
 """
 import json
 from pathlib import Path
@@ -98,7 +100,9 @@ def test_base_captures_match_reference_statistics(vrt, world, scenario):
           f"PSNR {m['hdrPsnrPeak']:.2f} vs {row['hdrPsnrPeak']:.2f} dB")
     assert d_ref.max() <= MEAN_TOL, d_ref
     assert d_test.max() <= MEAN_TOL, d_test
-    assert abs(m["hdrMse"] / row["hdrMse"] - 1.0) <= 0.25, (m["hdrMse"], row["hdrMse"])
+    # the same per-pixel RNG streams: far inside the gate (measured 0.06-0.15%)
+    assert max(d_ref.max(), d_test.max()) <= 0.005, (d_ref, d_test)
+    assert abs(m["hdrMse"] / row["hdrMse"] - 1.0) <= 0.05, (m["hdrMse"], row["hdrMse"])
 
 
 def test_ours_unbiased_capture_matches_reference_statistics(vrt, world):

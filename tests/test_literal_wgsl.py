@@ -118,7 +118,9 @@ def test_kernels_within_spec_of_literal_wgsl(vrt, orc, kind, n, seed, W, H, acc_
     s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, accum_f32=acc_f32, keep_radiance_f32=True)
 
     # the session keeps only dA and dB (the chain accum -> dA -> dB -> dA):
-    # the per-pass entry points let dA be read after the first iteration too
+    # the per-pass entry points let dA be read after the first iteration too.
+    # History and G-buffer are read after vrt_end_frame, which makes this
+    # frame's parity the one the read calls return.
     def kernel_side_passes(vox, b, m, n_, u, ub, acc_prev, gprev):
         s.pathtrace(u)
         s.temporal(u)
@@ -127,10 +129,9 @@ def test_kernels_within_spec_of_literal_wgsl(vrt, orc, kind, n, seed, W, H, acc_
         s.atrous(u, 1)
         s.atrous(u, 2)
         s.present(u)
-        out = {"rad32": s.radiance_f32(), "rad16": s.radiance(), "gbuf": s.gbuffer(), "alb8": s.albedo(),
-               "accum": s.accum(), "den": [d0, s.denoise(1), s.denoise(0)], "ldr": s.ldr()}
         s.end_frame()
-        return out
+        return {"rad32": s.radiance_f32(), "rad16": s.radiance(), "gbuf": s.gbuffer(), "alb8": s.albedo(),
+                "accum": s.accum(), "den": [d0, s.denoise(1), s.denoise(0)], "ldr": s.ldr()}
 
     diffs = _frames(vrt, orc, kind, n, seed, W, H, 3, acc_f32, kernel_side_passes)
     print(f"path differences / worst same-path radiance error per frame: {diffs}")

@@ -28,6 +28,17 @@ def _track(kind: str, obj) -> None:
     _LIVE[kind].add(obj)
 
 
+def _ctx_alive(obj) -> bool:
+    """False once the object's context was destroyed: destroying the object
+    would go through the freed context, so its device memory is left to the
+    process exit instead.  The garbage collector can finalize a context
+    before the objects that refer to it when both sit in one unreachable
+    cycle (a failed call's traceback, for one), after it has cleared the weak
+    references through which the context would have closed them first."""
+    c = getattr(obj, "ctx", None)
+    return c is None or bool(getattr(c, "h", None))
+
+
 @atexit.register
 def _close_all() -> None:
     for kind in ("server", "batch", "cache", "session", "scene", "context"):
@@ -266,7 +277,8 @@ class Scene:
 
     def close(self) -> None:
         if self.h:
-            lib.vrt_scene_destroy(self.h)
+            if _ctx_alive(self):
+                lib.vrt_scene_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -464,7 +476,8 @@ class Session:
 
     def close(self) -> None:
         if self.h:
-            lib.vrt_session_destroy(self.h)
+            if _ctx_alive(self):
+                lib.vrt_session_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -510,7 +523,8 @@ class Batch:
 
     def close(self) -> None:
         if self.h:
-            lib.vrt_batch_destroy(self.h)
+            if _ctx_alive(self):
+                lib.vrt_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -600,7 +614,8 @@ class Server:
 
     def close(self) -> None:
         if self.h:
-            lib.vrt_server_destroy(self.h)
+            if _ctx_alive(self):
+                lib.vrt_server_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -679,7 +694,8 @@ class RadianceCache:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            check(lib.vrt_mlp_destroy(self.h))
+            if _ctx_alive(self):
+                check(lib.vrt_mlp_destroy(self.h))
             self.h = None
 
     def __del__(self):
