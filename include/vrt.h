@@ -523,7 +523,10 @@ int vrt_selftest_bounded_wait(unsigned int spins);
  * vrt_session_restore loads one into a session of the same size, history
  * format and scene size (the scene's bricks, masks and bitmap are rebuilt;
  * its lights are rebuilt on next use); the session then renders the same
- * frames the checkpointed one would, bit for bit.  Host buffers; the calls
+ * frames the checkpointed one would -- bit for bit without the radiance
+ * cache; with it the network comes back exactly, and later frames agree to
+ * the order in which a frame's training samples are gathered, which is not
+ * fixed in the original session either.  Host buffers; the calls
  * synchronize the context's stream.  VRT_ERR_INVALID for a buffer that is
  * not a checkpoint of a matching session. */
 int vrt_session_checkpoint_size(VrtSession* s, uint64_t* bytes);

@@ -619,9 +619,19 @@ __global__ void __launch_bounds__(256, 1) k_mlp_grad(const __grid_constant__ Mlp
       float row[kHid];
       if (l < 3) tmem_row<kHid>(tbase, twa[l], row);
       else tmem_row<kOutPad>(tbase, twa[l], row);
-      if (g == 0 && r < kin[l]) {
+      // both groups read the same TMEM lanes; group g stores half of the row's
+      // columns, 16 bytes at a time (row offsets are multiples of 4 floats)
+      if (r < kin[l]) {
+        const int half = (l < 3 ? kHid : kOutPad) / 2;   // a constant once the layer loop is unrolled
+        float4* dst = reinterpret_cast<float4*>(pc + off[l] + r * nout[l] + g * half);
 #pragma unroll
-        for (int j = 0; j < (l < 3 ? kHid : kOutPad); j++) pc[off[l] + r * nout[l] + j] = first ? 0.0f : row[j];
+        for (int j = 0; j < kHid / 2; j += 4) {
+          if (j < half) {
+            const float4 lo = make_float4(row[j], row[j + 1], row[j + 2], row[j + 3]);
+            const float4 hi = make_float4(row[half + j], row[half + j + 1], row[half + j + 2], row[half + j + 3]);
+            dst[j / 4] = first ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : (g ? hi : lo);
+          }
+        }
       }
     }
   }
