@@ -844,7 +844,7 @@ def served_summary(sc, cc):
     sp, m = cc["speed_1080p"]["plain_2bounce"], cc["matched_mse_64frame"]["plain_2bounce"]
     cost = (m["frame_ms_at_matched_mse"] / sp["frame_ms"]) if m.get("frame_ms_at_matched_mse") else None
     seq = f["plain_sequential"]["capacity"]["frames_per_s"]
-    cb = f["cache_batched"]["capacity"]["frames_per_s"]
+    cb = f["cache_hybrid"]["capacity"]["frames_per_s"]
     out = {"metric": "served frames/s (capacity, queue never empty) and p50/p99 latency under Poisson arrivals; "
                      "cache-assisted continuous batching vs the plain form (requests one after another, unbatched)",
            "sessions": sc["sessions"], "session_pixels": sc["session_pixels"],
@@ -853,8 +853,11 @@ def served_summary(sc, cc):
            "forms": {k: {"frames_per_s": v["capacity"]["frames_per_s"],
                          "latency_ms": {str(int(r["rate_rps"])): [r["latency_ms_p50"], r["latency_ms_p99"]]
                                         for r in v["poisson"]}} for k, v in f.items()},
-           "speedup_cache_batched_vs_plain_sequential": round(cb / seq, 3),
+           "served_form": f"cache_hybrid: continuous batching of views below {sc['solo_pixels']} pixels, larger "
+                          "views alone through their own frame path",
+           "speedup_cache_served_vs_plain_sequential": round(cb / seq, 3),
            "speedup_plain_batched_vs_plain_sequential": round(f["plain_batched"]["capacity"]["frames_per_s"] / seq, 3),
+           "speedup_plain_hybrid_vs_plain_sequential": round(f["plain_hybrid"]["capacity"]["frames_per_s"] / seq, 3),
            "plain_cost_factor_at_matched_mse": round(cost, 3) if cost else None,
            "speedup_at_matched_mse": round(cb / seq * cost, 3) if cost else None,
            "latency_note": "latency_ms: rate (req/s) -> [p50, p99]",
@@ -1186,13 +1189,15 @@ def capacity(server, n_sessions, make_request, rng, n_req):
 
 
 def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320):
-    """The serving mix (32 sessions, edits between frames) served three ways
+    """The serving mix (32 sessions, edits between frames) served five ways
     over the same device-resident sessions: `plain_sequential`, the plain
     form -- requests one after another through each session's own frame path,
-    unbatched; `plain_batched` -- continuous batching; `cache_batched` --
-    continuous batching with each session's radiance cache (trained on 32
-    frames per session first).  Per form: capacity (the queue never empty)
-    and p50/p99 latency under Poisson arrivals at each rate."""
+    unbatched; `plain_batched` -- continuous batching of every request;
+    `plain_hybrid` -- continuous batching of views below 720p, larger views
+    alone; `cache_sequential` and `cache_hybrid` -- the same with each
+    session's radiance cache (trained on 32 frames per session first).  Per
+    form: capacity (the queue never empty) and p50/p99 latency under Poisson
+    arrivals at each rate."""
     import numpy as np
     import torch
 
@@ -1215,9 +1220,11 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
             server.drain()
 
     out = {}
-    for form in ("plain_sequential", "plain_batched", "cache_batched"):
-        server.set_sequential(form == "plain_sequential")
-        if form == "cache_batched":
+    solo = 1280 * 720      # views of 720p and up fill the GPU alone; smaller ones are batched
+    for form in ("plain_sequential", "plain_batched", "plain_hybrid", "cache_sequential", "cache_hybrid"):
+        server.set_sequential(form.endswith("sequential"))
+        server.set_solo_pixels(solo if form.endswith("hybrid") else 0)
+        if form == "cache_sequential":
             for k, s in enumerate(sessions):
                 s.set_cache(**dict(CACHE_CFG, seed=k + 1))
             warm(32)
@@ -1225,6 +1232,7 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
             warm(1)
         out[form] = {"capacity": capacity(server, len(sessions), make_request, rng, n_sat),
                      "poisson": sweep(a2, server, sessions, make_request, rng)}
+    out["solo_pixels"] = solo
     px = sum(w * h for _, w, h in meta)
     server.close()
     for s_ in sessions:
@@ -1232,7 +1240,8 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
     for sc in scenes:
         sc.close()
     ctx.close()
-    return {"sessions": len(sessions), "session_pixels": px, "forms": out}
+    solo = out.pop("solo_pixels")
+    return {"sessions": len(sessions), "session_pixels": px, "forms": out, "solo_pixels": solo}
 
 
 def churn_line(args, local, slots=32, close_p=0.02):

@@ -398,6 +398,12 @@ int vrt_server_sessions(VrtServer* sv, int* open, int* waiting);
  * the unbatched form the batched server is measured against.  Every session
  * needs its own path scratch (not VRT_PATH_BATCH_ONLY).  Only while idle. */
 int vrt_server_set_sequential(VrtServer* sv, int on);
+/* Batched mode with large sessions apart: a request of a session of at least
+ * `pixels` pixels that has its own path scratch renders alone through its
+ * frame path (a batch gains nothing from a view that fills the GPU by
+ * itself); smaller sessions are batched together.  0 (default): every
+ * request is batched. */
+int vrt_server_set_solo_pixels(VrtServer* sv, long long pixels);
 
 /* ---- scene lights -------------------------------------------------------- */
 /* The emissive-face light list, its power alias table and the per-brick

@@ -213,3 +213,41 @@ def test_sequential_server_equals_alone(ctx, vrt):
         s.close()
     for sc in srv_sc + ref_sc:
         sc.close()
+
+
+def test_hybrid_server_equals_alone(ctx, vrt):
+    """Large views alone through their own frame path, small ones batched
+    (vrt_server_set_solo_pixels): every request still renders what it renders
+    alone."""
+    vox, spawns, served, ref_sc, ref_s, srv_sc = [], [], [], [], [], []
+    for kind, n, sd, W, H, nb in SESSIONS:
+        v, sp = vrt.generate_scene(kind, n, sd)
+        spawns.append(sp)
+        sc = vrt.Scene(ctx, v, n)
+        srv_sc.append(sc)
+        served.append(vrt.Session(ctx, sc, W, H, firefly_clamp=10.0))
+        rsc = vrt.Scene(ctx, v, n)
+        ref_sc.append(rsc)
+        ref_s.append(vrt.Session(ctx, rsc, W, H, firefly_clamp=10.0))
+    reqs = _requests(vrt, spawns, 20, 21)
+    server = vrt.Server(ctx, served, max_in_flight=2)
+    server.set_solo_pixels(300 * 170)       # the 320x180 and 480x270 views render alone
+    outs = []
+    for i, (k, u, edits) in enumerate(reqs):
+        W, H = SESSIONS[k][3], SESSIONS[k][4]
+        buf = np.zeros(W * H * 4, np.uint8)
+        outs.append(buf)
+        server.submit(k, u, edits, ldr_out=buf)
+        if i % 4 == 3:
+            server.poll()
+    server.drain()
+    for i, (k, u, edits) in enumerate(reqs):
+        for e in edits:
+            ref_sc[k].edit_box(*e)
+        ref_s[k].frame(u)
+        assert np.array_equal(outs[i], ref_s[k].ldr().ravel()), f"request {i}"
+    server.close()
+    for s in served + ref_s:
+        s.close()
+    for sc in srv_sc + ref_sc:
+        sc.close()

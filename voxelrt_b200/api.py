@@ -583,6 +583,11 @@ class Server:
     def set_sequential(self, on: bool) -> None:
         check(lib.vrt_server_set_sequential(self.h, int(bool(on))))
 
+    def set_solo_pixels(self, pixels: int) -> None:
+        """Sessions of at least `pixels` pixels (with their own path scratch)
+        render alone; smaller ones are batched (0: batch everything)."""
+        check(lib.vrt_server_set_solo_pixels(self.h, int(pixels)))
+
     def now(self) -> float:
         return float(lib.vrt_server_now(self.h))
 

@@ -1338,6 +1338,7 @@ struct VrtServer {
   int n = 0;                     // slots
   int max_in_flight = 2;
   bool sequential = false;       // one request per launch through the session's own frame path
+  uint64_t solo_pixels = 0;      // batched mode: sessions this large (with their own path scratch) render alone
   std::deque<Req> pending;
   std::deque<Flight> flights;
   std::vector<int> busy;         // requests of the slot in flight
@@ -1408,6 +1409,23 @@ static int server_launch(VrtServer* sv) {
     take.push_back(std::move(sv->pending.front()));
     sv->pending.pop_front();
   } else {
+    auto solo = [&](const VrtSession* s) {
+      return sv->solo_pixels > 0 && s->path_kernel == VRT_PATH_WAVEFRONT && (uint64_t)s->W * s->H >= sv->solo_pixels;
+    };
+    // the oldest request of an idle session decides the launch: a large
+    // session renders alone through its own frame path; otherwise the oldest
+    // request of every idle small session joins one batch frame
+    for (auto it = sv->pending.begin(); it != sv->pending.end(); ++it) {
+      if (sv->busy[(size_t)it->session]) continue;
+      if (solo(sv->at(it->session))) {
+        take.push_back(std::move(*it));
+        sv->pending.erase(it);
+      }
+      break;
+    }
+  }
+  const bool alone = sv->sequential || !take.empty();
+  if (!alone) {
     // oldest pending request of every idle session, in arrival order, while
     // their pixels fit the pool
     std::vector<char> picked((size_t)sv->n, 0);
@@ -1416,7 +1434,8 @@ static int server_launch(VrtServer* sv) {
       const int k = it->session;
       VrtSession* s = sv->at(k);
       const uint64_t p = (uint64_t)s->W * s->H;
-      if (!sv->busy[(size_t)k] && !picked[(size_t)k] && pix + p <= sv->batch->P) {
+      const bool large = sv->solo_pixels > 0 && s->path_kernel == VRT_PATH_WAVEFRONT && p >= sv->solo_pixels;
+      if (!large && !sv->busy[(size_t)k] && !picked[(size_t)k] && pix + p <= sv->batch->P) {
         picked[(size_t)k] = 1;
         pix += p;
         take.push_back(std::move(*it));
@@ -1438,7 +1457,7 @@ static int server_launch(VrtServer* sv) {
     idx.push_back(r.session);
     us.push_back(r.u);
   }
-  if (sv->sequential) {
+  if (alone) {
     if (int rc = vrt_frame(sv->at(idx[0]), &us[0])) return rc;
   } else {
     if (int rc = batch_frame_impl(sv->batch, idx.data(), (int)idx.size(), us.data())) return rc;
@@ -1578,6 +1597,12 @@ int vrt_server_set_sequential(VrtServer* sv, int on) {
       if (sv->at(k) && sv->at(k)->path_kernel == VRT_PATH_BATCH_ONLY)
         return fail(VRT_ERR_STATE, "session %d has no path scratch of its own (VRT_PATH_BATCH_ONLY)", k);
   sv->sequential = on != 0;
+  return VRT_OK;
+}
+
+int vrt_server_set_solo_pixels(VrtServer* sv, long long pixels) {
+  if (!sv || pixels < 0) return fail(VRT_ERR_INVALID, "bad argument");
+  sv->solo_pixels = (uint64_t)pixels;
   return VRT_OK;
 }
 
