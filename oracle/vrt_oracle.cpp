@@ -182,13 +182,17 @@ inline float om_pow(float x, float y) {
 // ---------------------------------------------------------------------------
 // Storage formats
 // ---------------------------------------------------------------------------
-// binary32 -> binary16, round to nearest even (WebGPU rgba16float store).
+// binary32 -> binary16, round to nearest even (WebGPU rgba16float store);
+// finite values that would round beyond the half range store as the largest
+// finite half (65504): WebGPU leaves overflow to the backend (Vulkan allows
+// the largest finite value or infinity), and an infinite texel would turn a
+// running history mean infinite for good.  Infinity and NaN stay.
 inline uint16_t f32_to_f16(float f) {
   uint32_t x = fbits(f);
   uint32_t sign = (x >> 16) & 0x8000u;
   uint32_t ax = x & 0x7fffffffu;
   if (ax >= 0x7f800000u) return (uint16_t)(sign | (ax > 0x7f800000u ? 0x7e00u : 0x7c00u));
-  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7bffu);
   if (ax < 0x38800000u) {
     if (ax < 0x33000000u) return (uint16_t)sign;
     uint32_t e = ax >> 23;

@@ -340,30 +340,6 @@ __device__ __forceinline__ void stage_input(uint8_t* tile, int row, const float*
   store_row(tile, row, kIn, f);
 }
 
-// Columns [8 cg0, 8 (cg0 + ncg)) of row `row` of a row-chunked tile with C
-// columns, from v[0 .. 8 ncg) (16-byte stores).
-template <int ncg>
-__device__ __forceinline__ void store_cols(uint8_t* tile, int row, int C, int cg0, const float* v) {
-#pragma unroll
-  for (int k = 0; k < ncg; k++)
-    *reinterpret_cast<uint4*>(tile + umma::canon_off(row, 8 * (cg0 + k), C)) = pack8(v + 8 * k);
-}
-
-// Half `hf` of a query's encoded input (columns 40 hf .. 40 hf + 39) into
-// row `row` of the input tile; both halves compute the whole encoding.
-__device__ __forceinline__ void stage_query_half(uint8_t* tile, int row, const float* q, bool valid, float extent,
-                                                 int hf) {
-  float f[kIn];
-  if (valid) {
-    encode(q, extent, f);
-  } else {
-#pragma unroll
-    for (int j = 0; j < kIn; j++) f[j] = 0.0f;
-  }
-  if (hf == 0) store_cols<5>(tile, row, kIn, 0, f);
-  else store_cols<5>(tile, row, kIn, 5, f + 40);
-}
-
 // As stage_input with the query already in registers (valid: row holds a sample).
 __device__ __forceinline__ void stage_query(uint8_t* tile, int row, const float* q, bool valid, float extent) {
   float f[kIn];
@@ -412,16 +388,13 @@ __device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
 }
 
 // Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set.
-// A CTA keeps two 128-query tiles in flight, each with its own TMEM
-// accumulator (columns 64u..64u+63), its own activation tiles and its own
+// A CTA of 128 threads keeps two 128-query tiles in flight, each with its own
+// TMEM accumulator (columns 64u..64u+63), its own activation tiles and its own
 // mbarrier: while the tensor core runs one tile's layer, the threads unpack
 // the other tile's previous layer (TMEM load, ReLU, bf16 pack into the next
-// operand tile), so the MMA latency hides behind the epilogue work.  Each
-// row has two threads (256 per CTA): thread t owns row t % 128 of both tiles
-// and half t / 128 of its columns -- warps w and w + 4 read the same TMEM
-// lanes, different columns -- which doubles the warps that share the
-// encoding and epilogue work.  A task's CTAs stride over its tile pairs.
-__global__ void __launch_bounds__(256) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
+// operand tile), so the MMA latency hides behind the epilogue work.  Thread r
+// owns row r of both tiles.  A task's CTAs stride over its tile pairs.
+__global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
   using namespace mlp;
   const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
   int n = tk.n_max;
@@ -432,7 +405,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const __grid_constant__ MlpTa
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
-  const int t = threadIdx.x, warp = t >> 5, r = t & 127, hf = t >> 7;
+  const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
   if (t == 0) { umma::mbar_init(&mbar[0], 1); umma::mbar_init(&mbar[1], 1); }
   load_weights(smem, tk.wb);
@@ -450,7 +423,7 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const __grid_constant__ MlpTa
   auto fetch = [&](int pair_tile) {
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      const int idx = (pair_tile + u * tk.ctas) * 128 + r;
+      const int idx = (pair_tile + u * tk.ctas) * 128 + t;
       if (idx < n) {
 #pragma unroll
         for (int j = 0; j < 9; j++) q[u][j] = __ldg(tk.q9 + (size_t)idx * 9 + j);
@@ -478,15 +451,15 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const __grid_constant__ MlpTa
     float qq[2][9];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      idx[u] = (pt + u * tk.ctas) * 128 + r;
+      idx[u] = (pt + u * tk.ctas) * 128 + t;
 #pragma unroll
       for (int j = 0; j < 9; j++) qq[u][j] = q[u][j];
     }
     // stage tile 0 and start its first layer; stage tile 1 while it runs
-    stage_query_half(smem + X[0], r, qq[0], idx[0] < n, tk.extent, hf);
+    stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
     ok = publish_and(ok);
     if (ok) issue(0, 0);
-    stage_query_half(smem + X[1], r, qq[1], idx[1] < n, tk.extent, hf);
+    stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
     ok = publish_and(ok);
     if (ok) issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
@@ -496,14 +469,14 @@ __global__ void __launch_bounds__(256) k_mlp_infer(const __grid_constant__ MlpTa
       for (int u = 0; u < 2; u++) {
         wait(u);
         if (l < 3) {
-          float h[kHid / 2];
-          tmem_row<kHid / 2>(tbase, 64u * (uint32_t)u + 32u * (uint32_t)hf, h);
+          float h[kHid];
+          tmem_row<kHid>(tbase, 64u * (uint32_t)u, h);
 #pragma unroll
-          for (int j = 0; j < kHid / 2; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
-          store_cols<4>(smem + ((l & 1) ? X[u] : Y[u]), r, kHid, 4 * hf, h);
+          for (int j = 0; j < kHid; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
+          store_row(smem + ((l & 1) ? X[u] : Y[u]), t, kHid, h);
           ok = publish_and(ok);
           if (ok) issue(u, l + 1);
-        } else if (hf == 0) {
+        } else {
           float o[kOutPad];
           tmem_row<kOutPad>(tbase, 64u * (uint32_t)u, o);
           if (ok && idx[u] < n)
@@ -795,7 +768,7 @@ cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st) {
     attr = true;
   }
   const int grid = assign_ctas(ts, sm_count_mlp() * 2, 256);   // 2 x 100 KB of shared memory per SM
-  k_mlp_infer<<<grid, 256, mlp::kInferSmem, st>>>(ts);
+  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(ts);
   return cudaGetLastError();
 }
 

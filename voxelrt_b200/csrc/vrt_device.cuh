@@ -175,7 +175,15 @@ VRT_DI float pow_(float x, float y) {
 // ---------------------------------------------------------------------------
 // Storage formats
 // ---------------------------------------------------------------------------
-VRT_DI uint32_t h2bits(float x) { return (uint32_t)__half_as_ushort(__float2half_rn(x)); }
+// rgba16float store: round to nearest even; finite values beyond the half
+// range store as the largest finite half (65504).  WebGPU leaves the overflow
+// to the backend (Vulkan allows the largest finite value or infinity); an
+// infinite texel would turn a running history mean infinite for good.
+VRT_DI uint32_t h2bits(float x) {
+  const float ax = fabsf(x);
+  if (ax > 65504.0f && ax < INFINITY) x = copysignf(65504.0f, x);
+  return (uint32_t)__half_as_ushort(__float2half_rn(x));
+}
 VRT_DI float bits2f(uint32_t h) { return __half2float(__ushort_as_half((unsigned short)h)); }
 VRT_DI uint2 pack_h4(float a, float b, float c, float d) {
   return make_uint2(h2bits(a) | (h2bits(b) << 16), h2bits(c) | (h2bits(d) << 16));

@@ -868,6 +868,101 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
   }
 }
 
+// The tail of a frame whose remaining paths are few -- the radiance cache's
+// training paths after every other path ended at its first bounce: one
+// thread finishes each path of wave `wave`'s active list, tracing its pending
+// shadow and bounce rays with the same resumable DDA the queue tracer runs
+// (FlatDDA: same walk, hits and counters) and shading each vertex as
+// k_wf_shade does, until the path ends.  The per-wave form would launch a
+// trace and a shade kernel for every remaining bounce, each waiting for the
+// slowest of ~10^5 latency-bound walks; here each path runs its own
+// sequence.  Same per-path arithmetic and RNG draws, so the same image.
+template <class J, bool kSmem>
+__global__ void __launch_bounds__(256, 2) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
+  extern __shared__ uint32_t s_occ[];
+  if (kSmem) {
+    const DScene S0 = jobs.scene(0);
+    const int nwords = (S0.BG * S0.BG * S0.BG + 31) >> 5;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) s_occ[i] = __ldg(S0.bits + i);
+    __syncthreads();
+  }
+  const bool any_cache = jobs.any_cache();
+  const int n = b.ctr[4 * wave + 2];
+  const uint32_t* list = active_of(b, wave);
+  const int stride = gridDim.x * blockDim.x;
+  DCount c{0u, 0u, 0u, 0u};
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int i = base + threadIdx.x;
+    bool fin_train = false;
+    uint32_t ti = 0u;
+    F3 rfin = f3(0.0f, 0.0f, 0.0f);
+    int jc = 0;
+    if (i < n) {
+      const uint32_t g = list[i];
+      const int j = jobs.job_of(g);
+      jc = j;
+      const uint32_t lp = g - jobs.first(j);
+      const int W = jobs.width(j);
+      const CacheDev& cc = jobs.cache(j);
+      const int role = cache_role(cc, lp, W);
+      const Uni& u = jobs.uni(j);
+      const DScene S = jobs.scene(j);
+      const uint32_t* occ = kSmem ? s_occ : S.bits;
+      for (int w = wave;; w++) {
+        const float4 s0 = b.S0[g];
+        const float4 s1 = b.S1[g];
+        const float4 s2 = b.S2[g];
+        const float4 r0 = b.R0[g];
+        const float4 r1 = b.R1[g];
+        F3 radiance = xyz(s0);
+        F3 tp = xyz(s1);
+        uint32_t rng = __float_as_uint(s0.w);
+        const uint32_t mat1bits = __float_as_uint(s1.w);
+        const uint32_t flags = __float_as_uint(s2.w);
+        const F3 surf = xyz(r0);
+        if (flags & kFlagShadow) {   // the previous vertex's sun shadow ray
+          const float4 r2 = b.R2[g];
+          const F3 ld = xyz(r2);
+          FlatDDA d;
+          d.init(S, surf, ld, r2.w);
+          c.rays++;
+          while (!d.done()) d.step(S, occ, ld, c);
+          d.finish(S, c);
+          if (!(d.tHit >= 0.0f)) radiance = radiance + xyz(s2);
+        }
+        bool done = (flags & kFlagTerminal) != 0u;
+        if (!done) {
+          const F3 rd = xyz(r1);
+          FlatDDA d;
+          d.init(S, surf, rd, 1e4f);
+          c.rays++;
+          while (!d.done()) d.step(S, occ, rd, c);
+          d.finish(S, c);
+          if (d.tHit < 0.0f) {
+            radiance = radiance + tp * sky_color(u, rd, false);
+            done = true;
+          } else {
+            const F3 pos = surf + rd * d.tHit;
+            const F3 nrm = hit_normal(d.hit_axis(), rd);
+            const Mat mat = unpack_material(d.mat);
+            const uint32_t kmax = role == kRolePlain ? u.params0[1] : cc.train_bounces;
+            bool shadow = false, bounce = false;
+            done = !shade_vertex(u, b, g, (uint32_t)w, pos, nrm, mat, radiance, tp, rng, mat1bits, shadow, bounce,
+                                 kmax, rec_slot(cc, role, lp, W, (uint32_t)w));
+          }
+        }
+        if (done) {
+          finalize(jobs.outs(j), lp, radiance, mat1bits, jobs.clamp(j));
+          if (role == kRoleTrain) { fin_train = true; ti = train_index(cc, lp, W); rfin = radiance; }
+          break;
+        }
+      }
+    }
+    if (any_cache) cache_emit_samples(jobs.cache(jc), fin_train, ti, rfin);
+  }
+  if (stats) block_flush_stats(stats, c, 0u);   // kStatRays..kStatVReads
+}
+
 // Zeroes the per-frame query and sample counters of every cache job.
 template <class J>
 __global__ void k_cache_reset(J jobs, int njobs) {
@@ -1075,7 +1170,8 @@ cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int 
 template <class J, class ShadeFn, bool kVarMaxT = false>
 cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                          const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st, uint32_t* launches,
-                         cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves, ShadeFn shade) {
+                         cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves, ShadeFn shade,
+                         int tail_from = 0) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   const WfDev b = wf_view(wb);
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
@@ -1088,6 +1184,18 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
   nl++;
   int timed = 0;
   for (int w = 0; w < waves; w++) {
+    if (tail_from > 0 && w == tail_from) {   // the remaining paths, one thread each
+      const int tblocks = sms * 2;
+      if (smem > 0) {
+        e = cudaFuncSetAttribute(k_wf_tail<J, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess) k_wf_tail<J, true><<<tblocks, 256, smem, st>>>(jobs, b, w, stats);
+      } else {
+        k_wf_tail<J, false><<<tblocks, 256, 0, st>>>(jobs, b, w, stats);
+      }
+      if (e != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return e;
+      nl++;
+      break;
+    }
     const bool tm = trace_ev && w < max_timed_waves;
     if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
     const int impl = w == 0 ? (int)P : 0;
@@ -1114,7 +1222,7 @@ template <class J>
 cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                             const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
                             uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
-                            int njobs = 1) {
+                            int njobs = 1, int tail_from = 0) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   if (jobs.any_cache()) {
     k_cache_reset<J><<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
@@ -1125,7 +1233,7 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
                         if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
                         else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
                         return cudaGetLastError();
-                      });
+                      }, tail_from);
 }
 
 }  // namespace vrt
