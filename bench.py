@@ -592,7 +592,7 @@ def batched_line(args, local):
                                "log-uniform 320x180..2560x1440, bounces U{1..6}, 1 spp, temporal+a-trous+present",
                    "jobs": len(jobs), "pixels_per_step": pixels, "worlds": len(worlds),
                    "graph": True, "tuning": dict(zip(["refill_min", "trace_blocks_per_sm", "shade_blocks_per_sm",
-                                                      "trace_variant"], tune)),
+                                                      "trace_variant", "atrous_tile_rows", "tail_wave"], tune)),
                    "autotune_s": round(tune_s, 2),
                    "l2": "flushed before every timed batch frame and every sequential round"},
         "sequential": {"value": round(s_val, 2), "unit": "Mrays/s", "ms_per_step": round(statistics.mean(s_ms), 3)},

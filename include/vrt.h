@@ -112,6 +112,11 @@ typedef struct VrtTuning {
                                  4: (2,1), 5: (1,1)                              */
   int atrous_tile_rows;       /* a-trous output tile rows: 0 = 16 at steps 1-2
                                  and 8 at step 4 (default), 8 = 8 at every step  */
+  int tail_wave;              /* first wave whose remaining paths each finish on
+                                 one thread (their rays traced in turn, not in
+                                 per-wave launches); 0 = never, -1 = automatic
+                                 (wave 2 for cache-assisted views, else never);
+                                 the image is the same either way              */
 } VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,

@@ -17,11 +17,14 @@ def _setup(vrt, W, H, fclamp=10.0):
     return vox, spawn, ctx, sc, s
 
 
-@pytest.mark.parametrize("frame,rec", [(5, 3), (12, 1), (0, 8)])
-def test_cache_frame_matches_oracle(vrt, orc, frame, rec):
+@pytest.mark.parametrize("frame,rec,tail", [(5, 3, -1), (12, 1, -1), (0, 8, -1), (5, 3, 0)])
+def test_cache_frame_matches_oracle(vrt, orc, frame, rec, tail):
+    """tail -1: the training paths finish one thread each after the first
+    bounce (the default); 0: every wave is traced and shaded separately."""
     from oracle import mlp_ref as M
     W, H, fclamp = 128, 72, 10.0
     vox, spawn, ctx, sc, s = _setup(vrt, W, H, fclamp)
+    s.set_tuning(tail_wave=tail)
     s.set_cache(train_bounces=6, train_vertices=rec, seed=3)
     p0 = s.cache_params()                          # the weights this frame's inference uses
     u = vrt.make_uniforms(spawn, None, vrt.Lighting(), frame, 2, 0, W, H)

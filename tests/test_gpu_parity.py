@@ -383,3 +383,29 @@ def test_atrous_tile_shape_invariant(ctx, vrt):
     for a, b in zip(outs[0], outs[1]):
         assert np.array_equal(a, b)
     sc.close()
+
+
+@pytest.mark.parametrize("bounces", [2, 4, 6])
+def test_tail_kernel_invariant(ctx, vrt, bounces):
+    """Finishing the remaining paths one thread each from wave 2 or 3
+    (k_wf_tail) gives the same image and traversal counters as running every
+    wave."""
+    W, H, n = 320, 180, 128
+    vox, spawn = vrt.generate_scene(2, n, 3)
+    sc = vrt.Scene(ctx, vox, n)
+    u = vrt.make_uniforms(vrt.camera_spline(spawn, 20), None, vrt.Lighting(), 5, bounces, 3, W, H)
+    outs = []
+    for tail in (0, 2, 3):
+        s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, keep_radiance_f32=True)
+        s.set_tuning(tail_wave=tail)
+        s.frame(u)
+        st = s.stats()
+        outs.append((s.radiance_f32().copy(), s.gbuffer().copy(), s.albedo().copy(),
+                     (st.rays, st.dda_outer, st.dda_inner, st.voxel_reads)))
+        s.close()
+    for o in outs[1:]:
+        assert np.array_equal(o[0].view(np.uint32), outs[0][0].view(np.uint32))
+        assert np.array_equal(o[1].view(np.uint32), outs[0][1].view(np.uint32))
+        assert np.array_equal(o[2], outs[0][2])
+        assert o[3] == outs[0][3]
+    sc.close()

@@ -57,7 +57,7 @@ class VrtSessionConfig(C.Structure):
 
 class VrtTuning(C.Structure):
     _fields_ = [("refill_min", C.c_int), ("trace_blocks_per_sm", C.c_int), ("shade_blocks_per_sm", C.c_int),
-                ("trace_variant", C.c_int), ("atrous_tile_rows", C.c_int)]
+                ("trace_variant", C.c_int), ("atrous_tile_rows", C.c_int), ("tail_wave", C.c_int)]
 
 
 PATH_WAVEFRONT = 0

@@ -324,9 +324,9 @@ class Session:
         self.scene = scene
 
     def set_tuning(self, refill_min: int = 0, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
-                   trace_variant: int = 0, atrous_tile_rows: int = 0) -> None:
+                   trace_variant: int = 0, atrous_tile_rows: int = 0, tail_wave: int = -1) -> None:
         t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant),
-                      int(atrous_tile_rows))
+                      int(atrous_tile_rows), int(tail_wave))
         check(lib.vrt_session_set_tuning(self.h, C.byref(t)))
 
     def autotune(self, u: VrtUniforms, frames: int = 3):
@@ -336,12 +336,13 @@ class Session:
         ms = C.c_float()
         check(lib.vrt_session_autotune(self.h, C.byref(u), int(frames), C.byref(t), C.byref(ms)))
         return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant,
-                t.atrous_tile_rows), float(ms.value)
+                t.atrous_tile_rows, t.tail_wave), float(ms.value)
 
     def get_tuning(self) -> tuple:
         t = VrtTuning()
         check(lib.vrt_session_get_tuning(self.h, C.byref(t)))
-        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant, t.atrous_tile_rows)
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant, t.atrous_tile_rows,
+                t.tail_wave)
 
     def set_cache(self, enabled: bool = True, train_bounces: int = 6, train_vertices: int = 3,
                   train_batch: int = 65536, train_steps: int = 1, learning_rate: float = 1e-2, seed: int = 1) -> None:
@@ -505,8 +506,10 @@ class Batch:
     def set_graph(self, on: bool) -> None:
         check(lib.vrt_batch_set_graph(self.h, int(bool(on))))
 
-    def set_tuning(self, refill_min=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, trace_variant=0) -> None:
-        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant))
+    def set_tuning(self, refill_min=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, trace_variant=0,
+                   atrous_tile_rows=0, tail_wave=0) -> None:
+        t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant),
+                      int(atrous_tile_rows), int(tail_wave))
         check(lib.vrt_batch_set_tuning(self.h, C.byref(t)))
 
     def autotune(self, uniforms: list, frames: int = 2):
@@ -514,7 +517,8 @@ class Batch:
         t = VrtTuning()
         ms = C.c_float()
         check(lib.vrt_batch_autotune(self.h, arr, int(frames), C.byref(t), C.byref(ms)))
-        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant), float(ms.value)
+        return (t.refill_min, t.trace_blocks_per_sm, t.shade_blocks_per_sm, t.trace_variant, t.atrous_tile_rows,
+                t.tail_wave), float(ms.value)
 
     def stats(self) -> VrtFrameStats:
         s = VrtFrameStats()

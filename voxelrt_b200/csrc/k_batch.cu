@@ -75,7 +75,8 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   J.firsts = d_firsts;
   J.n = n;
   J.cache_jobs = ncl;
-  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n);
+  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n,
+                                  tune.tail_wave > 0 ? tune.tail_wave : 0);
   if (e != cudaSuccess) return e;
   // the cache jobs' inference, resolve and training, all jobs per launch
   if (ncl > 0 && (e = launch_cache_post(J, wf_view(wb), cls, ncl, stats, st, launches)) != cudaSuccess) return e;

@@ -81,9 +81,11 @@ cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fcl
   const int smem_occ = (int)(occ_words(s.BG) * sizeof(uint32_t));
   const int smem = smem_occ <= 64 * 1024 ? smem_occ : 0;
   // cache frames: every path but the training paths ends at its first bounce
-  // (wave 1), so the few paths left after it run to their end one thread each
+  // (wave 1), so by default the few paths left after it run to their end one
+  // thread each
+  const int tail = tune.tail_wave >= 0 ? tune.tail_wave : (job.cc.on ? 2 : 0);
   cudaError_t e = wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
-                                  max_timed_waves, timed_waves, 1, job.cc.on ? 2 : 0);
+                                  max_timed_waves, timed_waves, 1, tail);
   if (e != cudaSuccess || !job.cc.on) return e;
   if (cache_ev && (e = cudaEventRecord(cache_ev[0], st)) != cudaSuccess) return e;
   e = launch_cache_post(job, wf_view(wb), cache, 1, out.stats, st, launches);

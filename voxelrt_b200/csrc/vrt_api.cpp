@@ -493,6 +493,7 @@ int vrt_session_get_tuning(VrtSession* s, VrtTuning* t) {
   t->shade_blocks_per_sm = s->tune.shade_blocks_per_sm;
   t->trace_variant = s->tune.trace_variant;
   t->atrous_tile_rows = s->tune.atrous_rows;
+  t->tail_wave = s->tune.tail_wave;
   return VRT_OK;
 }
 
@@ -500,13 +501,14 @@ int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
       t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5 ||
-      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8))
+      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8) || t->tail_wave < -1 || t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   s->tune.refill_min = t->refill_min ? t->refill_min : 8;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   s->tune.trace_variant = t->trace_variant;
   s->tune.atrous_rows = t->atrous_tile_rows;
+  s->tune.tail_wave = t->tail_wave;
   return VRT_OK;
 }
 
@@ -551,6 +553,30 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
         if (med < win_ms) { win_ms = med; win = s->tune; }
       }
   s->tune = win;
+  // where the remaining paths finish one thread each: automatic, never, or
+  // from wave 2 / 3 (frames of more than one bounce)
+  {
+    const int nb = s->cache_on ? s->cache_cfg.train_bounces : (int)u->params0[1];
+    float best_tail = 1e30f;
+    int best_wave = win.tail_wave;
+    for (int tw : {-1, 0, 2, 3}) {
+      if (tw > 0 && tw >= nb + 2) continue;
+      s->tune.tail_wave = tw;
+      if (int r = vrt_pass_pathtrace(s, u)) { s->tune = keep; return r; }   // warm-up
+      for (int f = 0; f < frames; f++) {
+        CUDA_TRY(cudaEventRecord(s->ev[0], st));
+        if (int r = vrt_pass_pathtrace(s, u)) { s->tune = keep; return r; }
+        CUDA_TRY(cudaEventRecord(s->ev[1], st));
+        CUDA_TRY(cudaEventSynchronize(s->ev[1]));
+        CUDA_TRY(cudaEventElapsedTime(&ms[(size_t)f], s->ev[0], s->ev[1]));
+      }
+      std::sort(ms.begin(), ms.end());
+      if (ms[(size_t)frames / 2] < best_tail) { best_tail = ms[(size_t)frames / 2]; best_wave = tw; }
+    }
+    s->tune.tail_wave = best_wave;
+    win = s->tune;
+    win_ms = best_tail;
+  }
   // the a-trous tile shape: the three iterations of a frame timed per shape
   if (u->params0[2] & 2u) {
     if (int r = vrt_pass_temporal(s, u)) { s->tune = keep; return r; }
@@ -580,6 +606,7 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
     best->shade_blocks_per_sm = win.shade_blocks_per_sm;
     best->trace_variant = win.trace_variant;
     best->atrous_tile_rows = win.atrous_rows;
+    best->tail_wave = win.tail_wave;
   }
   if (best_ms) *best_ms = win_ms;
   return vrt_session_reset(s);
@@ -1101,18 +1128,21 @@ int vrt_batch_set_graph(VrtBatch* b, int enable) {
 int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
   if (!b || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5)
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5 ||
+      t->tail_wave < -1 || t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   b->tune.refill_min = t->refill_min ? t->refill_min : 8;
   b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
   b->tune.trace_variant = t->trace_variant;
+  b->tune.tail_wave = t->tail_wave;
   return VRT_OK;
 }
 
 static bool same_tuning(const WavefrontTuning& a, const WavefrontTuning& c) {
   return a.refill_min == c.refill_min && a.trace_blocks_per_sm == c.trace_blocks_per_sm &&
-         a.shade_blocks_per_sm == c.shade_blocks_per_sm && a.trace_variant == c.trace_variant;
+         a.shade_blocks_per_sm == c.shade_blocks_per_sm && a.trace_variant == c.trace_variant &&
+         a.tail_wave == c.tail_wave;
 }
 
 }  // extern "C"
@@ -1293,6 +1323,21 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
         std::sort(ms.begin(), ms.end());
         if (ms[(size_t)frames / 2] < win_ms) { win_ms = ms[(size_t)frames / 2]; win = b->tune; }
       }
+  // where the remaining paths of the batch finish one thread each (0: never)
+  for (int tw : {2, 3, 4}) {
+    b->tune = win;
+    b->tune.tail_wave = tw;
+    int r = vrt_batch_frame(b, u);
+    for (int f = 0; f < frames && !r; f++) {
+      r = vrt_batch_frame(b, u);
+      VrtFrameStats st;
+      if (!r) r = vrt_batch_last_stats(b, &st);
+      ms[(size_t)f] = st.ms_total;
+    }
+    if (r) { b->tune = keep; b->use_graph = keep_graph; return r; }
+    std::sort(ms.begin(), ms.end());
+    if (ms[(size_t)frames / 2] < win_ms) { win_ms = ms[(size_t)frames / 2]; win = b->tune; }
+  }
   b->tune = win;
   b->use_graph = keep_graph;
   batch_drop_graph(b);
@@ -1302,6 +1347,7 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
     best->shade_blocks_per_sm = win.shade_blocks_per_sm;
     best->trace_variant = win.trace_variant;
     best->atrous_tile_rows = 0;   // batch frames run the unstaged a-trous kernel over all jobs
+    best->tail_wave = win.tail_wave;
   }
   if (best_ms) *best_ms = win_ms;
   for (VrtSession* s : b->sessions)

@@ -83,6 +83,8 @@ struct WavefrontTuning {
   int trace_variant = 0;        // (DDA iterations per warp-bookkeeping pass, min blocks/SM):
                                 // 0: (8, 5)  1: (6, 5)  2: (6, 4)  3: (4, 4)  4: (2, 1)  5: (1, 1)
   int atrous_rows = 0;          // a-trous output tile rows: 0 = 16 at steps 1-2 and 8 at step 4, 8 = 8 at all steps
+  int tail_wave = -1;           // first wave whose paths finish one thread each (k_wf_tail); 0 = never;
+                                // -1 = automatic: wave 2 for cache-assisted single-view frames, else never
 };
 
 // Host mirror of the device job table entry (JobDev in wavefront_core.cuh):

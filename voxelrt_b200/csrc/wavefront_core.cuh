@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
 // slowest of ~10^5 latency-bound walks; here each path runs its own
 // sequence.  Same per-path arithmetic and RNG draws, so the same image.
 template <class J, bool kSmem>
-__global__ void __launch_bounds__(256, 2) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
+__global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
   if (kSmem) {
     const DScene S0 = jobs.scene(0);
@@ -1185,7 +1185,7 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
   int timed = 0;
   for (int w = 0; w < waves; w++) {
     if (tail_from > 0 && w == tail_from) {   // the remaining paths, one thread each
-      const int tblocks = sms * 2;
+      const int tblocks = sms * 3;
       if (smem > 0) {
         e = cudaFuncSetAttribute(k_wf_tail<J, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess) k_wf_tail<J, true><<<tblocks, 256, smem, st>>>(jobs, b, w, stats);
