@@ -523,6 +523,13 @@ int vrt_mlp_selftest_gemm(int mode, int K, int N, const uint16_t* A, const uint1
  * arrives on, with TMEM held.  Returns VRT_ERR_TIMEOUT (the expected outcome);
  * the context stays usable. */
 int vrt_selftest_bounded_wait(unsigned int spins);
+/* No counterpart in the reference.  The present pass maps each channel value
+ * below 8 to its rgba8 code through the context's threshold table instead of
+ * evaluating ACES and pow(1/2.2) (present.wgsl:40-55); this runs every float
+ * of [0, 8) through both and reports how many differ (*mismatches, 0 when the
+ * table path is exact) and the smallest differing bit pattern (*first_bits,
+ * 0xffffffff when none). */
+int vrt_selftest_present(VrtCtx* ctx, uint64_t* mismatches, uint32_t* first_bits);
 
 /* ---- session checkpoint / resume ----------------------------------------- */
 /* No counterpart in the browser renderer; VoxelBench resumes its reference

@@ -294,6 +294,47 @@ def test_full_size_temporal_atrous_from_device_inputs(ctx, vrt, orc):
     s.close(); sc.close()
 
 
+def test_present_table_is_exact_over_its_range(ctx):
+    """The present pass codes channel values below 8 through the context's
+    threshold table; every float of [0, 8) gives the exact arithmetic's code."""
+    bad, first = ctx.selftest_present()
+    assert bad == 0, f"{bad} values differ, first bit pattern {first:#x}"
+    assert first == 0xFFFFFFFF
+
+
+@pytest.mark.parametrize("exposure", [1.0, 2.5])
+def test_present_edge_values_match_oracle(ctx, vrt, orc, exposure):
+    """Present on chosen values through the pass entry point: uniform and
+    log-spread values, denormals, signed zeros, values at and above the table's
+    range, the half maximum, infinities and NaN."""
+    W, H = 64, 48
+    vox, spawn = vrt.generate_scene(1, 64, 1)
+    sc = vrt.Scene(ctx, vox, 64)
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, accum_f32=True)
+    light = vrt.Lighting()
+    for f in range(2):                          # albedo from a real frame; history parity 1 next
+        s.pathtrace(vrt.make_uniforms(spawn, None, light, f, 2, 0, W, H))
+        s.end_frame()
+    rng = np.random.default_rng(7)
+    n = W * H * 4
+    v = np.concatenate([
+        rng.uniform(0.0, 8.0, n // 4),
+        10.0 ** rng.uniform(-40.0, 6.0, n // 4),
+        rng.uniform(-1.0, 20.0, n // 4),
+        np.array([0.0, -0.0, 1e-45, 1.1754942e-38, 7.9999995, 8.0, 8.000001, 65504.0, 3.4e38,
+                  np.inf, -np.inf, np.nan, -1e-30, -5.0], np.float32),
+    ]).astype(np.float32)
+    v = np.resize(v, n).reshape(H, W, 4)
+    s.write_history(v, None)                   # history slot 1
+    s.end_frame()
+    u = vrt.make_uniforms(spawn, None, light, 2, 2, 0, W, H, exposure)
+    s.present(u)
+    got = s.ldr()
+    want = orc.present(vrt.uniforms_bytes(u), W, H, v, True, s.albedo())
+    assert np.array_equal(got, want)
+    s.close(); sc.close()
+
+
 # --------------------------------------------------------------------------
 # Behaviour
 # --------------------------------------------------------------------------

@@ -187,6 +187,7 @@ SIGNATURES = {
     "vrt_mlp_train_device": (I, [P, P, P, I, C.c_float, C.c_float, I, C.POINTER(C.c_float)]),
     "vrt_mlp_check": (I, [P]),
     "vrt_selftest_bounded_wait": (I, [C.c_uint]),
+    "vrt_selftest_present": (I, [P, P, P]),
     "vrt_scene_build_lights": (I, [P, P]),
     "vrt_scene_read_lights": (I, [P, P, C.c_size_t, P, C.c_size_t, P, C.c_size_t]),
     "vrt_hdr_accum_reset": (I, [P]),

@@ -196,6 +196,15 @@ class Context:
     def bytes_in_use(self) -> int:
         return int(lib.vrt_ctx_bytes_in_use(self.h))
 
+    def selftest_present(self) -> tuple[int, int]:
+        """(mismatches, smallest differing bit pattern or 0xffffffff) of the
+        present pass's threshold table against the exact arithmetic over every
+        float of [0, 8) (vrt_selftest_present)."""
+        n = C.c_uint64()
+        f = C.c_uint32()
+        check(lib.vrt_selftest_present(self.h, C.byref(n), C.byref(f)))
+        return int(n.value), int(f.value)
+
     def close(self) -> None:
         if self.h:
             # objects of this context still open (a test that failed midway, a

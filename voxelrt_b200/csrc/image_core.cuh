@@ -167,19 +167,57 @@ VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const
   return make_float4(sr / den, sg_ / den, sb / den, center.w);
 }
 
-// present.wgsl:40-55 for one pixel: illum * sqrtAlb^2 * exposure -> ACES ->
-// pow(1/2.2), packed rgba8.
-VRT_DI uint32_t present_pixel(float exposure, float4 il, uint32_t a) {
+// present.wgsl:40-55 for one channel: v = illum * sqrtAlb^2 * exposure ->
+// ACES -> clamp -> pow(1/2.2) -> rgba8unorm code.
+VRT_DI uint32_t present_code_exact(float v) {
+  const float num = v * (2.51f * v + 0.03f);
+  const float den = v * (2.43f * v + 0.59f) + 0.14f;
+  const float t = clamp_(num / den, 0.0f, 1.0f);
+  return unorm8_(pow_(t, 0.454545468f));
+}
+
+// Present lookup table (kPresentLut words per device context):
+//   [0, 256)    the albedo factor sqrtAlb^2 of each rgba8 byte, (b / 255)^2 as
+//               the shader forms it;
+//   [256, 513)  lo[0..256]: lo[k] = the least float of [0, kPresentFastMax)
+//               whose exact code is >= k (inf if none; non-decreasing in k);
+//   [513, 770)  hi[0..256]: the float just above the greatest v of the range
+//               whose exact code is < k (0 for k = 0);
+// then scratch for the scan that builds them.  The exact code is almost but
+// not quite non-decreasing in v: num / den rounds so that at 133 values next
+// to a code step it drops back by one.  Every v >= hi[k] has a code >= k and
+// every v < lo[k + 1] a code <= k, so outside the windows [lo[k], hi[k]) the
+// code is the largest k with lo[k] <= v.
+constexpr float kPresentFastMax = 8.0f;
+constexpr uint32_t kPresentFastMaxBits = 0x41000000u;   // bit pattern of kPresentFastMax
+constexpr int kPresentLo = 256, kPresentHi = 513;
+
+// present_code_exact(v) through the table: an estimate from the hardware's
+// approximate divide / log2 / exp2 starts a walk along lo[] that ends at the
+// largest k with lo[k] <= v; values inside that code's window [lo[k], hi[k]),
+// outside [0, kPresentFastMax) or NaN take the exact arithmetic.
+VRT_DI uint32_t present_code(float v, const float* __restrict__ lut) {
+  if (!(v >= 0.0f && v < kPresentFastMax)) return present_code_exact(v);
+  const float* lo = lut + kPresentLo;
+  const float num = v * __fmaf_rn(2.51f, v, 0.03f);
+  const float den = __fmaf_rn(v, __fmaf_rn(2.43f, v, 0.59f), 0.14f);
+  const float t = fminf(fmaxf(__fdividef(num, den), 0.0f), 1.0f);
+  int c = __float2int_rn(255.0f * __powf(t, 0.454545468f));
+  c = min(max(c, 0), 255);
+  while (c > 0 && v < __ldg(lo + c)) c--;
+  while (c < 255 && v >= __ldg(lo + c + 1)) c++;
+  if (v < __ldg(lut + kPresentHi + c)) return present_code_exact(v);
+  return (uint32_t)c;
+}
+
+// present.wgsl:40-55 for one pixel with the context's lookup table.
+VRT_DI uint32_t present_pixel(float exposure, float4 il, uint32_t a, const float* __restrict__ lut) {
   const float iv[3] = {il.x, il.y, il.z};
   uint32_t outw = 255u << 24;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const float as = (float)((a >> (8 * c)) & 0xffu) / 255.0f;
-    const float v = (iv[c] * (as * as)) * exposure;
-    const float num = v * (2.51f * v + 0.03f);
-    const float den = v * (2.43f * v + 0.59f) + 0.14f;
-    const float t = clamp_(num / den, 0.0f, 1.0f);
-    outw |= unorm8_(pow_(t, 0.454545468f)) << (8 * c);
+    const float v = (iv[c] * __ldg(lut + ((a >> (8 * c)) & 0xffu))) * exposure;
+    outw |= present_code(v, lut) << (8 * c);
   }
   return outw;
 }

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(256) k_b_atrous(MultiJob J, uint32_t P, int it
 }
 
 // present.wgsl:40-55 over all jobs.
-__global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P) {
+__global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P, const float* __restrict__ lut) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= P) return;
   const int j = J.job_of(g);
@@ -64,12 +64,13 @@ __global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P) {
   const uint32_t lp = g - jd.first;
   const bool denoise = (jd.u.params0[2] & 2u) != 0u;
   const float4 il = denoise ? load_px(jd.den0, false, lp) : load_px(jd.acc_cur, jd.acc_f32 != 0, lp);
-  jd.ldr[lp] = present_pixel(jd.u.params1[2], il, __ldg(jd.out.alb8 + lp));
+  jd.ldr[lp] = present_pixel(jd.u.params1[2], il, __ldg(jd.out.alb8 + lp), lut);
 }
 
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
-                               cudaStream_t st, uint32_t* launches, const CacheLaunch* cls, int ncl) {
+                               cudaStream_t st, uint32_t* launches, const float* present_lut, const CacheLaunch* cls,
+                               int ncl) {
   MultiJob J;
   J.jobs = (const JobDev*)d_jobs;
   J.firsts = d_firsts;
@@ -83,7 +84,7 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   const unsigned blocks = (P + 255) / 256;
   k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
   for (int it = 0; it < 3; it++) k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);
-  k_b_present<<<blocks, 256, 0, st>>>(J, P);
+  k_b_present<<<blocks, 256, 0, st>>>(J, P, present_lut);
   if (launches) *launches += 5;
   return cudaGetLastError();
 }

@@ -41,12 +41,81 @@ __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __rest
 // present.wgsl:40-55 as a compute pass writing a headless rgba8 buffer.
 template <bool kFinF32>
 __global__ void __launch_bounds__(256) k_present(float exposure, int W, int H, const void* __restrict__ fin,
-                                                 const uint32_t* __restrict__ alb8, uint32_t* __restrict__ ldr) {
+                                                 const uint32_t* __restrict__ alb8, uint32_t* __restrict__ ldr,
+                                                 const float* __restrict__ lut) {
   const int x = blockIdx.x * 32 + (threadIdx.x & 31);
   const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (x >= W || y >= H) return;
   const size_t p = (size_t)y * W + x;
-  ldr[p] = present_pixel(exposure, load_px(fin, kFinF32, p), __ldg(alb8 + p));
+  ldr[p] = present_pixel(exposure, load_px(fin, kFinF32, p), __ldg(alb8 + p), lut);
+}
+
+// Building the present lookup table (image_core.cuh), step 1: every float of
+// [0, kPresentFastMax) through the exact arithmetic.  A thread walks a run of
+// kPresentScanRun consecutive bit patterns (ordered like the values they
+// encode) and, per stretch of equal codes, lowers the code's least bit
+// pattern and raises its greatest.
+constexpr uint32_t kPresentScanRun = 4096u;
+__global__ void __launch_bounds__(256) k_present_scan(unsigned int* __restrict__ minb, unsigned int* __restrict__ maxb) {
+  const uint32_t end = kPresentFastMaxBits;
+  const uint32_t b0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPresentScanRun;
+  if (b0 >= end) return;
+  const uint32_t b1 = min(end, b0 + kPresentScanRun);
+  uint32_t code = present_code_exact(__uint_as_float(b0)), start = b0;
+  for (uint32_t b = b0 + 1u; b < b1; b++) {
+    const uint32_t c = present_code_exact(__uint_as_float(b));
+    if (c != code) {
+      atomicMin(minb + code, start);
+      atomicMax(maxb + code, b - 1u);
+      code = c;
+      start = b;
+    }
+  }
+  atomicMin(minb + code, start);
+  atomicMax(maxb + code, b1 - 1u);
+}
+
+// Step 2 (256 threads): thread k forms the albedo factor of byte k, lo[k] as
+// the least bit pattern of any code >= k and hi[k] as one above the greatest
+// bit pattern of any code < k.
+__global__ void __launch_bounds__(256) k_present_lut(float* __restrict__ lut, const unsigned int* __restrict__ minb,
+                                                     const unsigned int* __restrict__ maxb) {
+  const int k = threadIdx.x;
+  const float as = (float)k / 255.0f;
+  lut[k] = as * as;
+  uint32_t lo = 0x7f800000u;                       // inf: no code >= k in the range
+  for (int c = k; c < 256; c++)
+    if (minb[c] < kPresentFastMaxBits) lo = min(lo, minb[c]);
+  uint32_t hi = 0u;
+  bool any = false;
+  for (int c = 0; c < k; c++)
+    if (maxb[c] != 0xffffffffu) { hi = max(hi, maxb[c] + 1u); any = true; }
+  lut[kPresentLo + k] = __uint_as_float(lo);
+  lut[kPresentHi + k] = any ? __uint_as_float(hi) : 0.0f;
+  if (k == 0) {
+    lut[kPresentLo + 256] = __int_as_float(0x7f800000);
+    uint32_t h = 0u;
+    for (int c = 0; c < 256; c++)
+      if (maxb[c] != 0xffffffffu) h = max(h, maxb[c] + 1u);
+    lut[kPresentHi + 256] = __uint_as_float(h);
+  }
+}
+
+// Every float of [0, kPresentFastMax) through present_code and
+// present_code_exact; counts the values where they differ and keeps the
+// smallest such bit pattern.
+__global__ void __launch_bounds__(256) k_present_check(const float* __restrict__ lut, unsigned long long* __restrict__ bad,
+                                                       unsigned int* __restrict__ first) {
+  const uint32_t end = __float_as_uint(kPresentFastMax);
+  unsigned long long n = 0;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < end; b += gridDim.x * blockDim.x) {
+    const float v = __uint_as_float(b);
+    if (present_code(v, lut) != present_code_exact(v)) {
+      n++;
+      atomicMin(first, b);
+    }
+  }
+  if (n) atomicAdd(bad, n);
 }
 
 // ---------------------------------------------------------------------------
@@ -143,10 +212,27 @@ cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const voi
 }
 
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
-                           const uint32_t* alb8, uint32_t* ldr, cudaStream_t st) {
+                           const uint32_t* alb8, uint32_t* ldr, const float* lut, cudaStream_t st) {
   dim3 grid((W + 31) / 32, (H + 7) / 8);
-  if (fin_f32) k_present<true><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr);
-  else k_present<false><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr);
+  if (fin_f32) k_present<true><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr, lut);
+  else k_present<false><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr, lut);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_present_lut(float* lut, cudaStream_t st) {
+  unsigned int* minb = reinterpret_cast<unsigned int*>(lut + kPresentHi + 257);
+  unsigned int* maxb = minb + 256;
+  cudaError_t e = cudaMemsetAsync(minb, 0x7f, 256 * sizeof(unsigned int), st);   // 0x7f7f7f7f: "none"
+  if (e == cudaSuccess) e = cudaMemsetAsync(maxb, 0xff, 256 * sizeof(unsigned int), st);   // "none"
+  if (e != cudaSuccess) return e;
+  const uint32_t runs = (kPresentFastMaxBits + kPresentScanRun - 1u) / kPresentScanRun;
+  k_present_scan<<<(runs + 255u) / 256u, 256, 0, st>>>(minb, maxb);
+  k_present_lut<<<1, 256, 0, st>>>(lut, minb, maxb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_present_check(const float* lut, unsigned long long* bad, unsigned int* first, cudaStream_t st) {
+  k_present_check<<<148 * 8, 256, 0, st>>>(lut, bad, first);
   return cudaGetLastError();
 }
 

@@ -123,11 +123,11 @@ constexpr int kGA0 = 0, kGA1 = kGA0 + 128 * kIn * 2, kGA2 = kGA1 + 128 * kHid * 
 constexpr int kGDY = kGA3 + 128 * kHid * 2, kGStride = kGDY + 128 * kHid * 2;   // 84 KB per group
 constexpr int kGBase = kWEnd, kGEnd = kGBase + 2 * kGStride;
 constexpr int kTrainSmem = kGEnd + 1024;   // slack: MN-major views read up to 1 KB past a tile
-// inference kernel: forward weights + per tile (two in flight) an input tile
-// X (80 columns, later the 64-column layer-2 input) and a 64-column tile Y
-constexpr int kIX0 = kWEnd, kIY0 = kIX0 + 128 * kIn * 2, kIX1 = kIY0 + 128 * kHid * 2,
-              kIY1 = kIX1 + 128 * kIn * 2, kIEnd = kIY1 + 128 * kHid * 2;
-constexpr int kInferSmem = kIEnd;   // 100 KB: two CTAs per SM
+// inference kernel: forward weights + per tile (two in flight) one operand
+// tile X: the 80-column input, then each hidden layer's 64 columns written
+// over it once the MMAs that read it have completed
+constexpr int kIX0 = kWEnd, kIX1 = kIX0 + 128 * kIn * 2, kIEnd = kIX1 + 128 * kIn * 2;
+constexpr int kInferSmem = kIEnd;   // 68 KB: three CTAs per SM
 
 // TMEM columns (fp32): layer outputs / input gradients of group g at 64 g,
 // weight gradients accumulated over all of a CTA's samples at kTW*
@@ -389,12 +389,15 @@ __device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
 
 // Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set.
 // A CTA of 128 threads keeps two 128-query tiles in flight, each with its own
-// TMEM accumulator (columns 64u..64u+63), its own activation tiles and its own
+// TMEM accumulator (columns 64u..64u+63), its own operand tile and its own
 // mbarrier: while the tensor core runs one tile's layer, the threads unpack
 // the other tile's previous layer (TMEM load, ReLU, bf16 pack into the next
-// operand tile), so the MMA latency hides behind the epilogue work.  Thread r
-// owns row r of both tiles.  A task's CTAs stride over its tile pairs.
-__global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
+// operand tile), so the MMA latency hides behind the epilogue work.  A layer's
+// output overwrites its input tile: every thread waits for the layer's MMA
+// completion (which covers the MMAs' shared-memory reads) before it stores,
+// so one tile per query block is enough and three CTAs fit on an SM.  Thread
+// r owns row r of both tiles.  A task's CTAs stride over its tile pairs.
+__global__ void __launch_bounds__(128, 3) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
   using namespace mlp;
   const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
   int n = tk.n_max;
@@ -414,8 +417,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTa
   umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   const uint32_t s0 = umma::smem_u32(smem);
-  // per tile: X (input, 80 columns; later the layer-2 input, 64 columns) and Y
-  const int X[2] = {kIX0, kIX1}, Y[2] = {kIY0, kIY1};
+  // per tile: X (input, 80 columns; then each hidden layer, 64 columns)
+  const int X[2] = {kIX0, kIX1};
   uint32_t phase[2] = {0u, 0u};
   bool ok = true;
   const int stride = 2 * tk.ctas;          // a CTA's pairs: tiles (pt, pt + ctas), pt = cb + k stride
@@ -435,9 +438,9 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTa
     if (t != 0) return;
     const uint32_t acc = tbase + 64u * (uint32_t)u;
     if (l == 0) issue_fwd(acc, s0 + X[u], s0 + kWf0, kIn, kHid, false);
-    else if (l == 1) issue_fwd(acc, s0 + Y[u], s0 + kWf1, kHid, kHid, false);
+    else if (l == 1) issue_fwd(acc, s0 + X[u], s0 + kWf1, kHid, kHid, false);
     else if (l == 2) issue_fwd(acc, s0 + X[u], s0 + kWf2, kHid, kHid, false);
-    else issue_fwd(acc, s0 + Y[u], s0 + kWf3, kHid, kOutPad, false);
+    else issue_fwd(acc, s0 + X[u], s0 + kWf3, kHid, kOutPad, false);
     umma::commit(&mbar[u]);
   };
   auto wait = [&](int u) {
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const __grid_constant__ MlpTa
           tmem_row<kHid>(tbase, 64u * (uint32_t)u, h);
 #pragma unroll
           for (int j = 0; j < kHid; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
-          store_row(smem + ((l & 1) ? X[u] : Y[u]), t, kHid, h);
+          store_row(smem + X[u], t, kHid, h);
           ok = publish_and(ok);
           if (ok) issue(u, l + 1);
         } else {
@@ -767,7 +770,7 @@ cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = assign_ctas(ts, sm_count_mlp() * 2, 256);   // 2 x 100 KB of shared memory per SM
+  const int grid = assign_ctas(ts, sm_count_mlp() * 3, 256);   // 3 x 68 KB of shared memory per SM
   k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(ts);
   return cudaGetLastError();
 }

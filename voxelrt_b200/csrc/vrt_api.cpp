@@ -55,6 +55,7 @@ struct VrtCtx {
   cudaStream_t stream = nullptr;
   uint64_t budget = 0;   // 0 = unlimited
   uint64_t used = 0;
+  float* present_lut = nullptr;   // kPresentLut floats, built on the stream at creation
 };
 
 struct VrtScene {
@@ -184,7 +185,11 @@ int vrt_create(const VrtDeviceConfig* cfg, VrtCtx** out) {
   }
   e = cudaSetDevice(c->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c->present_lut, kPresentLut * sizeof(float));
+  if (e == cudaSuccess) e = launch_present_lut(c->present_lut, c->stream);
   if (e != cudaSuccess) {
+    if (c->present_lut) cudaFree(c->present_lut);
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return fail(VRT_ERR_CUDA, "context init: %s", cudaGetErrorString(e));
   }
@@ -199,6 +204,7 @@ int vrt_destroy(VrtCtx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
+  if (ctx->present_lut) cudaFree(ctx->present_lut);
   delete ctx;
   return VRT_OK;
 }
@@ -211,6 +217,28 @@ int vrt_ctx_synchronize(VrtCtx* ctx) {
 }
 
 uint64_t vrt_ctx_bytes_in_use(const VrtCtx* ctx) { return ctx ? ctx->used : 0; }
+
+int vrt_selftest_present(VrtCtx* ctx, uint64_t* mismatches, uint32_t* first_bits) {
+  if (!ctx || !mismatches || !first_bits) return fail(VRT_ERR_INVALID, "vrt_selftest_present: NULL argument");
+  if (int r = set_dev(ctx)) return r;
+  void* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, 16));
+  unsigned long long* bad = (unsigned long long*)d;
+  unsigned int* first = (unsigned int*)((char*)d + 8);
+  cudaError_t e = cudaMemsetAsync(bad, 0, 8, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(first, 0xff, 4, ctx->stream);
+  if (e == cudaSuccess) e = launch_present_check(ctx->present_lut, bad, first, ctx->stream);
+  unsigned long long hb = 0;
+  unsigned int hf = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, bad, 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hf, first, 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(VRT_ERR_CUDA, "vrt_selftest_present: %s", cudaGetErrorString(e));
+  *mismatches = hb;
+  *first_bits = hf;
+  return VRT_OK;
+}
 
 // ---------------------------------------------------------------------------
 // scenes
@@ -823,7 +851,7 @@ int vrt_pass_present(VrtSession* s, const VrtUniforms* u) {
   const bool denoise = (u->params0[2] & 2u) != 0u;
   bool f32;
   const void* fin = final_buf(s, parity_of(s), denoise, &f32);
-  CUDA_TRY(launch_present(*u, s->W, s->H, fin, f32, s->alb8, s->ldr, s->ctx->stream));
+  CUDA_TRY(launch_present(*u, s->W, s->H, fin, f32, s->alb8, s->ldr, s->ctx->present_lut, s->ctx->stream));
   s->launches++;
   s->last_denoise = denoise;
   return VRT_OK;
@@ -1219,7 +1247,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       uint32_t nl = 0;
       cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl,
-                                         cls.data(), (int)cls.size());
+                                         b->ctx->present_lut, cls.data(), (int)cls.size());
       cudaError_t e2 = cudaStreamEndCapture(st, &graph);
       if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1240,7 +1268,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
     CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches,
-                                cls.data(), (int)cls.size()));
+                                b->ctx->present_lut, cls.data(), (int)cls.size()));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
   for (int i = 0; i < m; i++) {

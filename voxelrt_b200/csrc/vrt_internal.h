@@ -137,7 +137,8 @@ struct CacheLaunch {
 // 3x a-trous, present.
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
-                               cudaStream_t st, uint32_t* launches, const CacheLaunch* cls = nullptr, int ncl = 0);
+                               cudaStream_t st, uint32_t* launches, const float* present_lut,
+                               const CacheLaunch* cls = nullptr, int ncl = 0);
 
 // Radiance-cache MLP kernels (k_mlp.cu).  q9: n x 9 floats (position in
 // metres, normal, albedo); y3: n x 3 target radiance; weights bf16 row-major.
@@ -240,8 +241,16 @@ cudaError_t launch_atrous_staged(int W, int H, const void* src, bool src_f32, co
                                  unsigned long long* err, cudaStream_t st, int rows = 0);
 cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const void* gbuf, void* dst, int step,
                           cudaStream_t st);
+// Present with the context's lookup table (kPresentLut 4-byte words: albedo
+// factor per byte, the code thresholds and windows, the scan's scratch), built
+// once per context by launch_present_lut.
+constexpr int kPresentLut = 256 + 257 + 257 + 512;
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
-                           const uint32_t* alb8, uint32_t* ldr, cudaStream_t st);
+                           const uint32_t* alb8, uint32_t* ldr, const float* lut, cudaStream_t st);
+cudaError_t launch_present_lut(float* lut, cudaStream_t st);
+// Counts the floats of the table's range where the table path and the exact
+// arithmetic give different codes (bad), and the smallest such bit pattern.
+cudaError_t launch_present_check(const float* lut, unsigned long long* bad, unsigned int* first, cudaStream_t st);
 
 // Reservoir flags of params2.x (common.wgsl:40-59).
 constexpr uint32_t kRfRestir = 1u, kRfTemporal = 2u, kRfSpatial = 4u, kRfPaired = 8u, kRfDupmap = 16u,
