@@ -38,23 +38,49 @@ __global__ void __launch_bounds__(256) k_atrous(int W, int H, const void* __rest
   dst[(size_t)py * W + px] = pack_h4(v.x, v.y, v.z, v.w);
 }
 
-// present.wgsl:40-55 as a compute pass writing a headless rgba8 buffer.
+// present.wgsl:40-55 as a compute pass writing a headless rgba8 buffer.  The
+// pass is per pixel and the buffers are dense, so each of the first n4
+// threads takes four consecutive pixels with 16-byte loads and stores; the
+// threads after them take the remaining P - 4 n4 pixels one each (n4 = 0
+// when a buffer is not 16-byte aligned).
 template <bool kFinF32>
-__global__ void __launch_bounds__(256) k_present(float exposure, int W, int H, const void* __restrict__ fin,
-                                                 const uint32_t* __restrict__ alb8, uint32_t* __restrict__ ldr,
-                                                 const float* __restrict__ lut) {
-  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
-  if (x >= W || y >= H) return;
-  const size_t p = (size_t)y * W + x;
-  ldr[p] = present_pixel(exposure, load_px(fin, kFinF32, p), __ldg(alb8 + p), lut);
+__global__ void __launch_bounds__(256) k_present(float exposure, uint32_t P, uint32_t n4,
+                                                 const void* __restrict__ fin, const uint32_t* __restrict__ alb8,
+                                                 uint32_t* __restrict__ ldr, const float* __restrict__ lut) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n4) {
+    float4 il[4];
+    if (kFinF32) {
+      const float4* f = reinterpret_cast<const float4*>(fin) + 4u * (size_t)i;
+#pragma unroll
+      for (int k = 0; k < 4; k++) il[k] = __ldg(f + k);
+    } else {
+      const uint4* f = reinterpret_cast<const uint4*>(fin) + 2u * (size_t)i;
+      const uint4 a = __ldg(f), b = __ldg(f + 1);
+      il[0] = unpack_h4(make_uint2(a.x, a.y));
+      il[1] = unpack_h4(make_uint2(a.z, a.w));
+      il[2] = unpack_h4(make_uint2(b.x, b.y));
+      il[3] = unpack_h4(make_uint2(b.z, b.w));
+    }
+    const uint4 al = __ldg(reinterpret_cast<const uint4*>(alb8) + i);
+    uint4 o;
+    o.x = present_pixel(exposure, il[0], al.x, lut);
+    o.y = present_pixel(exposure, il[1], al.y, lut);
+    o.z = present_pixel(exposure, il[2], al.z, lut);
+    o.w = present_pixel(exposure, il[3], al.w, lut);
+    reinterpret_cast<uint4*>(ldr)[i] = o;
+  } else {
+    const size_t p = 4u * (size_t)n4 + (i - n4);
+    if (p >= P) return;
+    ldr[p] = present_pixel(exposure, load_px(fin, kFinF32, p), __ldg(alb8 + p), lut);
+  }
 }
 
 // Building the present lookup table (image_core.cuh), step 1: every float of
 // [0, kPresentFastMax) through the exact arithmetic.  A thread walks a run of
 // kPresentScanRun consecutive bit patterns (ordered like the values they
 // encode) and, per stretch of equal codes, lowers the code's least bit
-// pattern and raises its greatest.
+// pattern (minb) and raises one past its greatest (maxb; 0: code not seen).
 constexpr uint32_t kPresentScanRun = 4096u;
 __global__ void __launch_bounds__(256) k_present_scan(unsigned int* __restrict__ minb, unsigned int* __restrict__ maxb) {
   const uint32_t end = kPresentFastMaxBits;
@@ -66,18 +92,19 @@ __global__ void __launch_bounds__(256) k_present_scan(unsigned int* __restrict__
     const uint32_t c = present_code_exact(__uint_as_float(b));
     if (c != code) {
       atomicMin(minb + code, start);
-      atomicMax(maxb + code, b - 1u);
+      atomicMax(maxb + code, b);
       code = c;
       start = b;
     }
   }
   atomicMin(minb + code, start);
-  atomicMax(maxb + code, b1 - 1u);
+  atomicMax(maxb + code, b1);
 }
 
 // Step 2 (256 threads): thread k forms the albedo factor of byte k, lo[k] as
 // the least bit pattern of any code >= k and hi[k] as one above the greatest
-// bit pattern of any code < k.
+// bit pattern of any code < k.  maxb holds one past a code's greatest bit
+// pattern, so the "not seen" 0 drops out of the maximum.
 __global__ void __launch_bounds__(256) k_present_lut(float* __restrict__ lut, const unsigned int* __restrict__ minb,
                                                      const unsigned int* __restrict__ maxb) {
   const int k = threadIdx.x;
@@ -86,17 +113,14 @@ __global__ void __launch_bounds__(256) k_present_lut(float* __restrict__ lut, co
   uint32_t lo = 0x7f800000u;                       // inf: no code >= k in the range
   for (int c = k; c < 256; c++)
     if (minb[c] < kPresentFastMaxBits) lo = min(lo, minb[c]);
-  uint32_t hi = 0u;
-  bool any = false;
-  for (int c = 0; c < k; c++)
-    if (maxb[c] != 0xffffffffu) { hi = max(hi, maxb[c] + 1u); any = true; }
+  uint32_t hi = 0u;                                // 0.0f: no code < k in the range
+  for (int c = 0; c < k; c++) hi = max(hi, maxb[c]);
   lut[kPresentLo + k] = __uint_as_float(lo);
-  lut[kPresentHi + k] = any ? __uint_as_float(hi) : 0.0f;
+  lut[kPresentHi + k] = __uint_as_float(hi);
   if (k == 0) {
     lut[kPresentLo + 256] = __int_as_float(0x7f800000);
     uint32_t h = 0u;
-    for (int c = 0; c < 256; c++)
-      if (maxb[c] != 0xffffffffu) h = max(h, maxb[c] + 1u);
+    for (int c = 0; c < 256; c++) h = max(h, maxb[c]);
     lut[kPresentHi + 256] = __uint_as_float(h);
   }
 }
@@ -213,9 +237,14 @@ cudaError_t launch_atrous(int W, int H, const void* src, bool src_f32, const voi
 
 cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, bool fin_f32,
                            const uint32_t* alb8, uint32_t* ldr, const float* lut, cudaStream_t st) {
-  dim3 grid((W + 31) / 32, (H + 7) / 8);
-  if (fin_f32) k_present<true><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr, lut);
-  else k_present<false><<<grid, 256, 0, st>>>(u.params1[2], W, H, fin, alb8, ldr, lut);
+  const uint32_t P = (uint32_t)W * (uint32_t)H;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(fin) | reinterpret_cast<uintptr_t>(alb8) |
+                         reinterpret_cast<uintptr_t>(ldr)) & 15u) == 0u;
+  const uint32_t n4 = aligned ? P >> 2 : 0u;
+  const uint32_t threads = n4 + (P - 4u * n4);
+  const unsigned blocks = (threads + 255u) / 256u;
+  if (fin_f32) k_present<true><<<blocks, 256, 0, st>>>(u.params1[2], P, n4, fin, alb8, ldr, lut);
+  else k_present<false><<<blocks, 256, 0, st>>>(u.params1[2], P, n4, fin, alb8, ldr, lut);
   return cudaGetLastError();
 }
 
@@ -223,7 +252,7 @@ cudaError_t launch_present_lut(float* lut, cudaStream_t st) {
   unsigned int* minb = reinterpret_cast<unsigned int*>(lut + kPresentHi + 257);
   unsigned int* maxb = minb + 256;
   cudaError_t e = cudaMemsetAsync(minb, 0x7f, 256 * sizeof(unsigned int), st);   // 0x7f7f7f7f: "none"
-  if (e == cudaSuccess) e = cudaMemsetAsync(maxb, 0xff, 256 * sizeof(unsigned int), st);   // "none"
+  if (e == cudaSuccess) e = cudaMemsetAsync(maxb, 0, 256 * sizeof(unsigned int), st);     // "not seen"
   if (e != cudaSuccess) return e;
   const uint32_t runs = (kPresentFastMaxBits + kPresentScanRun - 1u) / kPresentScanRun;
   k_present_scan<<<(runs + 255u) / 256u, 256, 0, st>>>(minb, maxb);

@@ -186,6 +186,25 @@ __device__ __forceinline__ void store_row(uint8_t* tile, int row, int C, const f
     *reinterpret_cast<uint4*>(tile + umma::canon_off(row, 8 * cg, C)) = pack8(v + 8 * cg);
 }
 
+// pack8 of max(v, 0): the conversion's .relu form clamps negative values to
+// zero in the same instruction (bf16 rounding keeps the sign, so the result
+// equals rounding after the ReLU).
+__device__ __forceinline__ uint4 pack8_relu(const float* v) {
+  uint4 r;
+  uint32_t* w = &r.x;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(w[i]) : "f"(v[2 * i + 1]), "f"(v[2 * i]));
+  return r;
+}
+
+// store_row of ReLU(v).
+__device__ __forceinline__ void store_row_relu(uint8_t* tile, int row, int C, const float* v) {
+#pragma unroll
+  for (int cg = 0; cg < C / 8; cg++)
+    *reinterpret_cast<uint4*>(tile + umma::canon_off(row, 8 * cg, C)) = pack8_relu(v + 8 * cg);
+}
+
 // The bf16 weight copy is kept in global memory as the kernels' shared-memory
 // image of the weights: for each layer W^T (rows N_out, columns K_in) in the
 // canonical no-swizzle layout at byte offset kWf<l>, kWEnd bytes in all.
@@ -474,9 +493,7 @@ __global__ void __launch_bounds__(128, 3) k_mlp_infer(const __grid_constant__ Ml
         if (l < 3) {
           float h[kHid];
           tmem_row<kHid>(tbase, 64u * (uint32_t)u, h);
-#pragma unroll
-          for (int j = 0; j < kHid; j++) h[j] = h[j] > 0.0f ? h[j] : 0.0f;
-          store_row(smem + X[u], t, kHid, h);
+          store_row_relu(smem + X[u], t, kHid, h);
           ok = publish_and(ok);
           if (ok) issue(u, l + 1);
         } else {
