@@ -123,11 +123,13 @@ constexpr int kGA0 = 0, kGA1 = kGA0 + 128 * kIn * 2, kGA2 = kGA1 + 128 * kHid * 
 constexpr int kGDY = kGA3 + 128 * kHid * 2, kGStride = kGDY + 128 * kHid * 2;   // 84 KB per group
 constexpr int kGBase = kWEnd, kGEnd = kGBase + 2 * kGStride;
 constexpr int kTrainSmem = kGEnd + 1024;   // slack: MN-major views read up to 1 KB past a tile
-// inference kernel: forward weights + per tile (two in flight) one operand
-// tile X: the 80-column input, then each hidden layer's 64 columns written
-// over it once the MMAs that read it have completed
-constexpr int kIX0 = kWEnd, kIX1 = kIX0 + 128 * kIn * 2, kIEnd = kIX1 + 128 * kIn * 2;
-constexpr int kInferSmem = kIEnd;   // 68 KB: three CTAs per SM
+// inference kernel: forward weights + per tile (two groups of threads, two
+// tiles in flight each) one operand tile X: the 80-column input, then each
+// hidden layer's 64 columns written over it once the MMAs that read it have
+// completed
+constexpr int kITile = 128 * kIn * 2;
+constexpr int kIX = kWEnd, kIEnd = kIX + 4 * kITile;
+constexpr int kInferSmem = kIEnd;   // 108 KB: two CTAs per SM
 
 // TMEM columns (fp32): layer outputs / input gradients of group g at 64 g,
 // weight gradients accumulated over all of a CTA's samples at kTW*
@@ -406,83 +408,108 @@ __device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
   return j;
 }
 
+// Barrier of the 128 threads of group g (named barrier 1 + g) that also
+// agrees on `ok` across them, with the handoff fences of publish_and.
+__device__ __forceinline__ bool group_publish_and(int g, bool ok) {
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  uint32_t all;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(all)
+      : "r"(ok ? 1u : 0u), "r"(1 + g)
+      : "memory");
+  umma::fence_after_sync();
+  return all != 0u;
+}
+
 // Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set.
-// A CTA of 128 threads keeps two 128-query tiles in flight, each with its own
-// TMEM accumulator (columns 64u..64u+63), its own operand tile and its own
-// mbarrier: while the tensor core runs one tile's layer, the threads unpack
-// the other tile's previous layer (TMEM load, ReLU, bf16 pack into the next
-// operand tile), so the MMA latency hides behind the epilogue work.  A layer's
-// output overwrites its input tile: every thread waits for the layer's MMA
-// completion (which covers the MMAs' shared-memory reads) before it stores,
-// so one tile per query block is enough and three CTAs fit on an SM.  Thread
-// r owns row r of both tiles.  A task's CTAs stride over its tile pairs.
-__global__ void __launch_bounds__(128, 3) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
+// A CTA of 256 threads is two groups of 128 (threads 128 g .. 128 g + 127)
+// that share the weights in shared memory and otherwise run independently,
+// synchronising on their own named barrier.  Each group keeps two 128-query
+// tiles in flight, each with its own TMEM accumulator (columns 64 (2g + u)),
+// its own operand tile and its own mbarrier: while the tensor core runs one
+// tile's layer, the group's threads unpack the other tile's previous layer
+// (TMEM load, ReLU, bf16 pack into the next operand tile), so the MMA latency
+// hides behind the epilogue work, and the other group's tiles fill the
+// tensor core's remaining gaps.  A layer's output overwrites its input tile:
+// every thread waits for the layer's MMA completion (which covers the MMAs'
+// shared-memory reads) before it stores.  Thread r of a group owns row r of
+// its tiles; the first thread of each group issues the group's MMAs.  The
+// groups of a task's CTAs stride over its tile pairs.
+__global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
   using namespace mlp;
   const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
   int n = tk.n_max;
   if (tk.n_dev) n = min(*tk.n_dev, n);
   const int tiles = (n + 127) / 128;
   const int cb = blockIdx.x - tk.cta0;
-  if (cb >= tiles) return;   // nothing for this CTA (before any TMEM allocation)
+  if (2 * cb >= tiles) return;   // nothing for this CTA (before any TMEM allocation)
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t mbar[2];
+  __shared__ uint64_t mbar[4];
   __shared__ uint32_t tmem_base;
-  const int t = threadIdx.x, warp = t >> 5;
-  if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
-  if (t == 0) { umma::mbar_init(&mbar[0], 1); umma::mbar_init(&mbar[1], 1); }
+  const int warp = threadIdx.x >> 5, g = threadIdx.x >> 7, t = threadIdx.x & 127;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 256);
+  if (threadIdx.x < 4) umma::mbar_init(&mbar[threadIdx.x], 1);
   load_weights(smem, tk.wb);
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   const uint32_t s0 = umma::smem_u32(smem);
-  // per tile: X (input, 80 columns; then each hidden layer, 64 columns)
-  const int X[2] = {kIX0, kIX1};
+  // this group's tiles: X (input, 80 columns; then each hidden layer, 64 columns)
+  const int X[2] = {kIX + (2 * g) * kITile, kIX + (2 * g + 1) * kITile};
+  const uint32_t acc[2] = {tbase + 64u * (uint32_t)(2 * g), tbase + 64u * (uint32_t)(2 * g + 1)};
+  uint64_t* mb = mbar + 2 * g;
   uint32_t phase[2] = {0u, 0u};
   bool ok = true;
-  const int stride = 2 * tk.ctas;          // a CTA's pairs: tiles (pt, pt + ctas), pt = cb + k stride
+  const int vctas = 2 * tk.ctas;           // groups of the task: pairs (pt, pt + vctas), pt = vb + k stride
+  const int vb = 2 * cb + g;
+  const int stride = 2 * vctas;
   float q[2][9];
   auto fetch = [&](int pair_tile) {
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      const int idx = (pair_tile + u * tk.ctas) * 128 + t;
+      const int idx = (pair_tile + u * vctas) * 128 + t;
       if (idx < n) {
 #pragma unroll
         for (int j = 0; j < 9; j++) q[u][j] = __ldg(tk.q9 + (size_t)idx * 9 + j);
       }
     }
   };
-  // tensor-core work of layer l of tile u (thread 0), completion on mbar[u]
+  // tensor-core work of layer l of tile u (the group's first thread), completion on mb[u]
   auto issue = [&](int u, int l) {
     if (t != 0) return;
-    const uint32_t acc = tbase + 64u * (uint32_t)u;
-    if (l == 0) issue_fwd(acc, s0 + X[u], s0 + kWf0, kIn, kHid, false);
-    else if (l == 1) issue_fwd(acc, s0 + X[u], s0 + kWf1, kHid, kHid, false);
-    else if (l == 2) issue_fwd(acc, s0 + X[u], s0 + kWf2, kHid, kHid, false);
-    else issue_fwd(acc, s0 + X[u], s0 + kWf3, kHid, kOutPad, false);
-    umma::commit(&mbar[u]);
+    if (l == 0) issue_fwd(acc[u], s0 + X[u], s0 + kWf0, kIn, kHid, false);
+    else if (l == 1) issue_fwd(acc[u], s0 + X[u], s0 + kWf1, kHid, kHid, false);
+    else if (l == 2) issue_fwd(acc[u], s0 + X[u], s0 + kWf2, kHid, kHid, false);
+    else issue_fwd(acc[u], s0 + X[u], s0 + kWf3, kHid, kOutPad, false);
+    umma::commit(&mb[u]);
   };
   auto wait = [&](int u) {
-    ok = umma::mbar_wait(&mbar[u], phase[u], kMbarSpin) && ok;
+    ok = umma::mbar_wait(&mb[u], phase[u], kMbarSpin) && ok;
     phase[u] ^= 1u;
     umma::fence_after_sync();
   };
-  fetch(cb);
-  for (int pt = cb; pt < tiles && ok; pt += stride) {
+  if (vb < tiles) fetch(vb);
+  for (int pt = vb; pt < tiles && ok; pt += stride) {
     int idx[2];
     float qq[2][9];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      idx[u] = (pt + u * tk.ctas) * 128 + t;
+      idx[u] = (pt + u * vctas) * 128 + t;
 #pragma unroll
       for (int j = 0; j < 9; j++) qq[u][j] = q[u][j];
     }
     // stage tile 0 and start its first layer; stage tile 1 while it runs
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
-    ok = publish_and(ok);
+    ok = group_publish_and(g, ok);
     if (ok) issue(0, 0);
     stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
-    ok = publish_and(ok);
+    ok = group_publish_and(g, ok);
     if (ok) issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
@@ -492,25 +519,25 @@ __global__ void __launch_bounds__(128, 3) k_mlp_infer(const __grid_constant__ Ml
         wait(u);
         if (l < 3) {
           float h[kHid];
-          tmem_row<kHid>(tbase, 64u * (uint32_t)u, h);
+          tmem_row<kHid>(acc[u], 0u, h);
           store_row_relu(smem + X[u], t, kHid, h);
-          ok = publish_and(ok);
+          ok = group_publish_and(g, ok);
           if (ok) issue(u, l + 1);
         } else {
           float o[kOutPad];
-          tmem_row<kOutPad>(tbase, 64u * (uint32_t)u, o);
+          tmem_row<kOutPad>(acc[u], 0u, o);
           if (ok && idx[u] < n)
             for (int j = 0; j < kOut; j++) tk.out3[(size_t)idx[u] * 3 + j] = o[j];
         }
       }
     }
-    // every thread has read this pair's last TMEM rows before the next pair's MMAs
-    ok = publish_and(ok);
+    // every thread of the group has read this pair's last TMEM rows before its next MMAs
+    ok = group_publish_and(g, ok);
   }
   if (!ok && t == 0) atomicExch(tk.err, 1);
   umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_free(tbase, 128);
+  if (warp == 0) umma::tmem_free(tbase, 256);
 }
 
 // One gradient pass: per-CTA partial dW (sum over the CTA's samples) of the
@@ -787,8 +814,8 @@ cudaError_t mlp_infer_tasks(MlpTaskSet& ts, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = assign_ctas(ts, sm_count_mlp() * 3, 256);   // 3 x 68 KB of shared memory per SM
-  k_mlp_infer<<<grid, 128, mlp::kInferSmem, st>>>(ts);
+  const int grid = assign_ctas(ts, sm_count_mlp() * 2, 512);   // 2 x 108 KB of shared memory per SM
+  k_mlp_infer<<<grid, 256, mlp::kInferSmem, st>>>(ts);
   return cudaGetLastError();
 }
 
