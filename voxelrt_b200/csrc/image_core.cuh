@@ -192,21 +192,34 @@ constexpr float kPresentFastMax = 8.0f;
 constexpr uint32_t kPresentFastMaxBits = 0x41000000u;   // bit pattern of kPresentFastMax
 constexpr int kPresentLo = 256, kPresentHi = 513;
 
-// present_code_exact(v) through the table: an estimate from the hardware's
-// approximate divide / log2 / exp2 starts a walk along lo[] that ends at the
-// largest k with lo[k] <= v; values inside that code's window [lo[k], hi[k]),
-// outside [0, kPresentFastMax) or NaN take the exact arithmetic.
+// present_code_exact out of line, for the table path's rare fallbacks (keeps
+// the unrolled per-pixel code small).
+__device__ __noinline__ uint32_t present_code_slow(float v) { return present_code_exact(v); }
+
+// present_code_exact(v) through the table: the code is the largest k with
+// lo[k] <= v unless v lies in that code's window [lo[k], hi[k]).  An estimate
+// c0 from the hardware's approximate divide / log2 / exp2, held to [1, 254],
+// is within one code of the answer; the seven table words around it are read
+// at once (no chain of dependent loads), and the answer is c0 - 1, c0 or
+// c0 + 1.  Values whose code is further from the estimate, values in a
+// window, values outside [0, kPresentFastMax) and NaN take the exact
+// arithmetic.
 VRT_DI uint32_t present_code(float v, const float* __restrict__ lut) {
-  if (!(v >= 0.0f && v < kPresentFastMax)) return present_code_exact(v);
+  if (!(v >= 0.0f && v < kPresentFastMax)) return present_code_slow(v);
   const float* lo = lut + kPresentLo;
+  const float* hi = lut + kPresentHi;
   const float num = v * __fmaf_rn(2.51f, v, 0.03f);
   const float den = __fmaf_rn(v, __fmaf_rn(2.43f, v, 0.59f), 0.14f);
   const float t = fminf(fmaxf(__fdividef(num, den), 0.0f), 1.0f);
-  int c = __float2int_rn(255.0f * __powf(t, 0.454545468f));
-  c = min(max(c, 0), 255);
-  while (c > 0 && v < __ldg(lo + c)) c--;
-  while (c < 255 && v >= __ldg(lo + c + 1)) c++;
-  if (v < __ldg(lut + kPresentHi + c)) return present_code_exact(v);
+  const int c0 = min(max(__float2int_rn(255.0f * __powf(t, 0.454545468f)), 1), 254);
+  const float lm = __ldg(lo + c0 - 1), l0 = __ldg(lo + c0), l1 = __ldg(lo + c0 + 1), l2 = __ldg(lo + c0 + 2);
+  const float hm = __ldg(hi + c0 - 1), h0 = __ldg(hi + c0), h1 = __ldg(hi + c0 + 1);
+  int c = c0;
+  float h = h0;
+  bool far = false;
+  if (v < l0) { c = c0 - 1; h = hm; far = v < lm; }
+  else if (v >= l1) { c = c0 + 1; h = h1; far = v >= l2; }
+  if (far || v < h) return present_code_slow(v);
   return (uint32_t)c;
 }
 
