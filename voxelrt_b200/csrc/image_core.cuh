@@ -194,7 +194,7 @@ constexpr int kPresentLo = 256, kPresentHi = 513;
 
 // present_code_exact out of line, for the table path's rare fallbacks (keeps
 // the unrolled per-pixel code small).
-__device__ __noinline__ uint32_t present_code_slow(float v) { return present_code_exact(v); }
+static __device__ __noinline__ uint32_t present_code_slow(float v) { return present_code_exact(v); }
 
 // present_code_exact(v) through the table: the code is the largest k with
 // lo[k] <= v unless v lies in that code's window [lo[k], hi[k]).  An estimate
