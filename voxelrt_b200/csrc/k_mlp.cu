@@ -495,7 +495,12 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
     umma::fence_after_sync();
   };
   if (vb < tiles) fetch(vb);
-  for (int pt = vb; pt < tiles && ok; pt += stride) {
+  // The loop runs while the group agrees on `ok` (every exit is decided on a
+  // value its barrier made uniform).  No barrier closes a pair: the next
+  // pair's first MMA is issued after the staging barrier, which each thread
+  // reaches after reading its last TMEM rows, and each thread writes the next
+  // input tile only after it has seen the MMAs that read the tile complete.
+  for (int pt = vb; pt < tiles; pt += stride) {
     int idx[2];
     float qq[2][9];
 #pragma unroll
@@ -507,10 +512,12 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
     // stage tile 0 and start its first layer; stage tile 1 while it runs
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
     ok = group_publish_and(g, ok);
-    if (ok) issue(0, 0);
+    if (!ok) break;
+    issue(0, 0);
     stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
     ok = group_publish_and(g, ok);
-    if (ok) issue(1, 0);
+    if (!ok) break;
+    issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
     for (int l = 0; l < 4 && ok; l++) {
@@ -531,9 +538,8 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
         }
       }
     }
-    // every thread of the group has read this pair's last TMEM rows before its next MMAs
-    ok = group_publish_and(g, ok);
   }
+  ok = group_publish_and(g, ok);           // the last pair's output waits, agreed
   if (!ok && t == 0) atomicExch(tk.err, 1);
   umma::fence_before_sync();
   __syncthreads();
