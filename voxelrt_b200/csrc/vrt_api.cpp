@@ -528,7 +528,7 @@ int vrt_session_get_tuning(VrtSession* s, VrtTuning* t) {
 int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5 ||
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 8 ||
       (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8) || t->tail_wave < -1 || t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   s->tune.refill_min = t->refill_min ? t->refill_min : 8;
@@ -1156,7 +1156,7 @@ int vrt_batch_set_graph(VrtBatch* b, int enable) {
 int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
   if (!b || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
-      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 5 ||
+      t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 8 ||
       t->tail_wave < -1 || t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   b->tune.refill_min = t->refill_min ? t->refill_min : 8;

@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(256) k_wf_generate(J jobs, uint32_t P, WfDev b
 // bookkeeping (idle-lane ballot, refill, drain check).  kVarMaxT: shadow rays
 // carry their own maxT in R2.w (otherwise every ray ends at 1e4 m, the plain
 // path's bound, and the tracer keeps its register budget).
-template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT>
+template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT, int kUnroll = kSteps>
 __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wave, int implicit_n,
                                                               int refill_min, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
     }
     passes++;
     if (active) {
-#pragma unroll
+#pragma unroll kUnroll
       for (int k = 0; k < kSteps; k++)
         if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
@@ -1198,10 +1198,10 @@ cudaError_t launch_cache_post(const J& jobs, const WfDev& b, const CacheLaunch* 
   return cudaSuccess;
 }
 
-template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT>
+template <class J, bool kSmem, int kSteps, int kMinB, bool kVarMaxT, int kUnroll = kSteps>
 cudaError_t wf_launch_trace(const J& jobs, int smem, int blocks_per_sm, int sms, const WfDev& b, int w,
                             int implicit_n, int refill, unsigned long long* stats, cudaStream_t st) {
-  auto* fn = k_wf_trace<J, kSmem, kSteps, kMinB, kVarMaxT>;
+  auto* fn = k_wf_trace<J, kSmem, kSteps, kMinB, kVarMaxT, kUnroll>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -1243,6 +1243,10 @@ cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int 
     case 3: return wf_launch_trace<J, kSmem, 4, 4, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 4: return wf_launch_trace<J, kSmem, 2, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 5: return wf_launch_trace<J, kSmem, 1, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    // the default shape with the step loop unrolled 1, 2 or 4 times instead of 8 (smaller code)
+    case 6: return wf_launch_trace<J, kSmem, 8, 5, false, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 7: return wf_launch_trace<J, kSmem, 8, 5, false, 2>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
+    case 8: return wf_launch_trace<J, kSmem, 8, 5, false, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     default: return wf_launch_trace<J, kSmem, 8, 5, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
   }
 }
