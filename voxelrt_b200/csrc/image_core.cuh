@@ -179,10 +179,10 @@ VRT_DI uint32_t present_code_exact(float v) {
 // Present lookup table (kPresentLut words per device context):
 //   [0, 256)    the albedo factor sqrtAlb^2 of each rgba8 byte, (b / 255)^2 as
 //               the shader forms it;
-//   [256, 513)  lo[0..256]: lo[k] = the least float of [0, kPresentFastMax)
-//               whose exact code is >= k (inf if none; non-decreasing in k);
-//   [513, 770)  hi[0..256]: the float just above the greatest v of the range
-//               whose exact code is < k (0 for k = 0);
+//   [256, 770)  (lo[k], hi[k]) pairs for k = 0..256: lo[k] = the least float of
+//               [0, kPresentFastMax) whose exact code is >= k (inf if none;
+//               non-decreasing in k); hi[k] = the float just above the
+//               greatest v of the range whose exact code is < k (0 for k = 0);
 // then scratch for the scan that builds them.  The exact code is almost but
 // not quite non-decreasing in v: num / den rounds so that at 133 values next
 // to a code step it drops back by one.  Every v >= hi[k] has a code >= k and
@@ -190,35 +190,46 @@ VRT_DI uint32_t present_code_exact(float v) {
 // code is the largest k with lo[k] <= v.
 constexpr float kPresentFastMax = 8.0f;
 constexpr uint32_t kPresentFastMaxBits = 0x41000000u;   // bit pattern of kPresentFastMax
-constexpr int kPresentLo = 256, kPresentHi = 513;
+constexpr int kPresentLoHi = 256;                        // float offset of the (lo, hi) pairs
 
 // present_code_exact out of line, for the table path's rare fallbacks (keeps
 // the unrolled per-pixel code small).
 static __device__ __noinline__ uint32_t present_code_slow(float v) { return present_code_exact(v); }
 
+// Approximate x^(1/2.2) for the code estimate: the hardware's log2 and exp2
+// with denormal inputs and results flushed to zero (a flushed estimate only
+// starts the table search elsewhere; the table decides the code).
+VRT_DI float present_gamma_estimate(float x) {
+  float l, r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l * 0.454545468f));
+  return r;
+}
+
 // present_code_exact(v) through the table: the code is the largest k with
 // lo[k] <= v unless v lies in that code's window [lo[k], hi[k]).  An estimate
-// c0 from the hardware's approximate divide / log2 / exp2, held to [1, 254],
-// is within one code of the answer; the seven table words around it are read
-// at once (no chain of dependent loads), and the answer is c0 - 1, c0 or
-// c0 + 1.  Values whose code is further from the estimate, values in a
+// c0 from the hardware's approximate reciprocal / log2 / exp2, held to
+// [1, 254], is within one code of the answer; the table entries c0 - 1 .. c0 + 2
+// are read at once (no chain of dependent loads), and the answer is c0 - 1, c0
+// or c0 + 1.  Values whose code is further from the estimate, values in a
 // window, values outside [0, kPresentFastMax) and NaN take the exact
 // arithmetic.
 VRT_DI uint32_t present_code(float v, const float* __restrict__ lut) {
   if (!(v >= 0.0f && v < kPresentFastMax)) return present_code_slow(v);
-  const float* lo = lut + kPresentLo;
-  const float* hi = lut + kPresentHi;
+  const float2* lh = reinterpret_cast<const float2*>(lut + kPresentLoHi);
   const float num = v * __fmaf_rn(2.51f, v, 0.03f);
   const float den = __fmaf_rn(v, __fmaf_rn(2.43f, v, 0.59f), 0.14f);
-  const float t = fminf(fmaxf(__fdividef(num, den), 0.0f), 1.0f);
-  const int c0 = min(max(__float2int_rn(255.0f * __powf(t, 0.454545468f)), 1), 254);
-  const float lm = __ldg(lo + c0 - 1), l0 = __ldg(lo + c0), l1 = __ldg(lo + c0 + 1), l2 = __ldg(lo + c0 + 2);
-  const float hm = __ldg(hi + c0 - 1), h0 = __ldg(hi + c0), h1 = __ldg(hi + c0 + 1);
+  float rden;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rden) : "f"(den));
+  const float t = fminf(fmaxf(num * rden, 0.0f), 1.0f);
+  const int c0 = min(max(__float2int_rn(255.0f * present_gamma_estimate(t)), 1), 254);
+  const float2 em = __ldg(lh + c0 - 1), e0 = __ldg(lh + c0), e1 = __ldg(lh + c0 + 1);
+  const float l2 = __ldg(lut + kPresentLoHi + 2 * (c0 + 2));
   int c = c0;
-  float h = h0;
+  float h = e0.y;
   bool far = false;
-  if (v < l0) { c = c0 - 1; h = hm; far = v < lm; }
-  else if (v >= l1) { c = c0 + 1; h = h1; far = v >= l2; }
+  if (v < e0.x) { c = c0 - 1; h = em.y; far = v < em.x; }
+  else if (v >= e1.x) { c = c0 + 1; h = e1.y; far = v >= l2; }
   if (far || v < h) return present_code_slow(v);
   return (uint32_t)c;
 }

@@ -115,13 +115,13 @@ __global__ void __launch_bounds__(256) k_present_lut(float* __restrict__ lut, co
     if (minb[c] < kPresentFastMaxBits) lo = min(lo, minb[c]);
   uint32_t hi = 0u;                                // 0.0f: no code < k in the range
   for (int c = 0; c < k; c++) hi = max(hi, maxb[c]);
-  lut[kPresentLo + k] = __uint_as_float(lo);
-  lut[kPresentHi + k] = __uint_as_float(hi);
+  lut[kPresentLoHi + 2 * k] = __uint_as_float(lo);
+  lut[kPresentLoHi + 2 * k + 1] = __uint_as_float(hi);
   if (k == 0) {
-    lut[kPresentLo + 256] = __int_as_float(0x7f800000);
+    lut[kPresentLoHi + 2 * 256] = __int_as_float(0x7f800000);
     uint32_t h = 0u;
     for (int c = 0; c < 256; c++) h = max(h, maxb[c]);
-    lut[kPresentHi + 256] = __uint_as_float(h);
+    lut[kPresentLoHi + 2 * 256 + 1] = __uint_as_float(h);
   }
 }
 
@@ -249,7 +249,7 @@ cudaError_t launch_present(const VrtUniforms& u, int W, int H, const void* fin, 
 }
 
 cudaError_t launch_present_lut(float* lut, cudaStream_t st) {
-  unsigned int* minb = reinterpret_cast<unsigned int*>(lut + kPresentHi + 257);
+  unsigned int* minb = reinterpret_cast<unsigned int*>(lut + kPresentLoHi + 2 * 257);
   unsigned int* maxb = minb + 256;
   cudaError_t e = cudaMemsetAsync(minb, 0x7f, 256 * sizeof(unsigned int), st);   // 0x7f7f7f7f: "none"
   if (e == cudaSuccess) e = cudaMemsetAsync(maxb, 0, 256 * sizeof(unsigned int), st);     // "not seen"

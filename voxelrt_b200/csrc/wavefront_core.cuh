@@ -456,30 +456,6 @@ VRT_DI void cache_emit_samples(const CacheDev& c, bool fin, uint32_t ti, F3 rfin
   cache_write_samples(c, ti, nrec, slot, rfin);
 }
 
-// cache_emit_samples for lanes that reach it together from divergent code,
-// each with a finished training path: lanes of the warp that share a sample
-// buffer take their slots from one atomicAdd (prefix of the record counts,
-// which are below 16, from four ballots).
-VRT_DI void cache_emit_samples_lane(const CacheDev& c, uint32_t ti, F3 rfin) {
-  const int nrec = c.rec_n[ti];
-  const unsigned m = __activemask();
-  const unsigned grp = __match_any_sync(m, (unsigned long long)c.cand_count);
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = grp & ((1u << lane) - 1u);
-  int before = 0, total = 0;
-#pragma unroll
-  for (int bit = 0; bit < 4; bit++) {
-    const unsigned bb = __ballot_sync(grp, ((nrec >> bit) & 1) != 0);
-    before += __popc(bb & lt) << bit;
-    total += __popc(bb) << bit;
-  }
-  const int leader = __ffs(grp) - 1;
-  int base = 0;
-  if (lane == leader && total > 0) base = atomicAdd(c.cand_count, total);
-  base = __shfl_sync(grp, base, leader);
-  cache_write_samples(c, ti, nrec, base + before, rfin);
-}
-
 // Appends a cache query of path g at its vertex 1.  All threads of the block
 // call it; one atomic per block when its queries go to one job's buffer.
 VRT_DI void cache_emit_query(const CacheDev& c, bool q, uint32_t g, F3 pos, F3 n, F3 alb) {
@@ -899,18 +875,18 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
 }
 
 // The tail of a frame whose remaining paths are few -- the radiance cache's
-// training paths after every other path ended at its first bounce: each lane
-// finishes paths of wave `wave`'s active list one at a time, tracing their
-// pending shadow and bounce rays with the same resumable DDA the queue tracer
-// runs (FlatDDA: same walk, hits and counters) and shading each vertex as
-// k_wf_shade does, until the path ends; then it takes the next path.  The
-// lanes of a warp step their walks together and each shades when its own ray
-// ends, so a warp waits for its slowest path, not for the slowest ray of every
-// bounce.  A per-wave form would launch a trace and a shade kernel for every
-// remaining bounce, each waiting for the slowest of ~10^5 latency-bound walks.
-// Same per-path arithmetic and RNG draws, so the same image; the radiance
-// gathered by a shadow ray goes back to the path state before the bounce ray,
-// as the wave kernels keep it.
+// training paths after every other path ended at its first bounce: one
+// thread finishes each path of wave `wave`'s active list, tracing its pending
+// shadow and bounce rays with the same resumable DDA the queue tracer runs
+// (FlatDDA: same walk, hits and counters) and shading each vertex as
+// k_wf_shade does, until the path ends.  The per-wave form would launch a
+// trace and a shade kernel for every remaining bounce, each waiting for the
+// slowest of ~10^5 latency-bound walks; here each path runs its own
+// sequence.  Same per-path arithmetic and RNG draws, so the same image.
+// (A per-lane state machine -- lanes stepping their walks together, each
+// shading when its own ray ends and then taking the next path -- ran 447
+// against 305 us per 1080p cache frame: some lane shades in nearly every pass,
+// so the warp runs the shading code far more often than once per bounce.)
 template <class J, bool kSmem>
 __global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
@@ -920,128 +896,79 @@ __global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, u
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) s_occ[i] = __ldg(S0.bits + i);
     __syncthreads();
   }
-  constexpr int kIdle = 0, kShadow = 1, kBounce = 2;
-  constexpr int kSteps = 8;
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
+  const bool any_cache = jobs.any_cache();
   const int n = b.ctr[4 * wave + 2];
   const uint32_t* list = active_of(b, wave);
-  int* head = b.ctr + 4 * wave + 1;   // this wave's trace-queue head: no trace launch of the wave uses it
+  const int stride = gridDim.x * blockDim.x;
   DCount c{0u, 0u, 0u, 0u};
-  FlatDDA d;
-  F3 rd = f3(0.0f, 0.0f, 0.0f);
-  uint32_t g = 0u;
-  int w = wave, phase = kIdle;
-  bool setup = false, drained = false;
-  while (true) {
-    const unsigned idle = __ballot_sync(full, phase == kIdle && !setup);
-    if (!drained && idle) {
-      const int nidle = __popc(idle);
-      int base = 0;
-      if (lane == 0) base = atomicAdd(head, nidle);
-      base = __shfl_sync(full, base, 0);
-      if (base + nidle >= n) drained = true;
-      if ((idle >> lane) & 1u) {
-        const int slot = base + __popc(idle & ((1u << lane) - 1u));
-        if (slot < n) {
-          g = list[slot];
-          w = wave;
-          setup = true;
-        }
-      }
-    }
-    if (!__any_sync(full, phase != kIdle || setup)) {
-      if (drained) break;
-      continue;
-    }
-    const int j = jobs.job_of(g);
-    const DScene S = jobs.scene(j);
-    const uint32_t* occ = kSmem ? s_occ : S.bits;
-    bool fin = false;
-    if (setup) {   // the pending rays of the path's previous vertex
-      setup = false;
-      const uint32_t flags = __float_as_uint(b.S2[g].w);
-      const F3 surf = xyz(b.R0[g]);
-      if (flags & kFlagShadow) {
-        const float4 r2 = b.R2[g];
-        rd = xyz(r2);
-        d.init(S, surf, rd, r2.w);
-        c.rays++;
-        phase = kShadow;
-      } else if (!(flags & kFlagTerminal)) {
-        rd = xyz(b.R1[g]);
-        d.init(S, surf, rd, 1e4f);
-        c.rays++;
-        phase = kBounce;
-      } else {
-        fin = true;
-      }
-    }
-    if (phase != kIdle) {
-#pragma unroll
-      for (int k = 0; k < kSteps; k++)
-        if (!d.done()) d.step(S, occ, rd, c);
-      if (d.done()) {
-        d.finish(S, c);
-        const uint32_t flags = __float_as_uint(b.S2[g].w);
-        if (phase == kShadow) {
-          if (!(d.tHit >= 0.0f)) {
-            const float4 s0 = b.S0[g];
-            const F3 r = xyz(s0) + xyz(b.S2[g]);
-            b.S0[g] = make_float4(r.x, r.y, r.z, s0.w);
-          }
-          if (flags & kFlagTerminal) {
-            phase = kIdle;
-            fin = true;
-          } else {
-            rd = xyz(b.R1[g]);
-            d.init(S, xyz(b.R0[g]), rd, 1e4f);
-            c.rays++;
-            phase = kBounce;
-          }
-        } else {
-          phase = kIdle;
-          const float4 s0 = b.S0[g];
-          const float4 s1 = b.S1[g];
-          F3 radiance = xyz(s0);
-          F3 tp = xyz(s1);
-          if (d.tHit < 0.0f) {
-            radiance = radiance + tp * sky_color(jobs.uni(j), rd, false);
-            b.S0[g] = make_float4(radiance.x, radiance.y, radiance.z, s0.w);
-            fin = true;
-          } else {
-            const uint32_t lp = g - jobs.first(j);
-            const int W = jobs.width(j);
-            const CacheDev& cc = jobs.cache(j);
-            const int role = cache_role(cc, lp, W);
-            const Uni& u = jobs.uni(j);
-            const F3 pos = xyz(b.R0[g]) + rd * d.tHit;
-            const F3 nrm = hit_normal(d.hit_axis(), rd);
-            const Mat mat = unpack_material(d.mat);
-            const uint32_t kmax = role == kRolePlain ? u.params0[1] : cc.train_bounces;
-            uint32_t rng = __float_as_uint(s0.w);
-            bool shadow = false, bounce = false;
-            const bool alive = shade_vertex(u, b, g, (uint32_t)w, pos, nrm, mat, radiance, tp, rng,
-                                            __float_as_uint(s1.w), shadow, bounce, kmax,
-                                            rec_slot(cc, role, lp, W, (uint32_t)w));
-            if (alive) {
-              w++;
-              setup = true;
-            } else {
-              fin = true;
-            }
-          }
-        }
-      }
-    }
-    if (fin) {   // the path's radiance is in its state
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int i = base + threadIdx.x;
+    bool fin_train = false;
+    uint32_t ti = 0u;
+    F3 rfin = f3(0.0f, 0.0f, 0.0f);
+    int jc = 0;
+    if (i < n) {
+      const uint32_t g = list[i];
+      const int j = jobs.job_of(g);
+      jc = j;
       const uint32_t lp = g - jobs.first(j);
       const int W = jobs.width(j);
       const CacheDev& cc = jobs.cache(j);
-      const F3 radiance = xyz(b.S0[g]);
-      finalize(jobs.outs(j), lp, radiance, __float_as_uint(b.S1[g].w), jobs.clamp(j));
-      if (cache_role(cc, lp, W) == kRoleTrain) cache_emit_samples_lane(cc, train_index(cc, lp, W), radiance);
+      const int role = cache_role(cc, lp, W);
+      const Uni& u = jobs.uni(j);
+      const DScene S = jobs.scene(j);
+      const uint32_t* occ = kSmem ? s_occ : S.bits;
+      for (int w = wave;; w++) {
+        const float4 s0 = b.S0[g];
+        const float4 s1 = b.S1[g];
+        const float4 s2 = b.S2[g];
+        const float4 r0 = b.R0[g];
+        const float4 r1 = b.R1[g];
+        F3 radiance = xyz(s0);
+        F3 tp = xyz(s1);
+        uint32_t rng = __float_as_uint(s0.w);
+        const uint32_t mat1bits = __float_as_uint(s1.w);
+        const uint32_t flags = __float_as_uint(s2.w);
+        const F3 surf = xyz(r0);
+        if (flags & kFlagShadow) {   // the previous vertex's sun shadow ray
+          const float4 r2 = b.R2[g];
+          const F3 ld = xyz(r2);
+          FlatDDA d;
+          d.init(S, surf, ld, r2.w);
+          c.rays++;
+          while (!d.done()) d.step(S, occ, ld, c);
+          d.finish(S, c);
+          if (!(d.tHit >= 0.0f)) radiance = radiance + xyz(s2);
+        }
+        bool done = (flags & kFlagTerminal) != 0u;
+        if (!done) {
+          const F3 rd = xyz(r1);
+          FlatDDA d;
+          d.init(S, surf, rd, 1e4f);
+          c.rays++;
+          while (!d.done()) d.step(S, occ, rd, c);
+          d.finish(S, c);
+          if (d.tHit < 0.0f) {
+            radiance = radiance + tp * sky_color(u, rd, false);
+            done = true;
+          } else {
+            const F3 pos = surf + rd * d.tHit;
+            const F3 nrm = hit_normal(d.hit_axis(), rd);
+            const Mat mat = unpack_material(d.mat);
+            const uint32_t kmax = role == kRolePlain ? u.params0[1] : cc.train_bounces;
+            bool shadow = false, bounce = false;
+            done = !shade_vertex(u, b, g, (uint32_t)w, pos, nrm, mat, radiance, tp, rng, mat1bits, shadow, bounce,
+                                 kmax, rec_slot(cc, role, lp, W, (uint32_t)w));
+          }
+        }
+        if (done) {
+          finalize(jobs.outs(j), lp, radiance, mat1bits, jobs.clamp(j));
+          if (role == kRoleTrain) { fin_train = true; ti = train_index(cc, lp, W); rfin = radiance; }
+          break;
+        }
+      }
     }
+    if (any_cache) cache_emit_samples(jobs.cache(jc), fin_train, ti, rfin);
   }
   if (stats) block_flush_stats(stats, c, 0u);   // kStatRays..kStatVReads
 }
