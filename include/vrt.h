@@ -116,8 +116,9 @@ typedef struct VrtTuning {
   int tail_wave;              /* first wave whose remaining paths each finish on
                                  one thread (their rays traced in turn, not in
                                  per-wave launches); 0 = never, -1 = automatic
-                                 (wave 2 for cache-assisted views, else never);
-                                 the image is the same either way              */
+                                 (wave 2 for a cache-assisted session, or for a
+                                 batch whose every job is cache-assisted; else
+                                 never); the image is the same either way      */
 } VrtTuning;
 
 /* One traced ray (vrt_trace_rays).  face: 0..5 = +x,-x,+y,-y,+z,-z normal,

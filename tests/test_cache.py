@@ -132,14 +132,19 @@ def test_trained_cache_gains_over_plain_and_untrained(vrt):
     assert rays_c < rays2
 
 
-def test_cache_jobs_in_a_batch_match_alone(vrt):
-    """Cache-assisted sessions inside a batch (with a plain session beside
-    them): the first frame is bit-identical to each session rendered alone
-    (queries and predictions do not depend on the order the batch appends
-    them in); later frames agree within the training's summation-order noise."""
+@pytest.mark.parametrize("plain_beside,tail", [(True, -1), (True, 2), (False, -1), (False, 0)])
+def test_cache_jobs_in_a_batch_match_alone(vrt, plain_beside, tail):
+    """Cache-assisted sessions inside a batch (with or without a plain
+    session beside them; the remaining paths finished per thread from wave 2
+    or wave by wave -- automatic: per thread when every job has the cache):
+    the first frame is bit-identical to each session rendered alone (queries
+    and predictions do not depend on the order the batch appends them in);
+    later frames agree within the training's summation-order noise."""
     ctx = vrt.Context(0)
     specs = [(vrt.VRT_SCENE_SMALL, 64, 1, 160, 90, True), (vrt.VRT_SCENE_RANDOM, 128, 7, 96, 64, False),
              (vrt.VRT_SCENE_SMALL, 64, 2, 200, 120, True)]
+    if not plain_beside:
+        specs = [sp for sp in specs if sp[5]]
     alone, inb, poses = [], [], []
     for kind, n, seed, W, H, cache in specs:
         vox, spawn = vrt.generate_scene(kind, n, seed)
@@ -153,6 +158,7 @@ def test_cache_jobs_in_a_batch_match_alone(vrt):
         inb.append(b)
         poses.append(spawn)
     batch = vrt.Batch(ctx, inb)
+    batch.set_tuning(tail_wave=tail)
     for f in range(3):
         us = [vrt.make_uniforms(poses[i], None, vrt.Lighting(), f, 2, 3, specs[i][3], specs[i][4])
               for i in range(len(specs))]

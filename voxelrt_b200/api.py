@@ -516,7 +516,7 @@ class Batch:
         check(lib.vrt_batch_set_graph(self.h, int(bool(on))))
 
     def set_tuning(self, refill_min=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, trace_variant=0,
-                   atrous_tile_rows=0, tail_wave=0) -> None:
+                   atrous_tile_rows=0, tail_wave=-1) -> None:
         t = VrtTuning(int(refill_min), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(trace_variant),
                       int(atrous_tile_rows), int(tail_wave))
         check(lib.vrt_batch_set_tuning(self.h, C.byref(t)))

@@ -76,8 +76,10 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   J.firsts = d_firsts;
   J.n = n;
   J.cache_jobs = ncl;
-  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n,
-                                  tune.tail_wave > 0 ? tune.tail_wave : 0);
+  // tail wave: as tuned; automatic (-1) = wave 2 when every job is cache-assisted (only the
+  // training paths remain after the first bounce), else never
+  const int tail = tune.tail_wave >= 0 ? tune.tail_wave : (ncl > 0 && ncl == n ? 2 : 0);
+  cudaError_t e = wf_launch_frame(J, P, waves, 0, wb, tune, stats, st, launches, nullptr, 0, nullptr, n, tail);
   if (e != cudaSuccess) return e;
   // the cache jobs' inference, resolve and training, all jobs per launch
   if (ncl > 0 && (e = launch_cache_post(J, wf_view(wb), cls, ncl, stats, st, launches)) != cudaSuccess) return e;

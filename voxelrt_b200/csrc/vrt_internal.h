@@ -85,7 +85,8 @@ struct WavefrontTuning {
                                 // 6, 7, 8: (8, 5) with the step loop unrolled 1, 2, 4 times
   int atrous_rows = 0;          // a-trous output tile rows: 0 = 16 at steps 1-2 and 8 at step 4, 8 = 8 at all steps
   int tail_wave = -1;           // first wave whose paths finish one thread each (k_wf_tail); 0 = never;
-                                // -1 = automatic: wave 2 for cache-assisted single-view frames, else never
+                                // -1 = automatic: wave 2 for cache-assisted frames (a session's, or a
+                                // batch's whose every job has the cache on), else never
 };
 
 // Host mirror of the device job table entry (JobDev in wavefront_core.cuh):
