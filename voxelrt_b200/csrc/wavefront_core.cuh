@@ -176,6 +176,10 @@ struct FlatDDA {
     state = kPending;
   }
 
+  // kSharedOcc: occ is the block's shared-memory copy of the occupancy bitmap;
+  // otherwise it is the scene's bitmap in global memory, read through the
+  // read-only path.
+  template <bool kSharedOcc>
   VRT_DI void step(const DScene& S, const uint32_t* occ, F3 rd, DCount& c) {
     const bool lv = (state & kLevelVoxel) != 0;
     if (state & kPending) {
@@ -209,7 +213,8 @@ struct FlatDDA {
     const uint32_t idx = (uint32_t)cx + (uint32_t)ext * ((uint32_t)cy + (uint32_t)ext * (uint32_t)cz);
     // two typed loads (the bitmap may be in shared memory, the masks are in
     // global memory) rather than one load through a selected pointer
-    const uint32_t word = lv ? __ldg(S.masks + (size_t)bi16 + (idx >> 5)) : occ[idx >> 5];
+    const uint32_t word = lv ? __ldg(S.masks + (size_t)bi16 + (idx >> 5))
+                             : (kSharedOcc ? occ[idx >> 5] : __ldg(occ + (idx >> 5)));
     if (!((word >> (idx & 31u)) & 1u)) {
       state |= kPending;
       return;
@@ -716,7 +721,7 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
     if (active) {
 #pragma unroll kUnroll
       for (int k = 0; k < kSteps; k++)
-        if (!d.done()) d.step(S, kSmem ? s_occ : S.bits, rd, c);
+        if (!d.done()) d.step<kSmem>(S, kSmem ? s_occ : S.bits, rd, c);
       if (d.done()) {
         d.finish(S, c);
         const uint32_t g = entry & ~kShadowBit;
@@ -936,7 +941,7 @@ __global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, u
           FlatDDA d;
           d.init(S, surf, ld, r2.w);
           c.rays++;
-          while (!d.done()) d.step(S, occ, ld, c);
+          while (!d.done()) d.step<kSmem>(S, occ, ld, c);
           d.finish(S, c);
           if (!(d.tHit >= 0.0f)) radiance = radiance + xyz(s2);
         }
@@ -946,7 +951,7 @@ __global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, u
           FlatDDA d;
           d.init(S, surf, rd, 1e4f);
           c.rays++;
-          while (!d.done()) d.step(S, occ, rd, c);
+          while (!d.done()) d.step<kSmem>(S, occ, rd, c);
           d.finish(S, c);
           if (d.tHit < 0.0f) {
             radiance = radiance + tp * sky_color(u, rd, false);
