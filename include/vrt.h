@@ -182,7 +182,9 @@ enum {
 };
 
 /* ---- context ----------------------------------------------------------- */
-/* Replaces WebGPU requestAdapter/requestDevice (main.js:138-159). */
+/* Replaces WebGPU requestAdapter/requestDevice (main.js:138-159).  Creates
+ * the context's stream and builds its present lookup table on it (an
+ * exhaustive pass over the floats below 8, ~5 ms of GPU time, asynchronous). */
 int vrt_create(const VrtDeviceConfig* cfg, VrtCtx** out);
 int vrt_destroy(VrtCtx* ctx);
 int vrt_ctx_synchronize(VrtCtx* ctx);

@@ -1486,22 +1486,21 @@ static int server_launch(VrtServer* sv) {
     auto solo = [&](const VrtSession* s) {
       return sv->solo_pixels > 0 && s->path_kernel == VRT_PATH_WAVEFRONT && (uint64_t)s->W * s->H >= sv->solo_pixels;
     };
-    // the oldest request of an idle session decides the launch: a large
-    // session renders alone through its own frame path; otherwise the oldest
-    // request of every idle small session joins one batch frame
-    for (auto it = sv->pending.begin(); it != sv->pending.end(); ++it) {
-      if (sv->busy[(size_t)it->session]) continue;
-      if (solo(sv->at(it->session))) {
-        take.push_back(std::move(*it));
-        sv->pending.erase(it);
-      }
-      break;
+    // the oldest request decides the launch: a large session renders alone
+    // through its own frame path; otherwise the oldest request of every small
+    // session joins one batch frame.  A session's next frame may be launched
+    // while its previous one is in flight: its frames run in stream order on
+    // the context's stream (history, edits and read-backs included), so the
+    // device always has the next launch queued
+    if (!sv->pending.empty() && solo(sv->at(sv->pending.front().session))) {
+      take.push_back(std::move(sv->pending.front()));
+      sv->pending.pop_front();
     }
   }
   const bool alone = sv->sequential || !take.empty();
   if (!alone) {
-    // oldest pending request of every idle session, in arrival order, while
-    // their pixels fit the pool
+    // oldest pending request of every session, in arrival order, while their
+    // pixels fit the pool
     std::vector<char> picked((size_t)sv->n, 0);
     uint64_t pix = 0;
     for (auto it = sv->pending.begin(); it != sv->pending.end();) {
@@ -1509,7 +1508,7 @@ static int server_launch(VrtServer* sv) {
       VrtSession* s = sv->at(k);
       const uint64_t p = (uint64_t)s->W * s->H;
       const bool large = sv->solo_pixels > 0 && s->path_kernel == VRT_PATH_WAVEFRONT && p >= sv->solo_pixels;
-      if (!large && !sv->busy[(size_t)k] && !picked[(size_t)k] && pix + p <= sv->batch->P) {
+      if (!large && !picked[(size_t)k] && pix + p <= sv->batch->P) {
         picked[(size_t)k] = 1;
         pix += p;
         take.push_back(std::move(*it));
@@ -1758,7 +1757,7 @@ int vrt_server_poll(VrtServer* sv, VrtCompletion* out, int max_out, int* n_out) 
   while ((int)sv->flights.size() < sv->max_in_flight && !sv->pending.empty()) {
     const size_t before = sv->flights.size();
     if (int r = server_launch(sv)) return r;
-    if (sv->flights.size() == before) break;   // every pending request waits for a busy session
+    if (sv->flights.size() == before) break;   // nothing could be launched
   }
   return VRT_OK;
 }
