@@ -1175,7 +1175,8 @@ cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int 
     case 3: return wf_launch_trace<J, kSmem, 4, 4, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 4: return wf_launch_trace<J, kSmem, 2, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 5: return wf_launch_trace<J, kSmem, 1, 1, false>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
-    // the default shape with the step loop unrolled 1, 2 or 4 times instead of 8 (smaller code)
+    // the default shape with the step loop unrolled 1, 2 or 4 times instead of 8 (smaller code;
+    // measured 1.396 / 1.354 / 1.358 ms of trace per 1080p frame against 1.349 fully unrolled)
     case 6: return wf_launch_trace<J, kSmem, 8, 5, false, 1>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 7: return wf_launch_trace<J, kSmem, 8, 5, false, 2>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
     case 8: return wf_launch_trace<J, kSmem, 8, 5, false, 4>(jobs, smem, tb, sms, b, w, impl, refill, stats, st);
