@@ -413,6 +413,12 @@ int vrt_server_set_sequential(VrtServer* sv, int on);
  * itself); smaller sessions are batched together.  0 (default): every
  * request is batched. */
 int vrt_server_set_solo_pixels(VrtServer* sv, long long pixels);
+/* Batched mode: while fewer than `sessions` sessions have pending requests,
+ * each launch renders the oldest request of a session with its own path
+ * scratch alone through its frame path (a small batch costs a whole frame's
+ * launch sequence and wave tails for a few views).  1 (default): always
+ * batch. */
+int vrt_server_set_min_batch(VrtServer* sv, int sessions);
 
 /* ---- scene lights -------------------------------------------------------- */
 /* The emissive-face light list, its power alias table and the per-brick

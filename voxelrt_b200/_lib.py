@@ -215,6 +215,7 @@ SIGNATURES = {
     "vrt_server_sessions": (I, [P, C.POINTER(I), C.POINTER(I)]),
     "vrt_server_set_sequential": (I, [P, I]),
     "vrt_server_set_solo_pixels": (I, [P, C.c_longlong]),
+    "vrt_server_set_min_batch": (I, [P, I]),
     "vrt_batch_create": (I, [P, C.POINTER(P), I, C.POINTER(P)]),
     "vrt_batch_destroy": (I, [P]),
     "vrt_batch_frame": (I, [P, C.POINTER(VrtUniforms)]),

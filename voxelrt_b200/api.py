@@ -601,6 +601,11 @@ class Server:
         render alone; smaller ones are batched (0: batch everything)."""
         check(lib.vrt_server_set_solo_pixels(self.h, int(pixels)))
 
+    def set_min_batch(self, sessions: int) -> None:
+        """While fewer than `sessions` sessions have pending requests, requests
+        render alone through their own frame path (1: always batch)."""
+        check(lib.vrt_server_set_min_batch(self.h, int(sessions)))
+
     def now(self) -> float:
         return float(lib.vrt_server_now(self.h))
 

@@ -1413,6 +1413,7 @@ struct VrtServer {
   int max_in_flight = 2;
   bool sequential = false;       // one request per launch through the session's own frame path
   uint64_t solo_pixels = 0;      // batched mode: sessions this large (with their own path scratch) render alone
+  int min_batch = 1;             // batched mode: fewer sessions with pending requests launch one request alone
   std::deque<Req> pending;
   std::deque<Flight> flights;
   std::vector<int> busy;         // requests of the slot in flight
@@ -1495,6 +1496,25 @@ static int server_launch(VrtServer* sv) {
     if (!sv->pending.empty() && solo(sv->at(sv->pending.front().session))) {
       take.push_back(std::move(sv->pending.front()));
       sv->pending.pop_front();
+    }
+  }
+  if (!sv->sequential && take.empty() && sv->min_batch > 1) {
+    // too few sessions to batch: the oldest request of a session with its
+    // own path scratch renders alone
+    std::vector<char> seen((size_t)sv->n, 0);
+    int distinct = 0;
+    for (const auto& r : sv->pending) {
+      if (seen[(size_t)r.session]) continue;
+      seen[(size_t)r.session] = 1;
+      if (++distinct >= sv->min_batch) break;
+    }
+    if (distinct < sv->min_batch) {
+      for (auto it = sv->pending.begin(); it != sv->pending.end(); ++it) {
+        if (sv->at(it->session)->path_kernel != VRT_PATH_WAVEFRONT) continue;
+        take.push_back(std::move(*it));
+        sv->pending.erase(it);
+        break;
+      }
     }
   }
   const bool alone = sv->sequential || !take.empty();
@@ -1676,6 +1696,12 @@ int vrt_server_set_sequential(VrtServer* sv, int on) {
 int vrt_server_set_solo_pixels(VrtServer* sv, long long pixels) {
   if (!sv || pixels < 0) return fail(VRT_ERR_INVALID, "bad argument");
   sv->solo_pixels = (uint64_t)pixels;
+  return VRT_OK;
+}
+
+int vrt_server_set_min_batch(VrtServer* sv, int sessions) {
+  if (!sv || sessions < 1 || sessions > 4096) return fail(VRT_ERR_INVALID, "bad argument");
+  sv->min_batch = sessions;
   return VRT_OK;
 }
 
