@@ -215,10 +215,12 @@ def test_sequential_server_equals_alone(ctx, vrt):
         sc.close()
 
 
-def test_hybrid_server_equals_alone(ctx, vrt):
+@pytest.mark.parametrize("solo,min_batch", [(300 * 170, 1), (0, 3), (300 * 170, 2)])
+def test_hybrid_server_equals_alone(ctx, vrt, solo, min_batch):
     """Large views alone through their own frame path, small ones batched
-    (vrt_server_set_solo_pixels): every request still renders what it renders
-    alone."""
+    (vrt_server_set_solo_pixels), and requests alone while fewer than
+    min_batch sessions wait (vrt_server_set_min_batch): every request still
+    renders what it renders alone."""
     vox, spawns, served, ref_sc, ref_s, srv_sc = [], [], [], [], [], []
     for kind, n, sd, W, H, nb in SESSIONS:
         v, sp = vrt.generate_scene(kind, n, sd)
@@ -231,7 +233,8 @@ def test_hybrid_server_equals_alone(ctx, vrt):
         ref_s.append(vrt.Session(ctx, rsc, W, H, firefly_clamp=10.0))
     reqs = _requests(vrt, spawns, 20, 21)
     server = vrt.Server(ctx, served, max_in_flight=2)
-    server.set_solo_pixels(300 * 170)       # the 320x180 and 480x270 views render alone
+    server.set_solo_pixels(solo)            # 300 x 170: the 320x180 and 480x270 views render alone
+    server.set_min_batch(min_batch)
     outs = []
     for i, (k, u, edits) in enumerate(reqs):
         W, H = SESSIONS[k][3], SESSIONS[k][4]
