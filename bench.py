@@ -857,7 +857,9 @@ def served_summary(sc, cc):
            "served_form": best,
            "forms_note": f"sequential: one request per launch through the session's own frame path; batched: "
                          f"continuous batching of every request; hybrid: continuous batching of views below "
-                         f"{sc['solo_pixels']} pixels, larger views alone",
+                         f"{sc['solo_pixels']} pixels, larger views alone; batched and hybrid render requests "
+                         f"alone while fewer than {SERVE_MIN_BATCH} sessions wait; every form serves the same "
+                         f"request stream (sessions, edits, arrival times)",
            "speedup_cache_served_vs_plain_sequential": round(cb / seq, 3),
            "speedup_plain_batched_vs_plain_sequential": round(f["plain_batched"]["capacity"]["frames_per_s"] / seq, 3),
            "speedup_plain_hybrid_vs_plain_sequential": round(f["plain_hybrid"]["capacity"]["frames_per_s"] / seq, 3),
@@ -1035,6 +1037,7 @@ def run_lights(args, local):
 
 
 SERVE_RES = [((640, 360), 0.40), ((1280, 720), 0.35), ((1920, 1080), 0.20), ((2560, 1440), 0.05)]
+SERVE_MIN_BATCH = 8    # batched forms: fewer sessions waiting than this render one request at a time
 
 
 def run_serve(args, local):
@@ -1228,14 +1231,18 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
                  "cache_hybrid"):
         server.set_sequential(form.endswith("sequential"))
         server.set_solo_pixels(solo if form.endswith("hybrid") else 0)
+        server.set_min_batch(SERVE_MIN_BATCH if not form.endswith("sequential") else 1)
         if form == "cache_sequential":
             for k, s in enumerate(sessions):
                 s.set_cache(**dict(CACHE_CFG, seed=k + 1))
             warm(32)
         else:
             warm(1)
-        out[form] = {"capacity": capacity(server, len(sessions), make_request, rng, n_sat),
-                     "poisson": sweep(a2, server, sessions, make_request, rng)}
+        # every form serves the same request stream: sessions, edits and arrival times from the same seeds
+        rq = np.random.default_rng(77)
+        mr = serve_requests(vrt, rq, spawns, meta, frames)
+        out[form] = {"capacity": capacity(server, len(sessions), mr, rq, n_sat),
+                     "poisson": sweep(a2, server, sessions, mr, np.random.default_rng(78))}
     out["solo_pixels"] = solo
     px = sum(w * h for _, w, h in meta)
     server.close()
