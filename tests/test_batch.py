@@ -82,6 +82,40 @@ def test_batch_equals_sessions_alone(ctx, vrt, use_graph):
         sc.close()
 
 
+@pytest.mark.parametrize("acc_f32", [False, True])
+def test_large_jobs_denoise_apart_and_match_alone(ctx, vrt, acc_f32):
+    """Frames launched without a graph denoise jobs of 512 K pixels and more
+    through the staged a-trous kernel with their own launches (the batch's
+    per-pixel a-trous kernel skips them): every job still equals the session
+    alone, beside small jobs and a job with the denoiser off."""
+    specs = [(2, 128, 3, 1024, 512, 3), (1, 64, 1, 200, 120, 3), (2, 128, 4, 1100, 480, 1),
+             (3, 64, 9, 96, 54, 3)]
+    scenes, alone, inbatch, spawns = [], [], [], []
+    for kind, n, seed, W, H, flags in specs:
+        vox, spawn = vrt.generate_scene(kind, n, seed)
+        sc = vrt.Scene(ctx, vox, n)
+        scenes.append(sc)
+        spawns.append(spawn)
+        alone.append(vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, accum_f32=acc_f32))
+        inbatch.append(vrt.Session(ctx, sc, W, H, firefly_clamp=10.0, accum_f32=acc_f32, path_kernel="batch_only"))
+    batch = vrt.Batch(ctx, inbatch)
+    batch.set_graph(False)
+    for f in range(3):
+        us = []
+        for i, (kind, n, seed, W, H, flags) in enumerate(specs):
+            pose, prev = _poses(vrt, spawns[i], f)
+            us.append(vrt.make_uniforms(pose, prev, vrt.Lighting(), 40 + f, 2, flags, W, H))
+        batch.frame(us)
+        for i in range(len(specs)):
+            alone[i].frame(us[i])
+            _check_same(_outputs(alone[i]), _outputs(inbatch[i]), f"frame {f} job {i}")
+    batch.close()
+    for s in alone + inbatch:
+        s.close()
+    for sc in scenes:
+        sc.close()
+
+
 def test_batch_only_session_refuses_single_frames(ctx, vrt):
     vox, spawn = vrt.generate_scene(1, 64, 1)
     sc = vrt.Scene(ctx, vox, 64)

@@ -1211,11 +1211,19 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   if (b->uploaded) CUDA_TRY(cudaEventSynchronize(b->ev_upload));
   uint32_t first = 0;
   std::vector<CacheLaunch> cls;
+  std::vector<AtrousJob> apart;
+  const bool graph = b->use_graph && full;
   for (int i = 0; i < m; i++) {
     VrtSession* s = ss[(size_t)i];
     JobHost& j = b->h_jobs[i];
     std::memset(&j, 0, sizeof j);
     const int p = parity_of(s);
+    // large jobs of frames launched without a graph denoise through the staged a-trous kernel, each with
+    // its own launches (a graph would bake one frame's history parity into them)
+    if (!graph && (u[i].params0[2] & 2u) && (uint64_t)s->W * s->H >= kAtrousApartPixels) {
+      j.atrous_apart = 1;
+      apart.push_back(AtrousJob{s->W, s->H, s->accum[p], s->acc_f32 ? 1 : 0, s->gbuf[p], s->den[0], s->den[1]});
+    }
     j.u = u[i];
     j.vox = s->scene->dev.vox; j.masks = s->scene->dev.masks; j.bits = s->scene->dev.bits;
     j.N = s->scene->dev.N; j.BG = s->scene->dev.BG;
@@ -1239,7 +1247,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   CUDA_TRY(cudaMemsetAsync(b->stats, 0, kStatCount * 8, st));
   CUDA_TRY(cudaEventRecord(b->ev_start, st));
   b->launches = 0;
-  if (b->use_graph && full) {
+  if (graph) {
     if (!b->gexec || b->graph_waves != waves || !same_tuning(b->graph_tune, b->tune) ||
         b->graph_cache_sig != cache_sig) {
       batch_drop_graph(b);
@@ -1268,7 +1276,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
     CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches,
-                                b->ctx->present_lut, cls.data(), (int)cls.size()));
+                                b->ctx->present_lut, cls.data(), (int)cls.size(), apart.data(), (int)apart.size()));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
   for (int i = 0; i < m; i++) {
