@@ -1238,9 +1238,10 @@ def served_comparison(args, local, rates=(200.0, 500.0), duration=1.0, n_sat=320
             warm(32)
         else:
             warm(1)
-        # every form serves the same request stream: sessions, edits and arrival times from the same seeds
+        # every form serves the same request stream: sessions, edits and arrival times from the same seeds,
+        # each session's camera path from the same frame on
         rq = np.random.default_rng(77)
-        mr = serve_requests(vrt, rq, spawns, meta, frames)
+        mr = serve_requests(vrt, rq, spawns, meta, [1000] * len(sessions))
         out[form] = {"capacity": capacity(server, len(sessions), mr, rq, n_sat),
                      "poisson": sweep(a2, server, sessions, mr, np.random.default_rng(78))}
     out["solo_pixels"] = solo
