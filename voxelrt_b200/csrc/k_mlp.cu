@@ -408,24 +408,41 @@ __device__ __forceinline__ int task_of(const MlpTaskSet& ts, int b) {
   return j;
 }
 
+// Barrier of the 128 threads of group g (named barrier 1 + g) that also
+// agrees on `ok` across them, with the handoff fences of publish_and.
+__device__ __forceinline__ bool group_publish_and(int g, bool ok) {
+  umma::fence_smem_to_async();
+  umma::fence_before_sync();
+  uint32_t all;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(all)
+      : "r"(ok ? 1u : 0u), "r"(1 + g)
+      : "memory");
+  umma::fence_after_sync();
+  return all != 0u;
+}
+
 // Inference: out3[i*3 + c] = MLP(encode(q_i)) for every task of the set.
 // A CTA of 256 threads is two groups of 128 (threads 128 g .. 128 g + 127)
-// that share the weights in shared memory and otherwise run independently.
-// Each group keeps two 128-query tiles in flight, each with its own TMEM
-// accumulator (columns 64 (2g + u)), its own operand tile and two mbarriers:
-// `done` (the tile's MMAs completed, signalled by tcgen05.commit) and `ready`
-// (all 128 rows of the tile's next operand are in shared memory and the TMEM
-// rows of its last result have been read: one arrival per thread).  Only the
-// group's first thread waits on `ready` before issuing; the others arrive and
-// go on to the other tile, so no thread of the group waits for the slowest one
-// except the issuer.  While the tensor core runs one tile's layer, the threads
-// unpack the other tile's previous layer (TMEM load, ReLU and bf16 pack into
-// the next operand tile).  A layer's output overwrites its input tile: every
-// thread waits for the layer's MMA completion (which covers the MMAs'
+// that share the weights in shared memory and otherwise run independently,
+// synchronising on their own named barrier.  Each group keeps two 128-query
+// tiles in flight, each with its own TMEM accumulator (columns 64 (2g + u)),
+// its own operand tile and its own mbarrier: while the tensor core runs one
+// tile's layer, the group's threads unpack the other tile's previous layer
+// (TMEM load, ReLU, bf16 pack into the next operand tile), so the MMA latency
+// hides behind the epilogue work, and the other group's tiles fill the
+// tensor core's remaining gaps.  A layer's output overwrites its input tile:
+// every thread waits for the layer's MMA completion (which covers the MMAs'
 // shared-memory reads) before it stores.  Thread r of a group owns row r of
-// its tiles.  The groups of a task's CTAs stride over its tile pairs.  Every
-// wait is bounded; a thread whose wait runs out stops, and the kernel reports
-// the error.
+// its tiles; the first thread of each group issues the group's MMAs.  The
+// groups of a task's CTAs stride over its tile pairs.  (Handing each operand
+// over through a per-tile mbarrier instead -- one arrival per thread, only the
+// issuing thread waiting -- ran 70.7 against 65.8 us for 983 K queries: the
+// issuer's polling and the warps it holds back cost more than the barrier.)
 __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ MlpTaskSet ts) {
   using namespace mlp;
   const MlpTask& tk = ts.t[task_of(ts, blockIdx.x)];
@@ -435,12 +452,11 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
   const int cb = blockIdx.x - tk.cta0;
   if (2 * cb >= tiles) return;   // nothing for this CTA (before any TMEM allocation)
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t mbar[8];   // done[g][u] at 2g + u, ready[g][u] at 4 + 2g + u
+  __shared__ uint64_t mbar[4];
   __shared__ uint32_t tmem_base;
   const int warp = threadIdx.x >> 5, g = threadIdx.x >> 7, t = threadIdx.x & 127;
   if (warp == 0) umma::tmem_alloc(&tmem_base, 256);
   if (threadIdx.x < 4) umma::mbar_init(&mbar[threadIdx.x], 1);
-  else if (threadIdx.x < 8) umma::mbar_init(&mbar[threadIdx.x], 128);
   load_weights(smem, tk.wb);
   umma::fence_before_sync();
   __syncthreads();
@@ -450,9 +466,8 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
   // this group's tiles: X (input, 80 columns; then each hidden layer, 64 columns)
   const int X[2] = {kIX + (2 * g) * kITile, kIX + (2 * g + 1) * kITile};
   const uint32_t acc[2] = {tbase + 64u * (uint32_t)(2 * g), tbase + 64u * (uint32_t)(2 * g + 1)};
-  uint64_t* done = mbar + 2 * g;
-  uint64_t* ready = mbar + 4 + 2 * g;
-  uint32_t pdone[2] = {0u, 0u}, pready[2] = {0u, 0u};
+  uint64_t* mb = mbar + 2 * g;
+  uint32_t phase[2] = {0u, 0u};
   bool ok = true;
   const int vctas = 2 * tk.ctas;           // groups of the task: pairs (pt, pt + vctas), pt = vb + k stride
   const int vb = 2 * cb + g;
@@ -468,29 +483,27 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
       }
     }
   };
-  // hand tile u's next operand to the issuer, which starts layer l when all 128 rows are in
-  auto handoff = [&](int u, int l) {
-    umma::fence_smem_to_async();
-    umma::fence_before_sync();
-    umma::mbar_arrive(&ready[u]);
+  // tensor-core work of layer l of tile u (the group's first thread), completion on mb[u]
+  auto issue = [&](int u, int l) {
     if (t != 0) return;
-    ok = umma::mbar_wait(&ready[u], pready[u], kMbarSpin) && ok;
-    pready[u] ^= 1u;
-    umma::fence_after_sync();
-    if (!ok) return;
     if (l == 0) issue_fwd(acc[u], s0 + X[u], s0 + kWf0, kIn, kHid, false);
     else if (l == 1) issue_fwd(acc[u], s0 + X[u], s0 + kWf1, kHid, kHid, false);
     else if (l == 2) issue_fwd(acc[u], s0 + X[u], s0 + kWf2, kHid, kHid, false);
     else issue_fwd(acc[u], s0 + X[u], s0 + kWf3, kHid, kOutPad, false);
-    umma::commit(&done[u]);
+    umma::commit(&mb[u]);
   };
   auto wait = [&](int u) {
-    ok = umma::mbar_wait(&done[u], pdone[u], kMbarSpin) && ok;
-    pdone[u] ^= 1u;
+    ok = umma::mbar_wait(&mb[u], phase[u], kMbarSpin) && ok;
+    phase[u] ^= 1u;
     umma::fence_after_sync();
   };
   if (vb < tiles) fetch(vb);
-  for (int pt = vb; pt < tiles && ok; pt += stride) {
+  // The loop runs while the group agrees on `ok` (every exit is decided on a
+  // value its barrier made uniform).  No barrier closes a pair: the next
+  // pair's first MMA is issued after the staging barrier, which each thread
+  // reaches after reading its last TMEM rows, and each thread writes the next
+  // input tile only after it has seen the MMAs that read the tile complete.
+  for (int pt = vb; pt < tiles; pt += stride) {
     int idx[2];
     float qq[2][9];
 #pragma unroll
@@ -501,9 +514,13 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
     }
     // stage tile 0 and start its first layer; stage tile 1 while it runs
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
-    handoff(0, 0);
+    ok = group_publish_and(g, ok);
+    if (!ok) break;
+    issue(0, 0);
     stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
-    handoff(1, 0);
+    ok = group_publish_and(g, ok);
+    if (!ok) break;
+    issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
     for (int l = 0; l < 4 && ok; l++) {
@@ -514,7 +531,8 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
           float h[kHid];
           tmem_row<kHid>(acc[u], 0u, h);
           store_row_relu(smem + X[u], t, kHid, h);
-          handoff(u, l + 1);
+          ok = group_publish_and(g, ok);
+          if (ok) issue(u, l + 1);
         } else {
           float o[kOutPad];
           tmem_row<kOutPad>(acc[u], 0u, o);
@@ -524,7 +542,8 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
       }
     }
   }
-  if (!ok) atomicExch(tk.err, 1);
+  ok = group_publish_and(g, ok);           // the last pair's output waits, agreed
+  if (!ok && t == 0) atomicExch(tk.err, 1);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 256);

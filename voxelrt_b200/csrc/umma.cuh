@@ -67,12 +67,6 @@ UMMA_DI void mbar_init(uint64_t* mbar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// One arrival on `mbar` (release: this thread's earlier writes are ordered
-// before the phase completes for whoever waits on it).
-UMMA_DI void mbar_arrive(uint64_t* mbar) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
-}
-
 // Bounded wait for phase `parity` of `mbar`; false when the bound ran out.
 UMMA_DI bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t max_iter) {
   const uint32_t a = smem_u32(mbar);
