@@ -147,22 +147,51 @@ __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint
 //   sin 2a = 2 sin a cos a,  cos 2a = (cos a - sin a)(cos a + sin a),
 // which keeps the per-query cost at 3 sincos_ calls (the rounding error
 // doubles per octave: ~2e-4 at octave 11, far below the bf16 step).
+// Packed fp32 pairs (sm_100a's f32x2 arithmetic): each lane rounds exactly
+// as the scalar instruction would.
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "mul.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "add.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "sub.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
 __device__ __forceinline__ void encode(const float* q, float extent, float* f) {
+  float sn[3], cs[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const float x = (q[a] / extent) * 0.5f;
     const float t = x - floorf(x);
-    float sn, cs;
-    sincos_(kTwoPi * t, sn, cs);
+    sincos_(kTwoPi * t, sn[a], cs[a]);
+  }
+  // the x and y axes' recurrences as packed pairs, z alone; same roundings
+  float2 s01 = make_float2(sn[0], sn[1]), c01 = make_float2(cs[0], cs[1]);
+  float s2 = sn[2], c2 = cs[2];
+  const float2 two = make_float2(2.0f, 2.0f);
 #pragma unroll
-    for (int k = 0; k < kFreqs; k++) {
-      f[6 * k + a] = sn;
-      f[6 * k + 3 + a] = cs;
-      const float s2 = (sn * cs) * 2.0f;
-      const float c2 = (cs - sn) * (cs + sn);
-      sn = s2;
-      cs = c2;
-    }
+  for (int k = 0; k < kFreqs; k++) {
+    f[6 * k + 0] = s01.x; f[6 * k + 1] = s01.y; f[6 * k + 2] = s2;
+    f[6 * k + 3] = c01.x; f[6 * k + 4] = c01.y; f[6 * k + 5] = c2;
+    const float2 ns01 = f2_mul(f2_mul(s01, c01), two);
+    const float2 nc01 = f2_mul(f2_sub(c01, s01), f2_add(c01, s01));
+    const float ns2 = (s2 * c2) * 2.0f;
+    const float nc2 = (c2 - s2) * (c2 + s2);
+    s01 = ns01; c01 = nc01; s2 = ns2; c2 = nc2;
   }
   f[72] = q[3]; f[73] = q[4]; f[74] = q[5];
   f[75] = q[6]; f[76] = q[7]; f[77] = q[8];
