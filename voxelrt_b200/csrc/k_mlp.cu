@@ -147,30 +147,6 @@ __device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint
 //   sin 2a = 2 sin a cos a,  cos 2a = (cos a - sin a)(cos a + sin a),
 // which keeps the per-query cost at 3 sincos_ calls (the rounding error
 // doubles per octave: ~2e-4 at octave 11, far below the bf16 step).
-// Packed fp32 pairs (sm_100a's f32x2 arithmetic): each lane rounds exactly
-// as the scalar instruction would.
-__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
-      "mul.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
-      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-__device__ __forceinline__ float2 f2_add(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
-      "add.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
-      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
-      "sub.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
-      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-
 __device__ __forceinline__ void encode(const float* q, float extent, float* f) {
   float sn[3], cs[3];
 #pragma unroll
@@ -541,14 +517,12 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
 #pragma unroll
       for (int j = 0; j < 9; j++) qq[u][j] = q[u][j];
     }
-    // stage tile 0 and start its first layer; stage tile 1 while it runs
+    // stage both tiles, then start both first layers (one barrier for the pair)
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
-    ok = group_publish_and(g, ok);
-    if (!ok) break;
-    issue(0, 0);
     stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
     ok = group_publish_and(g, ok);
     if (!ok) break;
+    issue(0, 0);
     issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
