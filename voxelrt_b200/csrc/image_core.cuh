@@ -92,8 +92,10 @@ VRT_DI float4 atrous_pixel(int W, int H, int px, int py, const void* __restrict_
   const float history = fmax_(center.w, 1.0f);
   const float lumC = luminance(center.x, center.y, center.z);
   const float sigmaL = fmax_(0.08f, 2.0f / __fsqrt_rn(history));
-  float2 rg = make_float2((center.x * 0.375f) * 0.375f, (center.y * 0.375f) * 0.375f);
-  float2 bw = make_float2((center.z * 0.375f) * 0.375f, 0.140625f);   // (sb, wSum)
+  float sr = (center.x * 0.375f) * 0.375f;
+  float sg = (center.y * 0.375f) * 0.375f;
+  float sb = (center.z * 0.375f) * 0.375f;
+  float wSum = 0.140625f;
   const float invD = 1.0f / (0.05f * g.w + 0.01f);
   const float invS = 1.0f / sigmaL;
 #pragma unroll
@@ -113,15 +115,18 @@ VRT_DI float4 atrous_pixel(int W, int H, int px, int py, const void* __restrict_
       const float wKernel = b3_weight(dx) * b3_weight(dy);
       const float e = exp_nonpos_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - luminance(cq.x, cq.y, cq.z)) * invS));
       const float w = (wKernel * n32) * e;
-      const float2 ww = make_float2(w, w);   // the accumulations as packed pairs (see atrous_pixel_tile)
-      rg = f2_fma(make_float2(cq.x, cq.y), ww, rg);
-      bw = f2_fma(make_float2(cq.z, 1.0f), ww, bw);
+      sr = __fmaf_rn(cq.x, w, sr);
+      sg = __fmaf_rn(cq.y, w, sg);
+      sb = __fmaf_rn(cq.z, w, sb);
+      wSum = wSum + w;
     }
   }
-  const float den = fmax_(bw.y, 1e-6f);
-  return make_float4(rg.x / den, rg.y / den, bw.x / den, center.w);
+  const float den = fmax_(wSum, 1e-6f);
+  return make_float4(sr / den, sg / den, sb / den, center.w);
 }
 
+// (Accumulating (r, g) and (b, weight) as packed fp32 pairs left the
+// iteration's instruction count and time unchanged, so the sums stay scalar.)
 // atrous_pixel with the input staged in shared memory: sg = G-buffer tile,
 // sc = source tile in fp32 with its luminance in .w, ci = this pixel's index
 // in the tile (rows of RW pixels); taps outside the image hold zeros and
@@ -133,8 +138,10 @@ VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const
   const float history = fmax_(center.w, 1.0f);
   const float lumC = luminance(center.x, center.y, center.z);
   const float sigmaL = fmax_(0.08f, 2.0f / __fsqrt_rn(history));
-  float2 rg = make_float2((center.x * 0.375f) * 0.375f, (center.y * 0.375f) * 0.375f);
-  float2 bw = make_float2((center.z * 0.375f) * 0.375f, 0.140625f);   // (sb, wSum)
+  float sr = (center.x * 0.375f) * 0.375f;
+  float sg_ = (center.y * 0.375f) * 0.375f;
+  float sb = (center.z * 0.375f) * 0.375f;
+  float wSum = 0.140625f;
   const float invD = 1.0f / (0.05f * g.w + 0.01f);
   const float invS = 1.0f / sigmaL;
 #pragma unroll
@@ -152,15 +159,14 @@ VRT_DI float4 atrous_pixel_tile(float4 center, float4 g, const float4* sg, const
       const float wKernel = b3_weight(dx) * b3_weight(dy);
       const float e = exp_nonpos_(-__fmaf_rn(fabsf(g.w - gq.w), invD, fabsf(lumC - cq.w) * invS));
       const float w = (wKernel * n32) * e;
-      // (sr, sg) += (r, g) w and (sb, wSum) += (b, 1) w as two packed fused
-      // multiply-adds: 1 * w is exact, so wSum + w rounds as the plain sum
-      const float2 ww = make_float2(w, w);
-      rg = f2_fma(make_float2(cq.x, cq.y), ww, rg);
-      bw = f2_fma(make_float2(cq.z, 1.0f), ww, bw);
+      sr = __fmaf_rn(cq.x, w, sr);
+      sg_ = __fmaf_rn(cq.y, w, sg_);
+      sb = __fmaf_rn(cq.z, w, sb);
+      wSum = wSum + w;
     }
   }
-  const float den = fmax_(bw.y, 1e-6f);
-  return make_float4(rg.x / den, rg.y / den, bw.x / den, center.w);
+  const float den = fmax_(wSum, 1e-6f);
+  return make_float4(sr / den, sg_ / den, sb / den, center.w);
 }
 
 // present.wgsl:40-55 for one channel: v = illum * sqrtAlb^2 * exposure ->

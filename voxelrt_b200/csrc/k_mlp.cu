@@ -517,7 +517,9 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
 #pragma unroll
       for (int j = 0; j < 9; j++) qq[u][j] = q[u][j];
     }
-    // stage both tiles, then start both first layers (one barrier for the pair)
+    // stage both tiles, then start both first layers (one barrier for the pair: 65.0 -> 63.1 us for 983 K
+    // queries; a barrier per tile within the layers is kept -- unpacking both tiles of a layer before one
+    // barrier ran 70.0 us, the tensor core then waits for both epilogues)
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
     stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
     ok = group_publish_and(g, ok);
@@ -527,7 +529,6 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
     for (int l = 0; l < 4 && ok; l++) {
-      // both tiles' layer l: unpack each as its MMAs complete, one barrier, both next layers
 #pragma unroll
       for (int u = 0; u < 2; u++) {
         wait(u);
@@ -535,16 +536,14 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
           float h[kHid];
           tmem_row<kHid>(acc[u], 0u, h);
           store_row_relu(smem + X[u], t, kHid, h);
+          ok = group_publish_and(g, ok);
+          if (ok) issue(u, l + 1);
         } else {
           float o[kOutPad];
           tmem_row<kOutPad>(acc[u], 0u, o);
           if (ok && idx[u] < n)
             for (int j = 0; j < kOut; j++) tk.out3[(size_t)idx[u] * 3 + j] = o[j];
         }
-      }
-      if (l < 3) {
-        ok = group_publish_and(g, ok);
-        if (ok) { issue(0, l + 1); issue(1, l + 1); }
       }
     }
   }

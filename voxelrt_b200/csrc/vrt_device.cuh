@@ -126,15 +126,6 @@ VRT_DI float2 f2_sub(float2 a, float2 b) {
       : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return r;
 }
-// a * b + c per lane with one rounding (as __fmaf_rn)
-VRT_DI float2 f2_fma(float2 a, float2 b, float2 c) {
-  float2 r;
-  asm("{\n\t.reg .b64 a, b, c, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
-      "mov.b64 c, {%6, %7};\n\tfma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;\n\t}"
-      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return r;
-}
-
 VRT_DI float pow2i_(int k) { return __uint_as_float((uint32_t)(k + 127) << 23); }
 
 // Horner steps as explicit fused multiply-adds (one rounding each; the CPU
