@@ -56,6 +56,62 @@ __global__ void __launch_bounds__(256) k_b_atrous(MultiJob J, uint32_t P, int it
   dst[lp] = pack_h4(v.x, v.y, v.z, v.w);
 }
 
+// The same iteration over shared-memory tiles: a CTA of 256 threads produces a
+// 32 x kTY tile of one job (kTY = 16 at steps 1-2, 8 at step 4), staging the
+// tile and its halo of 2 step pixels -- G-buffer as copied, source in fp32
+// with its luminance in .w, zeros outside the image, whose zero normal drops
+// the tap as the plain kernel's bounds test does -- with coalesced loads,
+// then evaluating the taps from shared memory (atrous_pixel_tile: the
+// arithmetic and order of atrous_pixel, so the same bits).  tiles: m + 1
+// prefix counts of the jobs' tiles; CTA b finds its job by binary search.
+template <int kTY>
+__global__ void __launch_bounds__(256) k_b_atrous_tiled(MultiJob J, const uint32_t* __restrict__ tiles, int it) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const uint32_t b = blockIdx.x;
+  int lo = 0, hi = J.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(tiles + mid) <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const JobDev& jd = J.jobs[lo];
+  if ((jd.u.params0[2] & 2u) == 0u || jd.atrous_apart) return;
+  const int W = jd.W, H = jd.H, step = 1 << it;
+  const int tb = (int)(b - __ldg(tiles + lo)), tw = (W + 31) / 32;
+  const int x0 = (tb % tw) * 32, y0 = (tb / tw) * kTY;
+  const int hx = 2 * step, RW = 32 + 2 * hx, RH = kTY + 2 * hx, npx = RW * RH;
+  float4* sg = reinterpret_cast<float4*>(smem);
+  float4* sc = sg + npx;
+  const void* src = it == 0 ? jd.acc_cur : (it == 1 ? (const void*)jd.den0 : (const void*)jd.den1);
+  const bool srcF32 = it == 0 && jd.acc_f32 != 0;
+  uint2* dst = it == 1 ? jd.den1 : jd.den0;
+  const float4* gb = jd.out.gbuf;
+  for (int i = threadIdx.x; i < npx; i += 256) {
+    const int qx = x0 - hx + i % RW, qy = y0 - hx + i / RW;
+    float4 g4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), c4 = g4;
+    if (qx >= 0 && qy >= 0 && qx < W && qy < H) {
+      const size_t q = (size_t)qy * W + qx;
+      g4 = __ldg(gb + q);
+      c4 = load_px(src, srcF32, q);
+      c4.w = luminance(c4.x, c4.y, c4.z);
+    }
+    sg[i] = g4;
+    sc[i] = c4;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int half = 0; half < kTY / 8; half++) {
+    const int lx = threadIdx.x & 31, ly = (threadIdx.x >> 5) + 8 * half;
+    const int px = x0 + lx, py = y0 + ly;
+    if (px >= W || py >= H) continue;
+    const int ci = (ly + hx) * RW + (lx + hx);
+    const size_t p = (size_t)py * W + px;
+    const float4 center = load_px(src, srcF32, p);
+    const float4 v = atrous_pixel_tile(center, sg[ci], sg, sc, ci, RW, step);
+    dst[p] = pack_h4(v.x, v.y, v.z, v.w);
+  }
+}
+
 // present.wgsl:40-55 over all jobs.
 __global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P, const float* __restrict__ lut) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,7 +127,7 @@ __global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P, const
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
                                cudaStream_t st, uint32_t* launches, const float* present_lut, const CacheLaunch* cls,
-                               int ncl, const AtrousJob* aj, int naj) {
+                               int ncl, const AtrousJob* aj, int naj, const AtrousTiles* at) {
   MultiJob J;
   J.jobs = (const JobDev*)d_jobs;
   J.firsts = d_firsts;
@@ -87,7 +143,18 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   const unsigned blocks = (P + 255) / 256;
   k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
   for (int it = 0; it < 3; it++) {
-    k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);
+    if (at && at->d16) {   // shared-memory tiles: 32 x 16 at steps 1-2, 32 x 8 at step 4
+      const int step = 1 << it, hx = 2 * step;
+      if (it < 2) {
+        const int smem = (32 + 2 * hx) * (16 + 2 * hx) * 32;
+        k_b_atrous_tiled<16><<<at->n16, 256, smem, st>>>(J, at->d16, it);
+      } else {
+        const int smem = (32 + 2 * hx) * (8 + 2 * hx) * 32;
+        k_b_atrous_tiled<8><<<at->n8, 256, smem, st>>>(J, at->d8, it);
+      }
+    } else {
+      k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);
+    }
     // the chain accum -> dA -> dB -> dA (main.js:503-507) of the jobs apart
     for (int k = 0; k < naj; k++) {
       const AtrousJob& a = aj[k];

@@ -1084,7 +1084,7 @@ int vrt_batch_destroy(VrtBatch* b) {
   cudaStreamSynchronize(c->stream);
   batch_drop_graph(b);
   dev_free(c, b->d_jobs, b->sessions.size() * sizeof(JobHost), &b->bytes);
-  dev_free(c, b->d_firsts, b->sessions.size() * 4, &b->bytes);
+  dev_free(c, b->d_firsts, (3 * b->sessions.size() + 2) * 4, &b->bytes);
   dev_free(c, b->wf_mem, b->wf_bytes, &b->bytes);
   dev_free(c, b->stats, kStatCount * 8, &b->bytes);
   if (b->h_jobs) cudaFreeHost(b->h_jobs);
@@ -1112,10 +1112,10 @@ static int batch_create_capacity(VrtCtx* ctx, VrtSession* const* sessions, int n
   b->wf_bytes = wavefront_bytes((int)b->P, 1, max_waves);
   int r = dev_alloc(ctx, &b->wf_mem, b->wf_bytes, &b->bytes);
   if (!r) r = dev_alloc(ctx, &b->d_jobs, (size_t)n * sizeof(JobHost), &b->bytes);
-  if (!r) r = dev_alloc(ctx, (void**)&b->d_firsts, (size_t)n * 4, &b->bytes);
+  if (!r) r = dev_alloc(ctx, (void**)&b->d_firsts, (size_t)(3 * n + 2) * 4, &b->bytes);   // firsts, tile tables
   if (!r) r = dev_alloc(ctx, (void**)&b->stats, kStatCount * 8, &b->bytes);
   if (!r && (cudaMallocHost((void**)&b->h_jobs, (size_t)n * sizeof(JobHost)) != cudaSuccess ||
-             cudaMallocHost((void**)&b->h_firsts, (size_t)n * 4) != cudaSuccess))
+             cudaMallocHost((void**)&b->h_firsts, (size_t)(3 * n + 2) * 4) != cudaSuccess))
     r = fail(VRT_ERR_OOM, "pinned job table");
   if (!r && (cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_end) != cudaSuccess ||
              cudaEventCreateWithFlags(&b->ev_upload, cudaEventDisableTiming) != cudaSuccess))
@@ -1240,8 +1240,19 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   }
   const uint32_t P = first;
   if (P > b->P) return fail(VRT_ERR_INVALID, "batch frame of %u pixels exceeds the pool's %u", P, b->P);
+  // a-trous tile tables: prefix counts of each job's 32 x 16 and 32 x 8 tiles
+  uint32_t* t16 = b->h_firsts + n;
+  uint32_t* t8 = t16 + n + 1;
+  t16[0] = t8[0] = 0u;
+  for (int i = 0; i < m; i++) {
+    const VrtSession* s = ss[(size_t)i];
+    const uint32_t tw = (uint32_t)(s->W + 31) / 32u;
+    t16[i + 1] = t16[i] + tw * (uint32_t)((s->H + 15) / 16);
+    t8[i + 1] = t8[i] + tw * (uint32_t)((s->H + 7) / 8);
+  }
+  const AtrousTiles at{b->d_firsts + n, b->d_firsts + 2 * n + 1, t16[m], t8[m]};
   CUDA_TRY(cudaMemcpyAsync(b->d_jobs, b->h_jobs, (size_t)m * sizeof(JobHost), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(b->d_firsts, b->h_firsts, (size_t)m * 4, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(b->d_firsts, b->h_firsts, (size_t)(3 * n + 2) * 4, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaEventRecord(b->ev_upload, st));
   b->uploaded = true;
   CUDA_TRY(cudaMemsetAsync(b->stats, 0, kStatCount * 8, st));
@@ -1255,7 +1266,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       uint32_t nl = 0;
       cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl,
-                                         b->ctx->present_lut, cls.data(), (int)cls.size());
+                                         b->ctx->present_lut, cls.data(), (int)cls.size(), nullptr, 0, &at);
       cudaError_t e2 = cudaStreamEndCapture(st, &graph);
       if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1276,7 +1287,8 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
     CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches,
-                                b->ctx->present_lut, cls.data(), (int)cls.size(), apart.data(), (int)apart.size()));
+                                b->ctx->present_lut, cls.data(), (int)cls.size(), apart.data(), (int)apart.size(),
+                                &at));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
   for (int i = 0; i < m; i++) {

@@ -421,9 +421,9 @@ VRT_DI DHit trace(const DScene& S, const uint32_t* occ, F3 roW, F3 rd, float max
 
   float t = tEnter;
   const F3 startP = ro + rd * (t + 1e-4f);
-  int bx = iclamp_(ifloor_(startP.x / 8.0f), 0, BG - 1);
-  int by = iclamp_(ifloor_(startP.y / 8.0f), 0, BG - 1);
-  int bz = iclamp_(ifloor_(startP.z / 8.0f), 0, BG - 1);
+  int bx = iclamp_(ifloor_(startP.x * 0.125f), 0, BG - 1);
+  int by = iclamp_(ifloor_(startP.y * 0.125f), 0, BG - 1);
+  int bz = iclamp_(ifloor_(startP.z * 0.125f), 0, BG - 1);
   const F3 absInv = f3(fabsf(invRd.x), fabsf(invRd.y), fabsf(invRd.z));
   const F3 tDeltaB = absInv * 8.0f;
   F3 tMaxB = ((f3((float)bx, (float)by, (float)bz) + stepGE) * 8.0f - ro) * invRd;

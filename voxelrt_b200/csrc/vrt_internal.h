@@ -116,6 +116,14 @@ struct JobHost {
   CacheDev cache;
 };
 
+// The batch a-trous tile tables: per job, the prefix counts of its 32 x 16 and
+// 32 x 8 output tiles (m + 1 entries each, in device memory) and their totals.
+struct AtrousTiles {
+  const uint32_t* d16;
+  const uint32_t* d8;
+  uint32_t n16, n8;
+};
+
 // Batch jobs of at least this many pixels run their a-trous chain apart (below
 // it the per-launch cost outweighs the staged kernel's gain).
 constexpr uint64_t kAtrousApartPixels = 512 * 1024;
@@ -158,7 +166,7 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
                                cudaStream_t st, uint32_t* launches, const float* present_lut,
                                const CacheLaunch* cls = nullptr, int ncl = 0, const AtrousJob* aj = nullptr,
-                               int naj = 0);
+                               int naj = 0, const AtrousTiles* at = nullptr);
 
 // Radiance-cache MLP kernels (k_mlp.cu).  q9: n x 9 floats (position in
 // metres, normal, albedo); y3: n x 3 target radiance; weights bf16 row-major.

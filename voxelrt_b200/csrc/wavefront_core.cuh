@@ -157,9 +157,10 @@ struct FlatDDA {
     else ax = 2;
     t = tEnter;
     const F3 sp = ro + rd * (t + 1e-4f);
-    cx = iclamp_(ifloor_(sp.x / 8.0f), 0, S.BG - 1);
-    cy = iclamp_(ifloor_(sp.y / 8.0f), 0, S.BG - 1);
-    cz = iclamp_(ifloor_(sp.z / 8.0f), 0, S.BG - 1);
+    // x / 8 as x * 0.125: the same real number, so the same rounding
+    cx = iclamp_(ifloor_(sp.x * 0.125f), 0, S.BG - 1);
+    cy = iclamp_(ifloor_(sp.y * 0.125f), 0, S.BG - 1);
+    cz = iclamp_(ifloor_(sp.z * 0.125f), 0, S.BG - 1);
     tm = ((f3((float)cx, (float)cy, (float)cz) + stepGE) * 8.0f - ro) * invRd;
     sc = 8.0f;
     ext = S.BG;
