@@ -83,11 +83,10 @@ def test_batch_equals_sessions_alone(ctx, vrt, use_graph):
 
 
 @pytest.mark.parametrize("acc_f32", [False, True])
-def test_large_jobs_denoise_apart_and_match_alone(ctx, vrt, acc_f32):
-    """Frames launched without a graph denoise jobs of 512 K pixels and more
-    through the staged a-trous kernel with their own launches (the batch's
-    per-pixel a-trous kernel skips them): every job still equals the session
-    alone, beside small jobs and a job with the denoiser off."""
+def test_large_and_small_jobs_without_graph_match_alone(ctx, vrt, acc_f32):
+    """Frames launched without a graph, jobs of half a megapixel beside small
+    ones and one with the denoiser off, both history formats: every job's
+    a-trous tiles and outputs equal the session alone."""
     specs = [(2, 128, 3, 1024, 512, 3), (1, 64, 1, 200, 120, 3), (2, 128, 4, 1100, 480, 1),
              (3, 64, 9, 96, 54, 3)]
     scenes, alone, inbatch, spawns = [], [], [], []

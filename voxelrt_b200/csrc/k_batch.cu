@@ -21,7 +21,6 @@ static_assert(offsetof(JobDev, out) == offsetof(JobHost, rad16), "job table layo
 static_assert(offsetof(JobDev, W) == offsetof(JobHost, W), "job table layouts differ");
 static_assert(offsetof(JobDev, acc_prev) == offsetof(JobHost, acc_prev), "job table layouts differ");
 static_assert(offsetof(JobDev, acc_f32) == offsetof(JobHost, acc_f32), "job table layouts differ");
-static_assert(offsetof(JobDev, atrous_apart) == offsetof(JobHost, atrous_apart), "job table layouts differ");
 static_assert(offsetof(JobDev, cache) == offsetof(JobHost, cache), "job table layouts differ");
 
 // temporal.wgsl:17-77 over all jobs.
@@ -45,7 +44,7 @@ __global__ void __launch_bounds__(256) k_b_atrous(MultiJob J, uint32_t P, int it
   if (g >= P) return;
   const int j = J.job_of(g);
   const JobDev& jd = J.jobs[j];
-  if ((jd.u.params0[2] & 2u) == 0u || jd.atrous_apart) return;
+  if ((jd.u.params0[2] & 2u) == 0u) return;
   const int W = jd.W, H = jd.H;
   const uint32_t lp = g - jd.first;
   const int x = (int)(lp % (uint32_t)W), y = (int)(lp / (uint32_t)W);
@@ -75,7 +74,7 @@ __global__ void __launch_bounds__(256) k_b_atrous_tiled(MultiJob J, const uint32
     else hi = mid - 1;
   }
   const JobDev& jd = J.jobs[lo];
-  if ((jd.u.params0[2] & 2u) == 0u || jd.atrous_apart) return;
+  if ((jd.u.params0[2] & 2u) == 0u) return;
   const int W = jd.W, H = jd.H, step = 1 << it;
   const int tb = (int)(b - __ldg(tiles + lo)), tw = (W + 31) / 32;
   const int x0 = (tb % tw) * 32, y0 = (tb / tw) * kTY;
@@ -127,7 +126,7 @@ __global__ void __launch_bounds__(256) k_b_present(MultiJob J, uint32_t P, const
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
                                cudaStream_t st, uint32_t* launches, const float* present_lut, const CacheLaunch* cls,
-                               int ncl, const AtrousJob* aj, int naj, const AtrousTiles* at) {
+                               int ncl, const AtrousTiles* at) {
   MultiJob J;
   J.jobs = (const JobDev*)d_jobs;
   J.firsts = d_firsts;
@@ -155,18 +154,9 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
     } else {
       k_b_atrous<<<blocks, 256, 0, st>>>(J, P, it);
     }
-    // the chain accum -> dA -> dB -> dA (main.js:503-507) of the jobs apart
-    for (int k = 0; k < naj; k++) {
-      const AtrousJob& a = aj[k];
-      const void* src = it == 0 ? a.acc : (it == 1 ? a.den0 : a.den1);
-      void* dst = it == 1 ? a.den1 : a.den0;
-      if ((e = launch_atrous_staged(a.W, a.H, src, it == 0 && a.acc_f32 != 0, a.gbuf, dst, 1 << it,
-                                    stats ? stats + kStatError : nullptr, st)) != cudaSuccess)
-        return e;
-    }
   }
   k_b_present<<<blocks, 256, 0, st>>>(J, P, present_lut);
-  if (launches) *launches += 5 + 3u * (uint32_t)naj;
+  if (launches) *launches += 5;
   return cudaGetLastError();
 }
 

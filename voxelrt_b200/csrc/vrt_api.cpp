@@ -1211,19 +1211,12 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
   if (b->uploaded) CUDA_TRY(cudaEventSynchronize(b->ev_upload));
   uint32_t first = 0;
   std::vector<CacheLaunch> cls;
-  std::vector<AtrousJob> apart;
   const bool graph = b->use_graph && full;
   for (int i = 0; i < m; i++) {
     VrtSession* s = ss[(size_t)i];
     JobHost& j = b->h_jobs[i];
     std::memset(&j, 0, sizeof j);
     const int p = parity_of(s);
-    // large jobs of frames launched without a graph denoise through the staged a-trous kernel, each with
-    // its own launches (a graph would bake one frame's history parity into them)
-    if (!graph && (u[i].params0[2] & 2u) && (uint64_t)s->W * s->H >= kAtrousApartPixels) {
-      j.atrous_apart = 1;
-      apart.push_back(AtrousJob{s->W, s->H, s->accum[p], s->acc_f32 ? 1 : 0, s->gbuf[p], s->den[0], s->den[1]});
-    }
     j.u = u[i];
     j.vox = s->scene->dev.vox; j.masks = s->scene->dev.masks; j.bits = s->scene->dev.bits;
     j.N = s->scene->dev.N; j.BG = s->scene->dev.BG;
@@ -1266,7 +1259,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
       CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       uint32_t nl = 0;
       cudaError_t e = launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &nl,
-                                         b->ctx->present_lut, cls.data(), (int)cls.size(), nullptr, 0, &at);
+                                         b->ctx->present_lut, cls.data(), (int)cls.size(), &at);
       cudaError_t e2 = cudaStreamEndCapture(st, &graph);
       if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1287,8 +1280,7 @@ static int batch_frame_impl(VrtBatch* b, const int* idx, int m, const VrtUniform
     CUDA_TRY(cudaGraphLaunch(b->gexec, st));
   } else {
     CUDA_TRY(launch_batch_frame(b->d_jobs, b->d_firsts, m, P, waves, b->wf, b->tune, b->stats, st, &b->launches,
-                                b->ctx->present_lut, cls.data(), (int)cls.size(), apart.data(), (int)apart.size(),
-                                &at));
+                                b->ctx->present_lut, cls.data(), (int)cls.size(), &at));
   }
   CUDA_TRY(cudaEventRecord(b->ev_end, st));
   for (int i = 0; i < m; i++) {

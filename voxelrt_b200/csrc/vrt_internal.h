@@ -111,8 +111,7 @@ struct JobHost {
   void* den1;
   uint32_t* ldr;
   int acc_f32;
-  int atrous_apart;   // 1: the job's a-trous chain runs as its own staged launches (AtrousJob)
-  int pad[2];
+  int pad[3];
   CacheDev cache;
 };
 
@@ -124,21 +123,6 @@ struct AtrousTiles {
   uint32_t n16, n8;
 };
 
-// Batch jobs of at least this many pixels run their a-trous chain apart (below
-// it the per-launch cost outweighs the staged kernel's gain).
-constexpr uint64_t kAtrousApartPixels = 512 * 1024;
-
-// A batch job whose a-trous chain runs through the staged kernel with its own
-// launches (frames launched without a graph: the launches bake the job's
-// buffers in); the batch's per-pixel a-trous kernel skips it.
-struct AtrousJob {
-  int W, H;
-  const void* acc;    // this frame's history (the chain's input)
-  int acc_f32;
-  const void* gbuf;   // this frame's G-buffer
-  void* den0;
-  void* den1;
-};
 
 // Post-wave cache work of one job: its queries, network and training state.
 struct CacheLaunch {
@@ -165,8 +149,7 @@ struct CacheLaunch {
 cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int n, uint32_t P, int waves,
                                const WavefrontBufs& wb, const WavefrontTuning& tune, unsigned long long* stats,
                                cudaStream_t st, uint32_t* launches, const float* present_lut,
-                               const CacheLaunch* cls = nullptr, int ncl = 0, const AtrousJob* aj = nullptr,
-                               int naj = 0, const AtrousTiles* at = nullptr);
+                               const CacheLaunch* cls = nullptr, int ncl = 0, const AtrousTiles* at = nullptr);
 
 // Radiance-cache MLP kernels (k_mlp.cu).  q9: n x 9 floats (position in
 // metres, normal, albedo); y3: n x 3 target radiance; weights bf16 row-major.

@@ -292,8 +292,7 @@ struct JobDev {
   uint2* den1;
   uint32_t* ldr;
   int acc_f32;
-  int atrous_apart;        // 1: the job's a-trous chain runs as its own staged launches
-  int pad[2];
+  int pad[3];
   CacheDev cache;          // radiance cache of the job's session (cache.on == 0: plain path)
 };
 
