@@ -111,8 +111,9 @@ typedef struct VrtTuning {
                                  0: (8,5) default, 1: (6,5), 2: (6,4), 3: (4,4),
                                  4: (2,1), 5: (1,1); 6, 7, 8: (8,5) with the
                                  step loop unrolled 1, 2, 4 times (not 8)        */
-  int atrous_tile_rows;       /* a-trous output tile rows: 0 = 16 at steps 1-2
-                                 and 8 at step 4 (default), 8 = 8 at every step  */
+  int atrous_tile_rows;       /* a-trous output tile rows: 0 (default) or 8 = 8
+                                 at every step, 16 = 16 at steps 1-2 and 8 at
+                                 step 4                                          */
   int tail_wave;              /* first wave whose remaining paths each finish on
                                  one thread (their rays traced in turn, not in
                                  per-wave launches); 0 = never, -1 = automatic

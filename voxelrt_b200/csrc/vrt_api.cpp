@@ -529,11 +529,12 @@ int vrt_session_set_tuning(VrtSession* s, const VrtTuning* t) {
   if (!s || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
       t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 8 ||
-      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8) || t->tail_wave < -1 || t->tail_wave > 64)
+      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8 && t->atrous_tile_rows != 16) || t->tail_wave < -1 ||
+      t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   s->tune.refill_min = t->refill_min ? t->refill_min : 8;
   s->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
-  s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
+  s->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 32;
   s->tune.trace_variant = t->trace_variant;
   s->tune.atrous_rows = t->atrous_tile_rows;
   s->tune.tail_wave = t->tail_wave;
@@ -610,7 +611,7 @@ int vrt_session_autotune(VrtSession* s, const VrtUniforms* u, int frames, VrtTun
     if (int r = vrt_pass_temporal(s, u)) { s->tune = keep; return r; }
     float best_atrous = 1e30f;
     int best_rows = win.atrous_rows;
-    for (int rows : {0, 8}) {
+    for (int rows : {0, 16}) {
       s->tune.atrous_rows = rows;
       for (int it = 0; it < 3; it++)
         if (int r = vrt_pass_atrous(s, u, it)) { s->tune = keep; return r; }   // warm-up
@@ -1161,7 +1162,7 @@ int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
     return fail(VRT_ERR_INVALID, "tuning out of range");
   b->tune.refill_min = t->refill_min ? t->refill_min : 8;
   b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
-  b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 16;
+  b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 32;
   b->tune.trace_variant = t->trace_variant;
   b->tune.tail_wave = t->tail_wave;
   return VRT_OK;

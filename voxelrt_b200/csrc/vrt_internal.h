@@ -79,11 +79,11 @@ struct CacheDev {
 struct WavefrontTuning {
   int refill_min = 8;           // idle lanes that trigger a warp refill
   int trace_blocks_per_sm = 0;  // 0 = occupancy maximum
-  int shade_blocks_per_sm = 16;
+  int shade_blocks_per_sm = 32;
   int trace_variant = 0;        // (DDA iterations per warp-bookkeeping pass, min blocks/SM):
                                 // 0: (8, 5)  1: (6, 5)  2: (6, 4)  3: (4, 4)  4: (2, 1)  5: (1, 1);
                                 // 6, 7, 8: (8, 5) with the step loop unrolled 1, 2, 4 times
-  int atrous_rows = 0;          // a-trous output tile rows: 0 = 16 at steps 1-2 and 8 at step 4, 8 = 8 at all steps
+  int atrous_rows = 0;          // a-trous output tile rows: 0 or 8 = 8 at all steps, 16 = 16 at steps 1-2 and 8 at step 4
   int tail_wave = -1;           // first wave whose paths finish one thread each (k_wf_tail); 0 = never;
                                 // -1 = automatic: wave 2 for cache-assisted frames (a session's, or a
                                 // batch's whose every job has the cache on), else never

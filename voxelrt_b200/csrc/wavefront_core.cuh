@@ -1199,7 +1199,7 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
   if (e != cudaSuccess) return e;
   const int sms = wf_sm_count();
   const int refill = tune.refill_min > 0 ? tune.refill_min : 8;
-  const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 16);
+  const int sblocks = sms * (tune.shade_blocks_per_sm > 0 ? tune.shade_blocks_per_sm : 32);
   uint32_t nl = 0;
   k_wf_generate<J><<<(P + 255) / 256, 256, 0, st>>>(jobs, P, b);
   nl++;
