@@ -142,9 +142,9 @@ cudaError_t launch_batch_frame(const void* d_jobs, const uint32_t* d_firsts, int
   const unsigned blocks = (P + 255) / 256;
   k_b_temporal<<<blocks, 256, 0, st>>>(J, P);
   for (int it = 0; it < 3; it++) {
-    if (at && at->d16) {   // shared-memory tiles: 32 x 16 at steps 1-2, 32 x 8 at step 4
+    if (at && at->d16) {   // shared-memory tiles: 32 x 8 (tile rows 16: 32 x 16 at steps 1-2)
       const int step = 1 << it, hx = 2 * step;
-      if (it < 2) {
+      if (it < 2 && tune.atrous_rows == 16) {
         const int smem = (32 + 2 * hx) * (16 + 2 * hx) * 32;
         k_b_atrous_tiled<16><<<at->n16, 256, smem, st>>>(J, at->d16, it);
       } else {

@@ -1158,9 +1158,11 @@ int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
   if (!b || !t) return fail(VRT_ERR_INVALID, "NULL argument");
   if (t->refill_min < 0 || t->refill_min > 32 || t->trace_blocks_per_sm < 0 || t->trace_blocks_per_sm > 32 ||
       t->shade_blocks_per_sm < 0 || t->shade_blocks_per_sm > 64 || t->trace_variant < 0 || t->trace_variant > 8 ||
-      t->tail_wave < -1 || t->tail_wave > 64)
+      (t->atrous_tile_rows != 0 && t->atrous_tile_rows != 8 && t->atrous_tile_rows != 16) || t->tail_wave < -1 ||
+      t->tail_wave > 64)
     return fail(VRT_ERR_INVALID, "tuning out of range");
   b->tune.refill_min = t->refill_min ? t->refill_min : 8;
+  b->tune.atrous_rows = t->atrous_tile_rows;
   b->tune.trace_blocks_per_sm = t->trace_blocks_per_sm;
   b->tune.shade_blocks_per_sm = t->shade_blocks_per_sm ? t->shade_blocks_per_sm : 32;
   b->tune.trace_variant = t->trace_variant;
@@ -1171,7 +1173,7 @@ int vrt_batch_set_tuning(VrtBatch* b, const VrtTuning* t) {
 static bool same_tuning(const WavefrontTuning& a, const WavefrontTuning& c) {
   return a.refill_min == c.refill_min && a.trace_blocks_per_sm == c.trace_blocks_per_sm &&
          a.shade_blocks_per_sm == c.shade_blocks_per_sm && a.trace_variant == c.trace_variant &&
-         a.tail_wave == c.tail_wave;
+         a.tail_wave == c.tail_wave && a.atrous_rows == c.atrous_rows;
 }
 
 }  // extern "C"
@@ -1379,6 +1381,21 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
     std::sort(ms.begin(), ms.end());
     if (ms[(size_t)frames / 2] < win_ms) { win_ms = ms[(size_t)frames / 2]; win = b->tune; }
   }
+  // the a-trous tile rows (8 at every step, or 16 at steps 1-2)
+  {
+    b->tune = win;
+    b->tune.atrous_rows = win.atrous_rows == 16 ? 0 : 16;
+    int r = vrt_batch_frame(b, u);
+    for (int f = 0; f < frames && !r; f++) {
+      r = vrt_batch_frame(b, u);
+      VrtFrameStats st;
+      if (!r) r = vrt_batch_last_stats(b, &st);
+      ms[(size_t)f] = st.ms_total;
+    }
+    if (r) { b->tune = keep; b->use_graph = keep_graph; return r; }
+    std::sort(ms.begin(), ms.end());
+    if (ms[(size_t)frames / 2] < win_ms) { win_ms = ms[(size_t)frames / 2]; win = b->tune; }
+  }
   b->tune = win;
   b->use_graph = keep_graph;
   batch_drop_graph(b);
@@ -1387,7 +1404,7 @@ int vrt_batch_autotune(VrtBatch* b, const VrtUniforms* u, int frames, VrtTuning*
     best->trace_blocks_per_sm = win.trace_blocks_per_sm;
     best->shade_blocks_per_sm = win.shade_blocks_per_sm;
     best->trace_variant = win.trace_variant;
-    best->atrous_tile_rows = 0;   // batch frames run the unstaged a-trous kernel over all jobs
+    best->atrous_tile_rows = win.atrous_rows;
     best->tail_wave = win.tail_wave;
   }
   if (best_ms) *best_ms = win_ms;
