@@ -1106,6 +1106,10 @@ static int batch_create_capacity(VrtCtx* ctx, VrtSession* const* sessions, int n
   if (int r = set_dev(ctx)) return r;
   VrtBatch* b = new VrtBatch();
   b->ctx = ctx;
+  // batch default launch shape: the tracer variant that holds its walk in registers for the batch's
+  // job lookups (6 steps per pass, 4 blocks per SM; the 8 x 5 shape spills there), refill at 16 idle lanes
+  b->tune.trace_variant = 2;
+  b->tune.refill_min = 16;
   if (sessions) b->sessions.assign(sessions, sessions + n);
   else b->sessions.assign((size_t)n, nullptr);
   b->P = (uint32_t)P;

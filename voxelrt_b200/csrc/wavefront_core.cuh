@@ -267,6 +267,7 @@ struct SingleJob {
   __host__ __device__ bool any_cache() const { return cc.on != 0; }
   VRT_DI const CacheDev& cache(int) const { return cc; }
   VRT_DI int job_of(uint32_t) const { return 0; }
+  VRT_DI int job_of_cached(uint32_t, int&, uint32_t&, uint32_t&) const { return 0; }
   VRT_DI const Uni& uni(int) const { return u; }
   VRT_DI DScene scene(int) const { return S; }
   VRT_DI JobOut outs(int) const { return out; }
@@ -313,6 +314,14 @@ struct MultiJob {
       else hi = mid - 1;
     }
     return lo;
+  }
+  // job_of with the caller's last answer (job jc for pixels [lo, hi)) tried first
+  VRT_DI int job_of_cached(uint32_t g, int& jc, uint32_t& lo, uint32_t& hi) const {
+    if (g - lo < hi - lo) return jc;
+    jc = job_of(g);
+    lo = __ldg(firsts + jc);
+    hi = jc + 1 < n ? __ldg(firsts + jc + 1) : 0xffffffffu;
+    return jc;
   }
   VRT_DI const Uni& uni(int j) const { return jobs[j].u; }
   VRT_DI DScene scene(int j) const { return jobs[j].S; }
@@ -668,6 +677,8 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
   DScene S = jobs.scene(0);
   F3 rd = f3(0.0f, 0.0f, 0.0f);
   uint32_t entry = 0u;
+  int jc = 0;                     // the lane's last job and its pixel range (empty: none yet)
+  uint32_t jlo = 1u, jhi = 0u;
   uint32_t passes = 0u;   // passes of the step loop with a lane walking (warp-uniform)
   bool active = false, drained = false;
   while (true) {
@@ -684,13 +695,14 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
           entry = implicit_n > 0 ? (uint32_t)slot
                                  : (slot < nf ? queue[slot] : queue[b.qcap - 1u - (uint32_t)(slot - nf)]);
           const uint32_t g = entry & ~kShadowBit;
-          S = jobs.scene(jobs.job_of(g));
+          const int j = jobs.job_of_cached(g, jc, jlo, jhi);   // consecutive rays mostly share a job
+          S = jobs.scene(j);
           // primary rays start at the camera: its position comes from the job's
           // uniforms (k_wf_generate writes no R0, so no wave-0 shading kernel
           // may read R0 either); later waves read the origin their shading stored
           F3 ro;
           if (implicit_n > 0) {
-            const Uni& uj = jobs.uni(jobs.job_of(g));
+            const Uni& uj = jobs.uni(j);
             ro = f3(uj.camPos[0], uj.camPos[1], uj.camPos[2]);
           } else {
             ro = xyz(b.R0[g]);
