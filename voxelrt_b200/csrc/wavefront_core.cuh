@@ -315,7 +315,8 @@ struct MultiJob {
     }
     return lo;
   }
-  // job_of with the caller's last answer (job jc for pixels [lo, hi)) tried first
+  // job_of with the caller's last answer (job jc for pixels [lo, hi), lo <= hi; lo == hi: none)
+  // tried first
   VRT_DI int job_of_cached(uint32_t g, int& jc, uint32_t& lo, uint32_t& hi) const {
     if (g - lo < hi - lo) return jc;
     jc = job_of(g);
@@ -677,8 +678,8 @@ __global__ void __launch_bounds__(256, kMinB) k_wf_trace(J jobs, WfDev b, int wa
   DScene S = jobs.scene(0);
   F3 rd = f3(0.0f, 0.0f, 0.0f);
   uint32_t entry = 0u;
-  int jc = 0;                     // the lane's last job and its pixel range (empty: none yet)
-  uint32_t jlo = 1u, jhi = 0u;
+  int jc = 0;                     // the lane's last job and its pixel range [jlo, jhi) (empty: none yet)
+  uint32_t jlo = 0u, jhi = 0u;
   uint32_t passes = 0u;   // passes of the step loop with a lane walking (warp-uniform)
   bool active = false, drained = false;
   while (true) {
