@@ -520,17 +520,21 @@ __global__ void __launch_bounds__(256, 2) k_mlp_infer(const __grid_constant__ Ml
     // stage both tiles, then start both first layers (one barrier for the pair: 65.0 -> 63.1 us for 983 K
     // queries; a barrier per tile within the layers is kept -- unpacking both tiles of a layer before one
     // barrier ran 70.0 us, the tensor core then waits for both epilogues)
+    // the group's last pair may hold one tile only (its second lies past the
+    // queries): then the second tile is neither staged nor computed
+    const int nu = pt + vctas < tiles ? 2 : 1;
     stage_query(smem + X[0], t, qq[0], idx[0] < n, tk.extent);
-    stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
+    if (nu == 2) stage_query(smem + X[1], t, qq[1], idx[1] < n, tk.extent);
     ok = group_publish_and(g, ok);
     if (!ok) break;
     issue(0, 0);
-    issue(1, 0);
+    if (nu == 2) issue(1, 0);
     fetch(pt + stride);                    // the next pair's queries, in flight during this pair
 #pragma unroll 1
     for (int l = 0; l < 4 && ok; l++) {
 #pragma unroll
       for (int u = 0; u < 2; u++) {
+        if (u >= nu) continue;
         wait(u);
         if (l < 3) {
           float h[kHid];
