@@ -84,10 +84,8 @@ cudaError_t launch_wavefront(const SceneDev& s, const VrtUniforms& uu, float fcl
   // (wave 1), so by default the few paths left after it run to their end one
   // thread each
   const int tail = tune.tail_wave >= 0 ? tune.tail_wave : (job.cc.on ? 2 : 0);
-  // the paths that can remain for the tail: the training paths of a cache frame, else every pixel's
-  const uint32_t tail_paths = job.cc.on ? (uint32_t)job.cc.TW * (uint32_t)((H + 3) / 4) : (uint32_t)(W * H);
   cudaError_t e = wf_launch_frame(job, (uint32_t)(W * H), waves, smem, wb, tune, out.stats, st, launches, trace_ev,
-                                  max_timed_waves, timed_waves, 1, tail, tail_paths);
+                                  max_timed_waves, timed_waves, 1, tail);
   if (e != cudaSuccess || !job.cc.on) return e;
   if (cache_ev && (e = cudaEventRecord(cache_ev[0], st)) != cudaSuccess) return e;
   e = launch_cache_post(job, wf_view(wb), cache, 1, out.stats, st, launches);

@@ -909,7 +909,6 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
 template <class J, bool kSmem>
 __global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
-  if ((int)(blockIdx.x * blockDim.x) >= b.ctr[4 * wave + 2]) return;   // no path for this block
   if (kSmem) {
     const DScene S0 = jobs.scene(0);
     const int nwords = (S0.BG * S0.BG * S0.BG + 31) >> 5;
@@ -1206,7 +1205,7 @@ template <class J, class ShadeFn, bool kVarMaxT = false>
 cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                          const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st, uint32_t* launches,
                          cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves, ShadeFn shade,
-                         int tail_from = 0, uint32_t tail_paths = 0) {
+                         int tail_from = 0) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   const WfDev b = wf_view(wb);
   cudaError_t e = cudaMemsetAsync(wb.ctr, 0, (size_t)wb.max_waves * 16, st);
@@ -1220,12 +1219,7 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
   int timed = 0;
   for (int w = 0; w < waves; w++) {
     if (tail_from > 0 && w == tail_from) {   // the remaining paths, one thread each
-      // one block per 256 of the paths that can remain (tail_paths, when known and at most 12
-      // blocks per SM): blocks that finish early make room for the rest, where a resident grid
-      // would start a block's second round only after its slowest path; else a resident grid
-      int tblocks = sms * 3;
-      const uint32_t nb = (tail_paths + 255u) / 256u;
-      if (tail_paths > 0 && nb <= (uint32_t)(sms * 12)) tblocks = std::max(tblocks, (int)nb);
+      const int tblocks = sms * 3;
       if (smem > 0) {
         e = cudaFuncSetAttribute(k_wf_tail<J, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess) k_wf_tail<J, true><<<tblocks, 256, smem, st>>>(jobs, b, w, stats);
@@ -1262,7 +1256,7 @@ template <class J>
 cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
                             const WavefrontTuning& tune, unsigned long long* stats, cudaStream_t st,
                             uint32_t* launches, cudaEvent_t* trace_ev, int max_timed_waves, int* timed_waves,
-                            int njobs = 1, int tail_from = 0, uint32_t tail_paths = 0) {
+                            int njobs = 1, int tail_from = 0) {
   if (waves + 1 > wb.max_waves) return cudaErrorInvalidValue;
   if (jobs.any_cache()) {
     k_cache_reset<J><<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
@@ -1273,7 +1267,7 @@ cudaError_t wf_launch_frame(const J& jobs, uint32_t P, int waves, int smem, cons
                         if (w == 0) k_wf_shade_primary<J><<<sblocks, 256, 0, st>>>(jobs, P, b, stats);
                         else k_wf_shade<J><<<sblocks, 256, 0, st>>>(jobs, b, w);
                         return cudaGetLastError();
-                      }, tail_from, tail_paths);
+                      }, tail_from);
 }
 
 }  // namespace vrt
