@@ -1201,7 +1201,7 @@ cudaError_t wf_dispatch_trace(int variant, const J& jobs, int smem, int tb, int 
 // Launches generate + (trace, shade) x waves; shade(b, w, blocks) launches
 // the shading kernel of wave w.  smem > 0 selects the shared-memory bitmap
 // tracer (single scene only).
-constexpr int kPrimaryRefill = 24;   // idle lanes that trigger a refill in the primary wave (at least)
+constexpr int kPrimaryRefill = 32;   // idle lanes that trigger a refill in the primary wave (at least)
 
 template <class J, class ShadeFn, bool kVarMaxT = false>
 cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const WavefrontBufs& wb,
@@ -1238,8 +1238,9 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
     if (tm && (e = cudaEventRecord(trace_ev[2 * w], st)) != cudaSuccess) return e;
     const int impl = w == 0 ? (int)P : 0;
     const int tb = tune.trace_blocks_per_sm;
-    // the coherent primary rays refill later: at 24 idle lanes the 1080p primary wave took 277 us against
-    // 299 at 8, while the later waves are fastest at 8 (490 / 426 / 143 us against 530 / 479 / 153 at 24)
+    // the coherent primary rays refill later: the 1080p primary wave took 299 / 290 / 285 / 277 / 271 us at
+    // 8 / 12 / 16 / 24 / 32 idle lanes (32: only whole warps refill), while the later waves are fastest at 8
+    // (490 / 426 / 143 us against 530 / 479 / 153 at 24)
     const int rf = w == 0 ? std::max(refill, kPrimaryRefill) : refill;
     if (smem > 0)
       e = wf_dispatch_trace<J, true, kVarMaxT>(tune.trace_variant, jobs, smem, tb, sms, b, w, impl, rf, stats, st);
