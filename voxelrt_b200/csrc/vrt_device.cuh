@@ -343,8 +343,8 @@ VRT_DI void block_flush_stats(unsigned long long* stats, const DCount& c, uint32
   __syncthreads();
   if (threadIdx.x < 5) {
     unsigned long long tot = 0ull;
-#pragma unroll
-    for (int q = 0; q < 8; q++) tot += s_part[q][threadIdx.x];
+    const int nw = (int)(blockDim.x >> 5);   // blocks of up to 256 threads
+    for (int q = 0; q < nw; q++) tot += s_part[q][threadIdx.x];
     if (tot) atomicAdd(stats + threadIdx.x, tot);
   }
 }

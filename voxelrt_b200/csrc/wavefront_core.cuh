@@ -400,8 +400,8 @@ VRT_DI uint32_t block_append1(int* ctr, int n) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int tot = 0;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
+    const int nw = (int)(blockDim.x >> 5);   // blocks of up to 256 threads
+    for (int k = 0; k < nw; k++) {
       const int v = s_cnt[k];
       s_cnt[k] = tot;
       tot += v;
@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(256, 5) k_wf_shade(J jobs, WfDev b, int wave) 
 // against 305 us per 1080p cache frame: some lane shades in nearly every pass,
 // so the warp runs the shading code far more often than once per bounce.)
 template <class J, bool kSmem>
-__global__ void __launch_bounds__(256, 3) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
+__global__ void __launch_bounds__(128, 6) k_wf_tail(J jobs, WfDev b, int wave, unsigned long long* stats) {
   extern __shared__ uint32_t s_occ[];
   if (kSmem) {
     const DScene S0 = jobs.scene(0);
@@ -1223,12 +1223,12 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
     if (tail_from > 0 && w == tail_from) {   // the remaining paths, one thread each
       // a resident grid (a grid of one block per 256 training paths, blocks without paths returning at
       // once, measured 291 against 282 us per 1080p cache frame)
-      const int tblocks = sms * 3;
+      const int tblocks = sms * 6;
       if (smem > 0) {
         e = cudaFuncSetAttribute(k_wf_tail<J, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess) k_wf_tail<J, true><<<tblocks, 256, smem, st>>>(jobs, b, w, stats);
+        if (e == cudaSuccess) k_wf_tail<J, true><<<tblocks, 128, smem, st>>>(jobs, b, w, stats);
       } else {
-        k_wf_tail<J, false><<<tblocks, 256, 0, st>>>(jobs, b, w, stats);
+        k_wf_tail<J, false><<<tblocks, 128, 0, st>>>(jobs, b, w, stats);
       }
       if (e != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return e;
       nl++;
