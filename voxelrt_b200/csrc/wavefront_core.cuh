@@ -1221,8 +1221,9 @@ cudaError_t wf_run_waves(const J& jobs, uint32_t P, int waves, int smem, const W
   int timed = 0;
   for (int w = 0; w < waves; w++) {
     if (tail_from > 0 && w == tail_from) {   // the remaining paths, one thread each
-      // a resident grid (a grid of one block per 256 training paths, blocks without paths returning at
-      // once, measured 291 against 282 us per 1080p cache frame)
+      // a resident grid of 128-thread blocks: 260 us per 1080p cache frame against 282 with 256-thread
+      // blocks (a block's round waits for its slowest path) and 262 with 64; a grid of one block per 256
+      // training paths, blocks without paths returning at once, ran 291
       const int tblocks = sms * 6;
       if (smem > 0) {
         e = cudaFuncSetAttribute(k_wf_tail<J, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
