@@ -48,7 +48,8 @@ def parse_args():
                     help="frame mode: skip the plain vs batched+cache comparison in the output line")
     ap.add_argument("--path-kernel", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--mode", default="frame", choices=["frame", "batched", "serve", "cache", "cache-frame", "lights",
-                                                        "restir", "restir-scenes", "voxelbench", "correctness"],
+                                                        "restir", "restir-scenes", "voxelbench", "correctness",
+                                                        "wave-sweep"],
                     help="frame: the full-size plain frame (default); batched: 64 mixed jobs in one launch; "
                          "serve: Poisson request stream over 32 sessions; cache: cache-assisted vs plain "
                          "path tracing at matched MSE; restir: the ReSTIR presets beside the plain frame; "
@@ -645,6 +646,33 @@ def cache_quality(vrt, ctx, scene, spawn, W, H, ref, bounces, cache, warm, K):
     var = max(m1 - mk, 0.0) * K / (K - 1)
     return {"mse_1spp": round(m1, 6), f"mse_{K}frame_mean": round(mk, 6), "var": round(var, 6),
             "bias2": round(mk - var / K, 7)}
+
+
+def run_wave_sweep(args, local):
+    """The bench frame (1080p / 256^3 / 2 bounces) at each refill threshold
+    (4, 8, 12, 16, 24, 32 idle lanes) and then each tracer variant (0, 1, 2,
+    3, 7), five frames per setting in that order: a command for per-wave launch
+    lists (`ncu --metrics gpu__time_duration.sum -k regex:k_wf_trace`); the
+    images do not depend on the settings."""
+    import torch
+
+    import voxelrt_b200 as vrt
+    torch.cuda.set_device(local)
+    n, W, H = WORKLOAD["n"], WORKLOAD["W"], WORKLOAD["H"]
+    vox, spawn = vrt.generate_scene(WORKLOAD["kind"], n, WORKLOAD["seed"])
+    ctx = vrt.Context(local)
+    sc = vrt.Scene(ctx, vox, n)
+    s = vrt.Session(ctx, sc, W, H, firefly_clamp=WORKLOAD["fclamp"])
+    settings = [dict(refill_min=r) for r in (4, 8, 12, 16, 24, 32)] + [dict(trace_variant=v) for v in (0, 1, 2, 3, 7)]
+    for st in settings:
+        s.set_tuning(**st)
+        for i in range(5):
+            s.frame(frame_uniforms(vrt, spawn, 10 + i))
+        ctx.synchronize()
+    print(json.dumps({"mode": "wave-sweep", "settings": settings, "frames_per_setting": 5}), flush=True)
+    s.close()
+    sc.close()
+    ctx.close()
 
 
 def run_cache_frame(args, local):
@@ -1728,6 +1756,9 @@ def main():
     elif args.mode == "cache-frame":
         if rank == 0:
             run_cache_frame(args, local)
+    elif args.mode == "wave-sweep":
+        if rank == 0:
+            run_wave_sweep(args, local)
     elif args.mode == "lights":
         if rank == 0:
             run_lights(args, local)
