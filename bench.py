@@ -55,7 +55,9 @@ def parse_args():
                          "path tracing at matched MSE; restir: the ReSTIR presets beside the plain frame; "
                          "restir-scenes: `ours` on the reference's own scenarios with its capture settings; "
                          "correctness: the reference's estimator-correctness captures against its recorded "
-                         "channel means and HDR errors")
+                         "channel means and HDR errors; cache-frame: one cache-assisted 1080p frame (for "
+                         "profiling); wave-sweep: the plain frame over refill thresholds and tracer variants "
+                         "(for per-wave launch lists)")
     ap.add_argument("--rates", default="200,500,1000,2000", help="serve: arrival rates (requests/s)")
     ap.add_argument("--duration", type=float, default=1.5, help="serve: seconds of arrivals per rate")
     ap.add_argument("--jobs", type=int, default=64)
